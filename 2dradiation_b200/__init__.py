@@ -1,0 +1,288 @@
+"""Python harness over the C-ABI of libgrlbm.so (include/grlbm.h).
+
+The product is the shared library built from ``csrc/`` (host set-up in C++,
+kernels and C-ABI in CUDA for sm_100a).  This module is the thin ctypes layer
+the tests and the benchmark drive it with; it mirrors the reference's
+``Radiation`` workflow (src/Radiation.h): construct, write the public input
+buffers, ``LoadInitialData``, ``UpdateFourierCoefficients``, then time steps.
+
+There is no CPU fallback: if ``libgrlbm.so`` is missing or no GPU is usable,
+the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import importlib
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "libgrlbm.so"
+
+workloads = importlib.import_module(__name__ + ".workloads")
+
+OK = 0
+ERRORS = {1: "ARGUMENT", 2: "CUDA", 3: "STATE", 4: "UNSUPPORTED", 5: "NONCONVERGED", 6: "HOST"}
+MINKOWSKI, SCHWARZSCHILD, KERRSCHILD = 0, 1, 2
+FLAT_FIXED, FLAT_ADAPTIVE, CURVED_FIXED, CURVED_ADAPTIVE, GEODESIC_FIXED = 0, 1, 2, 3, 4
+MOMENTS, INTENSITIES = 0, 1
+PLAIN_FP64, PRECISION_FP32 = 0, 1
+
+
+class GrlbmError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"grlbm error {code} ({ERRORS.get(code, '?')}): {msg}")
+        self.code = code
+
+
+class GridDesc(C.Structure):
+    _fields_ = [("nx_", C.c_int64), ("ny_", C.c_int64), ("startx", C.c_double), ("starty", C.c_double),
+                ("endx", C.c_double), ("endy", C.c_double), ("cfl", C.c_double)]
+
+
+class MetricDesc(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("m", C.c_double), ("a", C.c_double), ("excision", C.c_double)]
+
+
+class RunDesc(C.Structure):
+    _fields_ = [("n_dir", C.c_int32), ("n_fourier", C.c_int32), ("streaming_type", C.c_int32),
+                ("precision", C.c_int32), ("keep_source_nodes_active", C.c_int32),
+                ("initial_data_type", C.c_int32)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("steps", C.c_int64), ("max_iterations", C.c_int32), ("average_iterations", C.c_double),
+                ("rk_substeps", C.c_int64), ("rk_nonconverged", C.c_int32), ("table_ms", C.c_double)]
+
+
+_D = C.POINTER(C.c_double)
+_lib = None
+
+# Every entry point of include/grlbm.h with its argument types.
+SIGNATURES = {
+    "grlbm_create": ([C.POINTER(GridDesc), C.POINTER(MetricDesc), C.POINTER(RunDesc), C.c_int32,
+                      C.POINTER(C.c_void_p)], C.c_int),
+    "grlbm_destroy": ([C.c_void_p], None),
+    "grlbm_last_error": ([C.c_void_p], C.c_char_p),
+    "grlbm_get_grid": ([C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64), _D, _D, _D], C.c_int),
+    "grlbm_set_fields": ([C.c_void_p] + [_D] * 6, C.c_int),
+    "grlbm_set_initial_data": ([C.c_void_p, C.POINTER(C.c_uint8)] + [_D] * 7, C.c_int),
+    "grlbm_load_initial_data": ([C.c_void_p], C.c_int),
+    "grlbm_set_intensity": ([C.c_void_p, _D], C.c_int),
+    "grlbm_get_intensity": ([C.c_void_p, _D], C.c_int),
+    "grlbm_update_fourier_coefficients": ([C.c_void_p, C.c_double, C.c_int32], C.c_int),
+    "grlbm_get_fourier_coefficients": ([C.c_void_p] + [_D] * 5, C.c_int),
+    "grlbm_step": ([C.c_void_p, C.c_int32], C.c_int),
+    "grlbm_step_async": ([C.c_void_p, C.c_int32], C.c_int),
+    "grlbm_sync": ([C.c_void_p], C.c_int),
+    "grlbm_stream": ([C.c_void_p], C.c_void_p),
+    "grlbm_get_moments_if": ([C.c_void_p] + [_D] * 6, C.c_int),
+    "grlbm_compute_moments_lf": ([C.c_void_p] + [_D] * 7, C.c_int),
+    "grlbm_energy": ([C.c_void_p, _D], C.c_int),
+    "grlbm_get_stats": ([C.c_void_p, C.POINTER(Stats)], C.c_int),
+    "grlbm_host_stencil": ([C.c_int32, C.c_int32, _D, _D, _D, _D, C.POINTER(C.c_int64), _D], C.c_int),
+    "grlbm_host_flux_table": ([C.c_int32, C.POINTER(C.c_int32), _D, _D, _D, C.c_int32], C.c_int),
+    "grlbm_host_metric_arrays": ([C.POINTER(GridDesc), C.POINTER(MetricDesc), _D], C.c_int),
+    "grlbm_metric_array_count": ([], C.c_int32),
+}
+
+
+def lib() -> C.CDLL:
+    """Load libgrlbm.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise FileNotFoundError(f"{LIB_PATH} is missing: run __graft_entry__.build()")
+        L = C.CDLL(str(LIB_PATH))
+        for name, (args, res) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(_D)
+
+
+def _check(rc: int, ctx=None):
+    if rc != OK:
+        msg = lib().grlbm_last_error(ctx)
+        raise GrlbmError(rc, msg.decode() if msg else "")
+
+
+def grid_desc(case: dict) -> GridDesc:
+    return GridDesc(int(case["nx_"]), int(case["ny_"]), case["start"][0], case["start"][1],
+                    case["end"][0], case["end"][1], case["cfl"])
+
+
+def metric_desc(case: dict) -> MetricDesc:
+    return MetricDesc(int(case["metric_kind"]), case["m"], case["a"], case["excision"])
+
+
+# ------------------------------------------------------------- host helpers
+def host_stencil(n: int, intensity: bool = True) -> dict:
+    out = {k: np.zeros(n) for k in ("w", "phi", "cx", "cy")}
+    ng = 10 * n if intensity else 0
+    idx = np.zeros(max(4 * ng, 1), dtype=np.int64)
+    wt = np.zeros(max(4 * ng, 1))
+    _check(lib().grlbm_host_stencil(n, int(intensity), _p(out["w"]), _p(out["phi"]), _p(out["cx"]),
+                                    _p(out["cy"]), idx.ctypes.data_as(C.POINTER(C.c_int64)), _p(wt)))
+    out["ig_index"], out["ig_weight"] = idx[:4 * ng], wt[:4 * ng]
+    return out
+
+
+def host_flux_table(n: int) -> dict:
+    size = C.c_int32(0)
+    _check(lib().grlbm_host_flux_table(n, C.byref(size), None, None, None, 0))
+    k = size.value
+    a, s, z = np.zeros(k), np.zeros(k), np.zeros(k)
+    _check(lib().grlbm_host_flux_table(n, C.byref(size), _p(a), _p(s), _p(z), k))
+    return {"inputs": a, "sigma": s, "normalization": z}
+
+
+def host_metric_arrays(case: dict) -> np.ndarray:
+    nxy = workloads.nxy(case)
+    n = lib().grlbm_metric_array_count()
+    out = np.zeros(n * nxy)
+    g, m = grid_desc(case), metric_desc(case)
+    _check(lib().grlbm_host_metric_arrays(C.byref(g), C.byref(m), _p(out)))
+    return out.reshape(n, nxy)
+
+
+# ------------------------------------------------------------------ solver
+class Radiation:
+    """One problem resident on the GPU (a grlbm_ctx)."""
+
+    def __init__(self, case: dict, precision: int = PLAIN_FP64, device: int = -1):
+        self.case = case
+        self.nd = int(case["n_dir"])
+        self.nf = int(case["n_fourier"])
+        g, m = grid_desc(case), metric_desc(case)
+        r = RunDesc(self.nd, self.nf, int(case["streaming_type"]), precision,
+                    int(case["keep_source_nodes_active"]), int(case["initial_data_type"]))
+        h = C.c_void_p()
+        _check(lib().grlbm_create(C.byref(g), C.byref(m), C.byref(r), device, C.byref(h)))
+        self.h = h
+        nx, ny = C.c_int64(), C.c_int64()
+        dx, dy, dt = C.c_double(), C.c_double(), C.c_double()
+        _check(lib().grlbm_get_grid(h, C.byref(nx), C.byref(ny), C.byref(dx), C.byref(dy), C.byref(dt)), h)
+        self.nx, self.ny, self.dx, self.dy, self.dt = nx.value, ny.value, dx.value, dy.value, dt.value
+        self.nxy = self.nx * self.ny
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().grlbm_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _c(self, rc):
+        _check(rc, self.h)
+
+    @property
+    def stream(self) -> int:
+        return lib().grlbm_stream(self.h) or 0
+
+    def set_fields(self, f: dict):
+        arr = [np.ascontiguousarray(f[k], dtype=np.float64) for k in ("kappa0", "kappa1", "kappaA", "eta", "ux", "uy")]
+        self._c(lib().grlbm_set_fields(self.h, *[_p(a) for a in arr]))
+
+    def set_initial_data(self, f: dict):
+        mask = np.ascontiguousarray(f["is_initial"], dtype=np.uint8)
+        arr = [np.ascontiguousarray(f[k], dtype=np.float64) for k in
+               ("initial_I", "initial_E_LF", "initial_Fx_LF", "initial_Fy_LF", "initial_Pxx_LF",
+                "initial_Pxy_LF", "initial_Pyy_LF")]
+        self._c(lib().grlbm_set_initial_data(self.h, mask.ctypes.data_as(C.POINTER(C.c_uint8)),
+                                             *[_p(a) for a in arr]))
+
+    def load_initial_data(self):
+        self._c(lib().grlbm_load_initial_data(self.h))
+
+    def set_intensity(self, I: np.ndarray):
+        I = np.ascontiguousarray(I, dtype=np.float64).reshape(-1)
+        assert I.size == self.nxy * self.nd
+        self._c(lib().grlbm_set_intensity(self.h, _p(I)))
+
+    def intensity(self) -> np.ndarray:
+        out = np.zeros(self.nxy * self.nd)
+        self._c(lib().grlbm_get_intensity(self.h, _p(out)))
+        return out
+
+    def update_fourier_coefficients(self, rk_tol: float, max_substeps: int = 0):
+        self._c(lib().grlbm_update_fourier_coefficients(self.h, rk_tol, max_substeps))
+
+    def coefficients(self) -> dict:
+        out = {k: np.zeros(self.nxy * self.nf) for k in ("coefS", "coefX", "coefY", "coefCx", "coefCy")}
+        self._c(lib().grlbm_get_fourier_coefficients(self.h, *[_p(out[k]) for k in
+                                                               ("coefS", "coefX", "coefY", "coefCx", "coefCy")]))
+        return out
+
+    def step(self, n: int):
+        self._c(lib().grlbm_step(self.h, n))
+
+    def step_async(self, n: int):
+        self._c(lib().grlbm_step_async(self.h, n))
+
+    def sync(self):
+        self._c(lib().grlbm_sync(self.h))
+
+    def moments_if(self, out: dict | None = None) -> dict:
+        names = ("E", "Fx", "Fy", "Pxx", "Pxy", "Pyy")
+        out = out if out is not None else {k: np.zeros(self.nxy) for k in names}
+        self._c(lib().grlbm_get_moments_if(self.h, *[_p(out[k]) for k in names]))
+        return out
+
+    def moments_lf(self) -> dict:
+        names = ("E_LF", "Fx_LF", "Fy_LF", "Pxx_LF", "Pxy_LF", "Pyy_LF", "F_LF")
+        out = {k: np.zeros(self.nxy) for k in names}
+        self._c(lib().grlbm_compute_moments_lf(self.h, *[_p(out[k]) for k in names]))
+        return out
+
+    def energy(self) -> float:
+        v = C.c_double()
+        self._c(lib().grlbm_energy(self.h, C.byref(v)))
+        return v.value
+
+    def stats(self) -> dict:
+        s = Stats()
+        self._c(lib().grlbm_get_stats(self.h, C.byref(s)))
+        return {k: getattr(s, k) for k, _ in Stats._fields_}
+
+
+def prepare(case: dict, precision: int = PLAIN_FP64, device: int = -1) -> Radiation:
+    """Construct and load a case the way RunSimulation starts
+    (src/Radiation.cpp:745-746): inputs, LoadInitialData, then the geodesic
+    tables."""
+    r = Radiation(case, precision, device)
+    r.set_fields(case["fields"])
+    r.set_initial_data(case["fields"])
+    r.load_initial_data()
+    r.update_fourier_coefficients(case["rk_tol"])
+    return r
+
+
+def run(case: dict, precision: int = PLAIN_FP64, steps: int | None = None) -> dict:
+    """Whole run of a case; returns the same keys as the oracle's run()."""
+    with prepare(case, precision) as r:
+        r.step(int(case["n_steps"] if steps is None else steps))
+        res = dict(r.moments_if())
+        res.update(r.moments_lf())
+        res["I"] = r.intensity()
+        res.update(r.coefficients())
+        st = r.stats()
+        res["max_iterations"] = st["max_iterations"]
+        res["average_iterations"] = st["average_iterations"]
+        res["stats"] = st
+        res["energy"] = r.energy()
+        res["nx"], res["ny"] = r.nx, r.ny
+    return res

@@ -1,0 +1,401 @@
+#!/usr/bin/env python
+"""Benchmark of the GR lattice-Boltzmann radiation step on B200.
+
+Workload: the curved-scattering problem at scale -- Kerr-Schild M=1 a=0 on
+[-6,6]^2, 400x400 cells, 64 directions, Fourier order 16, excision r <= 2.4,
+RK45 tolerance 1e-10, lognormal absorption, uniform scattering, Gaussian
+emission (2dradiation_b200/workloads.py: curved_scatter), synthetic seeded
+fields.
+
+A bench *step* is one time step of the solver over all 160,000 interior cells
+and 64 directions (stream + moments + lambda-iteration collide, one fused
+kernel).  ``value`` is cell*direction updates per second of the precision form
+(FP32 intensities and stream/collide arithmetic, Kahan moments, FP64
+geodesic tables) with the state resident in HBM, each step timed with CUDA
+events on the library's stream and L2 flushed (256 MiB write) between timed
+steps.  The plain FP64 form is measured the same way and reported beside it,
+with the FP32-vs-FP64 relative error of E after the timed steps.
+
+``e2e`` goes through the C-ABI with host buffers: every e2e step uploads the
+fields and the initial intensities from pinned host memory, runs a full
+2000-step simulation and reads the inertial-frame moments back.
+
+``--impl reference`` times the reference's own CPU implementation (compiled
+from its sources into oracle/_ref, else the oracle restatement) with all host
+threads on the same workload, one solver step per bench step.
+
+Run: python bench.py [--gpus N --steps K --warmup W] (N>1 under torchrun:
+independent replicas per rank, max time over ranks).
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(ROOT / "oracle"))
+
+METRIC = "cell·dir updates/s, FP32+FP64-geodesic vs FP64 plain, at E rel-err ≤1e-5"
+UNIT = "cell·dir updates/s"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def args_parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=1000)
+    p.add_argument("--warmup", type=int, default=20)
+    p.add_argument("--impl", default="grlbm", choices=["grlbm", "reference"])
+    p.add_argument("--e2e-steps", type=int, default=2000)
+    p.add_argument("--e2e-reps", type=int, default=2)
+    p.add_argument("--cpu-steps", type=int, default=2, help="solver steps in the CPU-baseline sample")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--nx", type=int, default=400)
+    p.add_argument("--dirs", type=int, default=64)
+    p.add_argument("--fourier", type=int, default=16)
+    return p.parse_args()
+
+
+def workload_name(a) -> str:
+    return (f"curved_scatter {a.nx}x{a.nx} cells x {a.dirs} directions, Fourier order {a.fourier}, "
+            "Kerr-Schild M=1 a=0 on [-6,6]^2, excision r<=2.4, RK45 tol 1e-10")
+
+
+def dist_setup(a):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1 and a.impl == "grlbm":
+        import torch.distributed as dist
+        from datetime import timedelta
+        import torch
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        dist.init_process_group(backend, timeout=timedelta(seconds=300))
+        pg = dist
+    return world, rank, local, pg
+
+
+def max_over_ranks(x: float, pg, device=None) -> float:
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg, device=None):
+    if pg is not None:
+        import torch
+        t = torch.zeros(1, device=device)
+        pg.all_reduce(t)
+
+
+class Clocks:
+    """nvidia-smi sampler for the SM clock and throttle reasons while the GPU works."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100",
+                 "-i", str(self.index)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+
+        def num(s):
+            try:
+                return float(s)
+            except ValueError:
+                return None
+        sm = [num(r[1]) for r in self.rows if num(r[1]) is not None]
+        mx = [num(r[2]) for r in self.rows if num(r[2]) is not None]
+        pw = [num(r[3]) for r in self.rows if num(r[3]) is not None]
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({n for r in self.rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
+        loaded = [s for s, p in zip(sm, pw) if p is not None and p > 300] or sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows), "power_w_max": max(pw) if pw else None}
+
+
+def hbm_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            v = json.loads(p.read_text()).get("hbm_gbs")
+            if v:
+                return float(v), "measured"
+        except (ValueError, OSError):
+            pass
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def profiled_traffic(kernel: str):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, if any."""
+    p = ROOT / "profiles" / "traffic.json"
+    if not p.exists():
+        return None
+    try:
+        d = json.loads(p.read_text())
+        return d.get(kernel, {}).get("dram_bytes_per_launch")
+    except (ValueError, OSError):
+        return None
+
+
+def time_steps(G, r, steps: int, warmup: int, flush):
+    """Per-step device time (ms) on the library's stream, L2 flushed between steps."""
+    import torch
+    ext = torch.cuda.ExternalStream(r.stream)
+    with torch.cuda.stream(ext):
+        for _ in range(warmup):
+            r.step_async(1)
+            flush.zero_()
+        ext.synchronize()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for s, e in ev:
+            s.record(ext)
+            r.step_async(1)
+            e.record(ext)
+            flush.zero_()
+        ext.synchronize()
+    return [s.elapsed_time(e) for s, e in ev]
+
+
+def run_grlbm(a, world, rank, local, pg):
+    import torch
+    G = importlib.import_module("2dradiation_b200")
+    W = G.workloads
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    case = W.curved_scatter(nx_=a.nx, ny_=a.nx, n_dir=a.dirs, n_fourier=a.fourier, steps=a.e2e_steps)
+    ncell, nd = a.nx * a.nx, a.dirs
+    units = ncell * nd
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    peak, peak_kind = hbm_peak()
+    out = {}
+    with Clocks(local) as clk:
+        forms = {}
+        states = {}
+        for name, prec in (("fp32", G.PRECISION_FP32), ("fp64", G.PLAIN_FP64)):
+            r = G.prepare(case, prec, device=local)
+            st = r.stats()
+            barrier(pg, dev)
+            ms = time_steps(G, r, a.steps, a.warmup, flush)
+            total = max_over_ranks(sum(ms), pg, dev)
+            forms[name] = {"ms": ms, "total_ms": total, "table_ms": st["table_ms"], "rk_substeps": st["rk_substeps"]}
+            states[name] = r.moments_if()
+            forms[name]["iters"] = r.stats()
+            r.close()
+        # e2e through the C-ABI with pinned host buffers
+        f = case["fields"]
+        host = {k: torch.from_numpy(np.ascontiguousarray(v, dtype=np.float64)).pin_memory().numpy()
+                for k, v in f.items() if k != "is_initial"}
+        I0 = torch.zeros(W.nxy(case) * nd, dtype=torch.float64).pin_memory().numpy()
+        mom = {k: torch.zeros(W.nxy(case), dtype=torch.float64).pin_memory().numpy()
+               for k in ("E", "Fx", "Fy", "Pxx", "Pxy", "Pyy")}
+        r = G.prepare(case, G.PRECISION_FP32, device=local)
+        e2e_t = []
+        for rep in range(a.e2e_reps + 1):
+            barrier(pg, dev)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            r.set_fields(host)
+            r.set_intensity(I0)
+            r.step(a.e2e_steps)
+            r.moments_if(mom)
+            t1 = time.perf_counter()
+            if rep > 0:
+                e2e_t.append(t1 - t0)
+        r.close()
+        e2e_s = max_over_ranks(statistics.median(e2e_t), pg, dev)
+    clocks = clk.summary()
+
+    fp32, fp64 = forms["fp32"], forms["fp64"]
+    value = world * units * a.steps / (fp32["total_ms"] / 1e3)
+    plain = world * units * a.steps / (fp64["total_ms"] / 1e3)
+    # algorithmic bytes per cell*direction: I read + written, 4 inputs and 6
+    # moments per cell shared by the directions
+    b32 = 2 * 4 + (4 + 6) * 4 / nd
+    b64 = 2 * 8 + (4 + 6) * 8 / nd
+    avg32 = statistics.mean(fp32["ms"]) / 1e3
+    avg64 = statistics.mean(fp64["ms"]) / 1e3
+    ach32 = b32 * units / avg32 / 1e9
+    ach64 = b64 * units / avg64 / 1e9
+    E32, E64 = states["fp32"]["E"], states["fp64"]["E"]
+    rel = lambda x, y: float(np.linalg.norm(x - y) / max(np.linalg.norm(y), 1e-300))
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": a.steps,
+        "warmup": a.warmup,
+        "ms_per_step": fp32["total_ms"] / a.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {
+            "workload": workload_name(a),
+            "form": "precision: FP32 intensities and stream/collide, Kahan FP32 moments, FP64 geodesic tables",
+            "step": "one time step (fused stream + moments + lambda-iteration collide) over all interior cells",
+            "l2": "flushed between timed steps by a 256 MiB write (untimed)",
+            "parallelism": "single GPU" if world == 1 else f"{world} independent replicas, one per GPU",
+            "global_batch": units,
+        },
+        "roofline": {
+            "bound": "hbm",
+            "achieved": ach32,
+            "peak": peak,
+            "peak_kind": peak_kind,
+            "unit": "GB/s",
+            "frac": ach32 / peak,
+            "traffic": profiled_traffic("k_step_fp32"),
+            "algorithmic_bytes_per_update": b32,
+            "kernel": "k_step<float, curved>",
+        },
+        "plain_fp64": {
+            "value": plain,
+            "ms_per_step": fp64["total_ms"] / a.steps,
+            "roofline_frac": ach64 / peak,
+            "achieved_gbs": ach64,
+            "algorithmic_bytes_per_update": b64,
+            "traffic": profiled_traffic("k_step_fp64"),
+        },
+        "precision_vs_plain": value / plain,
+        "accuracy": {"E_rel_l2_fp32_vs_fp64": rel(E32, E64),
+                     "Fx_rel_l2_fp32_vs_fp64": rel(states["fp32"]["Fx"], states["fp64"]["Fx"]),
+                     "after_steps": a.warmup + a.steps},
+        "table_build_ms": {"fp32": fp32["table_ms"], "fp64": fp64["table_ms"]},
+        "lambda_iterations": {"fp32_avg": fp32["iters"]["average_iterations"],
+                              "fp64_avg": fp64["iters"]["average_iterations"],
+                              "max": fp64["iters"]["max_iterations"]},
+        "e2e": {
+            "value": world * units * a.e2e_steps / e2e_s,
+            "unit": UNIT,
+            "h2d_bytes_per_step": int(8 * (6 * W.nxy(case) + W.nxy(case) * nd)),
+            "d2h_bytes_per_step": int(8 * 6 * W.nxy(case)),
+            "step": f"C-ABI: set fields + set intensities (host) + {a.e2e_steps} solver steps + moments to host",
+            "seconds_per_step": e2e_s,
+        },
+        "gpu_launches": a.steps,
+        "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(a)
+    return line
+
+
+def cpu_run(a, steps: int):
+    import oracle
+    W = importlib.import_module("2dradiation_b200.workloads")
+    case = W.curved_scatter(nx_=a.nx, ny_=a.nx, n_dir=a.dirs, n_fourier=a.fourier, steps=steps)
+    kind = "ref_fast" if oracle.available("ref_fast") else "oracle"
+    cores = os.cpu_count() or 1
+    res = oracle.run(case, kind, n_threads=cores)
+    return res, kind, cores
+
+
+def cpu_baseline(a):
+    res, kind, cores = cpu_run(a, a.cpu_steps)
+    units = a.nx * a.nx * a.dirs * a.cpu_steps
+    return {"value": units / res["computation_time_s"], "unit": UNIT, "cores": cores,
+            "kind": "reference" if kind == "ref_fast" else "port",
+            "sample": f"{a.cpu_steps} solver steps of the same workload after its geodesic table build "
+                      f"({res['table_time_s']:.1f} s, untimed); reference built with -O3 -ffast-math -fopenmp",
+            "table_build_s": res["table_time_s"]}
+
+
+def run_reference(a, world, rank):
+    """The reference's CPU path, one solver step per bench step.  When the
+    requested steps would not finish in about three minutes at the full grid,
+    each step runs on the same problem at a coarser grid (same domain,
+    directions, Fourier order and fields): the work per cell*direction does
+    not depend on the grid size, so the rate is comparable."""
+    if rank != 0:
+        return None
+    cores = os.cpu_count() or 1
+    rate_guess = 3.2e6 * cores / 8.0  # measured: 3.2e6 cell*dir/s on 8 Xeon cores at 400x400x64
+    n = a.warmup + a.steps
+    nx = int((150.0 * rate_guess / (max(n, 1) * a.dirs)) ** 0.5)
+    nx = max(32, min(a.nx, nx))
+    sub = argparse.Namespace(**{**vars(a), "nx": nx})
+    res, kind, cores = cpu_run(sub, n)
+    t = res["step_times"][a.warmup:a.warmup + a.steps]
+    units = nx * nx * a.dirs
+    value = units * a.steps / float(np.sum(t))
+    sample = (f"{a.steps} timed solver steps after {a.warmup} warm-up steps on {nx}x{nx} cells "
+              f"(same domain, {a.dirs} directions, Fourier order {a.fourier}); geodesic table build "
+              f"{res['table_time_s']:.1f} s untimed; {'reference built -O3 -ffast-math -fopenmp' if kind == 'ref_fast' else 'oracle restatement'}")
+    return {
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * float(np.mean(t)),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": workload_name(a), "step": "one solver time step on the host cores (OpenMP)",
+                   "sample_grid": f"{nx}x{nx}"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores,
+                         "kind": "reference" if kind == "ref_fast" else "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    a = args_parse()
+    world, rank, local, pg = dist_setup(a)
+    try:
+        if a.impl == "reference":
+            line = run_reference(a, world, rank)
+        else:
+            line = run_grlbm(a, world, rank, local, pg)
+        if rank == 0 and line is not None:
+            print(json.dumps(line))
+    finally:
+        if pg is not None:
+            pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,209 @@
+/* grlbm.h -- C-ABI of the B200 implementation of the general-relativistic
+ * lattice-Boltzmann radiation step of Tom-Olsen/2dRadiation.
+ *
+ * One context (grlbm_ctx) holds one Radiation problem resident on one GPU:
+ * grid, metric arrays, stencil tables, fluid fields, geodesic tables and the
+ * intensity double buffer.  Every entry point replaces one piece of the
+ * reference's Radiation/Grid/Metric/Stencil interface, cited below as
+ * path:line inside the reference project.
+ *
+ * Conventions
+ *  - Every function returns GRLBM_OK (0) or a GRLBM_ERR_* code; none exits the
+ *    process.  grlbm_last_error(ctx) describes the last failure (ctx may be
+ *    NULL for failures of grlbm_create).
+ *  - Host arrays are plain C arrays in the reference's layouts: per-node
+ *    arrays have nx*ny entries indexed ij = i + j*nx with nx = nx_+2
+ *    (src/Grid.cpp:14, 44-47); intensities are cell-major I[ij*nDir + d]
+ *    (src/Radiation.cpp:89-92).  They are copied at call time; the caller
+ *    keeps ownership.  Device layouts are private (direction-major).
+ *  - A context is used by one host thread at a time; all GPU work is ordered
+ *    on the context's CUDA stream and every entry point returns after its
+ *    work has completed (synchronous), except where stated.
+ *  - Numbers: GRLBM_PLAIN_FP64 computes everything in IEEE FP64 and matches
+ *    the reference's CPU path to relative L2 <= 1e-12 on E and F;
+ *    GRLBM_PRECISION_FP32 keeps intensities and the stream/collide arithmetic
+ *    in FP32 (Kahan-compensated moment sums) on top of FP64 geodesic tables.
+ */
+#ifndef GRLBM_H
+#define GRLBM_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GRLBM_OK 0
+#define GRLBM_ERR_ARGUMENT 1    /* bad argument or size */
+#define GRLBM_ERR_CUDA 2        /* CUDA runtime error or no usable GPU */
+#define GRLBM_ERR_STATE 3       /* call out of order (e.g. step before tables) */
+#define GRLBM_ERR_UNSUPPORTED 4 /* valid in the reference, not in this build */
+#define GRLBM_ERR_NONCONVERGED 5/* an RK45 backtrace hit its substep cap */
+#define GRLBM_ERR_HOST 6        /* host-side failure (allocation, table build) */
+
+/* Metric kinds: the reference's Metric subclasses (src/Spacetimes.h:7-45) */
+#define GRLBM_MINKOWSKI 0
+#define GRLBM_SCHWARZSCHILD 1
+#define GRLBM_KERRSCHILD 2
+
+/* StreamingType (src/Config.hh:5-12); only the two fixed types are built */
+#define GRLBM_FLAT_FIXED 0
+#define GRLBM_FLAT_ADAPTIVE 1
+#define GRLBM_CURVED_FIXED 2
+#define GRLBM_CURVED_ADAPTIVE 3
+#define GRLBM_GEODESIC_FIXED 4
+
+/* InitialDataType (src/Config.hh:38-42) */
+#define GRLBM_MOMENTS 0
+#define GRLBM_INTENSITIES 1
+
+/* Arithmetic forms */
+#define GRLBM_PLAIN_FP64 0
+#define GRLBM_PRECISION_FP32 1
+
+typedef struct grlbm_ctx grlbm_ctx;
+
+/* Grid(nx_, ny_, start, end, halo = 1) followed by Grid::SetCFL(cfl)
+ * (src/Grid.cpp:4-37). */
+typedef struct
+{
+    int64_t nx_, ny_;
+    double startx, starty, endx, endy;
+    double cfl;
+} grlbm_grid_desc;
+
+/* Minkowski / SchwarzSchild / KerrSchild(grid, m, a) (src/Spacetimes.cpp).
+ * excision: InsideBH radius in units of m; <= 0 selects the reference's
+ * hard-coded 2.1 (src/Spacetimes.cpp:42,81). */
+typedef struct
+{
+    int32_t kind;
+    double m, a;
+    double excision;
+} grlbm_metric_desc;
+
+/* Stencil(n_dir, 0) and Stencil(n_fourier, 0, false) (src/Stencil.cpp:177)
+ * plus the Config fields that shape the step (src/Config.hh:45-60). */
+typedef struct
+{
+    int32_t n_dir;
+    int32_t n_fourier;
+    int32_t streaming_type;
+    int32_t precision;
+    int32_t keep_source_nodes_active;
+    int32_t initial_data_type;
+} grlbm_run_desc;
+
+typedef struct
+{
+    int64_t steps;            /* steps taken since the last reset */
+    int32_t max_iterations;   /* Radiation::maxItterationCount (src/Radiation.h:83) */
+    double average_iterations;/* sum over steps and interior cells / (steps*(nx-2)*(ny-2)),
+                                 as src/Radiation.cpp:856 */
+    int64_t rk_substeps;      /* accepted + rejected RK45 trials of the table build */
+    int32_t rk_nonconverged;  /* backtraces stopped by the substep cap */
+    double table_ms;          /* device time of the last table build */
+} grlbm_stats;
+
+/* ---- context ------------------------------------------------------------
+ * Replaces the constructor chain Grid -> Metric subclass -> Stencil x2 ->
+ * Radiation(metric, stencil, streamingStencil, config)
+ * (exe/main.cpp:540-569, src/Radiation.cpp:3-83): builds the metric arrays,
+ * stencil tables and identity Fourier coefficients on the host and uploads
+ * them.  device < 0 uses the current CUDA device. */
+int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric,
+                 const grlbm_run_desc *run, int32_t device, grlbm_ctx **out);
+void grlbm_destroy(grlbm_ctx *ctx);
+const char *grlbm_last_error(const grlbm_ctx *ctx);
+
+/* Grid members nx, ny, dx, dy, dt (src/Grid.h:17-21). */
+int grlbm_get_grid(const grlbm_ctx *ctx, int64_t *nx, int64_t *ny, double *dx, double *dy,
+                   double *dt);
+
+/* ---- inputs (the public buffers callers write, src/Radiation.h:28-39,62-68)
+ * Fluid fields kappa0, kappa1, kappaA, eta, ux, uy: nx*ny each. */
+int grlbm_set_fields(grlbm_ctx *ctx, const double *kappa0, const double *kappa1,
+                     const double *kappaA, const double *eta, const double *ux,
+                     const double *uy);
+/* isInitialGridPoint (nx*ny bytes), initialI (nx*ny*nDir, cell-major), and
+ * initialE_LF..initialPyy_LF (nx*ny each; used when initial_data_type is
+ * GRLBM_MOMENTS, may be NULL otherwise).  The source intensities are derived
+ * here once, as Radiation::LoadInitialData would (src/Radiation.cpp:103-182). */
+int grlbm_set_initial_data(grlbm_ctx *ctx, const uint8_t *is_initial, const double *initial_I,
+                           const double *E_LF, const double *Fx_LF, const double *Fy_LF,
+                           const double *Pxx_LF, const double *Pxy_LF, const double *Pyy_LF);
+/* Radiation::LoadInitialData (src/Radiation.cpp:128-182): writes the source
+ * intensities into the current intensity buffer. */
+int grlbm_load_initial_data(grlbm_ctx *ctx);
+/* The public member I (src/Radiation.h:71), cell-major, nx*ny*nDir. */
+int grlbm_set_intensity(grlbm_ctx *ctx, const double *I);
+int grlbm_get_intensity(grlbm_ctx *ctx, double *I);
+
+/* ---- geodesic tables ----------------------------------------------------
+ * Radiation::UpdateFourierCoefficients (src/Radiation.cpp:191-237): one FP64
+ * RK45 backtrace over dt per interior cell and streaming direction
+ * (src/GeodesicEquationSolver.cpp:80-188, tolerance rk_tol; the reference's
+ * maxTE is 1e-4), the Fourier projection of 1/s, x, y, vx, vy
+ * (src/FourierHarmonics.cpp:33-45), then the per-(cell, direction) departure
+ * records the stream reads.  max_substeps bounds each backtrace (0: 1e6);
+ * a backtrace that hits it is counted in grlbm_stats.rk_nonconverged and the
+ * call returns GRLBM_ERR_NONCONVERGED after finishing the others. */
+int grlbm_update_fourier_coefficients(grlbm_ctx *ctx, double rk_tol, int32_t max_substeps);
+/* coefficientsS/X/Y/Cx/Cy (src/Radiation.h:75-79): nx*ny*nF each. */
+int grlbm_get_fourier_coefficients(grlbm_ctx *ctx, double *S, double *X, double *Y,
+                                   double *Cx, double *Cy);
+
+/* ---- time steps -----------------------------------------------------------
+ * n_steps iterations of the loop body of Radiation::RunSimulation
+ * (src/Radiation.cpp:789-822): LoadInitialData when
+ * keep_source_nodes_active, StreamFlatFixed (:380-414) or StreamCurvedFixed
+ * (:454-512), ComputeMomentsIF (:239-269) and Collide (:641-736), fused into
+ * one kernel per step and replayed from a CUDA graph. */
+int grlbm_step(grlbm_ctx *ctx, int32_t n_steps);
+/* Same, but only enqueues the work on the context's stream and returns
+ * without waiting (for timing with events); grlbm_sync() waits. */
+int grlbm_step_async(grlbm_ctx *ctx, int32_t n_steps);
+int grlbm_sync(grlbm_ctx *ctx);
+/* The context's CUDA stream (a cudaStream_t), for callers that time or order
+ * work around the library's launches. */
+void *grlbm_stream(grlbm_ctx *ctx);
+
+/* Inertial-frame moments E, Fx, Fy, Pxx, Pxy, Pyy as left by the last step
+ * (src/Radiation.h:46-51), nx*ny each; any pointer may be NULL. */
+int grlbm_get_moments_if(grlbm_ctx *ctx, double *E, double *Fx, double *Fy, double *Pxx,
+                         double *Pxy, double *Pyy);
+/* Radiation::ComputeMomentsLF (src/Radiation.cpp:270-301): lab-frame moments
+ * E_LF, Fx_LF, Fy_LF, Pxx_LF, Pxy_LF, Pyy_LF, F_LF; any pointer may be NULL. */
+int grlbm_compute_moments_lf(grlbm_ctx *ctx, double *E, double *Fx, double *Fy, double *Pxx,
+                             double *Pxy, double *Pyy, double *F);
+/* Global energy: sum of the inertial-frame E over the interior cells, in FP64
+ * with a fixed reduction order (bitwise reproducible).  No reference
+ * counterpart; the conservation check of the precision form. */
+int grlbm_energy(grlbm_ctx *ctx, double *total);
+/* Lambda-iteration and table-build statistics (src/Radiation.cpp:723-733,
+ * 855-857). */
+int grlbm_get_stats(grlbm_ctx *ctx, grlbm_stats *stats);
+
+/* ---- host-only helpers (no GPU needed) ----------------------------------
+ * The set-up tables the context uploads, for inspection and tests.
+ * Stencil(n_order, 0, is_intensity): w, phi, cx, cy (n_order each) and, for an
+ * intensity stencil, the cubic interpolation grid InterpolationGrid(10*n_order)
+ * (src/Stencil.cpp:4-162, 177-297): ig_index and ig_weight hold 4 entries per
+ * row (40*n_order each).  Any output pointer may be NULL. */
+int grlbm_host_stencil(int32_t n_order, int32_t is_intensity, double *w, double *phi,
+                       double *cx, double *cy, int64_t *ig_index, double *ig_weight);
+/* Stencil::fluxToSigmaTable / fluxToNormalizationTable
+ * (src/Stencil.cpp:378-455): *size receives the entry count; up to capacity
+ * entries are written to inputs, sigma and normalization (may be NULL). */
+int grlbm_host_flux_table(int32_t n_order, int32_t *size, double *inputs, double *sigma,
+                          double *normalization, int32_t capacity);
+/* The 102 per-node metric arrays of the Metric class, in the member order of
+ * src/Metric.h:19-65 (102*nx*ny doubles). */
+int grlbm_host_metric_arrays(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric,
+                             double *out);
+/* Number of metric arrays written by grlbm_host_metric_arrays. */
+int32_t grlbm_metric_array_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1419,6 +1419,7 @@ int oracle_run(const grlbm_ref_params *p, const grlbm_ref_inputs *in, grlbm_ref_
     t0 = now_s();
     for (int n = 0; n < p->n_steps; n++)
     {
+        double ts = now_s();
         if (p->keep_source_nodes_active)
             load_initial(&R, in);
         if (p->streaming_type == 0)
@@ -1427,6 +1428,8 @@ int oracle_run(const grlbm_ref_params *p, const grlbm_ref_inputs *in, grlbm_ref_
             stream_curved(&R);
         moments_if(&R);
         collide(&R, in);
+        if (out->step_times)
+            out->step_times[n] = now_s() - ts;
     }
     out->computation_time_s = now_s() - t0;
     out->max_iterations = R.maxIter;

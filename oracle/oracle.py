@@ -85,6 +85,7 @@ class Outputs(C.Structure):
         ("ss_phi", _P), ("ss_w", _P),
         ("max_iterations", C.c_int32), ("average_iterations", C.c_double),
         ("computation_time_s", C.c_double), ("table_time_s", C.c_double),
+        ("step_times", _P),
     ]
 
 
@@ -181,6 +182,7 @@ def run(case: dict, kind: str = "oracle", metric_override: np.ndarray | None = N
     res["ig_weight"] = np.zeros(4 * 10 * nd)
     res["ss_phi"] = np.zeros(nf)
     res["ss_w"] = np.zeros(nf)
+    res["step_times"] = np.zeros(max(int(case["n_steps"]), 1))
     out = Outputs(**{k: (_ptr(v, C.c_int64) if v.dtype == np.int64 else _ptr(v))
                      for k, v in res.items() if v is not None})
     lib = library(kind)

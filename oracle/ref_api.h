@@ -89,6 +89,8 @@ typedef struct
     double average_iterations;
     double computation_time_s; /* the step loop only (Logger::ComputationTime) */
     double table_time_s;       /* UpdateFourierCoefficients */
+    /* optional: wall time of each step of the loop (n_steps entries) */
+    double *step_times;
 } grlbm_ref_outputs;
 
 int ref_run(const grlbm_ref_params *p, const grlbm_ref_inputs *in, grlbm_ref_outputs *out);

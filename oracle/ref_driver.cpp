@@ -174,6 +174,7 @@ extern "C" int ref_run(const grlbm_ref_params *p, const grlbm_ref_inputs *in, gr
         t0 = std::chrono::steady_clock::now();
         for (int n = 0; n < p->n_steps; n++)
         {
+            auto ts = std::chrono::steady_clock::now();
             if (config.keepSourceNodesActive)
                 r.LoadInitialData();
             switch (config.streamingType)
@@ -189,6 +190,8 @@ extern "C" int ref_run(const grlbm_ref_params *p, const grlbm_ref_inputs *in, gr
             }
             r.ComputeMomentsIF();
             r.Collide();
+            if (out->step_times)
+                out->step_times[n] = seconds_since(ts);
         }
         out->computation_time_s = seconds_since(t0);
         out->max_iterations = r.maxItterationCount;
