@@ -53,7 +53,8 @@ class RunDesc(C.Structure):
 
 class Stats(C.Structure):
     _fields_ = [("steps", C.c_int64), ("max_iterations", C.c_int32), ("average_iterations", C.c_double),
-                ("rk_substeps", C.c_int64), ("rk_nonconverged", C.c_int32), ("table_ms", C.c_double)]
+                ("rk_substeps", C.c_int64), ("rk_nonconverged", C.c_int32),
+                ("departures_off_grid", C.c_int32), ("table_ms", C.c_double)]
 
 
 _D = C.POINTER(C.c_double)
@@ -73,6 +74,7 @@ SIGNATURES = {
     "grlbm_get_intensity": ([C.c_void_p, _D], C.c_int),
     "grlbm_update_fourier_coefficients": ([C.c_void_p, C.c_double, C.c_int32], C.c_int),
     "grlbm_get_fourier_coefficients": ([C.c_void_p] + [_D] * 5, C.c_int),
+    "grlbm_set_fourier_coefficients": ([C.c_void_p] + [_D] * 5, C.c_int),
     "grlbm_step": ([C.c_void_p, C.c_int32], C.c_int),
     "grlbm_step_async": ([C.c_void_p, C.c_int32], C.c_int),
     "grlbm_sync": ([C.c_void_p], C.c_int),
@@ -226,6 +228,12 @@ class Radiation:
         self._c(lib().grlbm_get_fourier_coefficients(self.h, *[_p(out[k]) for k in
                                                                ("coefS", "coefX", "coefY", "coefCx", "coefCy")]))
         return out
+
+    def set_coefficients(self, coef: dict):
+        arr = [np.ascontiguousarray(coef[k], dtype=np.float64) for k in ("coefS", "coefX", "coefY", "coefCx", "coefCy")]
+        for a in arr:
+            assert a.size == self.nxy * self.nf
+        self._c(lib().grlbm_set_fourier_coefficients(self.h, *[_p(a) for a in arr]))
 
     def step(self, n: int):
         self._c(lib().grlbm_step(self.h, n))

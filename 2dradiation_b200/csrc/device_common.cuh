@@ -1,0 +1,174 @@
+// Types and launch entry points shared by the kernel translation units.
+//
+// Translation units and their floating-point contracts:
+//   kernels_tables.cu    geodesic backtrace, Fourier projection, departure
+//                        records, alpha-ratio cubes -- FP64, built with
+//                        -fmad=false (every product rounded once, as on the
+//                        reference's CPU)
+//   kernels_plain.cu     the plain FP64 step (stream + moments + collide),
+//                        LF moments, sources, energy -- FP64, -fmad=false; it
+//                        evaluates the reference's expressions in the
+//                        reference's association order, so identical inputs
+//                        give identical bits
+//   kernels_precision.cu the FP32 precision-form step -- contracted FMAs,
+//                        compact records, moment-space lambda iteration
+//
+// Device layouts (one problem, all in HBM):
+//   intensities  I[d * nxy + ij]          direction-major, two buffers
+//   plain record rec64[d * ncell + c]     {i_dep, j_dep, angle coordinate, s^3}
+//                                         (absolute grid coordinates of the
+//                                         departure point; angle < 0 marks a
+//                                         departure inside the excision)
+//   FP32 record  rec32[d * ncell + c]     {i_dep - i, j_dep - j, angle coordinate,
+//                                         s^3 alpha_c^3 (0 when excised)}
+//   rk fields    rkf[ij * kRkStride + f]  node-major pack of the 21 metric arrays
+//                                         the geodesic right-hand side reads and
+//                                         the 2x2 spatial tetrad blocks
+//   alpha cubes  acube[ij * 9 + 3(dj+1) + (di+1)] = (alpha_ij / alpha_n)^3 for
+//                                         the 3x3 neighbours n of interior ij
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace grlbm
+{
+constexpr int kRkStride = 32;
+enum RkField : int
+{
+    RF_ALPHA, RF_B1, RF_B2, RF_DA1, RF_DA2, RF_DB11, RF_DB12, RF_DB21, RF_DB22,
+    RF_K11, RF_K12, RF_K22, RF_GU11, RF_GU12, RF_GU22,
+    RF_DG111, RF_DG112, RF_DG122, RF_DG211, RF_DG212, RF_DG222,
+    RF_T11, RF_T12, RF_T21, RF_T22, RF_TI11, RF_TI12, RF_TI21, RF_TI22,
+    RF_COUNT
+};
+static_assert(RF_COUNT <= kRkStride, "rk pack stride");
+
+constexpr int kStepBlock = 128;
+constexpr int kMaxDirs = 256;
+constexpr int kMaxDirsPlain = 216;
+constexpr int kMaxFourier = 64;
+
+struct GridDev
+{
+    int64_t nx, ny, nxy, nx_, ny_, ncell;
+    double dx, dy, dt, startx, starty, endx, endy;
+    int kind;
+    double excision2;
+};
+
+#ifdef __CUDACC__
+__device__ __forceinline__ bool dev_outside(const GridDev &g, double x, double y)
+{
+    return x > g.endx || x < g.startx || y > g.endy || y < g.starty;
+}
+__device__ __forceinline__ bool dev_inside_bh(const GridDev &g, double x, double y)
+{
+    return g.kind != 0 && x * x + y * y <= g.excision2;
+}
+#endif
+
+struct GeodesicArgs
+{
+    GridDev g;
+    const double *rkf;
+    const double *ss_cx, *ss_cy; // streaming stencil directions (nf)
+    int nf;
+    double tol;
+    int max_trials;
+    double *data; // out: [5][ncell][nf]: 1/s, x, y, vIF_x, vIF_y
+    unsigned long long *trials_total;
+    int *nonconverged;
+};
+
+struct ProjectArgs
+{
+    GridDev g;
+    int nf;
+    const double *data;  // [5][ncell][nf]
+    const double *ss_w;  // nf
+    const double *basis; // [f][k] = Basis(k, phi_f)
+    double *coef;        // [5][nxy][nf]
+};
+
+struct DepartureArgs
+{
+    GridDev g;
+    int nf, nd, ng;
+    const double *coef;  // [5][nxy][nf]
+    const double *eval;  // [k][d] = Basis(k, phi_d) at the intensity directions
+    const double *alpha; // nxy
+    double rot_c, rot_s; // RotationMatrix(0) entries
+    double4 *rec64;      // plain records or null
+    float4 *rec32;       // precision records or null
+    int *clamped;
+};
+
+struct PlainStepArgs
+{
+    GridDev g;
+    int nd, ng;
+    const double *Iin;
+    double *Iout;
+    const double4 *rec;
+    const double *w, *n1, *n2; // nd
+    const double *cx, *cy;     // nd (flat departures)
+    const int *ig_index;       // ng*4
+    const double *ig_w;        // ng*4
+    const double *alpha;       // nxy
+    const double *acube;       // nxy*9
+    const uint8_t *flags;      // nxy: bit0 excised node (no collide), bit1 stream writes 0
+    const double *u1, *u2, *lor, *adt, *eta, *k0, *k3, *ka; // k3 = 3 kappa1
+    double *mom;               // 6*nxy
+    unsigned long long *iter_sum;
+    unsigned int *iter_max;
+};
+
+struct PrecStepArgs
+{
+    GridDev g;
+    int nd, ng;
+    const float *Iin;
+    float *Iout;
+    const float4 *rec;
+    const float *w, *n1, *n2; // nd
+    const double *cx, *cy;    // nd (flat departures)
+    const int *ig_base;       // ng: first direction of the cubic row
+    const int *ig_shift;      // ng: first(g+1) - first(g), 0 or 1
+    const float *ig_w;        // ng*4
+    const float *ia3;         // nxy: 1/alpha^3
+    const uint8_t *flags;
+    const float *u1, *u2, *lor, *adt, *eta, *k0, *k3, *ka;
+    const float *wmom;        // 18 stencil sums: sum_d w mu_q (q<6), * n1 (6), * n2 (6)
+    float *mom;               // 6*nxy
+    unsigned long long *iter_sum;
+    unsigned int *iter_max;
+};
+
+// ---- launchers (defined in the kernel translation units) ----
+void launch_geodesic(const GeodesicArgs &a, cudaStream_t s);
+void launch_project(const ProjectArgs &a, cudaStream_t s);
+void launch_departure(const DepartureArgs &a, cudaStream_t s);
+void launch_alpha_cube(const GridDev &g, const double *alpha, double *acube, cudaStream_t s);
+
+cudaError_t prepare_step_plain(int smem_bytes);
+void launch_step_plain(const PlainStepArgs &a, bool curved, cudaStream_t s);
+cudaError_t prepare_step_prec(int smem_bytes);
+void launch_step_prec(const PrecStepArgs &a, bool curved, cudaStream_t s);
+
+void launch_sources64(double *I, int64_t nxy, int nd, const int64_t *nodes, const double *vals, int64_t nsrc,
+                      cudaStream_t s);
+void launch_sources32(float *I, int64_t nxy, int nd, const int64_t *nodes, const float *vals, int64_t nsrc,
+                      cudaStream_t s);
+void launch_moments_lf64(int64_t nxy, const double *mom, const double *lfp, const uint8_t *bh, double *out,
+                         cudaStream_t s);
+void launch_moments_lf32(int64_t nxy, const float *mom, const double *lfp, const uint8_t *bh, double *out,
+                         cudaStream_t s);
+void launch_energy64(const GridDev &g, const double *E, double *partial, int nblocks, double *out, cudaStream_t s);
+void launch_energy32(const GridDev &g, const float *E, double *partial, int nblocks, double *out, cudaStream_t s);
+void launch_to_dirmajor64(const double *in, double *out, int64_t nxy, int nd, cudaStream_t s);
+void launch_to_dirmajor32(const double *in, float *out, int64_t nxy, int nd, cudaStream_t s);
+void launch_to_cellmajor64(const double *in, double *out, int64_t nxy, int nd, cudaStream_t s);
+void launch_to_cellmajor32(const float *in, double *out, int64_t nxy, int nd, cudaStream_t s);
+void launch_widen32(const float *in, double *out, int64_t n, cudaStream_t s);
+} // namespace grlbm

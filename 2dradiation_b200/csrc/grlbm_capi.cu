@@ -1,5 +1,6 @@
 // C-ABI of include/grlbm.h: context management, host<->device transfers,
-// the geodesic-table build and the graph-replayed time steps.
+// the geodesic-table build and the graph-replayed time steps.  Kernels live
+// in kernels_tables.cu, kernels_plain.cu and kernels_precision.cu.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -9,13 +10,12 @@
 #include <cstring>
 #include <memory>
 #include <string>
-#include <type_traits>
 #include <vector>
 
 #include "../../include/grlbm.h"
 #include "approx_math.hpp"
+#include "device_common.cuh"
 #include "host_setup.hpp"
-#include "kernels.cuh"
 
 using namespace grlbm;
 
@@ -27,6 +27,9 @@ struct DevBuf
 {
     void *p = nullptr;
     size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
     ~DevBuf()
     {
         if (p)
@@ -52,19 +55,21 @@ struct grlbm_ctx
     GridDev gd{};
     int64_t ncell = 0;
     int ng = 0;
-    // device buffers
-    DevBuf I[2], rec, w, n1, n2, cx, cy, ig_base, ig_shift, ig_w, ia3, flags, bhmask;
-    DevBuf cu1, cu2, clor, cadt, ceta, ck0, ck1, cka, mom, rkf, lfp, alpha;
+    // device buffers (storage type T = double for the plain form, float for the precision form)
+    DevBuf I[2], rec, w, n1, n2, cx, cy, flags, bhmask, alpha, acube;
+    DevBuf ig_index, ig_w64, ig_base, ig_shift, ig_w32, ia3, wmom;
+    DevBuf cu1, cu2, clor, cadt, ceta, ck0, ck3, cka, mom, rkf, lfp;
     DevBuf coef, ss_cx, ss_cy, ss_w, proj_basis, eval_basis, stage;
     DevBuf src_nodes, src_vals, lf_out, energy_partial, energy_out;
-    DevBuf counters; // [0] iter sum (u64), [1] iter max (u32 in low), [2] rk trials (u64), [3] nonconverged, [4] clamped
+    // counters: [0] iteration sum, [1] iteration max (low 32 bits), [2] RK45
+    // trials, [3] capped backtraces, [4] departures off the grid
+    DevBuf counters;
     int64_t nsrc = 0;
     int cur = 0;
     bool tables = false;
     int64_t steps = 0;
     double table_ms = 0;
-    // graphs of kGraphSteps steps starting from buffer 0 / 1
-    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    cudaGraphExec_t graph[2] = {nullptr, nullptr}; // kGraphSteps steps from buffer 0 / 1
     ~grlbm_ctx()
     {
         for (auto &g : graph)
@@ -94,12 +99,12 @@ int fail(grlbm_ctx *c, int code, const char *fmt, ...)
     return code;
 }
 
-#define CU(call)                                                                                  \
-    do                                                                                            \
-    {                                                                                             \
-        cudaError_t e_ = (call);                                                                  \
-        if (e_ != cudaSuccess)                                                                    \
-            return fail(ctx, GRLBM_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));    \
+#define CU(call)                                                                               \
+    do                                                                                         \
+    {                                                                                          \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess)                                                                 \
+            return fail(ctx, GRLBM_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_)); \
     } while (0)
 
 int alloc(grlbm_ctx *ctx, DevBuf &b, size_t bytes)
@@ -128,7 +133,7 @@ int upload(grlbm_ctx *ctx, DevBuf &b, const std::vector<T> &v)
     return GRLBM_OK;
 }
 
-// upload doubles as the context's storage type
+// doubles stored in the form's type
 int upload_t(grlbm_ctx *ctx, DevBuf &b, const std::vector<double> &v)
 {
     if (!ctx->fp32)
@@ -149,122 +154,84 @@ void invalidate_graphs(grlbm_ctx *ctx)
         }
 }
 
-// cell-major double [ij][d] <-> direction-major T [d][ij]
-template <class T>
-__global__ void k_to_dirmajor(const double *in, T *out, int64_t nxy, int nd)
-{
-    __shared__ double tile[32][33];
-    const int64_t ij0 = (int64_t)blockIdx.x * 32;
-    const int d0 = blockIdx.y * 32;
-    for (int r = threadIdx.y; r < 32; r += 8)
-    {
-        const int64_t ij = ij0 + r;
-        const int d = d0 + threadIdx.x;
-        if (ij < nxy && d < nd)
-            tile[r][threadIdx.x] = in[ij * nd + d];
-    }
-    __syncthreads();
-    for (int r = threadIdx.y; r < 32; r += 8)
-    {
-        const int d = d0 + r;
-        const int64_t ij = ij0 + threadIdx.x;
-        if (ij < nxy && d < nd)
-            out[(int64_t)d * nxy + ij] = (T)tile[threadIdx.x][r];
-    }
-}
-template <class T>
-__global__ void k_to_cellmajor(const T *in, double *out, int64_t nxy, int nd)
-{
-    __shared__ double tile[32][33];
-    const int64_t ij0 = (int64_t)blockIdx.x * 32;
-    const int d0 = blockIdx.y * 32;
-    for (int r = threadIdx.y; r < 32; r += 8)
-    {
-        const int d = d0 + r;
-        const int64_t ij = ij0 + threadIdx.x;
-        if (ij < nxy && d < nd)
-            tile[threadIdx.x][r] = (double)in[(int64_t)d * nxy + ij];
-    }
-    __syncthreads();
-    for (int r = threadIdx.y; r < 32; r += 8)
-    {
-        const int64_t ij = ij0 + r;
-        const int d = d0 + threadIdx.x;
-        if (ij < nxy && d < nd)
-            out[ij * nd + d] = tile[r][threadIdx.x];
-    }
-}
-template <class T>
-__global__ void k_copy_convert(const T *in, double *out, int64_t n)
-{
-    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k < n)
-        out[k] = (double)in[k];
-}
-
-int64_t blocks(int64_t n, int64_t b) { return (n + b - 1) / b; }
-
-template <class T>
-StepArgs<T> step_args(grlbm_ctx *ctx, int from)
-{
-    StepArgs<T> a{};
-    a.g = ctx->gd;
-    a.nd = ctx->st.n;
-    a.ng = ctx->ng;
-    a.Iin = ctx->I[from].as<T>();
-    a.Iout = ctx->I[from ^ 1].as<T>();
-    a.rec = static_cast<decltype(a.rec)>(ctx->rec.p);
-    a.w = ctx->w.as<T>();
-    a.n1 = ctx->n1.as<T>();
-    a.n2 = ctx->n2.as<T>();
-    a.cx = ctx->cx.as<double>();
-    a.cy = ctx->cy.as<double>();
-    a.ig_base = ctx->ig_base.as<int>();
-    a.ig_shift = ctx->ig_shift.as<int>();
-    a.ig_w = ctx->ig_w.as<T>();
-    a.ia3 = ctx->ia3.as<T>();
-    a.flags = ctx->flags.as<uint8_t>();
-    a.u1 = ctx->cu1.as<T>();
-    a.u2 = ctx->cu2.as<T>();
-    a.lor = ctx->clor.as<T>();
-    a.adt = ctx->cadt.as<T>();
-    a.eta = ctx->ceta.as<T>();
-    a.k0 = ctx->ck0.as<T>();
-    a.k1 = ctx->ck1.as<T>();
-    a.ka = ctx->cka.as<T>();
-    a.mom = ctx->mom.as<T>();
-    a.iter_sum = ctx->counters.as<unsigned long long>();
-    a.iter_max = reinterpret_cast<unsigned int *>(ctx->counters.as<unsigned long long>() + 1);
-    return a;
-}
-
-template <class T>
-size_t step_smem(const grlbm_ctx *ctx) { return (size_t)ctx->st.n * kStepBlock * sizeof(T); }
-
 // Enqueue one step starting from buffer `from` (no sync).
-template <class T>
-int enqueue_step_t(grlbm_ctx *ctx, int from)
-{
-    if (ctx->run.keep_source_nodes_active && ctx->nsrc > 0)
-    {
-        const int64_t n = ctx->nsrc * ctx->st.n;
-        k_sources<T><<<(unsigned)blocks(n, 256), 256, 0, ctx->stream>>>(
-            ctx->I[from].as<T>(), ctx->gd.nxy, ctx->st.n, ctx->src_nodes.as<int64_t>(), ctx->src_vals.as<T>(), ctx->nsrc);
-    }
-    const StepArgs<T> a = step_args<T>(ctx, from);
-    const unsigned nb = (unsigned)blocks(ctx->ncell, kStepBlock);
-    const size_t smem = step_smem<T>(ctx);
-    if (ctx->run.streaming_type == GRLBM_CURVED_FIXED)
-        k_step<T, true><<<nb, kStepBlock, smem, ctx->stream>>>(a);
-    else
-        k_step<T, false><<<nb, kStepBlock, smem, ctx->stream>>>(a);
-    CU(cudaGetLastError());
-    return GRLBM_OK;
-}
-
 int enqueue_step(grlbm_ctx *ctx, int from)
 {
-    return ctx->fp32 ? enqueue_step_t<float>(ctx, from) : enqueue_step_t<double>(ctx, from);
+    const bool curved = ctx->run.streaming_type == GRLBM_CURVED_FIXED;
+    unsigned long long *cnt = ctx->counters.as<unsigned long long>();
+    if (ctx->fp32)
+    {
+        if (ctx->run.keep_source_nodes_active && ctx->nsrc > 0)
+            launch_sources32(ctx->I[from].as<float>(), ctx->gd.nxy, ctx->st.n, ctx->src_nodes.as<int64_t>(),
+                             ctx->src_vals.as<float>(), ctx->nsrc, ctx->stream);
+        PrecStepArgs a{};
+        a.g = ctx->gd;
+        a.nd = ctx->st.n;
+        a.ng = ctx->ng;
+        a.Iin = ctx->I[from].as<float>();
+        a.Iout = ctx->I[from ^ 1].as<float>();
+        a.rec = ctx->rec.as<float4>();
+        a.w = ctx->w.as<float>();
+        a.n1 = ctx->n1.as<float>();
+        a.n2 = ctx->n2.as<float>();
+        a.cx = ctx->cx.as<double>();
+        a.cy = ctx->cy.as<double>();
+        a.ig_base = ctx->ig_base.as<int>();
+        a.ig_shift = ctx->ig_shift.as<int>();
+        a.ig_w = ctx->ig_w32.as<float>();
+        a.ia3 = ctx->ia3.as<float>();
+        a.flags = ctx->flags.as<uint8_t>();
+        a.u1 = ctx->cu1.as<float>();
+        a.u2 = ctx->cu2.as<float>();
+        a.lor = ctx->clor.as<float>();
+        a.adt = ctx->cadt.as<float>();
+        a.eta = ctx->ceta.as<float>();
+        a.k0 = ctx->ck0.as<float>();
+        a.k3 = ctx->ck3.as<float>();
+        a.ka = ctx->cka.as<float>();
+        a.wmom = ctx->wmom.as<float>();
+        a.mom = ctx->mom.as<float>();
+        a.iter_sum = cnt;
+        a.iter_max = reinterpret_cast<unsigned int *>(cnt + 1);
+        launch_step_prec(a, curved, ctx->stream);
+    }
+    else
+    {
+        if (ctx->run.keep_source_nodes_active && ctx->nsrc > 0)
+            launch_sources64(ctx->I[from].as<double>(), ctx->gd.nxy, ctx->st.n, ctx->src_nodes.as<int64_t>(),
+                             ctx->src_vals.as<double>(), ctx->nsrc, ctx->stream);
+        PlainStepArgs a{};
+        a.g = ctx->gd;
+        a.nd = ctx->st.n;
+        a.ng = ctx->ng;
+        a.Iin = ctx->I[from].as<double>();
+        a.Iout = ctx->I[from ^ 1].as<double>();
+        a.rec = ctx->rec.as<double4>();
+        a.w = ctx->w.as<double>();
+        a.n1 = ctx->n1.as<double>();
+        a.n2 = ctx->n2.as<double>();
+        a.cx = ctx->cx.as<double>();
+        a.cy = ctx->cy.as<double>();
+        a.ig_index = ctx->ig_index.as<int>();
+        a.ig_w = ctx->ig_w64.as<double>();
+        a.alpha = ctx->alpha.as<double>();
+        a.acube = ctx->acube.as<double>();
+        a.flags = ctx->flags.as<uint8_t>();
+        a.u1 = ctx->cu1.as<double>();
+        a.u2 = ctx->cu2.as<double>();
+        a.lor = ctx->clor.as<double>();
+        a.adt = ctx->cadt.as<double>();
+        a.eta = ctx->ceta.as<double>();
+        a.k0 = ctx->ck0.as<double>();
+        a.k3 = ctx->ck3.as<double>();
+        a.ka = ctx->cka.as<double>();
+        a.mom = ctx->mom.as<double>();
+        a.iter_sum = cnt;
+        a.iter_max = reinterpret_cast<unsigned int *>(cnt + 1);
+        launch_step_plain(a, curved, ctx->stream);
+    }
+    CU(cudaGetLastError());
+    return GRLBM_OK;
 }
 
 int build_graph(grlbm_ctx *ctx, int from)
@@ -291,23 +258,28 @@ int build_graph(grlbm_ctx *ctx, int from)
     return GRLBM_OK;
 }
 
-int set_smem_limits(grlbm_ctx *ctx)
+// departure records from the current Fourier coefficients
+int build_records(grlbm_ctx *ctx)
 {
-    const int sm = (int)(ctx->fp32 ? step_smem<float>(ctx) : step_smem<double>(ctx));
-    if (ctx->fp32)
-    {
-        CU(cudaFuncSetAttribute(k_step<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-        CU(cudaFuncSetAttribute(k_step<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-    }
-    else
-    {
-        CU(cudaFuncSetAttribute(k_step<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-        CU(cudaFuncSetAttribute(k_step<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-    }
+    DepartureArgs da{};
+    da.g = ctx->gd;
+    da.nf = ctx->ss.n;
+    da.nd = ctx->st.n;
+    da.ng = ctx->ng;
+    da.coef = ctx->coef.as<double>();
+    da.eval = ctx->eval_basis.as<double>();
+    da.alpha = ctx->alpha.as<double>();
+    da.rot_c = approx_cos(0.0);
+    da.rot_s = approx_sin(0.0);
+    da.rec64 = ctx->fp32 ? nullptr : ctx->rec.as<double4>();
+    da.rec32 = ctx->fp32 ? ctx->rec.as<float4>() : nullptr;
+    da.clamped = reinterpret_cast<int *>(ctx->counters.as<unsigned long long>() + 4);
+    CU(cudaMemsetAsync(ctx->counters.as<unsigned long long>() + 4, 0, sizeof(unsigned long long), ctx->stream));
+    launch_departure(da, ctx->stream);
+    CU(cudaGetLastError());
     return GRLBM_OK;
 }
 
-// identity Fourier coefficients of the constructor (src/Radiation.cpp:59-82)
 std::vector<double> identity_coefficients(const grlbm_ctx *ctx)
 {
     const int nf = ctx->ss.n;
@@ -345,6 +317,7 @@ std::vector<double> identity_coefficients(const grlbm_ctx *ctx)
 }
 } // namespace
 
+
 // =========================================================================
 extern "C" {
 
@@ -355,7 +328,6 @@ int32_t grlbm_metric_array_count(void) { return kMetricArrays; }
 int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, const grlbm_run_desc *run,
                  int32_t device, grlbm_ctx **out)
 {
-    grlbm_ctx *ctx = nullptr;
     if (!grid || !metric || !run || !out)
         return fail(nullptr, GRLBM_ERR_ARGUMENT, "null argument");
     *out = nullptr;
@@ -370,13 +342,13 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
     if (run->streaming_type != GRLBM_FLAT_FIXED && run->streaming_type != GRLBM_CURVED_FIXED)
     {
         if (run->streaming_type >= GRLBM_FLAT_FIXED && run->streaming_type <= GRLBM_GEODESIC_FIXED)
-            return fail(nullptr, GRLBM_ERR_UNSUPPORTED, "streaming type %d is not built (FlatFixed and CurvedFixed are)",
-                        run->streaming_type);
+            return fail(nullptr, GRLBM_ERR_UNSUPPORTED,
+                        "streaming type %d is not built (FlatFixed and CurvedFixed are)", run->streaming_type);
         return fail(nullptr, GRLBM_ERR_ARGUMENT, "Invalid StreamingType");
     }
     if (run->precision != GRLBM_PLAIN_FP64 && run->precision != GRLBM_PRECISION_FP32)
         return fail(nullptr, GRLBM_ERR_ARGUMENT, "unknown precision %d", run->precision);
-    const int maxdir = run->precision == GRLBM_PLAIN_FP64 ? 216 : kMaxDirs;
+    const int maxdir = run->precision == GRLBM_PLAIN_FP64 ? kMaxDirsPlain : kMaxDirs;
     if (run->n_dir < 4 || run->n_dir > maxdir)
         return fail(nullptr, GRLBM_ERR_ARGUMENT, "n_dir must be in [4, %d]", maxdir);
     if (run->n_fourier < 1 || run->n_fourier > kMaxFourier)
@@ -387,7 +359,7 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
     std::unique_ptr<grlbm_ctx> owner(new (std::nothrow) grlbm_ctx);
     if (!owner)
         return fail(nullptr, GRLBM_ERR_HOST, "out of host memory");
-    ctx = owner.get();
+    grlbm_ctx *ctx = owner.get();
     ctx->run = *run;
     ctx->mdesc = *metric;
     ctx->fp32 = run->precision == GRLBM_PRECISION_FP32;
@@ -439,17 +411,17 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
     gd.excision2 = ctx->M.excision2;
 
     int rc;
-#define TRY(x)                                                                     \
-    do                                                                             \
-    {                                                                              \
-        if ((rc = (x)) != GRLBM_OK)                                                \
-        {                                                                          \
-            g_create_error = ctx->err;                                             \
-            return rc;                                                             \
-        }                                                                          \
+#define TRY(x)                           \
+    do                                   \
+    {                                    \
+        if ((rc = (x)) != GRLBM_OK)      \
+        {                                \
+            g_create_error = ctx->err;   \
+            return rc;                   \
+        }                                \
     } while (0)
 
-    // stencil tables.  RotationMatrix(0) applied to c_d (src/DataTypes.hh:630-635)
+    // directions rotated by RotationMatrix(0) (src/DataTypes.hh:630-635)
     const double rc0 = approx_cos(0.0), rs0 = approx_sin(0.0);
     std::vector<double> n1(nd), n2(nd);
     for (int d = 0; d < nd; d++)
@@ -462,25 +434,48 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
     TRY(upload_t(ctx, ctx->n2, n2));
     TRY(upload(ctx, ctx->cx, ctx->st.cx));
     TRY(upload(ctx, ctx->cy, ctx->st.cy));
-    // cubic rows: first direction and the shift to the next row's first direction
-    std::vector<int> base(ctx->ng), shift(ctx->ng);
-    for (int g = 0; g < ctx->ng; g++)
+    if (ctx->fp32)
     {
-        base[g] = (int)ctx->st.ig_index[4 * g];
-        for (int k = 1; k < 4; k++)
-            if (ctx->st.ig_index[4 * g + k] != (base[g] + k) % nd)
-                return fail(nullptr, GRLBM_ERR_HOST, "interpolation row %d is not 4 consecutive directions", g);
+        // cubic rows as a first direction plus the step to the next row
+        std::vector<int> base(ctx->ng), shift(ctx->ng);
+        for (int g = 0; g < ctx->ng; g++)
+        {
+            base[g] = (int)ctx->st.ig_index[4 * g];
+            for (int k = 1; k < 4; k++)
+                if (ctx->st.ig_index[4 * g + k] != (base[g] + k) % nd)
+                    return fail(nullptr, GRLBM_ERR_HOST, "interpolation row %d is not 4 consecutive directions", g);
+        }
+        for (int g = 0; g < ctx->ng; g++)
+        {
+            shift[g] = ((base[(g + 1) % ctx->ng] - base[g]) % nd + nd) % nd;
+            if (shift[g] > 1)
+                return fail(nullptr, GRLBM_ERR_HOST, "interpolation rows %d, %d are %d directions apart", g, g + 1,
+                            shift[g]);
+        }
+        TRY(upload(ctx, ctx->ig_base, base));
+        TRY(upload(ctx, ctx->ig_shift, shift));
+        std::vector<float> w32(ctx->st.ig_weight.begin(), ctx->st.ig_weight.end());
+        TRY(upload(ctx, ctx->ig_w32, w32));
+        // stencil sums of the affine collide map: sum_d w mu_q, * n1, * n2
+        std::vector<double> wm(18, 0.0);
+        for (int d = 0; d < nd; d++)
+        {
+            const double mu[6] = {1.0, n1[d], n2[d], n1[d] * n1[d], n1[d] * n2[d], n2[d] * n2[d]};
+            for (int q = 0; q < 6; q++)
+            {
+                wm[q] += ctx->st.w[d] * mu[q];
+                wm[6 + q] += ctx->st.w[d] * mu[q] * n1[d];
+                wm[12 + q] += ctx->st.w[d] * mu[q] * n2[d];
+            }
+        }
+        TRY(upload_t(ctx, ctx->wmom, wm));
     }
-    for (int g = 0; g < ctx->ng; g++)
+    else
     {
-        const int nb = base[(g + 1) % ctx->ng];
-        shift[g] = ((nb - base[g]) % nd + nd) % nd;
-        if (shift[g] > 1)
-            return fail(nullptr, GRLBM_ERR_HOST, "interpolation rows %d and %d are %d directions apart", g, g + 1, shift[g]);
+        std::vector<int> idx(ctx->st.ig_index.begin(), ctx->st.ig_index.end());
+        TRY(upload(ctx, ctx->ig_index, idx));
+        TRY(upload(ctx, ctx->ig_w64, ctx->st.ig_weight));
     }
-    TRY(upload(ctx, ctx->ig_base, base));
-    TRY(upload(ctx, ctx->ig_shift, shift));
-    TRY(upload_t(ctx, ctx->ig_w, ctx->st.ig_weight));
 
     // per-node metric data
     const MetricArrays &M = ctx->M;
@@ -509,11 +504,18 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
     TRY(upload(ctx, ctx->rkf, rkf));
     TRY(upload(ctx, ctx->lfp, lfp));
     TRY(upload(ctx, ctx->alpha, alpha));
-    TRY(upload_t(ctx, ctx->ia3, ia3));
     TRY(upload(ctx, ctx->flags, flags));
     TRY(upload(ctx, ctx->bhmask, bh));
+    if (ctx->fp32)
+        TRY(upload_t(ctx, ctx->ia3, ia3));
+    else
+    {
+        TRY(alloc(ctx, ctx->acube, (size_t)nxy * 9 * sizeof(double)));
+        cudaMemset(ctx->acube.p, 0, ctx->acube.bytes);
+        launch_alpha_cube(gd, ctx->alpha.as<double>(), ctx->acube.as<double>(), ctx->stream);
+    }
 
-    // streaming stencil and Fourier bases
+    // streaming stencil and the two Fourier bases
     std::vector<double> pb((size_t)nf * nf), eb((size_t)nf * nd);
     for (int f = 0; f < nf; f++)
         for (int k = 0; k < nf; k++)
@@ -528,7 +530,7 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
     TRY(upload(ctx, ctx->eval_basis, eb));
     TRY(upload(ctx, ctx->coef, identity_coefficients(ctx)));
 
-    // state buffers
+    // state
     const size_t ib = (size_t)nxy * nd * tsize(ctx);
     TRY(alloc(ctx, ctx->I[0], ib));
     TRY(alloc(ctx, ctx->I[1], ib));
@@ -545,7 +547,9 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
     // fields default to zero (the reference's buffers are value-initialised)
     std::vector<double> zeros(nxy, 0.0);
     TRY(grlbm_set_fields(ctx, zeros.data(), zeros.data(), zeros.data(), zeros.data(), zeros.data(), zeros.data()));
-    TRY(set_smem_limits(ctx));
+    const int smem = (int)((size_t)nd * kStepBlock * tsize(ctx));
+    if ((ctx->fp32 ? prepare_step_prec(smem) : prepare_step_plain(smem)) != cudaSuccess)
+        return fail(nullptr, GRLBM_ERR_CUDA, "cannot reserve %d bytes of shared memory for the step kernel", smem);
     if (cudaDeviceSynchronize() != cudaSuccess)
         return fail(nullptr, GRLBM_ERR_CUDA, "device error during set-up");
 #undef TRY
@@ -584,12 +588,14 @@ void *grlbm_stream(grlbm_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr;
 int grlbm_set_fields(grlbm_ctx *ctx, const double *kappa0, const double *kappa1, const double *kappaA,
                      const double *eta, const double *ux, const double *uy)
 {
-    if (!ctx || !kappa0 || !kappa1 || !kappaA || !eta || !ux || !uy)
+    if (!ctx)
+        return GRLBM_ERR_ARGUMENT;
+    if (!kappa0 || !kappa1 || !kappaA || !eta || !ux || !uy)
         return fail(ctx, GRLBM_ERR_ARGUMENT, "null field");
     cudaSetDevice(ctx->device);
     const int64_t nxy = ctx->geo.nxy;
     const MetricArrays &M = ctx->M;
-    std::vector<double> u1(nxy), u2(nxy), lor(nxy), adt(nxy);
+    std::vector<double> u1(nxy), u2(nxy), lor(nxy), adt(nxy), k3(nxy);
     for (int64_t ij = 0; ij < nxy; ij++)
     {
         // TransformLFtoIF(uLF, GetTetrad(ij)) as Collide calls it (src/Radiation.cpp:652-657)
@@ -599,20 +605,18 @@ int grlbm_set_fields(grlbm_ctx *ctx, const double *kappa0, const double *kappa1,
         u2[ij] = b;
         lor[ij] = 1.0 / std::sqrt(1.0 - (a * a + b * b));
         adt[ij] = M.at(ALPHA, ij) * ctx->geo.dt;
+        k3[ij] = 3.0 * kappa1[ij];
     }
     int rc;
-    if ((rc = upload_t(ctx, ctx->cu1, u1)) || (rc = upload_t(ctx, ctx->cu2, u2)) || (rc = upload_t(ctx, ctx->clor, lor)) ||
-        (rc = upload_t(ctx, ctx->cadt, adt)))
+    if ((rc = upload_t(ctx, ctx->cu1, u1)) || (rc = upload_t(ctx, ctx->cu2, u2)) ||
+        (rc = upload_t(ctx, ctx->clor, lor)) || (rc = upload_t(ctx, ctx->cadt, adt)) ||
+        (rc = upload_t(ctx, ctx->ck3, k3)))
         return rc;
-    std::vector<double> tmp(nxy);
-    const double *src[4] = {eta, kappa0, kappa1, kappaA};
-    DevBuf *dst[4] = {&ctx->ceta, &ctx->ck0, &ctx->ck1, &ctx->cka};
-    for (int q = 0; q < 4; q++)
-    {
-        std::copy(src[q], src[q] + nxy, tmp.begin());
-        if ((rc = upload_t(ctx, *dst[q], tmp)))
+    const double *src[3] = {eta, kappa0, kappaA};
+    DevBuf *dst[3] = {&ctx->ceta, &ctx->ck0, &ctx->cka};
+    for (int q = 0; q < 3; q++)
+        if ((rc = upload_t(ctx, *dst[q], std::vector<double>(src[q], src[q] + nxy))))
             return rc;
-    }
     invalidate_graphs(ctx);
     return GRLBM_OK;
 }
@@ -621,8 +625,10 @@ int grlbm_set_initial_data(grlbm_ctx *ctx, const uint8_t *is_initial, const doub
                            const double *Fx_LF, const double *Fy_LF, const double *Pxx_LF, const double *Pxy_LF,
                            const double *Pyy_LF)
 {
-    if (!ctx || !is_initial)
-        return fail(ctx, GRLBM_ERR_ARGUMENT, "null argument");
+    if (!ctx)
+        return GRLBM_ERR_ARGUMENT;
+    if (!is_initial)
+        return fail(ctx, GRLBM_ERR_ARGUMENT, "null is_initial");
     if (ctx->run.initial_data_type == GRLBM_INTENSITIES && !initial_I)
         return fail(ctx, GRLBM_ERR_ARGUMENT, "initial_I is required for InitialDataType::Intensities");
     if (ctx->run.initial_data_type == GRLBM_MOMENTS && (!E_LF || !Fx_LF || !Fy_LF || !Pxx_LF || !Pxy_LF || !Pyy_LF))
@@ -653,16 +659,15 @@ int grlbm_load_initial_data(grlbm_ctx *ctx)
     cudaSetDevice(ctx->device);
     if (ctx->nsrc == 0)
         return GRLBM_OK;
-    const int64_t n = ctx->nsrc * ctx->st.n;
-    // both buffers: halo and excised nodes are read from whichever buffer is current
+    // both buffers: halo and excised nodes are read from whichever is current
     for (int b = 0; b < 2; b++)
     {
         if (ctx->fp32)
-            k_sources<float><<<(unsigned)blocks(n, 256), 256, 0, ctx->stream>>>(
-                ctx->I[b].as<float>(), ctx->gd.nxy, ctx->st.n, ctx->src_nodes.as<int64_t>(), ctx->src_vals.as<float>(), ctx->nsrc);
+            launch_sources32(ctx->I[b].as<float>(), ctx->gd.nxy, ctx->st.n, ctx->src_nodes.as<int64_t>(),
+                             ctx->src_vals.as<float>(), ctx->nsrc, ctx->stream);
         else
-            k_sources<double><<<(unsigned)blocks(n, 256), 256, 0, ctx->stream>>>(
-                ctx->I[b].as<double>(), ctx->gd.nxy, ctx->st.n, ctx->src_nodes.as<int64_t>(), ctx->src_vals.as<double>(), ctx->nsrc);
+            launch_sources64(ctx->I[b].as<double>(), ctx->gd.nxy, ctx->st.n, ctx->src_nodes.as<int64_t>(),
+                             ctx->src_vals.as<double>(), ctx->nsrc, ctx->stream);
     }
     CU(cudaGetLastError());
     CU(cudaStreamSynchronize(ctx->stream));
@@ -671,8 +676,10 @@ int grlbm_load_initial_data(grlbm_ctx *ctx)
 
 int grlbm_set_intensity(grlbm_ctx *ctx, const double *I)
 {
-    if (!ctx || !I)
-        return fail(ctx, GRLBM_ERR_ARGUMENT, "null argument");
+    if (!ctx)
+        return GRLBM_ERR_ARGUMENT;
+    if (!I)
+        return fail(ctx, GRLBM_ERR_ARGUMENT, "null intensities");
     cudaSetDevice(ctx->device);
     const int64_t nxy = ctx->gd.nxy;
     const int nd = ctx->st.n;
@@ -680,13 +687,12 @@ int grlbm_set_intensity(grlbm_ctx *ctx, const double *I)
     if (rc)
         return rc;
     CU(cudaMemcpyAsync(ctx->stage.p, I, ctx->stage.bytes, cudaMemcpyHostToDevice, ctx->stream));
-    dim3 grid((unsigned)blocks(nxy, 32), (unsigned)blocks(nd, 32)), blk(32, 8);
     for (int b = 0; b < 2; b++)
     {
         if (ctx->fp32)
-            k_to_dirmajor<float><<<grid, blk, 0, ctx->stream>>>(ctx->stage.as<double>(), ctx->I[b].as<float>(), nxy, nd);
+            launch_to_dirmajor32(ctx->stage.as<double>(), ctx->I[b].as<float>(), nxy, nd, ctx->stream);
         else
-            k_to_dirmajor<double><<<grid, blk, 0, ctx->stream>>>(ctx->stage.as<double>(), ctx->I[b].as<double>(), nxy, nd);
+            launch_to_dirmajor64(ctx->stage.as<double>(), ctx->I[b].as<double>(), nxy, nd, ctx->stream);
     }
     CU(cudaGetLastError());
     CU(cudaStreamSynchronize(ctx->stream));
@@ -695,19 +701,20 @@ int grlbm_set_intensity(grlbm_ctx *ctx, const double *I)
 
 int grlbm_get_intensity(grlbm_ctx *ctx, double *I)
 {
-    if (!ctx || !I)
-        return fail(ctx, GRLBM_ERR_ARGUMENT, "null argument");
+    if (!ctx)
+        return GRLBM_ERR_ARGUMENT;
+    if (!I)
+        return fail(ctx, GRLBM_ERR_ARGUMENT, "null intensities");
     cudaSetDevice(ctx->device);
     const int64_t nxy = ctx->gd.nxy;
     const int nd = ctx->st.n;
     int rc = alloc(ctx, ctx->stage, (size_t)nxy * nd * sizeof(double));
     if (rc)
         return rc;
-    dim3 grid((unsigned)blocks(nxy, 32), (unsigned)blocks(nd, 32)), blk(32, 8);
     if (ctx->fp32)
-        k_to_cellmajor<float><<<grid, blk, 0, ctx->stream>>>(ctx->I[ctx->cur].as<float>(), ctx->stage.as<double>(), nxy, nd);
+        launch_to_cellmajor32(ctx->I[ctx->cur].as<float>(), ctx->stage.as<double>(), nxy, nd, ctx->stream);
     else
-        k_to_cellmajor<double><<<grid, blk, 0, ctx->stream>>>(ctx->I[ctx->cur].as<double>(), ctx->stage.as<double>(), nxy, nd);
+        launch_to_cellmajor64(ctx->I[ctx->cur].as<double>(), ctx->stage.as<double>(), nxy, nd, ctx->stream);
     CU(cudaGetLastError());
     CU(cudaMemcpyAsync(I, ctx->stage.p, ctx->stage.bytes, cudaMemcpyDeviceToHost, ctx->stream));
     CU(cudaStreamSynchronize(ctx->stream));
@@ -721,10 +728,10 @@ int grlbm_update_fourier_coefficients(grlbm_ctx *ctx, double rk_tol, int32_t max
     if (!(rk_tol > 0))
         return fail(ctx, GRLBM_ERR_ARGUMENT, "rk_tol must be positive");
     cudaSetDevice(ctx->device);
-    const int nf = ctx->ss.n, nd = ctx->st.n;
+    const int nf = ctx->ss.n;
     const int64_t ncell = ctx->ncell;
     unsigned long long *cnt = ctx->counters.as<unsigned long long>();
-    CU(cudaMemsetAsync(cnt + 2, 0, 3 * sizeof(unsigned long long), ctx->stream));
+    CU(cudaMemsetAsync(cnt + 2, 0, 2 * sizeof(unsigned long long), ctx->stream));
     void *data = nullptr;
     CU(cudaMallocAsync(&data, (size_t)5 * ncell * nf * sizeof(double), ctx->stream));
     cudaEvent_t e0, e1;
@@ -743,7 +750,7 @@ int grlbm_update_fourier_coefficients(grlbm_ctx *ctx, double rk_tol, int32_t max
     ga.data = static_cast<double *>(data);
     ga.trials_total = cnt + 2;
     ga.nonconverged = reinterpret_cast<int *>(cnt + 3);
-    k_geodesic<<<(unsigned)blocks(ncell * nf, 128), 128, 0, ctx->stream>>>(ga);
+    launch_geodesic(ga, ctx->stream);
 
     ProjectArgs pa{};
     pa.g = ctx->gd;
@@ -752,22 +759,8 @@ int grlbm_update_fourier_coefficients(grlbm_ctx *ctx, double rk_tol, int32_t max
     pa.ss_w = ctx->ss_w.as<double>();
     pa.basis = ctx->proj_basis.as<double>();
     pa.coef = ctx->coef.as<double>();
-    k_fourier_project<<<(unsigned)blocks(5 * ncell * nf, 128), 128, 0, ctx->stream>>>(pa);
-
-    DepartureArgs da{};
-    da.g = ctx->gd;
-    da.nf = nf;
-    da.nd = nd;
-    da.ng = ctx->ng;
-    da.coef = ctx->coef.as<double>();
-    da.eval = ctx->eval_basis.as<double>();
-    da.alpha = ctx->alpha.as<double>();
-    da.rot_c = approx_cos(0.0);
-    da.rot_s = approx_sin(0.0);
-    da.rec64 = ctx->fp32 ? nullptr : ctx->rec.as<double4>();
-    da.rec32 = ctx->fp32 ? ctx->rec.as<float4>() : nullptr;
-    da.clamped = reinterpret_cast<int *>(cnt + 4);
-    k_departure<<<(unsigned)blocks(ncell * nd, 128), 128, 0, ctx->stream>>>(da);
+    launch_project(pa, ctx->stream);
+    int rc = build_records(ctx);
     cudaEventRecord(e1, ctx->stream);
     cudaError_t le = cudaGetLastError();
     cudaFreeAsync(data, ctx->stream);
@@ -776,6 +769,8 @@ int grlbm_update_fourier_coefficients(grlbm_ctx *ctx, double rk_tol, int32_t max
     cudaEventElapsedTime(&ms, e0, e1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    if (rc)
+        return rc;
     if (le != cudaSuccess || se != cudaSuccess)
         return fail(ctx, GRLBM_ERR_CUDA, "table build failed: %s", cudaGetErrorString(le != cudaSuccess ? le : se));
     ctx->table_ms = ms;
@@ -785,6 +780,27 @@ int grlbm_update_fourier_coefficients(grlbm_ctx *ctx, double rk_tol, int32_t max
     const int nonconv = (int)(unsigned)h[3];
     if (nonconv > 0)
         return fail(ctx, GRLBM_ERR_NONCONVERGED, "%d RK45 backtraces hit the substep cap", nonconv);
+    return GRLBM_OK;
+}
+
+int grlbm_set_fourier_coefficients(grlbm_ctx *ctx, const double *S, const double *X, const double *Y,
+                                   const double *Cx, const double *Cy)
+{
+    if (!ctx)
+        return GRLBM_ERR_ARGUMENT;
+    if (!S || !X || !Y || !Cx || !Cy)
+        return fail(ctx, GRLBM_ERR_ARGUMENT, "null coefficient array");
+    cudaSetDevice(ctx->device);
+    const size_t per = (size_t)ctx->gd.nxy * ctx->ss.n;
+    const double *src[5] = {S, X, Y, Cx, Cy};
+    for (int q = 0; q < 5; q++)
+        CU(cudaMemcpyAsync(ctx->coef.as<double>() + q * per, src[q], per * sizeof(double), cudaMemcpyHostToDevice,
+                           ctx->stream));
+    int rc = build_records(ctx);
+    if (rc)
+        return rc;
+    CU(cudaStreamSynchronize(ctx->stream));
+    ctx->tables = true;
     return GRLBM_OK;
 }
 
@@ -803,8 +819,10 @@ int grlbm_get_fourier_coefficients(grlbm_ctx *ctx, double *S, double *X, double 
 
 int grlbm_step_async(grlbm_ctx *ctx, int32_t n_steps)
 {
-    if (!ctx || n_steps < 0)
-        return fail(ctx, GRLBM_ERR_ARGUMENT, "bad step count");
+    if (!ctx)
+        return GRLBM_ERR_ARGUMENT;
+    if (n_steps < 0)
+        return fail(ctx, GRLBM_ERR_ARGUMENT, "negative step count");
     if (ctx->run.streaming_type == GRLBM_CURVED_FIXED && !ctx->tables)
         return fail(ctx, GRLBM_ERR_STATE, "curved streaming needs grlbm_update_fourier_coefficients first");
     cudaSetDevice(ctx->device);
@@ -815,7 +833,7 @@ int grlbm_step_async(grlbm_ctx *ctx, int32_t n_steps)
         if (!ctx->graph[ctx->cur] && (rc = build_graph(ctx, ctx->cur)))
             return rc;
         CU(cudaGraphLaunch(ctx->graph[ctx->cur], ctx->stream));
-        left -= kGraphSteps; // even count: the current buffer is unchanged
+        left -= kGraphSteps; // an even count: the current buffer is unchanged
     }
     for (; left > 0; left--)
     {
@@ -850,17 +868,19 @@ int grlbm_get_moments_if(grlbm_ctx *ctx, double *E, double *Fx, double *Fy, doub
     cudaSetDevice(ctx->device);
     const int64_t nxy = ctx->gd.nxy;
     double *dst[6] = {E, Fx, Fy, Pxx, Pxy, Pyy};
-    int rc = alloc(ctx, ctx->lf_out, (size_t)7 * nxy * sizeof(double));
-    if (rc)
-        return rc;
+    const double *from = ctx->mom.as<double>();
     if (ctx->fp32)
-        k_copy_convert<float><<<(unsigned)blocks(6 * nxy, 256), 256, 0, ctx->stream>>>(ctx->mom.as<float>(), ctx->lf_out.as<double>(), 6 * nxy);
-    else
-        k_copy_convert<double><<<(unsigned)blocks(6 * nxy, 256), 256, 0, ctx->stream>>>(ctx->mom.as<double>(), ctx->lf_out.as<double>(), 6 * nxy);
-    CU(cudaGetLastError());
+    {
+        int rc = alloc(ctx, ctx->lf_out, (size_t)7 * nxy * sizeof(double));
+        if (rc)
+            return rc;
+        launch_widen32(ctx->mom.as<float>(), ctx->lf_out.as<double>(), 6 * nxy, ctx->stream);
+        CU(cudaGetLastError());
+        from = ctx->lf_out.as<double>();
+    }
     for (int q = 0; q < 6; q++)
         if (dst[q])
-            CU(cudaMemcpyAsync(dst[q], ctx->lf_out.as<double>() + q * nxy, nxy * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+            CU(cudaMemcpyAsync(dst[q], from + q * nxy, nxy * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     CU(cudaStreamSynchronize(ctx->stream));
     return GRLBM_OK;
 }
@@ -876,28 +896,34 @@ int grlbm_compute_moments_lf(grlbm_ctx *ctx, double *E, double *Fx, double *Fy, 
     if (rc)
         return rc;
     if (ctx->fp32)
-        k_moments_lf<float><<<(unsigned)blocks(nxy, 256), 256, 0, ctx->stream>>>(nxy, ctx->mom.as<float>(), ctx->lfp.as<double>(), ctx->bhmask.as<uint8_t>(), ctx->lf_out.as<double>());
+        launch_moments_lf32(nxy, ctx->mom.as<float>(), ctx->lfp.as<double>(), ctx->bhmask.as<uint8_t>(),
+                            ctx->lf_out.as<double>(), ctx->stream);
     else
-        k_moments_lf<double><<<(unsigned)blocks(nxy, 256), 256, 0, ctx->stream>>>(nxy, ctx->mom.as<double>(), ctx->lfp.as<double>(), ctx->bhmask.as<uint8_t>(), ctx->lf_out.as<double>());
+        launch_moments_lf64(nxy, ctx->mom.as<double>(), ctx->lfp.as<double>(), ctx->bhmask.as<uint8_t>(),
+                            ctx->lf_out.as<double>(), ctx->stream);
     CU(cudaGetLastError());
     double *dst[7] = {E, Fx, Fy, Pxx, Pxy, Pyy, F};
     for (int q = 0; q < 7; q++)
         if (dst[q])
-            CU(cudaMemcpyAsync(dst[q], ctx->lf_out.as<double>() + q * nxy, nxy * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+            CU(cudaMemcpyAsync(dst[q], ctx->lf_out.as<double>() + q * nxy, nxy * sizeof(double),
+                               cudaMemcpyDeviceToHost, ctx->stream));
     CU(cudaStreamSynchronize(ctx->stream));
     return GRLBM_OK;
 }
 
 int grlbm_energy(grlbm_ctx *ctx, double *total)
 {
-    if (!ctx || !total)
+    if (!ctx)
         return GRLBM_ERR_ARGUMENT;
+    if (!total)
+        return fail(ctx, GRLBM_ERR_ARGUMENT, "null output");
     cudaSetDevice(ctx->device);
     if (ctx->fp32)
-        k_energy_partial<float><<<kPartialBlocks, 256, 0, ctx->stream>>>(ctx->gd, ctx->mom.as<float>(), ctx->energy_partial.as<double>());
+        launch_energy32(ctx->gd, ctx->mom.as<float>(), ctx->energy_partial.as<double>(), kPartialBlocks,
+                        ctx->energy_out.as<double>(), ctx->stream);
     else
-        k_energy_partial<double><<<kPartialBlocks, 256, 0, ctx->stream>>>(ctx->gd, ctx->mom.as<double>(), ctx->energy_partial.as<double>());
-    k_energy_final<<<1, 256, 0, ctx->stream>>>(ctx->energy_partial.as<double>(), kPartialBlocks, ctx->energy_out.as<double>());
+        launch_energy64(ctx->gd, ctx->mom.as<double>(), ctx->energy_partial.as<double>(), kPartialBlocks,
+                        ctx->energy_out.as<double>(), ctx->stream);
     CU(cudaGetLastError());
     CU(cudaMemcpyAsync(total, ctx->energy_out.p, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     CU(cudaStreamSynchronize(ctx->stream));
@@ -906,8 +932,10 @@ int grlbm_energy(grlbm_ctx *ctx, double *total)
 
 int grlbm_get_stats(grlbm_ctx *ctx, grlbm_stats *s)
 {
-    if (!ctx || !s)
+    if (!ctx)
         return GRLBM_ERR_ARGUMENT;
+    if (!s)
+        return fail(ctx, GRLBM_ERR_ARGUMENT, "null output");
     cudaSetDevice(ctx->device);
     unsigned long long h[5];
     CU(cudaStreamSynchronize(ctx->stream));
@@ -918,6 +946,7 @@ int grlbm_get_stats(grlbm_ctx *ctx, grlbm_stats *s)
     s->average_iterations = ctx->steps ? (double)h[0] / denom : 0.0;
     s->rk_substeps = (int64_t)h[2];
     s->rk_nonconverged = (int32_t)(unsigned)h[3];
+    s->departures_off_grid = (int32_t)(unsigned)h[4];
     s->table_ms = ctx->table_ms;
     return GRLBM_OK;
 }

@@ -1,0 +1,454 @@
+// Plain FP64 form of the radiation step, and the FP64 utility kernels.
+//
+// Built with -fmad=false: every multiply and add rounds on its own, and every
+// expression below follows the association order of the reference's C++
+// (src/Radiation.cpp), so that -- given the same geodesic tables -- the state
+// after each step is bit-identical to the reference's IEEE build.  That is
+// what the 1e-12 parity needs: the lambda iteration stops on the relative
+// change of all six moments, including ones that are pure rounding noise
+// (e.g. Fy of a nearly isotropic cell), so its iteration counts, and through
+// them E, follow the last bits of the streamed intensities.
+#include "device_common.cuh"
+
+namespace grlbm
+{
+namespace
+{
+// one stream value: StreamFlatFixed (src/Radiation.cpp:394-410) or
+// StreamCurvedFixed with IntensityAt (:478-508, 322-343)
+template <bool CURVED>
+__device__ __forceinline__ double stream_value(const PlainStepArgs &a, int d, int64_t c, int64_t i, int64_t j,
+                                               int64_t ij)
+{
+    const int64_t nxy = a.g.nxy, nx = a.g.nx;
+    if constexpr (CURVED)
+    {
+        const double4 r = a.rec[(int64_t)d * a.g.ncell + c];
+        if (r.z < 0.0) // departure point inside the excision
+            return 0.0;
+        const double it = r.x, jt = r.y;
+        // corners kept on the grid whatever the record holds
+        const int64_t i0 = min(max((int64_t)floor(it), (int64_t)0), nx - 2);
+        const int64_t j0 = min(max((int64_t)floor(jt), (int64_t)0), a.g.ny - 2);
+        int g0 = (int)floor(r.z) % a.ng;
+        g0 = g0 < 0 ? 0 : g0;
+        const int g1 = (g0 + 1) % a.ng;
+        const double t = r.z - (double)g0;
+        int idx0[4], idx1[4];
+        double w0[4], w1[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+        {
+            idx0[k] = __ldg(a.ig_index + 4 * g0 + k);
+            idx1[k] = __ldg(a.ig_index + 4 * g1 + k);
+            w0[k] = __ldg(a.ig_w + 4 * g0 + k);
+            w1[k] = __ldg(a.ig_w + 4 * g1 + k);
+        }
+        const double al = __ldg(a.alpha + ij);
+        double Iq[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) // corners 00, 01, 10, 11
+        {
+            const int64_t ci = i0 + (q >> 1), cj = j0 + (q & 1);
+            const int64_t n = ci + cj * nx;
+            double v0 = 0.0, v1 = 0.0;
+#pragma unroll
+            for (int k = 0; k < 4; k++)
+            {
+                v0 += w0[k] * __ldg(a.Iin + (int64_t)idx0[k] * nxy + n);
+                v1 += w1[k] * __ldg(a.Iin + (int64_t)idx1[k] * nxy + n);
+            }
+            double v = v0 * (1.0 - t) + v1 * t;
+            v = (0.0 < v) ? v : 0.0;
+            const int64_t di = ci - i, dj = cj - j;
+            double cube;
+            if (di >= -1 && di <= 1 && dj >= -1 && dj <= 1)
+                cube = __ldg(a.acube + ij * 9 + 3 * (dj + 1) + (di + 1));
+            else
+            {
+                const double rr = al / __ldg(a.alpha + n);
+                cube = rr * (rr * rr);
+            }
+            Iq[q] = cube * v;
+        }
+        const double fx = it - (double)i0, fy = jt - (double)j0;
+        const double f0 = Iq[0] * (1.0 - fx) + Iq[2] * fx;
+        const double f1 = Iq[1] * (1.0 - fx) + Iq[3] * fx;
+        return r.w * (f0 * (1.0 - fy) + f1 * fy);
+    }
+    else
+    {
+        double xt = a.g.startx + (double)i * a.g.dx;
+        double yt = a.g.starty + (double)j * a.g.dy;
+        xt -= __ldg(a.cx + d) * a.g.dt;
+        yt -= __ldg(a.cy + d) * a.g.dt;
+        const double it = (xt - a.g.startx) / a.g.dx, jt = (yt - a.g.starty) / a.g.dy;
+        const int64_t i0 = min(max((int64_t)floor(it), (int64_t)0), nx - 2);
+        const int64_t j0 = min(max((int64_t)floor(jt), (int64_t)0), a.g.ny - 2);
+        const double *plane = a.Iin + (int64_t)d * nxy;
+        const int64_t c00 = i0 + j0 * nx;
+        const double fx = it - (double)i0, fy = jt - (double)j0;
+        const double f0 = __ldg(plane + c00) * (1.0 - fx) + __ldg(plane + c00 + 1) * fx;
+        const double f1 = __ldg(plane + c00 + nx) * (1.0 - fx) + __ldg(plane + c00 + nx + 1) * fx;
+        return f0 * (1.0 - fy) + f1 * fy;
+    }
+}
+
+struct Moments
+{
+    double E, Fx, Fy, Pxx, Pxy, Pyy;
+    __device__ __forceinline__ void zero() { E = Fx = Fy = Pxx = Pxy = Pyy = 0.0; }
+    // ComputeMomentsIF / Collide accumulation order (src/Radiation.cpp:259-266, 706-712)
+    __device__ __forceinline__ void add(double w, double v, double n1, double n2)
+    {
+        const double c = w * v;
+        E += c;
+        Fx += c * n1;
+        Fy += c * n2;
+        Pxx += c * n1 * n1;
+        Pxy += c * n1 * n2;
+        Pyy += c * n2 * n2;
+    }
+};
+
+// one collided intensity (src/Radiation.cpp:690-703).  Divisions by A, A*A
+// and (lorentz + 1) are skipped only where they are exact no-ops (A == 1,
+// un == 0), so the result is the reference's bit for bit.
+__device__ __forceinline__ double collide_value(double I, double n1, double n2, double u1, double u2, double lor,
+                                                double adt, double eta, double k0, double k3, double kak0,
+                                                double fE, double fFx, double fFy)
+{
+    const double un = u1 * n1 + u2 * n2;
+    const double A = lor * (1.0 - un);
+    const double sc = (un == 0.0) ? lor : (1 - (lor * un) / (lor + 1)) * lor;
+    double nF1 = n1 - sc * u1, nF2 = n2 - sc * u2;
+    if (A != 1.0)
+    {
+        nF1 = nF1 / A;
+        nF2 = nF2 / A;
+    }
+    const double nF = nF1 * fFx + nF2 * fFy;
+    const double M = k0 * fE + k3 * nF;
+    double src = adt * (eta + M);
+    const double AA = A * A;
+    if (AA != 1.0)
+        src = src / AA;
+    return (I + src) / (1.0 + adt * kak0 * A);
+}
+
+template <bool CURVED>
+__global__ void __launch_bounds__(kStepBlock) k_step_plain(PlainStepArgs a)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double *Is = reinterpret_cast<double *>(smem_raw);
+    const int t = threadIdx.x;
+    const int64_t c = (int64_t)blockIdx.x * kStepBlock + t;
+    const bool active = c < a.g.ncell;
+    const int64_t cc = active ? c : 0;
+    const int64_t i = 1 + cc % a.g.nx_, j = 1 + cc / a.g.nx_;
+    const int64_t ij = i + j * a.g.nx;
+    const int64_t nxy = a.g.nxy;
+    const uint8_t fl = active ? a.flags[ij] : (uint8_t)3;
+    const bool zero_stream = CURVED && (fl & 2);
+
+    Moments m;
+    m.zero();
+    for (int d = 0; d < a.nd; d++)
+    {
+        const double val = (active && !zero_stream) ? stream_value<CURVED>(a, d, cc, i, j, ij) : 0.0;
+        Is[d * kStepBlock + t] = val;
+        m.add(__ldg(a.w + d), val, __ldg(a.n1 + d), __ldg(a.n2 + d));
+    }
+
+    int cycles = 0;
+    if (active && !(fl & 1))
+    {
+        const double u1 = a.u1[ij], u2 = a.u2[ij], lor = a.lor[ij], adt = a.adt[ij];
+        const double eta = a.eta[ij], k0 = a.k0[ij], k3 = a.k3[ij], kak0 = a.ka[ij] + a.k0[ij];
+        double diff = 1;
+        double fE = 0, fFx = 0, fFy = 0;
+        while (fabs(diff) > 1e-4 && cycles < 100)
+        {
+            cycles++;
+            const double pE = m.E, pFx = m.Fx, pFy = m.Fy, pPxx = m.Pxx, pPxy = m.Pxy, pPyy = m.Pyy;
+            // fluid-frame moments of the previous iterate (src/Radiation.cpp:672-678)
+            const double uF = u1 * pFx + u2 * pFy;
+            const double uxP = u1 * pPxx + u2 * pPxy;
+            const double uyP = u1 * pPxy + u2 * pPyy;
+            const double uuP = u1 * uxP + u2 * uyP;
+            fE = lor * lor * (pE - 2.0 * uF + uuP);
+            fFx = lor * lor * (pFx - lor * pE * u1 - uxP + u1 * lor / (1.0 + lor) * ((2.0 * lor + 1.0) * uF - lor * uuP));
+            fFy = lor * lor * (pFy - lor * pE * u2 - uyP + u2 * lor / (1.0 + lor) * ((2.0 * lor + 1.0) * uF - lor * uuP));
+            m.zero();
+            for (int d = 0; d < a.nd; d++)
+            {
+                const double n1 = __ldg(a.n1 + d), n2 = __ldg(a.n2 + d);
+                const double v = collide_value(Is[d * kStepBlock + t], n1, n2, u1, u2, lor, adt, eta, k0, k3, kak0,
+                                               fE, fFx, fFy);
+                m.add(__ldg(a.w + d), v, n1, n2);
+            }
+            const double e1 = (pE - m.E) / m.E, e2 = (pFx - m.Fx) / m.Fx, e3 = (pFy - m.Fy) / m.Fy;
+            const double e4 = (pPxx - m.Pxx) / m.Pxx, e5 = (pPxy - m.Pxy) / m.Pxy, e6 = (pPyy - m.Pyy) / m.Pyy;
+            diff = sqrt(e1 * e1 + e2 * e2 + e3 * e3 + e4 * e4 + e5 * e5 + e6 * e6);
+        }
+        // the last iterate, recomputed from the same operands
+        for (int d = 0; d < a.nd; d++)
+        {
+            const double v = collide_value(Is[d * kStepBlock + t], __ldg(a.n1 + d), __ldg(a.n2 + d), u1, u2, lor, adt,
+                                           eta, k0, k3, kak0, fE, fFx, fFy);
+            a.Iout[(int64_t)d * nxy + ij] = v;
+        }
+    }
+    if (active)
+    {
+        a.mom[ij] = m.E;
+        a.mom[ij + nxy] = m.Fx;
+        a.mom[ij + 2 * nxy] = m.Fy;
+        a.mom[ij + 3 * nxy] = m.Pxx;
+        a.mom[ij + 4 * nxy] = m.Pxy;
+        a.mom[ij + 5 * nxy] = m.Pyy;
+    }
+    __shared__ unsigned int s_sum, s_max;
+    if (t == 0)
+    {
+        s_sum = 0;
+        s_max = 0;
+    }
+    __syncthreads();
+    if (cycles)
+    {
+        atomicAdd(&s_sum, (unsigned int)cycles);
+        atomicMax(&s_max, (unsigned int)cycles);
+    }
+    __syncthreads();
+    if (t == 0 && s_sum)
+    {
+        atomicAdd(a.iter_sum, (unsigned long long)s_sum);
+        atomicMax(a.iter_max, s_max);
+    }
+}
+
+// Radiation::LoadInitialData for fixed streaming (src/Radiation.cpp:138-181)
+template <typename T>
+__global__ void k_sources(T *I, int64_t nxy, int nd, const int64_t *nodes, const T *vals, int64_t nsrc)
+{
+    const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= nsrc * nd)
+        return;
+    const int64_t s = tid / nd;
+    const int d = (int)(tid - s * nd);
+    I[(int64_t)d * nxy + nodes[s]] = vals[tid];
+}
+
+// Radiation::ComputeMomentsLF (src/Radiation.cpp:270-301)
+template <typename T>
+__global__ void k_moments_lf(int64_t nxy, const T *mom, const double *lfp, const uint8_t *bh, double *out)
+{
+    const int64_t ij = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (ij >= nxy)
+        return;
+    double o[7] = {0, 0, 0, 0, 0, 0, 0};
+    if (!bh[ij])
+    {
+        const double E = mom[ij], Fx = mom[ij + nxy], Fy = mom[ij + 2 * nxy];
+        const double Pxx = mom[ij + 3 * nxy], Pxy = mom[ij + 4 * nxy], Pyy = mom[ij + 5 * nxy];
+        const double Tm[9] = {E, Fx, Fy, Fx, Pxx, Pxy, Fy, Pxy, Pyy};
+        const double *e = lfp + ij * 12;
+        double L[9];
+#pragma unroll
+        for (int a_ = 0; a_ < 3; a_++)
+#pragma unroll
+            for (int b = 0; b < 3; b++)
+            {
+                double s = 0.0;
+#pragma unroll
+                for (int A = 0; A < 3; A++)
+#pragma unroll
+                    for (int B = 0; B < 3; B++)
+                        s += Tm[3 * A + B] * e[3 * a_ + A] * e[3 * b + B];
+                L[3 * a_ + b] = s;
+            }
+        o[0] = L[0];
+        o[1] = L[1];
+        o[2] = L[2];
+        o[3] = L[4];
+        o[4] = L[5];
+        o[5] = L[8];
+        const double g11 = e[9], g12 = e[10], g22 = e[11];
+        // Norm2 (src/SpecialMath.cpp:20-27): sum_i sum_j gamma_ij v_i v_j
+        double n2 = 0.0;
+        n2 += g11 * o[1] * o[1];
+        n2 += g12 * o[1] * o[2];
+        n2 += g12 * o[2] * o[1];
+        n2 += g22 * o[2] * o[2];
+        o[6] = sqrt(fabs(n2));
+    }
+#pragma unroll
+    for (int q = 0; q < 7; q++)
+        out[ij + q * nxy] = o[q];
+}
+
+// global energy: fixed-order partial sums of interior E, then one block
+template <typename T>
+__global__ void __launch_bounds__(256) k_energy_partial(GridDev g, const T *E, double *partial)
+{
+    __shared__ double s[256];
+    const int t = threadIdx.x;
+    double acc = 0.0;
+    for (int64_t c = (int64_t)blockIdx.x * 256 + t; c < g.ncell; c += (int64_t)gridDim.x * 256)
+    {
+        const int64_t i = 1 + c % g.nx_, j = 1 + c / g.nx_;
+        acc += (double)E[i + j * g.nx];
+    }
+    s[t] = acc;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1)
+    {
+        if (t < w)
+            s[t] += s[t + w];
+        __syncthreads();
+    }
+    if (t == 0)
+        partial[blockIdx.x] = s[0];
+}
+
+__global__ void __launch_bounds__(256) k_energy_final(const double *partial, int n, double *out)
+{
+    __shared__ double s[256];
+    const int t = threadIdx.x;
+    double acc = 0.0;
+    for (int k = t; k < n; k += 256)
+        acc += partial[k];
+    s[t] = acc;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1)
+    {
+        if (t < w)
+            s[t] += s[t + w];
+        __syncthreads();
+    }
+    if (t == 0)
+        *out = s[0];
+}
+
+// cell-major double [ij][d] <-> direction-major T [d][ij]
+template <class T>
+__global__ void k_to_dirmajor(const double *in, T *out, int64_t nxy, int nd)
+{
+    __shared__ double tile[32][33];
+    const int64_t ij0 = (int64_t)blockIdx.x * 32;
+    const int d0 = blockIdx.y * 32;
+    for (int r = threadIdx.y; r < 32; r += 8)
+    {
+        const int64_t ij = ij0 + r;
+        const int d = d0 + threadIdx.x;
+        if (ij < nxy && d < nd)
+            tile[r][threadIdx.x] = in[ij * nd + d];
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += 8)
+    {
+        const int d = d0 + r;
+        const int64_t ij = ij0 + threadIdx.x;
+        if (ij < nxy && d < nd)
+            out[(int64_t)d * nxy + ij] = (T)tile[threadIdx.x][r];
+    }
+}
+template <class T>
+__global__ void k_to_cellmajor(const T *in, double *out, int64_t nxy, int nd)
+{
+    __shared__ double tile[32][33];
+    const int64_t ij0 = (int64_t)blockIdx.x * 32;
+    const int d0 = blockIdx.y * 32;
+    for (int r = threadIdx.y; r < 32; r += 8)
+    {
+        const int d = d0 + r;
+        const int64_t ij = ij0 + threadIdx.x;
+        if (ij < nxy && d < nd)
+            tile[threadIdx.x][r] = (double)in[(int64_t)d * nxy + ij];
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += 8)
+    {
+        const int64_t ij = ij0 + r;
+        const int d = d0 + threadIdx.x;
+        if (ij < nxy && d < nd)
+            out[ij * nd + d] = tile[r][threadIdx.x];
+    }
+}
+__global__ void k_widen(const float *in, double *out, int64_t n)
+{
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n)
+        out[k] = (double)in[k];
+}
+
+inline unsigned nblk(int64_t n, int b) { return (unsigned)((n + b - 1) / b); }
+} // namespace
+
+cudaError_t prepare_step_plain(int smem_bytes)
+{
+    cudaError_t e = cudaFuncSetAttribute(k_step_plain<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
+    if (e != cudaSuccess)
+        return e;
+    return cudaFuncSetAttribute(k_step_plain<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
+}
+void launch_step_plain(const PlainStepArgs &a, bool curved, cudaStream_t s)
+{
+    const size_t smem = (size_t)a.nd * kStepBlock * sizeof(double);
+    if (curved)
+        k_step_plain<true><<<nblk(a.g.ncell, kStepBlock), kStepBlock, smem, s>>>(a);
+    else
+        k_step_plain<false><<<nblk(a.g.ncell, kStepBlock), kStepBlock, smem, s>>>(a);
+}
+void launch_sources64(double *I, int64_t nxy, int nd, const int64_t *nodes, const double *vals, int64_t nsrc,
+                      cudaStream_t s)
+{
+    k_sources<double><<<nblk(nsrc * nd, 256), 256, 0, s>>>(I, nxy, nd, nodes, vals, nsrc);
+}
+void launch_sources32(float *I, int64_t nxy, int nd, const int64_t *nodes, const float *vals, int64_t nsrc,
+                      cudaStream_t s)
+{
+    k_sources<float><<<nblk(nsrc * nd, 256), 256, 0, s>>>(I, nxy, nd, nodes, vals, nsrc);
+}
+void launch_moments_lf64(int64_t nxy, const double *mom, const double *lfp, const uint8_t *bh, double *out,
+                         cudaStream_t s)
+{
+    k_moments_lf<double><<<nblk(nxy, 256), 256, 0, s>>>(nxy, mom, lfp, bh, out);
+}
+void launch_moments_lf32(int64_t nxy, const float *mom, const double *lfp, const uint8_t *bh, double *out,
+                         cudaStream_t s)
+{
+    k_moments_lf<float><<<nblk(nxy, 256), 256, 0, s>>>(nxy, mom, lfp, bh, out);
+}
+void launch_energy64(const GridDev &g, const double *E, double *partial, int nblocks, double *out, cudaStream_t s)
+{
+    k_energy_partial<double><<<nblocks, 256, 0, s>>>(g, E, partial);
+    k_energy_final<<<1, 256, 0, s>>>(partial, nblocks, out);
+}
+void launch_energy32(const GridDev &g, const float *E, double *partial, int nblocks, double *out, cudaStream_t s)
+{
+    k_energy_partial<float><<<nblocks, 256, 0, s>>>(g, E, partial);
+    k_energy_final<<<1, 256, 0, s>>>(partial, nblocks, out);
+}
+void launch_to_dirmajor64(const double *in, double *out, int64_t nxy, int nd, cudaStream_t s)
+{
+    k_to_dirmajor<double><<<dim3(nblk(nxy, 32), nblk(nd, 32)), dim3(32, 8), 0, s>>>(in, out, nxy, nd);
+}
+void launch_to_dirmajor32(const double *in, float *out, int64_t nxy, int nd, cudaStream_t s)
+{
+    k_to_dirmajor<float><<<dim3(nblk(nxy, 32), nblk(nd, 32)), dim3(32, 8), 0, s>>>(in, out, nxy, nd);
+}
+void launch_to_cellmajor64(const double *in, double *out, int64_t nxy, int nd, cudaStream_t s)
+{
+    k_to_cellmajor<double><<<dim3(nblk(nxy, 32), nblk(nd, 32)), dim3(32, 8), 0, s>>>(in, out, nxy, nd);
+}
+void launch_to_cellmajor32(const float *in, double *out, int64_t nxy, int nd, cudaStream_t s)
+{
+    k_to_cellmajor<float><<<dim3(nblk(nxy, 32), nblk(nd, 32)), dim3(32, 8), 0, s>>>(in, out, nxy, nd);
+}
+void launch_widen32(const float *in, double *out, int64_t n, cudaStream_t s)
+{
+    k_widen<<<nblk(n, 256), 256, 0, s>>>(in, out, n);
+}
+} // namespace grlbm

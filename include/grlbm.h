@@ -101,6 +101,9 @@ typedef struct
                                  as src/Radiation.cpp:856 */
     int64_t rk_substeps;      /* accepted + rejected RK45 trials of the table build */
     int32_t rk_nonconverged;  /* backtraces stopped by the substep cap */
+    int32_t departures_off_grid; /* departure points outside the grid (whose
+                                    corners are clamped onto it); the reference
+                                    reads past its arrays there */
     double table_ms;          /* device time of the last table build */
 } grlbm_stats;
 
@@ -148,7 +151,12 @@ int grlbm_get_intensity(grlbm_ctx *ctx, double *I);
  * a backtrace that hits it is counted in grlbm_stats.rk_nonconverged and the
  * call returns GRLBM_ERR_NONCONVERGED after finishing the others. */
 int grlbm_update_fourier_coefficients(grlbm_ctx *ctx, double rk_tol, int32_t max_substeps);
-/* coefficientsS/X/Y/Cx/Cy (src/Radiation.h:75-79): nx*ny*nF each. */
+/* The public coefficient buffers coefficientsS/X/Y/Cx/Cy
+ * (src/Radiation.h:75-79, [ij*nF + k]), nx*ny*nF each: set them (as a caller
+ * of the reference may) and rebuild the departure records from them, or read
+ * them back. */
+int grlbm_set_fourier_coefficients(grlbm_ctx *ctx, const double *S, const double *X, const double *Y,
+                                   const double *Cx, const double *Cy);
 int grlbm_get_fourier_coefficients(grlbm_ctx *ctx, double *S, double *X, double *Y,
                                    double *Cx, double *Cy);
 
