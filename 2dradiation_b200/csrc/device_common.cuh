@@ -21,6 +21,8 @@
 //                                         departure inside the excision)
 //   FP32 record  rec32[d * ncell + c]     {i_dep - i, j_dep - j, angle coordinate,
 //                                         s^3 alpha_c^3 (0 when excised)}
+//   FP32 state   J = I / alpha^3 for curved streaming (I for flat); the
+//                                         C-ABI converts at its boundary
 //   rk fields    rkf[ij * kRkStride + f]  node-major pack of the 21 metric arrays
 //                                         the geodesic right-hand side reads and
 //                                         the 2x2 spatial tetrad blocks
@@ -131,18 +133,24 @@ struct PrecStepArgs
     const float *Iin;
     float *Iout;
     const float4 *rec;
-    const float *w, *n1, *n2; // nd
-    const double *cx, *cy;    // nd (flat departures)
-    const int *ig_base;       // ng: first direction of the cubic row
-    const int *ig_shift;      // ng: first(g+1) - first(g), 0 or 1
-    const float *ig_w;        // ng*4
-    const float *ia3;         // nxy: 1/alpha^3
+    float dir_per_row;        // nDir / nGrid: direction spacing of the interpolation grid rows
+    const float *ia3;         // nxy: 1/alpha^3 (scale of the stored state)
     const uint8_t *flags;
     const float *u1, *u2, *lor, *adt, *eta, *k0, *k3, *ka;
-    const float *wmom;        // 18 stencil sums: sum_d w mu_q (q<6), * n1 (6), * n2 (6)
     float *mom;               // 6*nxy
     unsigned long long *iter_sum;
     unsigned int *iter_max;
+};
+
+// Direction tables of the precision form, passed by value as a kernel
+// parameter (uniform constant-bank reads): quadrature weights, rotated
+// directions, flat-space departure offsets in cells, and the 18 stencil sums
+// of the affine collide map (sum_d w mu_q, times n1, times n2 for
+// mu = 1, n1, n2, n1^2, n1 n2, n2^2).
+struct DirTable
+{
+    float w[kMaxDirs], n1[kMaxDirs], n2[kMaxDirs], ox[kMaxDirs], oy[kMaxDirs];
+    float wmom[18];
 };
 
 // ---- launchers (defined in the kernel translation units) ----
@@ -154,7 +162,8 @@ void launch_alpha_cube(const GridDev &g, const double *alpha, double *acube, cud
 cudaError_t prepare_step_plain(int smem_bytes);
 void launch_step_plain(const PlainStepArgs &a, bool curved, cudaStream_t s);
 cudaError_t prepare_step_prec(int smem_bytes);
-void launch_step_prec(const PrecStepArgs &a, bool curved, cudaStream_t s);
+size_t step_prec_smem(int nd);
+void launch_step_prec(const PrecStepArgs &a, const DirTable &dt, bool curved, cudaStream_t s);
 
 void launch_sources64(double *I, int64_t nxy, int nd, const int64_t *nodes, const double *vals, int64_t nsrc,
                       cudaStream_t s);
@@ -167,8 +176,8 @@ void launch_moments_lf32(int64_t nxy, const float *mom, const double *lfp, const
 void launch_energy64(const GridDev &g, const double *E, double *partial, int nblocks, double *out, cudaStream_t s);
 void launch_energy32(const GridDev &g, const float *E, double *partial, int nblocks, double *out, cudaStream_t s);
 void launch_to_dirmajor64(const double *in, double *out, int64_t nxy, int nd, cudaStream_t s);
-void launch_to_dirmajor32(const double *in, float *out, int64_t nxy, int nd, cudaStream_t s);
+void launch_to_dirmajor32(const double *in, float *out, int64_t nxy, int nd, const float *scale, cudaStream_t s);
 void launch_to_cellmajor64(const double *in, double *out, int64_t nxy, int nd, cudaStream_t s);
-void launch_to_cellmajor32(const float *in, double *out, int64_t nxy, int nd, cudaStream_t s);
+void launch_to_cellmajor32(const float *in, double *out, int64_t nxy, int nd, const float *scale, cudaStream_t s);
 void launch_widen32(const float *in, double *out, int64_t n, cudaStream_t s);
 } // namespace grlbm

@@ -57,7 +57,8 @@ struct grlbm_ctx
     int ng = 0;
     // device buffers (storage type T = double for the plain form, float for the precision form)
     DevBuf I[2], rec, w, n1, n2, cx, cy, flags, bhmask, alpha, acube;
-    DevBuf ig_index, ig_w64, ig_base, ig_shift, ig_w32, ia3, wmom;
+    DevBuf ig_index, ig_w64, rows, ia3;
+    DirTable dirs{}; // precision-form direction tables (kernel parameter)
     DevBuf cu1, cu2, clor, cadt, ceta, ck0, ck3, cka, mom, rkf, lfp;
     DevBuf coef, ss_cx, ss_cy, ss_w, proj_basis, eval_basis, stage;
     DevBuf src_nodes, src_vals, lf_out, energy_partial, energy_out;
@@ -154,6 +155,12 @@ void invalidate_graphs(grlbm_ctx *ctx)
         }
 }
 
+// per-node factor between the precision form's stored state and I (null: none)
+const float *state_scale(const grlbm_ctx *ctx)
+{
+    return (ctx->fp32 && ctx->run.streaming_type == GRLBM_CURVED_FIXED) ? ctx->ia3.as<float>() : nullptr;
+}
+
 // Enqueue one step starting from buffer `from` (no sync).
 int enqueue_step(grlbm_ctx *ctx, int from)
 {
@@ -171,14 +178,7 @@ int enqueue_step(grlbm_ctx *ctx, int from)
         a.Iin = ctx->I[from].as<float>();
         a.Iout = ctx->I[from ^ 1].as<float>();
         a.rec = ctx->rec.as<float4>();
-        a.w = ctx->w.as<float>();
-        a.n1 = ctx->n1.as<float>();
-        a.n2 = ctx->n2.as<float>();
-        a.cx = ctx->cx.as<double>();
-        a.cy = ctx->cy.as<double>();
-        a.ig_base = ctx->ig_base.as<int>();
-        a.ig_shift = ctx->ig_shift.as<int>();
-        a.ig_w = ctx->ig_w32.as<float>();
+        a.dir_per_row = (float)((double)ctx->st.n / (double)ctx->ng);
         a.ia3 = ctx->ia3.as<float>();
         a.flags = ctx->flags.as<uint8_t>();
         a.u1 = ctx->cu1.as<float>();
@@ -189,11 +189,10 @@ int enqueue_step(grlbm_ctx *ctx, int from)
         a.k0 = ctx->ck0.as<float>();
         a.k3 = ctx->ck3.as<float>();
         a.ka = ctx->cka.as<float>();
-        a.wmom = ctx->wmom.as<float>();
         a.mom = ctx->mom.as<float>();
         a.iter_sum = cnt;
         a.iter_max = reinterpret_cast<unsigned int *>(cnt + 1);
-        launch_step_prec(a, curved, ctx->stream);
+        launch_step_prec(a, ctx->dirs, curved, ctx->stream);
     }
     else
     {
@@ -351,6 +350,9 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
     const int maxdir = run->precision == GRLBM_PLAIN_FP64 ? kMaxDirsPlain : kMaxDirs;
     if (run->n_dir < 4 || run->n_dir > maxdir)
         return fail(nullptr, GRLBM_ERR_ARGUMENT, "n_dir must be in [4, %d]", maxdir);
+    if (run->precision == GRLBM_PRECISION_FP32 &&
+        (double)(grid->nx_ + 2) * (double)(grid->ny_ + 2) * (double)run->n_dir >= 2147483648.0)
+        return fail(nullptr, GRLBM_ERR_ARGUMENT, "the precision form indexes with 32 bits: nx*ny*n_dir must be < 2^31");
     if (run->n_fourier < 1 || run->n_fourier > kMaxFourier)
         return fail(nullptr, GRLBM_ERR_ARGUMENT, "n_fourier must be in [1, %d]", kMaxFourier);
     if (run->initial_data_type != GRLBM_MOMENTS && run->initial_data_type != GRLBM_INTENSITIES)
@@ -436,8 +438,10 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
     TRY(upload(ctx, ctx->cy, ctx->st.cy));
     if (ctx->fp32)
     {
-        // cubic rows as a first direction plus the step to the next row
-        std::vector<int> base(ctx->ng), shift(ctx->ng);
+        // each cubic row g blended with row g+1 into one 5-direction window
+        // starting at row g's first direction: weights W0 + t D, packed as
+        // {W0[0..3]}, {D[0..3]}, {W0[4], D[4], first direction (int bits), 0}
+        std::vector<int> base(ctx->ng);
         for (int g = 0; g < ctx->ng; g++)
         {
             base[g] = (int)ctx->st.ig_index[4 * g];
@@ -445,21 +449,41 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
                 if (ctx->st.ig_index[4 * g + k] != (base[g] + k) % nd)
                     return fail(nullptr, GRLBM_ERR_HOST, "interpolation row %d is not 4 consecutive directions", g);
         }
+        std::vector<float> rows((size_t)ctx->ng * 12, 0.f);
         for (int g = 0; g < ctx->ng; g++)
         {
-            shift[g] = ((base[(g + 1) % ctx->ng] - base[g]) % nd + nd) % nd;
-            if (shift[g] > 1)
-                return fail(nullptr, GRLBM_ERR_HOST, "interpolation rows %d, %d are %d directions apart", g, g + 1,
-                            shift[g]);
+            const int g1 = (g + 1) % ctx->ng;
+            const int shift = ((base[g1] - base[g]) % nd + nd) % nd;
+            if (shift > 1)
+                return fail(nullptr, GRLBM_ERR_HOST, "interpolation rows %d, %d are %d directions apart", g, g1, shift);
+            double W0[5] = {0, 0, 0, 0, 0}, W1[5] = {0, 0, 0, 0, 0};
+            for (int k = 0; k < 4; k++)
+            {
+                W0[k] = ctx->st.ig_weight[4 * g + k];
+                W1[k + shift] = ctx->st.ig_weight[4 * g1 + k];
+            }
+            float *r = &rows[(size_t)g * 12];
+            for (int k = 0; k < 4; k++)
+            {
+                r[k] = (float)W0[k];
+                r[4 + k] = (float)(W1[k] - W0[k]);
+            }
+            r[8] = (float)W0[4];
+            r[9] = (float)(W1[4] - W0[4]);
+            std::memcpy(&r[10], &base[g], sizeof(int));
         }
-        TRY(upload(ctx, ctx->ig_base, base));
-        TRY(upload(ctx, ctx->ig_shift, shift));
-        std::vector<float> w32(ctx->st.ig_weight.begin(), ctx->st.ig_weight.end());
-        TRY(upload(ctx, ctx->ig_w32, w32));
-        // stencil sums of the affine collide map: sum_d w mu_q, * n1, * n2
-        std::vector<double> wm(18, 0.0);
+        TRY(upload(ctx, ctx->rows, rows));
+        // direction tables: weights, rotated directions, flat departures, and
+        // the stencil sums of the affine collide map
+        DirTable &dt = ctx->dirs;
+        double wm[18] = {0};
         for (int d = 0; d < nd; d++)
         {
+            dt.w[d] = (float)ctx->st.w[d];
+            dt.n1[d] = (float)n1[d];
+            dt.n2[d] = (float)n2[d];
+            dt.ox[d] = (float)(-ctx->st.cx[d] * G.dt / G.dx);
+            dt.oy[d] = (float)(-ctx->st.cy[d] * G.dt / G.dy);
             const double mu[6] = {1.0, n1[d], n2[d], n1[d] * n1[d], n1[d] * n2[d], n2[d] * n2[d]};
             for (int q = 0; q < 6; q++)
             {
@@ -468,7 +492,8 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
                 wm[12 + q] += ctx->st.w[d] * mu[q] * n2[d];
             }
         }
-        TRY(upload_t(ctx, ctx->wmom, wm));
+        for (int q = 0; q < 18; q++)
+            dt.wmom[q] = (float)wm[q];
     }
     else
     {
@@ -547,7 +572,7 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
     // fields default to zero (the reference's buffers are value-initialised)
     std::vector<double> zeros(nxy, 0.0);
     TRY(grlbm_set_fields(ctx, zeros.data(), zeros.data(), zeros.data(), zeros.data(), zeros.data(), zeros.data()));
-    const int smem = (int)((size_t)nd * kStepBlock * tsize(ctx));
+    const int smem = (int)(ctx->fp32 ? step_prec_smem(nd) : (size_t)nd * kStepBlock * sizeof(double));
     if ((ctx->fp32 ? prepare_step_prec(smem) : prepare_step_plain(smem)) != cudaSuccess)
         return fail(nullptr, GRLBM_ERR_CUDA, "cannot reserve %d bytes of shared memory for the step kernel", smem);
     if (cudaDeviceSynchronize() != cudaSuccess)
@@ -645,6 +670,18 @@ int grlbm_set_initial_data(grlbm_ctx *ctx, const uint8_t *is_initial, const doub
         return fail(ctx, GRLBM_ERR_HOST, "source set-up failed: %s", e.what());
     }
     ctx->nsrc = (int64_t)S.nodes.size();
+    if (ctx->fp32 && ctx->run.streaming_type == GRLBM_CURVED_FIXED)
+    {
+        // the precision form stores I / alpha^3
+        const int nd = ctx->st.n;
+        for (size_t s_ = 0; s_ < S.nodes.size(); s_++)
+        {
+            const double a = ctx->M.at(ALPHA, S.nodes[s_]);
+            const float scale = (float)(1.0 / (a * a * a));
+            for (int d = 0; d < nd; d++)
+                S.intensities[s_ * nd + d] = (double)((float)S.intensities[s_ * nd + d] * scale);
+        }
+    }
     int rc;
     if ((rc = upload(ctx, ctx->src_nodes, S.nodes)) || (rc = upload_t(ctx, ctx->src_vals, S.intensities)))
         return rc;
@@ -690,7 +727,7 @@ int grlbm_set_intensity(grlbm_ctx *ctx, const double *I)
     for (int b = 0; b < 2; b++)
     {
         if (ctx->fp32)
-            launch_to_dirmajor32(ctx->stage.as<double>(), ctx->I[b].as<float>(), nxy, nd, ctx->stream);
+            launch_to_dirmajor32(ctx->stage.as<double>(), ctx->I[b].as<float>(), nxy, nd, state_scale(ctx), ctx->stream);
         else
             launch_to_dirmajor64(ctx->stage.as<double>(), ctx->I[b].as<double>(), nxy, nd, ctx->stream);
     }
@@ -712,7 +749,8 @@ int grlbm_get_intensity(grlbm_ctx *ctx, double *I)
     if (rc)
         return rc;
     if (ctx->fp32)
-        launch_to_cellmajor32(ctx->I[ctx->cur].as<float>(), ctx->stage.as<double>(), nxy, nd, ctx->stream);
+        launch_to_cellmajor32(ctx->I[ctx->cur].as<float>(), ctx->stage.as<double>(), nxy, nd, state_scale(ctx),
+                              ctx->stream);
     else
         launch_to_cellmajor64(ctx->I[ctx->cur].as<double>(), ctx->stage.as<double>(), nxy, nd, ctx->stream);
     CU(cudaGetLastError());

@@ -333,7 +333,7 @@ __global__ void __launch_bounds__(256) k_energy_final(const double *partial, int
 
 // cell-major double [ij][d] <-> direction-major T [d][ij]
 template <class T>
-__global__ void k_to_dirmajor(const double *in, T *out, int64_t nxy, int nd)
+__global__ void k_to_dirmajor(const double *in, T *out, int64_t nxy, int nd, const float *scale)
 {
     __shared__ double tile[32][33];
     const int64_t ij0 = (int64_t)blockIdx.x * 32;
@@ -351,11 +351,11 @@ __global__ void k_to_dirmajor(const double *in, T *out, int64_t nxy, int nd)
         const int d = d0 + r;
         const int64_t ij = ij0 + threadIdx.x;
         if (ij < nxy && d < nd)
-            out[(int64_t)d * nxy + ij] = (T)tile[threadIdx.x][r];
+            out[(int64_t)d * nxy + ij] = scale ? (T)tile[threadIdx.x][r] * (T)scale[ij] : (T)tile[threadIdx.x][r];
     }
 }
 template <class T>
-__global__ void k_to_cellmajor(const T *in, double *out, int64_t nxy, int nd)
+__global__ void k_to_cellmajor(const T *in, double *out, int64_t nxy, int nd, const float *scale)
 {
     __shared__ double tile[32][33];
     const int64_t ij0 = (int64_t)blockIdx.x * 32;
@@ -365,7 +365,8 @@ __global__ void k_to_cellmajor(const T *in, double *out, int64_t nxy, int nd)
         const int d = d0 + r;
         const int64_t ij = ij0 + threadIdx.x;
         if (ij < nxy && d < nd)
-            tile[threadIdx.x][r] = (double)in[(int64_t)d * nxy + ij];
+            tile[threadIdx.x][r] = scale ? (double)in[(int64_t)d * nxy + ij] / (double)scale[ij]
+                                         : (double)in[(int64_t)d * nxy + ij];
     }
     __syncthreads();
     for (int r = threadIdx.y; r < 32; r += 8)
@@ -433,19 +434,19 @@ void launch_energy32(const GridDev &g, const float *E, double *partial, int nblo
 }
 void launch_to_dirmajor64(const double *in, double *out, int64_t nxy, int nd, cudaStream_t s)
 {
-    k_to_dirmajor<double><<<dim3(nblk(nxy, 32), nblk(nd, 32)), dim3(32, 8), 0, s>>>(in, out, nxy, nd);
+    k_to_dirmajor<double><<<dim3(nblk(nxy, 32), nblk(nd, 32)), dim3(32, 8), 0, s>>>(in, out, nxy, nd, nullptr);
 }
-void launch_to_dirmajor32(const double *in, float *out, int64_t nxy, int nd, cudaStream_t s)
+void launch_to_dirmajor32(const double *in, float *out, int64_t nxy, int nd, const float *scale, cudaStream_t s)
 {
-    k_to_dirmajor<float><<<dim3(nblk(nxy, 32), nblk(nd, 32)), dim3(32, 8), 0, s>>>(in, out, nxy, nd);
+    k_to_dirmajor<float><<<dim3(nblk(nxy, 32), nblk(nd, 32)), dim3(32, 8), 0, s>>>(in, out, nxy, nd, scale);
 }
 void launch_to_cellmajor64(const double *in, double *out, int64_t nxy, int nd, cudaStream_t s)
 {
-    k_to_cellmajor<double><<<dim3(nblk(nxy, 32), nblk(nd, 32)), dim3(32, 8), 0, s>>>(in, out, nxy, nd);
+    k_to_cellmajor<double><<<dim3(nblk(nxy, 32), nblk(nd, 32)), dim3(32, 8), 0, s>>>(in, out, nxy, nd, nullptr);
 }
-void launch_to_cellmajor32(const float *in, double *out, int64_t nxy, int nd, cudaStream_t s)
+void launch_to_cellmajor32(const float *in, double *out, int64_t nxy, int nd, const float *scale, cudaStream_t s)
 {
-    k_to_cellmajor<float><<<dim3(nblk(nxy, 32), nblk(nd, 32)), dim3(32, 8), 0, s>>>(in, out, nxy, nd);
+    k_to_cellmajor<float><<<dim3(nblk(nxy, 32), nblk(nd, 32)), dim3(32, 8), 0, s>>>(in, out, nxy, nd, scale);
 }
 void launch_widen32(const float *in, double *out, int64_t n, cudaStream_t s)
 {
