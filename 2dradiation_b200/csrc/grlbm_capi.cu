@@ -521,7 +521,10 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
         lfp[ij * 12 + 11] = M.at(GAM22L, ij);
         const double a = M.at(ALPHA, ij);
         alpha[ij] = a;
-        ia3[ij] = 1.0 / (a * a * a);
+        // A node exactly on the singularity has alpha = 0; it lies inside the
+        // excision, keeps its intensity, and stores it unscaled.
+        const double s = 1.0 / (a * a * a);
+        ia3[ij] = (std::isfinite(s) && std::isfinite((float)s) && (float)s > 0.f) ? s : 1.0;
         const bool inside = M.inside_bh(G.x((double)(ij % G.nx)), G.y((double)(ij / G.nx)));
         bh[ij] = inside;
         flags[ij] = inside ? 3 : 0;

@@ -293,7 +293,7 @@ def run_grlbm(a, world, rank, local, pg):
             "peak_kind": peak_kind,
             "unit": "GB/s",
             "frac": ach32 / peak,
-            "traffic": profiled_traffic("k_step_fp32"),
+            "traffic": profiled_traffic("k_step_prec"),
             "algorithmic_bytes_per_update": b32,
             "kernel": "k_step<float, curved>",
         },
@@ -303,7 +303,7 @@ def run_grlbm(a, world, rank, local, pg):
             "roofline_frac": ach64 / peak,
             "achieved_gbs": ach64,
             "algorithmic_bytes_per_update": b64,
-            "traffic": profiled_traffic("k_step_fp64"),
+            "traffic": profiled_traffic("k_step_plain"),
         },
         "precision_vs_plain": value / plain,
         "accuracy": {"E_rel_l2_fp32_vs_fp64": rel(E32, E64),

@@ -19,8 +19,16 @@
  *  - A context is used by one host thread at a time; all GPU work is ordered
  *    on the context's CUDA stream and every entry point returns after its
  *    work has completed (synchronous), except where stated.
- *  - Numbers: GRLBM_PLAIN_FP64 computes everything in IEEE FP64 and matches
- *    the reference's CPU path to relative L2 <= 1e-12 on E and F;
+ *  - Numbers: GRLBM_PLAIN_FP64 computes everything in IEEE FP64 without
+ *    contracted multiply-adds.  Given the same Fourier coefficients
+ *    (grlbm_set_fourier_coefficients) its steps reproduce the reference's
+ *    IEEE build bit for bit; the coefficients it builds itself match the
+ *    reference's to 1e-13 (the reference's pow(x, 0.25) step-size control is
+ *    libm's, which is not correctly rounded, so the tables cannot be
+ *    bitwise); whole runs match to relative L2 <= 1e-12 on E and F wherever
+ *    the reference's own lambda-iteration exit test is not decided by
+ *    rounding noise (scattering fluids at rest are: there the reference
+ *    itself moves by ~1e-4 under a one-ulp change of its inputs).
  *    GRLBM_PRECISION_FP32 keeps intensities and the stream/collide arithmetic
  *    in FP32 (Kahan-compensated moment sums) on top of FP64 geodesic tables.
  */

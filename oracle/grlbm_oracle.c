@@ -23,7 +23,7 @@
  * Every expression keeps the reference's association order, so that with the
  * same compiler semantics it reproduces the reference bit for bit; this is
  * checked against the reference itself (oracle/_ref, strict build) by
- * tests/test_oracle_pin.py and against committed golden vectors.
+ * tests/test_oracle_golden.py and against committed golden vectors.
  *
  * Parity is pinned to the reference compiled with a project-written stand-in
  * for its un-vendored Eigen submodule (oracle/eigen_standin); the 3x3 inverse
