@@ -82,6 +82,7 @@ SIGNATURES = {
     "grlbm_get_moments_if": ([C.c_void_p] + [_D] * 6, C.c_int),
     "grlbm_compute_moments_lf": ([C.c_void_p] + [_D] * 7, C.c_int),
     "grlbm_energy": ([C.c_void_p, _D], C.c_int),
+    "grlbm_energy_noalloc": ([C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p], C.c_int),
     "grlbm_get_stats": ([C.c_void_p, C.POINTER(Stats)], C.c_int),
     "grlbm_host_stencil": ([C.c_int32, C.c_int32, _D, _D, _D, _D, C.POINTER(C.c_int64), _D], C.c_int),
     "grlbm_host_flux_table": ([C.c_int32, C.POINTER(C.c_int32), _D, _D, _D, C.c_int32], C.c_int),

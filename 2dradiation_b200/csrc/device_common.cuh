@@ -153,6 +153,9 @@ struct DirTable
     float wmom[18];
 };
 
+// Records a message for grlbm_last_error(NULL) (defined in grlbm_capi.cu).
+void set_global_error(const char *msg);
+
 // ---- launchers (defined in the kernel translation units) ----
 void launch_geodesic(const GeodesicArgs &a, cudaStream_t s);
 void launch_project(const ProjectArgs &a, cudaStream_t s);

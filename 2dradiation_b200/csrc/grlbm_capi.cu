@@ -81,6 +81,11 @@ struct grlbm_ctx
     }
 };
 
+namespace grlbm
+{
+void set_global_error(const char *msg) { g_create_error = msg; }
+} // namespace grlbm
+
 namespace
 {
 constexpr int kGraphSteps = 32;

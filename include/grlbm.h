@@ -195,6 +195,21 @@ int grlbm_compute_moments_lf(grlbm_ctx *ctx, double *E, double *Fx, double *Fy, 
  * with a fixed reduction order (bitwise reproducible).  No reference
  * counterpart; the conservation check of the precision form. */
 int grlbm_energy(grlbm_ctx *ctx, double *total);
+/* Global energy without any device allocation: sum of the interior E of a
+ * caller-owned FP64 device array in the per-node layout (nx*ny entries, nx =
+ * nx_ + 2), written to the caller-owned device scalar *total, with the work
+ * enqueued on `stream` (a cudaStream_t; NULL for the legacy default stream).
+ * No counterpart in the reference: it exists for callers that cannot
+ * allocate device memory when they need the sum -- loops whose device-memory
+ * budget is fixed up front, and host applications that route every device
+ * allocation through their own pool (a library cudaMalloc would bypass its
+ * accounting and synchronise the device).  Its partial sums live in a fixed
+ * file-scope device array of 8192 doubles shared by every call on a device:
+ * at most 2,097,152 interior cells (larger grids return GRLBM_ERR_ARGUMENT);
+ * calls that overlap on the GPU race on that array; the first call on each
+ * device looks the array up and must come before any stream capture.  The
+ * call returns once the work is enqueued (asynchronous). */
+int grlbm_energy_noalloc(const double *E, int64_t nx_, int64_t ny_, double *total, void *stream);
 /* Lambda-iteration and table-build statistics (src/Radiation.cpp:723-733,
  * 855-857). */
 int grlbm_get_stats(grlbm_ctx *ctx, grlbm_stats *stats);
