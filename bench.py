@@ -295,7 +295,7 @@ def run_grlbm(a, world, rank, local, pg):
             "frac": ach32 / peak,
             "traffic": profiled_traffic("k_step_prec"),
             "algorithmic_bytes_per_update": b32,
-            "kernel": "k_step<float, curved>",
+            "kernel": "k_step_prec<curved>",
         },
         "plain_fp64": {
             "value": plain,
