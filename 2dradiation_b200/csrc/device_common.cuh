@@ -19,8 +19,11 @@
 //                                         (absolute grid coordinates of the
 //                                         departure point; angle < 0 marks a
 //                                         departure inside the excision)
-//   FP32 record  rec32[d * ncell + c]     {i_dep - i, j_dep - j, angle coordinate,
-//                                         s^3 alpha_c^3 (0 when excised)}
+//   FP32 record  rec32[d * ncell + c]     {packed window word, fx, fy, s^3 alpha_c^3
+//                                         (0 when excised)}: see PackedRecord below
+//   FP32 side    side32[d * ncell + c]    {i_dep - i, j_dep - j, angle coordinate,
+//                                         s^3 alpha_c^3}, read only for departures
+//                                         the packed word marks as far
 //   FP32 state   J = I / alpha^3 for curved streaming (I for flat); the
 //                                         C-ABI converts at its boundary
 //   rk fields    rkf[ij * kRkStride + f]  node-major pack of the 21 metric arrays
@@ -48,7 +51,6 @@ static_assert(RF_COUNT <= kRkStride, "rk pack stride");
 
 constexpr int kStepBlock = 128;
 constexpr int kMaxDirs = 256;
-constexpr int kMaxDirsPlain = 216;
 constexpr int kMaxFourier = 64;
 
 struct GridDev
@@ -93,6 +95,24 @@ struct ProjectArgs
     double *coef;        // [5][nxy][nf]
 };
 
+// Staging of the precision-form step: per direction chunk of kChunk
+// directions the kernel holds the planes [chunk0 - kBelow, chunk0 - kBelow +
+// kSpan) of a tile's patch; an angular window has kTaps directions.
+constexpr int kChunk = 8, kBelow = 4, kSpan = kChunk + 8, kTaps = 5;
+
+// Packed window word of a precision-form record (bit fields of .x):
+//   bits  0-17  t, the blend between interpolation rows, in units of 2^-18
+//   bits 18-22  row type of the departure's interpolation row
+//   bits 23-28  first direction of the angular window minus d, plus 32
+//   bits 29-30  corner code: floor(i_dep - i) + 1 + 2 (floor(j_dep - j) + 1)
+//   bit  31     far: the departure lies outside the cell's 3x3 neighbourhood
+//               or its window outside the staged planes (read the side record)
+namespace packed
+{
+constexpr unsigned kTBits = 18, kTypeShift = 18, kBaseShift = 23, kCodeShift = 29, kFarBit = 31;
+constexpr int kBaseBias = 32;
+} // namespace packed
+
 struct DepartureArgs
 {
     GridDev g;
@@ -102,8 +122,18 @@ struct DepartureArgs
     const double *alpha; // nxy
     double rot_c, rot_s; // RotationMatrix(0) entries
     double4 *rec64;      // plain records or null
-    float4 *rec32;       // precision records or null
+    float4 *rec32;       // precision records (packed) or null
+    float4 *side32;      // precision side records or null
+    int q, p;            // interpolation row period (row types) and its direction shift
+    int row_base[32];    // first window direction of each row type
     int *clamped;
+};
+
+// One row of the cubic interpolation grid: 4 directions and their weights.
+struct __align__(16) IgRow
+{
+    int4 idx;
+    double2 w01, w23;
 };
 
 struct PlainStepArgs
@@ -115,8 +145,7 @@ struct PlainStepArgs
     const double4 *rec;
     const double *w, *n1, *n2; // nd
     const double *cx, *cy;     // nd (flat departures)
-    const int *ig_index;       // ng*4
-    const double *ig_w;        // ng*4
+    const IgRow *ig_rows;      // ng
     const double *alpha;       // nxy
     const double *acube;       // nxy*9
     const uint8_t *flags;      // nxy: bit0 excised node (no collide), bit1 stream writes 0
@@ -132,8 +161,8 @@ struct PrecStepArgs
     int nd, ng;
     const float *Iin;
     float *Iout;
-    const float4 *rec;
-    float dir_per_row;        // nDir / nGrid: direction spacing of the interpolation grid rows
+    const float4 *rec;        // packed records
+    const float4 *side;       // side records
     const float *ia3;         // nxy: 1/alpha^3 (scale of the stored state)
     const uint8_t *flags;
     const float *u1, *u2, *lor, *adt, *eta, *k0, *k3, *ka;
@@ -147,10 +176,23 @@ struct PrecStepArgs
 // directions, flat-space departure offsets in cells, and the 18 stencil sums
 // of the affine collide map (sum_d w mu_q, times n1, times n2 for
 // mu = 1, n1, n2, n1^2, n1 n2, n2^2).
+//
+// The angular interpolation rows: row g of the interpolation grid blended
+// with row g+1 is a 5-direction window with weights W0 + t D.  The grid has
+// nGrid = 10 nDir rows, so with q = nGrid / gcd(nDir, nGrid) and
+// p = nDir / gcd(nDir, nGrid) row g = q m + r has the weights of row r and
+// starts p m directions further on: q row types of 12 floats
+// {W0[0..3]}, {D[0..3]}, {W0[4], D[4], first direction of row r, 0}.
+constexpr int kMaxRowTypes = 32;
 struct DirTable
 {
     float w[kMaxDirs], n1[kMaxDirs], n2[kMaxDirs], ox[kMaxDirs], oy[kMaxDirs];
     float wmom[18];
+    float rowtab[kMaxRowTypes * 12];
+    // moment-sum coefficients per direction: {w, w n1, w n2, w n1^2}, {w n1 n2, w n2^2, n1, n2}
+    float dirc[kMaxDirs * 8];
+    int q, p;
+    float inv_q;
 };
 
 // Records a message for grlbm_last_error(NULL) (defined in grlbm_capi.cu).

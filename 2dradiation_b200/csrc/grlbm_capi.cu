@@ -56,8 +56,8 @@ struct grlbm_ctx
     int64_t ncell = 0;
     int ng = 0;
     // device buffers (storage type T = double for the plain form, float for the precision form)
-    DevBuf I[2], rec, w, n1, n2, cx, cy, flags, bhmask, alpha, acube;
-    DevBuf ig_index, ig_w64, rows, ia3;
+    DevBuf I[2], rec, side, w, n1, n2, cx, cy, flags, bhmask, alpha, acube;
+    DevBuf ig_rows, ia3;
     DirTable dirs{}; // precision-form direction tables (kernel parameter)
     DevBuf cu1, cu2, clor, cadt, ceta, ck0, ck3, cka, mom, rkf, lfp;
     DevBuf coef, ss_cx, ss_cy, ss_w, proj_basis, eval_basis, stage;
@@ -183,7 +183,7 @@ int enqueue_step(grlbm_ctx *ctx, int from)
         a.Iin = ctx->I[from].as<float>();
         a.Iout = ctx->I[from ^ 1].as<float>();
         a.rec = ctx->rec.as<float4>();
-        a.dir_per_row = (float)((double)ctx->st.n / (double)ctx->ng);
+        a.side = ctx->side.as<float4>();
         a.ia3 = ctx->ia3.as<float>();
         a.flags = ctx->flags.as<uint8_t>();
         a.u1 = ctx->cu1.as<float>();
@@ -216,8 +216,7 @@ int enqueue_step(grlbm_ctx *ctx, int from)
         a.n2 = ctx->n2.as<double>();
         a.cx = ctx->cx.as<double>();
         a.cy = ctx->cy.as<double>();
-        a.ig_index = ctx->ig_index.as<int>();
-        a.ig_w = ctx->ig_w64.as<double>();
+        a.ig_rows = ctx->ig_rows.as<IgRow>();
         a.alpha = ctx->alpha.as<double>();
         a.acube = ctx->acube.as<double>();
         a.flags = ctx->flags.as<uint8_t>();
@@ -277,6 +276,11 @@ int build_records(grlbm_ctx *ctx)
     da.rot_s = approx_sin(0.0);
     da.rec64 = ctx->fp32 ? nullptr : ctx->rec.as<double4>();
     da.rec32 = ctx->fp32 ? ctx->rec.as<float4>() : nullptr;
+    da.side32 = ctx->fp32 ? ctx->side.as<float4>() : nullptr;
+    da.q = ctx->dirs.q;
+    da.p = ctx->dirs.p;
+    for (int r = 0; r < ctx->dirs.q && r < kMaxRowTypes; r++)
+        da.row_base[r] = (int)ctx->dirs.rowtab[r * 12 + 10];
     da.clamped = reinterpret_cast<int *>(ctx->counters.as<unsigned long long>() + 4);
     CU(cudaMemsetAsync(ctx->counters.as<unsigned long long>() + 4, 0, sizeof(unsigned long long), ctx->stream));
     launch_departure(da, ctx->stream);
@@ -352,7 +356,7 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
     }
     if (run->precision != GRLBM_PLAIN_FP64 && run->precision != GRLBM_PRECISION_FP32)
         return fail(nullptr, GRLBM_ERR_ARGUMENT, "unknown precision %d", run->precision);
-    const int maxdir = run->precision == GRLBM_PLAIN_FP64 ? kMaxDirsPlain : kMaxDirs;
+    const int maxdir = kMaxDirs;
     if (run->n_dir < 4 || run->n_dir > maxdir)
         return fail(nullptr, GRLBM_ERR_ARGUMENT, "n_dir must be in [4, %d]", maxdir);
     if (run->precision == GRLBM_PRECISION_FP32 &&
@@ -443,21 +447,36 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
     TRY(upload(ctx, ctx->cy, ctx->st.cy));
     if (ctx->fp32)
     {
-        // each cubic row g blended with row g+1 into one 5-direction window
-        // starting at row g's first direction: weights W0 + t D, packed as
-        // {W0[0..3]}, {D[0..3]}, {W0[4], D[4], first direction (int bits), 0}
-        std::vector<int> base(ctx->ng);
-        for (int g = 0; g < ctx->ng; g++)
+        // each cubic row g of the reference's interpolation grid blended with
+        // row g+1 into one 5-direction window starting at row g's first
+        // direction: weights W0 + t D.  The rows repeat with period q (shifted
+        // by p directions per period); the kernel keeps the q row types and
+        // every row is checked against its type here.
+        const int ng = ctx->ng;
+        std::vector<int> base(ng);
+        for (int g = 0; g < ng; g++)
         {
             base[g] = (int)ctx->st.ig_index[4 * g];
             for (int k = 1; k < 4; k++)
                 if (ctx->st.ig_index[4 * g + k] != (base[g] + k) % nd)
                     return fail(nullptr, GRLBM_ERR_HOST, "interpolation row %d is not 4 consecutive directions", g);
         }
-        std::vector<float> rows((size_t)ctx->ng * 12, 0.f);
-        for (int g = 0; g < ctx->ng; g++)
+        int gcd = nd, b = ng;
+        while (b)
         {
-            const int g1 = (g + 1) % ctx->ng;
+            const int r = gcd % b;
+            gcd = b;
+            b = r;
+        }
+        const int q = ng / gcd, pstep = nd / gcd;
+        if (q > kMaxRowTypes)
+            return fail(nullptr, GRLBM_ERR_UNSUPPORTED, "interpolation grid period %d exceeds %d row types", q,
+                        kMaxRowTypes);
+        DirTable &dt = ctx->dirs;
+        std::vector<double> eff_row(2 * nd), eff_type(2 * nd);
+        for (int g = 0; g < ng; g++)
+        {
+            const int g1 = (g + 1) % ng;
             const int shift = ((base[g1] - base[g]) % nd + nd) % nd;
             if (shift > 1)
                 return fail(nullptr, GRLBM_ERR_HOST, "interpolation rows %d, %d are %d directions apart", g, g1, shift);
@@ -467,26 +486,60 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
                 W0[k] = ctx->st.ig_weight[4 * g + k];
                 W1[k + shift] = ctx->st.ig_weight[4 * g1 + k];
             }
-            float *r = &rows[(size_t)g * 12];
+            float row[12];
             for (int k = 0; k < 4; k++)
             {
-                r[k] = (float)W0[k];
-                r[4 + k] = (float)(W1[k] - W0[k]);
+                row[k] = (float)W0[k];
+                row[4 + k] = (float)(W1[k] - W0[k]);
             }
-            r[8] = (float)W0[4];
-            r[9] = (float)(W1[4] - W0[4]);
-            std::memcpy(&r[10], &base[g], sizeof(int));
+            row[8] = (float)W0[4];
+            row[9] = (float)(W1[4] - W0[4]);
+            row[10] = (float)base[g];
+            row[11] = 0.f;
+            const int r = g % q, m = g / q;
+            float *t = &dt.rowtab[r * 12];
+            if (m == 0)
+                std::memcpy(t, row, sizeof row);
+            else
+            {
+                // The row must act on the same directions with the same
+                // weights as its type shifted by p m directions.  (A row that
+                // sits exactly on a direction may list its 4 neighbours one
+                // place earlier or later, with that direction's weight 1 and
+                // the others 0: the same interpolation.)
+                std::fill(eff_row.begin(), eff_row.end(), 0.0);
+                std::fill(eff_type.begin(), eff_type.end(), 0.0);
+                const int tb = ((int)t[10] + pstep * m) % nd;
+                for (int k = 0; k < 5; k++)
+                {
+                    const float rw0 = k < 4 ? row[k] : row[8], rdd = k < 4 ? row[4 + k] : row[9];
+                    const float tw0 = k < 4 ? t[k] : t[8], tdd = k < 4 ? t[4 + k] : t[9];
+                    eff_row[(base[g] + k) % nd] += rw0;
+                    eff_row[nd + (base[g] + k) % nd] += rdd;
+                    eff_type[(tb + k) % nd] += tw0;
+                    eff_type[nd + (tb + k) % nd] += tdd;
+                }
+                for (int k = 0; k < 2 * nd; k++)
+                    if (std::fabs(eff_row[k] - eff_type[k]) > 1e-6)
+                        return fail(nullptr, GRLBM_ERR_HOST, "interpolation row %d does not repeat row %d", g, r);
+            }
         }
-        TRY(upload(ctx, ctx->rows, rows));
+        dt.q = q;
+        dt.p = pstep;
+        dt.inv_q = 1.0f / (float)q;
         // direction tables: weights, rotated directions, flat departures, and
         // the stencil sums of the affine collide map
-        DirTable &dt = ctx->dirs;
         double wm[18] = {0};
         for (int d = 0; d < nd; d++)
         {
             dt.w[d] = (float)ctx->st.w[d];
             dt.n1[d] = (float)n1[d];
             dt.n2[d] = (float)n2[d];
+            const double wd = ctx->st.w[d];
+            const double cf[8] = {wd, wd * n1[d], wd * n2[d], wd * n1[d] * n1[d], wd * n1[d] * n2[d],
+                                  wd * n2[d] * n2[d], n1[d], n2[d]};
+            for (int k = 0; k < 8; k++)
+                dt.dirc[8 * d + k] = (float)cf[k];
             dt.ox[d] = (float)(-ctx->st.cx[d] * G.dt / G.dx);
             dt.oy[d] = (float)(-ctx->st.cy[d] * G.dt / G.dy);
             const double mu[6] = {1.0, n1[d], n2[d], n1[d] * n1[d], n1[d] * n2[d], n2[d] * n2[d]};
@@ -502,9 +555,16 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
     }
     else
     {
-        std::vector<int> idx(ctx->st.ig_index.begin(), ctx->st.ig_index.end());
-        TRY(upload(ctx, ctx->ig_index, idx));
-        TRY(upload(ctx, ctx->ig_w64, ctx->st.ig_weight));
+std::vector<IgRow> rows(ctx->ng);
+        for (int g = 0; g < ctx->ng; g++)
+        {
+            const int64_t *x = &ctx->st.ig_index[4 * g];
+            const double *w = &ctx->st.ig_weight[4 * g];
+            rows[g].idx = make_int4((int)x[0], (int)x[1], (int)x[2], (int)x[3]);
+            rows[g].w01 = make_double2(w[0], w[1]);
+            rows[g].w23 = make_double2(w[2], w[3]);
+        }
+        TRY(upload(ctx, ctx->ig_rows, rows));
     }
 
     // per-node metric data
@@ -569,6 +629,8 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
     TRY(alloc(ctx, ctx->I[1], ib));
     TRY(alloc(ctx, ctx->mom, (size_t)6 * nxy * tsize(ctx)));
     TRY(alloc(ctx, ctx->rec, (size_t)ctx->ncell * nd * (ctx->fp32 ? sizeof(float4) : sizeof(double4))));
+    if (ctx->fp32)
+        TRY(alloc(ctx, ctx->side, (size_t)ctx->ncell * nd * sizeof(float4)));
     TRY(alloc(ctx, ctx->counters, 8 * sizeof(unsigned long long)));
     TRY(alloc(ctx, ctx->energy_partial, kPartialBlocks * sizeof(double)));
     TRY(alloc(ctx, ctx->energy_out, sizeof(double)));
@@ -577,10 +639,12 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
     cudaMemset(ctx->mom.p, 0, ctx->mom.bytes);
     cudaMemset(ctx->counters.p, 0, ctx->counters.bytes);
     cudaMemset(ctx->rec.p, 0, ctx->rec.bytes);
+    if (ctx->side.p)
+        cudaMemset(ctx->side.p, 0, ctx->side.bytes);
     // fields default to zero (the reference's buffers are value-initialised)
     std::vector<double> zeros(nxy, 0.0);
     TRY(grlbm_set_fields(ctx, zeros.data(), zeros.data(), zeros.data(), zeros.data(), zeros.data(), zeros.data()));
-    const int smem = (int)(ctx->fp32 ? step_prec_smem(nd) : (size_t)nd * kStepBlock * sizeof(double));
+    const int smem = (int)(ctx->fp32 ? step_prec_smem(nd) : 0);
     if ((ctx->fp32 ? prepare_step_prec(smem) : prepare_step_plain(smem)) != cudaSuccess)
         return fail(nullptr, GRLBM_ERR_CUDA, "cannot reserve %d bytes of shared memory for the step kernel", smem);
     if (cudaDeviceSynchronize() != cudaSuccess)

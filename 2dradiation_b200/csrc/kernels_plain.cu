@@ -10,6 +10,11 @@
 // them E, follow the last bits of the streamed intensities.
 #include "device_common.cuh"
 
+// Resident blocks per SM the step kernel's register budget is sized for.
+#ifndef GRLBM_PLAIN_MIN_BLOCKS
+#define GRLBM_PLAIN_MIN_BLOCKS 4
+#endif
+
 namespace grlbm
 {
 namespace
@@ -17,13 +22,12 @@ namespace
 // one stream value: StreamFlatFixed (src/Radiation.cpp:394-410) or
 // StreamCurvedFixed with IntensityAt (:478-508, 322-343)
 template <bool CURVED>
-__device__ __forceinline__ double stream_value(const PlainStepArgs &a, int d, int64_t c, int64_t i, int64_t j,
+__device__ __forceinline__ double stream_value(const PlainStepArgs &a, int d, const double4 &r, int64_t i, int64_t j,
                                                int64_t ij)
 {
     const int64_t nxy = a.g.nxy, nx = a.g.nx;
     if constexpr (CURVED)
     {
-        const double4 r = a.rec[(int64_t)d * a.g.ncell + c];
         if (r.z < 0.0) // departure point inside the excision
             return 0.0;
         const double it = r.x, jt = r.y;
@@ -34,16 +38,11 @@ __device__ __forceinline__ double stream_value(const PlainStepArgs &a, int d, in
         g0 = g0 < 0 ? 0 : g0;
         const int g1 = (g0 + 1) % a.ng;
         const double t = r.z - (double)g0;
-        int idx0[4], idx1[4];
-        double w0[4], w1[4];
-#pragma unroll
-        for (int k = 0; k < 4; k++)
-        {
-            idx0[k] = __ldg(a.ig_index + 4 * g0 + k);
-            idx1[k] = __ldg(a.ig_index + 4 * g1 + k);
-            w0[k] = __ldg(a.ig_w + 4 * g0 + k);
-            w1[k] = __ldg(a.ig_w + 4 * g1 + k);
-        }
+        const IgRow R0 = a.ig_rows[g0], R1 = a.ig_rows[g1];
+        const int idx0[4] = {R0.idx.x, R0.idx.y, R0.idx.z, R0.idx.w};
+        const int idx1[4] = {R1.idx.x, R1.idx.y, R1.idx.z, R1.idx.w};
+        const double w0[4] = {R0.w01.x, R0.w01.y, R0.w23.x, R0.w23.y};
+        const double w1[4] = {R1.w01.x, R1.w01.y, R1.w23.x, R1.w23.y};
         const double al = __ldg(a.alpha + ij);
         double Iq[4];
 #pragma unroll
@@ -136,11 +135,27 @@ __device__ __forceinline__ double collide_value(double I, double n1, double n2, 
     return (I + src) / (1.0 + adt * kak0 * A);
 }
 
-template <bool CURVED>
-__global__ void __launch_bounds__(kStepBlock) k_step_plain(PlainStepArgs a)
+// num / den, correctly rounded, from r = RN(1/den): one refinement brings
+// RN(num r) (within 1.5 ulp of the quotient) to within one ulp, then one
+// Markstein step (P. Markstein, IBM J. Res. Dev. 34(1), 1990: with r within
+// half an ulp of 1/den and q within one ulp of num/den, the remainder
+// num - den q is exact in one fma and RN(q + rem r) is the correctly rounded
+// quotient) gives the IEEE result.  Used where den is the same for many
+// divisions; outside the range in which no step can underflow or overflow
+// the ordinary division is taken.  Requires 1 <= den < 2^100.
+__device__ __forceinline__ double div_rn(double num, double den, double r)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    double *Is = reinterpret_cast<double *>(smem_raw);
+    const double an = fabs(num);
+    if (an != 0.0 && !(an > 0x1p-900 && an < 0x1p+900))
+        return num / den;
+    double q = __dmul_rn(num, r);
+    q = __fma_rn(__fma_rn(-q, den, num), r, q);
+    return __fma_rn(__fma_rn(-q, den, num), r, q);
+}
+
+template <bool CURVED>
+__global__ void __launch_bounds__(kStepBlock, GRLBM_PLAIN_MIN_BLOCKS) k_step_plain(PlainStepArgs a)
+{
     const int t = threadIdx.x;
     const int64_t c = (int64_t)blockIdx.x * kStepBlock + t;
     const bool active = c < a.g.ncell;
@@ -150,21 +165,45 @@ __global__ void __launch_bounds__(kStepBlock) k_step_plain(PlainStepArgs a)
     const int64_t nxy = a.g.nxy;
     const uint8_t fl = active ? a.flags[ij] : (uint8_t)3;
     const bool zero_stream = CURVED && (fl & 2);
+    const bool collides = active && !(fl & 1);
+    // The streamed intensities of a colliding cell wait in its own output
+    // slots until the lambda iteration has converged (nothing else reads or
+    // writes them in this step); non-colliding cells keep their slots.
+    double *Is = a.Iout + ij;
 
     Moments m;
     m.zero();
+    // departure records, prefetched one direction ahead (the last stands in
+    // past the end)
+    const double4 *rp = a.rec + cc;
+    double4 r0 = make_double4(0, 0, 0, 0);
+    if (CURVED)
+        r0 = rp[0];
     for (int d = 0; d < a.nd; d++)
     {
-        const double val = (active && !zero_stream) ? stream_value<CURVED>(a, d, cc, i, j, ij) : 0.0;
-        Is[d * kStepBlock + t] = val;
+        double4 r1 = r0;
+        if (CURVED)
+            r1 = rp[(int64_t)min(d + 1, a.nd - 1) * a.g.ncell];
+        const double val = (active && !zero_stream) ? stream_value<CURVED>(a, d, r0, i, j, ij) : 0.0;
+        if (collides)
+            Is[(int64_t)d * nxy] = val;
         m.add(__ldg(a.w + d), val, __ldg(a.n1 + d), __ldg(a.n2 + d));
+        r0 = r1;
     }
 
     int cycles = 0;
-    if (active && !(fl & 1))
+    if (collides)
     {
         const double u1 = a.u1[ij], u2 = a.u2[ij], lor = a.lor[ij], adt = a.adt[ij];
         const double eta = a.eta[ij], k0 = a.k0[ij], k3 = a.k3[ij], kak0 = a.ka[ij] + a.k0[ij];
+        // A fluid at rest has u = 0 and lorentz = 1, so in collide_value
+        // A = 1, n_ff = n and AA = 1 exactly: the update reduces to
+        // (I + adt (eta + (k0 fE + k3 (n1 fFx + n2 fFy)))) / (1 + adt kak0)
+        // with the same roundings.
+        const bool rest = u1 == 0.0 && u2 == 0.0 && lor == 1.0;
+        const double den = 1.0 + adt * kak0;
+        const bool fast_div = rest && den >= 1.0 && den < 0x1p+100;
+        const double rden = __drcp_rn(den);
         double diff = 1;
         double fE = 0, fFx = 0, fFy = 0;
         while (fabs(diff) > 1e-4 && cycles < 100)
@@ -180,24 +219,45 @@ __global__ void __launch_bounds__(kStepBlock) k_step_plain(PlainStepArgs a)
             fFx = lor * lor * (pFx - lor * pE * u1 - uxP + u1 * lor / (1.0 + lor) * ((2.0 * lor + 1.0) * uF - lor * uuP));
             fFy = lor * lor * (pFy - lor * pE * u2 - uyP + u2 * lor / (1.0 + lor) * ((2.0 * lor + 1.0) * uF - lor * uuP));
             m.zero();
-            for (int d = 0; d < a.nd; d++)
+            if (rest)
             {
-                const double n1 = __ldg(a.n1 + d), n2 = __ldg(a.n2 + d);
-                const double v = collide_value(Is[d * kStepBlock + t], n1, n2, u1, u2, lor, adt, eta, k0, k3, kak0,
-                                               fE, fFx, fFy);
-                m.add(__ldg(a.w + d), v, n1, n2);
+                const double k0fE = k0 * fE;
+#pragma unroll 4
+                for (int d = 0; d < a.nd; d++)
+                {
+                    const double n1 = __ldg(a.n1 + d), n2 = __ldg(a.n2 + d);
+                    const double num = Is[(int64_t)d * nxy] + adt * (eta + (k0fE + k3 * (n1 * fFx + n2 * fFy)));
+                    const double v = fast_div ? div_rn(num, den, rden) : num / den;
+                    m.add(__ldg(a.w + d), v, n1, n2);
+                }
             }
+            else
+                for (int d = 0; d < a.nd; d++)
+                {
+                    const double n1 = __ldg(a.n1 + d), n2 = __ldg(a.n2 + d);
+                    const double v = collide_value(Is[(int64_t)d * nxy], n1, n2, u1, u2, lor, adt, eta, k0, k3,
+                                                   kak0, fE, fFx, fFy);
+                    m.add(__ldg(a.w + d), v, n1, n2);
+                }
             const double e1 = (pE - m.E) / m.E, e2 = (pFx - m.Fx) / m.Fx, e3 = (pFy - m.Fy) / m.Fy;
             const double e4 = (pPxx - m.Pxx) / m.Pxx, e5 = (pPxy - m.Pxy) / m.Pxy, e6 = (pPyy - m.Pyy) / m.Pyy;
             diff = sqrt(e1 * e1 + e2 * e2 + e3 * e3 + e4 * e4 + e5 * e5 + e6 * e6);
         }
-        // the last iterate, recomputed from the same operands
-        for (int d = 0; d < a.nd; d++)
+        // the last iterate, recomputed from the same operands, over the parked values
+        if (rest)
         {
-            const double v = collide_value(Is[d * kStepBlock + t], __ldg(a.n1 + d), __ldg(a.n2 + d), u1, u2, lor, adt,
-                                           eta, k0, k3, kak0, fE, fFx, fFy);
-            a.Iout[(int64_t)d * nxy + ij] = v;
+            const double k0fE = k0 * fE;
+            for (int d = 0; d < a.nd; d++)
+            {
+                const double n1 = __ldg(a.n1 + d), n2 = __ldg(a.n2 + d);
+                const double num = Is[(int64_t)d * nxy] + adt * (eta + (k0fE + k3 * (n1 * fFx + n2 * fFy)));
+                Is[(int64_t)d * nxy] = fast_div ? div_rn(num, den, rden) : num / den;
+            }
         }
+        else
+            for (int d = 0; d < a.nd; d++)
+                Is[(int64_t)d * nxy] = collide_value(Is[(int64_t)d * nxy], __ldg(a.n1 + d), __ldg(a.n2 + d), u1, u2,
+                                                     lor, adt, eta, k0, k3, kak0, fE, fFx, fFy);
     }
     if (active)
     {
@@ -208,23 +268,18 @@ __global__ void __launch_bounds__(kStepBlock) k_step_plain(PlainStepArgs a)
         a.mom[ij + 4 * nxy] = m.Pxy;
         a.mom[ij + 5 * nxy] = m.Pyy;
     }
-    __shared__ unsigned int s_sum, s_max;
-    if (t == 0)
+    // lambda-iteration statistics: warp sums and maxima, one atomic per warp
+    unsigned sum = (unsigned)cycles, mx = (unsigned)cycles;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
     {
-        s_sum = 0;
-        s_max = 0;
+        sum += __shfl_xor_sync(0xffffffffu, sum, o);
+        mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
     }
-    __syncthreads();
-    if (cycles)
+    if ((t & 31) == 0 && sum)
     {
-        atomicAdd(&s_sum, (unsigned int)cycles);
-        atomicMax(&s_max, (unsigned int)cycles);
-    }
-    __syncthreads();
-    if (t == 0 && s_sum)
-    {
-        atomicAdd(a.iter_sum, (unsigned long long)s_sum);
-        atomicMax(a.iter_max, s_max);
+        atomicAdd(a.iter_sum, (unsigned long long)sum);
+        atomicMax(a.iter_max, mx);
     }
 }
 
@@ -396,7 +451,7 @@ cudaError_t prepare_step_plain(int smem_bytes)
 }
 void launch_step_plain(const PlainStepArgs &a, bool curved, cudaStream_t s)
 {
-    const size_t smem = (size_t)a.nd * kStepBlock * sizeof(double);
+    const size_t smem = 0;
     if (curved)
         k_step_plain<true><<<nblk(a.g.ncell, kStepBlock), kStepBlock, smem, s>>>(a);
     else

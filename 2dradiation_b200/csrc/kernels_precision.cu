@@ -22,6 +22,15 @@
 // pass whose Kahan sums give the stored moments.
 #include "device_common.cuh"
 
+// Tuning of the step kernel: resident blocks per SM the register budget is
+// sized for, and the unroll of the per-direction loop.
+#ifndef GRLBM_PREC_MIN_BLOCKS
+#define GRLBM_PREC_MIN_BLOCKS 5
+#endif
+#ifndef GRLBM_PREC_UNROLL
+#define GRLBM_PREC_UNROLL 2
+#endif
+
 namespace grlbm
 {
 namespace
@@ -40,20 +49,19 @@ struct Kahan
 };
 
 // Moment sums compensated per block of directions: plain FP32 partial sums
-// over kBlockDirs directions, folded into Kahan accumulators.
-constexpr int kBlockDirs = 8;
+// over up to kChunk directions, folded into Kahan accumulators by the caller
+// after each block.  The direction coefficients c0 = {w, w n1, w n2, w n1^2},
+// c1 = {w n1 n2, w n2^2, n1, n2} come from the shared direction table.
 struct KMoments
 {
     Kahan E, Fx, Fy, Pxx, Pxy, Pyy;
     float p[6];
-    int n;
     __device__ __forceinline__ void zero()
     {
         E.zero(), Fx.zero(), Fy.zero(), Pxx.zero(), Pxy.zero(), Pyy.zero();
 #pragma unroll
         for (int q = 0; q < 6; q++)
             p[q] = 0.f;
-        n = 0;
     }
     __device__ __forceinline__ void fold()
     {
@@ -61,22 +69,16 @@ struct KMoments
 #pragma unroll
         for (int q = 0; q < 6; q++)
             p[q] = 0.f;
-        n = 0;
     }
-    __device__ __forceinline__ void add(float w, float v, float n1, float n2)
+    __device__ __forceinline__ void add(float v, const float4 &c0, const float4 &c1)
     {
-        const float c = w * v;
-        const float c1 = c * n1, c2 = c * n2;
-        p[0] += c;
-        p[1] += c1;
-        p[2] += c2;
-        p[3] += c1 * n1;
-        p[4] += c1 * n2;
-        p[5] += c2 * n2;
-        if (++n == kBlockDirs)
-            fold();
+        p[0] = fmaf(c0.x, v, p[0]);
+        p[1] = fmaf(c0.y, v, p[1]);
+        p[2] = fmaf(c0.z, v, p[2]);
+        p[3] = fmaf(c0.w, v, p[3]);
+        p[4] = fmaf(c1.x, v, p[4]);
+        p[5] = fmaf(c1.y, v, p[5]);
     }
-    __device__ __forceinline__ void finish() { fold(); }
 };
 
 // Tile of cells per block and the shared-memory stage of the state around it:
@@ -85,14 +87,19 @@ struct KMoments
 // reads virtual planes [kChunk k - kBelow, kChunk k + kSpan - kBelow) (a
 // departure's angular window starts at most 3 directions below its own and
 // spans 5; plane v holds direction v mod nDir).  Plane v lives in ring slot
-// (v + kBelow) mod kRing; the next chunk's planes are loaded by cp.async into
-// slots the current chunk does not read.
+// (v + kBelow) mod kRing; slots 0..kMirror-1 are also kept in slots
+// kRing..kRing+kMirror-1, so the 5 planes of any window sit at consecutive
+// slots and a window's taps are fixed offsets from one address.  The next
+// chunk's planes are loaded by cp.async into slots the current chunk does not
+// read.
 constexpr int kTileX = 32, kTileY = 4;
 static_assert(kTileX * kTileY == kStepBlock, "tile = block");
 constexpr int kPatchX = kTileX + 2, kPatchY = kTileY + 2, kPatch = kPatchX * kPatchY;
 static_assert(kPatch > kStepBlock && kPatch <= 2 * kStepBlock, "two staging loads per thread and plane");
-constexpr int kChunk = 8, kBelow = 4, kSpan = kChunk + 8, kRing = 32;
+constexpr int kPrecUnroll = GRLBM_PREC_UNROLL;
+constexpr int kRing = 32, kMirror = kTaps - 1;
 static_assert(kSpan + kChunk <= kRing && (kRing & (kRing - 1)) == 0, "ring");
+constexpr int kRingSlots = kRing + kMirror;
 
 __device__ __forceinline__ void cp_async4(float *dst, const float *src)
 {
@@ -127,7 +134,7 @@ __device__ __forceinline__ StageSlots stage_slots(const GridDev &g, int x0, int 
     return s;
 }
 
-// stage virtual planes [v0, v0 + n) into their ring slots
+// stage virtual planes [v0, v0 + n) into their ring slots (and mirrors)
 __device__ __forceinline__ void stage_planes(const PrecStepArgs &a, const StageSlots &ss, float *ring, int v0, int n)
 {
     const unsigned nxy = (unsigned)a.g.nxy;
@@ -135,143 +142,142 @@ __device__ __forceinline__ void stage_planes(const PrecStepArgs &a, const StageS
     d = d < 0 ? d + a.nd : d;
     for (int p = 0; p < n; p++)
     {
-        float *slot = ring + ((v0 + p + kBelow) & (kRing - 1)) * kPatch;
+        const int sl = (v0 + p + kBelow) & (kRing - 1);
+        float *slot = ring + sl * kPatch;
         const float *plane = a.Iin + (unsigned)d * nxy;
         if (ss.ok0)
             cp_async4(slot + ss.node0, plane + ss.goff0);
         if (ss.ok1)
             cp_async4(slot + ss.node1, plane + ss.goff1);
+        if (sl < kMirror)
+        {
+            float *mirror = slot + kRing * kPatch;
+            if (ss.ok0)
+                cp_async4(mirror + ss.node0, plane + ss.goff0);
+            if (ss.ok1)
+                cp_async4(mirror + ss.node1, plane + ss.goff1);
+        }
         d = (d + 1 == a.nd) ? 0 : d + 1;
     }
     cp_async_commit();
 }
 
-// cubic Lagrange weights at position f in [0,1) for nodes -1, 0, 1, 2
-__device__ __forceinline__ void cubic_weights(float f, float *l)
+// The four bilinear corners of a 5-tap angular window read from global
+// memory, each clamped at zero: the rare departures whose corners or window
+// fall outside the staged patch (kept out of line: it is cold code).
+__device__ __noinline__ float4 window_corners_global(const float *__restrict__ I, unsigned nxy, int nd, int base,
+                                                     unsigned c00, unsigned nx, float w0, float w1, float w2,
+                                                     float w3, float w4)
 {
-    const float fm = f - 1.f, fp = f + 1.f, f2 = f - 2.f;
-    l[0] = -f * fm * f2 * (1.f / 6.f);
-    l[1] = fp * fm * f2 * 0.5f;
-    l[2] = -fp * f * f2 * 0.5f;
-    l[3] = fp * f * fm * (1.f / 6.f);
+    const float w[kTaps] = {w0, w1, w2, w3, w4};
+    const unsigned off[4] = {c00, c00 + nx, c00 + 1u, c00 + nx + 1u}; // corners 00 01 10 11
+    float cv[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+    {
+        float v = 0.f;
+        int dk = base;
+#pragma unroll
+        for (int k = 0; k < kTaps; k++)
+        {
+            v = fmaf(w[k], __ldg(I + (unsigned)dk * nxy + off[q]), v);
+            dk = (dk + 1 == nd) ? 0 : dk + 1;
+        }
+        cv[q] = fmaxf(v, 0.f);
+    }
+    return make_float4(cv[0], cv[1], cv[2], cv[3]);
 }
 
-// one stream value from its departure record (curved) or from the flat
-// departure of direction d; taps inside the staged patch come from shared
-// memory, any other from global memory
-template <bool CURVED>
-__device__ __forceinline__ float stream_value(const PrecStepArgs &a, const DirTable &dt, const float *ring, int d,
-                                              int chunk0, const float4 &r, int i, int j, int x0, int y0)
+// One curved stream value from a side record {i_dep - i, j_dep - j, angle
+// coordinate, s^3 alpha_c^3}, all taps from global memory: the departures
+// whose packed record is marked far (cold code, kept out of line).
+__device__ __noinline__ float stream_curved_far(const float *__restrict__ Iin, const float4 *__restrict__ side,
+                                                unsigned nxy, int nx, int ny, int nd, int ng, const float *rowtab,
+                                                int q, int p, float inv_q, unsigned rec_index, int i, int j)
+{
+    const float4 r = side[rec_index];
+    const float fli = floorf(r.x), flj = floorf(r.y);
+    const float fx = r.x - fli, fy = r.y - flj;
+    const int i0 = min(max(i + (int)fli, 0), nx - 2);
+    const int j0 = min(max(j + (int)flj, 0), ny - 2);
+    const float z = r.z == r.z ? r.z : 0.f;
+    const float g = fminf(fmaxf(floorf(z), 0.f), (float)(ng - 1));
+    const float t = fminf(fmaxf(z - g, 0.f), 1.f);
+    const float m = floorf((g + 0.5f) * inv_q);
+    const int rt = min(max((int)fmaf(-m, (float)q, g), 0), q - 1);
+    const float *row = rowtab + rt * 12;
+    int base = (int)fmaf(m, (float)p, row[10]) % nd;
+    const float4 c = window_corners_global(Iin, nxy, nd, base, (unsigned)(i0 + j0 * nx),
+                                           (unsigned)nx, fmaf(t, row[4], row[0]), fmaf(t, row[5], row[1]),
+                                           fmaf(t, row[6], row[2]), fmaf(t, row[7], row[3]),
+                                           fmaf(t, row[9], row[8]));
+    const float f0 = fmaf(fx, c.z - c.x, c.x);
+    const float f1 = fmaf(fx, c.w - c.y, c.y);
+    return r.w * fmaf(fy, f1 - f0, f0);
+}
+
+// One curved stream value (StreamCurvedFixed with IntensityAt,
+// src/Radiation.cpp:478-508, 322-343) from its packed record: the 4 bilinear
+// corners of the departure, each the 5-tap angular window (the two cubic
+// rows of the interpolation grid, src/Stencil.cpp:109-162, blended in t)
+// clamped at zero, then bilinear in (fx, fy) and scaled by s^3 alpha_c^3.
+// `cell` is the patch offset of the cell's lower-left neighbour.
+__device__ __forceinline__ float stream_curved(const PrecStepArgs &a, const DirTable &dt, const float *ring,
+                                               const float *rowtab, int d, const float4 &r, int cell,
+                                               unsigned rec_index, int i, int j)
+{
+    const unsigned word = __float_as_uint(r.x);
+    if (word >> packed::kFarBit)
+        return stream_curved_far(a.Iin, a.side, (unsigned)a.g.nxy, (int)a.g.nx, (int)a.g.ny, a.nd, a.ng, rowtab, dt.q,
+                                 dt.p, dt.inv_q, rec_index, i, j);
+    const float t = (float)(word & ((1u << packed::kTBits) - 1u)) * (1.f / (float)(1u << packed::kTBits));
+    const float4 *row = reinterpret_cast<const float4 *>(rowtab + ((word >> packed::kTypeShift) & 31u) * 12);
+    const float4 R0 = row[0], R1 = row[1], R2 = row[2];
+    const float w0 = fmaf(t, R1.x, R0.x), w1 = fmaf(t, R1.y, R0.y), w2 = fmaf(t, R1.z, R0.z);
+    const float w3 = fmaf(t, R1.w, R0.w), w4 = fmaf(t, R2.y, R2.x);
+    // ring slot of the window's first plane: virtual plane d + dbase
+    const int slot = (d + (int)((word >> packed::kBaseShift) & 63u) - packed::kBaseBias + kBelow) & (kRing - 1);
+    const unsigned code = word >> packed::kCodeShift; // bit 31 is clear here
+    const float *p = ring + slot * kPatch + cell + (int)(code & 1u) + (int)(code >> 1) * kPatchX;
+#define GRLBM_WINDOW(o)                                                                                       \
+    fmaxf(fmaf(w4, p[4 * kPatch + (o)],                                                                       \
+               fmaf(w3, p[3 * kPatch + (o)], fmaf(w2, p[2 * kPatch + (o)], fmaf(w1, p[kPatch + (o)], w0 * p[(o)])))), \
+          0.f)
+    const float c00 = GRLBM_WINDOW(0);
+    const float c01 = GRLBM_WINDOW(kPatchX);
+    const float c10 = GRLBM_WINDOW(1);
+    const float c11 = GRLBM_WINDOW(kPatchX + 1);
+#undef GRLBM_WINDOW
+    const float f0 = fmaf(r.y, c10 - c00, c00);
+    const float f1 = fmaf(r.y, c11 - c01, c01);
+    return r.w * fmaf(r.z, f1 - f0, f0);
+}
+
+// One flat stream value of direction d (StreamFlatFixed, src/Radiation.cpp:394-410).
+__device__ __forceinline__ float stream_flat(const PrecStepArgs &a, const DirTable &dt, const float *ring, int d,
+                                             int chunk0, int i, int j, int x0, int y0)
 {
     const int nx = (int)a.g.nx;
-    const unsigned nxy = (unsigned)a.g.nxy;
-    float fx, fy, w[5];
-    int i0, j0, base, ntap;
-    if constexpr (CURVED)
-    {
-        if (r.w == 0.f)
-            return 0.f;
-        const float fli = floorf(r.x), flj = floorf(r.y);
-        fx = r.x - fli;
-        fy = r.y - flj;
-        i0 = min(max(i + (int)fli, 0), nx - 2);
-        j0 = min(max(j + (int)flj, 0), (int)a.g.ny - 2);
-        int g = (int)floorf(r.z);
-        g = max(0, min(g, a.ng - 1));
-        const float t = r.z - (float)g;
-        // Row g of the interpolation grid sits at direction coordinate
-        // u = g nDir/nGrid - 1/2 and interpolates with the cubic Lagrange
-        // polynomial through the 4 directions around it (src/Stencil.cpp:109-162);
-        // IntensityAt blends rows g and g+1 linearly in t.
-        const float u0 = (float)g * a.dir_per_row - 0.5f;
-        const float b0 = floorf(u0), b1 = floorf(u0 + a.dir_per_row);
-        float l0[4], l1[4];
-        cubic_weights(u0 - b0, l0);
-        cubic_weights(u0 + a.dir_per_row - b1, l1);
-        const float s = 1.f - t;
-        if (b1 == b0)
-        {
-            w[0] = s * l0[0] + t * l1[0];
-            w[1] = s * l0[1] + t * l1[1];
-            w[2] = s * l0[2] + t * l1[2];
-            w[3] = s * l0[3] + t * l1[3];
-            w[4] = 0.f;
-            ntap = 4;
-        }
-        else
-        {
-            w[0] = s * l0[0];
-            w[1] = s * l0[1] + t * l1[0];
-            w[2] = s * l0[2] + t * l1[1];
-            w[3] = s * l0[3] + t * l1[2];
-            w[4] = t * l1[3];
-            ntap = 5;
-        }
-        base = (int)b0 - 1;
-        base = base < 0 ? base + a.nd : base;
-    }
-    else
-    {
-        const float ox = dt.ox[d], oy = dt.oy[d];
-        const float fli = floorf(ox), flj = floorf(oy);
-        fx = ox - fli;
-        fy = oy - flj;
-        i0 = min(max(i + (int)fli, 0), nx - 2);
-        j0 = min(max(j + (int)flj, 0), (int)a.g.ny - 2);
-        w[0] = 1.f;
-        w[1] = w[2] = w[3] = w[4] = 0.f;
-        base = d;
-        ntap = 1;
-    }
+    const float ox = dt.ox[d], oy = dt.oy[d];
+    const float fli = floorf(ox), flj = floorf(oy);
+    const float fx = ox - fli, fy = oy - flj;
+    const int i0 = min(max(i + (int)fli, 0), nx - 2);
+    const int j0 = min(max(j + (int)flj, 0), (int)a.g.ny - 2);
     const int lx = i0 - x0, ly = j0 - y0;
-    // window start relative to the chunk's first staged plane, modulo nDir
-    int rel = base - chunk0 + kBelow;
-    rel = rel < 0 ? rel + a.nd : (rel >= a.nd ? rel - a.nd : rel);
-    float cv[4];
-    if (lx >= 0 && lx <= kTileX && ly >= 0 && ly <= kTileY && rel + ntap <= kSpan)
+    float c00, c01, c10, c11;
+    if ((unsigned)lx <= (unsigned)kTileX && (unsigned)ly <= (unsigned)kTileY)
     {
-        const int o = ly * kPatchX + lx;
-        const int s0 = chunk0 + rel; // ring slot of the window's first plane
-        const float *p0 = ring + (s0 & (kRing - 1)) * kPatch + o;
-        const float *pk[5];
-#pragma unroll
-        for (int k = 0; k < 5; k++)
-            pk[k] = ring + ((s0 + k) & (kRing - 1)) * kPatch + o;
-        const int off[4] = {0, kPatchX, 1, kPatchX + 1}; // corners 00 01 10 11
-#pragma unroll
-        for (int q = 0; q < 4; q++)
-        {
-            float v = w[0] * p0[off[q]];
-#pragma unroll
-            for (int k = 1; k < 5; k++)
-                if (k < ntap)
-                    v = fmaf(w[k], pk[k][off[q]], v);
-            cv[q] = v > 0.f ? v : 0.f;
-        }
+        const float *p = ring + ((d + kBelow) & (kRing - 1)) * kPatch + ly * kPatchX + lx;
+        c00 = p[0], c01 = p[kPatchX], c10 = p[1], c11 = p[kPatchX + 1];
     }
     else
     {
-        const unsigned c00 = (unsigned)(i0 + j0 * nx);
-        const unsigned off[4] = {c00, c00 + (unsigned)nx, c00 + 1u, c00 + (unsigned)nx + 1u};
-#pragma unroll
-        for (int q = 0; q < 4; q++)
-        {
-            float v = 0.f;
-#pragma unroll
-            for (int k = 0; k < 5; k++)
-                if (k < ntap)
-                {
-                    int dk = base + k;
-                    dk = dk >= a.nd ? dk - a.nd : dk;
-                    v = fmaf(w[k], __ldg(a.Iin + (unsigned)dk * nxy + off[q]), v);
-                }
-            cv[q] = v > 0.f ? v : 0.f;
-        }
+        const float *p = a.Iin + (unsigned)d * (unsigned)a.g.nxy + (unsigned)(i0 + j0 * nx);
+        c00 = __ldg(p), c01 = __ldg(p + nx), c10 = __ldg(p + 1), c11 = __ldg(p + nx + 1);
     }
-    const float f0 = cv[0] * (1.f - fx) + cv[2] * fx;
-    const float f1 = cv[1] * (1.f - fx) + cv[3] * fx;
-    const float bil = f0 * (1.f - fy) + f1 * fy;
-    return CURVED ? r.w * bil : bil;
+    const float f0 = fmaf(fx, c10 - c00, c00);
+    const float f1 = fmaf(fx, c11 - c01, c01);
+    return fmaf(fy, f1 - f0, f0);
 }
 
 // direction coefficients of the affine collide map for a moving fluid
@@ -288,7 +294,7 @@ __device__ __forceinline__ void collide_coeffs(float n1, float n2, float u1, flo
 }
 
 template <bool CURVED>
-__global__ void __launch_bounds__(kStepBlock, 6) k_step_prec(PrecStepArgs a, const __grid_constant__ DirTable dt)
+__global__ void __launch_bounds__(kStepBlock, GRLBM_PREC_MIN_BLOCKS) k_step_prec(PrecStepArgs a, const __grid_constant__ DirTable dt)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float *ring = reinterpret_cast<float *>(smem_raw);
@@ -309,58 +315,58 @@ __global__ void __launch_bounds__(kStepBlock, 6) k_step_prec(PrecStepArgs a, con
     // writes them in this step).
     float *Is = a.Iout + (unsigned)ij;
 
+    // row-type table of the angular interpolation and direction coefficients
+    // of the moment sums, from the kernel parameter
+    float *rowtab = ring + kRingSlots * kPatch;
+    float4 *dirc = reinterpret_cast<float4 *>(rowtab + kMaxRowTypes * 12);
+    if (CURVED)
+        for (int k = t; k < dt.q * 12; k += kStepBlock)
+            rowtab[k] = dt.rowtab[k];
+    for (int k = t; k < 2 * a.nd; k += kStepBlock)
+        dirc[k] = reinterpret_cast<const float4 *>(dt.dirc)[k];
+
     const StageSlots ss = stage_slots(a.g, x0, y0);
+    const int cell = ty * kPatchX + tx; // patch offset of node (i - 1, j - 1)
     stage_planes(a, ss, ring, -kBelow, kSpan);
 
     KMoments km;
     km.zero();
     // records are read once per step: streaming loads, prefetched two
-    // directions ahead, two directions per iteration
+    // directions ahead (the last record stands in past the end)
     const float4 *rp = a.rec + cc;
     const unsigned rs = (unsigned)a.g.ncell;
-    const float4 none = make_float4(0.f, 0.f, 0.f, 0.f);
-    float4 r0 = none, r1 = none;
-    if (CURVED && live)
+    const unsigned dlast = (unsigned)(a.nd - 1);
+    float4 r0 = make_float4(0.f, 0.f, 0.f, 0.f), r1 = r0;
+    if (CURVED)
     {
         r0 = __ldcs(rp);
-        if (a.nd > 1)
-            r1 = __ldcs(rp + rs);
+        r1 = __ldcs(rp + min(1u, dlast) * rs);
     }
-    int chunk0 = 0;
-    for (int d = 0; d < a.nd; d += 2)
+    for (int chunk0 = 0; chunk0 < a.nd; chunk0 += kChunk)
     {
-        if (d % kChunk == 0)
+        cp_async_wait_all();
+        __syncthreads(); // this chunk's planes visible; the previous chunk is done with its slots
+        if (chunk0 + kChunk < a.nd)
+            stage_planes(a, ss, ring, chunk0 + kSpan - kBelow, kChunk);
+        const int dend = min(chunk0 + kChunk, a.nd);
+#pragma unroll kPrecUnroll
+        for (int d = chunk0; d < dend; d++)
         {
-            chunk0 = d;
-            cp_async_wait_all();
-            __syncthreads(); // this chunk's planes visible; the previous chunk is done with its slots
-            if (d + kChunk < a.nd)
-                stage_planes(a, ss, ring, d + kSpan - kBelow, kChunk);
+            float4 r2 = r0;
+            if (CURVED)
+                r2 = __ldcs(rp + min((unsigned)(d + 2), dlast) * rs);
+            float v = 0.f;
+            if (live)
+                v = CURVED ? stream_curved(a, dt, ring, rowtab, d, r0, cell, (unsigned)cc + (unsigned)d * rs, ii, jj)
+                           : stream_flat(a, dt, ring, d, chunk0, ii, jj, x0, y0);
+            if (collides)
+                Is[(unsigned)d * nxy] = v;
+            km.add(v, dirc[2 * d], dirc[2 * d + 1]);
+            r0 = r1;
+            r1 = r2;
         }
-        float4 r2 = none, r3 = none;
-        if (CURVED && live)
-        {
-            if (d + 2 < a.nd)
-                r2 = __ldcs(rp + (unsigned)(d + 2) * rs);
-            if (d + 3 < a.nd)
-                r3 = __ldcs(rp + (unsigned)(d + 3) * rs);
-        }
-        const bool second = d + 1 < a.nd;
-        const float v0 = live ? stream_value<CURVED>(a, dt, ring, d, chunk0, r0, ii, jj, x0, y0) : 0.f;
-        const float v1 = (live && second) ? stream_value<CURVED>(a, dt, ring, d + 1, chunk0, r1, ii, jj, x0, y0) : 0.f;
-        if (collides)
-        {
-            Is[(unsigned)d * nxy] = v0;
-            if (second)
-                Is[(unsigned)(d + 1) * nxy] = v1;
-        }
-        km.add(dt.w[d], v0, dt.n1[d], dt.n2[d]);
-        if (second)
-            km.add(dt.w[d + 1], v1, dt.n1[d + 1], dt.n2[d + 1]);
-        r0 = r2;
-        r1 = r3;
+        km.fold();
     }
-    km.finish();
     float m[6] = {km.E.s, km.Fx.s, km.Fy.s, km.Pxx.s, km.Pxy.s, km.Pyy.s};
 
     int cycles = 0;
@@ -451,7 +457,8 @@ __global__ void __launch_bounds__(kStepBlock, 6) k_step_prec(PrecStepArgs a, con
                 const int d = d0 + k;
                 if (d >= a.nd)
                     break;
-                const float n1 = dt.n1[d], n2 = dt.n2[d];
+                const float4 c0 = dirc[2 * d], c1 = dirc[2 * d + 1];
+                const float n1 = c1.z, n2 = c1.w;
                 float v;
                 if (rest)
                     v = fmaf(g0, S[k], fmaf(rb1, n1, fmaf(rb2, n2, ra)));
@@ -462,10 +469,10 @@ __global__ void __launch_bounds__(kStepBlock, 6) k_step_prec(PrecStepArgs a, con
                     v = g * S[k] + h * (e + k3 * (q1 * fFx + q2 * fFy));
                 }
                 Is[(unsigned)d * nxy] = v * scale;
-                km.add(dt.w[d], v, n1, n2);
+                km.add(v, c0, c1);
             }
+            km.fold();
         }
-        km.finish();
         m[0] = km.E.s, m[1] = km.Fx.s, m[2] = km.Fy.s, m[3] = km.Pxx.s, m[4] = km.Pxy.s, m[5] = km.Pyy.s;
     }
     if (active)
@@ -492,7 +499,7 @@ __global__ void __launch_bounds__(kStepBlock, 6) k_step_prec(PrecStepArgs a, con
 inline unsigned nblk(int64_t n, int b) { return (unsigned)((n + b - 1) / b); }
 } // namespace
 
-size_t step_prec_smem(int) { return (size_t)kRing * kPatch * sizeof(float); }
+size_t step_prec_smem(int nd) { return ((size_t)kRingSlots * kPatch + kMaxRowTypes * 12 + 8 * (size_t)nd) * sizeof(float); }
 
 cudaError_t prepare_step_prec(int smem_bytes)
 {

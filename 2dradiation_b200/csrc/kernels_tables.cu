@@ -353,10 +353,12 @@ __global__ void __launch_bounds__(128) k_departure(DepartureArgs a)
     }
     double4 r64;
     float4 r32;
+    double dd; // angle coordinate of the departure direction
     if (dev_inside_bh(a.g, xt, yt))
     {
         r64 = make_double4((double)i, (double)j, -1.0, 0.0);
-        r32 = make_float4(0.f, 0.f, 10.f * d + 5.f, 0.f);
+        dd = 10.0 * d + 5.0;
+        r32 = make_float4(0.f, 0.f, (float)dd, 0.f);
     }
     else
     {
@@ -368,11 +370,11 @@ __global__ void __launch_bounds__(128) k_departure(DepartureArgs a)
         const double w1 = v1 * a.rot_c - v2 * a.rot_s;
         const double w2 = v1 * a.rot_s + v2 * a.rot_c;
         // InterpolationGrid::d (src/Stencil.cpp:35-38)
-        double dd = (double)a.ng * approx_phi(w1, w2) / (2.0 * kPi);
+        dd = (double)a.ng * approx_phi(w1, w2) / (2.0 * kPi);
         dd = dd < 1e-8 ? 1e-8 : (dd > (double)a.ng - 1e-8 ? (double)a.ng - 1e-8 : dd);
         const double s3 = s * (s * s);
         r64 = make_double4(it, jt, dd, s3);
-        // compact FP32 record: offsets kept on the grid, alpha_c^3 folded in
+        // FP32 side record: offsets kept on the grid, alpha_c^3 folded in
         double ox = it - (double)i, oy = jt - (double)j;
         const double lox = -(double)i, hix = (double)(a.g.nx - 2 - i) + 0.999;
         const double loy = -(double)j, hiy = (double)(a.g.ny - 2 - j) + 0.999;
@@ -385,10 +387,37 @@ __global__ void __launch_bounds__(128) k_departure(DepartureArgs a)
         const double al = a.alpha[ij];
         r32 = make_float4((float)ox, (float)oy, (float)dd, (float)(s3 * (al * al * al)));
     }
+    if (a.rec32)
+    {
+        // packed record: corner code, row type, window start and blend
+        const double fxd = floor((double)r32.x), fyd = floor((double)r32.y);
+        const bool near = (fxd == -1.0 || fxd == 0.0) && (fyd == -1.0 || fyd == 0.0);
+        double ddc = dd == dd ? dd : 0.0;
+        int g = (int)floor(ddc);
+        g = g < 0 ? 0 : (g > a.ng - 1 ? a.ng - 1 : g);
+        double t = ddc - (double)g;
+        t = t < 0.0 ? 0.0 : (t > 1.0 ? 1.0 : t);
+        const int rt = g % a.q, m = g / a.q;
+        int dbase = (a.row_base[rt] + a.p * m) % a.nd - d;
+        if (2 * dbase > a.nd)
+            dbase -= a.nd;
+        else if (2 * dbase <= -a.nd)
+            dbase += a.nd;
+        const int rel = d % kChunk + dbase + kBelow;
+        const bool inspan = rel >= 0 && rel <= kSpan - kTaps;
+        unsigned tq = (unsigned)(t * (double)(1u << packed::kTBits) + 0.5);
+        tq = tq > (1u << packed::kTBits) - 1u ? (1u << packed::kTBits) - 1u : tq;
+        const unsigned code = near ? (unsigned)(fxd + 1.0) + 2u * (unsigned)(fyd + 1.0) : 0u;
+        const bool far = !near || !inspan;
+        const unsigned word = tq | ((unsigned)rt << packed::kTypeShift) |
+                              ((unsigned)((far ? 0 : dbase) + packed::kBaseBias) << packed::kBaseShift) |
+                              (code << packed::kCodeShift) | ((far ? 1u : 0u) << packed::kFarBit);
+        const float fx = near ? (float)((double)r32.x - fxd) : 0.f, fy = near ? (float)((double)r32.y - fyd) : 0.f;
+        a.rec32[tid] = make_float4(__uint_as_float(word), fx, fy, r32.w);
+        a.side32[tid] = r32;
+    }
     if (a.rec64)
         a.rec64[tid] = r64;
-    if (a.rec32)
-        a.rec32[tid] = r32;
 }
 
 // (alpha_ij / alpha_n)^3 for the 3x3 neighbours n of each interior node, as

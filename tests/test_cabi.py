@@ -63,8 +63,9 @@ def test_create_rejects_bad_arguments(grlbm, W, over, code):
     assert msg
 
 
-def test_fp64_direction_limit(grlbm, W):
-    rc, msg = _create(grlbm, W.curved_shell(nx_=8, ny_=8, n_dir=256, steps=1))
+@pytest.mark.parametrize("precision", [0, 1])
+def test_direction_limit(grlbm, W, precision):
+    rc, msg = _create(grlbm, W.curved_shell(nx_=8, ny_=8, n_dir=257, steps=1), precision=precision)
     assert rc == 1 and "n_dir" in msg
 
 

@@ -124,7 +124,7 @@ def test_end_to_end_config2_scale(grlbm, W, oracle):
 @pytest.mark.parametrize("kw", [
     dict(nx_=37, ny_=23, n_dir=12, n_fourier=5),      # ragged interior, partial blocks
     dict(nx_=2, ny_=2, n_dir=8, n_fourier=3),         # smallest grid
-    dict(nx_=30, ny_=18, n_dir=200, n_fourier=7),     # widest FP64 stencil (200 KB shared memory)
+    dict(nx_=30, ny_=18, n_dir=200, n_fourier=7),     # wide stencil
     dict(nx_=21, ny_=21, n_dir=64, n_fourier=32),     # many harmonics
 ])
 def test_edge_shapes_bitwise_against_oracle(kw, grlbm, W, oracle):
