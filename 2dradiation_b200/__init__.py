@@ -84,6 +84,10 @@ SIGNATURES = {
     "grlbm_energy": ([C.c_void_p, _D], C.c_int),
     "grlbm_energy_noalloc": ([C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p], C.c_int),
     "grlbm_get_stats": ([C.c_void_p, C.POINTER(Stats)], C.c_int),
+    "grlbm_set_rows": ([C.c_void_p, C.c_int64, C.c_int64], C.c_int),
+    "grlbm_row_bytes": ([C.c_void_p, C.POINTER(C.c_int64)], C.c_int),
+    "grlbm_copy_rows": ([C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_int32], C.c_int),
+    "grlbm_departure_rows": ([C.c_void_p, C.POINTER(C.c_int32)], C.c_int),
     "grlbm_host_stencil": ([C.c_int32, C.c_int32, _D, _D, _D, _D, C.POINTER(C.c_int64), _D], C.c_int),
     "grlbm_host_flux_table": ([C.c_int32, C.POINTER(C.c_int32), _D, _D, _D, C.c_int32], C.c_int),
     "grlbm_host_metric_arrays": ([C.POINTER(GridDesc), C.POINTER(MetricDesc), _D], C.c_int),
@@ -161,6 +165,7 @@ class Radiation:
 
     def __init__(self, case: dict, precision: int = PLAIN_FP64, device: int = -1):
         self.case = case
+        self.precision = precision
         self.nd = int(case["n_dir"])
         self.nf = int(case["n_fourier"])
         g, m = grid_desc(case), metric_desc(case)
@@ -260,6 +265,25 @@ class Radiation:
     def energy(self) -> float:
         v = C.c_double()
         self._c(lib().grlbm_energy(self.h, C.byref(v)))
+        return v.value
+
+    # ---- slab decomposition (one band of interior node rows per rank) ----
+    def set_rows(self, j_first: int, j_end: int):
+        self._c(lib().grlbm_set_rows(self.h, j_first, j_end))
+
+    def row_bytes(self) -> int:
+        v = C.c_int64()
+        self._c(lib().grlbm_row_bytes(self.h, C.byref(v)))
+        return v.value
+
+    def copy_rows(self, j_first: int, n: int, buffer_ptr: int, to_buffer: bool):
+        """Rows [j_first, j_first + n) of the state to/from a device buffer
+        (stream-ordered on the context's stream)."""
+        self._c(lib().grlbm_copy_rows(self.h, j_first, n, C.c_void_p(buffer_ptr), 1 if to_buffer else 0))
+
+    def departure_rows(self) -> int:
+        v = C.c_int32()
+        self._c(lib().grlbm_departure_rows(self.h, C.byref(v)))
         return v.value
 
     def stats(self) -> dict:

@@ -56,6 +56,9 @@ constexpr int kMaxFourier = 64;
 struct GridDev
 {
     int64_t nx, ny, nxy, nx_, ny_, ncell;
+    // interior node rows [jlo, jhi) the step updates (a slab; all rows by
+    // default: 1, ny - 1)
+    int64_t jlo, jhi;
     double dx, dy, dt, startx, starty, endx, endy;
     int kind;
     double excision2;
@@ -127,6 +130,7 @@ struct DepartureArgs
     int q, p;            // interpolation row period (row types) and its direction shift
     int row_base[32];    // first window direction of each row type
     int *clamped;
+    int *row_extent;     // max over departures of the node rows away from the cell a gather reads
 };
 
 // One row of the cubic interpolation grid: 4 directions and their weights.

@@ -282,7 +282,8 @@ int build_records(grlbm_ctx *ctx)
     for (int r = 0; r < ctx->dirs.q && r < kMaxRowTypes; r++)
         da.row_base[r] = (int)ctx->dirs.rowtab[r * 12 + 10];
     da.clamped = reinterpret_cast<int *>(ctx->counters.as<unsigned long long>() + 4);
-    CU(cudaMemsetAsync(ctx->counters.as<unsigned long long>() + 4, 0, sizeof(unsigned long long), ctx->stream));
+    da.row_extent = reinterpret_cast<int *>(ctx->counters.as<unsigned long long>() + 5);
+    CU(cudaMemsetAsync(ctx->counters.as<unsigned long long>() + 4, 0, 2 * sizeof(unsigned long long), ctx->stream));
     launch_departure(da, ctx->stream);
     CU(cudaGetLastError());
     return GRLBM_OK;
@@ -411,6 +412,8 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
     gd.nx_ = grid->nx_;
     gd.ny_ = grid->ny_;
     gd.ncell = ctx->ncell;
+    gd.jlo = 1;
+    gd.jhi = G.ny - 1;
     gd.dx = G.dx;
     gd.dy = G.dy;
     gd.dt = G.dt;
@@ -1040,6 +1043,76 @@ int grlbm_energy(grlbm_ctx *ctx, double *total)
     return GRLBM_OK;
 }
 
+int grlbm_set_rows(grlbm_ctx *ctx, int64_t j_first, int64_t j_end)
+{
+    if (!ctx)
+        return GRLBM_ERR_ARGUMENT;
+    if (j_first < 1 || j_end > ctx->geo.ny - 1 || j_first >= j_end)
+        return fail(ctx, GRLBM_ERR_ARGUMENT, "rows [%lld, %lld) outside the interior rows [1, %lld)",
+                    (long long)j_first, (long long)j_end, (long long)(ctx->geo.ny - 1));
+    cudaSetDevice(ctx->device);
+    CU(cudaStreamSynchronize(ctx->stream));
+    ctx->gd.jlo = j_first;
+    ctx->gd.jhi = j_end;
+    invalidate_graphs(ctx);
+    return GRLBM_OK;
+}
+
+int grlbm_row_bytes(const grlbm_ctx *ctx, int64_t *bytes)
+{
+    if (!ctx || !bytes)
+        return GRLBM_ERR_ARGUMENT;
+    *bytes = ctx->geo.nx * (int64_t)ctx->st.n * (int64_t)tsize(ctx);
+    return GRLBM_OK;
+}
+
+int grlbm_copy_rows(grlbm_ctx *ctx, int64_t j_first, int64_t n, void *buffer, int32_t to_buffer)
+{
+    if (!ctx)
+        return GRLBM_ERR_ARGUMENT;
+    if (!buffer || n < 0 || j_first < 0 || j_first + n > ctx->geo.ny)
+        return fail(ctx, GRLBM_ERR_ARGUMENT, "rows [%lld, %lld) outside the grid's %lld rows", (long long)j_first,
+                    (long long)(j_first + n), (long long)ctx->geo.ny);
+    if (n == 0)
+        return GRLBM_OK;
+    cudaSetDevice(ctx->device);
+    const size_t es = tsize(ctx), width = (size_t)n * ctx->geo.nx * es, pitch = (size_t)ctx->geo.nxy * es;
+    char *state = static_cast<char *>(ctx->I[ctx->cur].p) + (size_t)j_first * ctx->geo.nx * es;
+    if (to_buffer)
+        CU(cudaMemcpy2DAsync(buffer, width, state, pitch, width, (size_t)ctx->st.n, cudaMemcpyDeviceToDevice,
+                             ctx->stream));
+    else
+        CU(cudaMemcpy2DAsync(state, pitch, buffer, width, width, (size_t)ctx->st.n, cudaMemcpyDeviceToDevice,
+                             ctx->stream));
+    return GRLBM_OK;
+}
+
+int grlbm_departure_rows(grlbm_ctx *ctx, int32_t *rows)
+{
+    if (!ctx || !rows)
+        return GRLBM_ERR_ARGUMENT;
+    if (ctx->run.streaming_type == GRLBM_FLAT_FIXED)
+    {
+        int ext = 0;
+        for (int d = 0; d < ctx->st.n; d++)
+        {
+            const double oy = -ctx->st.cy[d] * ctx->geo.dt / ctx->geo.dy;
+            const double jf = std::floor(oy);
+            ext = std::max(ext, (int)std::max(std::fabs(jf), std::fabs(jf + 1.0)));
+        }
+        *rows = ext;
+        return GRLBM_OK;
+    }
+    if (!ctx->tables)
+        return fail(ctx, GRLBM_ERR_STATE, "departure rows need the geodesic tables");
+    cudaSetDevice(ctx->device);
+    unsigned long long h[6];
+    CU(cudaStreamSynchronize(ctx->stream));
+    CU(cudaMemcpy(h, ctx->counters.p, sizeof h, cudaMemcpyDeviceToHost));
+    *rows = (int32_t)(unsigned)(h[5] & 0xffffffffu);
+    return GRLBM_OK;
+}
+
 int grlbm_get_stats(grlbm_ctx *ctx, grlbm_stats *s)
 {
     if (!ctx)
@@ -1052,7 +1125,7 @@ int grlbm_get_stats(grlbm_ctx *ctx, grlbm_stats *s)
     CU(cudaMemcpy(h, ctx->counters.p, sizeof h, cudaMemcpyDeviceToHost));
     s->steps = ctx->steps;
     s->max_iterations = (int32_t)(unsigned)(h[1] & 0xffffffffu);
-    const double denom = (double)ctx->steps * (double)(ctx->geo.nx - 2) * (double)(ctx->geo.ny - 2);
+    const double denom = (double)ctx->steps * (double)(ctx->geo.nx - 2) * (double)(ctx->gd.jhi - ctx->gd.jlo);
     s->average_iterations = ctx->steps ? (double)h[0] / denom : 0.0;
     s->rk_substeps = (int64_t)h[2];
     s->rk_nonconverged = (int32_t)(unsigned)h[3];

@@ -157,9 +157,11 @@ template <bool CURVED>
 __global__ void __launch_bounds__(kStepBlock, GRLBM_PLAIN_MIN_BLOCKS) k_step_plain(PlainStepArgs a)
 {
     const int t = threadIdx.x;
+    // cells of the slab rows [jlo, jhi), numbered from its first cell
+    const int64_t c0 = (a.g.jlo - 1) * a.g.nx_;
     const int64_t c = (int64_t)blockIdx.x * kStepBlock + t;
-    const bool active = c < a.g.ncell;
-    const int64_t cc = active ? c : 0;
+    const bool active = c < (a.g.jhi - a.g.jlo) * a.g.nx_;
+    const int64_t cc = c0 + (active ? c : 0);
     const int64_t i = 1 + cc % a.g.nx_, j = 1 + cc / a.g.nx_;
     const int64_t ij = i + j * a.g.nx;
     const int64_t nxy = a.g.nxy;
@@ -350,7 +352,8 @@ __global__ void __launch_bounds__(256) k_energy_partial(GridDev g, const T *E, d
     __shared__ double s[256];
     const int t = threadIdx.x;
     double acc = 0.0;
-    for (int64_t c = (int64_t)blockIdx.x * 256 + t; c < g.ncell; c += (int64_t)gridDim.x * 256)
+    const int64_t c0 = (g.jlo - 1) * g.nx_, c1 = (g.jhi - 1) * g.nx_; // the slab's cells
+    for (int64_t c = c0 + (int64_t)blockIdx.x * 256 + t; c < c1; c += (int64_t)gridDim.x * 256)
     {
         const int64_t i = 1 + c % g.nx_, j = 1 + c / g.nx_;
         acc += (double)E[i + j * g.nx];
@@ -452,10 +455,13 @@ cudaError_t prepare_step_plain(int smem_bytes)
 void launch_step_plain(const PlainStepArgs &a, bool curved, cudaStream_t s)
 {
     const size_t smem = 0;
+    const int64_t cells = (a.g.jhi - a.g.jlo) * a.g.nx_;
+    if (cells <= 0)
+        return;
     if (curved)
-        k_step_plain<true><<<nblk(a.g.ncell, kStepBlock), kStepBlock, smem, s>>>(a);
+        k_step_plain<true><<<nblk(cells, kStepBlock), kStepBlock, smem, s>>>(a);
     else
-        k_step_plain<false><<<nblk(a.g.ncell, kStepBlock), kStepBlock, smem, s>>>(a);
+        k_step_plain<false><<<nblk(cells, kStepBlock), kStepBlock, smem, s>>>(a);
 }
 void launch_sources64(double *I, int64_t nxy, int nd, const int64_t *nodes, const double *vals, int64_t nsrc,
                       cudaStream_t s)

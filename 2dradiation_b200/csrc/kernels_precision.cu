@@ -300,9 +300,10 @@ __global__ void __launch_bounds__(kStepBlock, GRLBM_PREC_MIN_BLOCKS) k_step_prec
     float *ring = reinterpret_cast<float *>(smem_raw);
     const int t = threadIdx.x;
     const int tx = t % kTileX, ty = t / kTileX;
-    const int x0 = blockIdx.x * kTileX, y0 = blockIdx.y * kTileY; // patch origin (node coordinates)
+    // patch origin (node coordinates); tiles cover the slab rows [jlo, jhi)
+    const int x0 = blockIdx.x * kTileX, y0 = (int)a.g.jlo - 1 + blockIdx.y * kTileY;
     const int i = 1 + x0 + tx, j = 1 + y0 + ty;
-    const bool active = i <= (int)a.g.nx_ && j <= (int)a.g.ny_;
+    const bool active = i <= (int)a.g.nx_ && j < (int)a.g.jhi;
     const int ii = active ? i : 1, jj = active ? j : 1;
     const int ij = ii + jj * (int)a.g.nx;
     const int cc = (ii - 1) + (jj - 1) * (int)a.g.nx_;
@@ -511,7 +512,9 @@ cudaError_t prepare_step_prec(int smem_bytes)
 void launch_step_prec(const PrecStepArgs &a, const DirTable &dt, bool curved, cudaStream_t s)
 {
     const size_t smem = step_prec_smem(a.nd);
-    const dim3 grid(nblk(a.g.nx_, kTileX), nblk(a.g.ny_, kTileY));
+    if (a.g.jhi <= a.g.jlo)
+        return;
+    const dim3 grid(nblk(a.g.nx_, kTileX), nblk(a.g.jhi - a.g.jlo, kTileY));
     if (curved)
         k_step_prec<true><<<grid, kStepBlock, smem, s>>>(a, dt);
     else

@@ -366,6 +366,13 @@ __global__ void __launch_bounds__(128) k_departure(DepartureArgs a)
         const double jt = (yt - a.g.starty) / a.g.dy;
         if (!(it >= 0.0 && it < (double)(a.g.nx - 1) && jt >= 0.0 && jt < (double)(a.g.ny - 1)))
             atomicAdd(a.clamped, 1);
+        if (jt == jt)
+        {
+            // node rows the bilinear gather reads, relative to the cell (a slab's ghost depth)
+            const double jf = floor(jt) - (double)j;
+            const double ext = fmax(fabs(jf), fabs(jf + 1.0));
+            atomicMax(a.row_extent, ext < 1e9 ? (int)ext : 1000000000);
+        }
         // RotationMatrix(0).Inverse() * v (src/DataTypes.hh:625-635)
         const double w1 = v1 * a.rot_c - v2 * a.rot_s;
         const double w2 = v1 * a.rot_s + v2 * a.rot_c;

@@ -24,8 +24,11 @@ fields and the initial intensities from pinned host memory, runs a full
 from its sources into oracle/_ref, else the oracle restatement) with all host
 threads on the same workload, one solver step per bench step.
 
-Run: python bench.py [--gpus N --steps K --warmup W] (N>1 under torchrun:
-independent replicas per rank, max time over ranks).
+Run: python bench.py [--gpus N --steps K --warmup W].  N>1 runs under
+torchrun as a slab decomposition (2dradiation_b200/slabs.py): the grid grows
+to 400 x 400N cells, each GPU steps one 400-row band and exchanges its ghost
+rows with its neighbours over NCCL before every step (weak scaling; device
+time per step, max over ranks).
 """
 from __future__ import annotations
 
@@ -183,23 +186,36 @@ def profiled_traffic(kernel: str):
         return None
 
 
-def time_steps(G, r, steps: int, warmup: int, flush):
-    """Per-step device time (ms) on the library's stream, L2 flushed between steps."""
+def time_steps(G, r, steps: int, warmup: int, flush, advance):
+    """Per-step device time (ms) on the library's stream, L2 flushed between
+    steps; `advance` enqueues one step (with its ghost-row exchange on
+    several GPUs)."""
     import torch
     ext = torch.cuda.ExternalStream(r.stream)
     with torch.cuda.stream(ext):
         for _ in range(warmup):
-            r.step_async(1)
+            advance()
             flush.zero_()
         ext.synchronize()
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
         for s, e in ev:
             s.record(ext)
-            r.step_async(1)
+            advance()
             e.record(ext)
             flush.zero_()
         ext.synchronize()
     return [s.elapsed_time(e) for s, e in ev]
+
+
+def open_form(G, case, prec, world, rank, local, pg):
+    """A context for one form: the whole grid on one GPU, or this rank's band
+    of a slab decomposition (ghost rows exchanged before every step)."""
+    if world == 1:
+        r = G.prepare(case, prec, device=local)
+        return r, (lambda: r.step_async(1)), None
+    S = importlib.import_module("2dradiation_b200.slabs")
+    r, slab = S.open_slab(case, prec, rank, world, local, pg)
+    return r, (lambda: slab.step(1)), slab
 
 
 def run_grlbm(a, world, rank, local, pg):
@@ -208,7 +224,8 @@ def run_grlbm(a, world, rank, local, pg):
     W = G.workloads
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    case = W.curved_scatter(nx_=a.nx, ny_=a.nx, n_dir=a.dirs, n_fourier=a.fourier, steps=a.e2e_steps)
+    # one 400-row band per GPU: the grid grows with the GPU count (weak scaling)
+    case = W.curved_scatter(nx_=a.nx, ny_=a.nx * world, n_dir=a.dirs, n_fourier=a.fourier, steps=a.e2e_steps)
     ncell, nd = a.nx * a.nx, a.dirs
     units = ncell * nd
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
@@ -218,13 +235,14 @@ def run_grlbm(a, world, rank, local, pg):
         forms = {}
         states = {}
         for name, prec in (("fp32", G.PRECISION_FP32), ("fp64", G.PLAIN_FP64)):
-            r = G.prepare(case, prec, device=local)
+            r, advance, slab = open_form(G, case, prec, world, rank, local, pg)
             st = r.stats()
             barrier(pg, dev)
-            ms = time_steps(G, r, a.steps, a.warmup, flush)
+            ms = time_steps(G, r, a.steps, a.warmup, flush, advance)
             total = max_over_ranks(sum(ms), pg, dev)
             forms[name] = {"ms": ms, "total_ms": total, "table_ms": st["table_ms"], "rk_substeps": st["rk_substeps"]}
-            states[name] = r.moments_if()
+            lo, hi = slab.band if slab is not None else (1, a.nx + 1)
+            states[name] = {k: v[lo * (a.nx + 2):hi * (a.nx + 2)] for k, v in r.moments_if().items()}
             forms[name]["iters"] = r.stats()
             r.close()
         # e2e through the C-ABI with pinned host buffers
@@ -234,7 +252,8 @@ def run_grlbm(a, world, rank, local, pg):
         I0 = torch.zeros(W.nxy(case) * nd, dtype=torch.float64).pin_memory().numpy()
         mom = {k: torch.zeros(W.nxy(case), dtype=torch.float64).pin_memory().numpy()
                for k in ("E", "Fx", "Fy", "Pxx", "Pxy", "Pyy")}
-        r = G.prepare(case, G.PRECISION_FP32, device=local) if a.e2e_reps > 0 else None
+        r, advance, slab = open_form(G, case, G.PRECISION_FP32, world, rank, local, pg) if a.e2e_reps > 0 \
+            else (None, None, None)
         e2e_t = []
         for rep in range(a.e2e_reps + 1 if r is not None else 0):
             barrier(pg, dev)
@@ -242,7 +261,10 @@ def run_grlbm(a, world, rank, local, pg):
             t0 = time.perf_counter()
             r.set_fields(host)
             r.set_intensity(I0)
-            r.step(a.e2e_steps)
+            if slab is None:
+                r.step(a.e2e_steps)
+            else:
+                slab.step(a.e2e_steps)
             r.moments_if(mom)
             t1 = time.perf_counter()
             if rep > 0:
@@ -283,7 +305,8 @@ def run_grlbm(a, world, rank, local, pg):
             "form": "precision: FP32 intensities and stream/collide, Kahan FP32 moments, FP64 geodesic tables",
             "step": "one time step (fused stream + moments + lambda-iteration collide) over all interior cells",
             "l2": "flushed between timed steps by a 256 MiB write (untimed)",
-            "parallelism": "single GPU" if world == 1 else f"{world} independent replicas, one per GPU",
+            "parallelism": "single GPU" if world == 1 else
+            f"slab decomposition: {world} bands of {a.nx} rows, one per GPU, ghost rows exchanged over NCCL every step",
             "global_batch": units,
         },
         "roofline": {

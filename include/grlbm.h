@@ -210,6 +210,26 @@ int grlbm_energy(grlbm_ctx *ctx, double *total);
  * device looks the array up and must come before any stream capture.  The
  * call returns once the work is enqueued (asynchronous). */
 int grlbm_energy_noalloc(const double *E, int64_t nx_, int64_t ny_, double *total, void *stream);
+/* ---- slab decomposition ---------------------------------------------------
+ * No counterpart in the reference (it runs on one node, Readme.txt:5-6): one
+ * context per GPU holds the whole grid but steps only a band of interior node
+ * rows; neighbouring ranks exchange the rows next to their bands between
+ * steps.  grlbm_step and grlbm_energy then cover interior node rows
+ * [j_first, j_end) only (1 <= j_first < j_end <= ny - 1; the default is all
+ * interior rows). */
+int grlbm_set_rows(grlbm_ctx *ctx, int64_t j_first, int64_t j_end);
+/* Bytes of one node row of the intensity state over all directions
+ * (nx * nDir * 8 for GRLBM_PLAIN_FP64, * 4 for GRLBM_PRECISION_FP32). */
+int grlbm_row_bytes(const grlbm_ctx *ctx, int64_t *bytes);
+/* Copies node rows [j_first, j_first + n) of the current intensity state
+ * (every direction) to (to_buffer = 1) or from (to_buffer = 0) a contiguous
+ * device buffer laid out [direction][row][i], n * row_bytes bytes.  Enqueued
+ * on the context's stream; returns before it completes. */
+int grlbm_copy_rows(grlbm_ctx *ctx, int64_t j_first, int64_t n, void *buffer, int32_t to_buffer);
+/* The most node rows away from its cell that any stream gather reads (from
+ * the departure records of the last table build; from the stencil for flat
+ * streaming): the ghost depth a band needs on each side. */
+int grlbm_departure_rows(grlbm_ctx *ctx, int32_t *rows);
 /* Lambda-iteration and table-build statistics (src/Radiation.cpp:723-733,
  * 855-857). */
 int grlbm_get_stats(grlbm_ctx *ctx, grlbm_stats *stats);

@@ -1,0 +1,65 @@
+"""Slab decomposition on one GPU: three contexts of the same problem, each
+stepping one band of interior rows (grlbm_set_rows), exchange the rows next
+to their bands through grlbm_copy_rows before every step -- the exchange a
+multi-GPU run does over NCCL, here as device copies between contexts.  The
+bands together must reproduce the whole-grid run bit for bit, in both forms:
+every cell's arithmetic is the same, only where it runs differs."""
+import importlib
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("maker,kw", [
+    ("curved_scatter", dict(nx_=64, ny_=45, n_dir=16, n_fourier=9, steps=12)),
+    ("moving_scatter", dict(nx_=40, ny_=33, n_dir=24, n_fourier=5, steps=10)),
+    ("flat_beam", dict(nx_=50, ny_=31, n_dir=20, steps=15)),
+])
+def test_bands_reproduce_whole_grid(grlbm, W, precision, maker, kw):
+    import torch
+    S = importlib.import_module("2dradiation_b200.slabs")
+    case = W.make_case(maker, **kw)
+    steps = int(case["n_steps"])
+    with grlbm.prepare(case, precision) as whole:
+        whole.step(steps)
+        ref = whole.moments_if()
+        refI = whole.intensity().reshape(whole.nxy, whole.nd)
+    world = 3
+    bands = S.partition(int(case["ny_"]), world)
+    rads = [grlbm.prepare(case, precision) for _ in range(world)]
+    try:
+        g = rads[0].departure_rows()
+        assert 1 <= g <= min(b - a for a, b in bands)
+        for r, b in zip(rads, bands):
+            r.set_rows(*b)
+        dtype = torch.float32 if precision == 1 else torch.float64
+        buf = torch.empty(g * rads[0].row_bytes() // dtype.itemsize, dtype=dtype, device="cuda")
+        for _ in range(steps):
+            for k in range(world - 1):
+                lo_of_next = bands[k + 1][0]
+                # rank k's top rows -> rank k+1's lower ghost rows
+                rads[k].copy_rows(lo_of_next - g, g, buf.data_ptr(), True)
+                rads[k].sync()
+                rads[k + 1].copy_rows(lo_of_next - g, g, buf.data_ptr(), False)
+                rads[k + 1].sync()
+                # rank k+1's bottom rows -> rank k's upper ghost rows
+                rads[k + 1].copy_rows(lo_of_next, g, buf.data_ptr(), True)
+                rads[k + 1].sync()
+                rads[k].copy_rows(lo_of_next, g, buf.data_ptr(), False)
+                rads[k].sync()
+            for r in rads:
+                r.step(1)
+        nx = rads[0].nx
+        for r, (lo, hi) in zip(rads, bands):
+            m = r.moments_if()
+            I = r.intensity().reshape(r.nxy, r.nd)
+            rows = slice(lo * nx, hi * nx)
+            for k in ("E", "Fx", "Fy", "Pxx", "Pxy", "Pyy"):
+                assert np.array_equal(m[k][rows], ref[k][rows]), (k, lo, hi)
+            assert np.array_equal(I[rows], refI[rows])
+    finally:
+        for r in rads:
+            r.close()
