@@ -84,6 +84,11 @@ SIGNATURES = {
     "grlbm_energy": ([C.c_void_p, _D], C.c_int),
     "grlbm_energy_noalloc": ([C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p], C.c_int),
     "grlbm_get_stats": ([C.c_void_p, C.POINTER(Stats)], C.c_int),
+    "grlbm_batch_create": ([C.POINTER(C.c_void_p), C.c_int32, C.POINTER(C.c_void_p)], C.c_int),
+    "grlbm_batch_destroy": ([C.c_void_p], None),
+    "grlbm_batch_last_error": ([C.c_void_p], C.c_char_p),
+    "grlbm_batch_step": ([C.c_void_p, C.c_int32], C.c_int),
+    "grlbm_batch_autotune": ([C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32)], C.c_int),
     "grlbm_set_rows": ([C.c_void_p, C.c_int64, C.c_int64], C.c_int),
     "grlbm_row_bytes": ([C.c_void_p, C.POINTER(C.c_int64)], C.c_int),
     "grlbm_copy_rows": ([C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_int32], C.c_int),
@@ -290,6 +295,49 @@ class Radiation:
         s = Stats()
         self._c(lib().grlbm_get_stats(self.h, C.byref(s)))
         return {k: getattr(s, k) for k, _ in Stats._fields_}
+
+
+class Batch:
+    """Several precision-form problems stepped together by one persistent
+    launch per step (grlbm_batch_*).  The Radiation objects stay usable."""
+
+    def __init__(self, problems: list):
+        self.problems = list(problems)
+        arr = (C.c_void_p * len(self.problems))(*[p.h for p in self.problems])
+        h = C.c_void_p()
+        rc = lib().grlbm_batch_create(arr, len(self.problems), C.byref(h))
+        if rc != OK:
+            raise GrlbmError(rc, (lib().grlbm_batch_last_error(None) or b"").decode())
+        self.h = h
+
+    def _c(self, rc):
+        if rc != OK:
+            raise GrlbmError(rc, (lib().grlbm_batch_last_error(self.h) or b"").decode())
+
+    def step(self, n: int):
+        self._c(lib().grlbm_batch_step(self.h, n))
+
+    def autotune(self, trial_steps: int = 4) -> dict:
+        bps, lf = C.c_int32(), C.c_int32()
+        self._c(lib().grlbm_batch_autotune(self.h, trial_steps, C.byref(bps), C.byref(lf)))
+        return {"blocks_per_sm": bps.value, "largest_first": bool(lf.value)}
+
+    def close(self):
+        if self.h:
+            lib().grlbm_batch_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def prepare(case: dict, precision: int = PLAIN_FP64, device: int = -1) -> Radiation:

@@ -34,6 +34,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <cstddef>
 #include <cstdint>
 
 namespace grlbm
@@ -188,15 +189,29 @@ struct PrecStepArgs
 // starts p m directions further on: q row types of 12 floats
 // {W0[0..3]}, {D[0..3]}, {W0[4], D[4], first direction of row r, 0}.
 constexpr int kMaxRowTypes = 32;
-struct DirTable
+struct __align__(16) DirTable
 {
     float w[kMaxDirs], n1[kMaxDirs], n2[kMaxDirs], ox[kMaxDirs], oy[kMaxDirs];
     float wmom[18];
-    float rowtab[kMaxRowTypes * 12];
+    // both read as float4 (from the parameter space, or from global memory in
+    // a batch), so 16-byte aligned
+    __align__(16) float rowtab[kMaxRowTypes * 12];
     // moment-sum coefficients per direction: {w, w n1, w n2, w n1^2}, {w n1 n2, w n2^2, n1, n2}
-    float dirc[kMaxDirs * 8];
+    __align__(16) float dirc[kMaxDirs * 8];
     int q, p;
     float inv_q;
+};
+static_assert(offsetof(DirTable, rowtab) % 16 == 0 && offsetof(DirTable, dirc) % 16 == 0 &&
+                  sizeof(DirTable) % 16 == 0,
+              "DirTable float4 members");
+
+// One problem of a batched precision-form step: its step arguments for
+// either buffer parity, its direction tables (device memory) and its tiles.
+struct BatchItem
+{
+    PrecStepArgs a[2]; // a[k]: the step that reads intensity buffer k
+    const DirTable *dt;
+    int tiles_x, tiles_y, curved, cur0;
 };
 
 // Records a message for grlbm_last_error(NULL) (defined in grlbm_capi.cu).
@@ -213,6 +228,11 @@ void launch_step_plain(const PlainStepArgs &a, bool curved, cudaStream_t s);
 cudaError_t prepare_step_prec(int smem_bytes);
 size_t step_prec_smem(int nd);
 void launch_step_prec(const PrecStepArgs &a, const DirTable &dt, bool curved, cudaStream_t s);
+int step_prec_tiles_x(int64_t nx_);
+int step_prec_tiles_y(int64_t rows);
+cudaError_t prepare_step_batch(int smem_bytes, int *blocks_per_sm);
+void launch_step_batch(const BatchItem *items, const int *first_tile, int n_items, int total_tiles, int flip,
+                       int blocks, int smem_bytes, cudaStream_t s);
 
 void launch_sources64(double *I, int64_t nxy, int nd, const int64_t *nodes, const double *vals, int64_t nsrc,
                       cudaStream_t s);

@@ -166,6 +166,34 @@ const float *state_scale(const grlbm_ctx *ctx)
     return (ctx->fp32 && ctx->run.streaming_type == GRLBM_CURVED_FIXED) ? ctx->ia3.as<float>() : nullptr;
 }
 
+// Arguments of the precision-form step that reads intensity buffer `from`.
+PrecStepArgs prec_args(grlbm_ctx *ctx, int from)
+{
+    unsigned long long *cnt = ctx->counters.as<unsigned long long>();
+    PrecStepArgs a{};
+    a.g = ctx->gd;
+    a.nd = ctx->st.n;
+    a.ng = ctx->ng;
+    a.Iin = ctx->I[from].as<float>();
+    a.Iout = ctx->I[from ^ 1].as<float>();
+    a.rec = ctx->rec.as<float4>();
+    a.side = ctx->side.as<float4>();
+    a.ia3 = ctx->ia3.as<float>();
+    a.flags = ctx->flags.as<uint8_t>();
+    a.u1 = ctx->cu1.as<float>();
+    a.u2 = ctx->cu2.as<float>();
+    a.lor = ctx->clor.as<float>();
+    a.adt = ctx->cadt.as<float>();
+    a.eta = ctx->ceta.as<float>();
+    a.k0 = ctx->ck0.as<float>();
+    a.k3 = ctx->ck3.as<float>();
+    a.ka = ctx->cka.as<float>();
+    a.mom = ctx->mom.as<float>();
+    a.iter_sum = cnt;
+    a.iter_max = reinterpret_cast<unsigned int *>(cnt + 1);
+    return a;
+}
+
 // Enqueue one step starting from buffer `from` (no sync).
 int enqueue_step(grlbm_ctx *ctx, int from)
 {
@@ -176,27 +204,7 @@ int enqueue_step(grlbm_ctx *ctx, int from)
         if (ctx->run.keep_source_nodes_active && ctx->nsrc > 0)
             launch_sources32(ctx->I[from].as<float>(), ctx->gd.nxy, ctx->st.n, ctx->src_nodes.as<int64_t>(),
                              ctx->src_vals.as<float>(), ctx->nsrc, ctx->stream);
-        PrecStepArgs a{};
-        a.g = ctx->gd;
-        a.nd = ctx->st.n;
-        a.ng = ctx->ng;
-        a.Iin = ctx->I[from].as<float>();
-        a.Iout = ctx->I[from ^ 1].as<float>();
-        a.rec = ctx->rec.as<float4>();
-        a.side = ctx->side.as<float4>();
-        a.ia3 = ctx->ia3.as<float>();
-        a.flags = ctx->flags.as<uint8_t>();
-        a.u1 = ctx->cu1.as<float>();
-        a.u2 = ctx->cu2.as<float>();
-        a.lor = ctx->clor.as<float>();
-        a.adt = ctx->cadt.as<float>();
-        a.eta = ctx->ceta.as<float>();
-        a.k0 = ctx->ck0.as<float>();
-        a.k3 = ctx->ck3.as<float>();
-        a.ka = ctx->cka.as<float>();
-        a.mom = ctx->mom.as<float>();
-        a.iter_sum = cnt;
-        a.iter_max = reinterpret_cast<unsigned int *>(cnt + 1);
+        const PrecStepArgs a = prec_args(ctx, from);
         launch_step_prec(a, ctx->dirs, curved, ctx->stream);
     }
     else
@@ -1191,6 +1199,320 @@ int grlbm_host_metric_arrays(const grlbm_grid_desc *grid, const grlbm_metric_des
     const GridGeom g = GridGeom::from(*grid);
     const MetricArrays M = MetricArrays::build(g, *metric);
     std::copy(M.arr.begin(), M.arr.end(), out);
+    return GRLBM_OK;
+}
+
+} // extern "C"
+
+// ---------------------------------------------------------------- batches
+struct grlbm_batch
+{
+    std::string err;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::vector<grlbm_ctx *> ctx;
+    std::vector<BatchItem> items; // in launch order
+    std::vector<int> order;       // items[k] is context order[k]
+    DevBuf d_items, d_first, d_dirs;
+    int total_tiles = 0, smem = 0, blocks_per_sm_max = 1, blocks_per_sm = 1, sms = 1;
+    int largest_first = 0;
+    int flip = 0; // parity of the steps taken since the items were built
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    ~grlbm_batch()
+    {
+        for (auto &g : graph)
+            if (g)
+                cudaGraphExecDestroy(g);
+        if (stream)
+            cudaStreamDestroy(stream);
+    }
+};
+
+namespace
+{
+int bfail(grlbm_batch *b, int code, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (b)
+        b->err = buf;
+    else
+        g_create_error = buf;
+    return code;
+}
+
+#define BCU(call)                                                                                  \
+    do                                                                                             \
+    {                                                                                              \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess)                                                                     \
+            return bfail(b, GRLBM_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));       \
+    } while (0)
+
+void batch_drop_graphs(grlbm_batch *b)
+{
+    for (auto &g : b->graph)
+        if (g)
+        {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+}
+
+// (Re)build the launch list from the contexts' current buffers, in the
+// chosen order, and upload it.
+int batch_build(grlbm_batch *b)
+{
+    const int n = (int)b->ctx.size();
+    std::vector<int> order(n);
+    for (int k = 0; k < n; k++)
+        order[k] = k;
+    if (b->largest_first)
+        std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+            const grlbm_ctx *a = b->ctx[x], *c = b->ctx[y];
+            return a->ncell * a->st.n > c->ncell * c->st.n;
+        });
+    b->order = order;
+    b->items.assign(n, BatchItem{});
+    std::vector<int> first(n + 1, 0);
+    const DirTable *dirs = b->d_dirs.as<DirTable>();
+    for (int k = 0; k < n; k++)
+    {
+        grlbm_ctx *c = b->ctx[order[k]];
+        BatchItem &it = b->items[k];
+        it.a[0] = prec_args(c, 0);
+        it.a[1] = prec_args(c, 1);
+        it.dt = dirs + order[k];
+        it.tiles_x = step_prec_tiles_x(c->gd.nx_);
+        it.tiles_y = step_prec_tiles_y(c->gd.jhi - c->gd.jlo);
+        it.curved = c->run.streaming_type == GRLBM_CURVED_FIXED;
+        it.cur0 = c->cur;
+        first[k + 1] = first[k] + it.tiles_x * it.tiles_y;
+    }
+    b->total_tiles = first[n];
+    if (alloc(nullptr, b->d_items, n * sizeof(BatchItem)) || alloc(nullptr, b->d_first, (n + 1) * sizeof(int)))
+        return bfail(b, GRLBM_ERR_CUDA, "cannot allocate the batch launch list");
+    BCU(cudaMemcpy(b->d_items.p, b->items.data(), n * sizeof(BatchItem), cudaMemcpyHostToDevice));
+    BCU(cudaMemcpy(b->d_first.p, first.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice));
+    b->flip = 0;
+    batch_drop_graphs(b);
+    return GRLBM_OK;
+}
+
+void batch_enqueue(grlbm_batch *b, int flip)
+{
+    launch_step_batch(b->d_items.as<BatchItem>(), b->d_first.as<int>(), (int)b->items.size(), b->total_tiles, flip,
+                      b->sms * b->blocks_per_sm, b->smem, b->stream);
+}
+
+// Brings the launch list in line with the contexts (stepped on their own
+// since the last batch step, or never batched): rebuilt when any context's
+// current buffer is not the one the list expects.
+int batch_sync_state(grlbm_batch *b)
+{
+    for (size_t k = 0; k < b->items.size(); k++)
+        if (b->ctx[b->order[k]]->cur != (b->items[k].cur0 ^ b->flip))
+            return batch_build(b);
+    return GRLBM_OK;
+}
+
+int batch_steps(grlbm_batch *b, int n)
+{
+    for (grlbm_ctx *c : b->ctx)
+        BCU(cudaStreamSynchronize(c->stream));
+    int rc = batch_sync_state(b);
+    if (rc)
+        return rc;
+    int left = n;
+    while (left >= kGraphSteps)
+    {
+        if (!b->graph[b->flip])
+        {
+            cudaGraph_t g = nullptr;
+            BCU(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+            for (int s = 0; s < kGraphSteps; s++)
+                batch_enqueue(b, b->flip ^ (s & 1));
+            cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+            if (e != cudaSuccess)
+                return bfail(b, GRLBM_ERR_CUDA, "batch graph capture failed: %s", cudaGetErrorString(e));
+            e = cudaGraphInstantiate(&b->graph[b->flip], g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess)
+                return bfail(b, GRLBM_ERR_CUDA, "batch graph instantiation failed: %s", cudaGetErrorString(e));
+        }
+        BCU(cudaGraphLaunch(b->graph[b->flip], b->stream));
+        left -= kGraphSteps; // even: parity unchanged
+    }
+    for (; left > 0; left--)
+    {
+        batch_enqueue(b, b->flip);
+        b->flip ^= 1;
+    }
+    BCU(cudaGetLastError());
+    BCU(cudaStreamSynchronize(b->stream));
+    for (size_t k = 0; k < b->items.size(); k++)
+    {
+        grlbm_ctx *c = b->ctx[b->order[k]];
+        c->cur = b->items[k].cur0 ^ b->flip;
+        c->steps += n;
+    }
+    return GRLBM_OK;
+}
+} // namespace
+
+extern "C" {
+
+int grlbm_batch_create(grlbm_ctx *const *ctxs, int32_t n, grlbm_batch **out)
+{
+    if (!ctxs || !out || n < 1)
+        return bfail(nullptr, GRLBM_ERR_ARGUMENT, "grlbm_batch_create: no contexts");
+    *out = nullptr;
+    std::unique_ptr<grlbm_batch> owner(new grlbm_batch);
+    grlbm_batch *b = owner.get();
+    int max_nd = 0;
+    for (int k = 0; k < n; k++)
+    {
+        grlbm_ctx *c = ctxs[k];
+        if (!c)
+            return bfail(nullptr, GRLBM_ERR_ARGUMENT, "grlbm_batch_create: context %d is null", k);
+        if (!c->fp32)
+            return bfail(nullptr, GRLBM_ERR_UNSUPPORTED, "grlbm_batch_create: context %d is not GRLBM_PRECISION_FP32", k);
+        if (c->device != ctxs[0]->device)
+            return bfail(nullptr, GRLBM_ERR_ARGUMENT, "grlbm_batch_create: contexts on different devices");
+        if (c->run.streaming_type == GRLBM_CURVED_FIXED && !c->tables)
+            return bfail(nullptr, GRLBM_ERR_STATE, "grlbm_batch_create: context %d has no geodesic tables", k);
+        if (c->run.keep_source_nodes_active && c->nsrc > 0)
+            return bfail(nullptr, GRLBM_ERR_UNSUPPORTED,
+                         "grlbm_batch_create: context %d keeps source nodes active (not batched)", k);
+        for (int j = 0; j < k; j++)
+            if (ctxs[j] == c)
+                return bfail(nullptr, GRLBM_ERR_ARGUMENT, "grlbm_batch_create: context %d appears twice", k);
+        max_nd = std::max(max_nd, c->st.n);
+        b->ctx.push_back(c);
+    }
+    b->device = ctxs[0]->device;
+    cudaSetDevice(b->device);
+    BCU(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+    b->smem = (int)step_prec_smem(max_nd);
+    BCU(prepare_step_batch(b->smem, &b->blocks_per_sm_max));
+    if (b->blocks_per_sm_max < 1)
+        return bfail(nullptr, GRLBM_ERR_CUDA, "grlbm_batch_create: the batched kernel does not fit on an SM");
+    b->blocks_per_sm = b->blocks_per_sm_max;
+    BCU(cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, b->device));
+    std::vector<DirTable> dirs(n);
+    for (int k = 0; k < n; k++)
+        dirs[k] = ctxs[k]->dirs;
+    if (upload(nullptr, b->d_dirs, dirs))
+        return bfail(nullptr, GRLBM_ERR_CUDA, "grlbm_batch_create: cannot upload the direction tables");
+    int rc = batch_build(b);
+    if (rc)
+        return bfail(nullptr, rc, "%s", b->err.c_str());
+    *out = owner.release();
+    return GRLBM_OK;
+}
+
+void grlbm_batch_destroy(grlbm_batch *b)
+{
+    if (b)
+    {
+        cudaSetDevice(b->device);
+        cudaStreamSynchronize(b->stream);
+        delete b;
+    }
+}
+
+const char *grlbm_batch_last_error(const grlbm_batch *b) { return b ? b->err.c_str() : g_create_error.c_str(); }
+
+int grlbm_batch_step(grlbm_batch *b, int32_t n_steps)
+{
+    if (!b)
+        return GRLBM_ERR_ARGUMENT;
+    if (n_steps < 0)
+        return bfail(b, GRLBM_ERR_ARGUMENT, "negative step count");
+    cudaSetDevice(b->device);
+    return batch_steps(b, n_steps);
+}
+
+int grlbm_batch_autotune(grlbm_batch *b, int32_t trial_steps, int32_t *blocks_per_sm, int32_t *largest_first)
+{
+    if (!b)
+        return GRLBM_ERR_ARGUMENT;
+    if (trial_steps < 1)
+        return bfail(b, GRLBM_ERR_ARGUMENT, "trial_steps must be positive");
+    cudaSetDevice(b->device);
+    for (grlbm_ctx *c : b->ctx)
+        BCU(cudaStreamSynchronize(c->stream));
+    int rc = batch_sync_state(b);
+    if (rc)
+        return rc;
+    // save every problem's state (current intensities, moments, counters);
+    // the trial steps are undone afterwards
+    const size_t n = b->ctx.size();
+    std::vector<std::unique_ptr<DevBuf>> saved(3 * n);
+    for (size_t k = 0; k < n; k++)
+    {
+        grlbm_ctx *c = b->ctx[k];
+        DevBuf *src[3] = {&c->I[c->cur], &c->mom, &c->counters};
+        for (int q = 0; q < 3; q++)
+        {
+            saved[3 * k + q].reset(new DevBuf);
+            if (alloc(nullptr, *saved[3 * k + q], src[q]->bytes))
+                return bfail(b, GRLBM_ERR_CUDA, "autotune: cannot allocate a state copy");
+            BCU(cudaMemcpy(saved[3 * k + q]->p, src[q]->p, src[q]->bytes, cudaMemcpyDeviceToDevice));
+        }
+    }
+    const int flip0 = b->flip;
+    float best = 0.f;
+    int best_bps = b->blocks_per_sm, best_lf = b->largest_first;
+    cudaEvent_t e0, e1;
+    BCU(cudaEventCreate(&e0));
+    BCU(cudaEventCreate(&e1));
+    for (int lf = 0; lf <= 1; lf++)
+        for (int bps = b->blocks_per_sm_max; bps >= 1 && bps >= b->blocks_per_sm_max - 2; bps--)
+        {
+            b->largest_first = lf;
+            b->blocks_per_sm = bps;
+            if ((rc = batch_build(b)))
+                break;
+            batch_enqueue(b, 0); // warm-up
+            cudaEventRecord(e0, b->stream);
+            for (int s = 0; s < trial_steps; s++)
+                batch_enqueue(b, (s + 1) & 1);
+            cudaEventRecord(e1, b->stream);
+            if (cudaStreamSynchronize(b->stream) != cudaSuccess)
+            {
+                rc = bfail(b, GRLBM_ERR_CUDA, "autotune: trial steps failed");
+                break;
+            }
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (best == 0.f || ms < best)
+                best = ms, best_bps = bps, best_lf = lf;
+        }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    // restore the saved state
+    for (size_t k = 0; k < n; k++)
+    {
+        grlbm_ctx *c = b->ctx[k];
+        DevBuf *dst[3] = {&c->I[c->cur], &c->mom, &c->counters};
+        for (int q = 0; q < 3; q++)
+            BCU(cudaMemcpy(dst[q]->p, saved[3 * k + q]->p, dst[q]->bytes, cudaMemcpyDeviceToDevice));
+    }
+    if (rc)
+        return rc;
+    b->blocks_per_sm = best_bps;
+    b->largest_first = best_lf;
+    (void)flip0;
+    if ((rc = batch_build(b)))
+        return rc;
+    if (blocks_per_sm)
+        *blocks_per_sm = best_bps;
+    if (largest_first)
+        *largest_first = best_lf;
     return GRLBM_OK;
 }
 

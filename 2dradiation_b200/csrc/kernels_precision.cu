@@ -293,15 +293,17 @@ __device__ __forceinline__ void collide_coeffs(float n1, float n2, float u1, flo
     h = adt / (A * A) * g;
 }
 
+// One tile (kTileX x kTileY cells of the slab rows) of one step: stream,
+// moments and collide for its cells.  bx, by: tile coordinates.
 template <bool CURVED>
-__global__ void __launch_bounds__(kStepBlock, GRLBM_PREC_MIN_BLOCKS) k_step_prec(PrecStepArgs a, const __grid_constant__ DirTable dt)
+__device__ __forceinline__ void step_tile(const PrecStepArgs &a, const DirTable &dt, int bx, int by,
+                                          unsigned char *smem_raw)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     float *ring = reinterpret_cast<float *>(smem_raw);
     const int t = threadIdx.x;
     const int tx = t % kTileX, ty = t / kTileX;
     // patch origin (node coordinates); tiles cover the slab rows [jlo, jhi)
-    const int x0 = blockIdx.x * kTileX, y0 = (int)a.g.jlo - 1 + blockIdx.y * kTileY;
+    const int x0 = bx * kTileX, y0 = (int)a.g.jlo - 1 + by * kTileY;
     const int i = 1 + x0 + tx, j = 1 + y0 + ty;
     const bool active = i <= (int)a.g.nx_ && j < (int)a.g.jhi;
     const int ii = active ? i : 1, jj = active ? j : 1;
@@ -497,8 +499,64 @@ __global__ void __launch_bounds__(kStepBlock, GRLBM_PREC_MIN_BLOCKS) k_step_prec
     }
 }
 
+template <bool CURVED>
+__global__ void __launch_bounds__(kStepBlock, GRLBM_PREC_MIN_BLOCKS)
+    k_step_prec(PrecStepArgs a, const __grid_constant__ DirTable dt)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    step_tile<CURVED>(a, dt, blockIdx.x, blockIdx.y, smem_raw);
+}
+
+// Many problems in one persistent launch: the blocks walk the concatenated
+// tile list (problem k owns tiles [first_tile[k], first_tile[k+1])) with a
+// grid-stride loop; each tile runs the same code as the single-problem
+// kernel, so every problem's result is the one it gets alone.
+__global__ void __launch_bounds__(kStepBlock, GRLBM_PREC_MIN_BLOCKS)
+    k_step_batch(const BatchItem *__restrict__ items, const int *__restrict__ first_tile, int n_items,
+                 int total_tiles, int flip)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x)
+    {
+        int lo = 0, hi = n_items - 1;
+        while (lo < hi)
+        {
+            const int mid = (lo + hi + 1) >> 1;
+            if (first_tile[mid] <= tile)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        const BatchItem &it = items[lo];
+        const int local = tile - first_tile[lo];
+        const int bx = local % it.tiles_x, by = local / it.tiles_x;
+        const PrecStepArgs &a = it.a[it.cur0 ^ flip];
+        if (it.curved)
+            step_tile<true>(a, *it.dt, bx, by, smem_raw);
+        else
+            step_tile<false>(a, *it.dt, bx, by, smem_raw);
+        __syncthreads(); // the next tile reuses the shared stage
+    }
+}
+
 inline unsigned nblk(int64_t n, int b) { return (unsigned)((n + b - 1) / b); }
 } // namespace
+
+int step_prec_tiles_x(int64_t nx_) { return (int)nblk(nx_, kTileX); }
+int step_prec_tiles_y(int64_t rows) { return (int)nblk(rows, kTileY); }
+
+cudaError_t prepare_step_batch(int smem_bytes, int *blocks_per_sm)
+{
+    cudaError_t e = cudaFuncSetAttribute(k_step_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
+    if (e != cudaSuccess)
+        return e;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_step_batch, kStepBlock, smem_bytes);
+}
+void launch_step_batch(const BatchItem *items, const int *first_tile, int n_items, int total_tiles, int flip,
+                       int blocks, int smem_bytes, cudaStream_t s)
+{
+    k_step_batch<<<blocks, kStepBlock, smem_bytes, s>>>(items, first_tile, n_items, total_tiles, flip);
+}
 
 size_t step_prec_smem(int nd) { return ((size_t)kRingSlots * kPatch + kMaxRowTypes * 12 + 8 * (size_t)nd) * sizeof(float); }
 

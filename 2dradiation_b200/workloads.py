@@ -175,6 +175,34 @@ WORKLOADS = {
 }
 
 
+def batch_instances(count=64, seed=10, sizes=(64, 128, 256, 512), dirs=(16, 32, 64), steps=500,
+                    n_fourier=5, rk_tol=1e-10):
+    """Independent problems of uneven size for the batched form: per instance
+    a grid size from `sizes` (square), a direction count from `dirs`, and flat
+    (Minkowski, flat streaming) or Schwarzschild M=1 (Kerr-Schild
+    coordinates, curved streaming, excision r <= 2.4) at random, on
+    [-6,6]^2.  Fields as the curved-shell problem (eta = 1 on 3.8 <= r <= 4.2,
+    kappaA ~ U[0, 0.5) for r < 5) plus scattering kappa0 ~ U[0, 1) for r < 5,
+    each instance with its own seeds; intensities start at zero."""
+    u = uniform(seed, 3 * count).reshape(count, 3)
+    out = []
+    for k in range(count):
+        n = int(sizes[min(int(u[k, 0] * len(sizes)), len(sizes) - 1)])
+        nd = int(dirs[min(int(u[k, 1] * len(dirs)), len(dirs) - 1)])
+        curved = u[k, 2] >= 0.5
+        c = _base(f"batch{k}", n, n, (-6, -6), (6, 6), nd, n_fourier, steps,
+                  KERRSCHILD if curved else MINKOWSKI, CURVED_FIXED if curved else FLAT_FIXED,
+                  excision=2.4 if curved else -1.0, rk_tol=rk_tol)
+        X, Y, _, _ = grid_coords(n, n, (-6, -6), (6, 6))
+        r = np.sqrt(X * X + Y * Y)
+        f = c["fields"]
+        f["eta"][(r >= 3.8) & (r <= 4.2)] = 1.0
+        f["kappaA"][:] = np.where(r < 5.0, 0.5 * uniform(1000 + 2 * k + seed, X.size), 0.0)
+        f["kappa0"][:] = np.where(r < 5.0, uniform(1001 + 2 * k + seed, X.size), 0.0)
+        out.append(c)
+    return out
+
+
 def make_case(name: str, **overrides) -> dict:
     return WORKLOADS[name](**overrides)
 

@@ -230,6 +230,29 @@ int grlbm_copy_rows(grlbm_ctx *ctx, int64_t j_first, int64_t n, void *buffer, in
  * the departure records of the last table build; from the stencil for flat
  * streaming): the ghost depth a band needs on each side. */
 int grlbm_departure_rows(grlbm_ctx *ctx, int32_t *rows);
+/* ---- batches ----------------------------------------------------------------
+ * No counterpart in the reference.  Many GRLBM_PRECISION_FP32 problems on one
+ * GPU (any grid sizes, direction counts, flat or curved streaming) stepped by
+ * one persistent kernel launch per time step, replayed from CUDA graphs of
+ * 32 steps.  Each problem's result is bit-identical to stepping it alone; its
+ * context stays usable (moments, intensities, statistics) between batch
+ * steps.  Problems that keep source nodes active are not batched
+ * (GRLBM_ERR_UNSUPPORTED).  A batch refers to its contexts: destroy it before
+ * them. */
+typedef struct grlbm_batch grlbm_batch;
+int grlbm_batch_create(grlbm_ctx *const *ctxs, int32_t n, grlbm_batch **out);
+void grlbm_batch_destroy(grlbm_batch *batch);
+/* Describes the last failure of a batch call (batch may be NULL for
+ * grlbm_batch_create). */
+const char *grlbm_batch_last_error(const grlbm_batch *batch);
+/* n_steps time steps of every problem (synchronous). */
+int grlbm_batch_step(grlbm_batch *batch, int32_t n_steps);
+/* Times trial_steps steps for each launch shape -- resident blocks per SM
+ * (the occupancy limit and up to two fewer) and the order of the problems'
+ * tiles (as given, or largest problem first) -- keeps the fastest, and puts
+ * every problem back in the state it had before the call.  The choice is
+ * returned in *blocks_per_sm and *largest_first (either may be NULL). */
+int grlbm_batch_autotune(grlbm_batch *batch, int32_t trial_steps, int32_t *blocks_per_sm, int32_t *largest_first);
 /* Lambda-iteration and table-build statistics (src/Radiation.cpp:723-733,
  * 855-857). */
 int grlbm_get_stats(grlbm_ctx *ctx, grlbm_stats *stats);

@@ -1,0 +1,49 @@
+"""Batched precision-form steps (grlbm_batch_*): problems of different grid
+sizes, direction counts and streaming types advanced by one persistent launch
+per step must each match their single-problem run bit for bit -- across
+graph-replayed and single steps, after autotuning (which must leave every
+problem as it was), and when a problem is also stepped on its own between
+batch steps."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def test_batch_matches_single_problems(grlbm, W):
+    cases = W.batch_instances(count=7, seed=12, sizes=(24, 37, 64), dirs=(8, 16, 32), steps=40)
+    assert len({c["n_dir"] for c in cases}) > 1 and len({c["streaming_type"] for c in cases}) > 1
+    P = grlbm.PRECISION_FP32
+    ref = []
+    for k, c in enumerate(cases):
+        with grlbm.prepare(c, P) as r:
+            r.step(37 + 6 + (1 if k == 0 else 0))
+            ref.append((r.moments_if()["E"], r.intensity(), r.stats()["average_iterations"]))
+    probs = [grlbm.prepare(c, P) for c in cases]
+    try:
+        with grlbm.Batch(probs) as b:
+            choice = b.autotune(3)
+            assert choice["blocks_per_sm"] >= 1
+            b.step(37)          # one 32-step graph and 5 single launches
+            probs[0].step(1)    # a problem stepped on its own in between
+            b.step(6)
+        for k, (r, (E, I, it)) in enumerate(zip(probs, ref)):
+            assert np.array_equal(r.moments_if()["E"], E), k
+            assert np.array_equal(r.intensity(), I), k
+            assert r.stats()["average_iterations"] == it, k
+    finally:
+        for r in probs:
+            r.close()
+
+
+def test_batch_rejects_plain_and_source_problems(grlbm, W):
+    c = W.batch_instances(count=1, seed=3, sizes=(24,), dirs=(8,), steps=2)[0]
+    with grlbm.prepare(c, grlbm.PLAIN_FP64) as r:
+        with pytest.raises(grlbm.GrlbmError) as e:
+            grlbm.Batch([r])
+        assert e.value.code == 4
+    beam = W.flat_beam(nx_=20, ny_=20, n_dir=8, steps=2)
+    with grlbm.prepare(beam, grlbm.PRECISION_FP32) as r:
+        with pytest.raises(grlbm.GrlbmError) as e:
+            grlbm.Batch([r])
+        assert e.value.code == 4
