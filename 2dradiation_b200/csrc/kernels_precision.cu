@@ -547,7 +547,8 @@ int step_prec_tiles_y(int64_t rows) { return (int)nblk(rows, kTileY); }
 
 cudaError_t prepare_step_batch(int smem_bytes, int *blocks_per_sm)
 {
-    cudaError_t e = cudaFuncSetAttribute(k_step_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
+    cudaError_t e = cudaFuncSetAttribute(k_step_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)step_prec_smem(kMaxDirs));
     if (e != cudaSuccess)
         return e;
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_step_batch, kStepBlock, smem_bytes);
@@ -560,8 +561,12 @@ void launch_step_batch(const BatchItem *items, const int *first_tile, int n_item
 
 size_t step_prec_smem(int nd) { return ((size_t)kRingSlots * kPatch + kMaxRowTypes * 12 + 8 * (size_t)nd) * sizeof(float); }
 
-cudaError_t prepare_step_prec(int smem_bytes)
+// The shared-memory limit is a property of the kernel, shared by every
+// context in the process: it is set for the largest direction count, so
+// that no context's set-up lowers it below another's launches.
+cudaError_t prepare_step_prec(int)
 {
+    const int smem_bytes = (int)step_prec_smem(kMaxDirs);
     cudaError_t e = cudaFuncSetAttribute(k_step_prec<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
     if (e != cudaSuccess)
         return e;

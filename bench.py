@@ -67,6 +67,8 @@ def args_parse():
     p.add_argument("--nx", type=int, default=400)
     p.add_argument("--dirs", type=int, default=64)
     p.add_argument("--fourier", type=int, default=16)
+    p.add_argument("--batch-steps", type=int, default=64,
+                   help="timed steps of the batched form (64 uneven problems); 0 skips it")
     return p.parse_args()
 
 
@@ -218,6 +220,42 @@ def open_form(G, case, prec, world, rank, local, pg):
     return r, (lambda: slab.step(1)), slab
 
 
+def run_batched(G, W, a, local):
+    """The batched form on 64 uneven problems (grid 64^2..512^2, 16..64
+    directions, flat or Schwarzschild, seed 10): after autotuning, `batch_steps`
+    steps of all problems in one persistent launch per step, against the same
+    problems stepped through their own contexts (one stream each, enqueued
+    back to back)."""
+    import torch
+    cases = W.batch_instances(count=64, seed=10, steps=a.batch_steps)
+    probs = [G.prepare(c, G.PRECISION_FP32, device=local) for c in cases]
+    units = sum(int(c["nx_"]) * int(c["ny_"]) * int(c["n_dir"]) for c in cases)
+    try:
+        for r in probs:  # one step each: graphs and caches warm
+            r.step(1)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for r in probs:
+            r.step_async(a.batch_steps)
+        for r in probs:
+            r.sync()
+        single_s = time.perf_counter() - t0
+        with G.Batch(probs) as b:
+            choice = b.autotune(3)
+            b.step(2)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            b.step(a.batch_steps)
+            batch_s = time.perf_counter() - t0
+    finally:
+        for r in probs:
+            r.close()
+    return {"problems": len(cases), "cell_dir_per_step": units, "steps": a.batch_steps,
+            "value": units * a.batch_steps / batch_s, "unit": UNIT,
+            "separate_contexts": units * a.batch_steps / single_s, "autotune": choice,
+            "timing": "host clock around the synchronous batch step (persistent launch per step, 32-step graphs)"}
+
+
 def run_grlbm(a, world, rank, local, pg):
     import torch
     G = importlib.import_module("2dradiation_b200")
@@ -272,6 +310,7 @@ def run_grlbm(a, world, rank, local, pg):
         if r is not None:
             r.close()
         e2e_s = max_over_ranks(statistics.median(e2e_t) if e2e_t else float("nan"), pg, dev)
+        batched = run_batched(G, W, a, local) if a.batch_steps > 0 and world == 1 else None
     clocks = clk.summary()
 
     fp32, fp64 = forms["fp32"], forms["fp64"]
@@ -345,6 +384,7 @@ def run_grlbm(a, world, rank, local, pg):
             "seconds_per_step": e2e_s,
         },
         "gpu_launches": a.steps,
+        "batched": batched,
         "clocks": clocks,
     }
     if rank == 0 and world == 1 and not a.no_cpu_baseline:

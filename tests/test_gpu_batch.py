@@ -47,3 +47,15 @@ def test_batch_rejects_plain_and_source_problems(grlbm, W):
         with pytest.raises(grlbm.GrlbmError) as e:
             grlbm.Batch([r])
         assert e.value.code == 4
+
+
+def test_contexts_of_different_direction_counts_coexist(grlbm, W):
+    """Kernel launch limits are per process: creating a context with fewer
+    directions must not break the launches of one with more."""
+    big = W.batch_instances(count=1, seed=5, sizes=(24,), dirs=(64,), steps=3)[0]
+    small = W.batch_instances(count=1, seed=6, sizes=(24,), dirs=(8,), steps=3)[0]
+    for P in (grlbm.PRECISION_FP32, grlbm.PLAIN_FP64):
+        with grlbm.prepare(big, P) as a, grlbm.prepare(small, P) as b:
+            a.step(3)
+            b.step(3)
+            assert np.isfinite(a.moments_if()["E"]).all() and np.isfinite(b.moments_if()["E"]).all()
