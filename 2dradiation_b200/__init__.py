@@ -89,6 +89,11 @@ SIGNATURES = {
     "grlbm_batch_last_error": ([C.c_void_p], C.c_char_p),
     "grlbm_batch_step": ([C.c_void_p, C.c_int32], C.c_int),
     "grlbm_batch_autotune": ([C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32)], C.c_int),
+    "grlbm_adjoint_create": ([C.c_void_p, C.c_int32, C.POINTER(C.c_void_p)], C.c_int),
+    "grlbm_adjoint_destroy": ([C.c_void_p], None),
+    "grlbm_adjoint_last_error": ([C.c_void_p], C.c_char_p),
+    "grlbm_adjoint_forward": ([C.c_void_p, C.c_int32], C.c_int),
+    "grlbm_adjoint_backward": ([C.c_void_p, _D, _D, _D, _D], C.c_int),
     "grlbm_set_rows": ([C.c_void_p, C.c_int64, C.c_int64], C.c_int),
     "grlbm_row_bytes": ([C.c_void_p, C.POINTER(C.c_int64)], C.c_int),
     "grlbm_copy_rows": ([C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_int32], C.c_int),
@@ -295,6 +300,51 @@ class Radiation:
         s = Stats()
         self._c(lib().grlbm_get_stats(self.h, C.byref(s)))
         return {k: getattr(s, k) for k, _ in Stats._fields_}
+
+
+class Adjoint:
+    """Gradients of a loss of the final E with respect to eta, kappaA and
+    kappa0 by the hand-written adjoint (grlbm_adjoint_*) of a plain-form
+    Radiation whose fields and tables are set."""
+
+    def __init__(self, rad: "Radiation", checkpoint_every: int = 20):
+        self.rad = rad
+        h = C.c_void_p()
+        rc = lib().grlbm_adjoint_create(rad.h, checkpoint_every, C.byref(h))
+        if rc != OK:
+            raise GrlbmError(rc, (lib().grlbm_adjoint_last_error(None) or b"").decode())
+        self.h = h
+
+    def _c(self, rc):
+        if rc != OK:
+            raise GrlbmError(rc, (lib().grlbm_adjoint_last_error(self.h) or b"").decode())
+
+    def forward(self, n_steps: int):
+        self._c(lib().grlbm_adjoint_forward(self.h, n_steps))
+
+    def backward(self, dL_dE: np.ndarray) -> dict:
+        n = self.rad.nxy
+        g = {k: np.zeros(n) for k in ("eta", "kappaA", "kappa0")}
+        d = np.ascontiguousarray(dL_dE, dtype=np.float64)
+        self._c(lib().grlbm_adjoint_backward(self.h, _p(d), _p(g["eta"]), _p(g["kappaA"]), _p(g["kappa0"])))
+        return g
+
+    def close(self):
+        if self.h:
+            lib().grlbm_adjoint_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Batch:

@@ -134,6 +134,15 @@ struct DepartureArgs
     int *row_extent;     // max over departures of the node rows away from the cell a gather reads
 };
 
+// What a recording plain step writes for the adjoint (indices over the
+// interior cells c and directions d of the whole grid).
+struct StepRecord
+{
+    uint8_t *clamp; // [d * ncell + c]: bit q set where corner q was not clamped
+    int *cycles;    // [c]: lambda-iteration cycles of the cell (0: no collide)
+    double *e0;     // [c]: E of the streamed intensities (first iterate)
+};
+
 // One row of the cubic interpolation grid: 4 directions and their weights.
 struct __align__(16) IgRow
 {
@@ -205,6 +214,32 @@ static_assert(offsetof(DirTable, rowtab) % 16 == 0 && offsetof(DirTable, dirc) %
                   sizeof(DirTable) % 16 == 0,
               "DirTable float4 members");
 
+struct AdjEntryArgs
+{
+    GridDev g;
+    int nd, ng, curved;
+    const double4 *rec;   // plain departure records (curved)
+    const IgRow *ig_rows; // interpolation rows (curved)
+    const double *alpha, *acube;
+    const uint8_t *flags;
+    const double *cx, *cy; // intensity directions (flat)
+};
+
+struct AdjCollideArgs
+{
+    GridDev g;
+    int nd;
+    const double *w;                   // nd
+    const uint8_t *flags;              // nxy
+    const double *adt, *eta, *k0, *ka; // nxy
+    const float *lam;                  // [d * nxy + ij]: adjoint of the step's output intensities
+    const double *Iout;                // [d * nxy + ij]: the step's output intensities
+    const int *cycles;                 // [c]
+    const double *e0;                  // [c]
+    float *lamS;                       // [d * ncell + c]: adjoint of the streamed intensities
+    double *g_eta, *g_ka, *g_k0;       // nxy: gradients, accumulated
+};
+
 // One problem of a batched precision-form step: its step arguments for
 // either buffer parity, its direction tables (device memory) and its tiles.
 struct BatchItem
@@ -213,6 +248,15 @@ struct BatchItem
     const DirTable *dt;
     int tiles_x, tiles_y, curved, cur0;
 };
+
+int64_t adj_entries_per_source(bool curved);
+cudaError_t adj_build_table(const AdjEntryArgs &a, int64_t *offsets, unsigned **srcq, float **coef,
+                            int64_t *n_entries, cudaStream_t s);
+void launch_adj_seed(const GridDev &g, int nd, const double *w, const uint8_t *flags, const double *dLdE, float *lam,
+                     cudaStream_t s);
+void launch_adj_collide(const AdjCollideArgs &a, cudaStream_t s);
+void launch_adj_stream(const int64_t *offsets, const unsigned *srcq, const float *coef, const uint8_t *clamp,
+                       const float *lamS, int64_t n_targets, float *lam, cudaStream_t s);
 
 // Records a message for grlbm_last_error(NULL) (defined in grlbm_capi.cu).
 void set_global_error(const char *msg);
@@ -224,7 +268,7 @@ void launch_departure(const DepartureArgs &a, cudaStream_t s);
 void launch_alpha_cube(const GridDev &g, const double *alpha, double *acube, cudaStream_t s);
 
 cudaError_t prepare_step_plain(int smem_bytes);
-void launch_step_plain(const PlainStepArgs &a, bool curved, cudaStream_t s);
+void launch_step_plain(const PlainStepArgs &a, bool curved, cudaStream_t s, const StepRecord *record = nullptr);
 cudaError_t prepare_step_prec(int smem_bytes);
 size_t step_prec_smem(int nd);
 void launch_step_prec(const PrecStepArgs &a, const DirTable &dt, bool curved, cudaStream_t s);

@@ -194,6 +194,40 @@ PrecStepArgs prec_args(grlbm_ctx *ctx, int from)
     return a;
 }
 
+// Arguments of the plain step that reads intensity buffer `from`.
+PlainStepArgs plain_args(grlbm_ctx *ctx, int from)
+{
+    unsigned long long *cnt = ctx->counters.as<unsigned long long>();
+    PlainStepArgs a{};
+    a.g = ctx->gd;
+    a.nd = ctx->st.n;
+    a.ng = ctx->ng;
+    a.Iin = ctx->I[from].as<double>();
+    a.Iout = ctx->I[from ^ 1].as<double>();
+    a.rec = ctx->rec.as<double4>();
+    a.w = ctx->w.as<double>();
+    a.n1 = ctx->n1.as<double>();
+    a.n2 = ctx->n2.as<double>();
+    a.cx = ctx->cx.as<double>();
+    a.cy = ctx->cy.as<double>();
+    a.ig_rows = ctx->ig_rows.as<IgRow>();
+    a.alpha = ctx->alpha.as<double>();
+    a.acube = ctx->acube.as<double>();
+    a.flags = ctx->flags.as<uint8_t>();
+    a.u1 = ctx->cu1.as<double>();
+    a.u2 = ctx->cu2.as<double>();
+    a.lor = ctx->clor.as<double>();
+    a.adt = ctx->cadt.as<double>();
+    a.eta = ctx->ceta.as<double>();
+    a.k0 = ctx->ck0.as<double>();
+    a.k3 = ctx->ck3.as<double>();
+    a.ka = ctx->cka.as<double>();
+    a.mom = ctx->mom.as<double>();
+    a.iter_sum = cnt;
+    a.iter_max = reinterpret_cast<unsigned int *>(cnt + 1);
+    return a;
+}
+
 // Enqueue one step starting from buffer `from` (no sync).
 int enqueue_step(grlbm_ctx *ctx, int from)
 {
@@ -212,33 +246,7 @@ int enqueue_step(grlbm_ctx *ctx, int from)
         if (ctx->run.keep_source_nodes_active && ctx->nsrc > 0)
             launch_sources64(ctx->I[from].as<double>(), ctx->gd.nxy, ctx->st.n, ctx->src_nodes.as<int64_t>(),
                              ctx->src_vals.as<double>(), ctx->nsrc, ctx->stream);
-        PlainStepArgs a{};
-        a.g = ctx->gd;
-        a.nd = ctx->st.n;
-        a.ng = ctx->ng;
-        a.Iin = ctx->I[from].as<double>();
-        a.Iout = ctx->I[from ^ 1].as<double>();
-        a.rec = ctx->rec.as<double4>();
-        a.w = ctx->w.as<double>();
-        a.n1 = ctx->n1.as<double>();
-        a.n2 = ctx->n2.as<double>();
-        a.cx = ctx->cx.as<double>();
-        a.cy = ctx->cy.as<double>();
-        a.ig_rows = ctx->ig_rows.as<IgRow>();
-        a.alpha = ctx->alpha.as<double>();
-        a.acube = ctx->acube.as<double>();
-        a.flags = ctx->flags.as<uint8_t>();
-        a.u1 = ctx->cu1.as<double>();
-        a.u2 = ctx->cu2.as<double>();
-        a.lor = ctx->clor.as<double>();
-        a.adt = ctx->cadt.as<double>();
-        a.eta = ctx->ceta.as<double>();
-        a.k0 = ctx->ck0.as<double>();
-        a.k3 = ctx->ck3.as<double>();
-        a.ka = ctx->cka.as<double>();
-        a.mom = ctx->mom.as<double>();
-        a.iter_sum = cnt;
-        a.iter_max = reinterpret_cast<unsigned int *>(cnt + 1);
+        const PlainStepArgs a = plain_args(ctx, from);
         launch_step_plain(a, curved, ctx->stream);
     }
     CU(cudaGetLastError());
@@ -1513,6 +1521,261 @@ int grlbm_batch_autotune(grlbm_batch *b, int32_t trial_steps, int32_t *blocks_pe
         *blocks_per_sm = best_bps;
     if (largest_first)
         *largest_first = best_lf;
+    return GRLBM_OK;
+}
+
+} // extern "C"
+
+// ---------------------------------------------------------------- adjoint
+struct grlbm_adjoint
+{
+    std::string err;
+    grlbm_ctx *ctx = nullptr;
+    int every = 20;          // checkpoint interval (steps)
+    int64_t n_steps = 0;     // steps of the last forward
+    int64_t n_entries = 0;   // inverse-table entries
+    DevBuf offsets;          // int64 [nd * nxy + 1]
+    unsigned *srcq = nullptr;
+    float *coef = nullptr;
+    std::vector<std::unique_ptr<DevBuf>> ckpt; // states at steps 0, every, 2 every, ...
+    std::vector<std::unique_ptr<DevBuf>> seg;  // the recomputed outputs of one segment
+    DevBuf clamp, cycles, e0;                  // records of one segment
+    DevBuf lam, lamS, grads, dLdE, mom, counters;
+    ~grlbm_adjoint()
+    {
+        cudaFree(srcq);
+        cudaFree(coef);
+    }
+};
+
+namespace
+{
+int afail(grlbm_adjoint *a, int code, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (a)
+        a->err = buf;
+    else
+        g_create_error = buf;
+    return code;
+}
+#define ACU(call)                                                                                  \
+    do                                                                                             \
+    {                                                                                              \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess)                                                                     \
+            return afail(adj, GRLBM_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));     \
+    } while (0)
+
+bool all_zero(const DevBuf &b, size_t n)
+{
+    std::vector<double> h(n);
+    if (cudaMemcpy(h.data(), b.p, n * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return false;
+    for (double v : h)
+        if (v != 0.0)
+            return false;
+    return true;
+}
+} // namespace
+
+extern "C" {
+
+int grlbm_adjoint_create(grlbm_ctx *ctx, int32_t checkpoint_every, grlbm_adjoint **out)
+{
+    grlbm_adjoint *adj = nullptr;
+    if (!ctx || !out || checkpoint_every < 1)
+        return afail(nullptr, GRLBM_ERR_ARGUMENT, "grlbm_adjoint_create: null context/output or interval < 1");
+    *out = nullptr;
+    if (ctx->fp32)
+        return afail(nullptr, GRLBM_ERR_UNSUPPORTED, "grlbm_adjoint_create: the adjoint follows GRLBM_PLAIN_FP64");
+    const bool curved = ctx->run.streaming_type == GRLBM_CURVED_FIXED;
+    if (curved && !ctx->tables)
+        return afail(nullptr, GRLBM_ERR_STATE, "grlbm_adjoint_create: build the geodesic tables first");
+    if (ctx->run.keep_source_nodes_active && ctx->nsrc > 0)
+        return afail(nullptr, GRLBM_ERR_UNSUPPORTED, "grlbm_adjoint_create: active source nodes are not differentiated");
+    if (ctx->gd.jlo != 1 || ctx->gd.jhi != ctx->geo.ny - 1)
+        return afail(nullptr, GRLBM_ERR_UNSUPPORTED, "grlbm_adjoint_create: the context steps a band of rows only");
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    const int64_t nxy = ctx->gd.nxy, ncell = ctx->gd.ncell;
+    const int nd = ctx->st.n;
+    if (!all_zero(ctx->cu1, nxy) || !all_zero(ctx->cu2, nxy) || !all_zero(ctx->ck3, nxy))
+        return afail(nullptr, GRLBM_ERR_UNSUPPORTED,
+                     "grlbm_adjoint_create: the adjoint needs a fluid at rest without anisotropic scattering "
+                     "(ux = uy = kappa1 = 0)");
+    if ((int64_t)nd * ncell >= (int64_t)1 << 30)
+        return afail(nullptr, GRLBM_ERR_ARGUMENT, "grlbm_adjoint_create: nDir * cells must stay below 2^30");
+    std::unique_ptr<grlbm_adjoint> owner(new grlbm_adjoint);
+    adj = owner.get();
+    adj->ctx = ctx;
+    adj->every = checkpoint_every;
+    if (alloc(nullptr, adj->offsets, (size_t)(nd * nxy + 1) * sizeof(int64_t)))
+        return afail(nullptr, GRLBM_ERR_CUDA, "grlbm_adjoint_create: %s", g_create_error.c_str());
+    AdjEntryArgs ea{};
+    ea.g = ctx->gd;
+    ea.nd = nd;
+    ea.ng = ctx->ng;
+    ea.curved = curved;
+    ea.rec = ctx->rec.as<double4>();
+    ea.ig_rows = ctx->ig_rows.as<IgRow>();
+    ea.alpha = ctx->alpha.as<double>();
+    ea.acube = ctx->acube.as<double>();
+    ea.flags = ctx->flags.as<uint8_t>();
+    ea.cx = ctx->cx.as<double>();
+    ea.cy = ctx->cy.as<double>();
+    cudaError_t e = adj_build_table(ea, adj->offsets.as<int64_t>(), &adj->srcq, &adj->coef, &adj->n_entries,
+                                    ctx->stream);
+    if (e != cudaSuccess)
+        return afail(nullptr, GRLBM_ERR_CUDA, "grlbm_adjoint_create: inverse table: %s", cudaGetErrorString(e));
+    const size_t sb = (size_t)nd * nxy * sizeof(double);
+    adj->seg.resize(checkpoint_every);
+    for (auto &b : adj->seg)
+    {
+        b.reset(new DevBuf);
+        if (alloc(nullptr, *b, sb))
+            return afail(nullptr, GRLBM_ERR_CUDA, "grlbm_adjoint_create: %s", g_create_error.c_str());
+    }
+    if (alloc(nullptr, adj->clamp, (size_t)checkpoint_every * nd * ncell) ||
+        alloc(nullptr, adj->cycles, (size_t)checkpoint_every * ncell * sizeof(int)) ||
+        alloc(nullptr, adj->e0, (size_t)checkpoint_every * ncell * sizeof(double)) ||
+        alloc(nullptr, adj->lam, (size_t)nd * nxy * sizeof(float)) ||
+        alloc(nullptr, adj->lamS, (size_t)nd * ncell * sizeof(float)) ||
+        alloc(nullptr, adj->grads, (size_t)3 * nxy * sizeof(double)) ||
+        alloc(nullptr, adj->dLdE, (size_t)nxy * sizeof(double)) ||
+        alloc(nullptr, adj->mom, (size_t)6 * nxy * sizeof(double)) ||
+        alloc(nullptr, adj->counters, 8 * sizeof(unsigned long long)))
+        return afail(nullptr, GRLBM_ERR_CUDA, "grlbm_adjoint_create: %s", g_create_error.c_str());
+    *out = owner.release();
+    return GRLBM_OK;
+}
+
+void grlbm_adjoint_destroy(grlbm_adjoint *adj)
+{
+    if (adj)
+    {
+        cudaSetDevice(adj->ctx->device);
+        cudaStreamSynchronize(adj->ctx->stream);
+        delete adj;
+    }
+}
+
+const char *grlbm_adjoint_last_error(const grlbm_adjoint *adj)
+{
+    return adj ? adj->err.c_str() : g_create_error.c_str();
+}
+
+int grlbm_adjoint_forward(grlbm_adjoint *adj, int32_t n_steps)
+{
+    if (!adj)
+        return GRLBM_ERR_ARGUMENT;
+    if (n_steps < 1)
+        return afail(adj, GRLBM_ERR_ARGUMENT, "n_steps must be positive");
+    grlbm_ctx *ctx = adj->ctx;
+    cudaSetDevice(ctx->device);
+    const size_t sb = (size_t)ctx->st.n * ctx->gd.nxy * sizeof(double);
+    const int n_ckpt = (n_steps + adj->every - 1) / adj->every;
+    while ((int)adj->ckpt.size() < n_ckpt)
+    {
+        adj->ckpt.emplace_back(new DevBuf);
+        if (alloc(nullptr, *adj->ckpt.back(), sb))
+            return afail(adj, GRLBM_ERR_CUDA, "checkpoint: %s", g_create_error.c_str());
+    }
+    // nodes the step never writes (halo, excision) keep the initial values in
+    // every state: the recompute buffers start from the initial state
+    for (auto &b : adj->seg)
+        ACU(cudaMemcpyAsync(b->p, ctx->I[ctx->cur].p, sb, cudaMemcpyDeviceToDevice, ctx->stream));
+    int rc;
+    for (int k = 0; k < n_ckpt; k++)
+    {
+        ACU(cudaMemcpyAsync(adj->ckpt[k]->p, ctx->I[ctx->cur].p, sb, cudaMemcpyDeviceToDevice, ctx->stream));
+        const int len = std::min(adj->every, n_steps - k * adj->every);
+        if ((rc = grlbm_step_async(ctx, len)))
+            return afail(adj, rc, "forward: %s", ctx->err.c_str());
+    }
+    ACU(cudaStreamSynchronize(ctx->stream));
+    adj->n_steps = n_steps;
+    return GRLBM_OK;
+}
+
+int grlbm_adjoint_backward(grlbm_adjoint *adj, const double *dL_dE, double *g_eta, double *g_kappaA,
+                           double *g_kappa0)
+{
+    if (!adj)
+        return GRLBM_ERR_ARGUMENT;
+    if (!dL_dE)
+        return afail(adj, GRLBM_ERR_ARGUMENT, "null dL/dE");
+    if (adj->n_steps < 1)
+        return afail(adj, GRLBM_ERR_STATE, "run grlbm_adjoint_forward first");
+    grlbm_ctx *ctx = adj->ctx;
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->stream;
+    const bool curved = ctx->run.streaming_type == GRLBM_CURVED_FIXED;
+    const int64_t nxy = ctx->gd.nxy, ncell = ctx->gd.ncell;
+    const int nd = ctx->st.n;
+    ACU(cudaMemcpyAsync(adj->dLdE.p, dL_dE, nxy * sizeof(double), cudaMemcpyHostToDevice, s));
+    ACU(cudaMemsetAsync(adj->grads.p, 0, adj->grads.bytes, s));
+    launch_adj_seed(ctx->gd, nd, ctx->w.as<double>(), ctx->flags.as<uint8_t>(), adj->dLdE.as<double>(),
+                    adj->lam.as<float>(), s);
+    double *g = adj->grads.as<double>();
+    const int n_seg = (int)((adj->n_steps + adj->every - 1) / adj->every);
+    for (int k = n_seg - 1; k >= 0; k--)
+    {
+        const int len = (int)std::min<int64_t>(adj->every, adj->n_steps - (int64_t)k * adj->every);
+        // recompute the segment, recording clamps, cycles and first iterates
+        const double *in = adj->ckpt[k]->as<double>();
+        for (int jj = 0; jj < len; jj++)
+        {
+            PlainStepArgs a = plain_args(ctx, 0);
+            a.Iin = in;
+            a.Iout = adj->seg[jj]->as<double>();
+            a.mom = adj->mom.as<double>();
+            a.iter_sum = adj->counters.as<unsigned long long>();
+            a.iter_max = reinterpret_cast<unsigned int *>(adj->counters.as<unsigned long long>() + 1);
+            StepRecord rec{};
+            rec.clamp = adj->clamp.as<uint8_t>() + (size_t)jj * nd * ncell;
+            rec.cycles = adj->cycles.as<int>() + (size_t)jj * ncell;
+            rec.e0 = adj->e0.as<double>() + (size_t)jj * ncell;
+            launch_step_plain(a, curved, s, &rec);
+            in = a.Iout;
+        }
+        ACU(cudaGetLastError());
+        // adjoint steps of the segment, last first
+        for (int jj = len - 1; jj >= 0; jj--)
+        {
+            AdjCollideArgs c{};
+            c.g = ctx->gd;
+            c.nd = nd;
+            c.w = ctx->w.as<double>();
+            c.flags = ctx->flags.as<uint8_t>();
+            c.adt = ctx->cadt.as<double>();
+            c.eta = ctx->ceta.as<double>();
+            c.k0 = ctx->ck0.as<double>();
+            c.ka = ctx->cka.as<double>();
+            c.lam = adj->lam.as<float>();
+            c.Iout = adj->seg[jj]->as<double>();
+            c.cycles = adj->cycles.as<int>() + (size_t)jj * ncell;
+            c.e0 = adj->e0.as<double>() + (size_t)jj * ncell;
+            c.lamS = adj->lamS.as<float>();
+            c.g_eta = g;
+            c.g_ka = g + nxy;
+            c.g_k0 = g + 2 * nxy;
+            launch_adj_collide(c, s);
+            launch_adj_stream(adj->offsets.as<int64_t>(), adj->srcq, adj->coef,
+                              curved ? adj->clamp.as<uint8_t>() + (size_t)jj * nd * ncell : nullptr,
+                              adj->lamS.as<float>(), (int64_t)nd * nxy, adj->lam.as<float>(), s);
+        }
+        ACU(cudaGetLastError());
+    }
+    double *outs[3] = {g_eta, g_kappaA, g_kappa0};
+    for (int q = 0; q < 3; q++)
+        if (outs[q])
+            ACU(cudaMemcpyAsync(outs[q], g + q * nxy, nxy * sizeof(double), cudaMemcpyDeviceToHost, s));
+    ACU(cudaStreamSynchronize(s));
     return GRLBM_OK;
 }
 

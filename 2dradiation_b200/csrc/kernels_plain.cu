@@ -21,10 +21,13 @@ namespace
 {
 // one stream value: StreamFlatFixed (src/Radiation.cpp:394-410) or
 // StreamCurvedFixed with IntensityAt (:478-508, 322-343)
+// `clamp_mask` receives bit q set where corner q's angular interpolation was
+// positive (kept by the clamp at zero); flat streaming keeps every corner.
 template <bool CURVED>
 __device__ __forceinline__ double stream_value(const PlainStepArgs &a, int d, const double4 &r, int64_t i, int64_t j,
-                                               int64_t ij)
+                                               int64_t ij, unsigned &clamp_mask)
 {
+    clamp_mask = 0xFu;
     const int64_t nxy = a.g.nxy, nx = a.g.nx;
     if constexpr (CURVED)
     {
@@ -58,6 +61,8 @@ __device__ __forceinline__ double stream_value(const PlainStepArgs &a, int d, co
                 v1 += w1[k] * __ldg(a.Iin + (int64_t)idx1[k] * nxy + n);
             }
             double v = v0 * (1.0 - t) + v1 * t;
+            if (!(0.0 < v))
+                clamp_mask &= ~(1u << q);
             v = (0.0 < v) ? v : 0.0;
             const int64_t di = ci - i, dj = cj - j;
             double cube;
@@ -153,8 +158,11 @@ __device__ __forceinline__ double div_rn(double num, double den, double r)
     return __fma_rn(__fma_rn(-q, den, num), r, q);
 }
 
-template <bool CURVED>
-__global__ void __launch_bounds__(kStepBlock, GRLBM_PLAIN_MIN_BLOCKS) k_step_plain(PlainStepArgs a)
+// RECORD: also writes what the adjoint needs about this step -- per (d, c)
+// the corner clamp mask, per cell the lambda-iteration count and the first
+// iterate's E -- without changing any result.
+template <bool CURVED, bool RECORD>
+__global__ void __launch_bounds__(kStepBlock, GRLBM_PLAIN_MIN_BLOCKS) k_step_plain(PlainStepArgs a, StepRecord rec)
 {
     const int t = threadIdx.x;
     // cells of the slab rows [jlo, jhi), numbered from its first cell
@@ -186,7 +194,10 @@ __global__ void __launch_bounds__(kStepBlock, GRLBM_PLAIN_MIN_BLOCKS) k_step_pla
         double4 r1 = r0;
         if (CURVED)
             r1 = rp[(int64_t)min(d + 1, a.nd - 1) * a.g.ncell];
-        const double val = (active && !zero_stream) ? stream_value<CURVED>(a, d, r0, i, j, ij) : 0.0;
+        unsigned cm = 0xFu;
+        const double val = (active && !zero_stream) ? stream_value<CURVED>(a, d, r0, i, j, ij, cm) : 0.0;
+        if (RECORD && active)
+            rec.clamp[(int64_t)d * a.g.ncell + cc] = (uint8_t)cm;
         if (collides)
             Is[(int64_t)d * nxy] = val;
         m.add(__ldg(a.w + d), val, __ldg(a.n1 + d), __ldg(a.n2 + d));
@@ -194,6 +205,8 @@ __global__ void __launch_bounds__(kStepBlock, GRLBM_PLAIN_MIN_BLOCKS) k_step_pla
     }
 
     int cycles = 0;
+    if (RECORD && active)
+        rec.e0[cc] = m.E;
     if (collides)
     {
         const double u1 = a.u1[ij], u2 = a.u2[ij], lor = a.lor[ij], adt = a.adt[ij];
@@ -261,6 +274,8 @@ __global__ void __launch_bounds__(kStepBlock, GRLBM_PLAIN_MIN_BLOCKS) k_step_pla
                 Is[(int64_t)d * nxy] = collide_value(Is[(int64_t)d * nxy], __ldg(a.n1 + d), __ldg(a.n2 + d), u1, u2,
                                                      lor, adt, eta, k0, k3, kak0, fE, fFx, fFy);
     }
+    if (RECORD && active)
+        rec.cycles[cc] = cycles;
     if (active)
     {
         a.mom[ij] = m.E;
@@ -447,21 +462,28 @@ inline unsigned nblk(int64_t n, int b) { return (unsigned)((n + b - 1) / b); }
 
 cudaError_t prepare_step_plain(int smem_bytes)
 {
-    cudaError_t e = cudaFuncSetAttribute(k_step_plain<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
-    if (e != cudaSuccess)
-        return e;
-    return cudaFuncSetAttribute(k_step_plain<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
+    (void)smem_bytes; // the plain step uses no dynamic shared memory
+    return cudaSuccess;
 }
-void launch_step_plain(const PlainStepArgs &a, bool curved, cudaStream_t s)
+void launch_step_plain(const PlainStepArgs &a, bool curved, cudaStream_t s, const StepRecord *record)
 {
     const size_t smem = 0;
     const int64_t cells = (a.g.jhi - a.g.jlo) * a.g.nx_;
     if (cells <= 0)
         return;
-    if (curved)
-        k_step_plain<true><<<nblk(cells, kStepBlock), kStepBlock, smem, s>>>(a);
+    const StepRecord none{};
+    const unsigned blocks = nblk(cells, kStepBlock);
+    if (record)
+    {
+        if (curved)
+            k_step_plain<true, true><<<blocks, kStepBlock, smem, s>>>(a, *record);
+        else
+            k_step_plain<false, true><<<blocks, kStepBlock, smem, s>>>(a, *record);
+    }
+    else if (curved)
+        k_step_plain<true, false><<<blocks, kStepBlock, smem, s>>>(a, none);
     else
-        k_step_plain<false><<<nblk(cells, kStepBlock), kStepBlock, smem, s>>>(a);
+        k_step_plain<false, false><<<blocks, kStepBlock, smem, s>>>(a, none);
 }
 void launch_sources64(double *I, int64_t nxy, int nd, const int64_t *nodes, const double *vals, int64_t nsrc,
                       cudaStream_t s)

@@ -203,6 +203,30 @@ def batch_instances(count=64, seed=10, sizes=(64, 128, 256, 512), dirs=(16, 32, 
     return out
 
 
+def gaussian_field(X, Y, seed, count=8, width=1.0, box=5.0):
+    """Sum of `count` Gaussians of the given width with amplitudes U[0, 1) and
+    centres U[-box, box)^2."""
+    u = uniform(seed, 3 * count).reshape(count, 3)
+    f = np.zeros_like(X)
+    for a, cx, cy in u:
+        f += a * np.exp(-((X - (2 * cx - 1) * box) ** 2 + (Y - (2 * cy - 1) * box) ** 2) / (2 * width * width))
+    return f
+
+
+def adjoint_case(nx_=256, ny_=256, n_dir=48, n_fourier=5, steps=200, seeds=(5, 6), rk_tol=1e-10):
+    """Fields of the adjoint workload: Schwarzschild M = 1 (Kerr-Schild
+    coordinates, excision r <= 2.4) on [-6,6]^2, eta and kappaA each a sum of
+    8 Gaussians of width 1 (seeds[0], seeds[1]), no scattering, fluid at rest,
+    intensities starting at zero.  The target of the loss comes from the same
+    problem with seeds (7, 8)."""
+    c = _base("adjoint", nx_, ny_, (-6, -6), (6, 6), n_dir, n_fourier, steps, KERRSCHILD, CURVED_FIXED,
+              excision=2.4, rk_tol=rk_tol)
+    X, Y, _, _ = grid_coords(nx_, ny_, (-6, -6), (6, 6))
+    c["fields"]["eta"][:] = gaussian_field(X, Y, seeds[0])
+    c["fields"]["kappaA"][:] = gaussian_field(X, Y, seeds[1])
+    return c
+
+
 def make_case(name: str, **overrides) -> dict:
     return WORKLOADS[name](**overrides)
 

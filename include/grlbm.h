@@ -253,6 +253,29 @@ int grlbm_batch_step(grlbm_batch *batch, int32_t n_steps);
  * every problem back in the state it had before the call.  The choice is
  * returned in *blocks_per_sm and *largest_first (either may be NULL). */
 int grlbm_batch_autotune(grlbm_batch *batch, int32_t trial_steps, int32_t *blocks_per_sm, int32_t *largest_first);
+/* ---- adjoint ------------------------------------------------------------------
+ * No counterpart in the reference.  Gradients of a loss of the final
+ * inertial-frame E with respect to the emissivity, absorption and scattering
+ * fields, by a hand-written adjoint of the plain step (GRLBM_PLAIN_FP64) for a
+ * fluid at rest without anisotropic scattering (ux = uy = kappa1 = 0; other
+ * fields give GRLBM_ERR_UNSUPPORTED).  The stream is transposed through an
+ * inverse (CSR) table of its gather built on the device; the adjoint state is
+ * FP32 and the gradients accumulate in FP64.  The forward keeps the state
+ * every checkpoint_every steps and the backward recomputes each segment. */
+typedef struct grlbm_adjoint grlbm_adjoint;
+/* After the context's fields and geodesic tables are set; the context must
+ * step all interior rows. */
+int grlbm_adjoint_create(grlbm_ctx *ctx, int32_t checkpoint_every, grlbm_adjoint **out);
+void grlbm_adjoint_destroy(grlbm_adjoint *adj);
+const char *grlbm_adjoint_last_error(const grlbm_adjoint *adj);
+/* n_steps plain steps of the context from its current intensities, with
+ * checkpoints; the context then holds the final state as after grlbm_step. */
+int grlbm_adjoint_forward(grlbm_adjoint *adj, int32_t n_steps);
+/* dL_dE: dL/dE of the final inertial-frame E (host, nx*ny; only interior
+ * nodes matter).  Writes dL/deta, dL/dkappaA, dL/dkappa0 (host, nx*ny each,
+ * any may be NULL) for the last forward, with the fields as they were then. */
+int grlbm_adjoint_backward(grlbm_adjoint *adj, const double *dL_dE, double *g_eta, double *g_kappaA,
+                           double *g_kappa0);
 /* Lambda-iteration and table-build statistics (src/Radiation.cpp:723-733,
  * 855-857). */
 int grlbm_get_stats(grlbm_ctx *ctx, grlbm_stats *stats);
