@@ -17,8 +17,12 @@
 // list of (source (d, c), corner q, weight) whose stream reads I[d'](n).
 // The table is built once per set of geodesic tables: every (d, c) writes its
 // up to 32 entries at fixed slots, a stable radix sort on (target, source)
-// orders them, and a binary search per target gives the row offsets -- the
-// order, and so every sum, is deterministic.
+// orders them, entries of the same (target, source, corner) -- the two
+// interpolation rows reading one direction -- are merged, and a binary search
+// per target gives the row lengths: the order, and so every sum, is
+// deterministic.  The rows are stored sliced (32 targets per slice, each
+// slice as wide as its longest row, entry k of the slice's rows contiguous),
+// so that the 32 threads of a warp read consecutive words.
 //
 // Adjoint state and table weights are FP32; the gradients accumulate in FP64.
 #include <cub/cub.cuh>
@@ -131,11 +135,35 @@ __global__ void k_adj_offsets(const unsigned long long *keys, int64_t n, int64_t
     offsets[t] = lo;
 }
 
-__global__ void k_adj_compact(const unsigned long long *keys, int64_t n, unsigned *srcq)
+// slice widths: the longest row of each slice of kSlice targets
+constexpr int kSlice = 32;
+__global__ void k_adj_slice_width(const int64_t *offsets, int64_t n_targets, int64_t n_slices, int64_t *width)
 {
-    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e < n)
-        srcq[e] = (unsigned)(keys[e] & 0xffffffffull);
+    const int64_t sl = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (sl >= n_slices)
+        return;
+    int64_t w = 0;
+    for (int64_t t = sl * kSlice; t < min((sl + 1) * kSlice, n_targets); t++)
+        w = max(w, offsets[t + 1] - offsets[t]);
+    width[sl] = w * kSlice;
+}
+
+// rows into the sliced layout, short rows padded with weight 0
+__global__ void k_adj_slice_fill(const int64_t *offsets, const unsigned long long *keys, const float *vals,
+                                 const int64_t *slice_start, int64_t n_targets, unsigned *srcq, float *coef)
+{
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_targets)
+        return;
+    const int64_t sl = t / kSlice, lane = t % kSlice;
+    const int64_t base = slice_start[sl], width = (slice_start[sl + 1] - base) / kSlice;
+    const int64_t e0 = offsets[t], cnt = offsets[t + 1] - e0;
+    for (int64_t k = 0; k < width; k++)
+    {
+        const int64_t dst = base + k * kSlice + lane;
+        srcq[dst] = k < cnt ? (unsigned)(keys[e0 + k] & 0xffffffffull) : 0u;
+        coef[dst] = k < cnt ? vals[e0 + k] : 0.f;
+    }
 }
 
 // adjoint of the final moments E: lambda_I[d](ij) = w_d dL/dE(ij) at colliding cells
@@ -207,23 +235,26 @@ __global__ void __launch_bounds__(128) k_adj_collide(AdjCollideArgs a)
 }
 
 // Stream adjoint: lambda[d'](n) = sum over the inverse-table row of (d', n)
-// of weight * (corner kept by the clamp) * lambda_S(source).
-__global__ void __launch_bounds__(256) k_adj_stream(const int64_t *offsets, const unsigned *srcq, const float *coef,
-                                                    const uint8_t *clamp, const float *lamS, int64_t n_targets,
-                                                    float *lam)
+// of weight * (corner kept by the clamp) * lambda_S(source), rows read from
+// the sliced layout.
+__global__ void __launch_bounds__(256) k_adj_stream(const int64_t *slice_start, const unsigned *srcq,
+                                                    const float *coef, const uint8_t *clamp, const float *lamS,
+                                                    int64_t n_targets, float *lam)
 {
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n_targets)
         return;
+    const int64_t sl = t / kSlice;
+    const int64_t e1 = slice_start[sl + 1];
     float acc = 0.f;
-    const int64_t e1 = offsets[t + 1];
-    for (int64_t e = offsets[t]; e < e1; e++)
+    for (int64_t e = slice_start[sl] + t % kSlice; e < e1; e += kSlice)
     {
-        const unsigned sq = srcq[e];
+        const unsigned sq = __ldcs(srcq + e);
+        const float w = __ldcs(coef + e);
         const unsigned src = sq >> 2;
         const bool kept = clamp ? ((clamp[src] >> (sq & 3u)) & 1u) : true;
         if (kept)
-            acc = fmaf(coef[e], lamS[src], acc);
+            acc = fmaf(w, lamS[src], acc);
     }
     lam[t] = acc;
 }
@@ -233,17 +264,19 @@ inline unsigned nblk(int64_t n, int b) { return (unsigned)((n + b - 1) / b); }
 
 int64_t adj_entries_per_source(bool curved) { return curved ? kEntriesCurved : kEntriesFlat; }
 
-cudaError_t adj_build_table(const AdjEntryArgs &a, int64_t *offsets, unsigned **srcq_out, float **coef_out,
+cudaError_t adj_build_table(const AdjEntryArgs &a, int64_t *slice_start, unsigned **srcq_out, float **coef_out,
                             int64_t *n_entries_out, cudaStream_t s)
 {
     const int64_t n_src = (int64_t)a.nd * a.g.ncell;
     const int64_t n = n_src * adj_entries_per_source(a.curved);
     const int64_t n_targets = (int64_t)a.nd * a.g.nxy;
-    unsigned long long *k0 = nullptr, *k1 = nullptr;
-    float *v0 = nullptr, *v1 = nullptr;
+    const int64_t n_slices = (n_targets + kSlice - 1) / kSlice;
+    unsigned long long *k0 = nullptr, *k1 = nullptr, *uk = nullptr;
+    float *v0 = nullptr, *v1 = nullptr, *uv = nullptr;
+    int64_t *offsets = nullptr, *n_unique_d = nullptr, *widths = nullptr;
     void *tmp = nullptr;
-    size_t tmp_bytes = 0;
-    int64_t n_valid = 0;
+    size_t tmp_bytes = 0, tmp2 = 0;
+    int64_t n_unique = 0, total = 0;
     cudaError_t e = cudaSuccess;
     *srcq_out = nullptr;
     *coef_out = nullptr;
@@ -259,27 +292,52 @@ cudaError_t adj_build_table(const AdjEntryArgs &a, int64_t *offsets, unsigned **
     ADJ_TRY(cudaMallocAsync(&k1, n * sizeof(unsigned long long), s));
     ADJ_TRY(cudaMallocAsync(&v0, n * sizeof(float), s));
     ADJ_TRY(cudaMallocAsync(&v1, n * sizeof(float), s));
+    ADJ_TRY(cudaMallocAsync(&offsets, (n_targets + 1) * sizeof(int64_t), s));
+    ADJ_TRY(cudaMallocAsync(&n_unique_d, sizeof(int64_t), s));
+    ADJ_TRY(cudaMallocAsync(&widths, (n_slices + 1) * sizeof(int64_t), s));
     k_adj_entries<<<nblk(n_src, 128), 128, 0, s>>>(a, k0, v0);
     ADJ_TRY(cudaGetLastError());
     kb = cub::DoubleBuffer<unsigned long long>(k0, k1);
     vb = cub::DoubleBuffer<float>(v0, v1);
     ADJ_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, kb, vb, n, 0, 64, s));
-    ADJ_TRY(cudaMallocAsync(&tmp, tmp_bytes, s));
+    // merge equal keys (the same target, source and corner) into the other buffers
+    uk = kb.Alternate();
+    uv = vb.Alternate();
+    ADJ_TRY(cub::DeviceReduce::ReduceByKey(nullptr, tmp2, kb.Current(), uk, vb.Current(), uv, n_unique_d,
+                                           cub::Sum(), n, s));
+    ADJ_TRY(cudaMallocAsync(&tmp, std::max(tmp_bytes, tmp2), s));
     ADJ_TRY(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, kb, vb, n, 0, 64, s));
-    k_adj_offsets<<<nblk(n_targets + 1, 256), 256, 0, s>>>(kb.Current(), n, n_targets, offsets);
-    ADJ_TRY(cudaGetLastError());
-    ADJ_TRY(cudaMemcpyAsync(&n_valid, offsets + n_targets, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    uk = kb.Alternate();
+    uv = vb.Alternate();
+    ADJ_TRY(cub::DeviceReduce::ReduceByKey(tmp, tmp2, kb.Current(), uk, vb.Current(), uv, n_unique_d, cub::Sum(), n,
+                                           s));
+    ADJ_TRY(cudaMemcpyAsync(&n_unique, n_unique_d, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     ADJ_TRY(cudaStreamSynchronize(s));
-    *n_entries_out = n_valid;
-    ADJ_TRY(cudaMalloc(srcq_out, (size_t)std::max<int64_t>(n_valid, 1) * sizeof(unsigned)));
-    ADJ_TRY(cudaMalloc(coef_out, (size_t)std::max<int64_t>(n_valid, 1) * sizeof(float)));
-    if (n_valid > 0)
+    // rows (the run of invalid keys, if any, sorts last and is excluded)
+    k_adj_offsets<<<nblk(n_targets + 1, 256), 256, 0, s>>>(uk, n_unique, n_targets, offsets);
+    ADJ_TRY(cudaGetLastError());
+    k_adj_slice_width<<<nblk(n_slices, 256), 256, 0, s>>>(offsets, n_targets, n_slices, widths);
+    ADJ_TRY(cudaGetLastError());
+    ADJ_TRY(cudaMemsetAsync(widths + n_slices, 0, sizeof(int64_t), s));
     {
-        k_adj_compact<<<nblk(n_valid, 256), 256, 0, s>>>(kb.Current(), n_valid, *srcq_out);
-        ADJ_TRY(cudaGetLastError());
-        ADJ_TRY(cudaMemcpyAsync(*coef_out, vb.Current(), (size_t)n_valid * sizeof(float), cudaMemcpyDeviceToDevice,
-                                s));
+        size_t tmp3 = 0;
+        ADJ_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tmp3, widths, slice_start, n_slices + 1, s));
+        if (tmp3 > std::max(tmp_bytes, tmp2))
+        {
+            cudaFreeAsync(tmp, s);
+            tmp = nullptr;
+            ADJ_TRY(cudaMallocAsync(&tmp, tmp3, s));
+        }
+        ADJ_TRY(cub::DeviceScan::ExclusiveSum(tmp, tmp3, widths, slice_start, n_slices + 1, s));
     }
+    ADJ_TRY(cudaMemcpyAsync(&total, slice_start + n_slices, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    ADJ_TRY(cudaStreamSynchronize(s));
+    *n_entries_out = total;
+    ADJ_TRY(cudaMalloc(srcq_out, (size_t)std::max<int64_t>(total, 1) * sizeof(unsigned)));
+    ADJ_TRY(cudaMalloc(coef_out, (size_t)std::max<int64_t>(total, 1) * sizeof(float)));
+    k_adj_slice_fill<<<nblk(n_targets, 256), 256, 0, s>>>(offsets, uk, uv, slice_start, n_targets, *srcq_out,
+                                                          *coef_out);
+    ADJ_TRY(cudaGetLastError());
     ADJ_TRY(cudaStreamSynchronize(s));
 done:
 #undef ADJ_TRY
@@ -287,6 +345,9 @@ done:
     cudaFreeAsync(k1, s);
     cudaFreeAsync(v0, s);
     cudaFreeAsync(v1, s);
+    cudaFreeAsync(offsets, s);
+    cudaFreeAsync(n_unique_d, s);
+    cudaFreeAsync(widths, s);
     if (tmp)
         cudaFreeAsync(tmp, s);
     cudaStreamSynchronize(s);
@@ -300,6 +361,8 @@ done:
     return e;
 }
 
+int64_t adj_slices(int64_t n_targets) { return (n_targets + kSlice - 1) / kSlice; }
+
 void launch_adj_seed(const GridDev &g, int nd, const double *w, const uint8_t *flags, const double *dLdE, float *lam,
                      cudaStream_t s)
 {
@@ -309,9 +372,9 @@ void launch_adj_collide(const AdjCollideArgs &a, cudaStream_t s)
 {
     k_adj_collide<<<nblk(a.g.ncell, 128), 128, 0, s>>>(a);
 }
-void launch_adj_stream(const int64_t *offsets, const unsigned *srcq, const float *coef, const uint8_t *clamp,
+void launch_adj_stream(const int64_t *slice_start, const unsigned *srcq, const float *coef, const uint8_t *clamp,
                        const float *lamS, int64_t n_targets, float *lam, cudaStream_t s)
 {
-    k_adj_stream<<<nblk(n_targets, 256), 256, 0, s>>>(offsets, srcq, coef, clamp, lamS, n_targets, lam);
+    k_adj_stream<<<nblk(n_targets, 256), 256, 0, s>>>(slice_start, srcq, coef, clamp, lamS, n_targets, lam);
 }
 } // namespace grlbm

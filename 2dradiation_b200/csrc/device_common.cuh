@@ -250,12 +250,14 @@ struct BatchItem
 };
 
 int64_t adj_entries_per_source(bool curved);
-cudaError_t adj_build_table(const AdjEntryArgs &a, int64_t *offsets, unsigned **srcq, float **coef,
+// slice_start: adj_slices(nd * nxy) + 1 entries
+int64_t adj_slices(int64_t n_targets);
+cudaError_t adj_build_table(const AdjEntryArgs &a, int64_t *slice_start, unsigned **srcq, float **coef,
                             int64_t *n_entries, cudaStream_t s);
 void launch_adj_seed(const GridDev &g, int nd, const double *w, const uint8_t *flags, const double *dLdE, float *lam,
                      cudaStream_t s);
 void launch_adj_collide(const AdjCollideArgs &a, cudaStream_t s);
-void launch_adj_stream(const int64_t *offsets, const unsigned *srcq, const float *coef, const uint8_t *clamp,
+void launch_adj_stream(const int64_t *slice_start, const unsigned *srcq, const float *coef, const uint8_t *clamp,
                        const float *lamS, int64_t n_targets, float *lam, cudaStream_t s);
 
 // Records a message for grlbm_last_error(NULL) (defined in grlbm_capi.cu).

@@ -1534,7 +1534,7 @@ struct grlbm_adjoint
     int every = 20;          // checkpoint interval (steps)
     int64_t n_steps = 0;     // steps of the last forward
     int64_t n_entries = 0;   // inverse-table entries
-    DevBuf offsets;          // int64 [nd * nxy + 1]
+    DevBuf slices;           // int64: first entry of each slice of the sliced inverse table, and the end
     unsigned *srcq = nullptr;
     float *coef = nullptr;
     std::vector<std::unique_ptr<DevBuf>> ckpt; // states at steps 0, every, 2 every, ...
@@ -1614,7 +1614,7 @@ int grlbm_adjoint_create(grlbm_ctx *ctx, int32_t checkpoint_every, grlbm_adjoint
     adj = owner.get();
     adj->ctx = ctx;
     adj->every = checkpoint_every;
-    if (alloc(nullptr, adj->offsets, (size_t)(nd * nxy + 1) * sizeof(int64_t)))
+    if (alloc(nullptr, adj->slices, (size_t)(adj_slices((int64_t)nd * nxy) + 1) * sizeof(int64_t)))
         return afail(nullptr, GRLBM_ERR_CUDA, "grlbm_adjoint_create: %s", g_create_error.c_str());
     AdjEntryArgs ea{};
     ea.g = ctx->gd;
@@ -1628,7 +1628,7 @@ int grlbm_adjoint_create(grlbm_ctx *ctx, int32_t checkpoint_every, grlbm_adjoint
     ea.flags = ctx->flags.as<uint8_t>();
     ea.cx = ctx->cx.as<double>();
     ea.cy = ctx->cy.as<double>();
-    cudaError_t e = adj_build_table(ea, adj->offsets.as<int64_t>(), &adj->srcq, &adj->coef, &adj->n_entries,
+    cudaError_t e = adj_build_table(ea, adj->slices.as<int64_t>(), &adj->srcq, &adj->coef, &adj->n_entries,
                                     ctx->stream);
     if (e != cudaSuccess)
         return afail(nullptr, GRLBM_ERR_CUDA, "grlbm_adjoint_create: inverse table: %s", cudaGetErrorString(e));
@@ -1765,7 +1765,7 @@ int grlbm_adjoint_backward(grlbm_adjoint *adj, const double *dL_dE, double *g_et
             c.g_ka = g + nxy;
             c.g_k0 = g + 2 * nxy;
             launch_adj_collide(c, s);
-            launch_adj_stream(adj->offsets.as<int64_t>(), adj->srcq, adj->coef,
+            launch_adj_stream(adj->slices.as<int64_t>(), adj->srcq, adj->coef,
                               curved ? adj->clamp.as<uint8_t>() + (size_t)jj * nd * ncell : nullptr,
                               adj->lamS.as<float>(), (int64_t)nd * nxy, adj->lam.as<float>(), s);
         }

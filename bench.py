@@ -67,6 +67,8 @@ def args_parse():
     p.add_argument("--nx", type=int, default=400)
     p.add_argument("--dirs", type=int, default=64)
     p.add_argument("--fourier", type=int, default=16)
+    p.add_argument("--adjoint-steps", type=int, default=200,
+                   help="steps of the adjoint workload (256^2 x 48, checkpoints every 20); 0 skips it")
     p.add_argument("--batch-steps", type=int, default=64,
                    help="timed steps of the batched form (64 uneven problems); 0 skips it")
     return p.parse_args()
@@ -256,6 +258,57 @@ def run_batched(G, W, a, local):
             "timing": "host clock around the synchronous batch step (persistent launch per step, 32-step graphs)"}
 
 
+def run_adjoint(G, W, a, local):
+    """The adjoint workload (Schwarzschild 256^2 x 48 directions, Gaussian-sum
+    eta and kappaA, `adjoint_steps` steps, checkpoints every 20): the plain
+    forward alone, the checkpointed forward, and the backward (recompute +
+    adjoint), each timed on the host around synchronous calls."""
+    import torch
+    case = W.adjoint_case(steps=a.adjoint_steps)
+    target = W.adjoint_case(steps=a.adjoint_steps, seeds=(7, 8))
+    n = a.adjoint_steps
+    with G.prepare(target, G.PLAIN_FP64, device=local) as t:
+        t.step(n)
+        Et = t.moments_if()["E"]
+    r = G.prepare(case, G.PLAIN_FP64, device=local)
+    try:
+        I0 = np.zeros(r.nxy * r.nd)
+        t0 = time.perf_counter()
+        adj = G.Adjoint(r, 20)
+        table_s = time.perf_counter() - t0
+        r.set_intensity(I0)
+        r.step(n)
+        r.set_intensity(I0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r.step(n)
+        plain_s = time.perf_counter() - t0
+        r.set_intensity(I0)
+        t0 = time.perf_counter()
+        adj.forward(n)
+        fwd_s = time.perf_counter() - t0
+        E = r.moments_if()["E"]
+        nx = r.nx
+        mask = np.zeros((r.ny, nx), bool)
+        mask[1:-1, 1:-1] = True
+        dLdE = np.where(mask.ravel(), E - Et, 0.0)
+        t0 = time.perf_counter()
+        g = adj.backward(dLdE)
+        bwd_s = time.perf_counter() - t0
+        adj.close()
+    finally:
+        r.close()
+    return {"workload": "adjoint: Schwarzschild 256x256 x 48 directions, eta/kappaA sums of 8 Gaussians, "
+                        f"{n} steps, checkpoints every 20, loss 0.5|E - E*|^2",
+            "loss": 0.5 * float(np.sum(dLdE ** 2)),
+            "inverse_table_s": table_s, "plain_forward_ms_per_step": 1e3 * plain_s / n,
+            "checkpointed_forward_ms_per_step": 1e3 * fwd_s / n,
+            "backward_ms_per_step": 1e3 * bwd_s / n,
+            "adjoint_step_over_forward_step": bwd_s / plain_s,
+            "grad_norms": {k: float(np.linalg.norm(v)) for k, v in g.items()},
+            "timing": "host clock around synchronous calls; the backward includes the forward recompute"}
+
+
 def run_grlbm(a, world, rank, local, pg):
     import torch
     G = importlib.import_module("2dradiation_b200")
@@ -311,6 +364,7 @@ def run_grlbm(a, world, rank, local, pg):
             r.close()
         e2e_s = max_over_ranks(statistics.median(e2e_t) if e2e_t else float("nan"), pg, dev)
         batched = run_batched(G, W, a, local) if a.batch_steps > 0 and world == 1 else None
+        adjoint = run_adjoint(G, W, a, local) if a.adjoint_steps > 0 and world == 1 else None
     clocks = clk.summary()
 
     fp32, fp64 = forms["fp32"], forms["fp64"]
@@ -385,6 +439,7 @@ def run_grlbm(a, world, rank, local, pg):
         },
         "gpu_launches": a.steps,
         "batched": batched,
+        "adjoint": adjoint,
         "clocks": clocks,
     }
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
