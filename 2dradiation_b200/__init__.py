@@ -94,6 +94,11 @@ SIGNATURES = {
     "grlbm_adjoint_last_error": ([C.c_void_p], C.c_char_p),
     "grlbm_adjoint_forward": ([C.c_void_p, C.c_int32], C.c_int),
     "grlbm_adjoint_backward": ([C.c_void_p, _D, _D, _D, _D], C.c_int),
+    "grlbm_host_write_frame_csv": ([C.POINTER(GridDesc), C.c_float, _D, _D, _D, _D, C.c_char_p, C.c_char_p],
+                                   C.c_int),
+    "grlbm_write_frame_csv": ([C.c_void_p, C.c_float, C.c_char_p, C.c_char_p], C.c_int),
+    "grlbm_run_simulation": ([C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_int32, C.c_char_p,
+                              C.POINTER(C.c_int64)], C.c_int),
     "grlbm_set_rows": ([C.c_void_p, C.c_int64, C.c_int64], C.c_int),
     "grlbm_row_bytes": ([C.c_void_p, C.POINTER(C.c_int64)], C.c_int),
     "grlbm_copy_rows": ([C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_int32], C.c_int),
@@ -276,6 +281,17 @@ class Radiation:
         v = C.c_double()
         self._c(lib().grlbm_energy(self.h, C.byref(v)))
         return v.value
+
+    # ---- frames and the simulation loop (Grid::WriteFrametoCsv, RunSimulation) ----
+    def write_frame(self, time: float, directory: str, name: str = ""):
+        self._c(lib().grlbm_write_frame_csv(self.h, time, directory.encode(), name.encode()))
+
+    def run_simulation(self, sim_time: float, write_period: float, directory: str | None,
+                       t0: float = 0.0, save_initial: bool = True) -> int:
+        n = C.c_int64()
+        self._c(lib().grlbm_run_simulation(self.h, t0, sim_time, write_period, 1 if save_initial else 0,
+                                           directory.encode() if directory else None, C.byref(n)))
+        return n.value
 
     # ---- slab decomposition (one band of interior node rows per rank) ----
     def set_rows(self, j_first: int, j_end: int):

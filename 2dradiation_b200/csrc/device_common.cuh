@@ -295,4 +295,9 @@ void launch_to_dirmajor32(const double *in, float *out, int64_t nxy, int nd, con
 void launch_to_cellmajor64(const double *in, double *out, int64_t nxy, int nd, cudaStream_t s);
 void launch_to_cellmajor32(const float *in, double *out, int64_t nxy, int nd, const float *scale, cudaStream_t s);
 void launch_widen32(const float *in, double *out, int64_t n, cudaStream_t s);
+// ComputeMomentsIF from the current intensities (FP64 out, 6 * nxy)
+void launch_moments_from_I64(const double *I, int64_t nxy, int nd, const double *w, const double *n1,
+                             const double *n2, double *mom, cudaStream_t s);
+void launch_moments_from_I32(const float *J, int64_t nxy, int nd, const double *w, const double *n1,
+                             const double *n2, const float *scale, double *mom, cudaStream_t s);
 } // namespace grlbm

@@ -15,6 +15,7 @@
 #include "../../include/grlbm.h"
 #include "approx_math.hpp"
 #include "device_common.cuh"
+#include "frames.hpp"
 #include "host_setup.hpp"
 
 using namespace grlbm;
@@ -57,6 +58,7 @@ struct grlbm_ctx
     int ng = 0;
     // device buffers (storage type T = double for the plain form, float for the precision form)
     DevBuf I[2], rec, side, w, n1, n2, cx, cy, flags, bhmask, alpha, acube;
+    DevBuf dirs64, frame_mom; // FP64 {w, n1, n2} and moments for frame output
     DevBuf ig_rows, ia3;
     DirTable dirs{}; // precision-form direction tables (kernel parameter)
     DevBuf cu1, cu2, clor, cadt, ceta, ck0, ck3, cka, mom, rkf, lfp;
@@ -458,6 +460,12 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
     {
         n1[d] = ctx->st.cx[d] * rc0 - ctx->st.cy[d] * rs0;
         n2[d] = ctx->st.cx[d] * rs0 + ctx->st.cy[d] * rc0;
+    }
+    {
+        std::vector<double> d64(ctx->st.w.begin(), ctx->st.w.end());
+        d64.insert(d64.end(), n1.begin(), n1.end());
+        d64.insert(d64.end(), n2.begin(), n2.end());
+        TRY(upload(ctx, ctx->dirs64, d64));
     }
     TRY(upload_t(ctx, ctx->w, ctx->st.w));
     TRY(upload_t(ctx, ctx->n1, n1));
@@ -1037,6 +1045,114 @@ int grlbm_compute_moments_lf(grlbm_ctx *ctx, double *E, double *Fx, double *Fy, 
             CU(cudaMemcpyAsync(dst[q], ctx->lf_out.as<double>() + q * nxy, nxy * sizeof(double),
                                cudaMemcpyDeviceToHost, ctx->stream));
     CU(cudaStreamSynchronize(ctx->stream));
+    return GRLBM_OK;
+}
+
+int grlbm_host_write_frame_csv(const grlbm_grid_desc *grid, float time, const double *r, const double *g,
+                               const double *b, const double *a, const char *directory, const char *name)
+{
+    if (!grid || !r || !g || !b || !a || !directory)
+        return fail(nullptr, GRLBM_ERR_ARGUMENT, "grlbm_host_write_frame_csv: null argument");
+    GridGeom G;
+    try
+    {
+        G = GridGeom::from(*grid);
+    }
+    catch (const std::exception &e)
+    {
+        return fail(nullptr, GRLBM_ERR_ARGUMENT, "grlbm_host_write_frame_csv: %s", e.what());
+    }
+    std::string err;
+    if (!write_frame_csv(G, time, r, g, b, a, directory, name ? name : "", err))
+        return fail(nullptr, GRLBM_ERR_HOST, "%s", err.c_str());
+    return GRLBM_OK;
+}
+
+int grlbm_write_frame_csv(grlbm_ctx *ctx, float time, const char *directory, const char *name)
+{
+    if (!ctx)
+        return GRLBM_ERR_ARGUMENT;
+    if (!directory)
+        return fail(ctx, GRLBM_ERR_ARGUMENT, "null directory");
+    cudaSetDevice(ctx->device);
+    const int64_t nxy = ctx->gd.nxy;
+    const int nd = ctx->st.n;
+    int rc;
+    if ((rc = alloc(ctx, ctx->frame_mom, (size_t)6 * nxy * sizeof(double))) ||
+        (rc = alloc(ctx, ctx->lf_out, (size_t)7 * nxy * sizeof(double))))
+        return rc;
+    // ComputeMomentsIF from the current intensities, then ComputeMomentsLF
+    // (src/Radiation.cpp:239-301), as RunSimulation does before each frame
+    const double *d64 = ctx->dirs64.as<double>();
+    if (ctx->fp32)
+        launch_moments_from_I32(ctx->I[ctx->cur].as<float>(), nxy, nd, d64, d64 + nd, d64 + 2 * nd,
+                                state_scale(ctx), ctx->frame_mom.as<double>(), ctx->stream);
+    else
+    {
+        launch_moments_from_I64(ctx->I[ctx->cur].as<double>(), nxy, nd, d64, d64 + nd, d64 + 2 * nd,
+                                ctx->frame_mom.as<double>(), ctx->stream);
+        // the moments E..Pyy now hold ComputeMomentsIF's values, as in the reference
+        CU(cudaMemcpyAsync(ctx->mom.p, ctx->frame_mom.p, (size_t)6 * nxy * sizeof(double),
+                           cudaMemcpyDeviceToDevice, ctx->stream));
+    }
+    launch_moments_lf64(nxy, ctx->frame_mom.as<double>(), ctx->lfp.as<double>(), ctx->bhmask.as<uint8_t>(),
+                        ctx->lf_out.as<double>(), ctx->stream);
+    CU(cudaGetLastError());
+    std::vector<double> h((size_t)7 * nxy);
+    CU(cudaMemcpyAsync(h.data(), ctx->lf_out.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    std::string err;
+    // E_LF, Fx_LF, Fy_LF, F_LF (src/Radiation.cpp:780)
+    if (!write_frame_csv(ctx->geo, time, h.data(), h.data() + nxy, h.data() + 2 * nxy, h.data() + 6 * nxy,
+                         directory, name ? name : "", err))
+        return fail(ctx, GRLBM_ERR_HOST, "%s", err.c_str());
+    return GRLBM_OK;
+}
+
+int grlbm_run_simulation(grlbm_ctx *ctx, double t0, double sim_time, double write_period, int32_t save_initial,
+                         const char *directory, int64_t *steps_out)
+{
+    if (!ctx)
+        return GRLBM_ERR_ARGUMENT;
+    if (!(sim_time >= 0.0) || !(write_period > 0.0))
+        return fail(ctx, GRLBM_ERR_ARGUMENT, "sim_time must be >= 0 and write_period > 0");
+    // src/Radiation.cpp:748-750, 772-832 (the tables are built beforehand,
+    // grlbm_update_fourier_coefficients; no console or profiler output)
+    const int64_t time_steps = (int64_t)std::ceil(sim_time / ctx->geo.dt);
+    double current = t0, since = 0.0;
+    int rc;
+    const bool write = directory != nullptr;
+    if (write && save_initial)
+    {
+        if ((rc = grlbm_write_frame_csv(ctx, (float)current, directory, "")))
+            return rc;
+        since = 0.0;
+    }
+    int64_t pending = 0; // steps enqueued since the last frame
+    for (int64_t n = 0; n < time_steps; n++)
+    {
+        pending++;
+        current += ctx->geo.dt;
+        since += ctx->geo.dt;
+        if (write && since >= write_period - 1e-8)
+        {
+            if ((rc = grlbm_step(ctx, (int32_t)pending)))
+                return rc;
+            pending = 0;
+            if ((rc = grlbm_write_frame_csv(ctx, (float)current, directory, "")))
+                return rc;
+            since = 0.0;
+        }
+    }
+    if (pending && (rc = grlbm_step(ctx, (int32_t)pending)))
+        return rc;
+    if (write && since != 0.0)
+    {
+        if ((rc = grlbm_write_frame_csv(ctx, (float)current, directory, "")))
+            return rc;
+    }
+    if (steps_out)
+        *steps_out = time_steps;
     return GRLBM_OK;
 }
 

@@ -300,6 +300,37 @@ __global__ void __launch_bounds__(kStepBlock, GRLBM_PLAIN_MIN_BLOCKS) k_step_pla
     }
 }
 
+// Radiation::ComputeMomentsIF (src/Radiation.cpp:239-269): the six moments
+// of the current intensities at every node, halo included, in the
+// reference's order.  The precision form's state is converted back to I
+// (J / (1 / alpha^3)) first.
+template <typename T>
+__global__ void k_moments_from_I(const T *I, int64_t nxy, int nd, const double *w, const double *n1,
+                                 const double *n2, const float *scale, double *mom)
+{
+    const int64_t ij = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (ij >= nxy)
+        return;
+    Moments m;
+    m.zero();
+    for (int d = 0; d < nd; d++)
+    {
+        const double wd = __ldg(w + d);
+        if (wd == 0.0)
+            continue;
+        double v = (double)I[(int64_t)d * nxy + ij];
+        if (scale)
+            v = v / (double)scale[ij];
+        m.add(wd, v, __ldg(n1 + d), __ldg(n2 + d));
+    }
+    mom[ij] = m.E;
+    mom[ij + nxy] = m.Fx;
+    mom[ij + 2 * nxy] = m.Fy;
+    mom[ij + 3 * nxy] = m.Pxx;
+    mom[ij + 4 * nxy] = m.Pxy;
+    mom[ij + 5 * nxy] = m.Pyy;
+}
+
 // Radiation::LoadInitialData for fixed streaming (src/Radiation.cpp:138-181)
 template <typename T>
 __global__ void k_sources(T *I, int64_t nxy, int nd, const int64_t *nodes, const T *vals, int64_t nsrc)
@@ -530,6 +561,16 @@ void launch_to_cellmajor64(const double *in, double *out, int64_t nxy, int nd, c
 void launch_to_cellmajor32(const float *in, double *out, int64_t nxy, int nd, const float *scale, cudaStream_t s)
 {
     k_to_cellmajor<float><<<dim3(nblk(nxy, 32), nblk(nd, 32)), dim3(32, 8), 0, s>>>(in, out, nxy, nd, scale);
+}
+void launch_moments_from_I64(const double *I, int64_t nxy, int nd, const double *w, const double *n1,
+                             const double *n2, double *mom, cudaStream_t s)
+{
+    k_moments_from_I<double><<<nblk(nxy, 128), 128, 0, s>>>(I, nxy, nd, w, n1, n2, nullptr, mom);
+}
+void launch_moments_from_I32(const float *J, int64_t nxy, int nd, const double *w, const double *n1,
+                             const double *n2, const float *scale, double *mom, cudaStream_t s)
+{
+    k_moments_from_I<float><<<nblk(nxy, 128), 128, 0, s>>>(J, nxy, nd, w, n1, n2, scale, mom);
 }
 void launch_widen32(const float *in, double *out, int64_t n, cudaStream_t s)
 {

@@ -276,6 +276,25 @@ int grlbm_adjoint_forward(grlbm_adjoint *adj, int32_t n_steps);
  * any may be NULL) for the last forward, with the fields as they were then. */
 int grlbm_adjoint_backward(grlbm_adjoint *adj, const double *dL_dE, double *g_eta, double *g_kappaA,
                            double *g_kappa0);
+/* ---- frames and the simulation loop ---------------------------------------
+ * Grid::WriteFrametoCsv (src/Grid.cpp:110-137) for host arrays: writes
+ * directory + name + Format(time, 3) + "t <nx>x <ny>y.csv" ("data" when name
+ * is NULL or empty; the directory string is used as given, so end it with
+ * '/'), creating the directory if needed.  Byte-identical to the
+ * reference's file for the same arrays.  No GPU needed. */
+int grlbm_host_write_frame_csv(const grlbm_grid_desc *grid, float time, const double *r, const double *g,
+                               const double *b, const double *a, const char *directory, const char *name);
+/* The frame RunSimulation writes (src/Radiation.cpp:778-781): ComputeMomentsIF
+ * of the current intensities (which then become the context's inertial-frame
+ * moments), ComputeMomentsLF, and E_LF, Fx_LF, Fy_LF, F_LF to a CSV file. */
+int grlbm_write_frame_csv(grlbm_ctx *ctx, float time, const char *directory, const char *name);
+/* The time loop of Radiation::RunSimulation (src/Radiation.cpp:748-832) after
+ * its set-up (build the tables first): ceil(sim_time / dt) steps from time
+ * t0, a frame at t0 when save_initial, one each time write_period has passed,
+ * and a final one; no frames when directory is NULL.  *steps_out (may be
+ * NULL) receives the step count. */
+int grlbm_run_simulation(grlbm_ctx *ctx, double t0, double sim_time, double write_period, int32_t save_initial,
+                         const char *directory, int64_t *steps_out);
 /* Lambda-iteration and table-build statistics (src/Radiation.cpp:723-733,
  * 855-857). */
 int grlbm_get_stats(grlbm_ctx *ctx, grlbm_stats *stats);

@@ -115,6 +115,28 @@ def library(kind: str = "oracle") -> C.CDLL:
     return lib
 
 
+def set_frames(kind: str, write_period: float | None, workdir: str | None):
+    """Frame output of the reference's RunSimulation (run(..., use_run_simulation=True)):
+    every write_period, written under <workdir>/../output/ref_run/Moments/;
+    workdir None turns it off.  Reference libraries only."""
+    lib = library(kind)
+    lib.ref_set_frames.argtypes = [C.c_double, C.c_char_p]
+    lib.ref_set_frames.restype = None
+    lib.ref_set_frames(float(write_period or 1e300), workdir.encode() if workdir else None)
+
+
+def write_frame(kind: str, case: dict, time: float, r, g, b, a, directory: str, name: str = ""):
+    """The reference's Grid::WriteFrametoCsv for host arrays (reference libraries only)."""
+    lib = library(kind)
+    lib.ref_write_frame.argtypes = [C.POINTER(Params), C.c_float] + [C.POINTER(C.c_double)] * 4 + \
+        [C.c_char_p, C.c_char_p]
+    lib.ref_write_frame.restype = C.c_int
+    p = Params(nx_=int(case["nx_"]), ny_=int(case["ny_"]), startx=case["start"][0], starty=case["start"][1],
+               endx=case["end"][0], endy=case["end"][1], cfl=case["cfl"])
+    arrs = [np.ascontiguousarray(x, dtype=np.float64) for x in (r, g, b, a)]
+    return lib.ref_write_frame(C.byref(p), float(time), *[_ptr(x) for x in arrs], directory.encode(), name.encode())
+
+
 def available(kind: str) -> bool:
     try:
         library(kind)

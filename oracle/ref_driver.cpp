@@ -18,11 +18,16 @@
 #include <chrono>
 #include <cstring>
 #include <omp.h>
+#include <unistd.h>
 
 extern double maxTE; // from ref_geodesic_tu.cpp
 
 namespace
 {
+// Frame output of RunSimulation (ref_set_frames): off unless a directory is set.
+double g_frame_period = 1e300;
+std::string g_frame_workdir;
+
 using MetricArray = DoubleBuffer Metric::*;
 // Member order of src/Metric.h:19-65.
 const MetricArray kMetricArrays[GRLBM_N_METRIC_ARRAYS] = {
@@ -124,14 +129,14 @@ extern "C" int ref_run(const grlbm_ref_params *p, const grlbm_ref_inputs *in, gr
         .name = "ref_run",
         .t0 = 0,
         .simTime = (p->n_steps - 0.5) * grid.dt,
-        .writePeriod = 1e300,
+        .writePeriod = g_frame_workdir.empty() ? 1e300 : g_frame_period,
         .updateFourierHarmonics = false,
         .keepSourceNodesActive = p->keep_source_nodes_active != 0,
-        .writeData = false,
+        .writeData = !g_frame_workdir.empty(),
         .printSetup = false,
         .printProgress = false,
         .printResults = false,
-        .saveInitialData = false,
+        .saveInitialData = !g_frame_workdir.empty(),
         .streamingType = (StreamingType)p->streaming_type,
         .initialDataType = (InitialDataType)p->initial_data_type,
     };
@@ -157,7 +162,18 @@ extern "C" int ref_run(const grlbm_ref_params *p, const grlbm_ref_inputs *in, gr
 
     if (p->use_run_simulation)
     {
+        // with frames on, the reference writes under ../output/<name>/ relative
+        // to the working directory: run it from <workdir>/run
+        char cwd[4096] = {0};
+        const bool frames = !g_frame_workdir.empty();
+        if (frames)
+        {
+            if (!getcwd(cwd, sizeof cwd) || chdir(g_frame_workdir.c_str()) != 0)
+                return -2;
+        }
         r.RunSimulation();
+        if (frames && chdir(cwd) != 0)
+            return -2;
         out->computation_time_s = r.logger.ComputationTime();
         out->table_time_s = Profiler::Session::Get().GetTotalTime("void Radiation::UpdateFourierCoefficients()");
         out->max_iterations = r.logger.maxItterationCount;
@@ -248,5 +264,29 @@ extern "C" int ref_run(const grlbm_ref_params *p, const grlbm_ref_inputs *in, gr
     }
     delete rad;
     delete metric;
+    return 0;
+}
+
+// Frame output for the next RunSimulation runs (use_run_simulation): every
+// write_period and at the start and end, into <workdir>/../output/ref_run/
+// Moments/; workdir NULL turns it off.
+extern "C" void ref_set_frames(double write_period, const char *workdir)
+{
+    g_frame_period = write_period;
+    g_frame_workdir = workdir ? workdir : "";
+}
+
+// Grid::WriteFrametoCsv of a grid built like ref_run's, for host arrays.
+extern "C" int ref_write_frame(const grlbm_ref_params *p, float time, const double *r, const double *g,
+                               const double *b, const double *a, const char *directory, const char *name)
+{
+    Grid grid(p->nx_, p->ny_, Coord(p->startx, p->starty), Coord(p->endx, p->endy));
+    grid.SetCFL(p->cfl);
+    DoubleBuffer R(grid.nxy), G(grid.nxy), B(grid.nxy), A(grid.nxy);
+    std::memcpy(R.data(), r, grid.nxy * sizeof(double));
+    std::memcpy(G.data(), g, grid.nxy * sizeof(double));
+    std::memcpy(B.data(), b, grid.nxy * sizeof(double));
+    std::memcpy(A.data(), a, grid.nxy * sizeof(double));
+    grid.WriteFrametoCsv(time, R, G, B, A, directory, name ? name : "");
     return 0;
 }

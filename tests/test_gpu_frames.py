@@ -1,0 +1,33 @@
+"""RunSimulation with frame output: grlbm_run_simulation against the
+reference's own RunSimulation writing its CSV frames (initial, every write
+period, final) for the flat beam, whose steps are bit-identical: the frame
+files must match byte for byte, names included."""
+import os
+
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def test_run_simulation_frames_match_reference(grlbm, W, oracle, tmp_path):
+    if not oracle.available("ref_strict"):
+        pytest.skip("the reference build is absent")
+    case = W.flat_beam(nx_=30, ny_=24, n_dir=12, steps=41)
+    work = tmp_path / "ref" / "run"
+    work.mkdir(parents=True)
+    with grlbm.prepare(case) as r:
+        dt = r.dt
+        period = 7.5 * dt
+        try:
+            oracle.set_frames("ref_strict", period, str(work))
+            oracle.run(case, "ref_strict", use_run_simulation=True)
+        finally:
+            oracle.set_frames("ref_strict", None, None)
+        ours = tmp_path / "ours"
+        steps = r.run_simulation((int(case["n_steps"]) - 0.5) * dt, period, str(ours) + "/")
+    assert steps == int(case["n_steps"])
+    ref_dir = tmp_path / "ref" / "output" / "ref_run" / "Moments"
+    a, b = sorted(os.listdir(ours)), sorted(os.listdir(ref_dir))
+    assert a == b and len(a) == 7  # initial, 5 periods, final
+    for name in a:
+        assert (ours / name).read_bytes() == (ref_dir / name).read_bytes(), name
