@@ -94,6 +94,7 @@ SIGNATURES = {
     "grlbm_adjoint_last_error": ([C.c_void_p], C.c_char_p),
     "grlbm_adjoint_forward": ([C.c_void_p, C.c_int32], C.c_int),
     "grlbm_adjoint_backward": ([C.c_void_p, _D, _D, _D, _D], C.c_int),
+    "grlbm_set_update_tables_each_step": ([C.c_void_p, C.c_int32, C.c_double, C.c_int32], C.c_int),
     "grlbm_host_write_frame_csv": ([C.POINTER(GridDesc), C.c_float, _D, _D, _D, _D, C.c_char_p, C.c_char_p],
                                    C.c_int),
     "grlbm_write_frame_csv": ([C.c_void_p, C.c_float, C.c_char_p, C.c_char_p], C.c_int),
@@ -281,6 +282,10 @@ class Radiation:
         v = C.c_double()
         self._c(lib().grlbm_energy(self.h, C.byref(v)))
         return v.value
+
+    def update_tables_each_step(self, enabled: bool, rk_tol: float = 1e-4, max_substeps: int = 0):
+        """Config::updateFourierHarmonics: rebuild the geodesic tables before every step."""
+        self._c(lib().grlbm_set_update_tables_each_step(self.h, 1 if enabled else 0, rk_tol, max_substeps))
 
     # ---- frames and the simulation loop (Grid::WriteFrametoCsv, RunSimulation) ----
     def write_frame(self, time: float, directory: str, name: str = ""):

@@ -70,6 +70,10 @@ struct grlbm_ctx
     int64_t nsrc = 0;
     int cur = 0;
     bool tables = false;
+    // config.updateFourierHarmonics: rebuild the tables before every step
+    bool update_each_step = false;
+    double update_tol = 1e-4;
+    int32_t update_max_substeps = 0;
     int64_t steps = 0;
     double table_ms = 0;
     cudaGraphExec_t graph[2] = {nullptr, nullptr}; // kGraphSteps steps from buffer 0 / 1
@@ -964,6 +968,20 @@ int grlbm_step_async(grlbm_ctx *ctx, int32_t n_steps)
         return fail(ctx, GRLBM_ERR_STATE, "curved streaming needs grlbm_update_fourier_coefficients first");
     cudaSetDevice(ctx->device);
     int rc;
+    if (ctx->update_each_step)
+    {
+        // UpdateFourierCoefficients at the top of every step (src/Radiation.cpp:790-791)
+        for (int k = 0; k < n_steps; k++)
+        {
+            if ((rc = grlbm_update_fourier_coefficients(ctx, ctx->update_tol, ctx->update_max_substeps)))
+                return rc;
+            if ((rc = enqueue_step(ctx, ctx->cur)))
+                return rc;
+            ctx->cur ^= 1;
+            ctx->steps++;
+        }
+        return GRLBM_OK;
+    }
     int left = n_steps;
     while (left >= kGraphSteps)
     {
@@ -1045,6 +1063,18 @@ int grlbm_compute_moments_lf(grlbm_ctx *ctx, double *E, double *Fx, double *Fy, 
             CU(cudaMemcpyAsync(dst[q], ctx->lf_out.as<double>() + q * nxy, nxy * sizeof(double),
                                cudaMemcpyDeviceToHost, ctx->stream));
     CU(cudaStreamSynchronize(ctx->stream));
+    return GRLBM_OK;
+}
+
+int grlbm_set_update_tables_each_step(grlbm_ctx *ctx, int32_t enabled, double rk_tol, int32_t max_substeps)
+{
+    if (!ctx)
+        return GRLBM_ERR_ARGUMENT;
+    if (enabled && !(rk_tol > 0))
+        return fail(ctx, GRLBM_ERR_ARGUMENT, "rk_tol must be positive");
+    ctx->update_each_step = enabled != 0;
+    ctx->update_tol = rk_tol;
+    ctx->update_max_substeps = max_substeps;
     return GRLBM_OK;
 }
 

@@ -92,7 +92,10 @@ struct KMoments
 // slots and a window's taps are fixed offsets from one address.  The next
 // chunk's planes are loaded by cp.async into slots the current chunk does not
 // read.
-constexpr int kTileX = 32, kTileY = 4;
+#ifndef GRLBM_PREC_TILE_X
+#define GRLBM_PREC_TILE_X 32
+#endif
+constexpr int kTileX = GRLBM_PREC_TILE_X, kTileY = kStepBlock / GRLBM_PREC_TILE_X;
 static_assert(kTileX * kTileY == kStepBlock, "tile = block");
 constexpr int kPatchX = kTileX + 2, kPatchY = kTileY + 2, kPatch = kPatchX * kPatchY;
 static_assert(kPatch > kStepBlock && kPatch <= 2 * kStepBlock, "two staging loads per thread and plane");

@@ -276,6 +276,12 @@ int grlbm_adjoint_forward(grlbm_adjoint *adj, int32_t n_steps);
  * any may be NULL) for the last forward, with the fields as they were then. */
 int grlbm_adjoint_backward(grlbm_adjoint *adj, const double *dL_dE, double *g_eta, double *g_kappaA,
                            double *g_kappa0);
+/* Config::updateFourierHarmonics (src/Config.hh:51, src/Radiation.cpp:790-791):
+ * when enabled, every step first rebuilds the geodesic tables
+ * (grlbm_update_fourier_coefficients with rk_tol and max_substeps), as the
+ * reference does at the top of each step; steps are then launched one by one. */
+int grlbm_set_update_tables_each_step(grlbm_ctx *ctx, int32_t enabled, double rk_tol, int32_t max_substeps);
+
 /* ---- frames and the simulation loop ---------------------------------------
  * Grid::WriteFrametoCsv (src/Grid.cpp:110-137) for host arrays: writes
  * directory + name + Format(time, 3) + "t <nx>x <ny>y.csv" ("data" when name
