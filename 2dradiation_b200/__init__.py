@@ -94,6 +94,7 @@ SIGNATURES = {
     "grlbm_adjoint_last_error": ([C.c_void_p], C.c_char_p),
     "grlbm_adjoint_forward": ([C.c_void_p, C.c_int32], C.c_int),
     "grlbm_adjoint_backward": ([C.c_void_p, _D, _D, _D, _D], C.c_int),
+    "grlbm_set_initial_flux_angle": ([C.c_void_p, _D], C.c_int),
     "grlbm_set_update_tables_each_step": ([C.c_void_p, C.c_int32, C.c_double, C.c_int32], C.c_int),
     "grlbm_host_write_frame_csv": ([C.POINTER(GridDesc), C.c_float, _D, _D, _D, _D, C.c_char_p, C.c_char_p],
                                    C.c_int),

@@ -167,6 +167,11 @@ struct PlainStepArgs
     double *mom;               // 6*nxy
     unsigned long long *iter_sum;
     unsigned int *iter_max;
+    // adaptive streaming only (null otherwise): rotation angles before and
+    // after this step's update (nxy), and the Fourier coefficients
+    const double *ang_old, *ang_new;
+    const double *coef; // [5][nxy][nf]
+    int nf;
 };
 
 struct PrecStepArgs
@@ -296,8 +301,10 @@ void launch_to_cellmajor64(const double *in, double *out, int64_t nxy, int nd, c
 void launch_to_cellmajor32(const float *in, double *out, int64_t nxy, int nd, const float *scale, cudaStream_t s);
 void launch_widen32(const float *in, double *out, int64_t n, cudaStream_t s);
 // ComputeMomentsIF from the current intensities (FP64 out, 6 * nxy)
+// (ang: per-node rotation angles of adaptive streaming, with n1/n2 the
+// unrotated stencil directions; null otherwise)
 void launch_moments_from_I64(const double *I, int64_t nxy, int nd, const double *w, const double *n1,
-                             const double *n2, double *mom, cudaStream_t s);
+                             const double *n2, const double *ang, double *mom, cudaStream_t s);
 void launch_moments_from_I32(const float *J, int64_t nxy, int nd, const double *w, const double *n1,
                              const double *n2, const float *scale, double *mom, cudaStream_t s);
 } // namespace grlbm

@@ -59,6 +59,11 @@ struct grlbm_ctx
     // device buffers (storage type T = double for the plain form, float for the precision form)
     DevBuf I[2], rec, side, w, n1, n2, cx, cy, flags, bhmask, alpha, acube;
     DevBuf dirs64, frame_mom; // FP64 {w, n1, n2} and moments for frame output
+    // adaptive streaming: rotation angles (ang[cur] current, ang[cur ^ 1] the
+    // next), the source nodes' angles, and initialFluxAngle_IF
+    DevBuf ang[2], src_ang_nodes, src_ang_vals;
+    int64_t nsrc_ang = 0;
+    std::vector<double> flux_angle;
     DevBuf ig_rows, ia3;
     DirTable dirs{}; // precision-form direction tables (kernel parameter)
     DevBuf cu1, cu2, clor, cadt, ceta, ck0, ck3, cka, mom, rkf, lfp;
@@ -234,10 +239,19 @@ PlainStepArgs plain_args(grlbm_ctx *ctx, int from)
     return a;
 }
 
+bool is_curved(const grlbm_ctx *ctx)
+{
+    return ctx->run.streaming_type == GRLBM_CURVED_FIXED || ctx->run.streaming_type == GRLBM_CURVED_ADAPTIVE;
+}
+bool is_adaptive(const grlbm_ctx *ctx)
+{
+    return ctx->run.streaming_type == GRLBM_FLAT_ADAPTIVE || ctx->run.streaming_type == GRLBM_CURVED_ADAPTIVE;
+}
+
 // Enqueue one step starting from buffer `from` (no sync).
 int enqueue_step(grlbm_ctx *ctx, int from)
 {
-    const bool curved = ctx->run.streaming_type == GRLBM_CURVED_FIXED;
+    const bool curved = is_curved(ctx);
     unsigned long long *cnt = ctx->counters.as<unsigned long long>();
     if (ctx->fp32)
     {
@@ -252,7 +266,18 @@ int enqueue_step(grlbm_ctx *ctx, int from)
         if (ctx->run.keep_source_nodes_active && ctx->nsrc > 0)
             launch_sources64(ctx->I[from].as<double>(), ctx->gd.nxy, ctx->st.n, ctx->src_nodes.as<int64_t>(),
                              ctx->src_vals.as<double>(), ctx->nsrc, ctx->stream);
-        const PlainStepArgs a = plain_args(ctx, from);
+        PlainStepArgs a = plain_args(ctx, from);
+        if (is_adaptive(ctx))
+        {
+            // LoadInitialData also sets the source nodes' angles (src/Radiation.cpp:170-176)
+            if (ctx->run.keep_source_nodes_active && ctx->nsrc_ang > 0)
+                launch_sources64(ctx->ang[from].as<double>(), ctx->gd.nxy, 1, ctx->src_ang_nodes.as<int64_t>(),
+                                 ctx->src_ang_vals.as<double>(), ctx->nsrc_ang, ctx->stream);
+            a.ang_old = ctx->ang[from].as<double>();
+            a.ang_new = ctx->ang[from ^ 1].as<double>();
+            a.coef = ctx->coef.as<double>();
+            a.nf = ctx->ss.n;
+        }
         launch_step_plain(a, curved, ctx->stream);
     }
     CU(cudaGetLastError());
@@ -370,13 +395,14 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
         return fail(nullptr, GRLBM_ERR_ARGUMENT, "cfl must be positive");
     if (metric->kind < GRLBM_MINKOWSKI || metric->kind > GRLBM_KERRSCHILD)
         return fail(nullptr, GRLBM_ERR_ARGUMENT, "unknown metric kind %d", metric->kind);
-    if (run->streaming_type != GRLBM_FLAT_FIXED && run->streaming_type != GRLBM_CURVED_FIXED)
-    {
-        if (run->streaming_type >= GRLBM_FLAT_FIXED && run->streaming_type <= GRLBM_GEODESIC_FIXED)
-            return fail(nullptr, GRLBM_ERR_UNSUPPORTED,
-                        "streaming type %d is not built (FlatFixed and CurvedFixed are)", run->streaming_type);
+    if (run->streaming_type < GRLBM_FLAT_FIXED || run->streaming_type > GRLBM_GEODESIC_FIXED)
         return fail(nullptr, GRLBM_ERR_ARGUMENT, "Invalid StreamingType");
-    }
+    if (run->streaming_type == GRLBM_GEODESIC_FIXED)
+        return fail(nullptr, GRLBM_ERR_UNSUPPORTED,
+                    "GeodesicFixed (a performance test of the reference) is not built");
+    if ((run->streaming_type == GRLBM_FLAT_ADAPTIVE || run->streaming_type == GRLBM_CURVED_ADAPTIVE) &&
+        run->precision != GRLBM_PLAIN_FP64)
+        return fail(nullptr, GRLBM_ERR_UNSUPPORTED, "adaptive streaming is built for GRLBM_PLAIN_FP64 only");
     if (run->precision != GRLBM_PLAIN_FP64 && run->precision != GRLBM_PRECISION_FP32)
         return fail(nullptr, GRLBM_ERR_ARGUMENT, "unknown precision %d", run->precision);
     const int maxdir = kMaxDirs;
@@ -667,6 +693,16 @@ std::vector<IgRow> rows(ctx->ng);
     TRY(alloc(ctx, ctx->energy_out, sizeof(double)));
     cudaMemset(ctx->I[0].p, 0, ib);
     cudaMemset(ctx->I[1].p, 0, ib);
+    if (is_adaptive(ctx))
+    {
+        // rotationAngle and rotationAngleNew start at zero (src/Radiation.cpp:3-60)
+        for (auto &b : ctx->ang)
+        {
+            TRY(alloc(ctx, b, (size_t)nxy * sizeof(double)));
+            cudaMemset(b.p, 0, b.bytes);
+        }
+        ctx->flux_angle.assign(nxy, 0.0);
+    }
     cudaMemset(ctx->mom.p, 0, ctx->mom.bytes);
     cudaMemset(ctx->counters.p, 0, ctx->counters.bytes);
     cudaMemset(ctx->rec.p, 0, ctx->rec.bytes);
@@ -766,7 +802,8 @@ int grlbm_set_initial_data(grlbm_ctx *ctx, const uint8_t *is_initial, const doub
     try
     {
         S = build_sources(ctx->M, ctx->st, ctx->run.initial_data_type, is_initial, initial_I, E_LF, Fx_LF, Fy_LF,
-                          Pxx_LF, Pxy_LF, Pyy_LF);
+                          Pxx_LF, Pxy_LF, Pyy_LF, is_adaptive(ctx),
+                          ctx->flux_angle.empty() ? nullptr : ctx->flux_angle.data());
     }
     catch (const std::exception &e)
     {
@@ -788,6 +825,12 @@ int grlbm_set_initial_data(grlbm_ctx *ctx, const uint8_t *is_initial, const doub
     int rc;
     if ((rc = upload(ctx, ctx->src_nodes, S.nodes)) || (rc = upload_t(ctx, ctx->src_vals, S.intensities)))
         return rc;
+    if (is_adaptive(ctx))
+    {
+        ctx->nsrc_ang = (int64_t)S.angle_nodes.size();
+        if ((rc = upload(ctx, ctx->src_ang_nodes, S.angle_nodes)) || (rc = upload(ctx, ctx->src_ang_vals, S.angles)))
+            return rc;
+    }
     invalidate_graphs(ctx);
     return GRLBM_OK;
 }
@@ -809,8 +852,24 @@ int grlbm_load_initial_data(grlbm_ctx *ctx)
             launch_sources64(ctx->I[b].as<double>(), ctx->gd.nxy, ctx->st.n, ctx->src_nodes.as<int64_t>(),
                              ctx->src_vals.as<double>(), ctx->nsrc, ctx->stream);
     }
+    // and the source nodes' rotation angles, into the current angles only
+    if (is_adaptive(ctx) && ctx->nsrc_ang > 0)
+        launch_sources64(ctx->ang[ctx->cur].as<double>(), ctx->gd.nxy, 1, ctx->src_ang_nodes.as<int64_t>(),
+                         ctx->src_ang_vals.as<double>(), ctx->nsrc_ang, ctx->stream);
     CU(cudaGetLastError());
     CU(cudaStreamSynchronize(ctx->stream));
+    return GRLBM_OK;
+}
+
+int grlbm_set_initial_flux_angle(grlbm_ctx *ctx, const double *angle)
+{
+    if (!ctx)
+        return GRLBM_ERR_ARGUMENT;
+    if (!angle)
+        return fail(ctx, GRLBM_ERR_ARGUMENT, "null angles");
+    if (!is_adaptive(ctx))
+        return fail(ctx, GRLBM_ERR_STATE, "initialFluxAngle_IF is read by the adaptive streaming types only");
+    ctx->flux_angle.assign(angle, angle + ctx->gd.nxy);
     return GRLBM_OK;
 }
 
@@ -964,7 +1023,7 @@ int grlbm_step_async(grlbm_ctx *ctx, int32_t n_steps)
         return GRLBM_ERR_ARGUMENT;
     if (n_steps < 0)
         return fail(ctx, GRLBM_ERR_ARGUMENT, "negative step count");
-    if (ctx->run.streaming_type == GRLBM_CURVED_FIXED && !ctx->tables)
+    if (is_curved(ctx) && !ctx->tables)
         return fail(ctx, GRLBM_ERR_STATE, "curved streaming needs grlbm_update_fourier_coefficients first");
     cudaSetDevice(ctx->device);
     int rc;
@@ -1119,8 +1178,13 @@ int grlbm_write_frame_csv(grlbm_ctx *ctx, float time, const char *directory, con
                                 state_scale(ctx), ctx->frame_mom.as<double>(), ctx->stream);
     else
     {
-        launch_moments_from_I64(ctx->I[ctx->cur].as<double>(), nxy, nd, d64, d64 + nd, d64 + 2 * nd,
-                                ctx->frame_mom.as<double>(), ctx->stream);
+        if (is_adaptive(ctx))
+            launch_moments_from_I64(ctx->I[ctx->cur].as<double>(), nxy, nd, d64, ctx->cx.as<double>(),
+                                    ctx->cy.as<double>(), ctx->ang[ctx->cur].as<double>(),
+                                    ctx->frame_mom.as<double>(), ctx->stream);
+        else
+            launch_moments_from_I64(ctx->I[ctx->cur].as<double>(), nxy, nd, d64, d64 + nd, d64 + 2 * nd, nullptr,
+                                    ctx->frame_mom.as<double>(), ctx->stream);
         // the moments E..Pyy now hold ComputeMomentsIF's values, as in the reference
         CU(cudaMemcpyAsync(ctx->mom.p, ctx->frame_mom.p, (size_t)6 * nxy * sizeof(double),
                            cudaMemcpyDeviceToDevice, ctx->stream));
@@ -1209,6 +1273,8 @@ int grlbm_set_rows(grlbm_ctx *ctx, int64_t j_first, int64_t j_end)
 {
     if (!ctx)
         return GRLBM_ERR_ARGUMENT;
+    if (is_adaptive(ctx))
+        return fail(ctx, GRLBM_ERR_UNSUPPORTED, "adaptive streaming is not split into bands");
     if (j_first < 1 || j_end > ctx->geo.ny - 1 || j_first >= j_end)
         return fail(ctx, GRLBM_ERR_ARGUMENT, "rows [%lld, %lld) outside the interior rows [1, %lld)",
                     (long long)j_first, (long long)j_end, (long long)(ctx->geo.ny - 1));
@@ -1253,6 +1319,8 @@ int grlbm_departure_rows(grlbm_ctx *ctx, int32_t *rows)
 {
     if (!ctx || !rows)
         return GRLBM_ERR_ARGUMENT;
+    if (is_adaptive(ctx))
+        return fail(ctx, GRLBM_ERR_UNSUPPORTED, "adaptive streaming is not split into bands");
     if (ctx->run.streaming_type == GRLBM_FLAT_FIXED)
     {
         int ext = 0;
@@ -1739,6 +1807,8 @@ int grlbm_adjoint_create(grlbm_ctx *ctx, int32_t checkpoint_every, grlbm_adjoint
     *out = nullptr;
     if (ctx->fp32)
         return afail(nullptr, GRLBM_ERR_UNSUPPORTED, "grlbm_adjoint_create: the adjoint follows GRLBM_PLAIN_FP64");
+    if (is_adaptive(ctx))
+        return afail(nullptr, GRLBM_ERR_UNSUPPORTED, "grlbm_adjoint_create: the adjoint follows the fixed streaming types");
     const bool curved = ctx->run.streaming_type == GRLBM_CURVED_FIXED;
     if (curved && !ctx->tables)
         return afail(nullptr, GRLBM_ERR_STATE, "grlbm_adjoint_create: build the geodesic tables first");

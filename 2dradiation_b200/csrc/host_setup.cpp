@@ -419,7 +419,7 @@ MetricArrays MetricArrays::build(const GridGeom &g, const grlbm_metric_desc &d)
 Sources build_sources(const MetricArrays &M, const StencilTables &st, int initial_data_type,
                       const uint8_t *is_initial, const double *initial_I, const double *E,
                       const double *Fx, const double *Fy, const double *Pxx, const double *Pxy,
-                      const double *Pyy)
+                      const double *Pyy, bool adaptive, const double *flux_angle)
 {
     Sources S;
     const int nd = st.n;
@@ -435,6 +435,12 @@ Sources build_sources(const MetricArrays &M, const StencilTables &st, int initia
         {
             for (int d = 0; d < nd; d++)
                 I[d] = initial_I ? initial_I[ij * nd + d] : 0.0;
+            if (adaptive)
+            {
+                // rotationAngle[ij] = initialFluxAngle_IF[ij] (src/Radiation.cpp:177)
+                S.angle_nodes.push_back(ij);
+                S.angles.push_back(flux_angle ? flux_angle[ij] : 0.0);
+            }
             continue;
         }
         // InitialDataLFtoIF (src/Radiation.cpp:103-127): E from the boosted
@@ -458,11 +464,17 @@ Sources build_sources(const MetricArrays &M, const StencilTables &st, int initia
         // LoadInitialData, InitialDataType::Moments (src/Radiation.cpp:150-174)
         const double f = std::sqrt(fx * fx + fy * fy);
         const double rel = f / e00;
-        double dir1 = fx / f, dir2 = fy / f;
+        double dir1 = adaptive ? 1.0 : fx / f, dir2 = adaptive ? 0.0 : fy / f;
         if (f < 1e-16)
         {
             dir1 = 1;
             dir2 = 0;
+        }
+        if (adaptive && !(f < 1e-16))
+        {
+            // rotationAngle[ij] (src/Radiation.cpp:170-171)
+            S.angle_nodes.push_back(ij);
+            S.angles.push_back(std::fmod(approx_atan2(fy, fx) + 2.0 * kPi, 2.0 * kPi));
         }
         const double sigma = st.lut_eval(st.lut_sigma, rel);
         const double norm = st.lut_eval(st.lut_norm, rel);

@@ -91,11 +91,16 @@ struct Sources
 {
     std::vector<int64_t> nodes;
     std::vector<double> intensities; // nodes.size() * nDir, node-major
+    // adaptive streaming: the rotation angles LoadInitialData sets
+    std::vector<int64_t> angle_nodes;
+    std::vector<double> angles;
 };
+// adaptive: the adaptive streaming types (von Mises distributions around
+// direction (1, 0), angles from the flux or from flux_angle (nx*ny; NULL: 0)).
 Sources build_sources(const MetricArrays &M, const StencilTables &st, int initial_data_type,
                       const uint8_t *is_initial, const double *initial_I, const double *E,
                       const double *Fx, const double *Fy, const double *Pxx, const double *Pxy,
-                      const double *Pyy);
+                      const double *Pyy, bool adaptive = false, const double *flux_angle = nullptr);
 
 // Fourier basis of src/FourierHarmonics.cpp:5-14 (libm cos/sin).
 double fourier_basis(int k, double phi);

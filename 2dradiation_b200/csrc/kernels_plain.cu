@@ -8,6 +8,7 @@
 // change of all six moments, including ones that are pure rounding noise
 // (e.g. Fy of a nearly isotropic cell), so its iteration counts, and through
 // them E, follow the last bits of the streamed intensities.
+#include "approx_math.hpp"
 #include "device_common.cuh"
 
 // Resident blocks per SM the step kernel's register budget is sized for.
@@ -158,10 +159,123 @@ __device__ __forceinline__ double div_rn(double num, double den, double r)
     return __fma_rn(__fma_rn(-q, den, num), r, q);
 }
 
+// Fourier::GetValue (src/FourierHarmonics.cpp:56-61) with Fourier::Basis
+// (:5-14) at a run-time angle.
+__device__ __forceinline__ double fourier_value(const double *coef, int nf, double phi)
+{
+    const double sqrt2 = 1.4142135623730951; // sqrt(2), correctly rounded
+    double result = 0;
+    for (int k = 0; k < nf; k++)
+    {
+        double b;
+        if (k == 0)
+            b = 1.0;
+        else if (k % 2 != 0)
+            b = sqrt2 * cos(phi * (k + 1.0) / 2.0);
+        else
+            b = sqrt2 * sin(phi * k / 2.0);
+        result += coef[k] * b;
+    }
+    return result;
+}
+
+// IntensityAt (src/Radiation.cpp:322-343) of node n for the (unrotated)
+// direction (v1, v2): rotated into the node's stencil frame by the inverse of
+// its previous rotation angle, then the two cubic rows of the interpolation
+// grid, blended and clamped at zero.
+__device__ __forceinline__ double intensity_at(const PlainStepArgs &a, int64_t n, double v1, double v2)
+{
+    const double th = fmod(-a.ang_old[n] + 2.0 * kPi, 2.0 * kPi); // RotationMatrix(angle).Inverse()
+    const double sn = approx_sin(th), cs = approx_cos(th);
+    const double w1 = v1 * cs - v2 * sn, w2 = v1 * sn + v2 * cs;
+    double dd = (double)a.ng * approx_phi(w1, w2) / (2.0 * kPi); // InterpolationGrid::d
+    dd = dd < 1e-8 ? 1e-8 : ((double)a.ng - 1e-8 < dd ? (double)a.ng - 1e-8 : dd);
+    const int g0 = (int)floor(dd) % a.ng, g1 = (g0 + 1) % a.ng;
+    const IgRow R0 = a.ig_rows[g0], R1 = a.ig_rows[g1];
+    const int idx0[4] = {R0.idx.x, R0.idx.y, R0.idx.z, R0.idx.w};
+    const int idx1[4] = {R1.idx.x, R1.idx.y, R1.idx.z, R1.idx.w};
+    const double w0[4] = {R0.w01.x, R0.w01.y, R0.w23.x, R0.w23.y};
+    const double wr1[4] = {R1.w01.x, R1.w01.y, R1.w23.x, R1.w23.y};
+    double value0 = 0, value1 = 0;
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+    {
+        value0 += w0[k] * __ldg(a.Iin + (int64_t)idx0[k] * a.g.nxy + n);
+        value1 += wr1[k] * __ldg(a.Iin + (int64_t)idx1[k] * a.g.nxy + n);
+    }
+    const double t = dd - (double)g0;
+    const double v = value0 * (1.0 - t) + value1 * t;
+    return (0.0 < v) ? v : 0.0;
+}
+
+// One stream value of adaptive streaming: StreamFlatAdaptive
+// (src/Radiation.cpp:415-452) or StreamCurvedAdaptive (:513-575), for the
+// cell's direction d rotated by the cell's new angle (sine sc, cosine cc).
+template <bool CURVED>
+__device__ __forceinline__ double stream_value_adaptive(const PlainStepArgs &a, int d, int64_t i, int64_t j,
+                                                        int64_t ij, double sc, double cc)
+{
+    const int64_t nx = a.g.nx;
+    const double cx = __ldg(a.cx + d), cy = __ldg(a.cy + d);
+    const double dir1 = cx * cc - cy * sc, dir2 = cx * sc + cy * cc;
+    double it, jt, v1, v2, s3 = 1.0;
+    if constexpr (CURVED)
+    {
+        const double phi = approx_phi(dir1, dir2);
+        const int64_t fs = a.g.nxy * a.nf;
+        const double *cf = a.coef + ij * a.nf;
+        const double sh = fourier_value(cf, a.nf, phi);
+        const double xt = fourier_value(cf + fs, a.nf, phi);
+        const double yt = fourier_value(cf + 2 * fs, a.nf, phi);
+        v1 = fourier_value(cf + 3 * fs, a.nf, phi);
+        v2 = fourier_value(cf + 4 * fs, a.nf, phi);
+        if (dev_inside_bh(a.g, xt, yt))
+            return 0.0;
+        it = (xt - a.g.startx) / a.g.dx;
+        jt = (yt - a.g.starty) / a.g.dy;
+        s3 = sh * (sh * sh);
+    }
+    else
+    {
+        double xt = a.g.startx + (double)i * a.g.dx, yt = a.g.starty + (double)j * a.g.dy;
+        xt -= dir1 * a.g.dt;
+        yt -= dir2 * a.g.dt;
+        it = (xt - a.g.startx) / a.g.dx;
+        jt = (yt - a.g.starty) / a.g.dy;
+        v1 = dir1;
+        v2 = dir2;
+    }
+    // corners kept on the grid whatever the departure
+    const int64_t i0 = min(max((int64_t)floor(it), (int64_t)0), nx - 2);
+    const int64_t j0 = min(max((int64_t)floor(jt), (int64_t)0), a.g.ny - 2);
+    const double al = CURVED ? __ldg(a.alpha + ij) : 1.0;
+    double Iq[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) // corners 00, 01, 10, 11
+    {
+        const int64_t n = (i0 + (q >> 1)) + (j0 + (q & 1)) * nx;
+        double v = intensity_at(a, n, v1, v2);
+        if (CURVED)
+        {
+            const double rr = al / __ldg(a.alpha + n);
+            v = rr * (rr * rr) * v;
+        }
+        Iq[q] = v;
+    }
+    const double fx = it - (double)i0, fy = jt - (double)j0;
+    const double f0 = Iq[0] * (1.0 - fx) + Iq[2] * fx;
+    const double f1 = Iq[1] * (1.0 - fx) + Iq[3] * fx;
+    const double bil = f0 * (1.0 - fy) + f1 * fy;
+    return CURVED ? s3 * bil : bil;
+}
+
 // RECORD: also writes what the adjoint needs about this step -- per (d, c)
 // the corner clamp mask, per cell the lambda-iteration count and the first
-// iterate's E -- without changing any result.
-template <bool CURVED, bool RECORD>
+// iterate's E -- without changing any result.  ADAPTIVE: the adaptive
+// streaming types -- each cell's stencil is rotated by its new angle (its
+// directions in stream, moments and collide) and corners are read in their
+// previous frames.
+template <bool CURVED, bool RECORD, bool ADAPTIVE>
 __global__ void __launch_bounds__(kStepBlock, GRLBM_PLAIN_MIN_BLOCKS) k_step_plain(PlainStepArgs a, StepRecord rec)
 {
     const int t = threadIdx.x;
@@ -180,6 +294,16 @@ __global__ void __launch_bounds__(kStepBlock, GRLBM_PLAIN_MIN_BLOCKS) k_step_pla
     // slots until the lambda iteration has converged (nothing else reads or
     // writes them in this step); non-colliding cells keep their slots.
     double *Is = a.Iout + ij;
+    // the cell's rotation (RotationMatrix(rotationAngle[ij]), src/DataTypes.hh:630-635)
+    double rot_s = 0.0, rot_c = 1.0;
+    if (ADAPTIVE)
+    {
+        const double th = a.ang_new[ij];
+        rot_s = approx_sin(th);
+        rot_c = approx_cos(th);
+    }
+#define GRLBM_N1(d) (ADAPTIVE ? __ldg(a.cx + (d)) * rot_c - __ldg(a.cy + (d)) * rot_s : __ldg(a.n1 + (d)))
+#define GRLBM_N2(d) (ADAPTIVE ? __ldg(a.cx + (d)) * rot_s + __ldg(a.cy + (d)) * rot_c : __ldg(a.n2 + (d)))
 
     Moments m;
     m.zero();
@@ -187,20 +311,23 @@ __global__ void __launch_bounds__(kStepBlock, GRLBM_PLAIN_MIN_BLOCKS) k_step_pla
     // past the end)
     const double4 *rp = a.rec + cc;
     double4 r0 = make_double4(0, 0, 0, 0);
-    if (CURVED)
+    if (CURVED && !ADAPTIVE)
         r0 = rp[0];
     for (int d = 0; d < a.nd; d++)
     {
         double4 r1 = r0;
-        if (CURVED)
+        if (CURVED && !ADAPTIVE)
             r1 = rp[(int64_t)min(d + 1, a.nd - 1) * a.g.ncell];
         unsigned cm = 0xFu;
-        const double val = (active && !zero_stream) ? stream_value<CURVED>(a, d, r0, i, j, ij, cm) : 0.0;
+        double val = 0.0;
+        if (active && !zero_stream)
+            val = ADAPTIVE ? stream_value_adaptive<CURVED>(a, d, i, j, ij, rot_s, rot_c)
+                           : stream_value<CURVED>(a, d, r0, i, j, ij, cm);
         if (RECORD && active)
             rec.clamp[(int64_t)d * a.g.ncell + cc] = (uint8_t)cm;
         if (collides)
             Is[(int64_t)d * nxy] = val;
-        m.add(__ldg(a.w + d), val, __ldg(a.n1 + d), __ldg(a.n2 + d));
+        m.add(__ldg(a.w + d), val, GRLBM_N1(d), GRLBM_N2(d));
         r0 = r1;
     }
 
@@ -240,7 +367,7 @@ __global__ void __launch_bounds__(kStepBlock, GRLBM_PLAIN_MIN_BLOCKS) k_step_pla
 #pragma unroll 4
                 for (int d = 0; d < a.nd; d++)
                 {
-                    const double n1 = __ldg(a.n1 + d), n2 = __ldg(a.n2 + d);
+                    const double n1 = GRLBM_N1(d), n2 = GRLBM_N2(d);
                     const double num = Is[(int64_t)d * nxy] + adt * (eta + (k0fE + k3 * (n1 * fFx + n2 * fFy)));
                     const double v = fast_div ? div_rn(num, den, rden) : num / den;
                     m.add(__ldg(a.w + d), v, n1, n2);
@@ -249,7 +376,7 @@ __global__ void __launch_bounds__(kStepBlock, GRLBM_PLAIN_MIN_BLOCKS) k_step_pla
             else
                 for (int d = 0; d < a.nd; d++)
                 {
-                    const double n1 = __ldg(a.n1 + d), n2 = __ldg(a.n2 + d);
+                    const double n1 = GRLBM_N1(d), n2 = GRLBM_N2(d);
                     const double v = collide_value(Is[(int64_t)d * nxy], n1, n2, u1, u2, lor, adt, eta, k0, k3,
                                                    kak0, fE, fFx, fFy);
                     m.add(__ldg(a.w + d), v, n1, n2);
@@ -264,14 +391,14 @@ __global__ void __launch_bounds__(kStepBlock, GRLBM_PLAIN_MIN_BLOCKS) k_step_pla
             const double k0fE = k0 * fE;
             for (int d = 0; d < a.nd; d++)
             {
-                const double n1 = __ldg(a.n1 + d), n2 = __ldg(a.n2 + d);
+                const double n1 = GRLBM_N1(d), n2 = GRLBM_N2(d);
                 const double num = Is[(int64_t)d * nxy] + adt * (eta + (k0fE + k3 * (n1 * fFx + n2 * fFy)));
                 Is[(int64_t)d * nxy] = fast_div ? div_rn(num, den, rden) : num / den;
             }
         }
         else
             for (int d = 0; d < a.nd; d++)
-                Is[(int64_t)d * nxy] = collide_value(Is[(int64_t)d * nxy], __ldg(a.n1 + d), __ldg(a.n2 + d), u1, u2,
+                Is[(int64_t)d * nxy] = collide_value(Is[(int64_t)d * nxy], GRLBM_N1(d), GRLBM_N2(d), u1, u2,
                                                      lor, adt, eta, k0, k3, kak0, fE, fFx, fFy);
     }
     if (RECORD && active)
@@ -298,19 +425,69 @@ __global__ void __launch_bounds__(kStepBlock, GRLBM_PLAIN_MIN_BLOCKS) k_step_pla
         atomicAdd(a.iter_sum, (unsigned long long)sum);
         atomicMax(a.iter_max, mx);
     }
+#undef GRLBM_N1
+#undef GRLBM_N2
+}
+
+// UpdateRotationMatrizes (src/Radiation.cpp:361-378): for the interior cells
+// of the slab, the angle of the flux averaged over the 3x3 neighbourhood
+// where at least 1% of the light moves along it, else the previous angle.
+__global__ void k_rotation_update(GridDev g, const double *mom, const double *ang_old, double *ang_new)
+{
+    const int64_t c0 = (g.jlo - 1) * g.nx_;
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= (g.jhi - g.jlo) * g.nx_)
+        return;
+    const int64_t cc = c0 + c;
+    const int64_t i = 1 + cc % g.nx_, j = 1 + cc / g.nx_;
+    const int64_t ij = i + j * g.nx, nxy = g.nxy;
+    double fx = 0.0, fy = 0.0;
+    for (int b = -1; b <= 1; b++)
+        for (int a = -1; a <= 1; a++)
+        {
+            const int64_t n = (i + a) + (j + b) * g.nx;
+            fx += mom[n + nxy];
+            fy += mom[n + 2 * nxy];
+        }
+    fx /= 9.0;
+    fy /= 9.0;
+    const double norm = sqrt(fx * fx + fy * fy);
+    const double E = mom[ij];
+    ang_new[ij] = (E > 1e-16 && norm / E > 0.01) ? approx_phi(fx, fy) : ang_old[ij];
+}
+
+// The moments at the halo nodes, which the reference recomputes after every
+// stream from intensities it never writes there (zero).
+__global__ void k_zero_halo_moments(GridDev g, double *mom)
+{
+    const int64_t ij = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (ij >= g.nxy)
+        return;
+    const int64_t i = ij % g.nx, j = ij / g.nx;
+    if (i == 0 || i == g.nx - 1 || j == 0 || j == g.ny - 1)
+        for (int q = 0; q < 6; q++)
+            mom[ij + q * g.nxy] = 0.0;
 }
 
 // Radiation::ComputeMomentsIF (src/Radiation.cpp:239-269): the six moments
 // of the current intensities at every node, halo included, in the
 // reference's order.  The precision form's state is converted back to I
 // (J / (1 / alpha^3)) first.
+// With `ang` (adaptive streaming) the directions are the stencil's rotated
+// by each node's angle, n1/n2 then holding the unrotated directions.
 template <typename T>
 __global__ void k_moments_from_I(const T *I, int64_t nxy, int nd, const double *w, const double *n1,
-                                 const double *n2, const float *scale, double *mom)
+                                 const double *n2, const float *scale, const double *ang, double *mom)
 {
     const int64_t ij = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (ij >= nxy)
         return;
+    double rs = 0.0, rc = 1.0;
+    if (ang)
+    {
+        rs = approx_sin(ang[ij]);
+        rc = approx_cos(ang[ij]);
+    }
     Moments m;
     m.zero();
     for (int d = 0; d < nd; d++)
@@ -321,7 +498,11 @@ __global__ void k_moments_from_I(const T *I, int64_t nxy, int nd, const double *
         double v = (double)I[(int64_t)d * nxy + ij];
         if (scale)
             v = v / (double)scale[ij];
-        m.add(wd, v, __ldg(n1 + d), __ldg(n2 + d));
+        const double c1 = __ldg(n1 + d), c2 = __ldg(n2 + d);
+        if (ang)
+            m.add(wd, v, c1 * rc - c2 * rs, c1 * rs + c2 * rc);
+        else
+            m.add(wd, v, c1, c2);
     }
     mom[ij] = m.E;
     mom[ij + nxy] = m.Fx;
@@ -504,17 +685,26 @@ void launch_step_plain(const PlainStepArgs &a, bool curved, cudaStream_t s, cons
         return;
     const StepRecord none{};
     const unsigned blocks = nblk(cells, kStepBlock);
-    if (record)
+    if (a.ang_new) // adaptive streaming
+    {
+        k_rotation_update<<<nblk(cells, 128), 128, 0, s>>>(a.g, a.mom, a.ang_old, const_cast<double *>(a.ang_new));
+        if (curved)
+            k_step_plain<true, false, true><<<blocks, kStepBlock, smem, s>>>(a, none);
+        else
+            k_step_plain<false, false, true><<<blocks, kStepBlock, smem, s>>>(a, none);
+        k_zero_halo_moments<<<nblk(a.g.nxy, 256), 256, 0, s>>>(a.g, a.mom);
+    }
+    else if (record)
     {
         if (curved)
-            k_step_plain<true, true><<<blocks, kStepBlock, smem, s>>>(a, *record);
+            k_step_plain<true, true, false><<<blocks, kStepBlock, smem, s>>>(a, *record);
         else
-            k_step_plain<false, true><<<blocks, kStepBlock, smem, s>>>(a, *record);
+            k_step_plain<false, true, false><<<blocks, kStepBlock, smem, s>>>(a, *record);
     }
     else if (curved)
-        k_step_plain<true, false><<<blocks, kStepBlock, smem, s>>>(a, none);
+        k_step_plain<true, false, false><<<blocks, kStepBlock, smem, s>>>(a, none);
     else
-        k_step_plain<false, false><<<blocks, kStepBlock, smem, s>>>(a, none);
+        k_step_plain<false, false, false><<<blocks, kStepBlock, smem, s>>>(a, none);
 }
 void launch_sources64(double *I, int64_t nxy, int nd, const int64_t *nodes, const double *vals, int64_t nsrc,
                       cudaStream_t s)
@@ -563,14 +753,14 @@ void launch_to_cellmajor32(const float *in, double *out, int64_t nxy, int nd, co
     k_to_cellmajor<float><<<dim3(nblk(nxy, 32), nblk(nd, 32)), dim3(32, 8), 0, s>>>(in, out, nxy, nd, scale);
 }
 void launch_moments_from_I64(const double *I, int64_t nxy, int nd, const double *w, const double *n1,
-                             const double *n2, double *mom, cudaStream_t s)
+                             const double *n2, const double *ang, double *mom, cudaStream_t s)
 {
-    k_moments_from_I<double><<<nblk(nxy, 128), 128, 0, s>>>(I, nxy, nd, w, n1, n2, nullptr, mom);
+    k_moments_from_I<double><<<nblk(nxy, 128), 128, 0, s>>>(I, nxy, nd, w, n1, n2, nullptr, ang, mom);
 }
 void launch_moments_from_I32(const float *J, int64_t nxy, int nd, const double *w, const double *n1,
                              const double *n2, const float *scale, double *mom, cudaStream_t s)
 {
-    k_moments_from_I<float><<<nblk(nxy, 128), 128, 0, s>>>(J, nxy, nd, w, n1, n2, scale, mom);
+    k_moments_from_I<float><<<nblk(nxy, 128), 128, 0, s>>>(J, nxy, nd, w, n1, n2, scale, nullptr, mom);
 }
 void launch_widen32(const float *in, double *out, int64_t n, cudaStream_t s)
 {

@@ -36,7 +36,7 @@ import math
 import numpy as np
 
 MINKOWSKI, SCHWARZSCHILD, KERRSCHILD = 0, 1, 2
-FLAT_FIXED, CURVED_FIXED = 0, 2
+FLAT_FIXED, FLAT_ADAPTIVE, CURVED_FIXED, CURVED_ADAPTIVE = 0, 1, 2, 3
 MOMENTS, INTENSITIES = 0, 1
 
 _GOLDEN = np.uint64(0x9E3779B97F4A7C15)

@@ -53,7 +53,9 @@ extern "C" {
 #define GRLBM_SCHWARZSCHILD 1
 #define GRLBM_KERRSCHILD 2
 
-/* StreamingType (src/Config.hh:5-12); only the two fixed types are built */
+/* StreamingType (src/Config.hh:5-12).  FlatFixed and CurvedFixed are built for
+ * both arithmetic forms, FlatAdaptive and CurvedAdaptive for GRLBM_PLAIN_FP64;
+ * GeodesicFixed (a performance test of the reference) is not built. */
 #define GRLBM_FLAT_FIXED 0
 #define GRLBM_FLAT_ADAPTIVE 1
 #define GRLBM_CURVED_FIXED 2
@@ -142,6 +144,11 @@ int grlbm_set_fields(grlbm_ctx *ctx, const double *kappa0, const double *kappa1,
 int grlbm_set_initial_data(grlbm_ctx *ctx, const uint8_t *is_initial, const double *initial_I,
                            const double *E_LF, const double *Fx_LF, const double *Fy_LF,
                            const double *Pxx_LF, const double *Pxy_LF, const double *Pyy_LF);
+/* initialFluxAngle_IF (src/Radiation.h:39, nx*ny): the rotation angles
+ * LoadInitialData gives the source nodes under the adaptive streaming types
+ * with InitialDataType::Intensities (default 0).  Call before
+ * grlbm_set_initial_data. */
+int grlbm_set_initial_flux_angle(grlbm_ctx *ctx, const double *angle);
 /* Radiation::LoadInitialData (src/Radiation.cpp:128-182): writes the source
  * intensities into the current intensity buffer. */
 int grlbm_load_initial_data(grlbm_ctx *ctx);

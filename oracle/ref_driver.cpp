@@ -201,6 +201,14 @@ extern "C" int ref_run(const grlbm_ref_params *p, const grlbm_ref_inputs *in, gr
             case StreamingType::CurvedFixed:
                 r.StreamCurvedFixed();
                 break;
+            case StreamingType::FlatAdaptive:
+                r.UpdateRotationMatrizes();
+                r.StreamFlatAdaptive();
+                break;
+            case StreamingType::CurvedAdaptive:
+                r.UpdateRotationMatrizes();
+                r.StreamCurvedAdaptive();
+                break;
             default:
                 return -2;
             }

@@ -48,3 +48,29 @@ def test_tables_rebuilt_every_step(grlbm, W):
         Eb = b.moments_if()["E"]
         assert b.stats()["table_ms"] > 0
     assert np.array_equal(Ea, Eb)
+
+
+def test_adaptive_run_simulation_frames_match_reference(grlbm, W, oracle, tmp_path):
+    """The same with FlatAdaptive streaming: the frames' moments use each
+    node's rotated stencil, and the moments a frame computes feed the next
+    rotation update, as in the reference."""
+    if not oracle.available("ref_strict"):
+        pytest.skip("the reference build is absent")
+    case = W.flat_beam(nx_=30, ny_=24, n_dir=12, steps=23)
+    case["streaming_type"] = W.FLAT_ADAPTIVE
+    work = tmp_path / "ref" / "run"
+    work.mkdir(parents=True)
+    with grlbm.prepare(case) as r:
+        period = 5.5 * r.dt
+        try:
+            oracle.set_frames("ref_strict", period, str(work))
+            oracle.run(case, "ref_strict", use_run_simulation=True)
+        finally:
+            oracle.set_frames("ref_strict", None, None)
+        ours = tmp_path / "ours"
+        r.run_simulation((int(case["n_steps"]) - 0.5) * r.dt, period, str(ours) + "/")
+    ref_dir = tmp_path / "ref" / "output" / "ref_run" / "Moments"
+    a, b = sorted(os.listdir(ours)), sorted(os.listdir(ref_dir))
+    assert a == b and len(a) >= 5
+    for name in a:
+        assert (ours / name).read_bytes() == (ref_dir / name).read_bytes(), name
