@@ -67,6 +67,8 @@ def args_parse():
     p.add_argument("--nx", type=int, default=400)
     p.add_argument("--dirs", type=int, default=64)
     p.add_argument("--fourier", type=int, default=16)
+    p.add_argument("--no-configs", action="store_true",
+                   help="skip the flat-beam and curved-shell configurations")
     p.add_argument("--adjoint-steps", type=int, default=200,
                    help="steps of the adjoint workload (256^2 x 48, checkpoints every 20); 0 skips it")
     p.add_argument("--batch-steps", type=int, default=64,
@@ -222,6 +224,40 @@ def open_form(G, case, prec, world, rank, local, pg):
     return r, (lambda: slab.step(1)), slab
 
 
+def run_configs(G, W, local):
+    """The two smaller configurations at their full sizes: the flat beam
+    (100^2 x 20, 500 steps, plain form) and the curved shell (200^2 x 32, 1000
+    steps, both forms, with the FP32 form's relative error of E).  Device time
+    of the whole run with CUDA events (graph-replayed steps, inputs resident,
+    no L2 flush: these problems fit in L2)."""
+    import torch
+    out = {}
+    for name, case, forms in (
+            ("flat_beam 100x100 x 20 directions, 500 steps", W.flat_beam(), (G.PLAIN_FP64,)),
+            ("curved_shell 200x200 x 32 directions, Fourier order 5, 1000 steps", W.curved_shell(),
+             (G.PLAIN_FP64, G.PRECISION_FP32))):
+        n = int(case["n_steps"])
+        units = int(case["nx_"]) * int(case["ny_"]) * int(case["n_dir"]) * n
+        res, E = {}, {}
+        for prec in forms:
+            with G.prepare(case, prec, device=local) as r:
+                ext = torch.cuda.ExternalStream(r.stream)
+                with torch.cuda.stream(ext):
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record(ext)
+                    r.step_async(n)
+                    e1.record(ext)
+                    ext.synchronize()
+                key = "fp64" if prec == G.PLAIN_FP64 else "fp32"
+                res[key] = units / (e0.elapsed_time(e1) / 1e3)
+                E[key] = r.moments_if()["E"]
+        entry = {"cell_dir_per_s": res}
+        if "fp32" in E:
+            entry["E_rel_l2_fp32_vs_fp64"] = float(np.linalg.norm(E["fp32"] - E["fp64"]) / np.linalg.norm(E["fp64"]))
+        out[name] = entry
+    return out
+
+
 def run_batched(G, W, a, local):
     """The batched form on 64 uneven problems (grid 64^2..512^2, 16..64
     directions, flat or Schwarzschild, seed 10): after autotuning, `batch_steps`
@@ -364,6 +400,7 @@ def run_grlbm(a, world, rank, local, pg):
             r.close()
         e2e_s = max_over_ranks(statistics.median(e2e_t) if e2e_t else float("nan"), pg, dev)
         batched = run_batched(G, W, a, local) if a.batch_steps > 0 and world == 1 else None
+        other = run_configs(G, W, local) if not a.no_configs and world == 1 else None
         adjoint = run_adjoint(G, W, a, local) if a.adjoint_steps > 0 and world == 1 else None
     clocks = clk.summary()
 
@@ -439,6 +476,7 @@ def run_grlbm(a, world, rank, local, pg):
         },
         "gpu_launches": a.steps,
         "batched": batched,
+        "other_configs": other,
         "adjoint": adjoint,
         "clocks": clocks,
     }
