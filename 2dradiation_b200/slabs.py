@@ -55,6 +55,9 @@ class RadiationRows:
     def step(self, n: int = 1):
         self.rad.step_async(n)
 
+    def energy(self) -> float:
+        return self.rad.energy()  # grlbm_energy: the band's interior cells
+
 
 class Slab:
     """One rank's band and its exchange with the neighbouring bands.
@@ -112,6 +115,14 @@ class Slab:
         for _ in range(n):
             self.exchange()
             self.state.step(1)
+
+    def energy(self) -> float:
+        """The global energy: the bands' FP64 sums added by one all-reduce."""
+        e = torch.tensor([self.state.energy()], dtype=torch.float64,
+                         device=self.state.device if self.state.stream is not None else "cpu")
+        if self.world > 1:
+            dist.all_reduce(e, group=self.group)
+        return float(e.item())
 
 
 class _Null:

@@ -27,6 +27,7 @@ def test_bands_reproduce_whole_grid(grlbm, W, precision, maker, kw):
         whole.step(steps)
         ref = whole.moments_if()
         refI = whole.intensity().reshape(whole.nxy, whole.nd)
+        ref_energy = whole.energy()
     world = 3
     bands = S.partition(int(case["ny_"]), world)
     rads = [grlbm.prepare(case, precision) for _ in range(world)]
@@ -60,6 +61,9 @@ def test_bands_reproduce_whole_grid(grlbm, W, precision, maker, kw):
             for k in ("E", "Fx", "Fy", "Pxx", "Pxy", "Pyy"):
                 assert np.array_equal(m[k][rows], ref[k][rows]), (k, lo, hi)
             assert np.array_equal(I[rows], refI[rows])
+        # the bands' energies (grlbm_energy over each band) add up to the whole grid's
+        total = sum(r.energy() for r in rads)
+        assert abs(total - ref_energy) <= 1e-12 * abs(ref_energy)
     finally:
         for r in rads:
             r.close()

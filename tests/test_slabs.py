@@ -51,6 +51,10 @@ class CpuRows:
         else:
             self.state[:, j:j + n, :] = view
 
+    def energy(self):
+        lo, hi = self.band
+        return float(self.state[:, lo:hi, 1:-1].sum())
+
     def step(self, n=1):
         g, (lo, hi) = self.ghost, self.band
         s = self.state
@@ -72,6 +76,7 @@ def _worker(rank, world, port, nx, ny_, nd, ghost, steps, out):
         slab = S.Slab(rows, rank, world, ny_, ghost)
         slab.step(steps)
         out[rank] = rows.state[:, band[0]:band[1], :].clone()
+        out[("energy", rank)] = slab.energy()
     finally:
         dist.destroy_process_group()
 
@@ -99,4 +104,8 @@ def test_two_rank_exchange_equals_one_rank(ghost):
             p.join(120)
             assert p.exitcode == 0
         got = torch.cat([out[0], out[1]], dim=1)
+        energies = (out[("energy", 0)], out[("energy", 1)])
     assert torch.equal(got, single.state[:, 1:ny_ + 1, :])
+    # the all-reduced energy is the same on both ranks and is the whole grid's
+    assert energies[0] == energies[1]
+    assert abs(energies[0] - single.energy()) <= 1e-12 * abs(single.energy())
