@@ -8,10 +8,12 @@
 // (src/Radiation.cpp:502-505, 342); as alpha_n^-3 > 0 commutes with the clamp,
 // gathering J gives the same value without loading alpha at every corner.
 //
-// Stream: one thread per interior cell loops over the directions; each
-// (cell, direction) reads a 16-byte record and a 48-byte angular row (the
-// two cubic rows of IntensityAt pre-blended into a 5-direction window whose
-// weights are W0 + t D), gathers the window at the 4 bilinear corners and
+// Stream: one thread per interior cell loops over the directions, staged in
+// shared memory a chunk of planes at a time; each (cell, direction) reads its
+// 16-byte packed record (window row type, window start, blend t, corner code,
+// fx, fy, s^3 alpha_c^3), takes the window's weights W0 + t D from the
+// row-type table (the two cubic rows of IntensityAt pre-blended into a
+// 5-direction window), gathers the window at the 4 bilinear corners and
 // multiplies by s^3 alpha_c^3.  Offsets are 32-bit.
 //
 // Collide: the lambda iteration of src/Radiation.cpp:661-722 is affine in

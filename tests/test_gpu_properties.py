@@ -88,7 +88,7 @@ def test_precision_form_against_oracle(maker, kw, grlbm, W, oracle):
     ("flat_beam", dict(nx_=50, ny_=30, n_dir=20, steps=40)),
 ])
 def test_precision_form_edge_shapes(maker, kw, grlbm, W):
-    """The FP32 form (shared-memory staged stream, analytic angular weights)
+    """The FP32 form (shared-memory staged stream, packed records, row-type weights)
     against the FP64 form, on problems whose result is stable under rounding
     (no scattering fluid at rest: see test_gpu_parity)."""
     case = W.make_case(maker, **kw)
