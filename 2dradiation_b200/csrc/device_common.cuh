@@ -14,7 +14,11 @@
 //                        compact records, moment-space lambda iteration
 //
 // Device layouts (one problem, all in HBM):
-//   intensities  I[d * nxy + ij]          direction-major, two buffers
+//   intensities  I[d * plane + i + j * pitch]  direction-major, two buffers;
+//                                         FP64: pitch = nx, plane = nxy; FP32: pitch =
+//                                         nx rounded up to 4 floats, plane = pitch * ny
+//                                         (every row starts on a 16-byte boundary, as
+//                                         the step's TMA tensor copies need)
 //   plain record rec64[d * ncell + c]     {i_dep, j_dep, angle coordinate, s^3}
 //                                         (absolute grid coordinates of the
 //                                         departure point; angle < 0 marks a
@@ -32,6 +36,7 @@
 //   alpha cubes  acube[ij * 9 + 3(dj+1) + (di+1)] = (alpha_ij / alpha_n)^3 for
 //                                         the 3x3 neighbours n of interior ij
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstddef>
@@ -53,6 +58,20 @@ static_assert(RF_COUNT <= kRkStride, "rk pack stride");
 constexpr int kStepBlock = 128;
 constexpr int kMaxDirs = 256;
 constexpr int kMaxFourier = 64;
+
+// Where node ij = i + j nx of a direction plane sits in a state buffer.
+struct StateLayout
+{
+    int64_t nx, pitch, plane; // grid row length, state row pitch, plane stride (elements)
+    __host__ __device__ int64_t at(int64_t ij) const { return pitch == nx ? ij : ij + (ij / nx) * (pitch - nx); }
+    static StateLayout dense(int64_t nx, int64_t ny) { return StateLayout{nx, nx, nx * ny}; }
+    // FP32 state: rows padded to 16 bytes
+    static StateLayout padded32(int64_t nx, int64_t ny)
+    {
+        const int64_t pitch = (nx + 3) & ~(int64_t)3;
+        return StateLayout{nx, pitch, pitch * ny};
+    }
+};
 
 struct GridDev
 {
@@ -188,6 +207,9 @@ struct PrecStepArgs
     float *mom;               // 6*nxy
     unsigned long long *iter_sum;
     unsigned int *iter_max;
+    unsigned pitch, plane;    // state row pitch (a multiple of 4 floats) and plane stride
+    unsigned *fault;          // set to 1 when a staging copy does not land within its time limit
+    CUtensorMap in_map;       // TMA map of Iin: 2D, {pitch, ny * nd} floats, box of one patch plane
 };
 
 // Direction tables of the precision form, passed by value as a kernel
@@ -278,6 +300,9 @@ cudaError_t prepare_step_plain(int smem_bytes);
 void launch_step_plain(const PlainStepArgs &a, bool curved, cudaStream_t s, const StepRecord *record = nullptr);
 cudaError_t prepare_step_prec(int smem_bytes);
 size_t step_prec_smem(int nd);
+// The TMA map the precision step stages Iin through (a state buffer of
+// layout L and nd planes over ny rows each).
+cudaError_t encode_state_map(CUtensorMap *map, const float *state, const StateLayout &L, int64_t ny, int nd);
 void launch_step_prec(const PrecStepArgs &a, const DirTable &dt, bool curved, cudaStream_t s);
 int step_prec_tiles_x(int64_t nx_);
 int step_prec_tiles_y(int64_t rows);
@@ -287,7 +312,7 @@ void launch_step_batch(const BatchItem *items, const int *first_tile, int n_item
 
 void launch_sources64(double *I, int64_t nxy, int nd, const int64_t *nodes, const double *vals, int64_t nsrc,
                       cudaStream_t s);
-void launch_sources32(float *I, int64_t nxy, int nd, const int64_t *nodes, const float *vals, int64_t nsrc,
+void launch_sources32(float *I, const StateLayout &L, int nd, const int64_t *nodes, const float *vals, int64_t nsrc,
                       cudaStream_t s);
 void launch_moments_lf64(int64_t nxy, const double *mom, const double *lfp, const uint8_t *bh, double *out,
                          cudaStream_t s);
@@ -296,15 +321,17 @@ void launch_moments_lf32(int64_t nxy, const float *mom, const double *lfp, const
 void launch_energy64(const GridDev &g, const double *E, double *partial, int nblocks, double *out, cudaStream_t s);
 void launch_energy32(const GridDev &g, const float *E, double *partial, int nblocks, double *out, cudaStream_t s);
 void launch_to_dirmajor64(const double *in, double *out, int64_t nxy, int nd, cudaStream_t s);
-void launch_to_dirmajor32(const double *in, float *out, int64_t nxy, int nd, const float *scale, cudaStream_t s);
+void launch_to_dirmajor32(const double *in, float *out, int64_t nxy, const StateLayout &L, int nd,
+                          const float *scale, cudaStream_t s);
 void launch_to_cellmajor64(const double *in, double *out, int64_t nxy, int nd, cudaStream_t s);
-void launch_to_cellmajor32(const float *in, double *out, int64_t nxy, int nd, const float *scale, cudaStream_t s);
+void launch_to_cellmajor32(const float *in, double *out, int64_t nxy, const StateLayout &L, int nd,
+                           const float *scale, cudaStream_t s);
 void launch_widen32(const float *in, double *out, int64_t n, cudaStream_t s);
 // ComputeMomentsIF from the current intensities (FP64 out, 6 * nxy)
 // (ang: per-node rotation angles of adaptive streaming, with n1/n2 the
 // unrotated stencil directions; null otherwise)
 void launch_moments_from_I64(const double *I, int64_t nxy, int nd, const double *w, const double *n1,
                              const double *n2, const double *ang, double *mom, cudaStream_t s);
-void launch_moments_from_I32(const float *J, int64_t nxy, int nd, const double *w, const double *n1,
-                             const double *n2, const float *scale, double *mom, cudaStream_t s);
+void launch_moments_from_I32(const float *J, int64_t nxy, const StateLayout &L, int nd, const double *w,
+                             const double *n1, const double *n2, const float *scale, double *mom, cudaStream_t s);
 } // namespace grlbm

@@ -54,6 +54,9 @@ struct grlbm_ctx
     MetricArrays M;
     bool fp32 = false;
     GridDev gd{};
+    StateLayout sl{};          // node positions in the state buffers
+    CUtensorMap in_map[2];     // precision form: TMA maps of the state buffers
+    unsigned *fault = nullptr; // mapped host word: a precision step's staging wait timed out
     int64_t ncell = 0;
     int ng = 0;
     // device buffers (storage type T = double for the plain form, float for the precision form)
@@ -89,6 +92,8 @@ struct grlbm_ctx
                 cudaGraphExecDestroy(g);
         if (stream)
             cudaStreamDestroy(stream);
+        if (fault)
+            cudaFreeHost(fault);
     }
 };
 
@@ -123,6 +128,17 @@ int fail(grlbm_ctx *c, int code, const char *fmt, ...)
         if (e_ != cudaSuccess)                                                                 \
             return fail(ctx, GRLBM_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_)); \
     } while (0)
+
+// The precision step gives up on a tile whose staged planes do not land
+// within the kernel's time limit and raises the context's fault word; the
+// state is then invalid.  Read after a stream synchronisation.
+int check_fault(grlbm_ctx *ctx)
+{
+    if (ctx->fault && *reinterpret_cast<volatile unsigned *>(ctx->fault))
+        return fail(ctx, GRLBM_ERR_CUDA,
+                    "a precision step's shared-memory staging did not complete within its time limit");
+    return GRLBM_OK;
+}
 
 int alloc(grlbm_ctx *ctx, DevBuf &b, size_t bytes)
 {
@@ -202,6 +218,10 @@ PrecStepArgs prec_args(grlbm_ctx *ctx, int from)
     a.mom = ctx->mom.as<float>();
     a.iter_sum = cnt;
     a.iter_max = reinterpret_cast<unsigned int *>(cnt + 1);
+    a.pitch = (unsigned)ctx->sl.pitch;
+    a.plane = (unsigned)ctx->sl.plane;
+    a.fault = ctx->fault;
+    a.in_map = ctx->in_map[from];
     return a;
 }
 
@@ -256,7 +276,7 @@ int enqueue_step(grlbm_ctx *ctx, int from)
     if (ctx->fp32)
     {
         if (ctx->run.keep_source_nodes_active && ctx->nsrc > 0)
-            launch_sources32(ctx->I[from].as<float>(), ctx->gd.nxy, ctx->st.n, ctx->src_nodes.as<int64_t>(),
+            launch_sources32(ctx->I[from].as<float>(), ctx->sl, ctx->st.n, ctx->src_nodes.as<int64_t>(),
                              ctx->src_vals.as<float>(), ctx->nsrc, ctx->stream);
         const PrecStepArgs a = prec_args(ctx, from);
         launch_step_prec(a, ctx->dirs, curved, ctx->stream);
@@ -409,7 +429,7 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
     if (run->n_dir < 4 || run->n_dir > maxdir)
         return fail(nullptr, GRLBM_ERR_ARGUMENT, "n_dir must be in [4, %d]", maxdir);
     if (run->precision == GRLBM_PRECISION_FP32 &&
-        (double)(grid->nx_ + 2) * (double)(grid->ny_ + 2) * (double)run->n_dir >= 2147483648.0)
+        (double)StateLayout::padded32(grid->nx_ + 2, grid->ny_ + 2).plane * (double)run->n_dir >= 2147483648.0)
         return fail(nullptr, GRLBM_ERR_ARGUMENT, "the precision form indexes with 32 bits: nx*ny*n_dir must be < 2^31");
     if (run->n_fourier < 1 || run->n_fourier > kMaxFourier)
         return fail(nullptr, GRLBM_ERR_ARGUMENT, "n_fourier must be in [1, %d]", kMaxFourier);
@@ -681,7 +701,15 @@ std::vector<IgRow> rows(ctx->ng);
     TRY(upload(ctx, ctx->coef, identity_coefficients(ctx)));
 
     // state
-    const size_t ib = (size_t)nxy * nd * tsize(ctx);
+    ctx->sl = ctx->fp32 ? StateLayout::padded32(G.nx, G.ny) : StateLayout::dense(G.nx, G.ny);
+    const size_t ib = (size_t)ctx->sl.plane * nd * tsize(ctx);
+    if (ctx->fp32)
+    {
+        if (cudaHostAlloc(reinterpret_cast<void **>(&ctx->fault), sizeof(unsigned),
+                          cudaHostAllocMapped | cudaHostAllocPortable) != cudaSuccess)
+            return fail(nullptr, GRLBM_ERR_CUDA, "cudaHostAlloc of the fault word failed");
+        *ctx->fault = 0;
+    }
     TRY(alloc(ctx, ctx->I[0], ib));
     TRY(alloc(ctx, ctx->I[1], ib));
     TRY(alloc(ctx, ctx->mom, (size_t)6 * nxy * tsize(ctx)));
@@ -693,6 +721,13 @@ std::vector<IgRow> rows(ctx->ng);
     TRY(alloc(ctx, ctx->energy_out, sizeof(double)));
     cudaMemset(ctx->I[0].p, 0, ib);
     cudaMemset(ctx->I[1].p, 0, ib);
+    if (ctx->fp32)
+        for (int k = 0; k < 2; k++)
+        {
+            const cudaError_t e = encode_state_map(&ctx->in_map[k], ctx->I[k].as<float>(), ctx->sl, G.ny, nd);
+            if (e != cudaSuccess)
+                return fail(nullptr, GRLBM_ERR_CUDA, "TMA map of the state: %s", cudaGetErrorString(e));
+        }
     if (is_adaptive(ctx))
     {
         // rotationAngle and rotationAngleNew start at zero (src/Radiation.cpp:3-60)
@@ -846,7 +881,7 @@ int grlbm_load_initial_data(grlbm_ctx *ctx)
     for (int b = 0; b < 2; b++)
     {
         if (ctx->fp32)
-            launch_sources32(ctx->I[b].as<float>(), ctx->gd.nxy, ctx->st.n, ctx->src_nodes.as<int64_t>(),
+            launch_sources32(ctx->I[b].as<float>(), ctx->sl, ctx->st.n, ctx->src_nodes.as<int64_t>(),
                              ctx->src_vals.as<float>(), ctx->nsrc, ctx->stream);
         else
             launch_sources64(ctx->I[b].as<double>(), ctx->gd.nxy, ctx->st.n, ctx->src_nodes.as<int64_t>(),
@@ -889,7 +924,8 @@ int grlbm_set_intensity(grlbm_ctx *ctx, const double *I)
     for (int b = 0; b < 2; b++)
     {
         if (ctx->fp32)
-            launch_to_dirmajor32(ctx->stage.as<double>(), ctx->I[b].as<float>(), nxy, nd, state_scale(ctx), ctx->stream);
+            launch_to_dirmajor32(ctx->stage.as<double>(), ctx->I[b].as<float>(), nxy, ctx->sl, nd,
+                                 state_scale(ctx), ctx->stream);
         else
             launch_to_dirmajor64(ctx->stage.as<double>(), ctx->I[b].as<double>(), nxy, nd, ctx->stream);
     }
@@ -911,7 +947,7 @@ int grlbm_get_intensity(grlbm_ctx *ctx, double *I)
     if (rc)
         return rc;
     if (ctx->fp32)
-        launch_to_cellmajor32(ctx->I[ctx->cur].as<float>(), ctx->stage.as<double>(), nxy, nd, state_scale(ctx),
+        launch_to_cellmajor32(ctx->I[ctx->cur].as<float>(), ctx->stage.as<double>(), nxy, ctx->sl, nd, state_scale(ctx),
                               ctx->stream);
     else
         launch_to_cellmajor64(ctx->I[ctx->cur].as<double>(), ctx->stage.as<double>(), nxy, nd, ctx->stream);
@@ -1064,7 +1100,7 @@ int grlbm_sync(grlbm_ctx *ctx)
     if (!ctx)
         return GRLBM_ERR_ARGUMENT;
     CU(cudaStreamSynchronize(ctx->stream));
-    return GRLBM_OK;
+    return check_fault(ctx);
 }
 
 int grlbm_step(grlbm_ctx *ctx, int32_t n_steps)
@@ -1174,7 +1210,7 @@ int grlbm_write_frame_csv(grlbm_ctx *ctx, float time, const char *directory, con
     // (src/Radiation.cpp:239-301), as RunSimulation does before each frame
     const double *d64 = ctx->dirs64.as<double>();
     if (ctx->fp32)
-        launch_moments_from_I32(ctx->I[ctx->cur].as<float>(), nxy, nd, d64, d64 + nd, d64 + 2 * nd,
+        launch_moments_from_I32(ctx->I[ctx->cur].as<float>(), nxy, ctx->sl, nd, d64, d64 + nd, d64 + 2 * nd,
                                 state_scale(ctx), ctx->frame_mom.as<double>(), ctx->stream);
     else
     {
@@ -1290,7 +1326,7 @@ int grlbm_row_bytes(const grlbm_ctx *ctx, int64_t *bytes)
 {
     if (!ctx || !bytes)
         return GRLBM_ERR_ARGUMENT;
-    *bytes = ctx->geo.nx * (int64_t)ctx->st.n * (int64_t)tsize(ctx);
+    *bytes = ctx->sl.pitch * (int64_t)ctx->st.n * (int64_t)tsize(ctx);
     return GRLBM_OK;
 }
 
@@ -1304,8 +1340,8 @@ int grlbm_copy_rows(grlbm_ctx *ctx, int64_t j_first, int64_t n, void *buffer, in
     if (n == 0)
         return GRLBM_OK;
     cudaSetDevice(ctx->device);
-    const size_t es = tsize(ctx), width = (size_t)n * ctx->geo.nx * es, pitch = (size_t)ctx->geo.nxy * es;
-    char *state = static_cast<char *>(ctx->I[ctx->cur].p) + (size_t)j_first * ctx->geo.nx * es;
+    const size_t es = tsize(ctx), width = (size_t)n * ctx->sl.pitch * es, pitch = (size_t)ctx->sl.plane * es;
+    char *state = static_cast<char *>(ctx->I[ctx->cur].p) + (size_t)j_first * ctx->sl.pitch * es;
     if (to_buffer)
         CU(cudaMemcpy2DAsync(buffer, width, state, pitch, width, (size_t)ctx->st.n, cudaMemcpyDeviceToDevice,
                              ctx->stream));
@@ -1353,6 +1389,8 @@ int grlbm_get_stats(grlbm_ctx *ctx, grlbm_stats *s)
     unsigned long long h[5];
     CU(cudaStreamSynchronize(ctx->stream));
     CU(cudaMemcpy(h, ctx->counters.p, sizeof h, cudaMemcpyDeviceToHost));
+    if (int rc = check_fault(ctx))
+        return rc;
     s->steps = ctx->steps;
     s->max_iterations = (int32_t)(unsigned)(h[1] & 0xffffffffu);
     const double denom = (double)ctx->steps * (double)(ctx->geo.nx - 2) * (double)(ctx->gd.jhi - ctx->gd.jlo);
@@ -1581,6 +1619,9 @@ int batch_steps(grlbm_batch *b, int n)
         c->cur = b->items[k].cur0 ^ b->flip;
         c->steps += n;
     }
+    for (grlbm_ctx *c : b->ctx)
+        if (check_fault(c))
+            return bfail(b, GRLBM_ERR_CUDA, "problem %p: %s", (void *)c, c->err.c_str());
     return GRLBM_OK;
 }
 } // namespace

@@ -476,8 +476,9 @@ __global__ void k_zero_halo_moments(GridDev g, double *mom)
 // With `ang` (adaptive streaming) the directions are the stencil's rotated
 // by each node's angle, n1/n2 then holding the unrotated directions.
 template <typename T>
-__global__ void k_moments_from_I(const T *I, int64_t nxy, int nd, const double *w, const double *n1,
-                                 const double *n2, const float *scale, const double *ang, double *mom)
+__global__ void k_moments_from_I(const T *I, int64_t nxy, StateLayout L, int nd, const double *w,
+                                 const double *n1, const double *n2, const float *scale, const double *ang,
+                                 double *mom)
 {
     const int64_t ij = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (ij >= nxy)
@@ -490,12 +491,13 @@ __global__ void k_moments_from_I(const T *I, int64_t nxy, int nd, const double *
     }
     Moments m;
     m.zero();
+    const int64_t sij = L.at(ij);
     for (int d = 0; d < nd; d++)
     {
         const double wd = __ldg(w + d);
         if (wd == 0.0)
             continue;
-        double v = (double)I[(int64_t)d * nxy + ij];
+        double v = (double)I[(int64_t)d * L.plane + sij];
         if (scale)
             v = v / (double)scale[ij];
         const double c1 = __ldg(n1 + d), c2 = __ldg(n2 + d);
@@ -514,14 +516,14 @@ __global__ void k_moments_from_I(const T *I, int64_t nxy, int nd, const double *
 
 // Radiation::LoadInitialData for fixed streaming (src/Radiation.cpp:138-181)
 template <typename T>
-__global__ void k_sources(T *I, int64_t nxy, int nd, const int64_t *nodes, const T *vals, int64_t nsrc)
+__global__ void k_sources(T *I, StateLayout L, int nd, const int64_t *nodes, const T *vals, int64_t nsrc)
 {
     const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (tid >= nsrc * nd)
         return;
     const int64_t s = tid / nd;
     const int d = (int)(tid - s * nd);
-    I[(int64_t)d * nxy + nodes[s]] = vals[tid];
+    I[(int64_t)d * L.plane + L.at(nodes[s])] = vals[tid];
 }
 
 // Radiation::ComputeMomentsLF (src/Radiation.cpp:270-301)
@@ -618,7 +620,7 @@ __global__ void __launch_bounds__(256) k_energy_final(const double *partial, int
 
 // cell-major double [ij][d] <-> direction-major T [d][ij]
 template <class T>
-__global__ void k_to_dirmajor(const double *in, T *out, int64_t nxy, int nd, const float *scale)
+__global__ void k_to_dirmajor(const double *in, T *out, int64_t nxy, StateLayout L, int nd, const float *scale)
 {
     __shared__ double tile[32][33];
     const int64_t ij0 = (int64_t)blockIdx.x * 32;
@@ -636,11 +638,11 @@ __global__ void k_to_dirmajor(const double *in, T *out, int64_t nxy, int nd, con
         const int d = d0 + r;
         const int64_t ij = ij0 + threadIdx.x;
         if (ij < nxy && d < nd)
-            out[(int64_t)d * nxy + ij] = scale ? (T)tile[threadIdx.x][r] * (T)scale[ij] : (T)tile[threadIdx.x][r];
+            out[(int64_t)d * L.plane + L.at(ij)] = scale ? (T)tile[threadIdx.x][r] * (T)scale[ij] : (T)tile[threadIdx.x][r];
     }
 }
 template <class T>
-__global__ void k_to_cellmajor(const T *in, double *out, int64_t nxy, int nd, const float *scale)
+__global__ void k_to_cellmajor(const T *in, double *out, int64_t nxy, StateLayout L, int nd, const float *scale)
 {
     __shared__ double tile[32][33];
     const int64_t ij0 = (int64_t)blockIdx.x * 32;
@@ -650,8 +652,8 @@ __global__ void k_to_cellmajor(const T *in, double *out, int64_t nxy, int nd, co
         const int d = d0 + r;
         const int64_t ij = ij0 + threadIdx.x;
         if (ij < nxy && d < nd)
-            tile[threadIdx.x][r] = scale ? (double)in[(int64_t)d * nxy + ij] / (double)scale[ij]
-                                         : (double)in[(int64_t)d * nxy + ij];
+            tile[threadIdx.x][r] = scale ? (double)in[(int64_t)d * L.plane + L.at(ij)] / (double)scale[ij]
+                                         : (double)in[(int64_t)d * L.plane + L.at(ij)];
     }
     __syncthreads();
     for (int r = threadIdx.y; r < 32; r += 8)
@@ -709,12 +711,12 @@ void launch_step_plain(const PlainStepArgs &a, bool curved, cudaStream_t s, cons
 void launch_sources64(double *I, int64_t nxy, int nd, const int64_t *nodes, const double *vals, int64_t nsrc,
                       cudaStream_t s)
 {
-    k_sources<double><<<nblk(nsrc * nd, 256), 256, 0, s>>>(I, nxy, nd, nodes, vals, nsrc);
+    k_sources<double><<<nblk(nsrc * nd, 256), 256, 0, s>>>(I, StateLayout{nxy, nxy, nxy}, nd, nodes, vals, nsrc);
 }
-void launch_sources32(float *I, int64_t nxy, int nd, const int64_t *nodes, const float *vals, int64_t nsrc,
+void launch_sources32(float *I, const StateLayout &L, int nd, const int64_t *nodes, const float *vals, int64_t nsrc,
                       cudaStream_t s)
 {
-    k_sources<float><<<nblk(nsrc * nd, 256), 256, 0, s>>>(I, nxy, nd, nodes, vals, nsrc);
+    k_sources<float><<<nblk(nsrc * nd, 256), 256, 0, s>>>(I, L, nd, nodes, vals, nsrc);
 }
 void launch_moments_lf64(int64_t nxy, const double *mom, const double *lfp, const uint8_t *bh, double *out,
                          cudaStream_t s)
@@ -738,29 +740,34 @@ void launch_energy32(const GridDev &g, const float *E, double *partial, int nblo
 }
 void launch_to_dirmajor64(const double *in, double *out, int64_t nxy, int nd, cudaStream_t s)
 {
-    k_to_dirmajor<double><<<dim3(nblk(nxy, 32), nblk(nd, 32)), dim3(32, 8), 0, s>>>(in, out, nxy, nd, nullptr);
+    k_to_dirmajor<double><<<dim3(nblk(nxy, 32), nblk(nd, 32)), dim3(32, 8), 0, s>>>(in, out, nxy, StateLayout{nxy, nxy, nxy}, nd,
+                                                                                      nullptr);
 }
-void launch_to_dirmajor32(const double *in, float *out, int64_t nxy, int nd, const float *scale, cudaStream_t s)
+void launch_to_dirmajor32(const double *in, float *out, int64_t nxy, const StateLayout &L, int nd,
+                          const float *scale, cudaStream_t s)
 {
-    k_to_dirmajor<float><<<dim3(nblk(nxy, 32), nblk(nd, 32)), dim3(32, 8), 0, s>>>(in, out, nxy, nd, scale);
+    k_to_dirmajor<float><<<dim3(nblk(nxy, 32), nblk(nd, 32)), dim3(32, 8), 0, s>>>(in, out, nxy, L, nd, scale);
 }
 void launch_to_cellmajor64(const double *in, double *out, int64_t nxy, int nd, cudaStream_t s)
 {
-    k_to_cellmajor<double><<<dim3(nblk(nxy, 32), nblk(nd, 32)), dim3(32, 8), 0, s>>>(in, out, nxy, nd, nullptr);
+    k_to_cellmajor<double><<<dim3(nblk(nxy, 32), nblk(nd, 32)), dim3(32, 8), 0, s>>>(in, out, nxy, StateLayout{nxy, nxy, nxy}, nd,
+                                                                                       nullptr);
 }
-void launch_to_cellmajor32(const float *in, double *out, int64_t nxy, int nd, const float *scale, cudaStream_t s)
+void launch_to_cellmajor32(const float *in, double *out, int64_t nxy, const StateLayout &L, int nd,
+                           const float *scale, cudaStream_t s)
 {
-    k_to_cellmajor<float><<<dim3(nblk(nxy, 32), nblk(nd, 32)), dim3(32, 8), 0, s>>>(in, out, nxy, nd, scale);
+    k_to_cellmajor<float><<<dim3(nblk(nxy, 32), nblk(nd, 32)), dim3(32, 8), 0, s>>>(in, out, nxy, L, nd, scale);
 }
 void launch_moments_from_I64(const double *I, int64_t nxy, int nd, const double *w, const double *n1,
                              const double *n2, const double *ang, double *mom, cudaStream_t s)
 {
-    k_moments_from_I<double><<<nblk(nxy, 128), 128, 0, s>>>(I, nxy, nd, w, n1, n2, nullptr, ang, mom);
+    k_moments_from_I<double><<<nblk(nxy, 128), 128, 0, s>>>(I, nxy, StateLayout{nxy, nxy, nxy}, nd, w, n1, n2, nullptr, ang,
+                                                             mom);
 }
-void launch_moments_from_I32(const float *J, int64_t nxy, int nd, const double *w, const double *n1,
-                             const double *n2, const float *scale, double *mom, cudaStream_t s)
+void launch_moments_from_I32(const float *J, int64_t nxy, const StateLayout &L, int nd, const double *w,
+                             const double *n1, const double *n2, const float *scale, double *mom, cudaStream_t s)
 {
-    k_moments_from_I<float><<<nblk(nxy, 128), 128, 0, s>>>(J, nxy, nd, w, n1, n2, scale, nullptr, mom);
+    k_moments_from_I<float><<<nblk(nxy, 128), 128, 0, s>>>(J, nxy, L, nd, w, n1, n2, scale, nullptr, mom);
 }
 void launch_widen32(const float *in, double *out, int64_t n, cudaStream_t s)
 {

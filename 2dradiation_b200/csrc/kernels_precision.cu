@@ -22,6 +22,8 @@
 // per-cell sums of the direction terms (O(1) per iteration instead of a pass
 // over the directions); the converged intensities are written in one final
 // pass whose Kahan sums give the stored moments.
+#include <cudaTypedefs.h>
+
 #include "device_common.cuh"
 
 // Tuning of the step kernel: resident blocks per SM the register budget is
@@ -92,90 +94,141 @@ struct KMoments
 // (v + kBelow) mod kRing; slots 0..kMirror-1 are also kept in slots
 // kRing..kRing+kMirror-1, so the 5 planes of any window sit at consecutive
 // slots and a window's taps are fixed offsets from one address.  The next
-// chunk's planes are loaded by cp.async into slots the current chunk does not
-// read.
+// chunk's planes are brought in while the current chunk runs, into slots it
+// does not read.
+//
+// Staging is done by the TMA engine: the state is one 2D tensor of
+// {pitch, ny * nDir} floats (rows padded to 16 bytes), and each patch plane
+// is one tensor copy (cp.async.bulk.tensor) of a kBoxX x kPatchY box into its
+// slot, completing on the block's mbarrier.  One thread issues a chunk's
+// copies; every thread waits on the barrier with a time limit.  Box columns
+// past the grid's row (x >= pitch) arrive as zeros and rows past the last
+// plane too; none of them is read.
 #ifndef GRLBM_PREC_TILE_X
 #define GRLBM_PREC_TILE_X 32
 #endif
 constexpr int kTileX = GRLBM_PREC_TILE_X, kTileY = kStepBlock / GRLBM_PREC_TILE_X;
 static_assert(kTileX * kTileY == kStepBlock, "tile = block");
-constexpr int kPatchX = kTileX + 2, kPatchY = kTileY + 2, kPatch = kPatchX * kPatchY;
-static_assert(kPatch > kStepBlock && kPatch <= 2 * kStepBlock, "two staging loads per thread and plane");
+static_assert(kTileX % 4 == 0, "tile origins on 16-byte boundaries");
+constexpr int kPatchX = kTileX + 2, kPatchY = kTileY + 2;
 constexpr int kPrecUnroll = GRLBM_PREC_UNROLL;
 constexpr int kRing = 32, kMirror = kTaps - 1;
 static_assert(kSpan + kChunk <= kRing && (kRing & (kRing - 1)) == 0, "ring");
 constexpr int kRingSlots = kRing + kMirror;
+// the box: a patch row rounded up to 16 bytes, the slot: a box rounded up to
+// 128 bytes (the alignment of a tensor copy's shared destination)
+constexpr int kBoxX = (kPatchX + 3) / 4 * 4;
+constexpr unsigned kBoxBytes = kBoxX * kPatchY * sizeof(float);
+constexpr int kSlot = (kBoxX * kPatchY + 31) / 32 * 32;
+constexpr int kRingAlign = 128;
+// time limits of a staging wait (copies land within microseconds), and of
+// the drain of copies in flight after one has run out
+constexpr unsigned long long kWaitNs = 200000000ull, kDrainNs = 1000000ull;
 
-__device__ __forceinline__ void cp_async4(float *dst, const float *src)
+__device__ __forceinline__ unsigned smem_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count)
 {
-    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
 }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
-
-// this thread's share of one patch plane: patch nodes t and t + kStepBlock
-struct StageSlots
+// the issuing thread's arrival on the current phase, announcing `bytes` of copies
+__device__ __forceinline__ void mbar_arrive_expect(unsigned bar, unsigned bytes)
 {
-    int node0, node1;        // patch node indices (node1 < 0: none)
-    unsigned goff0, goff1;   // node offsets in a global plane
-    bool ok0, ok1;           // node inside the grid
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
+}
+// one box of a 2D tensor at element coordinates (x, y) into shared memory
+__device__ __forceinline__ void tma_load_2d(unsigned dst, const CUtensorMap *map, int x, int y, unsigned bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+        "[%4];\n" ::"r"(dst),
+        "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
+__device__ __forceinline__ bool mbar_test(unsigned bar, unsigned parity)
+{
+    unsigned done;
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, "
+                 "p;\n}\n"
+                 : "=r"(done)
+                 : "r"(bar), "r"(parity)
+                 : "memory");
+    return done != 0;
+}
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// Wait for the phase of the given parity to complete, for limit_ns at most;
+// false at once when another block has already raised the fault word.
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity, unsigned long long limit_ns,
+                                          const unsigned *fault)
+{
+    if (mbar_test(bar, parity))
+        return true;
+    if (fault && *reinterpret_cast<const volatile unsigned *>(fault))
+        return false;
+    const unsigned long long t0 = global_ns();
+    do
+    {
+        if (mbar_test(bar, parity))
+            return true;
+    } while (global_ns() - t0 < limit_ns);
+    return false;
+}
+
+// the tile's stage: shared addresses of slot 0 and of the mbarrier, and the
+// patch origin (node coordinates)
+struct Stage
+{
+    unsigned ring, bar;
+    int x0, y0;
 };
 
-__device__ __forceinline__ StageSlots stage_slots(const GridDev &g, int x0, int y0)
+// Shared layout: the mbarrier (16 bytes), then the ring from the next
+// kRingAlign boundary, the row-type table and the direction coefficients.
+constexpr int kBarBytes = 16;
+__device__ __forceinline__ float *ring_base(unsigned char *smem_raw)
 {
-    StageSlots s;
-    const int t = threadIdx.x;
-    s.node0 = t;
-    int py = t / kPatchX, px = t - py * kPatchX;
-    s.ok0 = (x0 + px < (int)g.nx) && (y0 + py < (int)g.ny);
-    s.goff0 = (unsigned)((x0 + px) + (y0 + py) * (int)g.nx);
-    const int n1 = t + kStepBlock;
-    s.node1 = n1 < kPatch ? n1 : -1;
-    py = n1 / kPatchX;
-    px = n1 - py * kPatchX;
-    s.ok1 = s.node1 >= 0 && (x0 + px < (int)g.nx) && (y0 + py < (int)g.ny);
-    s.goff1 = (unsigned)((x0 + px) + (y0 + py) * (int)g.nx);
-    return s;
+    const unsigned at = smem_addr(smem_raw) + kBarBytes;
+    return reinterpret_cast<float *>(smem_raw + kBarBytes + ((kRingAlign - (at & (kRingAlign - 1))) & (kRingAlign - 1)));
 }
 
-// stage virtual planes [v0, v0 + n) into their ring slots (and mirrors)
-__device__ __forceinline__ void stage_planes(const PrecStepArgs &a, const StageSlots &ss, float *ring, int v0, int n)
+// Stage virtual planes [v0, v0 + n) into their ring slots (and mirrors):
+// one phase of the mbarrier, issued by thread 0.
+__device__ __forceinline__ void stage_planes(const PrecStepArgs &a, const Stage &st, int v0, int n)
 {
-    const unsigned nxy = (unsigned)a.g.nxy;
+    if (threadIdx.x != 0)
+        return;
+    unsigned boxes = 0;
+    for (int p = 0; p < n; p++)
+        boxes += (((v0 + p + kBelow) & (kRing - 1)) < kMirror) ? 2u : 1u;
+    mbar_arrive_expect(st.bar, boxes * kBoxBytes);
     int d = v0 % a.nd;
     d = d < 0 ? d + a.nd : d;
     for (int p = 0; p < n; p++)
     {
         const int sl = (v0 + p + kBelow) & (kRing - 1);
-        float *slot = ring + sl * kPatch;
-        const float *plane = a.Iin + (unsigned)d * nxy;
-        if (ss.ok0)
-            cp_async4(slot + ss.node0, plane + ss.goff0);
-        if (ss.ok1)
-            cp_async4(slot + ss.node1, plane + ss.goff1);
+        const int y = d * (int)a.g.ny + st.y0;
+        tma_load_2d(st.ring + (unsigned)(sl * kSlot) * 4u, &a.in_map, st.x0, y, st.bar);
         if (sl < kMirror)
-        {
-            float *mirror = slot + kRing * kPatch;
-            if (ss.ok0)
-                cp_async4(mirror + ss.node0, plane + ss.goff0);
-            if (ss.ok1)
-                cp_async4(mirror + ss.node1, plane + ss.goff1);
-        }
+            tma_load_2d(st.ring + (unsigned)((sl + kRing) * kSlot) * 4u, &a.in_map, st.x0, y, st.bar);
         d = (d + 1 == a.nd) ? 0 : d + 1;
     }
-    cp_async_commit();
 }
 
 // The four bilinear corners of a 5-tap angular window read from global
 // memory, each clamped at zero: the rare departures whose corners or window
 // fall outside the staged patch (kept out of line: it is cold code).
-__device__ __noinline__ float4 window_corners_global(const float *__restrict__ I, unsigned nxy, int nd, int base,
-                                                     unsigned c00, unsigned nx, float w0, float w1, float w2,
+__device__ __noinline__ float4 window_corners_global(const float *__restrict__ I, unsigned plane, int nd, int base,
+                                                     unsigned c00, unsigned pitch, float w0, float w1, float w2,
                                                      float w3, float w4)
 {
     const float w[kTaps] = {w0, w1, w2, w3, w4};
-    const unsigned off[4] = {c00, c00 + nx, c00 + 1u, c00 + nx + 1u}; // corners 00 01 10 11
+    const unsigned off[4] = {c00, c00 + pitch, c00 + 1u, c00 + pitch + 1u}; // corners 00 01 10 11
     float cv[4];
 #pragma unroll
     for (int q = 0; q < 4; q++)
@@ -185,7 +238,7 @@ __device__ __noinline__ float4 window_corners_global(const float *__restrict__ I
 #pragma unroll
         for (int k = 0; k < kTaps; k++)
         {
-            v = fmaf(w[k], __ldg(I + (unsigned)dk * nxy + off[q]), v);
+            v = fmaf(w[k], __ldg(I + (unsigned)dk * plane + off[q]), v);
             dk = (dk + 1 == nd) ? 0 : dk + 1;
         }
         cv[q] = fmaxf(v, 0.f);
@@ -197,7 +250,8 @@ __device__ __noinline__ float4 window_corners_global(const float *__restrict__ I
 // coordinate, s^3 alpha_c^3}, all taps from global memory: the departures
 // whose packed record is marked far (cold code, kept out of line).
 __device__ __noinline__ float stream_curved_far(const float *__restrict__ Iin, const float4 *__restrict__ side,
-                                                unsigned nxy, int nx, int ny, int nd, int ng, const float *rowtab,
+                                                unsigned plane, unsigned pitch, int nx, int ny, int nd, int ng,
+                                                const float *rowtab,
                                                 int q, int p, float inv_q, unsigned rec_index, int i, int j)
 {
     const float4 r = side[rec_index];
@@ -212,8 +266,7 @@ __device__ __noinline__ float stream_curved_far(const float *__restrict__ Iin, c
     const int rt = min(max((int)fmaf(-m, (float)q, g), 0), q - 1);
     const float *row = rowtab + rt * 12;
     int base = (int)fmaf(m, (float)p, row[10]) % nd;
-    const float4 c = window_corners_global(Iin, nxy, nd, base, (unsigned)(i0 + j0 * nx),
-                                           (unsigned)nx, fmaf(t, row[4], row[0]), fmaf(t, row[5], row[1]),
+    const float4 c = window_corners_global(Iin, plane, nd, base, (unsigned)i0 + (unsigned)j0 * pitch, pitch, fmaf(t, row[4], row[0]), fmaf(t, row[5], row[1]),
                                            fmaf(t, row[6], row[2]), fmaf(t, row[7], row[3]),
                                            fmaf(t, row[9], row[8]));
     const float f0 = fmaf(fx, c.z - c.x, c.x);
@@ -226,14 +279,14 @@ __device__ __noinline__ float stream_curved_far(const float *__restrict__ Iin, c
 // corners of the departure, each the 5-tap angular window (the two cubic
 // rows of the interpolation grid, src/Stencil.cpp:109-162, blended in t)
 // clamped at zero, then bilinear in (fx, fy) and scaled by s^3 alpha_c^3.
-// `cell` is the patch offset of the cell's lower-left neighbour.
+// `cell` is the slot offset of the cell's lower-left neighbour.
 __device__ __forceinline__ float stream_curved(const PrecStepArgs &a, const DirTable &dt, const float *ring,
                                                const float *rowtab, int d, const float4 &r, int cell,
                                                unsigned rec_index, int i, int j)
 {
     const unsigned word = __float_as_uint(r.x);
     if (word >> packed::kFarBit)
-        return stream_curved_far(a.Iin, a.side, (unsigned)a.g.nxy, (int)a.g.nx, (int)a.g.ny, a.nd, a.ng, rowtab, dt.q,
+        return stream_curved_far(a.Iin, a.side, a.plane, a.pitch, (int)a.g.nx, (int)a.g.ny, a.nd, a.ng, rowtab, dt.q,
                                  dt.p, dt.inv_q, rec_index, i, j);
     const float t = (float)(word & ((1u << packed::kTBits) - 1u)) * (1.f / (float)(1u << packed::kTBits));
     const float4 *row = reinterpret_cast<const float4 *>(rowtab + ((word >> packed::kTypeShift) & 31u) * 12);
@@ -243,15 +296,15 @@ __device__ __forceinline__ float stream_curved(const PrecStepArgs &a, const DirT
     // ring slot of the window's first plane: virtual plane d + dbase
     const int slot = (d + (int)((word >> packed::kBaseShift) & 63u) - packed::kBaseBias + kBelow) & (kRing - 1);
     const unsigned code = word >> packed::kCodeShift; // bit 31 is clear here
-    const float *p = ring + slot * kPatch + cell + (int)(code & 1u) + (int)(code >> 1) * kPatchX;
-#define GRLBM_WINDOW(o)                                                                                       \
-    fmaxf(fmaf(w4, p[4 * kPatch + (o)],                                                                       \
-               fmaf(w3, p[3 * kPatch + (o)], fmaf(w2, p[2 * kPatch + (o)], fmaf(w1, p[kPatch + (o)], w0 * p[(o)])))), \
+    const float *p = ring + slot * kSlot + cell + (int)(code & 1u) + (int)(code >> 1) * kBoxX;
+#define GRLBM_WINDOW(o)                                                                                    \
+    fmaxf(fmaf(w4, p[4 * kSlot + (o)],                                                                     \
+               fmaf(w3, p[3 * kSlot + (o)], fmaf(w2, p[2 * kSlot + (o)], fmaf(w1, p[kSlot + (o)], w0 * p[(o)])))), \
           0.f)
     const float c00 = GRLBM_WINDOW(0);
-    const float c01 = GRLBM_WINDOW(kPatchX);
+    const float c01 = GRLBM_WINDOW(kBoxX);
     const float c10 = GRLBM_WINDOW(1);
-    const float c11 = GRLBM_WINDOW(kPatchX + 1);
+    const float c11 = GRLBM_WINDOW(kBoxX + 1);
 #undef GRLBM_WINDOW
     const float f0 = fmaf(r.y, c10 - c00, c00);
     const float f1 = fmaf(r.y, c11 - c01, c01);
@@ -260,8 +313,9 @@ __device__ __forceinline__ float stream_curved(const PrecStepArgs &a, const DirT
 
 // One flat stream value of direction d (StreamFlatFixed, src/Radiation.cpp:394-410).
 __device__ __forceinline__ float stream_flat(const PrecStepArgs &a, const DirTable &dt, const float *ring, int d,
-                                             int chunk0, int i, int j, int x0, int y0)
+                                             const Stage &st, int i, int j)
 {
+    const int x0 = st.x0, y0 = st.y0;
     const int nx = (int)a.g.nx;
     const float ox = dt.ox[d], oy = dt.oy[d];
     const float fli = floorf(ox), flj = floorf(oy);
@@ -272,13 +326,14 @@ __device__ __forceinline__ float stream_flat(const PrecStepArgs &a, const DirTab
     float c00, c01, c10, c11;
     if ((unsigned)lx <= (unsigned)kTileX && (unsigned)ly <= (unsigned)kTileY)
     {
-        const float *p = ring + ((d + kBelow) & (kRing - 1)) * kPatch + ly * kPatchX + lx;
-        c00 = p[0], c01 = p[kPatchX], c10 = p[1], c11 = p[kPatchX + 1];
+        const float *p = ring + ((d + kBelow) & (kRing - 1)) * kSlot + ly * kBoxX + lx;
+        c00 = p[0], c01 = p[kBoxX], c10 = p[1], c11 = p[kBoxX + 1];
     }
     else
     {
-        const float *p = a.Iin + (unsigned)d * (unsigned)a.g.nxy + (unsigned)(i0 + j0 * nx);
-        c00 = __ldg(p), c01 = __ldg(p + nx), c10 = __ldg(p + 1), c11 = __ldg(p + nx + 1);
+        const unsigned pitch = a.pitch;
+        const float *p = a.Iin + (unsigned)d * a.plane + (unsigned)i0 + (unsigned)j0 * pitch;
+        c00 = __ldg(p), c01 = __ldg(p + pitch), c10 = __ldg(p + 1), c11 = __ldg(p + pitch + 1);
     }
     const float f0 = fmaf(fx, c10 - c00, c00);
     const float f1 = fmaf(fx, c11 - c01, c01);
@@ -299,12 +354,15 @@ __device__ __forceinline__ void collide_coeffs(float n1, float n2, float u1, flo
 }
 
 // One tile (kTileX x kTileY cells of the slab rows) of one step: stream,
-// moments and collide for its cells.  bx, by: tile coordinates.
+// moments and collide for its cells.  bx, by: tile coordinates; parity: the
+// phase parity of the block's staging mbarrier, carried from tile to tile.
+// Returns false (for the whole block) when a staging wait ran out of time:
+// the fault word is then set and the tile is abandoned.
 template <bool CURVED>
-__device__ __forceinline__ void step_tile(const PrecStepArgs &a, const DirTable &dt, int bx, int by,
-                                          unsigned char *smem_raw)
+__device__ __forceinline__ bool step_tile(const PrecStepArgs &a, const DirTable &dt, int bx, int by,
+                                          unsigned char *smem_raw, unsigned &parity)
 {
-    float *ring = reinterpret_cast<float *>(smem_raw);
+    float *ring = ring_base(smem_raw);
     const int t = threadIdx.x;
     const int tx = t % kTileX, ty = t / kTileX;
     // patch origin (node coordinates); tiles cover the slab rows [jlo, jhi)
@@ -314,18 +372,18 @@ __device__ __forceinline__ void step_tile(const PrecStepArgs &a, const DirTable 
     const int ii = active ? i : 1, jj = active ? j : 1;
     const int ij = ii + jj * (int)a.g.nx;
     const int cc = (ii - 1) + (jj - 1) * (int)a.g.nx_;
-    const unsigned nxy = (unsigned)a.g.nxy;
+    const unsigned nxy = (unsigned)a.g.nxy, plane = a.plane;
     const uint8_t fl = active ? a.flags[ij] : (uint8_t)3;
     const bool live = active && !(CURVED && (fl & 2));
     const bool collides = active && !(fl & 1);
     // The streamed intensities of a colliding cell wait in its own output
     // slots until the lambda iteration has converged (nothing else reads or
     // writes them in this step).
-    float *Is = a.Iout + (unsigned)ij;
+    float *Is = a.Iout + (unsigned)ii + (unsigned)jj * a.pitch;
 
     // row-type table of the angular interpolation and direction coefficients
     // of the moment sums, from the kernel parameter
-    float *rowtab = ring + kRingSlots * kPatch;
+    float *rowtab = ring + kRingSlots * kSlot;
     float4 *dirc = reinterpret_cast<float4 *>(rowtab + kMaxRowTypes * 12);
     if (CURVED)
         for (int k = t; k < dt.q * 12; k += kStepBlock)
@@ -333,9 +391,9 @@ __device__ __forceinline__ void step_tile(const PrecStepArgs &a, const DirTable 
     for (int k = t; k < 2 * a.nd; k += kStepBlock)
         dirc[k] = reinterpret_cast<const float4 *>(dt.dirc)[k];
 
-    const StageSlots ss = stage_slots(a.g, x0, y0);
-    const int cell = ty * kPatchX + tx; // patch offset of node (i - 1, j - 1)
-    stage_planes(a, ss, ring, -kBelow, kSpan);
+    const Stage st{smem_addr(ring), smem_addr(smem_raw), x0, y0};
+    const int cell = ty * kBoxX + tx; // slot offset of node (i - 1, j - 1)
+    stage_planes(a, st, -kBelow, kSpan);
 
     KMoments km;
     km.zero();
@@ -352,10 +410,20 @@ __device__ __forceinline__ void step_tile(const PrecStepArgs &a, const DirTable 
     }
     for (int chunk0 = 0; chunk0 < a.nd; chunk0 += kChunk)
     {
-        cp_async_wait_all();
-        __syncthreads(); // this chunk's planes visible; the previous chunk is done with its slots
+        // this chunk's planes landed and are visible; the previous chunk is
+        // done with its slots
+        const bool landed = mbar_wait(st.bar, parity, kWaitNs, a.fault);
+        if (__syncthreads_or(!landed))
+        {
+            // report it, let the copies in flight land and give up the tile
+            if (t == 0 && a.fault)
+                *reinterpret_cast<volatile unsigned *>(a.fault) = 1u;
+            mbar_wait(st.bar, parity, kDrainNs, nullptr);
+            return false;
+        }
+        parity ^= 1u;
         if (chunk0 + kChunk < a.nd)
-            stage_planes(a, ss, ring, chunk0 + kSpan - kBelow, kChunk);
+            stage_planes(a, st, chunk0 + kSpan - kBelow, kChunk);
         const int dend = min(chunk0 + kChunk, a.nd);
 #pragma unroll kPrecUnroll
         for (int d = chunk0; d < dend; d++)
@@ -366,9 +434,9 @@ __device__ __forceinline__ void step_tile(const PrecStepArgs &a, const DirTable 
             float v = 0.f;
             if (live)
                 v = CURVED ? stream_curved(a, dt, ring, rowtab, d, r0, cell, (unsigned)cc + (unsigned)d * rs, ii, jj)
-                           : stream_flat(a, dt, ring, d, chunk0, ii, jj, x0, y0);
+                           : stream_flat(a, dt, ring, d, st, ii, jj);
             if (collides)
-                Is[(unsigned)d * nxy] = v;
+                Is[(unsigned)d * plane] = v;
             km.add(v, dirc[2 * d], dirc[2 * d + 1]);
             r0 = r1;
             r1 = r2;
@@ -410,7 +478,7 @@ __device__ __forceinline__ void step_tile(const PrecStepArgs &a, const DirTable 
                 float g, h, q1, q2;
                 collide_coeffs(n1, n2, u1, u2, lor, adt, kak0, g, h, q1, q2);
                 const float mu[6] = {1.f, n1, n2, n1 * n1, n1 * n2, n2 * n2};
-                const float gs = w * g * Is[(unsigned)d * nxy], wh = w * h;
+                const float gs = w * g * Is[(unsigned)d * plane], wh = w * h;
 #pragma unroll
                 for (int q = 0; q < 6; q++)
                 {
@@ -458,7 +526,7 @@ __device__ __forceinline__ void step_tile(const PrecStepArgs &a, const DirTable 
             float S[8];
 #pragma unroll
             for (int k = 0; k < 8; k++)
-                S[k] = (d0 + k < a.nd) ? Is[(unsigned)(d0 + k) * nxy] : 0.f;
+                S[k] = (d0 + k < a.nd) ? Is[(unsigned)(d0 + k) * plane] : 0.f;
 #pragma unroll
             for (int k = 0; k < 8; k++)
             {
@@ -476,7 +544,7 @@ __device__ __forceinline__ void step_tile(const PrecStepArgs &a, const DirTable 
                     collide_coeffs(n1, n2, u1, u2, lor, adt, kak0, g, h, q1, q2);
                     v = g * S[k] + h * (e + k3 * (q1 * fFx + q2 * fFy));
                 }
-                Is[(unsigned)d * nxy] = v * scale;
+                Is[(unsigned)d * plane] = v * scale;
                 km.add(v, c0, c1);
             }
             km.fold();
@@ -502,14 +570,19 @@ __device__ __forceinline__ void step_tile(const PrecStepArgs &a, const DirTable 
         atomicAdd(a.iter_sum, (unsigned long long)sum);
         atomicMax(a.iter_max, mx);
     }
+    return true;
 }
 
 template <bool CURVED>
 __global__ void __launch_bounds__(kStepBlock, GRLBM_PREC_MIN_BLOCKS)
-    k_step_prec(PrecStepArgs a, const __grid_constant__ DirTable dt)
+    k_step_prec(const __grid_constant__ PrecStepArgs a, const __grid_constant__ DirTable dt)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    step_tile<CURVED>(a, dt, blockIdx.x, blockIdx.y, smem_raw);
+    if (threadIdx.x == 0)
+        mbar_init(smem_addr(smem_raw), 1);
+    __syncthreads();
+    unsigned parity = 0;
+    step_tile<CURVED>(a, dt, blockIdx.x, blockIdx.y, smem_raw, parity);
 }
 
 // Many problems in one persistent launch: the blocks walk the concatenated
@@ -521,6 +594,10 @@ __global__ void __launch_bounds__(kStepBlock, GRLBM_PREC_MIN_BLOCKS)
                  int total_tiles, int flip)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    if (threadIdx.x == 0)
+        mbar_init(smem_addr(smem_raw), 1);
+    __syncthreads();
+    unsigned parity = 0;
     for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x)
     {
         int lo = 0, hi = n_items - 1;
@@ -536,10 +613,10 @@ __global__ void __launch_bounds__(kStepBlock, GRLBM_PREC_MIN_BLOCKS)
         const int local = tile - first_tile[lo];
         const int bx = local % it.tiles_x, by = local / it.tiles_x;
         const PrecStepArgs &a = it.a[it.cur0 ^ flip];
-        if (it.curved)
-            step_tile<true>(a, *it.dt, bx, by, smem_raw);
-        else
-            step_tile<false>(a, *it.dt, bx, by, smem_raw);
+        const bool ok = it.curved ? step_tile<true>(a, *it.dt, bx, by, smem_raw, parity)
+                                  : step_tile<false>(a, *it.dt, bx, by, smem_raw, parity);
+        if (!ok)
+            return; // the barrier's phase is unknown: the block stops (the fault word is set)
         __syncthreads(); // the next tile reuses the shared stage
     }
 }
@@ -564,7 +641,39 @@ void launch_step_batch(const BatchItem *items, const int *first_tile, int n_item
     k_step_batch<<<blocks, kStepBlock, smem_bytes, s>>>(items, first_tile, n_items, total_tiles, flip);
 }
 
-size_t step_prec_smem(int nd) { return ((size_t)kRingSlots * kPatch + kMaxRowTypes * 12 + 8 * (size_t)nd) * sizeof(float); }
+// The state as a 2D tensor of {pitch, ny * nd} floats (row y = d ny + j),
+// read in boxes of one patch plane.
+cudaError_t encode_state_map(CUtensorMap *map, const float *state, const StateLayout &L, int64_t ny, int nd)
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode)
+    {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        const cudaError_t e =
+            cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &fn, 12000, cudaEnableDefault, &q);
+        if (e != cudaSuccess)
+            return e;
+        if (q != cudaDriverEntryPointSuccess || !fn)
+            return cudaErrorNotSupported;
+        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    if (L.pitch % 4 != 0 || reinterpret_cast<uintptr_t>(state) % 16 != 0)
+        return cudaErrorInvalidValue;
+    const cuuint64_t dims[2] = {(cuuint64_t)L.pitch, (cuuint64_t)(ny * nd)};
+    const cuuint64_t strides[1] = {(cuuint64_t)L.pitch * sizeof(float)};
+    const cuuint32_t box[2] = {(cuuint32_t)kBoxX, (cuuint32_t)kPatchY};
+    const cuuint32_t elem[2] = {1, 1};
+    const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float *>(state), dims, strides, box,
+                              elem, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+size_t step_prec_smem(int nd)
+{
+    return kBarBytes + kRingAlign + ((size_t)kRingSlots * kSlot + kMaxRowTypes * 12 + 8 * (size_t)nd) * sizeof(float);
+}
 
 // The shared-memory limit is a property of the kernel, shared by every
 // context in the process: it is set for the largest direction count, so

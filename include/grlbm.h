@@ -226,12 +226,14 @@ int grlbm_energy_noalloc(const double *E, int64_t nx_, int64_t ny_, double *tota
  * interior rows). */
 int grlbm_set_rows(grlbm_ctx *ctx, int64_t j_first, int64_t j_end);
 /* Bytes of one node row of the intensity state over all directions
- * (nx * nDir * 8 for GRLBM_PLAIN_FP64, * 4 for GRLBM_PRECISION_FP32). */
+ * (nx * nDir * 8 for GRLBM_PLAIN_FP64; GRLBM_PRECISION_FP32 keeps its rows
+ * padded to a multiple of 4 floats: ((nx + 3) / 4 * 4) * nDir * 4). */
 int grlbm_row_bytes(const grlbm_ctx *ctx, int64_t *bytes);
 /* Copies node rows [j_first, j_first + n) of the current intensity state
  * (every direction) to (to_buffer = 1) or from (to_buffer = 0) a contiguous
- * device buffer laid out [direction][row][i], n * row_bytes bytes.  Enqueued
- * on the context's stream; returns before it completes. */
+ * device buffer laid out [direction][row][i] (i over the padded row for
+ * GRLBM_PRECISION_FP32), n * row_bytes bytes.  Enqueued on the context's
+ * stream; returns before it completes. */
 int grlbm_copy_rows(grlbm_ctx *ctx, int64_t j_first, int64_t n, void *buffer, int32_t to_buffer);
 /* The most node rows away from its cell that any stream gather reads (from
  * the departure records of the last table build; from the stencil for flat
