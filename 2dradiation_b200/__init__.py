@@ -89,6 +89,7 @@ SIGNATURES = {
     "grlbm_batch_last_error": ([C.c_void_p], C.c_char_p),
     "grlbm_batch_step": ([C.c_void_p, C.c_int32], C.c_int),
     "grlbm_batch_autotune": ([C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32)], C.c_int),
+    "grlbm_batch_set_shape": ([C.c_void_p, C.c_int32, C.c_int32], C.c_int),
     "grlbm_adjoint_create": ([C.c_void_p, C.c_int32, C.POINTER(C.c_void_p)], C.c_int),
     "grlbm_adjoint_destroy": ([C.c_void_p], None),
     "grlbm_adjoint_last_error": ([C.c_void_p], C.c_char_p),
@@ -370,8 +371,9 @@ class Adjoint:
 
 
 class Batch:
-    """Several precision-form problems stepped together by one persistent
-    launch per step (grlbm_batch_*).  The Radiation objects stay usable."""
+    """Several precision-form problems stepped together (grlbm_batch_*): one
+    persistent launch per step, or the problems' own kernels launched
+    concurrently.  The Radiation objects stay usable."""
 
     def __init__(self, problems: list):
         self.problems = list(problems)
@@ -388,6 +390,11 @@ class Batch:
 
     def step(self, n: int):
         self._c(lib().grlbm_batch_step(self.h, n))
+
+    def set_shape(self, blocks_per_sm: int, largest_first: bool = True):
+        """blocks_per_sm >= 1: the persistent launch; 0: each problem's own
+        kernel, the problems' launches concurrent."""
+        self._c(lib().grlbm_batch_set_shape(self.h, int(blocks_per_sm), int(bool(largest_first))))
 
     def autotune(self, trial_steps: int = 4) -> dict:
         bps, lf = C.c_int32(), C.c_int32()

@@ -1478,11 +1478,21 @@ struct grlbm_batch
     int largest_first = 0;
     int flip = 0; // parity of the steps taken since the items were built
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    // blocks_per_sm == 0: each problem's own step kernel, the problems'
+    // launch chains running concurrently on their streams, forked from and
+    // joined back to the batch stream by these events
+    cudaEvent_t fork = nullptr;
+    std::vector<cudaEvent_t> join;
     ~grlbm_batch()
     {
         for (auto &g : graph)
             if (g)
                 cudaGraphExecDestroy(g);
+        if (fork)
+            cudaEventDestroy(fork);
+        for (cudaEvent_t e : join)
+            if (e)
+                cudaEventDestroy(e);
         if (stream)
             cudaStreamDestroy(stream);
     }
@@ -1562,10 +1572,31 @@ int batch_build(grlbm_batch *b)
     return GRLBM_OK;
 }
 
-void batch_enqueue(grlbm_batch *b, int flip)
+// Enqueue n steps of every problem on the batch stream, the first reading
+// the buffers of parity `flip`: one persistent launch per step, or (shape 0)
+// each problem's chain of step kernels on its own stream between a fork and
+// a join on the batch stream.
+int batch_enqueue(grlbm_batch *b, int n, int flip)
 {
-    launch_step_batch(b->d_items.as<BatchItem>(), b->d_first.as<int>(), (int)b->items.size(), b->total_tiles, flip,
-                      b->sms * b->blocks_per_sm, b->smem, b->stream);
+    if (b->blocks_per_sm > 0)
+    {
+        for (int s = 0; s < n; s++)
+            launch_step_batch(b->d_items.as<BatchItem>(), b->d_first.as<int>(), (int)b->items.size(),
+                              b->total_tiles, flip ^ (s & 1), b->sms * b->blocks_per_sm, b->smem, b->stream);
+        return GRLBM_OK;
+    }
+    BCU(cudaEventRecord(b->fork, b->stream));
+    for (size_t k = 0; k < b->items.size(); k++)
+    {
+        grlbm_ctx *c = b->ctx[b->order[k]];
+        BCU(cudaStreamWaitEvent(c->stream, b->fork, 0));
+        for (int s = 0; s < n; s++)
+            launch_step_prec(prec_args(c, b->items[k].cur0 ^ flip ^ (s & 1)), c->dirs, b->items[k].curved,
+                             c->stream);
+        BCU(cudaEventRecord(b->join[k], c->stream));
+        BCU(cudaStreamWaitEvent(b->stream, b->join[k], 0));
+    }
+    return GRLBM_OK;
 }
 
 // Brings the launch list in line with the contexts (stepped on their own
@@ -1593,9 +1624,14 @@ int batch_steps(grlbm_batch *b, int n)
         {
             cudaGraph_t g = nullptr;
             BCU(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-            for (int s = 0; s < kGraphSteps; s++)
-                batch_enqueue(b, b->flip ^ (s & 1));
+            const int erc = batch_enqueue(b, kGraphSteps, b->flip);
             cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+            if (erc)
+            {
+                if (g)
+                    cudaGraphDestroy(g);
+                return erc;
+            }
             if (e != cudaSuccess)
                 return bfail(b, GRLBM_ERR_CUDA, "batch graph capture failed: %s", cudaGetErrorString(e));
             e = cudaGraphInstantiate(&b->graph[b->flip], g, 0);
@@ -1606,10 +1642,11 @@ int batch_steps(grlbm_batch *b, int n)
         BCU(cudaGraphLaunch(b->graph[b->flip], b->stream));
         left -= kGraphSteps; // even: parity unchanged
     }
-    for (; left > 0; left--)
+    if (left > 0)
     {
-        batch_enqueue(b, b->flip);
-        b->flip ^= 1;
+        if ((rc = batch_enqueue(b, left, b->flip)))
+            return rc;
+        b->flip ^= left & 1;
     }
     BCU(cudaGetLastError());
     BCU(cudaStreamSynchronize(b->stream));
@@ -1659,6 +1696,10 @@ int grlbm_batch_create(grlbm_ctx *const *ctxs, int32_t n, grlbm_batch **out)
     b->device = ctxs[0]->device;
     cudaSetDevice(b->device);
     BCU(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+    BCU(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+    b->join.assign(n, nullptr);
+    for (int k = 0; k < n; k++)
+        BCU(cudaEventCreateWithFlags(&b->join[k], cudaEventDisableTiming));
     b->smem = (int)step_prec_smem(max_nd);
     BCU(prepare_step_batch(b->smem, &b->blocks_per_sm_max));
     if (b->blocks_per_sm_max < 1)
@@ -1699,6 +1740,20 @@ int grlbm_batch_step(grlbm_batch *b, int32_t n_steps)
     return batch_steps(b, n_steps);
 }
 
+int grlbm_batch_set_shape(grlbm_batch *b, int32_t blocks_per_sm, int32_t largest_first)
+{
+    if (!b)
+        return GRLBM_ERR_ARGUMENT;
+    if (blocks_per_sm < 0 || blocks_per_sm > b->blocks_per_sm_max)
+        return bfail(b, GRLBM_ERR_ARGUMENT, "blocks_per_sm must be in [0, %d]", b->blocks_per_sm_max);
+    cudaSetDevice(b->device);
+    for (grlbm_ctx *c : b->ctx)
+        BCU(cudaStreamSynchronize(c->stream));
+    b->blocks_per_sm = blocks_per_sm;
+    b->largest_first = largest_first != 0;
+    return batch_build(b);
+}
+
 int grlbm_batch_autotune(grlbm_batch *b, int32_t trial_steps, int32_t *blocks_per_sm, int32_t *largest_first)
 {
     if (!b)
@@ -1733,28 +1788,35 @@ int grlbm_batch_autotune(grlbm_batch *b, int32_t trial_steps, int32_t *blocks_pe
     cudaEvent_t e0, e1;
     BCU(cudaEventCreate(&e0));
     BCU(cudaEventCreate(&e1));
+    // persistent launches (largest problem first or not, at each resident
+    // block count), and the problems' own kernels launched concurrently
+    std::vector<std::pair<int, int>> shapes;
     for (int lf = 0; lf <= 1; lf++)
         for (int bps = b->blocks_per_sm_max; bps >= 1 && bps >= b->blocks_per_sm_max - 2; bps--)
+            shapes.emplace_back(bps, lf);
+    shapes.emplace_back(0, 1);
+    for (const auto &shape : shapes)
+    {
+        b->blocks_per_sm = shape.first;
+        b->largest_first = shape.second;
+        if ((rc = batch_build(b)))
+            break;
+        if ((rc = batch_enqueue(b, 1, 0))) // warm-up
+            break;
+        cudaEventRecord(e0, b->stream);
+        if ((rc = batch_enqueue(b, trial_steps, 1)))
+            break;
+        cudaEventRecord(e1, b->stream);
+        if (cudaStreamSynchronize(b->stream) != cudaSuccess)
         {
-            b->largest_first = lf;
-            b->blocks_per_sm = bps;
-            if ((rc = batch_build(b)))
-                break;
-            batch_enqueue(b, 0); // warm-up
-            cudaEventRecord(e0, b->stream);
-            for (int s = 0; s < trial_steps; s++)
-                batch_enqueue(b, (s + 1) & 1);
-            cudaEventRecord(e1, b->stream);
-            if (cudaStreamSynchronize(b->stream) != cudaSuccess)
-            {
-                rc = bfail(b, GRLBM_ERR_CUDA, "autotune: trial steps failed");
-                break;
-            }
-            float ms = 0.f;
-            cudaEventElapsedTime(&ms, e0, e1);
-            if (best == 0.f || ms < best)
-                best = ms, best_bps = bps, best_lf = lf;
+            rc = bfail(b, GRLBM_ERR_CUDA, "autotune: trial steps failed");
+            break;
         }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (best == 0.f || ms < best)
+            best = ms, best_bps = shape.first, best_lf = shape.second;
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     // restore the saved state

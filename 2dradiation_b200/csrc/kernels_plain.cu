@@ -13,13 +13,18 @@
 
 // Resident blocks per SM the step kernel's register budget is sized for.
 #ifndef GRLBM_PLAIN_MIN_BLOCKS
-#define GRLBM_PLAIN_MIN_BLOCKS 4
+#define GRLBM_PLAIN_MIN_BLOCKS 3
+#endif
+// Unroll of the step's per-direction stream loop.
+#ifndef GRLBM_PLAIN_UNROLL
+#define GRLBM_PLAIN_UNROLL 1
 #endif
 
 namespace grlbm
 {
 namespace
 {
+constexpr int kPlainUnroll = GRLBM_PLAIN_UNROLL;
 // one stream value: StreamFlatFixed (src/Radiation.cpp:394-410) or
 // StreamCurvedFixed with IntensityAt (:478-508, 322-343)
 // `clamp_mask` receives bit q set where corner q's angular interpolation was
@@ -313,6 +318,7 @@ __global__ void __launch_bounds__(kStepBlock, GRLBM_PLAIN_MIN_BLOCKS) k_step_pla
     double4 r0 = make_double4(0, 0, 0, 0);
     if (CURVED && !ADAPTIVE)
         r0 = rp[0];
+#pragma unroll kPlainUnroll
     for (int d = 0; d < a.nd; d++)
     {
         double4 r1 = r0;

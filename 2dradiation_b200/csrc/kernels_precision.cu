@@ -26,13 +26,20 @@
 
 #include "device_common.cuh"
 
-// Tuning of the step kernel: resident blocks per SM the register budget is
-// sized for, and the unroll of the per-direction loop.
+// Tuning of the step kernels: resident blocks per SM the register budget is
+// sized for, and the unroll of the per-direction loop (the batch kernel,
+// which holds both streaming types, keeps the smaller one).
 #ifndef GRLBM_PREC_MIN_BLOCKS
 #define GRLBM_PREC_MIN_BLOCKS 5
 #endif
 #ifndef GRLBM_PREC_UNROLL
-#define GRLBM_PREC_UNROLL 2
+#define GRLBM_PREC_UNROLL 4
+#endif
+#ifndef GRLBM_BATCH_UNROLL
+#define GRLBM_BATCH_UNROLL 1
+#endif
+#ifndef GRLBM_PREC_PREFETCH
+#define GRLBM_PREC_PREFETCH 2
 #endif
 
 namespace grlbm
@@ -111,7 +118,6 @@ constexpr int kTileX = GRLBM_PREC_TILE_X, kTileY = kStepBlock / GRLBM_PREC_TILE_
 static_assert(kTileX * kTileY == kStepBlock, "tile = block");
 static_assert(kTileX % 4 == 0, "tile origins on 16-byte boundaries");
 constexpr int kPatchX = kTileX + 2, kPatchY = kTileY + 2;
-constexpr int kPrecUnroll = GRLBM_PREC_UNROLL;
 constexpr int kRing = 32, kMirror = kTaps - 1;
 static_assert(kSpan + kChunk <= kRing && (kRing & (kRing - 1)) == 0, "ring");
 constexpr int kRingSlots = kRing + kMirror;
@@ -199,7 +205,8 @@ __device__ __forceinline__ float *ring_base(unsigned char *smem_raw)
 
 // Stage virtual planes [v0, v0 + n) into their ring slots (and mirrors):
 // one phase of the mbarrier, issued by thread 0.
-__device__ __forceinline__ void stage_planes(const PrecStepArgs &a, const Stage &st, int v0, int n)
+__device__ __forceinline__ void stage_planes(const PrecStepArgs &a, const CUtensorMap *map, const Stage &st, int v0,
+                                             int n)
 {
     if (threadIdx.x != 0)
         return;
@@ -213,9 +220,9 @@ __device__ __forceinline__ void stage_planes(const PrecStepArgs &a, const Stage 
     {
         const int sl = (v0 + p + kBelow) & (kRing - 1);
         const int y = d * (int)a.g.ny + st.y0;
-        tma_load_2d(st.ring + (unsigned)(sl * kSlot) * 4u, &a.in_map, st.x0, y, st.bar);
+        tma_load_2d(st.ring + (unsigned)(sl * kSlot) * 4u, map, st.x0, y, st.bar);
         if (sl < kMirror)
-            tma_load_2d(st.ring + (unsigned)((sl + kRing) * kSlot) * 4u, &a.in_map, st.x0, y, st.bar);
+            tma_load_2d(st.ring + (unsigned)((sl + kRing) * kSlot) * 4u, map, st.x0, y, st.bar);
         d = (d + 1 == a.nd) ? 0 : d + 1;
     }
 }
@@ -358,9 +365,9 @@ __device__ __forceinline__ void collide_coeffs(float n1, float n2, float u1, flo
 // phase parity of the block's staging mbarrier, carried from tile to tile.
 // Returns false (for the whole block) when a staging wait ran out of time:
 // the fault word is then set and the tile is abandoned.
-template <bool CURVED>
-__device__ __forceinline__ bool step_tile(const PrecStepArgs &a, const DirTable &dt, int bx, int by,
-                                          unsigned char *smem_raw, unsigned &parity)
+template <bool CURVED, int UNROLL>
+__device__ __forceinline__ bool step_tile(const PrecStepArgs &a, const CUtensorMap *map, const DirTable &dt, int bx,
+                                          int by, unsigned char *smem_raw, unsigned &parity)
 {
     float *ring = ring_base(smem_raw);
     const int t = threadIdx.x;
@@ -393,7 +400,7 @@ __device__ __forceinline__ bool step_tile(const PrecStepArgs &a, const DirTable 
 
     const Stage st{smem_addr(ring), smem_addr(smem_raw), x0, y0};
     const int cell = ty * kBoxX + tx; // slot offset of node (i - 1, j - 1)
-    stage_planes(a, st, -kBelow, kSpan);
+    stage_planes(a, map, st, -kBelow, kSpan);
 
     KMoments km;
     km.zero();
@@ -403,10 +410,16 @@ __device__ __forceinline__ bool step_tile(const PrecStepArgs &a, const DirTable 
     const unsigned rs = (unsigned)a.g.ncell;
     const unsigned dlast = (unsigned)(a.nd - 1);
     float4 r0 = make_float4(0.f, 0.f, 0.f, 0.f), r1 = r0;
+#if GRLBM_PREC_PREFETCH == 3
+    float4 r1b = r0;
+#endif
     if (CURVED)
     {
         r0 = __ldcs(rp);
         r1 = __ldcs(rp + min(1u, dlast) * rs);
+#if GRLBM_PREC_PREFETCH == 3
+        r1b = __ldcs(rp + min(2u, dlast) * rs);
+#endif
     }
     for (int chunk0 = 0; chunk0 < a.nd; chunk0 += kChunk)
     {
@@ -423,14 +436,14 @@ __device__ __forceinline__ bool step_tile(const PrecStepArgs &a, const DirTable 
         }
         parity ^= 1u;
         if (chunk0 + kChunk < a.nd)
-            stage_planes(a, st, chunk0 + kSpan - kBelow, kChunk);
+            stage_planes(a, map, st, chunk0 + kSpan - kBelow, kChunk);
         const int dend = min(chunk0 + kChunk, a.nd);
-#pragma unroll kPrecUnroll
+#pragma unroll(UNROLL)
         for (int d = chunk0; d < dend; d++)
         {
             float4 r2 = r0;
             if (CURVED)
-                r2 = __ldcs(rp + min((unsigned)(d + 2), dlast) * rs);
+                r2 = __ldcs(rp + min((unsigned)(d + GRLBM_PREC_PREFETCH), dlast) * rs);
             float v = 0.f;
             if (live)
                 v = CURVED ? stream_curved(a, dt, ring, rowtab, d, r0, cell, (unsigned)cc + (unsigned)d * rs, ii, jj)
@@ -439,7 +452,12 @@ __device__ __forceinline__ bool step_tile(const PrecStepArgs &a, const DirTable 
                 Is[(unsigned)d * plane] = v;
             km.add(v, dirc[2 * d], dirc[2 * d + 1]);
             r0 = r1;
+#if GRLBM_PREC_PREFETCH == 3
+            r1 = r1b;
+            r1b = r2;
+#else
             r1 = r2;
+#endif
         }
         km.fold();
     }
@@ -582,7 +600,7 @@ __global__ void __launch_bounds__(kStepBlock, GRLBM_PREC_MIN_BLOCKS)
         mbar_init(smem_addr(smem_raw), 1);
     __syncthreads();
     unsigned parity = 0;
-    step_tile<CURVED>(a, dt, blockIdx.x, blockIdx.y, smem_raw, parity);
+    step_tile<CURVED, GRLBM_PREC_UNROLL>(a, &a.in_map, dt, blockIdx.x, blockIdx.y, smem_raw, parity);
 }
 
 // Many problems in one persistent launch: the blocks walk the concatenated
@@ -613,8 +631,8 @@ __global__ void __launch_bounds__(kStepBlock, GRLBM_PREC_MIN_BLOCKS)
         const int local = tile - first_tile[lo];
         const int bx = local % it.tiles_x, by = local / it.tiles_x;
         const PrecStepArgs &a = it.a[it.cur0 ^ flip];
-        const bool ok = it.curved ? step_tile<true>(a, *it.dt, bx, by, smem_raw, parity)
-                                  : step_tile<false>(a, *it.dt, bx, by, smem_raw, parity);
+        const bool ok = it.curved ? step_tile<true, GRLBM_BATCH_UNROLL>(a, &a.in_map, *it.dt, bx, by, smem_raw, parity)
+                                  : step_tile<false, GRLBM_BATCH_UNROLL>(a, &a.in_map, *it.dt, bx, by, smem_raw, parity);
         if (!ok)
             return; // the barrier's phase is unknown: the block stops (the fault word is set)
         __syncthreads(); // the next tile reuses the shared stage

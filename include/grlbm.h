@@ -241,9 +241,12 @@ int grlbm_copy_rows(grlbm_ctx *ctx, int64_t j_first, int64_t n, void *buffer, in
 int grlbm_departure_rows(grlbm_ctx *ctx, int32_t *rows);
 /* ---- batches ----------------------------------------------------------------
  * No counterpart in the reference.  Many GRLBM_PRECISION_FP32 problems on one
- * GPU (any grid sizes, direction counts, flat or curved streaming) stepped by
- * one persistent kernel launch per time step, replayed from CUDA graphs of
- * 32 steps.  Each problem's result is bit-identical to stepping it alone; its
+ * GPU (any grid sizes, direction counts, flat or curved streaming) stepped
+ * together, replayed from CUDA graphs of 32 steps, in one of two launch
+ * shapes: one persistent kernel launch per time step over all problems'
+ * tiles, or each problem's own step kernel with the problems' launch chains
+ * running concurrently inside the graph.  Each problem's result is
+ * bit-identical to stepping it alone; its
  * context stays usable (moments, intensities, statistics) between batch
  * steps.  Problems that keep source nodes active are not batched
  * (GRLBM_ERR_UNSUPPORTED).  A batch refers to its contexts: destroy it before
@@ -256,11 +259,16 @@ void grlbm_batch_destroy(grlbm_batch *batch);
 const char *grlbm_batch_last_error(const grlbm_batch *batch);
 /* n_steps time steps of every problem (synchronous). */
 int grlbm_batch_step(grlbm_batch *batch, int32_t n_steps);
-/* Times trial_steps steps for each launch shape -- resident blocks per SM
- * (the occupancy limit and up to two fewer) and the order of the problems'
- * tiles (as given, or largest problem first) -- keeps the fastest, and puts
- * every problem back in the state it had before the call.  The choice is
- * returned in *blocks_per_sm and *largest_first (either may be NULL). */
+/* Sets the launch shape: blocks_per_sm in [1, occupancy limit] for the
+ * persistent launch (with the problems' tiles as given or largest problem
+ * first), or 0 for the problems' own kernels launched concurrently. */
+int grlbm_batch_set_shape(grlbm_batch *batch, int32_t blocks_per_sm, int32_t largest_first);
+/* Times trial_steps steps for each launch shape -- the persistent launch at
+ * resident blocks per SM (the occupancy limit and up to two fewer) with the
+ * problems' tiles as given or largest problem first, and the concurrent
+ * launches (0) -- keeps the fastest, and puts every problem back in the
+ * state it had before the call.  The choice is returned in *blocks_per_sm and
+ * *largest_first (either may be NULL). */
 int grlbm_batch_autotune(grlbm_batch *batch, int32_t trial_steps, int32_t *blocks_per_sm, int32_t *largest_first);
 /* ---- adjoint ------------------------------------------------------------------
  * No counterpart in the reference.  Gradients of a loss of the final

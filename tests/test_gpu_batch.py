@@ -1,9 +1,9 @@
 """Batched precision-form steps (grlbm_batch_*): problems of different grid
-sizes, direction counts and streaming types advanced by one persistent launch
-per step must each match their single-problem run bit for bit -- across
-graph-replayed and single steps, after autotuning (which must leave every
-problem as it was), and when a problem is also stepped on its own between
-batch steps."""
+sizes, direction counts and streaming types advanced together -- by one
+persistent launch per step or by their own kernels launched concurrently --
+must each match their single-problem run bit for bit, across graph-replayed
+and single steps, after autotuning (which must leave every problem as it
+was), and when a problem is also stepped on its own between batch steps."""
 import numpy as np
 import pytest
 
@@ -23,7 +23,7 @@ def test_batch_matches_single_problems(grlbm, W):
     try:
         with grlbm.Batch(probs) as b:
             choice = b.autotune(3)
-            assert choice["blocks_per_sm"] >= 1
+            assert choice["blocks_per_sm"] >= 0
             b.step(37)          # one 32-step graph and 5 single launches
             probs[0].step(1)    # a problem stepped on its own in between
             b.step(6)
@@ -31,6 +31,34 @@ def test_batch_matches_single_problems(grlbm, W):
             assert np.array_equal(r.moments_if()["E"], E), k
             assert np.array_equal(r.intensity(), I), k
             assert r.stats()["average_iterations"] == it, k
+    finally:
+        for r in probs:
+            r.close()
+
+
+@pytest.mark.parametrize("shape", [(0, True), (1, False), (5, True)])
+def test_batch_shapes_match_single_problems(grlbm, W, shape):
+    """Each launch shape, set explicitly: the concurrent launches (0) and the
+    persistent launch at 1 and 5 blocks per SM (capped at the occupancy limit)."""
+    cases = W.batch_instances(count=5, seed=21, sizes=(24, 37, 64), dirs=(8, 16, 32), steps=40)
+    P = grlbm.PRECISION_FP32
+    ref = []
+    for c in cases:
+        with grlbm.prepare(c, P) as r:
+            r.step(35)
+            ref.append(r.intensity())
+    probs = [grlbm.prepare(c, P) for c in cases]
+    try:
+        with grlbm.Batch(probs) as b:
+            bps, lf = shape
+            try:
+                b.set_shape(bps, lf)
+            except grlbm.GrlbmError:
+                assert bps > 1  # above this kernel's occupancy limit
+                b.set_shape(1, lf)
+            b.step(35)  # one 32-step graph and 3 single steps
+        for k, (r, I) in enumerate(zip(probs, ref)):
+            assert np.array_equal(r.intensity(), I), k
     finally:
         for r in probs:
             r.close()
