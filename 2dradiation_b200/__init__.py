@@ -83,6 +83,8 @@ SIGNATURES = {
     "grlbm_compute_moments_lf": ([C.c_void_p] + [_D] * 7, C.c_int),
     "grlbm_energy": ([C.c_void_p, _D], C.c_int),
     "grlbm_energy_noalloc": ([C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p], C.c_int),
+    "grlbm_selftest_staging_wait": ([C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_int32),
+                                     C.POINTER(C.c_double)], C.c_int),
     "grlbm_get_stats": ([C.c_void_p, C.POINTER(Stats)], C.c_int),
     "grlbm_batch_create": ([C.POINTER(C.c_void_p), C.c_int32, C.POINTER(C.c_void_p)], C.c_int),
     "grlbm_batch_destroy": ([C.c_void_p], None),
@@ -417,6 +419,15 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def selftest_staging_wait(arrive: bool, limit_us: int, device: int = -1) -> dict:
+    """One block's bounded wait on an mbarrier phase that nothing (arrive
+    False) or one thread (arrive True) completes: {"completed", "waited_us"}."""
+    done, waited = C.c_int32(-1), C.c_double(0.0)
+    _check(lib().grlbm_selftest_staging_wait(device, int(bool(arrive)), int(limit_us), C.byref(done),
+                                             C.byref(waited)))
+    return {"completed": bool(done.value), "waited_us": waited.value}
 
 
 def prepare(case: dict, precision: int = PLAIN_FP64, device: int = -1) -> Radiation:

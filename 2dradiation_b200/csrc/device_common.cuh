@@ -300,6 +300,9 @@ cudaError_t prepare_step_plain(int smem_bytes);
 void launch_step_plain(const PlainStepArgs &a, bool curved, cudaStream_t s, const StepRecord *record = nullptr);
 cudaError_t prepare_step_prec(int smem_bytes);
 size_t step_prec_smem(int nd);
+// One block's bounded wait on an mbarrier phase nothing (arrive = 0) or one
+// arrival (arrive = 1) completes; synchronous.
+cudaError_t run_wait_selftest(int arrive, unsigned long long limit_ns, int *completed, unsigned long long *waited_ns);
 // The TMA map the precision step stages Iin through (a state buffer of
 // layout L and nd planes over ny rows each).
 cudaError_t encode_state_map(CUtensorMap *map, const float *state, const StateLayout &L, int64_t ny, int nd);

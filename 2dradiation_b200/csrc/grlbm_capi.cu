@@ -399,6 +399,28 @@ extern "C" {
 
 const char *grlbm_last_error(const grlbm_ctx *ctx) { return ctx ? ctx->err.c_str() : g_create_error.c_str(); }
 
+int grlbm_selftest_staging_wait(int32_t device, int32_t arrive, int32_t limit_us, int32_t *completed,
+                                double *waited_us)
+{
+    if (!completed || !waited_us || limit_us < 1 || limit_us > 1000000)
+        return fail(nullptr, GRLBM_ERR_ARGUMENT, "need outputs and a limit in [1, 1000000] us");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(nullptr, GRLBM_ERR_CUDA, "no CUDA device available");
+    if (device >= ndev)
+        return fail(nullptr, GRLBM_ERR_ARGUMENT, "device %d does not exist", device);
+    if (device >= 0 && cudaSetDevice(device) != cudaSuccess)
+        return fail(nullptr, GRLBM_ERR_CUDA, "cudaSetDevice failed");
+    int done = -1;
+    unsigned long long ns = 0;
+    const cudaError_t e = run_wait_selftest(arrive != 0, (unsigned long long)limit_us * 1000ull, &done, &ns);
+    if (e != cudaSuccess)
+        return fail(nullptr, GRLBM_ERR_CUDA, "staging-wait self-test: %s", cudaGetErrorString(e));
+    *completed = done;
+    *waited_us = (double)ns / 1e3;
+    return GRLBM_OK;
+}
+
 int32_t grlbm_metric_array_count(void) { return kMetricArrays; }
 
 int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, const grlbm_run_desc *run,

@@ -38,9 +38,6 @@
 #ifndef GRLBM_BATCH_UNROLL
 #define GRLBM_BATCH_UNROLL 1
 #endif
-#ifndef GRLBM_PREC_PREFETCH
-#define GRLBM_PREC_PREFETCH 2
-#endif
 
 namespace grlbm
 {
@@ -410,16 +407,10 @@ __device__ __forceinline__ bool step_tile(const PrecStepArgs &a, const CUtensorM
     const unsigned rs = (unsigned)a.g.ncell;
     const unsigned dlast = (unsigned)(a.nd - 1);
     float4 r0 = make_float4(0.f, 0.f, 0.f, 0.f), r1 = r0;
-#if GRLBM_PREC_PREFETCH == 3
-    float4 r1b = r0;
-#endif
     if (CURVED)
     {
         r0 = __ldcs(rp);
         r1 = __ldcs(rp + min(1u, dlast) * rs);
-#if GRLBM_PREC_PREFETCH == 3
-        r1b = __ldcs(rp + min(2u, dlast) * rs);
-#endif
     }
     for (int chunk0 = 0; chunk0 < a.nd; chunk0 += kChunk)
     {
@@ -443,7 +434,7 @@ __device__ __forceinline__ bool step_tile(const PrecStepArgs &a, const CUtensorM
         {
             float4 r2 = r0;
             if (CURVED)
-                r2 = __ldcs(rp + min((unsigned)(d + GRLBM_PREC_PREFETCH), dlast) * rs);
+                r2 = __ldcs(rp + min((unsigned)(d + 2), dlast) * rs);
             float v = 0.f;
             if (live)
                 v = CURVED ? stream_curved(a, dt, ring, rowtab, d, r0, cell, (unsigned)cc + (unsigned)d * rs, ii, jj)
@@ -452,12 +443,7 @@ __device__ __forceinline__ bool step_tile(const PrecStepArgs &a, const CUtensorM
                 Is[(unsigned)d * plane] = v;
             km.add(v, dirc[2 * d], dirc[2 * d + 1]);
             r0 = r1;
-#if GRLBM_PREC_PREFETCH == 3
-            r1 = r1b;
-            r1b = r2;
-#else
             r1 = r2;
-#endif
         }
         km.fold();
     }
@@ -639,8 +625,50 @@ __global__ void __launch_bounds__(kStepBlock, GRLBM_PREC_MIN_BLOCKS)
     }
 }
 
+// The bounded staging wait on its own: one block waits on a phase of its
+// mbarrier that nothing completes (arrive = 0) or that thread 0 completes
+// (arrive = 1); the wait returns either way.
+__global__ void k_wait_selftest(int arrive, unsigned long long limit_ns, int *completed, unsigned long long *waited_ns)
+{
+    __shared__ __align__(8) unsigned long long bar_word;
+    const unsigned bar = smem_addr(&bar_word);
+    if (threadIdx.x == 0)
+        mbar_init(bar, 1);
+    __syncthreads();
+    if (arrive && threadIdx.x == 0)
+        mbar_arrive_expect(bar, 0u);
+    const unsigned long long t0 = global_ns();
+    const bool done = mbar_wait(bar, 0u, limit_ns, nullptr);
+    const unsigned long long t1 = global_ns();
+    if (threadIdx.x == 0)
+    {
+        *completed = done ? 1 : 0;
+        *waited_ns = t1 - t0;
+    }
+}
+
 inline unsigned nblk(int64_t n, int b) { return (unsigned)((n + b - 1) / b); }
 } // namespace
+
+cudaError_t run_wait_selftest(int arrive, unsigned long long limit_ns, int *completed, unsigned long long *waited_ns)
+{
+    void *buf = nullptr;
+    cudaError_t e = cudaMalloc(&buf, 16);
+    if (e != cudaSuccess)
+        return e;
+    int *d_done = static_cast<int *>(buf);
+    unsigned long long *d_ns = reinterpret_cast<unsigned long long *>(static_cast<char *>(buf) + 8);
+    k_wait_selftest<<<1, 32>>>(arrive, limit_ns, d_done, d_ns);
+    e = cudaGetLastError();
+    if (e == cudaSuccess)
+        e = cudaDeviceSynchronize();
+    if (e == cudaSuccess)
+        e = cudaMemcpy(completed, d_done, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(waited_ns, d_ns, sizeof(unsigned long long), cudaMemcpyDeviceToHost);
+    cudaFree(buf);
+    return e;
+}
 
 int step_prec_tiles_x(int64_t nx_) { return (int)nblk(nx_, kTileX); }
 int step_prec_tiles_y(int64_t rows) { return (int)nblk(rows, kTileY); }

@@ -127,6 +127,15 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric,
                  const grlbm_run_desc *run, int32_t device, grlbm_ctx **out);
 void grlbm_destroy(grlbm_ctx *ctx);
 const char *grlbm_last_error(const grlbm_ctx *ctx);
+/* No counterpart in the reference.  Exercises the time limit of the
+ * precision step's shared-memory staging wait on `device` (-1: the current
+ * one): one block waits on an mbarrier phase that nothing completes
+ * (arrive = 0) or that one of its threads completes (arrive = 1), for at most
+ * limit_us microseconds (1 .. 1,000,000).  *completed receives 1 when the
+ * phase completed and 0 when the wait ran out; *waited_us the wait's length
+ * on the device clock.  The kernel returns either way; nothing faults. */
+int grlbm_selftest_staging_wait(int32_t device, int32_t arrive, int32_t limit_us, int32_t *completed,
+                                double *waited_us);
 
 /* Grid members nx, ny, dx, dy, dt (src/Grid.h:17-21). */
 int grlbm_get_grid(const grlbm_ctx *ctx, int64_t *nx, int64_t *ny, double *dx, double *dy,

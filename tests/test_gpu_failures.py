@@ -39,3 +39,20 @@ def test_bad_host_arguments(grlbm, W):
         assert grlbm.lib().grlbm_step(r.h, -1) == 1
         assert grlbm.lib().grlbm_update_fourier_coefficients(r.h, -1.0, 0) == 1
         assert "rk_tol" in grlbm.lib().grlbm_last_error(r.h).decode()
+
+
+def test_staging_wait_runs_out_and_returns(grlbm, W):
+    """The precision step's staging wait has a time limit: a wait on an
+    mbarrier phase that nothing completes returns after the limit (and the
+    context stays usable); with one arrival it returns at once."""
+    out = grlbm.selftest_staging_wait(arrive=False, limit_us=2000)
+    assert out["completed"] is False
+    assert 2000 <= out["waited_us"] < 1e6
+    out = grlbm.selftest_staging_wait(arrive=True, limit_us=2000)
+    assert out["completed"] is True and out["waited_us"] < 2000
+    case = W.curved_shell(nx_=24, ny_=24, n_dir=16, n_fourier=5, steps=2)
+    res = grlbm.run(case, 1)
+    assert np.isfinite(res["E"]).all()
+    with pytest.raises(grlbm.GrlbmError) as e:
+        grlbm.selftest_staging_wait(arrive=False, limit_us=0)
+    assert e.value.code == 1
