@@ -191,6 +191,7 @@ struct PlainStepArgs
     const double *ang_old, *ang_new;
     const double *coef; // [5][nxy][nf]
     int nf;
+    int sms; // SMs of the device (chooses the launch's register budget)
 };
 
 struct PrecStepArgs

@@ -45,6 +45,7 @@ struct grlbm_ctx
 {
     std::string err;
     int device = 0;
+    int sms = 1; // the device's SM count
     cudaStream_t stream = nullptr;
     // host tables
     GridGeom geo;
@@ -256,6 +257,7 @@ PlainStepArgs plain_args(grlbm_ctx *ctx, int from)
     a.mom = ctx->mom.as<double>();
     a.iter_sum = cnt;
     a.iter_max = reinterpret_cast<unsigned int *>(cnt + 1);
+    a.sms = ctx->sms;
     return a;
 }
 
@@ -476,6 +478,7 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
             return fail(nullptr, GRLBM_ERR_CUDA, "cudaSetDevice failed");
     }
     cudaGetDevice(&ctx->device);
+    cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, ctx->device);
     if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess)
         return fail(nullptr, GRLBM_ERR_CUDA, "cudaStreamCreate failed");
 

@@ -11,10 +11,10 @@
 #include "approx_math.hpp"
 #include "device_common.cuh"
 
-// Resident blocks per SM the step kernel's register budget is sized for.
-#ifndef GRLBM_PLAIN_MIN_BLOCKS
-#define GRLBM_PLAIN_MIN_BLOCKS 3
-#endif
+// Resident blocks per SM the step kernel's register budget is sized for:
+// the kernel is built for both, and each launch takes the one whose grid
+// needs fewer waves (the larger budget when they tie: it does not spill).
+constexpr int kPlainBlocksLo = 3, kPlainBlocksHi = 4;
 // Unroll of the step's per-direction stream loop.
 #ifndef GRLBM_PLAIN_UNROLL
 #define GRLBM_PLAIN_UNROLL 1
@@ -280,8 +280,8 @@ __device__ __forceinline__ double stream_value_adaptive(const PlainStepArgs &a, 
 // streaming types -- each cell's stencil is rotated by its new angle (its
 // directions in stream, moments and collide) and corners are read in their
 // previous frames.
-template <bool CURVED, bool RECORD, bool ADAPTIVE>
-__global__ void __launch_bounds__(kStepBlock, GRLBM_PLAIN_MIN_BLOCKS) k_step_plain(PlainStepArgs a, StepRecord rec)
+template <bool CURVED, bool RECORD, bool ADAPTIVE, int MINB>
+__global__ void __launch_bounds__(kStepBlock, MINB) k_step_plain(PlainStepArgs a, StepRecord rec)
 {
     const int t = threadIdx.x;
     // cells of the slab rows [jlo, jhi), numbered from its first cell
@@ -685,34 +685,48 @@ cudaError_t prepare_step_plain(int smem_bytes)
     (void)smem_bytes; // the plain step uses no dynamic shared memory
     return cudaSuccess;
 }
-void launch_step_plain(const PlainStepArgs &a, bool curved, cudaStream_t s, const StepRecord *record)
+template <int MINB>
+void launch_step_plain_as(const PlainStepArgs &a, bool curved, cudaStream_t s, const StepRecord *record,
+                          unsigned blocks)
 {
-    const size_t smem = 0;
-    const int64_t cells = (a.g.jhi - a.g.jlo) * a.g.nx_;
-    if (cells <= 0)
-        return;
     const StepRecord none{};
-    const unsigned blocks = nblk(cells, kStepBlock);
     if (a.ang_new) // adaptive streaming
     {
-        k_rotation_update<<<nblk(cells, 128), 128, 0, s>>>(a.g, a.mom, a.ang_old, const_cast<double *>(a.ang_new));
         if (curved)
-            k_step_plain<true, false, true><<<blocks, kStepBlock, smem, s>>>(a, none);
+            k_step_plain<true, false, true, MINB><<<blocks, kStepBlock, 0, s>>>(a, none);
         else
-            k_step_plain<false, false, true><<<blocks, kStepBlock, smem, s>>>(a, none);
-        k_zero_halo_moments<<<nblk(a.g.nxy, 256), 256, 0, s>>>(a.g, a.mom);
+            k_step_plain<false, false, true, MINB><<<blocks, kStepBlock, 0, s>>>(a, none);
     }
     else if (record)
     {
         if (curved)
-            k_step_plain<true, true, false><<<blocks, kStepBlock, smem, s>>>(a, *record);
+            k_step_plain<true, true, false, MINB><<<blocks, kStepBlock, 0, s>>>(a, *record);
         else
-            k_step_plain<false, true, false><<<blocks, kStepBlock, smem, s>>>(a, *record);
+            k_step_plain<false, true, false, MINB><<<blocks, kStepBlock, 0, s>>>(a, *record);
     }
     else if (curved)
-        k_step_plain<true, false, false><<<blocks, kStepBlock, smem, s>>>(a, none);
+        k_step_plain<true, false, false, MINB><<<blocks, kStepBlock, 0, s>>>(a, none);
     else
-        k_step_plain<false, false, false><<<blocks, kStepBlock, smem, s>>>(a, none);
+        k_step_plain<false, false, false, MINB><<<blocks, kStepBlock, 0, s>>>(a, none);
+}
+
+void launch_step_plain(const PlainStepArgs &a, bool curved, cudaStream_t s, const StepRecord *record)
+{
+    const int64_t cells = (a.g.jhi - a.g.jlo) * a.g.nx_;
+    if (cells <= 0)
+        return;
+    const unsigned blocks = nblk(cells, kStepBlock);
+    const int64_t sms = a.sms > 0 ? a.sms : 1;
+    const int64_t waves_lo = (blocks + kPlainBlocksLo * sms - 1) / (kPlainBlocksLo * sms);
+    const int64_t waves_hi = (blocks + kPlainBlocksHi * sms - 1) / (kPlainBlocksHi * sms);
+    if (a.ang_new)
+        k_rotation_update<<<nblk(cells, 128), 128, 0, s>>>(a.g, a.mom, a.ang_old, const_cast<double *>(a.ang_new));
+    if (waves_hi < waves_lo)
+        launch_step_plain_as<kPlainBlocksHi>(a, curved, s, record, blocks);
+    else
+        launch_step_plain_as<kPlainBlocksLo>(a, curved, s, record, blocks);
+    if (a.ang_new)
+        k_zero_halo_moments<<<nblk(a.g.nxy, 256), 256, 0, s>>>(a.g, a.mom);
 }
 void launch_sources64(double *I, int64_t nxy, int nd, const int64_t *nodes, const double *vals, int64_t nsrc,
                       cudaStream_t s)
