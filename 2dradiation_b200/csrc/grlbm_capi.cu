@@ -69,6 +69,7 @@ struct grlbm_ctx
     int64_t nsrc_ang = 0;
     std::vector<double> flux_angle;
     DevBuf ig_rows, ia3;
+    DevBuf streamed; // plain form, fixed streaming: the streamed values of a step
     DirTable dirs{}; // precision-form direction tables (kernel parameter)
     DevBuf cu1, cu2, clor, cadt, ceta, ck0, ck3, cka, mom, rkf, lfp;
     DevBuf coef, ss_cx, ss_cy, ss_w, proj_basis, eval_basis, stage;
@@ -258,6 +259,7 @@ PlainStepArgs plain_args(grlbm_ctx *ctx, int from)
     a.iter_sum = cnt;
     a.iter_max = reinterpret_cast<unsigned int *>(cnt + 1);
     a.sms = ctx->sms;
+    a.S = ctx->streamed.as<double>();
     return a;
 }
 
@@ -737,6 +739,8 @@ std::vector<IgRow> rows(ctx->ng);
     }
     TRY(alloc(ctx, ctx->I[0], ib));
     TRY(alloc(ctx, ctx->I[1], ib));
+    if (!ctx->fp32 && !is_adaptive(ctx))
+        TRY(alloc(ctx, ctx->streamed, (size_t)nxy * nd * sizeof(double)));
     TRY(alloc(ctx, ctx->mom, (size_t)6 * nxy * tsize(ctx)));
     TRY(alloc(ctx, ctx->rec, (size_t)ctx->ncell * nd * (ctx->fp32 ? sizeof(float4) : sizeof(double4))));
     if (ctx->fp32)

@@ -280,63 +280,22 @@ __device__ __forceinline__ double stream_value_adaptive(const PlainStepArgs &a, 
 // streaming types -- each cell's stencil is rotated by its new angle (its
 // directions in stream, moments and collide) and corners are read in their
 // previous frames.
-template <bool CURVED, bool RECORD, bool ADAPTIVE, int MINB>
-__global__ void __launch_bounds__(kStepBlock, MINB) k_step_plain(PlainStepArgs a, StepRecord rec)
-{
-    const int t = threadIdx.x;
-    // cells of the slab rows [jlo, jhi), numbered from its first cell
-    const int64_t c0 = (a.g.jlo - 1) * a.g.nx_;
-    const int64_t c = (int64_t)blockIdx.x * kStepBlock + t;
-    const bool active = c < (a.g.jhi - a.g.jlo) * a.g.nx_;
-    const int64_t cc = c0 + (active ? c : 0);
-    const int64_t i = 1 + cc % a.g.nx_, j = 1 + cc / a.g.nx_;
-    const int64_t ij = i + j * a.g.nx;
-    const int64_t nxy = a.g.nxy;
-    const uint8_t fl = active ? a.flags[ij] : (uint8_t)3;
-    const bool zero_stream = CURVED && (fl & 2);
-    const bool collides = active && !(fl & 1);
-    // The streamed intensities of a colliding cell wait in its own output
-    // slots until the lambda iteration has converged (nothing else reads or
-    // writes them in this step); non-colliding cells keep their slots.
-    double *Is = a.Iout + ij;
-    // the cell's rotation (RotationMatrix(rotationAngle[ij]), src/DataTypes.hh:630-635)
-    double rot_s = 0.0, rot_c = 1.0;
-    if (ADAPTIVE)
-    {
-        const double th = a.ang_new[ij];
-        rot_s = approx_sin(th);
-        rot_c = approx_cos(th);
-    }
+// direction d of a cell's stencil (rotated by the cell's angle in adaptive streaming)
 #define GRLBM_N1(d) (ADAPTIVE ? __ldg(a.cx + (d)) * rot_c - __ldg(a.cy + (d)) * rot_s : __ldg(a.n1 + (d)))
 #define GRLBM_N2(d) (ADAPTIVE ? __ldg(a.cx + (d)) * rot_s + __ldg(a.cy + (d)) * rot_c : __ldg(a.n2 + (d)))
 
-    Moments m;
-    m.zero();
-    // departure records, prefetched one direction ahead (the last stands in
-    // past the end)
-    const double4 *rp = a.rec + cc;
-    double4 r0 = make_double4(0, 0, 0, 0);
-    if (CURVED && !ADAPTIVE)
-        r0 = rp[0];
-#pragma unroll kPlainUnroll
-    for (int d = 0; d < a.nd; d++)
-    {
-        double4 r1 = r0;
-        if (CURVED && !ADAPTIVE)
-            r1 = rp[(int64_t)min(d + 1, a.nd - 1) * a.g.ncell];
-        unsigned cm = 0xFu;
-        double val = 0.0;
-        if (active && !zero_stream)
-            val = ADAPTIVE ? stream_value_adaptive<CURVED>(a, d, i, j, ij, rot_s, rot_c)
-                           : stream_value<CURVED>(a, d, r0, i, j, ij, cm);
-        if (RECORD && active)
-            rec.clamp[(int64_t)d * a.g.ncell + cc] = (uint8_t)cm;
-        if (collides)
-            Is[(int64_t)d * nxy] = val;
-        m.add(__ldg(a.w + d), val, GRLBM_N1(d), GRLBM_N2(d));
-        r0 = r1;
-    }
-
+// The rest of a step for one cell once its streamed values are known: m
+// holds their moments; Sin points at them (direction stride nxy), Sout at the
+// cell's output slots (the same slots in the fused step).  Collide
+// (src/Radiation.cpp:641-736) for a colliding cell, then the stored moments
+// and the lambda-iteration statistics.
+template <bool RECORD, bool ADAPTIVE>
+__device__ __forceinline__ void finish_cell(const PlainStepArgs &a, const StepRecord &rec, bool active, bool collides,
+                                            int64_t ij, int64_t cc, Moments m, const double *Sin, double *Sout,
+                                            double rot_s, double rot_c)
+{
+    const int t = threadIdx.x;
+    const int64_t nxy = a.g.nxy;
     int cycles = 0;
     if (RECORD && active)
         rec.e0[cc] = m.E;
@@ -374,7 +333,7 @@ __global__ void __launch_bounds__(kStepBlock, MINB) k_step_plain(PlainStepArgs a
                 for (int d = 0; d < a.nd; d++)
                 {
                     const double n1 = GRLBM_N1(d), n2 = GRLBM_N2(d);
-                    const double num = Is[(int64_t)d * nxy] + adt * (eta + (k0fE + k3 * (n1 * fFx + n2 * fFy)));
+                    const double num = Sin[(int64_t)d * nxy] + adt * (eta + (k0fE + k3 * (n1 * fFx + n2 * fFy)));
                     const double v = fast_div ? div_rn(num, den, rden) : num / den;
                     m.add(__ldg(a.w + d), v, n1, n2);
                 }
@@ -383,7 +342,7 @@ __global__ void __launch_bounds__(kStepBlock, MINB) k_step_plain(PlainStepArgs a
                 for (int d = 0; d < a.nd; d++)
                 {
                     const double n1 = GRLBM_N1(d), n2 = GRLBM_N2(d);
-                    const double v = collide_value(Is[(int64_t)d * nxy], n1, n2, u1, u2, lor, adt, eta, k0, k3,
+                    const double v = collide_value(Sin[(int64_t)d * nxy], n1, n2, u1, u2, lor, adt, eta, k0, k3,
                                                    kak0, fE, fFx, fFy);
                     m.add(__ldg(a.w + d), v, n1, n2);
                 }
@@ -398,13 +357,13 @@ __global__ void __launch_bounds__(kStepBlock, MINB) k_step_plain(PlainStepArgs a
             for (int d = 0; d < a.nd; d++)
             {
                 const double n1 = GRLBM_N1(d), n2 = GRLBM_N2(d);
-                const double num = Is[(int64_t)d * nxy] + adt * (eta + (k0fE + k3 * (n1 * fFx + n2 * fFy)));
-                Is[(int64_t)d * nxy] = fast_div ? div_rn(num, den, rden) : num / den;
+                const double num = Sin[(int64_t)d * nxy] + adt * (eta + (k0fE + k3 * (n1 * fFx + n2 * fFy)));
+                Sout[(int64_t)d * nxy] = fast_div ? div_rn(num, den, rden) : num / den;
             }
         }
         else
             for (int d = 0; d < a.nd; d++)
-                Is[(int64_t)d * nxy] = collide_value(Is[(int64_t)d * nxy], GRLBM_N1(d), GRLBM_N2(d), u1, u2,
+                Sout[(int64_t)d * nxy] = collide_value(Sin[(int64_t)d * nxy], GRLBM_N1(d), GRLBM_N2(d), u1, u2,
                                                      lor, adt, eta, k0, k3, kak0, fE, fFx, fFy);
     }
     if (RECORD && active)
@@ -431,9 +390,117 @@ __global__ void __launch_bounds__(kStepBlock, MINB) k_step_plain(PlainStepArgs a
         atomicAdd(a.iter_sum, (unsigned long long)sum);
         atomicMax(a.iter_max, mx);
     }
+}
+
+template <bool CURVED, bool RECORD, bool ADAPTIVE, int MINB>
+__global__ void __launch_bounds__(kStepBlock, MINB) k_step_plain(PlainStepArgs a, StepRecord rec)
+{
+    const int t = threadIdx.x;
+    // cells of the slab rows [jlo, jhi), numbered from its first cell
+    const int64_t c0 = (a.g.jlo - 1) * a.g.nx_;
+    const int64_t c = (int64_t)blockIdx.x * kStepBlock + t;
+    const bool active = c < (a.g.jhi - a.g.jlo) * a.g.nx_;
+    const int64_t cc = c0 + (active ? c : 0);
+    const int64_t i = 1 + cc % a.g.nx_, j = 1 + cc / a.g.nx_;
+    const int64_t ij = i + j * a.g.nx;
+    const int64_t nxy = a.g.nxy;
+    const uint8_t fl = active ? a.flags[ij] : (uint8_t)3;
+    const bool zero_stream = CURVED && (fl & 2);
+    const bool collides = active && !(fl & 1);
+    // The streamed intensities of a colliding cell wait in its own output
+    // slots until the lambda iteration has converged (nothing else reads or
+    // writes them in this step); non-colliding cells keep their slots.
+    double *Is = a.Iout + ij;
+    // the cell's rotation (RotationMatrix(rotationAngle[ij]), src/DataTypes.hh:630-635)
+    double rot_s = 0.0, rot_c = 1.0;
+    if (ADAPTIVE)
+    {
+        const double th = a.ang_new[ij];
+        rot_s = approx_sin(th);
+        rot_c = approx_cos(th);
+    }
+    Moments m;
+    m.zero();
+    // departure records, prefetched one direction ahead (the last stands in
+    // past the end)
+    const double4 *rp = a.rec + cc;
+    double4 r0 = make_double4(0, 0, 0, 0);
+    if (CURVED && !ADAPTIVE)
+        r0 = rp[0];
+#pragma unroll kPlainUnroll
+    for (int d = 0; d < a.nd; d++)
+    {
+        double4 r1 = r0;
+        if (CURVED && !ADAPTIVE)
+            r1 = rp[(int64_t)min(d + 1, a.nd - 1) * a.g.ncell];
+        unsigned cm = 0xFu;
+        double val = 0.0;
+        if (active && !zero_stream)
+            val = ADAPTIVE ? stream_value_adaptive<CURVED>(a, d, i, j, ij, rot_s, rot_c)
+                           : stream_value<CURVED>(a, d, r0, i, j, ij, cm);
+        if (RECORD && active)
+            rec.clamp[(int64_t)d * a.g.ncell + cc] = (uint8_t)cm;
+        if (collides)
+            Is[(int64_t)d * nxy] = val;
+        m.add(__ldg(a.w + d), val, GRLBM_N1(d), GRLBM_N2(d));
+        r0 = r1;
+    }
+
+    finish_cell<RECORD, ADAPTIVE>(a, rec, active, collides, ij, cc, m, Is, Is, rot_s, rot_c);
+}
+
+// The fixed streaming types run the step as two kernels, so that the
+// stream's dependent gathers (record, interpolation rows, 32 corner taps)
+// of different directions run in different threads instead of one after the
+// other in one thread per cell.  Stream: one thread per (cell, direction) of
+// the slab rows writes the streamed value to S (and, recording, the corner
+// clamp mask).
+template <bool CURVED, bool RECORD>
+__global__ void __launch_bounds__(kStepBlock) k_stream_plain(PlainStepArgs a, StepRecord rec)
+{
+    const int64_t c = (int64_t)blockIdx.x * kStepBlock + threadIdx.x;
+    const int d = blockIdx.y;
+    if (c >= (a.g.jhi - a.g.jlo) * a.g.nx_)
+        return;
+    const int64_t cc = (a.g.jlo - 1) * a.g.nx_ + c;
+    const int64_t i = 1 + cc % a.g.nx_, j = 1 + cc / a.g.nx_;
+    const int64_t ij = i + j * a.g.nx;
+    unsigned cm = 0xFu;
+    double val = 0.0;
+    if (!(CURVED && (a.flags[ij] & 2)))
+    {
+        const double4 r = CURVED ? a.rec[(int64_t)d * a.g.ncell + cc] : make_double4(0, 0, 0, 0);
+        val = stream_value<CURVED>(a, d, r, i, j, ij, cm);
+    }
+    if (RECORD)
+        rec.clamp[(int64_t)d * a.g.ncell + cc] = (uint8_t)cm;
+    a.S[(int64_t)d * a.g.nxy + ij] = val;
+}
+
+// Moments and collide: one thread per cell sums the moments of its streamed
+// values in direction order (ComputeMomentsIF's order, as the fused step
+// does) and finishes the cell; the collided intensities go to Iout.
+template <bool RECORD>
+__global__ void __launch_bounds__(kStepBlock) k_collide_plain(PlainStepArgs a, StepRecord rec)
+{
+    const int64_t c0 = (a.g.jlo - 1) * a.g.nx_;
+    const int64_t c = (int64_t)blockIdx.x * kStepBlock + threadIdx.x;
+    const bool active = c < (a.g.jhi - a.g.jlo) * a.g.nx_;
+    const int64_t cc = c0 + (active ? c : 0);
+    const int64_t i = 1 + cc % a.g.nx_, j = 1 + cc / a.g.nx_;
+    const int64_t ij = i + j * a.g.nx;
+    const int64_t nxy = a.g.nxy;
+    const bool collides = active && !(a.flags[ij] & 1);
+    const double *Sin = a.S + ij;
+    Moments m;
+    m.zero();
+    if (active)
+        for (int d = 0; d < a.nd; d++)
+            m.add(__ldg(a.w + d), Sin[(int64_t)d * nxy], __ldg(a.n1 + d), __ldg(a.n2 + d));
+    finish_cell<RECORD, false>(a, rec, active, collides, ij, cc, m, Sin, a.Iout + ij, 0.0, 1.0);
+}
 #undef GRLBM_N1
 #undef GRLBM_N2
-}
 
 // UpdateRotationMatrizes (src/Radiation.cpp:361-378): for the interior cells
 // of the slab, the angle of the flux averaged over the 3x3 neighbourhood
@@ -686,28 +753,13 @@ cudaError_t prepare_step_plain(int smem_bytes)
     return cudaSuccess;
 }
 template <int MINB>
-void launch_step_plain_as(const PlainStepArgs &a, bool curved, cudaStream_t s, const StepRecord *record,
-                          unsigned blocks)
+void launch_step_adaptive_as(const PlainStepArgs &a, bool curved, cudaStream_t s, unsigned blocks)
 {
     const StepRecord none{};
-    if (a.ang_new) // adaptive streaming
-    {
-        if (curved)
-            k_step_plain<true, false, true, MINB><<<blocks, kStepBlock, 0, s>>>(a, none);
-        else
-            k_step_plain<false, false, true, MINB><<<blocks, kStepBlock, 0, s>>>(a, none);
-    }
-    else if (record)
-    {
-        if (curved)
-            k_step_plain<true, true, false, MINB><<<blocks, kStepBlock, 0, s>>>(a, *record);
-        else
-            k_step_plain<false, true, false, MINB><<<blocks, kStepBlock, 0, s>>>(a, *record);
-    }
-    else if (curved)
-        k_step_plain<true, false, false, MINB><<<blocks, kStepBlock, 0, s>>>(a, none);
+    if (curved)
+        k_step_plain<true, false, true, MINB><<<blocks, kStepBlock, 0, s>>>(a, none);
     else
-        k_step_plain<false, false, false, MINB><<<blocks, kStepBlock, 0, s>>>(a, none);
+        k_step_plain<false, false, true, MINB><<<blocks, kStepBlock, 0, s>>>(a, none);
 }
 
 void launch_step_plain(const PlainStepArgs &a, bool curved, cudaStream_t s, const StepRecord *record)
@@ -716,17 +768,33 @@ void launch_step_plain(const PlainStepArgs &a, bool curved, cudaStream_t s, cons
     if (cells <= 0)
         return;
     const unsigned blocks = nblk(cells, kStepBlock);
-    const int64_t sms = a.sms > 0 ? a.sms : 1;
-    const int64_t waves_lo = (blocks + kPlainBlocksLo * sms - 1) / (kPlainBlocksLo * sms);
-    const int64_t waves_hi = (blocks + kPlainBlocksHi * sms - 1) / (kPlainBlocksHi * sms);
-    if (a.ang_new)
+    if (a.ang_new) // adaptive streaming: the fused step
+    {
+        const int64_t sms = a.sms > 0 ? a.sms : 1;
+        const int64_t waves_lo = (blocks + kPlainBlocksLo * sms - 1) / (kPlainBlocksLo * sms);
+        const int64_t waves_hi = (blocks + kPlainBlocksHi * sms - 1) / (kPlainBlocksHi * sms);
         k_rotation_update<<<nblk(cells, 128), 128, 0, s>>>(a.g, a.mom, a.ang_old, const_cast<double *>(a.ang_new));
-    if (waves_hi < waves_lo)
-        launch_step_plain_as<kPlainBlocksHi>(a, curved, s, record, blocks);
-    else
-        launch_step_plain_as<kPlainBlocksLo>(a, curved, s, record, blocks);
-    if (a.ang_new)
+        if (waves_hi < waves_lo)
+            launch_step_adaptive_as<kPlainBlocksHi>(a, curved, s, blocks);
+        else
+            launch_step_adaptive_as<kPlainBlocksLo>(a, curved, s, blocks);
         k_zero_halo_moments<<<nblk(a.g.nxy, 256), 256, 0, s>>>(a.g, a.mom);
+        return;
+    }
+    // fixed streaming: stream, then moments and collide
+    const StepRecord none{};
+    const StepRecord &rec = record ? *record : none;
+    const dim3 sgrid(blocks, (unsigned)a.nd);
+    if (curved)
+        record ? k_stream_plain<true, true><<<sgrid, kStepBlock, 0, s>>>(a, rec)
+               : k_stream_plain<true, false><<<sgrid, kStepBlock, 0, s>>>(a, rec);
+    else
+        record ? k_stream_plain<false, true><<<sgrid, kStepBlock, 0, s>>>(a, rec)
+               : k_stream_plain<false, false><<<sgrid, kStepBlock, 0, s>>>(a, rec);
+    if (record)
+        k_collide_plain<true><<<blocks, kStepBlock, 0, s>>>(a, rec);
+    else
+        k_collide_plain<false><<<blocks, kStepBlock, 0, s>>>(a, rec);
 }
 void launch_sources64(double *I, int64_t nxy, int nd, const int64_t *nodes, const double *vals, int64_t nsrc,
                       cudaStream_t s)
