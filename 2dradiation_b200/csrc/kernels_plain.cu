@@ -34,18 +34,21 @@ __device__ __forceinline__ double stream_value(const PlainStepArgs &a, int d, co
                                                int64_t ij, unsigned &clamp_mask)
 {
     clamp_mask = 0xFu;
-    const int64_t nxy = a.g.nxy, nx = a.g.nx;
+    const int64_t nxy = a.g.nxy;
+    const int nx = (int)a.g.nx; // node indices fit in 32 bits (nx * ny < 2^31)
     if constexpr (CURVED)
     {
         if (r.z < 0.0) // departure point inside the excision
             return 0.0;
         const double it = r.x, jt = r.y;
         // corners kept on the grid whatever the record holds
-        const int64_t i0 = min(max((int64_t)floor(it), (int64_t)0), nx - 2);
-        const int64_t j0 = min(max((int64_t)floor(jt), (int64_t)0), a.g.ny - 2);
-        int g0 = (int)floor(r.z) % a.ng;
+        const int i0 = min(max((int)floor(it), 0), nx - 2); // the conversion saturates: same clamp
+        const int j0 = min(max((int)floor(jt), 0), (int)a.g.ny - 2);
+        // g0 = floor(z) % nGrid, taken without the division when in range
+        const int gz = (int)floor(r.z);
+        int g0 = (unsigned)gz < (unsigned)a.ng ? gz : gz % a.ng;
         g0 = g0 < 0 ? 0 : g0;
-        const int g1 = (g0 + 1) % a.ng;
+        const int g1 = g0 + 1 == a.ng ? 0 : g0 + 1; // (g0 + 1) % nGrid
         const double t = r.z - (double)g0;
         const IgRow R0 = a.ig_rows[g0], R1 = a.ig_rows[g1];
         const int idx0[4] = {R0.idx.x, R0.idx.y, R0.idx.z, R0.idx.w};
@@ -57,8 +60,8 @@ __device__ __forceinline__ double stream_value(const PlainStepArgs &a, int d, co
 #pragma unroll
         for (int q = 0; q < 4; q++) // corners 00, 01, 10, 11
         {
-            const int64_t ci = i0 + (q >> 1), cj = j0 + (q & 1);
-            const int64_t n = ci + cj * nx;
+            const int ci = i0 + (q >> 1), cj = j0 + (q & 1);
+            const int n = ci + cj * nx;
             double v0 = 0.0, v1 = 0.0;
 #pragma unroll
             for (int k = 0; k < 4; k++)
@@ -70,7 +73,7 @@ __device__ __forceinline__ double stream_value(const PlainStepArgs &a, int d, co
             if (!(0.0 < v))
                 clamp_mask &= ~(1u << q);
             v = (0.0 < v) ? v : 0.0;
-            const int64_t di = ci - i, dj = cj - j;
+            const int di = ci - (int)i, dj = cj - (int)j;
             double cube;
             if (di >= -1 && di <= 1 && dj >= -1 && dj <= 1)
                 cube = __ldg(a.acube + ij * 9 + 3 * (dj + 1) + (di + 1));
@@ -93,10 +96,10 @@ __device__ __forceinline__ double stream_value(const PlainStepArgs &a, int d, co
         xt -= __ldg(a.cx + d) * a.g.dt;
         yt -= __ldg(a.cy + d) * a.g.dt;
         const double it = (xt - a.g.startx) / a.g.dx, jt = (yt - a.g.starty) / a.g.dy;
-        const int64_t i0 = min(max((int64_t)floor(it), (int64_t)0), nx - 2);
-        const int64_t j0 = min(max((int64_t)floor(jt), (int64_t)0), a.g.ny - 2);
+        const int i0 = min(max((int)floor(it), 0), nx - 2);
+        const int j0 = min(max((int)floor(jt), 0), (int)a.g.ny - 2);
         const double *plane = a.Iin + (int64_t)d * nxy;
-        const int64_t c00 = i0 + j0 * nx;
+        const int c00 = i0 + j0 * nx;
         const double fx = it - (double)i0, fy = jt - (double)j0;
         const double f0 = __ldg(plane + c00) * (1.0 - fx) + __ldg(plane + c00 + 1) * fx;
         const double f1 = __ldg(plane + c00 + nx) * (1.0 - fx) + __ldg(plane + c00 + nx + 1) * fx;
@@ -455,16 +458,25 @@ __global__ void __launch_bounds__(kStepBlock, MINB) k_step_plain(PlainStepArgs a
 // other in one thread per cell.  Stream: one thread per (cell, direction) of
 // the slab rows writes the streamed value to S (and, recording, the corner
 // clamp mask).
+// Blocks are 32 x 4 tiles of cells (blockIdx.x, blockIdx.y over the slab
+// rows) of one direction (blockIdx.z).
+#ifndef GRLBM_SPLIT_TILE_X
+#define GRLBM_SPLIT_TILE_X 16
+#endif
+constexpr int kSplitTileX = GRLBM_SPLIT_TILE_X, kSplitTileY = kStepBlock / kSplitTileX;
+#ifndef GRLBM_STREAM_MIN_BLOCKS
+#define GRLBM_STREAM_MIN_BLOCKS 1
+#endif
 template <bool CURVED, bool RECORD>
-__global__ void __launch_bounds__(kStepBlock) k_stream_plain(PlainStepArgs a, StepRecord rec)
+__global__ void __launch_bounds__(kStepBlock, GRLBM_STREAM_MIN_BLOCKS) k_stream_plain(PlainStepArgs a, StepRecord rec)
 {
-    const int64_t c = (int64_t)blockIdx.x * kStepBlock + threadIdx.x;
-    const int d = blockIdx.y;
-    if (c >= (a.g.jhi - a.g.jlo) * a.g.nx_)
+    const int d = blockIdx.z;
+    const int i = 1 + (int)blockIdx.x * kSplitTileX + (int)(threadIdx.x % kSplitTileX);
+    const int j = (int)a.g.jlo + (int)blockIdx.y * kSplitTileY + (int)(threadIdx.x / kSplitTileX);
+    if (i > a.g.nx_ || j >= a.g.jhi)
         return;
-    const int64_t cc = (a.g.jlo - 1) * a.g.nx_ + c;
-    const int64_t i = 1 + cc % a.g.nx_, j = 1 + cc / a.g.nx_;
-    const int64_t ij = i + j * a.g.nx;
+    const int64_t cc = (int64_t)(i - 1) + (int64_t)(j - 1) * a.g.nx_;
+    const int64_t ij = (int64_t)i + (int64_t)j * a.g.nx;
     unsigned cm = 0xFu;
     double val = 0.0;
     if (!(CURVED && (a.flags[ij] & 2)))
@@ -483,11 +495,11 @@ __global__ void __launch_bounds__(kStepBlock) k_stream_plain(PlainStepArgs a, St
 template <bool RECORD>
 __global__ void __launch_bounds__(kStepBlock) k_collide_plain(PlainStepArgs a, StepRecord rec)
 {
-    const int64_t c0 = (a.g.jlo - 1) * a.g.nx_;
-    const int64_t c = (int64_t)blockIdx.x * kStepBlock + threadIdx.x;
-    const bool active = c < (a.g.jhi - a.g.jlo) * a.g.nx_;
-    const int64_t cc = c0 + (active ? c : 0);
-    const int64_t i = 1 + cc % a.g.nx_, j = 1 + cc / a.g.nx_;
+    const int ti = 1 + (int)blockIdx.x * kSplitTileX + (int)(threadIdx.x % kSplitTileX);
+    const int tj = (int)a.g.jlo + (int)blockIdx.y * kSplitTileY + (int)(threadIdx.x / kSplitTileX);
+    const bool active = ti <= a.g.nx_ && tj < a.g.jhi;
+    const int64_t i = active ? ti : 1, j = active ? tj : 1;
+    const int64_t cc = (i - 1) + (j - 1) * a.g.nx_;
     const int64_t ij = i + j * a.g.nx;
     const int64_t nxy = a.g.nxy;
     const bool collides = active && !(a.flags[ij] & 1);
@@ -784,7 +796,8 @@ void launch_step_plain(const PlainStepArgs &a, bool curved, cudaStream_t s, cons
     // fixed streaming: stream, then moments and collide
     const StepRecord none{};
     const StepRecord &rec = record ? *record : none;
-    const dim3 sgrid(blocks, (unsigned)a.nd);
+    const unsigned tx = nblk(a.g.nx_, kSplitTileX), ty = nblk(a.g.jhi - a.g.jlo, kSplitTileY);
+    const dim3 sgrid(tx, ty, (unsigned)a.nd), cgrid(tx, ty);
     if (curved)
         record ? k_stream_plain<true, true><<<sgrid, kStepBlock, 0, s>>>(a, rec)
                : k_stream_plain<true, false><<<sgrid, kStepBlock, 0, s>>>(a, rec);
@@ -792,9 +805,9 @@ void launch_step_plain(const PlainStepArgs &a, bool curved, cudaStream_t s, cons
         record ? k_stream_plain<false, true><<<sgrid, kStepBlock, 0, s>>>(a, rec)
                : k_stream_plain<false, false><<<sgrid, kStepBlock, 0, s>>>(a, rec);
     if (record)
-        k_collide_plain<true><<<blocks, kStepBlock, 0, s>>>(a, rec);
+        k_collide_plain<true><<<cgrid, kStepBlock, 0, s>>>(a, rec);
     else
-        k_collide_plain<false><<<blocks, kStepBlock, 0, s>>>(a, rec);
+        k_collide_plain<false><<<cgrid, kStepBlock, 0, s>>>(a, rec);
 }
 void launch_sources64(double *I, int64_t nxy, int nd, const int64_t *nodes, const double *vals, int64_t nsrc,
                       cudaStream_t s)
