@@ -284,18 +284,20 @@ __device__ __forceinline__ double stream_value_adaptive(const PlainStepArgs &a, 
 // directions in stream, moments and collide) and corners are read in their
 // previous frames.
 // direction d of a cell's stencil (rotated by the cell's angle in adaptive streaming)
-#define GRLBM_N1(d) (ADAPTIVE ? __ldg(a.cx + (d)) * rot_c - __ldg(a.cy + (d)) * rot_s : __ldg(a.n1 + (d)))
-#define GRLBM_N2(d) (ADAPTIVE ? __ldg(a.cx + (d)) * rot_s + __ldg(a.cy + (d)) * rot_c : __ldg(a.n2 + (d)))
+#define GRLBM_N1(d) (ADAPTIVE ? __ldg(a.cx + (d)) * rot_c - __ldg(a.cy + (d)) * rot_s : tn1[d])
+#define GRLBM_N2(d) (ADAPTIVE ? __ldg(a.cx + (d)) * rot_s + __ldg(a.cy + (d)) * rot_c : tn2[d])
 
 // The rest of a step for one cell once its streamed values are known: m
 // holds their moments; Sin points at them (direction stride nxy), Sout at the
 // cell's output slots (the same slots in the fused step).  Collide
 // (src/Radiation.cpp:641-736) for a colliding cell, then the stored moments
 // and the lambda-iteration statistics.
+// tw, tn1, tn2: the stencil's weights and directions (global or shared memory).
 template <bool RECORD, bool ADAPTIVE>
 __device__ __forceinline__ void finish_cell(const PlainStepArgs &a, const StepRecord &rec, bool active, bool collides,
                                             int64_t ij, int64_t cc, Moments m, const double *Sin, double *Sout,
-                                            double rot_s, double rot_c)
+                                            double rot_s, double rot_c, const double *tw, const double *tn1,
+                                            const double *tn2)
 {
     const int t = threadIdx.x;
     const int64_t nxy = a.g.nxy;
@@ -338,7 +340,7 @@ __device__ __forceinline__ void finish_cell(const PlainStepArgs &a, const StepRe
                     const double n1 = GRLBM_N1(d), n2 = GRLBM_N2(d);
                     const double num = Sin[(int64_t)d * nxy] + adt * (eta + (k0fE + k3 * (n1 * fFx + n2 * fFy)));
                     const double v = fast_div ? div_rn(num, den, rden) : num / den;
-                    m.add(__ldg(a.w + d), v, n1, n2);
+                    m.add(tw[d], v, n1, n2);
                 }
             }
             else
@@ -347,7 +349,7 @@ __device__ __forceinline__ void finish_cell(const PlainStepArgs &a, const StepRe
                     const double n1 = GRLBM_N1(d), n2 = GRLBM_N2(d);
                     const double v = collide_value(Sin[(int64_t)d * nxy], n1, n2, u1, u2, lor, adt, eta, k0, k3,
                                                    kak0, fE, fFx, fFy);
-                    m.add(__ldg(a.w + d), v, n1, n2);
+                    m.add(tw[d], v, n1, n2);
                 }
             const double e1 = (pE - m.E) / m.E, e2 = (pFx - m.Fx) / m.Fx, e3 = (pFy - m.Fy) / m.Fy;
             const double e4 = (pPxx - m.Pxx) / m.Pxx, e5 = (pPxy - m.Pxy) / m.Pxy, e6 = (pPyy - m.Pyy) / m.Pyy;
@@ -422,6 +424,7 @@ __global__ void __launch_bounds__(kStepBlock, MINB) k_step_plain(PlainStepArgs a
         rot_s = approx_sin(th);
         rot_c = approx_cos(th);
     }
+    const double *tn1 = a.n1, *tn2 = a.n2;
     Moments m;
     m.zero();
     // departure records, prefetched one direction ahead (the last stands in
@@ -449,7 +452,7 @@ __global__ void __launch_bounds__(kStepBlock, MINB) k_step_plain(PlainStepArgs a
         r0 = r1;
     }
 
-    finish_cell<RECORD, ADAPTIVE>(a, rec, active, collides, ij, cc, m, Is, Is, rot_s, rot_c);
+    finish_cell<RECORD, ADAPTIVE>(a, rec, active, collides, ij, cc, m, Is, Is, rot_s, rot_c, a.w, a.n1, a.n2);
 }
 
 // The fixed streaming types run the step as two kernels, so that the
@@ -460,6 +463,13 @@ __global__ void __launch_bounds__(kStepBlock, MINB) k_step_plain(PlainStepArgs a
 // clamp mask).
 // Blocks are 32 x 4 tiles of cells (blockIdx.x, blockIdx.y over the slab
 // rows) of one direction (blockIdx.z).
+#ifndef GRLBM_COLLIDE_SMEM_TABLES
+#define GRLBM_COLLIDE_SMEM_TABLES 1
+#endif
+#ifndef GRLBM_COLLIDE_UNROLL
+#define GRLBM_COLLIDE_UNROLL 8
+#endif
+constexpr int kCollideUnroll = GRLBM_COLLIDE_UNROLL;
 #ifndef GRLBM_SPLIT_TILE_X
 #define GRLBM_SPLIT_TILE_X 16
 #endif
@@ -504,12 +514,25 @@ __global__ void __launch_bounds__(kStepBlock) k_collide_plain(PlainStepArgs a, S
     const int64_t nxy = a.g.nxy;
     const bool collides = active && !(a.flags[ij] & 1);
     const double *Sin = a.S + ij;
+#if GRLBM_COLLIDE_SMEM_TABLES
+    // the stencil's weights and directions, read by every cell of the block
+    __shared__ double sw[kMaxDirs], sn1[kMaxDirs], sn2[kMaxDirs];
+    for (int d = threadIdx.x; d < a.nd; d += kStepBlock)
+        sw[d] = a.w[d], sn1[d] = a.n1[d], sn2[d] = a.n2[d];
+    __syncthreads();
+    const double *tw = sw, *tn1 = sn1, *tn2 = sn2;
+#else
+    const double *tw = a.w, *tn1 = a.n1, *tn2 = a.n2;
+#endif
     Moments m;
     m.zero();
     if (active)
+    {
+#pragma unroll kCollideUnroll
         for (int d = 0; d < a.nd; d++)
-            m.add(__ldg(a.w + d), Sin[(int64_t)d * nxy], __ldg(a.n1 + d), __ldg(a.n2 + d));
-    finish_cell<RECORD, false>(a, rec, active, collides, ij, cc, m, Sin, a.Iout + ij, 0.0, 1.0);
+            m.add(tw[d], Sin[(int64_t)d * nxy], tn1[d], tn2[d]);
+    }
+    finish_cell<RECORD, false>(a, rec, active, collides, ij, cc, m, Sin, a.Iout + ij, 0.0, 1.0, tw, tn1, tn2);
 }
 #undef GRLBM_N1
 #undef GRLBM_N2
