@@ -168,11 +168,13 @@ __device__ __forceinline__ double div_rn(double num, double den, double r)
 }
 
 // Fourier::GetValue (src/FourierHarmonics.cpp:56-61) with Fourier::Basis
-// (:5-14) at a run-time angle.
-__device__ __forceinline__ double fourier_value(const double *coef, int nf, double phi)
+// (:5-14) at a run-time angle, for the five series of a node's geodesic
+// tables (S, X, Y, Cx, Cy, fs apart) at once: each basis value is computed
+// once and used by all five, and every sum keeps its order over k.
+__device__ __forceinline__ void fourier_values5(const double *coef, int64_t fs, int nf, double phi, double out[5])
 {
     const double sqrt2 = 1.4142135623730951; // sqrt(2), correctly rounded
-    double result = 0;
+    double r0 = 0, r1 = 0, r2 = 0, r3 = 0, r4 = 0;
     for (int k = 0; k < nf; k++)
     {
         double b;
@@ -182,9 +184,13 @@ __device__ __forceinline__ double fourier_value(const double *coef, int nf, doub
             b = sqrt2 * cos(phi * (k + 1.0) / 2.0);
         else
             b = sqrt2 * sin(phi * k / 2.0);
-        result += coef[k] * b;
+        r0 += coef[k] * b;
+        r1 += coef[fs + k] * b;
+        r2 += coef[2 * fs + k] * b;
+        r3 += coef[3 * fs + k] * b;
+        r4 += coef[4 * fs + k] * b;
     }
-    return result;
+    out[0] = r0, out[1] = r1, out[2] = r2, out[3] = r3, out[4] = r4;
 }
 
 // IntensityAt (src/Radiation.cpp:322-343) of node n for the (unrotated)
@@ -232,11 +238,11 @@ __device__ __forceinline__ double stream_value_adaptive(const PlainStepArgs &a, 
         const double phi = approx_phi(dir1, dir2);
         const int64_t fs = a.g.nxy * a.nf;
         const double *cf = a.coef + ij * a.nf;
-        const double sh = fourier_value(cf, a.nf, phi);
-        const double xt = fourier_value(cf + fs, a.nf, phi);
-        const double yt = fourier_value(cf + 2 * fs, a.nf, phi);
-        v1 = fourier_value(cf + 3 * fs, a.nf, phi);
-        v2 = fourier_value(cf + 4 * fs, a.nf, phi);
+        double fv[5];
+        fourier_values5(cf, fs, a.nf, phi, fv);
+        const double sh = fv[0], xt = fv[1], yt = fv[2];
+        v1 = fv[3];
+        v2 = fv[4];
         if (dev_inside_bh(a.g, xt, yt))
             return 0.0;
         it = (xt - a.g.startx) / a.g.dx;
