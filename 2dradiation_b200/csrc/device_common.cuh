@@ -191,8 +191,7 @@ struct PlainStepArgs
     const double *ang_old, *ang_new;
     const double *coef; // [5][nxy][nf]
     int nf;
-    int sms; // SMs of the device (chooses the launch's register budget)
-    double *S; // fixed streaming: the streamed values of the step, [d * nxy + ij]
+    double *S; // the streamed values of the step, [d * nxy + ij]
 };
 
 struct PrecStepArgs

@@ -45,7 +45,6 @@ struct grlbm_ctx
 {
     std::string err;
     int device = 0;
-    int sms = 1; // the device's SM count
     cudaStream_t stream = nullptr;
     // host tables
     GridGeom geo;
@@ -69,7 +68,7 @@ struct grlbm_ctx
     int64_t nsrc_ang = 0;
     std::vector<double> flux_angle;
     DevBuf ig_rows, ia3;
-    DevBuf streamed; // plain form, fixed streaming: the streamed values of a step
+    DevBuf streamed; // plain form: the streamed values of a step
     DirTable dirs{}; // precision-form direction tables (kernel parameter)
     DevBuf cu1, cu2, clor, cadt, ceta, ck0, ck3, cka, mom, rkf, lfp;
     DevBuf coef, ss_cx, ss_cy, ss_w, proj_basis, eval_basis, stage;
@@ -258,7 +257,6 @@ PlainStepArgs plain_args(grlbm_ctx *ctx, int from)
     a.mom = ctx->mom.as<double>();
     a.iter_sum = cnt;
     a.iter_max = reinterpret_cast<unsigned int *>(cnt + 1);
-    a.sms = ctx->sms;
     a.S = ctx->streamed.as<double>();
     return a;
 }
@@ -480,7 +478,6 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
             return fail(nullptr, GRLBM_ERR_CUDA, "cudaSetDevice failed");
     }
     cudaGetDevice(&ctx->device);
-    cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, ctx->device);
     if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess)
         return fail(nullptr, GRLBM_ERR_CUDA, "cudaStreamCreate failed");
 
@@ -739,7 +736,7 @@ std::vector<IgRow> rows(ctx->ng);
     }
     TRY(alloc(ctx, ctx->I[0], ib));
     TRY(alloc(ctx, ctx->I[1], ib));
-    if (!ctx->fp32 && !is_adaptive(ctx))
+    if (!ctx->fp32)
         TRY(alloc(ctx, ctx->streamed, (size_t)nxy * nd * sizeof(double)));
     TRY(alloc(ctx, ctx->mom, (size_t)6 * nxy * tsize(ctx)));
     TRY(alloc(ctx, ctx->rec, (size_t)ctx->ncell * nd * (ctx->fp32 ? sizeof(float4) : sizeof(double4))));

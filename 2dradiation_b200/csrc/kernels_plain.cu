@@ -11,20 +11,10 @@
 #include "approx_math.hpp"
 #include "device_common.cuh"
 
-// Resident blocks per SM the step kernel's register budget is sized for:
-// the kernel is built for both, and each launch takes the one whose grid
-// needs fewer waves (the larger budget when they tie: it does not spill).
-constexpr int kPlainBlocksLo = 3, kPlainBlocksHi = 4;
-// Unroll of the step's per-direction stream loop.
-#ifndef GRLBM_PLAIN_UNROLL
-#define GRLBM_PLAIN_UNROLL 1
-#endif
-
 namespace grlbm
 {
 namespace
 {
-constexpr int kPlainUnroll = GRLBM_PLAIN_UNROLL;
 // one stream value: StreamFlatFixed (src/Radiation.cpp:394-410) or
 // StreamCurvedFixed with IntensityAt (:478-508, 322-343)
 // `clamp_mask` receives bit q set where corner q's angular interpolation was
@@ -283,15 +273,17 @@ __device__ __forceinline__ double stream_value_adaptive(const PlainStepArgs &a, 
     return CURVED ? s3 * bil : bil;
 }
 
-// RECORD: also writes what the adjoint needs about this step -- per (d, c)
-// the corner clamp mask, per cell the lambda-iteration count and the first
-// iterate's E -- without changing any result.  ADAPTIVE: the adaptive
-// streaming types -- each cell's stencil is rotated by its new angle (its
-// directions in stream, moments and collide) and corners are read in their
-// previous frames.
-// direction d of a cell's stencil (rotated by the cell's angle in adaptive streaming)
-#define GRLBM_N1(d) (ADAPTIVE ? __ldg(a.cx + (d)) * rot_c - __ldg(a.cy + (d)) * rot_s : tn1[d])
-#define GRLBM_N2(d) (ADAPTIVE ? __ldg(a.cx + (d)) * rot_s + __ldg(a.cy + (d)) * rot_c : tn2[d])
+// Template switches of the step's kernels.  RECORD: also write what the
+// adjoint needs about this step -- per (d, c) the corner clamp mask, per cell
+// the lambda-iteration count and the first iterate's E -- without changing
+// any result.  ADAPTIVE: the adaptive streaming types -- each cell's stencil
+// is rotated by its new angle (its directions in stream, moments and
+// collide) and corners are read in their previous frames.
+//
+// Direction d of a cell's stencil (tn1, tn2: the stencil's directions;
+// rotated by the cell's angle in adaptive streaming).
+#define GRLBM_N1(d) (ADAPTIVE ? tn1[d] * rot_c - tn2[d] * rot_s : tn1[d])
+#define GRLBM_N2(d) (ADAPTIVE ? tn1[d] * rot_s + tn2[d] * rot_c : tn2[d])
 
 // The rest of a step for one cell once its streamed values are known: m
 // holds their moments; Sin points at them (direction stride nxy), Sout at the
@@ -299,6 +291,7 @@ __device__ __forceinline__ double stream_value_adaptive(const PlainStepArgs &a, 
 // (src/Radiation.cpp:641-736) for a colliding cell, then the stored moments
 // and the lambda-iteration statistics.
 // tw, tn1, tn2: the stencil's weights and directions (global or shared memory).
+// rot_s, rot_c: the cell's rotation (adaptive streaming).
 template <bool RECORD, bool ADAPTIVE>
 __device__ __forceinline__ void finish_cell(const PlainStepArgs &a, const StepRecord &rec, bool active, bool collides,
                                             int64_t ij, int64_t cc, Moments m, const double *Sin, double *Sout,
@@ -403,63 +396,6 @@ __device__ __forceinline__ void finish_cell(const PlainStepArgs &a, const StepRe
     }
 }
 
-template <bool CURVED, bool RECORD, bool ADAPTIVE, int MINB>
-__global__ void __launch_bounds__(kStepBlock, MINB) k_step_plain(PlainStepArgs a, StepRecord rec)
-{
-    const int t = threadIdx.x;
-    // cells of the slab rows [jlo, jhi), numbered from its first cell
-    const int64_t c0 = (a.g.jlo - 1) * a.g.nx_;
-    const int64_t c = (int64_t)blockIdx.x * kStepBlock + t;
-    const bool active = c < (a.g.jhi - a.g.jlo) * a.g.nx_;
-    const int64_t cc = c0 + (active ? c : 0);
-    const int64_t i = 1 + cc % a.g.nx_, j = 1 + cc / a.g.nx_;
-    const int64_t ij = i + j * a.g.nx;
-    const int64_t nxy = a.g.nxy;
-    const uint8_t fl = active ? a.flags[ij] : (uint8_t)3;
-    const bool zero_stream = CURVED && (fl & 2);
-    const bool collides = active && !(fl & 1);
-    // The streamed intensities of a colliding cell wait in its own output
-    // slots until the lambda iteration has converged (nothing else reads or
-    // writes them in this step); non-colliding cells keep their slots.
-    double *Is = a.Iout + ij;
-    // the cell's rotation (RotationMatrix(rotationAngle[ij]), src/DataTypes.hh:630-635)
-    double rot_s = 0.0, rot_c = 1.0;
-    if (ADAPTIVE)
-    {
-        const double th = a.ang_new[ij];
-        rot_s = approx_sin(th);
-        rot_c = approx_cos(th);
-    }
-    const double *tn1 = a.n1, *tn2 = a.n2;
-    Moments m;
-    m.zero();
-    // departure records, prefetched one direction ahead (the last stands in
-    // past the end)
-    const double4 *rp = a.rec + cc;
-    double4 r0 = make_double4(0, 0, 0, 0);
-    if (CURVED && !ADAPTIVE)
-        r0 = rp[0];
-#pragma unroll kPlainUnroll
-    for (int d = 0; d < a.nd; d++)
-    {
-        double4 r1 = r0;
-        if (CURVED && !ADAPTIVE)
-            r1 = rp[(int64_t)min(d + 1, a.nd - 1) * a.g.ncell];
-        unsigned cm = 0xFu;
-        double val = 0.0;
-        if (active && !zero_stream)
-            val = ADAPTIVE ? stream_value_adaptive<CURVED>(a, d, i, j, ij, rot_s, rot_c)
-                           : stream_value<CURVED>(a, d, r0, i, j, ij, cm);
-        if (RECORD && active)
-            rec.clamp[(int64_t)d * a.g.ncell + cc] = (uint8_t)cm;
-        if (collides)
-            Is[(int64_t)d * nxy] = val;
-        m.add(__ldg(a.w + d), val, GRLBM_N1(d), GRLBM_N2(d));
-        r0 = r1;
-    }
-
-    finish_cell<RECORD, ADAPTIVE>(a, rec, active, collides, ij, cc, m, Is, Is, rot_s, rot_c, a.w, a.n1, a.n2);
-}
 
 // The fixed streaming types run the step as two kernels, so that the
 // stream's dependent gathers (record, interpolation rows, 32 corner taps)
@@ -483,7 +419,7 @@ constexpr int kSplitTileX = GRLBM_SPLIT_TILE_X, kSplitTileY = kStepBlock / kSpli
 #ifndef GRLBM_STREAM_MIN_BLOCKS
 #define GRLBM_STREAM_MIN_BLOCKS 1
 #endif
-template <bool CURVED, bool RECORD>
+template <bool CURVED, bool RECORD, bool ADAPTIVE>
 __global__ void __launch_bounds__(kStepBlock, GRLBM_STREAM_MIN_BLOCKS) k_stream_plain(PlainStepArgs a, StepRecord rec)
 {
     const int d = blockIdx.z;
@@ -497,8 +433,17 @@ __global__ void __launch_bounds__(kStepBlock, GRLBM_STREAM_MIN_BLOCKS) k_stream_
     double val = 0.0;
     if (!(CURVED && (a.flags[ij] & 2)))
     {
-        const double4 r = CURVED ? a.rec[(int64_t)d * a.g.ncell + cc] : make_double4(0, 0, 0, 0);
-        val = stream_value<CURVED>(a, d, r, i, j, ij, cm);
+        if constexpr (ADAPTIVE)
+        {
+            // the cell's rotation (RotationMatrix(rotationAngle[ij]), src/DataTypes.hh:630-635)
+            const double th = a.ang_new[ij];
+            val = stream_value_adaptive<CURVED>(a, d, i, j, ij, approx_sin(th), approx_cos(th));
+        }
+        else
+        {
+            const double4 r = CURVED ? a.rec[(int64_t)d * a.g.ncell + cc] : make_double4(0, 0, 0, 0);
+            val = stream_value<CURVED>(a, d, r, i, j, ij, cm);
+        }
     }
     if (RECORD)
         rec.clamp[(int64_t)d * a.g.ncell + cc] = (uint8_t)cm;
@@ -508,7 +453,7 @@ __global__ void __launch_bounds__(kStepBlock, GRLBM_STREAM_MIN_BLOCKS) k_stream_
 // Moments and collide: one thread per cell sums the moments of its streamed
 // values in direction order (ComputeMomentsIF's order, as the fused step
 // does) and finishes the cell; the collided intensities go to Iout.
-template <bool RECORD>
+template <bool RECORD, bool ADAPTIVE>
 __global__ void __launch_bounds__(kStepBlock) k_collide_plain(PlainStepArgs a, StepRecord rec)
 {
     const int ti = 1 + (int)blockIdx.x * kSplitTileX + (int)(threadIdx.x % kSplitTileX);
@@ -523,22 +468,32 @@ __global__ void __launch_bounds__(kStepBlock) k_collide_plain(PlainStepArgs a, S
 #if GRLBM_COLLIDE_SMEM_TABLES
     // the stencil's weights and directions, read by every cell of the block
     __shared__ double sw[kMaxDirs], sn1[kMaxDirs], sn2[kMaxDirs];
+    const double *dn1 = ADAPTIVE ? a.cx : a.n1, *dn2 = ADAPTIVE ? a.cy : a.n2;
     for (int d = threadIdx.x; d < a.nd; d += kStepBlock)
-        sw[d] = a.w[d], sn1[d] = a.n1[d], sn2[d] = a.n2[d];
+        sw[d] = a.w[d], sn1[d] = dn1[d], sn2[d] = dn2[d];
     __syncthreads();
     const double *tw = sw, *tn1 = sn1, *tn2 = sn2;
 #else
-    const double *tw = a.w, *tn1 = a.n1, *tn2 = a.n2;
+    const double *tw = a.w, *tn1 = ADAPTIVE ? a.cx : a.n1, *tn2 = ADAPTIVE ? a.cy : a.n2;
 #endif
+    // the cell's rotation (adaptive streaming)
+    double rot_s = 0.0, rot_c = 1.0;
+    if (ADAPTIVE)
+    {
+        const double th = a.ang_new[ij];
+        rot_s = approx_sin(th);
+        rot_c = approx_cos(th);
+    }
     Moments m;
     m.zero();
     if (active)
     {
 #pragma unroll kCollideUnroll
         for (int d = 0; d < a.nd; d++)
-            m.add(tw[d], Sin[(int64_t)d * nxy], tn1[d], tn2[d]);
+            m.add(tw[d], Sin[(int64_t)d * nxy], GRLBM_N1(d), GRLBM_N2(d));
     }
-    finish_cell<RECORD, false>(a, rec, active, collides, ij, cc, m, Sin, a.Iout + ij, 0.0, 1.0, tw, tn1, tn2);
+    finish_cell<RECORD, ADAPTIVE>(a, rec, active, collides, ij, cc, m, Sin, a.Iout + ij, rot_s, rot_c, tw, tn1,
+                                  tn2);
 }
 #undef GRLBM_N1
 #undef GRLBM_N2
@@ -793,50 +748,37 @@ cudaError_t prepare_step_plain(int smem_bytes)
     (void)smem_bytes; // the plain step uses no dynamic shared memory
     return cudaSuccess;
 }
-template <int MINB>
-void launch_step_adaptive_as(const PlainStepArgs &a, bool curved, cudaStream_t s, unsigned blocks)
-{
-    const StepRecord none{};
-    if (curved)
-        k_step_plain<true, false, true, MINB><<<blocks, kStepBlock, 0, s>>>(a, none);
-    else
-        k_step_plain<false, false, true, MINB><<<blocks, kStepBlock, 0, s>>>(a, none);
-}
-
 void launch_step_plain(const PlainStepArgs &a, bool curved, cudaStream_t s, const StepRecord *record)
 {
     const int64_t cells = (a.g.jhi - a.g.jlo) * a.g.nx_;
     if (cells <= 0)
         return;
-    const unsigned blocks = nblk(cells, kStepBlock);
-    if (a.ang_new) // adaptive streaming: the fused step
-    {
-        const int64_t sms = a.sms > 0 ? a.sms : 1;
-        const int64_t waves_lo = (blocks + kPlainBlocksLo * sms - 1) / (kPlainBlocksLo * sms);
-        const int64_t waves_hi = (blocks + kPlainBlocksHi * sms - 1) / (kPlainBlocksHi * sms);
-        k_rotation_update<<<nblk(cells, 128), 128, 0, s>>>(a.g, a.mom, a.ang_old, const_cast<double *>(a.ang_new));
-        if (waves_hi < waves_lo)
-            launch_step_adaptive_as<kPlainBlocksHi>(a, curved, s, blocks);
-        else
-            launch_step_adaptive_as<kPlainBlocksLo>(a, curved, s, blocks);
-        k_zero_halo_moments<<<nblk(a.g.nxy, 256), 256, 0, s>>>(a.g, a.mom);
-        return;
-    }
-    // fixed streaming: stream, then moments and collide
+    const bool adaptive = a.ang_new != nullptr;
     const StepRecord none{};
-    const StepRecord &rec = record ? *record : none;
+    const StepRecord &rec = record && !adaptive ? *record : none;
     const unsigned tx = nblk(a.g.nx_, kSplitTileX), ty = nblk(a.g.jhi - a.g.jlo, kSplitTileY);
     const dim3 sgrid(tx, ty, (unsigned)a.nd), cgrid(tx, ty);
-    if (curved)
-        record ? k_stream_plain<true, true><<<sgrid, kStepBlock, 0, s>>>(a, rec)
-               : k_stream_plain<true, false><<<sgrid, kStepBlock, 0, s>>>(a, rec);
+    if (adaptive) // UpdateRotationMatrizes from the previous moments, before the stream
+        k_rotation_update<<<nblk(cells, 128), 128, 0, s>>>(a.g, a.mom, a.ang_old, const_cast<double *>(a.ang_new));
+    // stream
+    if (adaptive)
+        curved ? k_stream_plain<true, false, true><<<sgrid, kStepBlock, 0, s>>>(a, rec)
+               : k_stream_plain<false, false, true><<<sgrid, kStepBlock, 0, s>>>(a, rec);
+    else if (curved)
+        record ? k_stream_plain<true, true, false><<<sgrid, kStepBlock, 0, s>>>(a, rec)
+               : k_stream_plain<true, false, false><<<sgrid, kStepBlock, 0, s>>>(a, rec);
     else
-        record ? k_stream_plain<false, true><<<sgrid, kStepBlock, 0, s>>>(a, rec)
-               : k_stream_plain<false, false><<<sgrid, kStepBlock, 0, s>>>(a, rec);
-    if (record)
-        k_collide_plain<true><<<cgrid, kStepBlock, 0, s>>>(a, rec);
+        record ? k_stream_plain<false, true, false><<<sgrid, kStepBlock, 0, s>>>(a, rec)
+               : k_stream_plain<false, false, false><<<sgrid, kStepBlock, 0, s>>>(a, rec);
+    // moments and collide
+    if (adaptive)
+        k_collide_plain<false, true><<<cgrid, kStepBlock, 0, s>>>(a, rec);
+    else if (record)
+        k_collide_plain<true, false><<<cgrid, kStepBlock, 0, s>>>(a, rec);
     else
-        k_collide_plain<false><<<cgrid, kStepBlock, 0, s>>>(a, rec);
+        k_collide_plain<false, false><<<cgrid, kStepBlock, 0, s>>>(a, rec);
+    if (adaptive) // the halo moments, recomputed by the reference from unwritten (zero) intensities
+        k_zero_halo_moments<<<nblk(a.g.nxy, 256), 256, 0, s>>>(a.g, a.mom);
 }
 void launch_sources64(double *I, int64_t nxy, int nd, const int64_t *nodes, const double *vals, int64_t nsrc,
                       cudaStream_t s)
