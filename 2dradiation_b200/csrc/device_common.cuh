@@ -189,7 +189,7 @@ struct PlainStepArgs
     // adaptive streaming only (null otherwise): rotation angles before and
     // after this step's update (nxy), and the Fourier coefficients
     const double *ang_old, *ang_new;
-    const double *coef; // [5][nxy][nf]
+    const double *coef; // [5][nf][nxy]: the Fourier coefficients, node index fastest
     int nf;
     double *S; // the streamed values of the step, [d * nxy + ij]
 };
@@ -318,6 +318,8 @@ void launch_sources64(double *I, int64_t nxy, int nd, const int64_t *nodes, cons
                       cudaStream_t s);
 void launch_sources32(float *I, const StateLayout &L, int nd, const int64_t *nodes, const float *vals, int64_t nsrc,
                       cudaStream_t s);
+// [5][nxy][nf] -> [5][nf][nxy]
+void launch_coef_k_major(const double *coef, double *coef_k, int64_t nxy, int nf, cudaStream_t s);
 void launch_moments_lf64(int64_t nxy, const double *mom, const double *lfp, const uint8_t *bh, double *out,
                          cudaStream_t s);
 void launch_moments_lf32(int64_t nxy, const float *mom, const double *lfp, const uint8_t *bh, double *out,

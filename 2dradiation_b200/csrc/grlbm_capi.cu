@@ -69,6 +69,7 @@ struct grlbm_ctx
     std::vector<double> flux_angle;
     DevBuf ig_rows, ia3;
     DevBuf streamed; // plain form: the streamed values of a step
+    DevBuf coef_k;   // adaptive streaming: the coefficients as [5][nf][nxy]
     DirTable dirs{}; // precision-form direction tables (kernel parameter)
     DevBuf cu1, cu2, clor, cadt, ceta, ck0, ck3, cka, mom, rkf, lfp;
     DevBuf coef, ss_cx, ss_cy, ss_w, proj_basis, eval_basis, stage;
@@ -297,7 +298,7 @@ int enqueue_step(grlbm_ctx *ctx, int from)
                                  ctx->src_ang_vals.as<double>(), ctx->nsrc_ang, ctx->stream);
             a.ang_old = ctx->ang[from].as<double>();
             a.ang_new = ctx->ang[from ^ 1].as<double>();
-            a.coef = ctx->coef.as<double>();
+            a.coef = ctx->coef_k.as<double>();
             a.nf = ctx->ss.n;
         }
         launch_step_plain(a, curved, ctx->stream);
@@ -354,6 +355,15 @@ int build_records(grlbm_ctx *ctx)
     da.row_extent = reinterpret_cast<int *>(ctx->counters.as<unsigned long long>() + 5);
     CU(cudaMemsetAsync(ctx->counters.as<unsigned long long>() + 4, 0, 2 * sizeof(unsigned long long), ctx->stream));
     launch_departure(da, ctx->stream);
+    if (is_adaptive(ctx))
+    {
+        // adaptive streaming evaluates the series at run time: a copy with
+        // the coefficients of neighbouring nodes side by side
+        int rc = alloc(ctx, ctx->coef_k, ctx->coef.bytes);
+        if (rc)
+            return rc;
+        launch_coef_k_major(ctx->coef.as<double>(), ctx->coef_k.as<double>(), ctx->gd.nxy, ctx->ss.n, ctx->stream);
+    }
     CU(cudaGetLastError());
     return GRLBM_OK;
 }

@@ -159,9 +159,11 @@ __device__ __forceinline__ double div_rn(double num, double den, double r)
 
 // Fourier::GetValue (src/FourierHarmonics.cpp:56-61) with Fourier::Basis
 // (:5-14) at a run-time angle, for the five series of a node's geodesic
-// tables (S, X, Y, Cx, Cy, fs apart) at once: each basis value is computed
-// once and used by all five, and every sum keeps its order over k.
-__device__ __forceinline__ void fourier_values5(const double *coef, int64_t fs, int nf, double phi, double out[5])
+// tables (S, X, Y, Cx, Cy) at once: coefficient k of series q at
+// coef[q * fs + k * sk].  Each basis value is computed once and used by all
+// five, and every sum keeps its order over k.
+__device__ __forceinline__ void fourier_values5(const double *coef, int64_t fs, int64_t sk, int nf, double phi,
+                                                double out[5])
 {
     const double sqrt2 = 1.4142135623730951; // sqrt(2), correctly rounded
     double r0 = 0, r1 = 0, r2 = 0, r3 = 0, r4 = 0;
@@ -174,11 +176,12 @@ __device__ __forceinline__ void fourier_values5(const double *coef, int64_t fs, 
             b = sqrt2 * cos(phi * (k + 1.0) / 2.0);
         else
             b = sqrt2 * sin(phi * k / 2.0);
-        r0 += coef[k] * b;
-        r1 += coef[fs + k] * b;
-        r2 += coef[2 * fs + k] * b;
-        r3 += coef[3 * fs + k] * b;
-        r4 += coef[4 * fs + k] * b;
+        const double *c = coef + k * sk;
+        r0 += c[0] * b;
+        r1 += c[fs] * b;
+        r2 += c[2 * fs] * b;
+        r3 += c[3 * fs] * b;
+        r4 += c[4 * fs] * b;
     }
     out[0] = r0, out[1] = r1, out[2] = r2, out[3] = r3, out[4] = r4;
 }
@@ -226,10 +229,10 @@ __device__ __forceinline__ double stream_value_adaptive(const PlainStepArgs &a, 
     if constexpr (CURVED)
     {
         const double phi = approx_phi(dir1, dir2);
+        // coefficients k of neighbouring nodes side by side: coalesced loads
         const int64_t fs = a.g.nxy * a.nf;
-        const double *cf = a.coef + ij * a.nf;
         double fv[5];
-        fourier_values5(cf, fs, a.nf, phi, fv);
+        fourier_values5(a.coef + ij, fs, a.g.nxy, a.nf, phi, fv);
         const double sh = fv[0], xt = fv[1], yt = fv[2];
         v1 = fv[3];
         v2 = fv[4];
@@ -412,6 +415,11 @@ __device__ __forceinline__ void finish_cell(const PlainStepArgs &a, const StepRe
 #define GRLBM_COLLIDE_UNROLL 8
 #endif
 constexpr int kCollideUnroll = GRLBM_COLLIDE_UNROLL;
+// Grid order of the stream kernel: directions fastest for adaptive streaming
+// (the blocks of one tile, which read the same Fourier coefficients, run
+// together), tiles fastest for fixed streaming (measured: 2% faster and 3%
+// slower respectively the other way round).
+constexpr bool kDirFastestAdaptive = true, kDirFastestFixed = false;
 #ifndef GRLBM_SPLIT_TILE_X
 #define GRLBM_SPLIT_TILE_X 16
 #endif
@@ -422,9 +430,11 @@ constexpr int kSplitTileX = GRLBM_SPLIT_TILE_X, kSplitTileY = kStepBlock / kSpli
 template <bool CURVED, bool RECORD, bool ADAPTIVE>
 __global__ void __launch_bounds__(kStepBlock, GRLBM_STREAM_MIN_BLOCKS) k_stream_plain(PlainStepArgs a, StepRecord rec)
 {
-    const int d = blockIdx.z;
-    const int i = 1 + (int)blockIdx.x * kSplitTileX + (int)(threadIdx.x % kSplitTileX);
-    const int j = (int)a.g.jlo + (int)blockIdx.y * kSplitTileY + (int)(threadIdx.x / kSplitTileX);
+    constexpr bool DFAST = ADAPTIVE ? kDirFastestAdaptive : kDirFastestFixed;
+    const int d = DFAST ? blockIdx.x : blockIdx.z;
+    const int bx = DFAST ? blockIdx.y : blockIdx.x, by = DFAST ? blockIdx.z : blockIdx.y;
+    const int i = 1 + bx * kSplitTileX + (int)(threadIdx.x % kSplitTileX);
+    const int j = (int)a.g.jlo + by * kSplitTileY + (int)(threadIdx.x / kSplitTileX);
     if (i > a.g.nx_ || j >= a.g.jhi)
         return;
     const int64_t cc = (int64_t)(i - 1) + (int64_t)(j - 1) * a.g.nx_;
@@ -687,6 +697,18 @@ __global__ void __launch_bounds__(256) k_energy_final(const double *partial, int
         *out = s[0];
 }
 
+// Fourier coefficients [5][nxy][nf] -> [5][nf][nxy]
+__global__ void k_coef_k_major(const double *coef, double *coef_k, int64_t nxy, int nf)
+{
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t per = nxy * nf;
+    if (t >= 5 * per)
+        return;
+    const int64_t q = t / per, r = t - q * per; // r = k * nxy + ij
+    const int64_t k = r / nxy, ij = r - k * nxy;
+    coef_k[t] = coef[q * per + ij * nf + k];
+}
+
 // cell-major double [ij][d] <-> direction-major T [d][ij]
 template <class T>
 __global__ void k_to_dirmajor(const double *in, T *out, int64_t nxy, StateLayout L, int nd, const float *scale)
@@ -757,19 +779,20 @@ void launch_step_plain(const PlainStepArgs &a, bool curved, cudaStream_t s, cons
     const StepRecord none{};
     const StepRecord &rec = record && !adaptive ? *record : none;
     const unsigned tx = nblk(a.g.nx_, kSplitTileX), ty = nblk(a.g.jhi - a.g.jlo, kSplitTileY);
-    const dim3 sgrid(tx, ty, (unsigned)a.nd), cgrid(tx, ty);
+    const dim3 sgrid(tx, ty, (unsigned)a.nd), sgrid_df((unsigned)a.nd, tx, ty), cgrid(tx, ty);
     if (adaptive) // UpdateRotationMatrizes from the previous moments, before the stream
         k_rotation_update<<<nblk(cells, 128), 128, 0, s>>>(a.g, a.mom, a.ang_old, const_cast<double *>(a.ang_new));
     // stream
+    const dim3 ga = kDirFastestAdaptive ? sgrid_df : sgrid, gf = kDirFastestFixed ? sgrid_df : sgrid;
     if (adaptive)
-        curved ? k_stream_plain<true, false, true><<<sgrid, kStepBlock, 0, s>>>(a, rec)
-               : k_stream_plain<false, false, true><<<sgrid, kStepBlock, 0, s>>>(a, rec);
+        curved ? k_stream_plain<true, false, true><<<ga, kStepBlock, 0, s>>>(a, rec)
+               : k_stream_plain<false, false, true><<<ga, kStepBlock, 0, s>>>(a, rec);
     else if (curved)
-        record ? k_stream_plain<true, true, false><<<sgrid, kStepBlock, 0, s>>>(a, rec)
-               : k_stream_plain<true, false, false><<<sgrid, kStepBlock, 0, s>>>(a, rec);
+        record ? k_stream_plain<true, true, false><<<gf, kStepBlock, 0, s>>>(a, rec)
+               : k_stream_plain<true, false, false><<<gf, kStepBlock, 0, s>>>(a, rec);
     else
-        record ? k_stream_plain<false, true, false><<<sgrid, kStepBlock, 0, s>>>(a, rec)
-               : k_stream_plain<false, false, false><<<sgrid, kStepBlock, 0, s>>>(a, rec);
+        record ? k_stream_plain<false, true, false><<<gf, kStepBlock, 0, s>>>(a, rec)
+               : k_stream_plain<false, false, false><<<gf, kStepBlock, 0, s>>>(a, rec);
     // moments and collide
     if (adaptive)
         k_collide_plain<false, true><<<cgrid, kStepBlock, 0, s>>>(a, rec);
@@ -789,6 +812,10 @@ void launch_sources32(float *I, const StateLayout &L, int nd, const int64_t *nod
                       cudaStream_t s)
 {
     k_sources<float><<<nblk(nsrc * nd, 256), 256, 0, s>>>(I, L, nd, nodes, vals, nsrc);
+}
+void launch_coef_k_major(const double *coef, double *coef_k, int64_t nxy, int nf, cudaStream_t s)
+{
+    k_coef_k_major<<<nblk(5 * nxy * nf, 256), 256, 0, s>>>(coef, coef_k, nxy, nf);
 }
 void launch_moments_lf64(int64_t nxy, const double *mom, const double *lfp, const uint8_t *bh, double *out,
                          cudaStream_t s)
