@@ -211,6 +211,13 @@ struct PrecStepArgs
     unsigned pitch, plane;    // state row pitch (a multiple of 4 floats) and plane stride
     unsigned *fault;          // set to 1 when a staging copy does not land within its time limit
     CUtensorMap in_map;       // TMA map of Iin: 2D, {pitch, ny * nd} floats, box of one patch plane
+    // adaptive streaming only (null otherwise)
+    const double *ang_old, *ang_new; // rotation angles before and after this step's update (nxy)
+    const double *coef_k;            // [5][nf][nxy]: the Fourier coefficients, node index fastest
+    const double *cx, *cy;           // nd: the stencil's unrotated directions
+    const IgRow *ig_rows;            // ng: the interpolation grid
+    float *S;                        // [d * nxy + ij]: the streamed values of the step
+    int nf;
 };
 
 // Direction tables of the precision form, passed by value as a kernel
@@ -308,6 +315,9 @@ cudaError_t run_wait_selftest(int arrive, unsigned long long limit_ns, int *comp
 // layout L and nd planes over ny rows each).
 cudaError_t encode_state_map(CUtensorMap *map, const float *state, const StateLayout &L, int64_t ny, int nd);
 void launch_step_prec(const PrecStepArgs &a, const DirTable &dt, bool curved, cudaStream_t s);
+// the adaptive streaming types in the precision form: stream, then moments
+// and collide (and the rotation update before, the halo moments after)
+void launch_step_prec_adaptive(const PrecStepArgs &a, const DirTable &dt, bool curved, cudaStream_t s);
 int step_prec_tiles_x(int64_t nx_);
 int step_prec_tiles_y(int64_t rows);
 cudaError_t prepare_step_batch(int smem_bytes, int *blocks_per_sm);
@@ -339,5 +349,9 @@ void launch_widen32(const float *in, double *out, int64_t n, cudaStream_t s);
 void launch_moments_from_I64(const double *I, int64_t nxy, int nd, const double *w, const double *n1,
                              const double *n2, const double *ang, double *mom, cudaStream_t s);
 void launch_moments_from_I32(const float *J, int64_t nxy, const StateLayout &L, int nd, const double *w,
-                             const double *n1, const double *n2, const float *scale, double *mom, cudaStream_t s);
+                             const double *n1, const double *n2, const float *scale, const double *ang, double *mom,
+                             cudaStream_t s);
+void launch_rotation_update32(const GridDev &g, const float *mom, const double *ang_old, double *ang_new,
+                              cudaStream_t s);
+void launch_zero_halo_moments32(const GridDev &g, float *mom, cudaStream_t s);
 } // namespace grlbm

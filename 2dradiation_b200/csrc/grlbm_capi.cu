@@ -192,7 +192,8 @@ void invalidate_graphs(grlbm_ctx *ctx)
 // per-node factor between the precision form's stored state and I (null: none)
 const float *state_scale(const grlbm_ctx *ctx)
 {
-    return (ctx->fp32 && ctx->run.streaming_type == GRLBM_CURVED_FIXED) ? ctx->ia3.as<float>() : nullptr;
+    const int st = ctx->run.streaming_type;
+    return (ctx->fp32 && (st == GRLBM_CURVED_FIXED || st == GRLBM_CURVED_ADAPTIVE)) ? ctx->ia3.as<float>() : nullptr;
 }
 
 // Arguments of the precision-form step that reads intensity buffer `from`.
@@ -224,6 +225,13 @@ PrecStepArgs prec_args(grlbm_ctx *ctx, int from)
     a.plane = (unsigned)ctx->sl.plane;
     a.fault = ctx->fault;
     a.in_map = ctx->in_map[from];
+    // adaptive streaming (the angles are set per step)
+    a.coef_k = ctx->coef_k.as<double>();
+    a.cx = ctx->cx.as<double>();
+    a.cy = ctx->cy.as<double>();
+    a.ig_rows = ctx->ig_rows.as<IgRow>();
+    a.S = ctx->streamed.as<float>();
+    a.nf = ctx->ss.n;
     return a;
 }
 
@@ -281,8 +289,19 @@ int enqueue_step(grlbm_ctx *ctx, int from)
         if (ctx->run.keep_source_nodes_active && ctx->nsrc > 0)
             launch_sources32(ctx->I[from].as<float>(), ctx->sl, ctx->st.n, ctx->src_nodes.as<int64_t>(),
                              ctx->src_vals.as<float>(), ctx->nsrc, ctx->stream);
-        const PrecStepArgs a = prec_args(ctx, from);
-        launch_step_prec(a, ctx->dirs, curved, ctx->stream);
+        PrecStepArgs a = prec_args(ctx, from);
+        if (is_adaptive(ctx))
+        {
+            // LoadInitialData also sets the source nodes' angles (src/Radiation.cpp:170-176)
+            if (ctx->run.keep_source_nodes_active && ctx->nsrc_ang > 0)
+                launch_sources64(ctx->ang[from].as<double>(), ctx->gd.nxy, 1, ctx->src_ang_nodes.as<int64_t>(),
+                                 ctx->src_ang_vals.as<double>(), ctx->nsrc_ang, ctx->stream);
+            a.ang_old = ctx->ang[from].as<double>();
+            a.ang_new = ctx->ang[from ^ 1].as<double>();
+            launch_step_prec_adaptive(a, ctx->dirs, curved, ctx->stream);
+        }
+        else
+            launch_step_prec(a, ctx->dirs, curved, ctx->stream);
     }
     else
     {
@@ -454,9 +473,6 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
     if (run->streaming_type == GRLBM_GEODESIC_FIXED)
         return fail(nullptr, GRLBM_ERR_UNSUPPORTED,
                     "GeodesicFixed (a performance test of the reference) is not built");
-    if ((run->streaming_type == GRLBM_FLAT_ADAPTIVE || run->streaming_type == GRLBM_CURVED_ADAPTIVE) &&
-        run->precision != GRLBM_PLAIN_FP64)
-        return fail(nullptr, GRLBM_ERR_UNSUPPORTED, "adaptive streaming is built for GRLBM_PLAIN_FP64 only");
     if (run->precision != GRLBM_PLAIN_FP64 && run->precision != GRLBM_PRECISION_FP32)
         return fail(nullptr, GRLBM_ERR_ARGUMENT, "unknown precision %d", run->precision);
     const int maxdir = kMaxDirs;
@@ -664,9 +680,11 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
         for (int q = 0; q < 18; q++)
             dt.wmom[q] = (float)wm[q];
     }
-    else
+    // the interpolation grid's rows: the plain form's stream, and adaptive
+    // streaming in either form
+    if (!ctx->fp32 || is_adaptive(ctx))
     {
-std::vector<IgRow> rows(ctx->ng);
+        std::vector<IgRow> rows(ctx->ng);
         for (int g = 0; g < ctx->ng; g++)
         {
             const int64_t *x = &ctx->st.ig_index[4 * g];
@@ -746,8 +764,8 @@ std::vector<IgRow> rows(ctx->ng);
     }
     TRY(alloc(ctx, ctx->I[0], ib));
     TRY(alloc(ctx, ctx->I[1], ib));
-    if (!ctx->fp32)
-        TRY(alloc(ctx, ctx->streamed, (size_t)nxy * nd * sizeof(double)));
+    if (!ctx->fp32 || is_adaptive(ctx))
+        TRY(alloc(ctx, ctx->streamed, (size_t)nxy * nd * tsize(ctx)));
     TRY(alloc(ctx, ctx->mom, (size_t)6 * nxy * tsize(ctx)));
     TRY(alloc(ctx, ctx->rec, (size_t)ctx->ncell * nd * (ctx->fp32 ? sizeof(float4) : sizeof(double4))));
     if (ctx->fp32)
@@ -881,7 +899,7 @@ int grlbm_set_initial_data(grlbm_ctx *ctx, const uint8_t *is_initial, const doub
         return fail(ctx, GRLBM_ERR_HOST, "source set-up failed: %s", e.what());
     }
     ctx->nsrc = (int64_t)S.nodes.size();
-    if (ctx->fp32 && ctx->run.streaming_type == GRLBM_CURVED_FIXED)
+    if (ctx->fp32 && is_curved(ctx))
     {
         // the precision form stores I / alpha^3
         const int nd = ctx->st.n;
@@ -1246,8 +1264,15 @@ int grlbm_write_frame_csv(grlbm_ctx *ctx, float time, const char *directory, con
     // (src/Radiation.cpp:239-301), as RunSimulation does before each frame
     const double *d64 = ctx->dirs64.as<double>();
     if (ctx->fp32)
-        launch_moments_from_I32(ctx->I[ctx->cur].as<float>(), nxy, ctx->sl, nd, d64, d64 + nd, d64 + 2 * nd,
-                                state_scale(ctx), ctx->frame_mom.as<double>(), ctx->stream);
+    {
+        if (is_adaptive(ctx))
+            launch_moments_from_I32(ctx->I[ctx->cur].as<float>(), nxy, ctx->sl, nd, d64, ctx->cx.as<double>(),
+                                    ctx->cy.as<double>(), state_scale(ctx), ctx->ang[ctx->cur].as<double>(),
+                                    ctx->frame_mom.as<double>(), ctx->stream);
+        else
+            launch_moments_from_I32(ctx->I[ctx->cur].as<float>(), nxy, ctx->sl, nd, d64, d64 + nd, d64 + 2 * nd,
+                                    state_scale(ctx), nullptr, ctx->frame_mom.as<double>(), ctx->stream);
+    }
     else
     {
         if (is_adaptive(ctx))
@@ -1723,6 +1748,9 @@ int grlbm_batch_create(grlbm_ctx *const *ctxs, int32_t n, grlbm_batch **out)
         if (c->run.keep_source_nodes_active && c->nsrc > 0)
             return bfail(nullptr, GRLBM_ERR_UNSUPPORTED,
                          "grlbm_batch_create: context %d keeps source nodes active (not batched)", k);
+        if (is_adaptive(c))
+            return bfail(nullptr, GRLBM_ERR_UNSUPPORTED,
+                         "grlbm_batch_create: context %d streams adaptively (not batched)", k);
         for (int j = 0; j < k; j++)
             if (ctxs[j] == c)
                 return bfail(nullptr, GRLBM_ERR_ARGUMENT, "grlbm_batch_create: context %d appears twice", k);

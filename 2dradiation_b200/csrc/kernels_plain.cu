@@ -511,7 +511,8 @@ __global__ void __launch_bounds__(kStepBlock) k_collide_plain(PlainStepArgs a, S
 // UpdateRotationMatrizes (src/Radiation.cpp:361-378): for the interior cells
 // of the slab, the angle of the flux averaged over the 3x3 neighbourhood
 // where at least 1% of the light moves along it, else the previous angle.
-__global__ void k_rotation_update(GridDev g, const double *mom, const double *ang_old, double *ang_new)
+template <typename T>
+__global__ void k_rotation_update(GridDev g, const T *mom, const double *ang_old, double *ang_new)
 {
     const int64_t c0 = (g.jlo - 1) * g.nx_;
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -525,19 +526,20 @@ __global__ void k_rotation_update(GridDev g, const double *mom, const double *an
         for (int a = -1; a <= 1; a++)
         {
             const int64_t n = (i + a) + (j + b) * g.nx;
-            fx += mom[n + nxy];
-            fy += mom[n + 2 * nxy];
+            fx += (double)mom[n + nxy];
+            fy += (double)mom[n + 2 * nxy];
         }
     fx /= 9.0;
     fy /= 9.0;
     const double norm = sqrt(fx * fx + fy * fy);
-    const double E = mom[ij];
+    const double E = (double)mom[ij];
     ang_new[ij] = (E > 1e-16 && norm / E > 0.01) ? approx_phi(fx, fy) : ang_old[ij];
 }
 
 // The moments at the halo nodes, which the reference recomputes after every
 // stream from intensities it never writes there (zero).
-__global__ void k_zero_halo_moments(GridDev g, double *mom)
+template <typename T>
+__global__ void k_zero_halo_moments(GridDev g, T *mom)
 {
     const int64_t ij = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (ij >= g.nxy)
@@ -545,7 +547,7 @@ __global__ void k_zero_halo_moments(GridDev g, double *mom)
     const int64_t i = ij % g.nx, j = ij / g.nx;
     if (i == 0 || i == g.nx - 1 || j == 0 || j == g.ny - 1)
         for (int q = 0; q < 6; q++)
-            mom[ij + q * g.nxy] = 0.0;
+            mom[ij + q * g.nxy] = (T)0;
 }
 
 // Radiation::ComputeMomentsIF (src/Radiation.cpp:239-269): the six moments
@@ -781,7 +783,7 @@ void launch_step_plain(const PlainStepArgs &a, bool curved, cudaStream_t s, cons
     const unsigned tx = nblk(a.g.nx_, kSplitTileX), ty = nblk(a.g.jhi - a.g.jlo, kSplitTileY);
     const dim3 sgrid(tx, ty, (unsigned)a.nd), sgrid_df((unsigned)a.nd, tx, ty), cgrid(tx, ty);
     if (adaptive) // UpdateRotationMatrizes from the previous moments, before the stream
-        k_rotation_update<<<nblk(cells, 128), 128, 0, s>>>(a.g, a.mom, a.ang_old, const_cast<double *>(a.ang_new));
+        k_rotation_update<double><<<nblk(cells, 128), 128, 0, s>>>(a.g, a.mom, a.ang_old, const_cast<double *>(a.ang_new));
     // stream
     const dim3 ga = kDirFastestAdaptive ? sgrid_df : sgrid, gf = kDirFastestFixed ? sgrid_df : sgrid;
     if (adaptive)
@@ -801,7 +803,7 @@ void launch_step_plain(const PlainStepArgs &a, bool curved, cudaStream_t s, cons
     else
         k_collide_plain<false, false><<<cgrid, kStepBlock, 0, s>>>(a, rec);
     if (adaptive) // the halo moments, recomputed by the reference from unwritten (zero) intensities
-        k_zero_halo_moments<<<nblk(a.g.nxy, 256), 256, 0, s>>>(a.g, a.mom);
+        k_zero_halo_moments<double><<<nblk(a.g.nxy, 256), 256, 0, s>>>(a.g, a.mom);
 }
 void launch_sources64(double *I, int64_t nxy, int nd, const int64_t *nodes, const double *vals, int64_t nsrc,
                       cudaStream_t s)
@@ -816,6 +818,19 @@ void launch_sources32(float *I, const StateLayout &L, int nd, const int64_t *nod
 void launch_coef_k_major(const double *coef, double *coef_k, int64_t nxy, int nf, cudaStream_t s)
 {
     k_coef_k_major<<<nblk(5 * nxy * nf, 256), 256, 0, s>>>(coef, coef_k, nxy, nf);
+}
+// UpdateRotationMatrizes before, and the halo moments after, an adaptive
+// precision-form step (FP32 moments)
+void launch_rotation_update32(const GridDev &g, const float *mom, const double *ang_old, double *ang_new,
+                              cudaStream_t s)
+{
+    const int64_t cells = (g.jhi - g.jlo) * g.nx_;
+    if (cells > 0)
+        k_rotation_update<float><<<nblk(cells, 128), 128, 0, s>>>(g, mom, ang_old, ang_new);
+}
+void launch_zero_halo_moments32(const GridDev &g, float *mom, cudaStream_t s)
+{
+    k_zero_halo_moments<float><<<nblk(g.nxy, 256), 256, 0, s>>>(g, mom);
 }
 void launch_moments_lf64(int64_t nxy, const double *mom, const double *lfp, const uint8_t *bh, double *out,
                          cudaStream_t s)
@@ -864,9 +879,10 @@ void launch_moments_from_I64(const double *I, int64_t nxy, int nd, const double 
                                                              mom);
 }
 void launch_moments_from_I32(const float *J, int64_t nxy, const StateLayout &L, int nd, const double *w,
-                             const double *n1, const double *n2, const float *scale, double *mom, cudaStream_t s)
+                             const double *n1, const double *n2, const float *scale, const double *ang, double *mom,
+                             cudaStream_t s)
 {
-    k_moments_from_I<float><<<nblk(nxy, 128), 128, 0, s>>>(J, nxy, L, nd, w, n1, n2, scale, nullptr, mom);
+    k_moments_from_I<float><<<nblk(nxy, 128), 128, 0, s>>>(J, nxy, L, nd, w, n1, n2, scale, ang, mom);
 }
 void launch_widen32(const float *in, double *out, int64_t n, cudaStream_t s)
 {

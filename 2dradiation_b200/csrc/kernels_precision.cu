@@ -24,6 +24,7 @@
 // pass whose Kahan sums give the stored moments.
 #include <cudaTypedefs.h>
 
+#include "approx_math.hpp"
 #include "device_common.cuh"
 
 // Tuning of the step kernels: resident blocks per SM the register budget is
@@ -625,6 +626,272 @@ __global__ void __launch_bounds__(kStepBlock, GRLBM_PREC_MIN_BLOCKS)
     }
 }
 
+// ---------------------------------------------------------------------------
+// Adaptive streaming in the precision form (FlatAdaptive, CurvedAdaptive;
+// src/Radiation.cpp:415-452, 513-575), as two kernels: one thread per (cell,
+// direction) streams into S, then one thread per cell takes the moments and
+// collides.  FP32 arithmetic, FP32 state (J = I / alpha^3 for curved
+// streaming); the Fourier series sum in FP64 over an FP32 basis.
+constexpr int kATileX = 16, kATileY = kStepBlock / kATileX;
+constexpr float kTwoPiF = 6.28318530717958647692f;
+
+// IntensityAt (src/Radiation.cpp:322-343) on the FP32 state: the direction
+// (v1, v2) rotated into node n's previous frame, the two cubic rows of the
+// interpolation grid at its angle, blended and clamped at zero.  sidx: the
+// node's place in a state plane.
+__device__ __forceinline__ float intensity_at32(const PrecStepArgs &a, int n, unsigned sidx, float v1, float v2)
+{
+    // the inverse of the node's previous rotation, with the reference's
+    // polynomial trigonometry (as the plain form)
+    const double th = fmod(-a.ang_old[n] + 2.0 * kPi, 2.0 * kPi);
+    const float sn = (float)approx_sin(th), cs = (float)approx_cos(th);
+    const float w1 = v1 * cs - v2 * sn, w2 = v1 * sn + v2 * cs;
+    float dd = (float)((double)a.ng * approx_phi((double)w1, (double)w2) / (2.0 * kPi));
+    dd = fminf(fmaxf(dd, 1e-8f), nextafterf((float)a.ng, 0.f)); // InterpolationGrid's clamp, in FP32
+    const int g0 = min((int)dd, a.ng - 1), g1 = g0 + 1 == a.ng ? 0 : g0 + 1;
+    const float t = dd - (float)g0;
+    const IgRow R0 = a.ig_rows[g0], R1 = a.ig_rows[g1];
+    const int idx0[4] = {R0.idx.x, R0.idx.y, R0.idx.z, R0.idx.w};
+    const int idx1[4] = {R1.idx.x, R1.idx.y, R1.idx.z, R1.idx.w};
+    const float wa[4] = {(float)R0.w01.x, (float)R0.w01.y, (float)R0.w23.x, (float)R0.w23.y};
+    const float wb[4] = {(float)R1.w01.x, (float)R1.w01.y, (float)R1.w23.x, (float)R1.w23.y};
+    float x0 = 0.f, x1 = 0.f;
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+    {
+        x0 = fmaf(wa[k], __ldg(a.Iin + (unsigned)idx0[k] * a.plane + sidx), x0);
+        x1 = fmaf(wb[k], __ldg(a.Iin + (unsigned)idx1[k] * a.plane + sidx), x1);
+    }
+    return fmaxf(fmaf(t, x1 - x0, x0), 0.f);
+}
+
+// One adaptive stream value (I, not J) of cell (i, j) for its direction d
+// rotated by the cell's new angle.
+template <bool CURVED>
+__device__ __forceinline__ float stream_adaptive32(const PrecStepArgs &a, int d, int i, int j, int ij)
+{
+    const int nx = (int)a.g.nx;
+    const double th = a.ang_new[ij];
+    const float sc = (float)approx_sin(th), cc = (float)approx_cos(th);
+    const float cxd = (float)a.cx[d], cyd = (float)a.cy[d];
+    const float dir1 = cxd * cc - cyd * sc, dir2 = cxd * sc + cyd * cc;
+    float it, jt, v1, v2, s3 = 1.f;
+    if constexpr (CURVED)
+    {
+        // the five series (S, X, Y, Cx, Cy) at the direction's angle: basis
+        // {1, sqrt2 cos(m phi), sqrt2 sin(m phi)} from one sincos and the
+        // angle-addition recurrence
+        const float phi = (float)approx_phi((double)dir1, (double)dir2);
+        float s1, c1;
+        sincosf(phi, &s1, &c1);
+        const int64_t fs = a.g.nxy * a.nf;
+        const double *cf = a.coef_k + ij;
+        double r[5];
+#pragma unroll
+        for (int q = 0; q < 5; q++)
+            r[q] = cf[q * fs];
+        float cm = 1.f, sm = 0.f;
+        const float sqrt2 = 1.41421356237f;
+        for (int k = 1; k < a.nf; k++)
+        {
+            if (k & 1) // the next multiple of phi
+            {
+                const float c2 = cm * c1 - sm * s1;
+                sm = sm * c1 + cm * s1;
+                cm = c2;
+            }
+            const double b = (double)(sqrt2 * ((k & 1) ? cm : sm));
+            const double *ck = cf + (int64_t)k * a.g.nxy;
+#pragma unroll
+            for (int q = 0; q < 5; q++)
+                r[q] = fma(ck[q * fs], b, r[q]);
+        }
+        const double xt = r[1], yt = r[2];
+        if (dev_inside_bh(a.g, xt, yt))
+            return 0.f;
+        it = (float)((xt - a.g.startx) / a.g.dx);
+        jt = (float)((yt - a.g.starty) / a.g.dy);
+        const float sh = (float)r[0];
+        s3 = sh * sh * sh;
+        v1 = (float)r[3];
+        v2 = (float)r[4];
+    }
+    else
+    {
+        it = (float)i - dir1 * (float)(a.g.dt / a.g.dx);
+        jt = (float)j - dir2 * (float)(a.g.dt / a.g.dy);
+        v1 = dir1;
+        v2 = dir2;
+    }
+    const int i0 = min(max((int)floorf(it), 0), nx - 2);
+    const int j0 = min(max((int)floorf(jt), 0), (int)a.g.ny - 2);
+    const float fx = it - (float)i0, fy = jt - (float)j0;
+    float Iq[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) // corners 00, 01, 10, 11
+    {
+        const int ci = i0 + (q >> 1), cj = j0 + (q & 1);
+        Iq[q] = intensity_at32(a, ci + cj * nx, (unsigned)ci + (unsigned)cj * a.pitch, v1, v2);
+    }
+    const float f0 = fmaf(fx, Iq[2] - Iq[0], Iq[0]);
+    const float f1 = fmaf(fx, Iq[3] - Iq[1], Iq[1]);
+    const float bil = fmaf(fy, f1 - f0, f0);
+    // corners hold J = I / alpha^3: (alpha_ij / alpha_c)^3 I_c = alpha_ij^3 J_c
+    return CURVED ? s3 * bil / a.ia3[ij] : bil;
+}
+
+// Stream: blocks are 16 x 8 tiles of cells of one direction, directions
+// fastest in the grid (the blocks of one tile share its coefficients).
+template <bool CURVED>
+__global__ void __launch_bounds__(kStepBlock) k_stream_prec_adaptive(PrecStepArgs a)
+{
+    const int d = blockIdx.x;
+    const int i = 1 + (int)blockIdx.y * kATileX + (int)(threadIdx.x % kATileX);
+    const int j = (int)a.g.jlo + (int)blockIdx.z * kATileY + (int)(threadIdx.x / kATileX);
+    if (i > a.g.nx_ || j >= a.g.jhi)
+        return;
+    const int ij = i + j * (int)a.g.nx;
+    float v = 0.f;
+    if (!(CURVED && (a.flags[ij] & 2)))
+        v = stream_adaptive32<CURVED>(a, d, i, j, ij);
+    a.S[(size_t)d * (size_t)a.g.nxy + (size_t)ij] = v;
+}
+
+// Moments and collide of one cell from its streamed values, with its
+// stencil rotated by its new angle: Kahan moments of the streamed values,
+// the lambda iteration in moment space (as the fixed-streaming kernel's
+// moving-fluid path), the collided state J = I / alpha^3 and its moments.
+template <bool CURVED>
+__global__ void __launch_bounds__(kStepBlock) k_collide_prec_adaptive(PrecStepArgs a, const __grid_constant__ DirTable dt)
+{
+    const int ti = 1 + (int)blockIdx.x * kATileX + (int)(threadIdx.x % kATileX);
+    const int tj = (int)a.g.jlo + (int)blockIdx.y * kATileY + (int)(threadIdx.x / kATileX);
+    const bool active = ti <= a.g.nx_ && tj < a.g.jhi;
+    const int i = active ? ti : 1, j = active ? tj : 1;
+    const int ij = i + j * (int)a.g.nx;
+    const unsigned nxy = (unsigned)a.g.nxy;
+    const uint8_t fl = active ? a.flags[ij] : (uint8_t)3;
+    const bool collides = active && !(fl & 1);
+    const float *S = a.S + ij;
+    // the cell's stencil, rotated (shared by the block's threads per direction)
+    __shared__ float sw[kMaxDirs], scx[kMaxDirs], scy[kMaxDirs];
+    for (int d = threadIdx.x; d < a.nd; d += kStepBlock)
+        sw[d] = dt.w[d], scx[d] = (float)a.cx[d], scy[d] = (float)a.cy[d];
+    __syncthreads();
+    const float rs = (float)approx_sin(a.ang_new[ij]), rc = (float)approx_cos(a.ang_new[ij]);
+#define GRLBM_RN1(d) (scx[d] * rc - scy[d] * rs)
+#define GRLBM_RN2(d) (scx[d] * rs + scy[d] * rc)
+    KMoments km;
+    km.zero();
+    for (int d0 = 0; d0 < a.nd; d0 += kChunk)
+    {
+        const int dend = min(d0 + kChunk, a.nd);
+        for (int d = d0; d < dend; d++)
+        {
+            const float n1 = GRLBM_RN1(d), n2 = GRLBM_RN2(d), w = sw[d];
+            const float wn1 = w * n1, wn2 = w * n2;
+            km.add(S[(unsigned)d * nxy], make_float4(w, wn1, wn2, wn1 * n1), make_float4(wn1 * n2, wn2 * n2, n1, n2));
+        }
+        km.fold();
+    }
+    float m[6] = {km.E.s, km.Fx.s, km.Fy.s, km.Pxx.s, km.Pxy.s, km.Pyy.s};
+    int cycles = 0;
+    if (collides)
+    {
+        const float u1 = a.u1[ij], u2 = a.u2[ij], lor = a.lor[ij], adt = a.adt[ij];
+        const float eta = a.eta[ij], k0 = a.k0[ij], k3 = a.k3[ij], kak0 = a.ka[ij] + a.k0[ij];
+        // m_new[q] = A[q] + (eta + k0 fE) B[q] + k3 (fFx C[q] + fFy D[q])
+        float A6[6], B6[6], C6[6], D6[6];
+#pragma unroll
+        for (int q = 0; q < 6; q++)
+            A6[q] = B6[q] = C6[q] = D6[q] = 0.f;
+        for (int d = 0; d < a.nd; d++)
+        {
+            const float n1 = GRLBM_RN1(d), n2 = GRLBM_RN2(d), w = sw[d];
+            float g, h, q1, q2;
+            collide_coeffs(n1, n2, u1, u2, lor, adt, kak0, g, h, q1, q2);
+            const float mu[6] = {1.f, n1, n2, n1 * n1, n1 * n2, n2 * n2};
+            const float gs = w * g * S[(unsigned)d * nxy], wh = w * h;
+#pragma unroll
+            for (int q = 0; q < 6; q++)
+            {
+                A6[q] += gs * mu[q];
+                B6[q] += wh * mu[q];
+                C6[q] += wh * q1 * mu[q];
+                D6[q] += wh * q2 * mu[q];
+            }
+        }
+        float diff = 1.f;
+        float fE = 0.f, fFx = 0.f, fFy = 0.f;
+        while (fabsf(diff) > 1e-4f && cycles < 100)
+        {
+            cycles++;
+            const float pE = m[0], pFx = m[1], pFy = m[2], pPxx = m[3], pPxy = m[4], pPyy = m[5];
+            const float uF = u1 * pFx + u2 * pFy;
+            const float uxP = u1 * pPxx + u2 * pPxy;
+            const float uyP = u1 * pPxy + u2 * pPyy;
+            const float uuP = u1 * uxP + u2 * uyP;
+            fE = lor * lor * (pE - 2.f * uF + uuP);
+            const float rr = lor / (1.f + lor) * ((2.f * lor + 1.f) * uF - lor * uuP);
+            fFx = lor * lor * (pFx - lor * pE * u1 - uxP + u1 * rr);
+            fFy = lor * lor * (pFy - lor * pE * u2 - uyP + u2 * rr);
+            const float e = eta + k0 * fE;
+            const float prev[6] = {pE, pFx, pFy, pPxx, pPxy, pPyy};
+            float s2 = 0.f;
+#pragma unroll
+            for (int q = 0; q < 6; q++)
+            {
+                m[q] = A6[q] + e * B6[q] + k3 * (fFx * C6[q] + fFy * D6[q]);
+                const float x = (prev[q] - m[q]) / m[q];
+                s2 += x * x;
+            }
+            diff = sqrtf(s2);
+        }
+        // the last iterate: the collided state and its compensated moments
+        km.zero();
+        const float e = eta + k0 * fE;
+        const float scale = CURVED ? a.ia3[ij] : 1.f;
+        float *out = a.Iout + (unsigned)i + (unsigned)j * a.pitch;
+        for (int d0 = 0; d0 < a.nd; d0 += kChunk)
+        {
+            const int dend = min(d0 + kChunk, a.nd);
+            for (int d = d0; d < dend; d++)
+            {
+                const float n1 = GRLBM_RN1(d), n2 = GRLBM_RN2(d), w = sw[d];
+                float g, h, q1, q2;
+                collide_coeffs(n1, n2, u1, u2, lor, adt, kak0, g, h, q1, q2);
+                const float v = g * S[(unsigned)d * nxy] + h * (e + k3 * (q1 * fFx + q2 * fFy));
+                out[(unsigned)d * a.plane] = v * scale;
+                const float wn1 = w * n1, wn2 = w * n2;
+                km.add(v, make_float4(w, wn1, wn2, wn1 * n1), make_float4(wn1 * n2, wn2 * n2, n1, n2));
+            }
+            km.fold();
+        }
+        m[0] = km.E.s, m[1] = km.Fx.s, m[2] = km.Fy.s, m[3] = km.Pxx.s, m[4] = km.Pxy.s, m[5] = km.Pyy.s;
+    }
+#undef GRLBM_RN1
+#undef GRLBM_RN2
+    if (active)
+    {
+#pragma unroll
+        for (int q = 0; q < 6; q++)
+            a.mom[(unsigned)ij + q * nxy] = m[q];
+    }
+    // lambda-iteration statistics: warp sums and maxima, one atomic per warp
+    unsigned sum = (unsigned)cycles, mx = (unsigned)cycles;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+    {
+        sum += __shfl_xor_sync(0xffffffffu, sum, o);
+        mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    }
+    if ((threadIdx.x & 31) == 0 && sum)
+    {
+        atomicAdd(a.iter_sum, (unsigned long long)sum);
+        atomicMax(a.iter_max, mx);
+    }
+}
+
 // The bounded staging wait on its own: one block waits on a phase of its
 // mbarrier that nothing completes (arrive = 0) or that thread 0 completes
 // (arrive = 1); the wait returns either way.
@@ -732,6 +999,29 @@ cudaError_t prepare_step_prec(int)
         return e;
     return cudaFuncSetAttribute(k_step_prec<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
 }
+void launch_step_prec_adaptive(const PrecStepArgs &a, const DirTable &dt, bool curved, cudaStream_t s)
+{
+    const int64_t rows = a.g.jhi - a.g.jlo;
+    if (rows <= 0 || a.g.nx_ <= 0)
+        return;
+    const unsigned tx = nblk(a.g.nx_, kATileX), ty = nblk(rows, kATileY);
+    // UpdateRotationMatrizes from the previous moments, before the stream
+    launch_rotation_update32(a.g, a.mom, a.ang_old, const_cast<double *>(a.ang_new), s);
+    const dim3 sgrid((unsigned)a.nd, tx, ty), cgrid(tx, ty);
+    if (curved)
+    {
+        k_stream_prec_adaptive<true><<<sgrid, kStepBlock, 0, s>>>(a);
+        k_collide_prec_adaptive<true><<<cgrid, kStepBlock, 0, s>>>(a, dt);
+    }
+    else
+    {
+        k_stream_prec_adaptive<false><<<sgrid, kStepBlock, 0, s>>>(a);
+        k_collide_prec_adaptive<false><<<cgrid, kStepBlock, 0, s>>>(a, dt);
+    }
+    // the halo moments, which the reference recomputes from unwritten (zero) intensities
+    launch_zero_halo_moments32(a.g, a.mom, s);
+}
+
 void launch_step_prec(const PrecStepArgs &a, const DirTable &dt, bool curved, cudaStream_t s)
 {
     const size_t smem = step_prec_smem(a.nd);

@@ -53,9 +53,9 @@ extern "C" {
 #define GRLBM_SCHWARZSCHILD 1
 #define GRLBM_KERRSCHILD 2
 
-/* StreamingType (src/Config.hh:5-12).  FlatFixed and CurvedFixed are built for
- * both arithmetic forms, FlatAdaptive and CurvedAdaptive for GRLBM_PLAIN_FP64;
- * GeodesicFixed (a performance test of the reference) is not built. */
+/* StreamingType (src/Config.hh:5-12).  FlatFixed, CurvedFixed, FlatAdaptive
+ * and CurvedAdaptive are built for both arithmetic forms; GeodesicFixed (a
+ * performance test of the reference) is not built. */
 #define GRLBM_FLAT_FIXED 0
 #define GRLBM_FLAT_ADAPTIVE 1
 #define GRLBM_CURVED_FIXED 2
@@ -257,8 +257,8 @@ int grlbm_departure_rows(grlbm_ctx *ctx, int32_t *rows);
  * running concurrently inside the graph.  Each problem's result is
  * bit-identical to stepping it alone; its
  * context stays usable (moments, intensities, statistics) between batch
- * steps.  Problems that keep source nodes active are not batched
- * (GRLBM_ERR_UNSUPPORTED).  A batch refers to its contexts: destroy it before
+ * steps.  Problems that keep source nodes active, and adaptive streaming
+ * problems, are not batched (GRLBM_ERR_UNSUPPORTED).  A batch refers to its contexts: destroy it before
  * them. */
 typedef struct grlbm_batch grlbm_batch;
 int grlbm_batch_create(grlbm_ctx *const *ctxs, int32_t n, grlbm_batch **out);

@@ -53,7 +53,7 @@ def _create(grlbm, case, **over):
 
 @pytest.mark.parametrize("over,code", [
     (dict(nx_=1), 1), (dict(endx=-7.0), 1), (dict(cfl=0.0), 1), (dict(kind=7), 1),
-    (dict(streaming_type=1, precision=1), 4), (dict(streaming_type=3, precision=1), 4), (dict(streaming_type=4), 4),
+    (dict(streaming_type=4), 4),
     (dict(streaming_type=9), 1), (dict(n_dir=2), 1), (dict(n_fourier=0), 1), (dict(n_fourier=65), 1),
     (dict(precision=3), 1), (dict(initial_data_type=5), 1),
 ])

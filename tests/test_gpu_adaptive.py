@@ -64,3 +64,29 @@ def test_curved_adaptive_matches_reference(grlbm, W, oracle):
     ours = run_ours(grlbm, case, ref)
     for key in ("E", "Fx", "Fy"):
         assert rel_l2(ours[key], ref[key]) <= 1e-11, (key, rel_l2(ours[key], ref[key]))
+
+
+def precision_cases(W):
+    """Adaptive cases for the precision form: the flat beam, a moving
+    anisotropically scattering fluid (flat and curved), and a curved shell."""
+    beam = W.flat_beam(nx_=40, ny_=30, n_dir=16, steps=25)
+    beam["streaming_type"] = W.FLAT_ADAPTIVE
+    shell = W.curved_shell(nx_=48, ny_=40, n_dir=24, n_fourier=7, steps=20)
+    shell["streaming_type"] = W.CURVED_ADAPTIVE
+    return [beam,
+            W.moving_scatter(nx_=30, ny_=26, n_dir=20, steps=12, metric_kind=W.MINKOWSKI,
+                             streaming_type=W.FLAT_ADAPTIVE),
+            W.moving_scatter(nx_=30, ny_=26, n_dir=20, steps=12, streaming_type=W.CURVED_ADAPTIVE),
+            shell]
+
+
+@pytest.mark.parametrize("k", [0, 1, 2, 3])
+def test_precision_form_adaptive_against_plain(grlbm, W, k):
+    """Adaptive streaming in the precision form (FP32 stream and moment-space
+    collide, FP32 Fourier basis) against the plain form on the same tables:
+    the precision form's tolerance."""
+    case = precision_cases(W)[k]
+    ref = grlbm.run(case, grlbm.PLAIN_FP64)
+    res = grlbm.run(case, grlbm.PRECISION_FP32)
+    for key in ("E", "Fx", "Fy"):
+        assert rel_l2(res[key], ref[key]) <= 2e-5, (key, rel_l2(res[key], ref[key]))

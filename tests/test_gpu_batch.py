@@ -64,7 +64,7 @@ def test_batch_shapes_match_single_problems(grlbm, W, shape):
             r.close()
 
 
-def test_batch_rejects_plain_and_source_problems(grlbm, W):
+def test_batch_rejects_plain_source_and_adaptive_problems(grlbm, W):
     c = W.batch_instances(count=1, seed=3, sizes=(24,), dirs=(8,), steps=2)[0]
     with grlbm.prepare(c, grlbm.PLAIN_FP64) as r:
         with pytest.raises(grlbm.GrlbmError) as e:
@@ -72,6 +72,12 @@ def test_batch_rejects_plain_and_source_problems(grlbm, W):
         assert e.value.code == 4
     beam = W.flat_beam(nx_=20, ny_=20, n_dir=8, steps=2)
     with grlbm.prepare(beam, grlbm.PRECISION_FP32) as r:
+        with pytest.raises(grlbm.GrlbmError) as e:
+            grlbm.Batch([r])
+        assert e.value.code == 4
+    c = dict(c)
+    c["streaming_type"] = W.FLAT_ADAPTIVE
+    with grlbm.prepare(c, grlbm.PRECISION_FP32) as r:
         with pytest.raises(grlbm.GrlbmError) as e:
             grlbm.Batch([r])
         assert e.value.code == 4
