@@ -800,7 +800,10 @@ __global__ void __launch_bounds__(kStepBlock) k_collide_prec_adaptive(PrecStepAr
     {
         const float u1 = a.u1[ij], u2 = a.u2[ij], lor = a.lor[ij], adt = a.adt[ij];
         const float eta = a.eta[ij], k0 = a.k0[ij], k3 = a.k3[ij], kak0 = a.ka[ij] + a.k0[ij];
-        // m_new[q] = A[q] + (eta + k0 fE) B[q] + k3 (fFx C[q] + fFy D[q])
+        // m_new[q] = A[q] + (eta + k0 fE) B[q] + k3 (fFx C[q] + fFy D[q]);
+        // at rest g and h are the same for every direction and q = n
+        const bool rest = (u1 == 0.f) && (u2 == 0.f);
+        const float g0 = 1.f / (1.f + adt * kak0), h0 = adt * g0;
         float A6[6], B6[6], C6[6], D6[6];
 #pragma unroll
         for (int q = 0; q < 6; q++)
@@ -808,8 +811,9 @@ __global__ void __launch_bounds__(kStepBlock) k_collide_prec_adaptive(PrecStepAr
         for (int d = 0; d < a.nd; d++)
         {
             const float n1 = GRLBM_RN1(d), n2 = GRLBM_RN2(d), w = sw[d];
-            float g, h, q1, q2;
-            collide_coeffs(n1, n2, u1, u2, lor, adt, kak0, g, h, q1, q2);
+            float g = g0, h = h0, q1 = n1, q2 = n2;
+            if (!rest)
+                collide_coeffs(n1, n2, u1, u2, lor, adt, kak0, g, h, q1, q2);
             const float mu[6] = {1.f, n1, n2, n1 * n1, n1 * n2, n2 * n2};
             const float gs = w * g * S[(unsigned)d * nxy], wh = w * h;
 #pragma unroll
@@ -858,8 +862,9 @@ __global__ void __launch_bounds__(kStepBlock) k_collide_prec_adaptive(PrecStepAr
             for (int d = d0; d < dend; d++)
             {
                 const float n1 = GRLBM_RN1(d), n2 = GRLBM_RN2(d), w = sw[d];
-                float g, h, q1, q2;
-                collide_coeffs(n1, n2, u1, u2, lor, adt, kak0, g, h, q1, q2);
+                float g = g0, h = h0, q1 = n1, q2 = n2;
+                if (!rest)
+                    collide_coeffs(n1, n2, u1, u2, lor, adt, kak0, g, h, q1, q2);
                 const float v = g * S[(unsigned)d * nxy] + h * (e + k3 * (q1 * fFx + q2 * fFy));
                 out[(unsigned)d * a.plane] = v * scale;
                 const float wn1 = w * n1, wn2 = w * n2;
