@@ -225,17 +225,20 @@ def open_form(G, case, prec, world, rank, local, pg):
 
 
 def run_configs(G, W, local):
-    """The two smaller configurations at their full sizes: the flat beam
-    (100^2 x 20, 500 steps) and the curved shell (200^2 x 32, 1000 steps), in
-    both forms, with the FP32 form's relative error of E.  Device time
-    of the whole run with CUDA events (graph-replayed steps, inputs resident,
-    no L2 flush: these problems fit in L2)."""
+    """The two smaller configurations at their full sizes -- the flat beam
+    (100^2 x 20, 500 steps) and the curved shell (200^2 x 32, 1000 steps) --
+    and the bench workload with adaptive streaming (50 steps), in both forms,
+    with the FP32 form's relative error of E.  Device time of the whole run
+    with CUDA events (graph-replayed steps, inputs resident, no L2 flush
+    between steps)."""
     import torch
     out = {}
     for name, case, forms in (
             ("flat_beam 100x100 x 20 directions, 500 steps", W.flat_beam(), (G.PLAIN_FP64, G.PRECISION_FP32)),
             ("curved_shell 200x200 x 32 directions, Fourier order 5, 1000 steps", W.curved_shell(),
-             (G.PLAIN_FP64, G.PRECISION_FP32))):
+             (G.PLAIN_FP64, G.PRECISION_FP32)),
+            ("curved_scatter adaptive (CurvedAdaptive) 400x400 x 64 directions, Fourier order 16, 50 steps",
+             dict(W.curved_scatter(steps=50), streaming_type=W.CURVED_ADAPTIVE), (G.PLAIN_FP64, G.PRECISION_FP32))):
         n = int(case["n_steps"])
         units = int(case["nx_"]) * int(case["ny_"]) * int(case["n_dir"]) * n
         res, E = {}, {}
