@@ -50,10 +50,13 @@ enum RkField : int
     RF_ALPHA, RF_B1, RF_B2, RF_DA1, RF_DA2, RF_DB11, RF_DB12, RF_DB21, RF_DB22,
     RF_K11, RF_K12, RF_K22, RF_GU11, RF_GU12, RF_GU22,
     RF_DG111, RF_DG112, RF_DG122, RF_DG211, RF_DG212, RF_DG222,
+    RF_PAD, // zero: the tetrad blocks start on 16-byte boundaries
     RF_T11, RF_T12, RF_T21, RF_T22, RF_TI11, RF_TI12, RF_TI21, RF_TI22,
     RF_COUNT
 };
 static_assert(RF_COUNT <= kRkStride, "rk pack stride");
+static_assert(RF_DG222 % 2 == 0 && RF_T11 % 2 == 0 && RF_TI11 % 2 == 0 && kRkStride % 2 == 0,
+              "fields read in pairs (16-byte loads)");
 
 constexpr int kStepBlock = 128;
 constexpr int kMaxDirs = 256;

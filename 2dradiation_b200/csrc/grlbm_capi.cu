@@ -703,11 +703,11 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
     static const int rkmap[RF_COUNT] = {ALPHA, BETA1U, BETA2U, D1ALPHA, D2ALPHA, D1BETA1LU, D1BETA2LU,
                                         D2BETA1LU, D2BETA2LU, K11L, K12L, K22L, GAM11U, GAM12U, GAM22U,
                                         D1GAM11LLL, D1GAM12LLL, D1GAM22LLL, D2GAM11LLL, D2GAM12LLL, D2GAM22LLL,
-                                        TET11, TET12, TET21, TET22, ITET11, ITET12, ITET21, ITET22};
+                                        -1, TET11, TET12, TET21, TET22, ITET11, ITET12, ITET21, ITET22};
     for (int64_t ij = 0; ij < nxy; ij++)
     {
         for (int f = 0; f < RF_COUNT; f++)
-            rkf[ij * kRkStride + f] = M.at(rkmap[f], ij);
+            rkf[ij * kRkStride + f] = rkmap[f] < 0 ? 0.0 : M.at(rkmap[f], ij);
         for (int q = 0; q < 9; q++)
             lfp[ij * 12 + q] = M.at(TET00 + q, ij);
         lfp[ij * 12 + 9] = M.at(GAM11L, ij);

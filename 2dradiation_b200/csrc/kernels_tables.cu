@@ -35,13 +35,21 @@ __device__ __forceinline__ void rk_local(const GridDev &g, const double *__restr
     const double *p10 = p00 + kRkStride;
     const double *p01 = p00 + g.nx * kRkStride;
     const double *p11 = p01 + kRkStride;
-    double v[RF_TI22 + 1];
+    // the fields in pairs (16-byte loads; the pair after RF_DG222 is the pad)
+    double v[RF_DG222 + 2];
 #pragma unroll
-    for (int f = 0; f <= RF_DG222; f++)
+    for (int f = 0; f <= RF_DG222; f += 2)
     {
-        const double f0 = __ldg(p00 + f) * (1.0 - tx) + __ldg(p10 + f) * tx;
-        const double f1 = __ldg(p01 + f) * (1.0 - tx) + __ldg(p11 + f) * tx;
+        const double2 a00 = __ldg(reinterpret_cast<const double2 *>(p00 + f));
+        const double2 a10 = __ldg(reinterpret_cast<const double2 *>(p10 + f));
+        const double2 a01 = __ldg(reinterpret_cast<const double2 *>(p01 + f));
+        const double2 a11 = __ldg(reinterpret_cast<const double2 *>(p11 + f));
+        double f0 = a00.x * (1.0 - tx) + a10.x * tx;
+        double f1 = a01.x * (1.0 - tx) + a11.x * tx;
         v[f] = f0 * (1.0 - ty) + f1 * ty;
+        f0 = a00.y * (1.0 - tx) + a10.y * tx;
+        f1 = a01.y * (1.0 - tx) + a11.y * tx;
+        v[f + 1] = f0 * (1.0 - ty) + f1 * ty;
     }
     L.alpha = v[RF_ALPHA];
     L.b1 = v[RF_B1];
@@ -87,11 +95,18 @@ __device__ __forceinline__ void tetrad_block(const GridDev &g, const double *__r
     const double *p11 = p01 + kRkStride;
     double v[4];
 #pragma unroll
-    for (int f = 0; f < 4; f++)
+    for (int f = 0; f < 4; f += 2) // in pairs: `first` is even
     {
-        const double f0 = __ldg(p00 + f) * (1.0 - tx) + __ldg(p10 + f) * tx;
-        const double f1 = __ldg(p01 + f) * (1.0 - tx) + __ldg(p11 + f) * tx;
+        const double2 a00 = __ldg(reinterpret_cast<const double2 *>(p00 + f));
+        const double2 a10 = __ldg(reinterpret_cast<const double2 *>(p10 + f));
+        const double2 a01 = __ldg(reinterpret_cast<const double2 *>(p01 + f));
+        const double2 a11 = __ldg(reinterpret_cast<const double2 *>(p11 + f));
+        double f0 = a00.x * (1.0 - tx) + a10.x * tx;
+        double f1 = a01.x * (1.0 - tx) + a11.x * tx;
         v[f] = f0 * (1.0 - ty) + f1 * ty;
+        f0 = a00.y * (1.0 - tx) + a10.y * tx;
+        f1 = a01.y * (1.0 - tx) + a11.y * tx;
+        v[f + 1] = f0 * (1.0 - ty) + f1 * ty;
     }
     a11 = v[0];
     a12 = v[1];
