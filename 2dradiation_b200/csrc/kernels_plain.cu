@@ -289,7 +289,7 @@ __device__ __forceinline__ double stream_value_adaptive(const PlainStepArgs &a, 
 #define GRLBM_N2(d) (ADAPTIVE ? tn1[d] * rot_s + tn2[d] * rot_c : tn2[d])
 
 // The rest of a step for one cell once its streamed values are known: m
-// holds their moments; Sin points at them (direction stride nxy), Sout at the
+// holds their moments; Sin points at them (direction stride sst), Sout at the
 // cell's output slots (the same slots in the fused step).  Collide
 // (src/Radiation.cpp:641-736) for a colliding cell, then the stored moments
 // and the lambda-iteration statistics.
@@ -297,7 +297,8 @@ __device__ __forceinline__ double stream_value_adaptive(const PlainStepArgs &a, 
 // rot_s, rot_c: the cell's rotation (adaptive streaming).
 template <bool RECORD, bool ADAPTIVE>
 __device__ __forceinline__ void finish_cell(const PlainStepArgs &a, const StepRecord &rec, bool active, bool collides,
-                                            int64_t ij, int64_t cc, Moments m, const double *Sin, double *Sout,
+                                            int64_t ij, int64_t cc, Moments m, const double *Sin, int64_t sst,
+                                            double *Sout,
                                             double rot_s, double rot_c, const double *tw, const double *tn1,
                                             const double *tn2)
 {
@@ -340,7 +341,7 @@ __device__ __forceinline__ void finish_cell(const PlainStepArgs &a, const StepRe
                 for (int d = 0; d < a.nd; d++)
                 {
                     const double n1 = GRLBM_N1(d), n2 = GRLBM_N2(d);
-                    const double num = Sin[(int64_t)d * nxy] + adt * (eta + (k0fE + k3 * (n1 * fFx + n2 * fFy)));
+                    const double num = Sin[(int64_t)d * sst] + adt * (eta + (k0fE + k3 * (n1 * fFx + n2 * fFy)));
                     const double v = fast_div ? div_rn(num, den, rden) : num / den;
                     m.add(tw[d], v, n1, n2);
                 }
@@ -349,7 +350,7 @@ __device__ __forceinline__ void finish_cell(const PlainStepArgs &a, const StepRe
                 for (int d = 0; d < a.nd; d++)
                 {
                     const double n1 = GRLBM_N1(d), n2 = GRLBM_N2(d);
-                    const double v = collide_value(Sin[(int64_t)d * nxy], n1, n2, u1, u2, lor, adt, eta, k0, k3,
+                    const double v = collide_value(Sin[(int64_t)d * sst], n1, n2, u1, u2, lor, adt, eta, k0, k3,
                                                    kak0, fE, fFx, fFy);
                     m.add(tw[d], v, n1, n2);
                 }
@@ -364,13 +365,13 @@ __device__ __forceinline__ void finish_cell(const PlainStepArgs &a, const StepRe
             for (int d = 0; d < a.nd; d++)
             {
                 const double n1 = GRLBM_N1(d), n2 = GRLBM_N2(d);
-                const double num = Sin[(int64_t)d * nxy] + adt * (eta + (k0fE + k3 * (n1 * fFx + n2 * fFy)));
+                const double num = Sin[(int64_t)d * sst] + adt * (eta + (k0fE + k3 * (n1 * fFx + n2 * fFy)));
                 Sout[(int64_t)d * nxy] = fast_div ? div_rn(num, den, rden) : num / den;
             }
         }
         else
             for (int d = 0; d < a.nd; d++)
-                Sout[(int64_t)d * nxy] = collide_value(Sin[(int64_t)d * nxy], GRLBM_N1(d), GRLBM_N2(d), u1, u2,
+                Sout[(int64_t)d * nxy] = collide_value(Sin[(int64_t)d * sst], GRLBM_N1(d), GRLBM_N2(d), u1, u2,
                                                      lor, adt, eta, k0, k3, kak0, fE, fFx, fFy);
     }
     if (RECORD && active)
@@ -408,9 +409,6 @@ __device__ __forceinline__ void finish_cell(const PlainStepArgs &a, const StepRe
 // clamp mask).
 // Blocks are 32 x 4 tiles of cells (blockIdx.x, blockIdx.y over the slab
 // rows) of one direction (blockIdx.z).
-#ifndef GRLBM_COLLIDE_SMEM_TABLES
-#define GRLBM_COLLIDE_SMEM_TABLES 1
-#endif
 #ifndef GRLBM_COLLIDE_UNROLL
 #define GRLBM_COLLIDE_UNROLL 8
 #endif
@@ -462,30 +460,32 @@ __global__ void __launch_bounds__(kStepBlock, GRLBM_STREAM_MIN_BLOCKS) k_stream_
 
 // Moments and collide: one thread per cell sums the moments of its streamed
 // values in direction order (ComputeMomentsIF's order, as the fused step
-// does) and finishes the cell; the collided intensities go to Iout.
-template <bool RECORD, bool ADAPTIVE>
+// does) and finishes the cell; the collided intensities go to Iout.  With
+// COLUMN (when the block's values fit in 48 KB of shared memory) each thread
+// keeps its cell's streamed values in its own column of shared memory for
+// the lambda iteration's passes, instead of re-reading them from L2.
+constexpr int kColumnTileY = 4; // 16 x 4 cells per block with COLUMN
+template <bool RECORD, bool ADAPTIVE, bool COLUMN>
 __global__ void __launch_bounds__(kStepBlock) k_collide_plain(PlainStepArgs a, StepRecord rec)
 {
-    const int ti = 1 + (int)blockIdx.x * kSplitTileX + (int)(threadIdx.x % kSplitTileX);
-    const int tj = (int)a.g.jlo + (int)blockIdx.y * kSplitTileY + (int)(threadIdx.x / kSplitTileX);
+    constexpr int TY = COLUMN ? kColumnTileY : kSplitTileY, NT = kSplitTileX * TY;
+    const int t = threadIdx.x;
+    const int ti = 1 + (int)blockIdx.x * kSplitTileX + t % kSplitTileX;
+    const int tj = (int)a.g.jlo + (int)blockIdx.y * TY + t / kSplitTileX;
     const bool active = ti <= a.g.nx_ && tj < a.g.jhi;
     const int64_t i = active ? ti : 1, j = active ? tj : 1;
     const int64_t cc = (i - 1) + (j - 1) * a.g.nx_;
     const int64_t ij = i + j * a.g.nx;
     const int64_t nxy = a.g.nxy;
     const bool collides = active && !(a.flags[ij] & 1);
-    const double *Sin = a.S + ij;
-#if GRLBM_COLLIDE_SMEM_TABLES
     // the stencil's weights and directions, read by every cell of the block
-    __shared__ double sw[kMaxDirs], sn1[kMaxDirs], sn2[kMaxDirs];
+    extern __shared__ double dyn[];
+    double *sw = dyn, *sn1 = dyn + a.nd, *sn2 = dyn + 2 * a.nd;
     const double *dn1 = ADAPTIVE ? a.cx : a.n1, *dn2 = ADAPTIVE ? a.cy : a.n2;
-    for (int d = threadIdx.x; d < a.nd; d += kStepBlock)
+    for (int d = t; d < a.nd; d += NT)
         sw[d] = a.w[d], sn1[d] = dn1[d], sn2[d] = dn2[d];
     __syncthreads();
     const double *tw = sw, *tn1 = sn1, *tn2 = sn2;
-#else
-    const double *tw = a.w, *tn1 = ADAPTIVE ? a.cx : a.n1, *tn2 = ADAPTIVE ? a.cy : a.n2;
-#endif
     // the cell's rotation (adaptive streaming)
     double rot_s = 0.0, rot_c = 1.0;
     if (ADAPTIVE)
@@ -494,16 +494,23 @@ __global__ void __launch_bounds__(kStepBlock) k_collide_plain(PlainStepArgs a, S
         rot_s = approx_sin(th);
         rot_c = approx_cos(th);
     }
+    const double *S = a.S + ij;
+    double *col = dyn + 3 * a.nd + t; // COLUMN: this cell's values, stride NT
     Moments m;
     m.zero();
     if (active)
     {
 #pragma unroll kCollideUnroll
         for (int d = 0; d < a.nd; d++)
-            m.add(tw[d], Sin[(int64_t)d * nxy], GRLBM_N1(d), GRLBM_N2(d));
+        {
+            const double v = S[(int64_t)d * nxy];
+            if (COLUMN)
+                col[d * NT] = v;
+            m.add(tw[d], v, GRLBM_N1(d), GRLBM_N2(d));
+        }
     }
-    finish_cell<RECORD, ADAPTIVE>(a, rec, active, collides, ij, cc, m, Sin, a.Iout + ij, rot_s, rot_c, tw, tn1,
-                                  tn2);
+    finish_cell<RECORD, ADAPTIVE>(a, rec, active, collides, ij, cc, m, COLUMN ? col : S, COLUMN ? NT : nxy,
+                                  a.Iout + ij, rot_s, rot_c, tw, tn1, tn2);
 }
 #undef GRLBM_N1
 #undef GRLBM_N2
@@ -795,13 +802,26 @@ void launch_step_plain(const PlainStepArgs &a, bool curved, cudaStream_t s, cons
     else
         record ? k_stream_plain<false, true, false><<<gf, kStepBlock, 0, s>>>(a, rec)
                : k_stream_plain<false, false, false><<<gf, kStepBlock, 0, s>>>(a, rec);
-    // moments and collide
-    if (adaptive)
-        k_collide_plain<false, true><<<cgrid, kStepBlock, 0, s>>>(a, rec);
+    // moments and collide: with each cell's values in shared memory when they fit
+    const size_t tables = 3 * (size_t)a.nd * sizeof(double);
+    const size_t column = tables + (size_t)a.nd * kSplitTileX * kColumnTileY * sizeof(double);
+    if (column <= 48 * 1024)
+    {
+        const dim3 kgrid(tx, nblk(a.g.jhi - a.g.jlo, kColumnTileY));
+        const unsigned nt = kSplitTileX * kColumnTileY;
+        if (adaptive)
+            k_collide_plain<false, true, true><<<kgrid, nt, column, s>>>(a, rec);
+        else if (record)
+            k_collide_plain<true, false, true><<<kgrid, nt, column, s>>>(a, rec);
+        else
+            k_collide_plain<false, false, true><<<kgrid, nt, column, s>>>(a, rec);
+    }
+    else if (adaptive)
+        k_collide_plain<false, true, false><<<cgrid, kStepBlock, tables, s>>>(a, rec);
     else if (record)
-        k_collide_plain<true, false><<<cgrid, kStepBlock, 0, s>>>(a, rec);
+        k_collide_plain<true, false, false><<<cgrid, kStepBlock, tables, s>>>(a, rec);
     else
-        k_collide_plain<false, false><<<cgrid, kStepBlock, 0, s>>>(a, rec);
+        k_collide_plain<false, false, false><<<cgrid, kStepBlock, tables, s>>>(a, rec);
     if (adaptive) // the halo moments, recomputed by the reference from unwritten (zero) intensities
         k_zero_halo_moments<double><<<nblk(a.g.nxy, 256), 256, 0, s>>>(a.g, a.mom);
 }
