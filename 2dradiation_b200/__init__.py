@@ -54,7 +54,8 @@ class RunDesc(C.Structure):
 class Stats(C.Structure):
     _fields_ = [("steps", C.c_int64), ("max_iterations", C.c_int32), ("average_iterations", C.c_double),
                 ("rk_substeps", C.c_int64), ("rk_nonconverged", C.c_int32),
-                ("departures_off_grid", C.c_int32), ("table_ms", C.c_double)]
+                ("departures_off_grid", C.c_int32), ("table_ms", C.c_double),
+                ("far_departures", C.c_int64)]
 
 
 _D = C.POINTER(C.c_double)

@@ -153,6 +153,7 @@ struct DepartureArgs
     int q, p;            // interpolation row period (row types) and its direction shift
     int row_base[32];    // first window direction of each row type
     int *clamped;
+    unsigned long long *far; // packed records marked far (precision form)
     int *row_extent;     // max over departures of the node rows away from the cell a gather reads
 };
 

@@ -75,7 +75,8 @@ struct grlbm_ctx
     DevBuf coef, ss_cx, ss_cy, ss_w, proj_basis, eval_basis, stage;
     DevBuf src_nodes, src_vals, lf_out, energy_partial, energy_out;
     // counters: [0] iteration sum, [1] iteration max (low 32 bits), [2] RK45
-    // trials, [3] capped backtraces, [4] departures off the grid
+    // trials, [3] capped backtraces, [4] departures off the grid, [5] row
+    // extent of the gathers, [6] far precision-form departures
     DevBuf counters;
     int64_t nsrc = 0;
     int cur = 0;
@@ -372,7 +373,8 @@ int build_records(grlbm_ctx *ctx)
         da.row_base[r] = (int)ctx->dirs.rowtab[r * 12 + 10];
     da.clamped = reinterpret_cast<int *>(ctx->counters.as<unsigned long long>() + 4);
     da.row_extent = reinterpret_cast<int *>(ctx->counters.as<unsigned long long>() + 5);
-    CU(cudaMemsetAsync(ctx->counters.as<unsigned long long>() + 4, 0, 2 * sizeof(unsigned long long), ctx->stream));
+    da.far = ctx->counters.as<unsigned long long>() + 6;
+    CU(cudaMemsetAsync(ctx->counters.as<unsigned long long>() + 4, 0, 3 * sizeof(unsigned long long), ctx->stream));
     launch_departure(da, ctx->stream);
     if (is_adaptive(ctx))
     {
@@ -1447,7 +1449,7 @@ int grlbm_get_stats(grlbm_ctx *ctx, grlbm_stats *s)
     if (!s)
         return fail(ctx, GRLBM_ERR_ARGUMENT, "null output");
     cudaSetDevice(ctx->device);
-    unsigned long long h[5];
+    unsigned long long h[7];
     CU(cudaStreamSynchronize(ctx->stream));
     CU(cudaMemcpy(h, ctx->counters.p, sizeof h, cudaMemcpyDeviceToHost));
     if (int rc = check_fault(ctx))
@@ -1460,6 +1462,7 @@ int grlbm_get_stats(grlbm_ctx *ctx, grlbm_stats *s)
     s->rk_nonconverged = (int32_t)(unsigned)h[3];
     s->departures_off_grid = (int32_t)(unsigned)h[4];
     s->table_ms = ctx->table_ms;
+    s->far_departures = ctx->fp32 ? (int64_t)h[6] : 0;
     return GRLBM_OK;
 }
 

@@ -436,6 +436,8 @@ __global__ void __launch_bounds__(128) k_departure(DepartureArgs a)
                               (code << packed::kCodeShift) | ((far ? 1u : 0u) << packed::kFarBit);
         const float fx = near ? (float)((double)r32.x - fxd) : 0.f, fy = near ? (float)((double)r32.y - fyd) : 0.f;
         a.rec32[tid] = make_float4(__uint_as_float(word), fx, fy, r32.w);
+        if (far && a.far)
+            atomicAdd(a.far, 1ull);
         a.side32[tid] = r32;
     }
     if (a.rec64)

@@ -115,6 +115,9 @@ typedef struct
                                     corners are clamped onto it); the reference
                                     reads past its arrays there */
     double table_ms;          /* device time of the last table build */
+    int64_t far_departures;   /* precision form: (cell, direction) pairs of the
+                                 last table build whose gather leaves the
+                                 staged patch (read from global memory) */
 } grlbm_stats;
 
 /* ---- context ------------------------------------------------------------

@@ -79,6 +79,29 @@ def test_precision_form_against_oracle(maker, kw, grlbm, W, oracle):
         assert rel_l2(res[k], ref[k]) <= 1e-5, k
 
 
+@pytest.mark.parametrize("cfl,far_min", [(0.9, 0.0), (1.5, 0.3), (2.5, 0.6)])
+def test_precision_form_far_departures(cfl, far_min, grlbm, W):
+    """Departures more than a cell away, or whose angular window leaves the
+    staged planes, are gathered from global memory (the packed record's far
+    bit).  At CFL 0.9 on the shell every departure is served from the staged
+    patch; at CFL 1.5 and 2.5 most are far, some off the grid, and the FP32
+    form still follows the FP64 form."""
+    case = W.make_case("curved_shell", nx_=64, ny_=64, n_dir=32, n_fourier=5, steps=20)
+    case["cfl"] = cfl
+    r = grlbm.prepare(case, 1)
+    far = r.stats()["far_departures"]
+    r.close()
+    total = 64 * 64 * 32
+    if far_min == 0.0:
+        assert far == 0
+    else:
+        assert far >= far_min * total, far
+    ref = grlbm.run(case, 0)
+    res = grlbm.run(case, 1)
+    for k in ("E", "Fx", "Fy", "I"):
+        assert rel_l2(res[k], ref[k]) <= 2e-5, k
+
+
 @pytest.mark.parametrize("maker,kw", [
     ("curved_shell", dict(nx_=37, ny_=23, n_dir=12, n_fourier=5, steps=20)),     # ragged tiles, plane ring wraps
     ("flat_beam", dict(nx_=2, ny_=2, n_dir=8, steps=3)),                          # smallest grid
