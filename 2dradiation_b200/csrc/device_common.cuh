@@ -193,6 +193,7 @@ struct PlainStepArgs
     // adaptive streaming only (null otherwise): rotation angles before and
     // after this step's update (nxy), and the Fourier coefficients
     const double *ang_old, *ang_new;
+    const double2 *rot_inv, *rot_new; // per node {sin, cos}: inverse previous rotation, new rotation
     const double *coef; // [5][nf][nxy]: the Fourier coefficients, node index fastest
     int nf;
     double *S; // the streamed values of the step, [d * nxy + ij]
@@ -217,6 +218,7 @@ struct PrecStepArgs
     CUtensorMap in_map;       // TMA map of Iin: 2D, {pitch, ny * nd} floats, box of one patch plane
     // adaptive streaming only (null otherwise)
     const double *ang_old, *ang_new; // rotation angles before and after this step's update (nxy)
+    const double2 *rot_inv, *rot_new; // per node {sin, cos}: inverse previous rotation, new rotation
     const double *coef_k;            // [5][nf][nxy]: the Fourier coefficients, node index fastest
     const double *cx, *cy;           // nd: the stencil's unrotated directions
     const IgRow *ig_rows;            // ng: the interpolation grid
@@ -355,6 +357,11 @@ void launch_moments_from_I64(const double *I, int64_t nxy, int nd, const double 
 void launch_moments_from_I32(const float *J, int64_t nxy, const StateLayout &L, int nd, const double *w,
                              const double *n1, const double *n2, const float *scale, const double *ang, double *mom,
                              cudaStream_t s);
+// Per node {sin, cos} of the inverse of the previous rotation and of the new
+// rotation of an adaptive step (the reference's polynomial trigonometry,
+// evaluated once per node instead of once per gather).
+void launch_rotation_trig(int64_t nxy, const double *ang_old, const double *ang_new, double2 *rot_inv,
+                          double2 *rot_new, cudaStream_t s);
 void launch_rotation_update32(const GridDev &g, const float *mom, const double *ang_old, double *ang_new,
                               cudaStream_t s);
 void launch_zero_halo_moments32(const GridDev &g, float *mom, cudaStream_t s);

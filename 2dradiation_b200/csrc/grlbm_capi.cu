@@ -65,6 +65,7 @@ struct grlbm_ctx
     // adaptive streaming: rotation angles (ang[cur] current, ang[cur ^ 1] the
     // next), the source nodes' angles, and initialFluxAngle_IF
     DevBuf ang[2], src_ang_nodes, src_ang_vals;
+    DevBuf rot; // adaptive: per node {sin, cos} of the inverse previous and the new rotation
     int64_t nsrc_ang = 0;
     std::vector<double> flux_angle;
     DevBuf ig_rows, ia3;
@@ -299,6 +300,8 @@ int enqueue_step(grlbm_ctx *ctx, int from)
                                  ctx->src_ang_vals.as<double>(), ctx->nsrc_ang, ctx->stream);
             a.ang_old = ctx->ang[from].as<double>();
             a.ang_new = ctx->ang[from ^ 1].as<double>();
+            a.rot_inv = ctx->rot.as<double2>();
+            a.rot_new = ctx->rot.as<double2>() + ctx->gd.nxy;
             launch_step_prec_adaptive(a, ctx->dirs, curved, ctx->stream);
         }
         else
@@ -318,6 +321,8 @@ int enqueue_step(grlbm_ctx *ctx, int from)
                                  ctx->src_ang_vals.as<double>(), ctx->nsrc_ang, ctx->stream);
             a.ang_old = ctx->ang[from].as<double>();
             a.ang_new = ctx->ang[from ^ 1].as<double>();
+            a.rot_inv = ctx->rot.as<double2>();
+            a.rot_new = ctx->rot.as<double2>() + ctx->gd.nxy;
             a.coef = ctx->coef_k.as<double>();
             a.nf = ctx->ss.n;
         }
@@ -792,6 +797,7 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
             TRY(alloc(ctx, b, (size_t)nxy * sizeof(double)));
             cudaMemset(b.p, 0, b.bytes);
         }
+        TRY(alloc(ctx, ctx->rot, 2 * (size_t)nxy * sizeof(double2)));
         ctx->flux_angle.assign(nxy, 0.0);
     }
     cudaMemset(ctx->mom.p, 0, ctx->mom.bytes);

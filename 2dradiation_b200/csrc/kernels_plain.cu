@@ -192,8 +192,8 @@ __device__ __forceinline__ void fourier_values5(const double *coef, int64_t fs, 
 // grid, blended and clamped at zero.
 __device__ __forceinline__ double intensity_at(const PlainStepArgs &a, int64_t n, double v1, double v2)
 {
-    const double th = fmod(-a.ang_old[n] + 2.0 * kPi, 2.0 * kPi); // RotationMatrix(angle).Inverse()
-    const double sn = approx_sin(th), cs = approx_cos(th);
+    const double2 rinv = a.rot_inv[n]; // RotationMatrix(angle).Inverse()
+    const double sn = rinv.x, cs = rinv.y;
     const double w1 = v1 * cs - v2 * sn, w2 = v1 * sn + v2 * cs;
     double dd = (double)a.ng * approx_phi(w1, w2) / (2.0 * kPi); // InterpolationGrid::d
     dd = dd < 1e-8 ? 1e-8 : ((double)a.ng - 1e-8 < dd ? (double)a.ng - 1e-8 : dd);
@@ -218,9 +218,12 @@ __device__ __forceinline__ double intensity_at(const PlainStepArgs &a, int64_t n
 // One stream value of adaptive streaming: StreamFlatAdaptive
 // (src/Radiation.cpp:415-452) or StreamCurvedAdaptive (:513-575), for the
 // cell's direction d rotated by the cell's new angle (sine sc, cosine cc).
+// Curved streaming reads coefficient k of series q of the cell at
+// cf[q * qs + k * ks].
 template <bool CURVED>
 __device__ __forceinline__ double stream_value_adaptive(const PlainStepArgs &a, int d, int64_t i, int64_t j,
-                                                        int64_t ij, double sc, double cc)
+                                                        int64_t ij, double sc, double cc, const double *cf,
+                                                        int qs, int ks)
 {
     const int64_t nx = a.g.nx;
     const double cx = __ldg(a.cx + d), cy = __ldg(a.cy + d);
@@ -229,10 +232,8 @@ __device__ __forceinline__ double stream_value_adaptive(const PlainStepArgs &a, 
     if constexpr (CURVED)
     {
         const double phi = approx_phi(dir1, dir2);
-        // coefficients k of neighbouring nodes side by side: coalesced loads
-        const int64_t fs = a.g.nxy * a.nf;
         double fv[5];
-        fourier_values5(a.coef + ij, fs, a.g.nxy, a.nf, phi, fv);
+        fourier_values5(cf, qs, ks, a.nf, phi, fv);
         const double sh = fv[0], xt = fv[1], yt = fv[2];
         v1 = fv[3];
         v2 = fv[4];
@@ -444,8 +445,8 @@ __global__ void __launch_bounds__(kStepBlock, GRLBM_STREAM_MIN_BLOCKS) k_stream_
         if constexpr (ADAPTIVE)
         {
             // the cell's rotation (RotationMatrix(rotationAngle[ij]), src/DataTypes.hh:630-635)
-            const double th = a.ang_new[ij];
-            val = stream_value_adaptive<CURVED>(a, d, i, j, ij, approx_sin(th), approx_cos(th));
+            const double2 rn = a.rot_new[ij];
+            val = stream_value_adaptive<CURVED>(a, d, i, j, ij, rn.x, rn.y, nullptr, 0, 0);
         }
         else
         {
@@ -455,6 +456,42 @@ __global__ void __launch_bounds__(kStepBlock, GRLBM_STREAM_MIN_BLOCKS) k_stream_
     }
     if (RECORD)
         rec.clamp[(int64_t)d * a.g.ncell + cc] = (uint8_t)cm;
+    a.S[(int64_t)d * a.g.nxy + ij] = val;
+}
+
+// Curved adaptive stream: a block takes 16 cells of one row for kPDirs
+// directions.  It first stages the row's Fourier coefficients (5 nF x 16
+// doubles, at most 40 KB) in shared memory, where its directions share
+// them; each warp then covers 16 cells x 2 directions.
+constexpr int kPDirs = kStepBlock / kSplitTileX;
+__global__ void __launch_bounds__(kStepBlock) k_stream_plain_curved_adaptive(PlainStepArgs a)
+{
+    extern __shared__ double sco[]; // [q * nF + k][cell]
+    // blockIdx.x: direction group fastest, then the row; blockIdx.y: the run of 16 cells
+    const int ndg = (a.nd + kPDirs - 1) / kPDirs;
+    const int t = threadIdx.x, c = t % kSplitTileX;
+    const int d = (int)(blockIdx.x % (unsigned)ndg) * kPDirs + t / kSplitTileX;
+    const int x0 = 1 + (int)blockIdx.y * kSplitTileX, i = x0 + c;
+    const int j = (int)a.g.jlo + (int)(blockIdx.x / (unsigned)ndg);
+    const int nrow = min(kSplitTileX, (int)a.g.nx_ + 1 - x0);
+    const int64_t row0 = (int64_t)x0 + (int64_t)j * a.g.nx;
+    // coefficient k of series q of node ij sits at coef[(q nF + k) nxy + ij]
+    for (int e = t; e < 5 * a.nf * kSplitTileX; e += kStepBlock)
+    {
+        const int p = e / kSplitTileX, cc = e % kSplitTileX;
+        sco[e] = cc < nrow ? a.coef[(int64_t)p * a.g.nxy + row0 + cc] : 0.0;
+    }
+    __syncthreads();
+    if (c >= nrow || d >= a.nd)
+        return;
+    const int64_t ij = row0 + c;
+    double val = 0.0;
+    if (!(a.flags[ij] & 2))
+    {
+        // the cell's rotation (RotationMatrix(rotationAngle[ij]), src/DataTypes.hh:630-635)
+        const double2 rn = a.rot_new[ij];
+        val = stream_value_adaptive<true>(a, d, i, j, ij, rn.x, rn.y, sco + c, a.nf * kSplitTileX, kSplitTileX);
+    }
     a.S[(int64_t)d * a.g.nxy + ij] = val;
 }
 
@@ -490,9 +527,9 @@ __global__ void __launch_bounds__(kStepBlock) k_collide_plain(PlainStepArgs a, S
     double rot_s = 0.0, rot_c = 1.0;
     if (ADAPTIVE)
     {
-        const double th = a.ang_new[ij];
-        rot_s = approx_sin(th);
-        rot_c = approx_cos(th);
+        const double2 rn = a.rot_new[ij];
+        rot_s = rn.x;
+        rot_c = rn.y;
     }
     const double *S = a.S + ij;
     double *col = dyn + 3 * a.nd + t; // COLUMN: this cell's values, stride NT
@@ -541,6 +578,22 @@ __global__ void k_rotation_update(GridDev g, const T *mom, const double *ang_old
     const double norm = sqrt(fx * fx + fy * fy);
     const double E = (double)mom[ij];
     ang_new[ij] = (E > 1e-16 && norm / E > 0.01) ? approx_phi(fx, fy) : ang_old[ij];
+}
+
+// The rotations an adaptive step reads at every node: the inverse of the
+// previous one (RotationMatrix(angle).Inverse(), src/DataTypes.hh:625-635,
+// as IntensityAt uses it at each corner) and the new one (the cell's own
+// stencil), as {sin, cos}.
+__global__ void k_rotation_trig(int64_t nxy, const double *ang_old, const double *ang_new, double2 *rot_inv,
+                                double2 *rot_new)
+{
+    const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= nxy)
+        return;
+    const double th = fmod(-ang_old[n] + 2.0 * kPi, 2.0 * kPi);
+    rot_inv[n] = make_double2(approx_sin(th), approx_cos(th));
+    const double tn = ang_new[n];
+    rot_new[n] = make_double2(approx_sin(tn), approx_cos(tn));
 }
 
 // The moments at the halo nodes, which the reference recomputes after every
@@ -790,12 +843,18 @@ void launch_step_plain(const PlainStepArgs &a, bool curved, cudaStream_t s, cons
     const unsigned tx = nblk(a.g.nx_, kSplitTileX), ty = nblk(a.g.jhi - a.g.jlo, kSplitTileY);
     const dim3 sgrid(tx, ty, (unsigned)a.nd), sgrid_df((unsigned)a.nd, tx, ty), cgrid(tx, ty);
     if (adaptive) // UpdateRotationMatrizes from the previous moments, before the stream
+    {
         k_rotation_update<double><<<nblk(cells, 128), 128, 0, s>>>(a.g, a.mom, a.ang_old, const_cast<double *>(a.ang_new));
+        launch_rotation_trig(a.g.nxy, a.ang_old, a.ang_new, const_cast<double2 *>(a.rot_inv),
+                             const_cast<double2 *>(a.rot_new), s);
+    }
     // stream
     const dim3 ga = kDirFastestAdaptive ? sgrid_df : sgrid, gf = kDirFastestFixed ? sgrid_df : sgrid;
-    if (adaptive)
-        curved ? k_stream_plain<true, false, true><<<ga, kStepBlock, 0, s>>>(a, rec)
-               : k_stream_plain<false, false, true><<<ga, kStepBlock, 0, s>>>(a, rec);
+    if (adaptive && curved)
+        k_stream_plain_curved_adaptive<<<dim3(nblk(a.nd, kPDirs) * (unsigned)(a.g.jhi - a.g.jlo), tx), kStepBlock,
+                                         (size_t)5 * a.nf * kSplitTileX * sizeof(double), s>>>(a);
+    else if (adaptive)
+        k_stream_plain<false, false, true><<<ga, kStepBlock, 0, s>>>(a, rec);
     else if (curved)
         record ? k_stream_plain<true, true, false><<<gf, kStepBlock, 0, s>>>(a, rec)
                : k_stream_plain<true, false, false><<<gf, kStepBlock, 0, s>>>(a, rec);
@@ -838,6 +897,11 @@ void launch_sources32(float *I, const StateLayout &L, int nd, const int64_t *nod
 void launch_coef_k_major(const double *coef, double *coef_k, int64_t nxy, int nf, cudaStream_t s)
 {
     k_coef_k_major<<<nblk(5 * nxy * nf, 256), 256, 0, s>>>(coef, coef_k, nxy, nf);
+}
+void launch_rotation_trig(int64_t nxy, const double *ang_old, const double *ang_new, double2 *rot_inv,
+                          double2 *rot_new, cudaStream_t s)
+{
+    k_rotation_trig<<<nblk(nxy, 256), 256, 0, s>>>(nxy, ang_old, ang_new, rot_inv, rot_new);
 }
 // UpdateRotationMatrizes before, and the halo moments after, an adaptive
 // precision-form step (FP32 moments)

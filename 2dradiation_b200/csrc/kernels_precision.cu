@@ -633,7 +633,41 @@ __global__ void __launch_bounds__(kStepBlock, GRLBM_PREC_MIN_BLOCKS)
 // collides.  FP32 arithmetic, FP32 state (J = I / alpha^3 for curved
 // streaming); the Fourier series sum in FP64 over an FP32 basis.
 constexpr int kATileX = 16, kATileY = kStepBlock / kATileX;
-constexpr float kTwoPiF = 6.28318530717958647692f;
+
+// The reference's polynomial atan2 and Phi (MyAtan2<9>, Tensor2::Phi;
+// src/Utility.hh:179-254, src/DataTypes.hh:166-170) evaluated in FP32, in
+// grid-row units: nGrid * Phi(x, y) / (2 pi).  The same octants and
+// polynomial as approx_phi; the FP32 rounding adds an error of the order of
+// the FP32 rounding of the row coordinate itself.
+__device__ __forceinline__ float atan_poly9_f(float z)
+{
+    const float zz = z * z;
+    return z * (0.9998660f + zz * (-0.3302995f + zz * (0.1801410f + zz * (-0.0851330f + zz * 0.0208351f))));
+}
+__device__ __forceinline__ float grid_row_of(float x, float y, float rows_per_rad)
+{
+    const float pi = 3.14159265358979f, half_pi = 1.57079632679490f;
+    float p;
+    if (x != 0.f)
+    {
+        if (fabsf(x) > fabsf(y))
+        {
+            p = atan_poly9_f(y / x);
+            if (x < 0.f)
+                p = (y >= 0.f) ? p + pi : p - pi;
+        }
+        else
+        {
+            const float q = atan_poly9_f(x / y);
+            p = (y > 0.f) ? half_pi - q : -q - half_pi;
+        }
+    }
+    else
+        p = y > 0.f ? half_pi : (y < 0.f ? -half_pi : 0.f);
+    if (p < 0.f)
+        p += 2.f * pi;
+    return p * rows_per_rad;
+}
 
 // IntensityAt (src/Radiation.cpp:322-343) on the FP32 state: the direction
 // (v1, v2) rotated into node n's previous frame, the two cubic rows of the
@@ -642,11 +676,11 @@ constexpr float kTwoPiF = 6.28318530717958647692f;
 __device__ __forceinline__ float intensity_at32(const PrecStepArgs &a, int n, unsigned sidx, float v1, float v2)
 {
     // the inverse of the node's previous rotation, with the reference's
-    // polynomial trigonometry (as the plain form)
-    const double th = fmod(-a.ang_old[n] + 2.0 * kPi, 2.0 * kPi);
-    const float sn = (float)approx_sin(th), cs = (float)approx_cos(th);
+    // polynomial trigonometry (the plain form's values)
+    const double2 rinv = a.rot_inv[n];
+    const float sn = (float)rinv.x, cs = (float)rinv.y;
     const float w1 = v1 * cs - v2 * sn, w2 = v1 * sn + v2 * cs;
-    float dd = (float)((double)a.ng * approx_phi((double)w1, (double)w2) / (2.0 * kPi));
+    float dd = grid_row_of(w1, w2, (float)a.ng * 0.159154943091895f);
     dd = fminf(fmaxf(dd, 1e-8f), nextafterf((float)a.ng, 0.f)); // InterpolationGrid's clamp, in FP32
     const int g0 = min((int)dd, a.ng - 1), g1 = g0 + 1 == a.ng ? 0 : g0 + 1;
     const float t = dd - (float)g0;
@@ -666,13 +700,15 @@ __device__ __forceinline__ float intensity_at32(const PrecStepArgs &a, int n, un
 }
 
 // One adaptive stream value (I, not J) of cell (i, j) for its direction d
-// rotated by the cell's new angle.
+// rotated by the cell's new angle.  Curved streaming reads coefficient k of
+// series q of the cell at cf[q * qs + k * ks].
 template <bool CURVED>
-__device__ __forceinline__ float stream_adaptive32(const PrecStepArgs &a, int d, int i, int j, int ij)
+__device__ __forceinline__ float stream_adaptive32(const PrecStepArgs &a, int d, int i, int j, int ij,
+                                                   const double *cf, int ks, int qs)
 {
     const int nx = (int)a.g.nx;
-    const double th = a.ang_new[ij];
-    const float sc = (float)approx_sin(th), cc = (float)approx_cos(th);
+    const double2 rn = a.rot_new[ij];
+    const float sc = (float)rn.x, cc = (float)rn.y;
     const float cxd = (float)a.cx[d], cyd = (float)a.cy[d];
     const float dir1 = cxd * cc - cyd * sc, dir2 = cxd * sc + cyd * cc;
     float it, jt, v1, v2, s3 = 1.f;
@@ -681,15 +717,13 @@ __device__ __forceinline__ float stream_adaptive32(const PrecStepArgs &a, int d,
         // the five series (S, X, Y, Cx, Cy) at the direction's angle: basis
         // {1, sqrt2 cos(m phi), sqrt2 sin(m phi)} from one sincos and the
         // angle-addition recurrence
-        const float phi = (float)approx_phi((double)dir1, (double)dir2);
+        const float phi = grid_row_of(dir1, dir2, 1.f);
         float s1, c1;
         sincosf(phi, &s1, &c1);
-        const int64_t fs = a.g.nxy * a.nf;
-        const double *cf = a.coef_k + ij;
         double r[5];
 #pragma unroll
         for (int q = 0; q < 5; q++)
-            r[q] = cf[q * fs];
+            r[q] = cf[q * qs];
         float cm = 1.f, sm = 0.f;
         const float sqrt2 = 1.41421356237f;
         for (int k = 1; k < a.nf; k++)
@@ -701,10 +735,10 @@ __device__ __forceinline__ float stream_adaptive32(const PrecStepArgs &a, int d,
                 cm = c2;
             }
             const double b = (double)(sqrt2 * ((k & 1) ? cm : sm));
-            const double *ck = cf + (int64_t)k * a.g.nxy;
+            const double *ck = cf + k * ks;
 #pragma unroll
             for (int q = 0; q < 5; q++)
-                r[q] = fma(ck[q * fs], b, r[q]);
+                r[q] = fma(ck[q * qs], b, r[q]);
         }
         const double xt = r[1], yt = r[2];
         if (dev_inside_bh(a.g, xt, yt))
@@ -740,10 +774,9 @@ __device__ __forceinline__ float stream_adaptive32(const PrecStepArgs &a, int d,
     return CURVED ? s3 * bil / a.ia3[ij] : bil;
 }
 
-// Stream: blocks are 16 x 8 tiles of cells of one direction, directions
-// fastest in the grid (the blocks of one tile share its coefficients).
-template <bool CURVED>
-__global__ void __launch_bounds__(kStepBlock) k_stream_prec_adaptive(PrecStepArgs a)
+// Flat stream: blocks are 16 x 8 tiles of cells of one direction,
+// directions fastest in the grid.
+__global__ void __launch_bounds__(kStepBlock) k_stream_prec_adaptive_flat(PrecStepArgs a)
 {
     const int d = blockIdx.x;
     const int i = 1 + (int)blockIdx.y * kATileX + (int)(threadIdx.x % kATileX);
@@ -751,9 +784,38 @@ __global__ void __launch_bounds__(kStepBlock) k_stream_prec_adaptive(PrecStepArg
     if (i > a.g.nx_ || j >= a.g.jhi)
         return;
     const int ij = i + j * (int)a.g.nx;
+    a.S[(size_t)d * (size_t)a.g.nxy + (size_t)ij] = stream_adaptive32<false>(a, d, i, j, ij, nullptr, 0, 0);
+}
+
+// Curved stream: a block takes 16 cells of one row for kADirs directions.
+// It first stages the row's Fourier coefficients (5 nF x 16 doubles, at most
+// 40 KB) in shared memory, where its directions share them; each warp then
+// covers 16 cells x 2 directions, so a tap load reads two 16-node runs.
+constexpr int kADirs = kStepBlock / kATileX;
+__global__ void __launch_bounds__(kStepBlock) k_stream_prec_adaptive_curved(PrecStepArgs a)
+{
+    extern __shared__ double sco[]; // [q * nF + k][cell]
+    // blockIdx.x: direction group fastest, then the row; blockIdx.y: the run of 16 cells
+    const int ndg = (a.nd + kADirs - 1) / kADirs;
+    const int t = threadIdx.x, c = t % kATileX;
+    const int d = (int)(blockIdx.x % (unsigned)ndg) * kADirs + t / kATileX;
+    const int x0 = 1 + (int)blockIdx.y * kATileX, i = x0 + c;
+    const int j = (int)a.g.jlo + (int)(blockIdx.x / (unsigned)ndg);
+    const int nrow = min(kATileX, (int)a.g.nx_ + 1 - x0);
+    const int row0 = x0 + j * (int)a.g.nx;
+    // coefficient k of series q of node ij sits at coef_k[(q nF + k) nxy + ij]
+    for (int e = t; e < 5 * a.nf * kATileX; e += kStepBlock)
+    {
+        const int p = e / kATileX, cc = e % kATileX;
+        sco[e] = cc < nrow ? a.coef_k[(size_t)p * (size_t)a.g.nxy + (size_t)(row0 + cc)] : 0.0;
+    }
+    __syncthreads();
+    if (c >= nrow || d >= a.nd)
+        return;
+    const int ij = row0 + c;
     float v = 0.f;
-    if (!(CURVED && (a.flags[ij] & 2)))
-        v = stream_adaptive32<CURVED>(a, d, i, j, ij);
+    if (!(a.flags[ij] & 2))
+        v = stream_adaptive32<true>(a, d, i, j, ij, sco + c, kATileX, a.nf * kATileX);
     a.S[(size_t)d * (size_t)a.g.nxy + (size_t)ij] = v;
 }
 
@@ -778,7 +840,8 @@ __global__ void __launch_bounds__(kStepBlock) k_collide_prec_adaptive(PrecStepAr
     for (int d = threadIdx.x; d < a.nd; d += kStepBlock)
         sw[d] = dt.w[d], scx[d] = (float)a.cx[d], scy[d] = (float)a.cy[d];
     __syncthreads();
-    const float rs = (float)approx_sin(a.ang_new[ij]), rc = (float)approx_cos(a.ang_new[ij]);
+    const double2 rn = a.rot_new[ij];
+    const float rs = (float)rn.x, rc = (float)rn.y;
 #define GRLBM_RN1(d) (scx[d] * rc - scy[d] * rs)
 #define GRLBM_RN2(d) (scx[d] * rs + scy[d] * rc)
     KMoments km;
@@ -1012,15 +1075,19 @@ void launch_step_prec_adaptive(const PrecStepArgs &a, const DirTable &dt, bool c
     const unsigned tx = nblk(a.g.nx_, kATileX), ty = nblk(rows, kATileY);
     // UpdateRotationMatrizes from the previous moments, before the stream
     launch_rotation_update32(a.g, a.mom, a.ang_old, const_cast<double *>(a.ang_new), s);
-    const dim3 sgrid((unsigned)a.nd, tx, ty), cgrid(tx, ty);
+    launch_rotation_trig(a.g.nxy, a.ang_old, a.ang_new, const_cast<double2 *>(a.rot_inv),
+                         const_cast<double2 *>(a.rot_new), s);
+    const dim3 cgrid(tx, ty);
     if (curved)
     {
-        k_stream_prec_adaptive<true><<<sgrid, kStepBlock, 0, s>>>(a);
+        const dim3 sgrid(nblk(a.nd, kADirs) * (unsigned)rows, tx);
+        const size_t coef_bytes = (size_t)5 * a.nf * kATileX * sizeof(double);
+        k_stream_prec_adaptive_curved<<<sgrid, kStepBlock, coef_bytes, s>>>(a);
         k_collide_prec_adaptive<true><<<cgrid, kStepBlock, 0, s>>>(a, dt);
     }
     else
     {
-        k_stream_prec_adaptive<false><<<sgrid, kStepBlock, 0, s>>>(a);
+        k_stream_prec_adaptive_flat<<<dim3((unsigned)a.nd, tx, ty), kStepBlock, 0, s>>>(a);
         k_collide_prec_adaptive<false><<<cgrid, kStepBlock, 0, s>>>(a, dt);
     }
     // the halo moments, which the reference recomputes from unwritten (zero) intensities
