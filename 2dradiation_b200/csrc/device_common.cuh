@@ -172,6 +172,12 @@ struct __align__(16) IgRow
     int4 idx;
     double2 w01, w23;
 };
+// The same with the weights rounded to FP32 (the precision form).
+struct __align__(16) IgRow32
+{
+    int4 idx;
+    float4 w;
+};
 
 struct PlainStepArgs
 {
@@ -219,9 +225,12 @@ struct PrecStepArgs
     // adaptive streaming only (null otherwise)
     const double *ang_old, *ang_new; // rotation angles before and after this step's update (nxy)
     const double2 *rot_inv, *rot_new; // per node {sin, cos}: inverse previous rotation, new rotation
-    const double *coef_k;            // [5][nf][nxy]: the Fourier coefficients, node index fastest
+    // [5][nf][nxy]: the Fourier coefficients in FP32, node index fastest, with
+    // the X and Y series taken about the node (its coordinates subtracted)
+    const float *coef32;
+    float inv_dx, inv_dy;            // 1 / dx, 1 / dy
     const double *cx, *cy;           // nd: the stencil's unrotated directions
-    const IgRow *ig_rows;            // ng: the interpolation grid
+    const IgRow32 *ig_rows;          // ng: the interpolation grid
     float *S;                        // [d * nxy + ij]: the streamed values of the step
     int nf;
 };
@@ -362,6 +371,10 @@ void launch_moments_from_I32(const float *J, int64_t nxy, const StateLayout &L, 
 // evaluated once per node instead of once per gather).
 void launch_rotation_trig(int64_t nxy, const double *ang_old, const double *ang_new, double2 *rot_inv,
                           double2 *rot_new, cudaStream_t s);
+// The FP32 coefficient copy of adaptive streaming in the precision form:
+// coef [5][nxy][nf] (FP64) to [5][nf][nxy] (FP32), the node's x and y
+// subtracted from the constant terms of the X and Y series in FP64 first.
+void launch_coef_about_node32(const GridDev &g, const double *coef, float *coef32, int nf, cudaStream_t s);
 void launch_rotation_update32(const GridDev &g, const float *mom, const double *ang_old, double *ang_new,
                               cudaStream_t s);
 void launch_zero_halo_moments32(const GridDev &g, float *mom, cudaStream_t s);

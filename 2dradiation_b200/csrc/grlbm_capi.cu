@@ -69,6 +69,7 @@ struct grlbm_ctx
     int64_t nsrc_ang = 0;
     std::vector<double> flux_angle;
     DevBuf ig_rows, ia3;
+    DevBuf coef32; // adaptive streaming in the precision form: FP32 coefficients, X and Y about the node
     DevBuf streamed; // plain form: the streamed values of a step
     DevBuf coef_k;   // adaptive streaming: the coefficients as [5][nf][nxy]
     DirTable dirs{}; // precision-form direction tables (kernel parameter)
@@ -228,10 +229,12 @@ PrecStepArgs prec_args(grlbm_ctx *ctx, int from)
     a.fault = ctx->fault;
     a.in_map = ctx->in_map[from];
     // adaptive streaming (the angles are set per step)
-    a.coef_k = ctx->coef_k.as<double>();
+    a.coef32 = ctx->coef32.as<float>();
+    a.inv_dx = (float)(1.0 / ctx->gd.dx);
+    a.inv_dy = (float)(1.0 / ctx->gd.dy);
     a.cx = ctx->cx.as<double>();
     a.cy = ctx->cy.as<double>();
-    a.ig_rows = ctx->ig_rows.as<IgRow>();
+    a.ig_rows = ctx->ig_rows.as<IgRow32>();
     a.S = ctx->streamed.as<float>();
     a.nf = ctx->ss.n;
     return a;
@@ -384,11 +387,24 @@ int build_records(grlbm_ctx *ctx)
     if (is_adaptive(ctx))
     {
         // adaptive streaming evaluates the series at run time: a copy with
-        // the coefficients of neighbouring nodes side by side
-        int rc = alloc(ctx, ctx->coef_k, ctx->coef.bytes);
-        if (rc)
-            return rc;
-        launch_coef_k_major(ctx->coef.as<double>(), ctx->coef_k.as<double>(), ctx->gd.nxy, ctx->ss.n, ctx->stream);
+        // the coefficients of neighbouring nodes side by side (FP32, X and Y
+        // about the node, for the precision form)
+        if (ctx->fp32)
+        {
+            int rc = alloc(ctx, ctx->coef32, ctx->coef.bytes / 2);
+            if (rc)
+                return rc;
+            launch_coef_about_node32(ctx->gd, ctx->coef.as<double>(), ctx->coef32.as<float>(), ctx->ss.n,
+                                     ctx->stream);
+        }
+        else
+        {
+            int rc = alloc(ctx, ctx->coef_k, ctx->coef.bytes);
+            if (rc)
+                return rc;
+            launch_coef_k_major(ctx->coef.as<double>(), ctx->coef_k.as<double>(), ctx->gd.nxy, ctx->ss.n,
+                                ctx->stream);
+        }
     }
     CU(cudaGetLastError());
     return GRLBM_OK;
@@ -689,7 +705,7 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
     }
     // the interpolation grid's rows: the plain form's stream, and adaptive
     // streaming in either form
-    if (!ctx->fp32 || is_adaptive(ctx))
+    if (!ctx->fp32)
     {
         std::vector<IgRow> rows(ctx->ng);
         for (int g = 0; g < ctx->ng; g++)
@@ -699,6 +715,18 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
             rows[g].idx = make_int4((int)x[0], (int)x[1], (int)x[2], (int)x[3]);
             rows[g].w01 = make_double2(w[0], w[1]);
             rows[g].w23 = make_double2(w[2], w[3]);
+        }
+        TRY(upload(ctx, ctx->ig_rows, rows));
+    }
+    else if (is_adaptive(ctx))
+    {
+        std::vector<IgRow32> rows(ctx->ng);
+        for (int g = 0; g < ctx->ng; g++)
+        {
+            const int64_t *x = &ctx->st.ig_index[4 * g];
+            const double *w = &ctx->st.ig_weight[4 * g];
+            rows[g].idx = make_int4((int)x[0], (int)x[1], (int)x[2], (int)x[3]);
+            rows[g].w = make_float4((float)w[0], (float)w[1], (float)w[2], (float)w[3]);
         }
         TRY(upload(ctx, ctx->ig_rows, rows));
     }

@@ -684,11 +684,11 @@ __device__ __forceinline__ float intensity_at32(const PrecStepArgs &a, int n, un
     dd = fminf(fmaxf(dd, 1e-8f), nextafterf((float)a.ng, 0.f)); // InterpolationGrid's clamp, in FP32
     const int g0 = min((int)dd, a.ng - 1), g1 = g0 + 1 == a.ng ? 0 : g0 + 1;
     const float t = dd - (float)g0;
-    const IgRow R0 = a.ig_rows[g0], R1 = a.ig_rows[g1];
+    const IgRow32 R0 = a.ig_rows[g0], R1 = a.ig_rows[g1];
     const int idx0[4] = {R0.idx.x, R0.idx.y, R0.idx.z, R0.idx.w};
     const int idx1[4] = {R1.idx.x, R1.idx.y, R1.idx.z, R1.idx.w};
-    const float wa[4] = {(float)R0.w01.x, (float)R0.w01.y, (float)R0.w23.x, (float)R0.w23.y};
-    const float wb[4] = {(float)R1.w01.x, (float)R1.w01.y, (float)R1.w23.x, (float)R1.w23.y};
+    const float wa[4] = {R0.w.x, R0.w.y, R0.w.z, R0.w.w};
+    const float wb[4] = {R1.w.x, R1.w.y, R1.w.z, R1.w.w};
     float x0 = 0.f, x1 = 0.f;
 #pragma unroll
     for (int k = 0; k < 4; k++)
@@ -701,10 +701,10 @@ __device__ __forceinline__ float intensity_at32(const PrecStepArgs &a, int n, un
 
 // One adaptive stream value (I, not J) of cell (i, j) for its direction d
 // rotated by the cell's new angle.  Curved streaming reads coefficient k of
-// series q of the cell at cf[q * qs + k * ks].
+// series q of the cell at cf[q * qs + k * ks] (FP32, X and Y about the node).
 template <bool CURVED>
 __device__ __forceinline__ float stream_adaptive32(const PrecStepArgs &a, int d, int i, int j, int ij,
-                                                   const double *cf, int ks, int qs)
+                                                   const float *cf, int ks, int qs)
 {
     const int nx = (int)a.g.nx;
     const double2 rn = a.rot_new[ij];
@@ -714,13 +714,13 @@ __device__ __forceinline__ float stream_adaptive32(const PrecStepArgs &a, int d,
     float it, jt, v1, v2, s3 = 1.f;
     if constexpr (CURVED)
     {
-        // the five series (S, X, Y, Cx, Cy) at the direction's angle: basis
-        // {1, sqrt2 cos(m phi), sqrt2 sin(m phi)} from one sincos and the
-        // angle-addition recurrence
+        // the five series (S, X - x, Y - y, Cx, Cy) at the direction's angle:
+        // basis {1, sqrt2 cos(m phi), sqrt2 sin(m phi)} from one sincos and
+        // the angle-addition recurrence
         const float phi = grid_row_of(dir1, dir2, 1.f);
         float s1, c1;
         sincosf(phi, &s1, &c1);
-        double r[5];
+        float r[5];
 #pragma unroll
         for (int q = 0; q < 5; q++)
             r[q] = cf[q * qs];
@@ -734,21 +734,23 @@ __device__ __forceinline__ float stream_adaptive32(const PrecStepArgs &a, int d,
                 sm = sm * c1 + cm * s1;
                 cm = c2;
             }
-            const double b = (double)(sqrt2 * ((k & 1) ? cm : sm));
-            const double *ck = cf + k * ks;
+            const float b = sqrt2 * ((k & 1) ? cm : sm);
+            const float *ck = cf + k * ks;
 #pragma unroll
             for (int q = 0; q < 5; q++)
-                r[q] = fma(ck[q * qs], b, r[q]);
+                r[q] = fmaf(ck[q * qs], b, r[q]);
         }
-        const double xt = r[1], yt = r[2];
+        // the departure point, absolute for the excision test
+        const double xt = a.g.startx + (double)i * a.g.dx + (double)r[1];
+        const double yt = a.g.starty + (double)j * a.g.dy + (double)r[2];
         if (dev_inside_bh(a.g, xt, yt))
             return 0.f;
-        it = (float)((xt - a.g.startx) / a.g.dx);
-        jt = (float)((yt - a.g.starty) / a.g.dy);
-        const float sh = (float)r[0];
+        it = (float)i + r[1] * a.inv_dx;
+        jt = (float)j + r[2] * a.inv_dy;
+        const float sh = r[0];
         s3 = sh * sh * sh;
-        v1 = (float)r[3];
-        v2 = (float)r[4];
+        v1 = r[3];
+        v2 = r[4];
     }
     else
     {
@@ -788,13 +790,13 @@ __global__ void __launch_bounds__(kStepBlock) k_stream_prec_adaptive_flat(PrecSt
 }
 
 // Curved stream: a block takes 16 cells of one row for kADirs directions.
-// It first stages the row's Fourier coefficients (5 nF x 16 doubles, at most
-// 40 KB) in shared memory, where its directions share them; each warp then
+// It first stages the row's Fourier coefficients (5 nF x 16 floats, at most
+// 20 KB) in shared memory, where its directions share them; each warp then
 // covers 16 cells x 2 directions, so a tap load reads two 16-node runs.
 constexpr int kADirs = kStepBlock / kATileX;
 __global__ void __launch_bounds__(kStepBlock) k_stream_prec_adaptive_curved(PrecStepArgs a)
 {
-    extern __shared__ double sco[]; // [q * nF + k][cell]
+    extern __shared__ float sco[]; // [q * nF + k][cell]
     // blockIdx.x: direction group fastest, then the row; blockIdx.y: the run of 16 cells
     const int ndg = (a.nd + kADirs - 1) / kADirs;
     const int t = threadIdx.x, c = t % kATileX;
@@ -803,11 +805,11 @@ __global__ void __launch_bounds__(kStepBlock) k_stream_prec_adaptive_curved(Prec
     const int j = (int)a.g.jlo + (int)(blockIdx.x / (unsigned)ndg);
     const int nrow = min(kATileX, (int)a.g.nx_ + 1 - x0);
     const int row0 = x0 + j * (int)a.g.nx;
-    // coefficient k of series q of node ij sits at coef_k[(q nF + k) nxy + ij]
+    // coefficient k of series q of node ij sits at coef32[(q nF + k) nxy + ij]
     for (int e = t; e < 5 * a.nf * kATileX; e += kStepBlock)
     {
         const int p = e / kATileX, cc = e % kATileX;
-        sco[e] = cc < nrow ? a.coef_k[(size_t)p * (size_t)a.g.nxy + (size_t)(row0 + cc)] : 0.0;
+        sco[e] = cc < nrow ? a.coef32[(size_t)p * (size_t)a.g.nxy + (size_t)(row0 + cc)] : 0.f;
     }
     __syncthreads();
     if (c >= nrow || d >= a.nd)
@@ -1067,6 +1069,26 @@ cudaError_t prepare_step_prec(int)
         return e;
     return cudaFuncSetAttribute(k_step_prec<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
 }
+__global__ void k_coef_about_node32(GridDev g, const double *coef, float *coef32, int nf)
+{
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t per = g.nxy * nf;
+    if (t >= 5 * per)
+        return;
+    const int64_t q = t / per, r = t - q * per; // r = k * nxy + ij
+    const int64_t k = r / g.nxy, ij = r - k * g.nxy;
+    double v = coef[q * per + ij * nf + k];
+    if (k == 0 && q == 1)
+        v -= g.startx + (double)(ij % g.nx) * g.dx;
+    else if (k == 0 && q == 2)
+        v -= g.starty + (double)(ij / g.nx) * g.dy;
+    coef32[t] = (float)v;
+}
+void launch_coef_about_node32(const GridDev &g, const double *coef, float *coef32, int nf, cudaStream_t s)
+{
+    k_coef_about_node32<<<nblk(5 * g.nxy * nf, 256), 256, 0, s>>>(g, coef, coef32, nf);
+}
+
 void launch_step_prec_adaptive(const PrecStepArgs &a, const DirTable &dt, bool curved, cudaStream_t s)
 {
     const int64_t rows = a.g.jhi - a.g.jlo;
@@ -1081,7 +1103,7 @@ void launch_step_prec_adaptive(const PrecStepArgs &a, const DirTable &dt, bool c
     if (curved)
     {
         const dim3 sgrid(nblk(a.nd, kADirs) * (unsigned)rows, tx);
-        const size_t coef_bytes = (size_t)5 * a.nf * kATileX * sizeof(double);
+        const size_t coef_bytes = (size_t)5 * a.nf * kATileX * sizeof(float);
         k_stream_prec_adaptive_curved<<<sgrid, kStepBlock, coef_bytes, s>>>(a);
         k_collide_prec_adaptive<true><<<cgrid, kStepBlock, 0, s>>>(a, dt);
     }
