@@ -167,15 +167,21 @@ __device__ __forceinline__ void fourier_values5(const double *coef, int64_t fs, 
 {
     const double sqrt2 = 1.4142135623730951; // sqrt(2), correctly rounded
     double r0 = 0, r1 = 0, r2 = 0, r3 = 0, r4 = 0;
+    // the argument of term 2m - 1, phi * (2m - 1 + 1.0) / 2.0, and of term 2m,
+    // phi * 2m / 2.0, round alike: one sincos serves both
+    double sin_m = 0.0, cos_m = 1.0;
     for (int k = 0; k < nf; k++)
     {
         double b;
         if (k == 0)
             b = 1.0;
         else if (k % 2 != 0)
-            b = sqrt2 * cos(phi * (k + 1.0) / 2.0);
+        {
+            sincos(phi * (k + 1.0) / 2.0, &sin_m, &cos_m);
+            b = sqrt2 * cos_m;
+        }
         else
-            b = sqrt2 * sin(phi * k / 2.0);
+            b = sqrt2 * sin_m;
         const double *c = coef + k * sk;
         r0 += c[0] * b;
         r1 += c[fs] * b;
