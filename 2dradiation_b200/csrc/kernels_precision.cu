@@ -839,8 +839,29 @@ __global__ void __launch_bounds__(kStepBlock) k_collide_prec_adaptive(PrecStepAr
     const float *S = a.S + ij;
     // the cell's stencil, rotated (shared by the block's threads per direction)
     __shared__ float sw[kMaxDirs], scx[kMaxDirs], scy[kMaxDirs];
+    // the unrotated stencil's weighted moments: sum w, sum w c_a, sum w c_a c_b,
+    // sum w c_a c_b c_c (a <= b <= c)
+    __shared__ float smom[10];
     for (int d = threadIdx.x; d < a.nd; d += kStepBlock)
         sw[d] = dt.w[d], scx[d] = (float)a.cx[d], scy[d] = (float)a.cy[d];
+    __syncthreads();
+    if (threadIdx.x < 10)
+    {
+        // component t: x-powers px, y-powers py of w c_x^px c_y^py
+        constexpr int px[10] = {0, 1, 0, 2, 1, 0, 3, 2, 1, 0}, py[10] = {0, 0, 1, 0, 1, 2, 0, 1, 2, 3};
+        const int t = threadIdx.x;
+        float s = 0.f;
+        for (int d = 0; d < a.nd; d++)
+        {
+            float v = sw[d];
+            for (int p = 0; p < px[t]; p++)
+                v *= scx[d];
+            for (int p = 0; p < py[t]; p++)
+                v *= scy[d];
+            s += v;
+        }
+        smom[t] = s;
+    }
     __syncthreads();
     const double2 rn = a.rot_new[ij];
     const float rs = (float)rn.x, rc = (float)rn.y;
@@ -850,12 +871,20 @@ __global__ void __launch_bounds__(kStepBlock) k_collide_prec_adaptive(PrecStepAr
     km.zero();
     for (int d0 = 0; d0 < a.nd; d0 += kChunk)
     {
-        const int dend = min(d0 + kChunk, a.nd);
-        for (int d = d0; d < dend; d++)
+        // the streamed values of a chunk, loaded together
+        float Sv[kChunk];
+#pragma unroll
+        for (int k = 0; k < kChunk; k++)
+            Sv[k] = d0 + k < a.nd ? S[(unsigned)(d0 + k) * nxy] : 0.f;
+#pragma unroll
+        for (int k = 0; k < kChunk; k++)
         {
+            const int d = d0 + k;
+            if (d >= a.nd)
+                break;
             const float n1 = GRLBM_RN1(d), n2 = GRLBM_RN2(d), w = sw[d];
             const float wn1 = w * n1, wn2 = w * n2;
-            km.add(S[(unsigned)d * nxy], make_float4(w, wn1, wn2, wn1 * n1), make_float4(wn1 * n2, wn2 * n2, n1, n2));
+            km.add(Sv[k], make_float4(w, wn1, wn2, wn1 * n1), make_float4(wn1 * n2, wn2 * n2, n1, n2));
         }
         km.fold();
     }
@@ -870,24 +899,84 @@ __global__ void __launch_bounds__(kStepBlock) k_collide_prec_adaptive(PrecStepAr
         const bool rest = (u1 == 0.f) && (u2 == 0.f);
         const float g0 = 1.f / (1.f + adt * kak0), h0 = adt * g0;
         float A6[6], B6[6], C6[6], D6[6];
-#pragma unroll
-        for (int q = 0; q < 6; q++)
-            A6[q] = B6[q] = C6[q] = D6[q] = 0.f;
-        for (int d = 0; d < a.nd; d++)
+        if (rest)
         {
-            const float n1 = GRLBM_RN1(d), n2 = GRLBM_RN2(d), w = sw[d];
-            float g = g0, h = h0, q1 = n1, q2 = n2;
-            if (!rest)
-                collide_coeffs(n1, n2, u1, u2, lor, adt, kak0, g, h, q1, q2);
-            const float mu[6] = {1.f, n1, n2, n1 * n1, n1 * n2, n2 * n2};
-            const float gs = w * g * S[(unsigned)d * nxy], wh = w * h;
+            // A = g0 m; B, C, D: h0 times the rotated stencil's weighted
+            // moments of orders 0-3, from the unrotated ones (n = R c,
+            // R = {{rc, -rs}, {rs, rc}})
+            const float R[2][2] = {{rc, -rs}, {rs, rc}};
+            const float m1[2] = {smom[1], smom[2]};
+            const float m2[2][2] = {{smom[3], smom[4]}, {smom[4], smom[5]}};
+            float m3[2][2][2];
+#pragma unroll
+            for (int x = 0; x < 2; x++)
+#pragma unroll
+                for (int y = 0; y < 2; y++)
+#pragma unroll
+                    for (int z = 0; z < 2; z++)
+                        m3[x][y][z] = smom[6 + x + y + z];
+            float r1[2], r2[2][2], r3[2][2][2];
+#pragma unroll
+            for (int p = 0; p < 2; p++)
+            {
+                r1[p] = R[p][0] * m1[0] + R[p][1] * m1[1];
+#pragma unroll
+                for (int q = 0; q < 2; q++)
+                {
+                    float s2 = 0.f;
+#pragma unroll
+                    for (int x = 0; x < 2; x++)
+#pragma unroll
+                        for (int y = 0; y < 2; y++)
+                            s2 += R[p][x] * R[q][y] * m2[x][y];
+                    r2[p][q] = s2;
+#pragma unroll
+                    for (int o = 0; o < 2; o++)
+                    {
+                        float s3 = 0.f;
+#pragma unroll
+                        for (int x = 0; x < 2; x++)
+#pragma unroll
+                            for (int y = 0; y < 2; y++)
+#pragma unroll
+                                for (int z = 0; z < 2; z++)
+                                    s3 += R[p][x] * R[q][y] * R[o][z] * m3[x][y][z];
+                        r3[p][q][o] = s3;
+                    }
+                }
+            }
+            const float b6[6] = {smom[0], r1[0], r1[1], r2[0][0], r2[0][1], r2[1][1]};
+            const float c6[6] = {r1[0], r2[0][0], r2[0][1], r3[0][0][0], r3[0][0][1], r3[0][1][1]};
+            const float d6[6] = {r1[1], r2[0][1], r2[1][1], r3[0][0][1], r3[0][1][1], r3[1][1][1]};
 #pragma unroll
             for (int q = 0; q < 6; q++)
             {
-                A6[q] += gs * mu[q];
-                B6[q] += wh * mu[q];
-                C6[q] += wh * q1 * mu[q];
-                D6[q] += wh * q2 * mu[q];
+                A6[q] = g0 * m[q];
+                B6[q] = h0 * b6[q];
+                C6[q] = h0 * c6[q];
+                D6[q] = h0 * d6[q];
+            }
+        }
+        else
+        {
+#pragma unroll
+            for (int q = 0; q < 6; q++)
+                A6[q] = B6[q] = C6[q] = D6[q] = 0.f;
+            for (int d = 0; d < a.nd; d++)
+            {
+                const float n1 = GRLBM_RN1(d), n2 = GRLBM_RN2(d), w = sw[d];
+                float g, h, q1, q2;
+                collide_coeffs(n1, n2, u1, u2, lor, adt, kak0, g, h, q1, q2);
+                const float mu[6] = {1.f, n1, n2, n1 * n1, n1 * n2, n2 * n2};
+                const float gs = w * g * S[(unsigned)d * nxy], wh = w * h;
+#pragma unroll
+                for (int q = 0; q < 6; q++)
+                {
+                    A6[q] += gs * mu[q];
+                    B6[q] += wh * mu[q];
+                    C6[q] += wh * q1 * mu[q];
+                    D6[q] += wh * q2 * mu[q];
+                }
             }
         }
         float diff = 1.f;
@@ -923,14 +1012,21 @@ __global__ void __launch_bounds__(kStepBlock) k_collide_prec_adaptive(PrecStepAr
         float *out = a.Iout + (unsigned)i + (unsigned)j * a.pitch;
         for (int d0 = 0; d0 < a.nd; d0 += kChunk)
         {
-            const int dend = min(d0 + kChunk, a.nd);
-            for (int d = d0; d < dend; d++)
+            float Sv[kChunk];
+#pragma unroll
+            for (int k = 0; k < kChunk; k++)
+                Sv[k] = d0 + k < a.nd ? S[(unsigned)(d0 + k) * nxy] : 0.f;
+#pragma unroll
+            for (int k = 0; k < kChunk; k++)
             {
+                const int d = d0 + k;
+                if (d >= a.nd)
+                    break;
                 const float n1 = GRLBM_RN1(d), n2 = GRLBM_RN2(d), w = sw[d];
                 float g = g0, h = h0, q1 = n1, q2 = n2;
                 if (!rest)
                     collide_coeffs(n1, n2, u1, u2, lor, adt, kak0, g, h, q1, q2);
-                const float v = g * S[(unsigned)d * nxy] + h * (e + k3 * (q1 * fFx + q2 * fFy));
+                const float v = g * Sv[k] + h * (e + k3 * (q1 * fFx + q2 * fFy));
                 out[(unsigned)d * a.plane] = v * scale;
                 const float wn1 = w * n1, wn2 = w * n2;
                 km.add(v, make_float4(w, wn1, wn2, wn1 * n1), make_float4(wn1 * n2, wn2 * n2, n1, n2));
