@@ -55,10 +55,14 @@ def test_flat_adaptive_is_bit_identical(grlbm, W, oracle, k):
         assert np.array_equal(ours[key], ref[key]), (key, rel_l2(ours[key], ref[key]))
 
 
-def test_curved_adaptive_matches_reference(grlbm, W, oracle):
+@pytest.mark.parametrize("kw", [
+    dict(nx_=40, ny_=36, n_dir=16, n_fourier=5, steps=20),
+    dict(nx_=37, ny_=23, n_dir=12, n_fourier=64, steps=10),  # ragged rows, 12 directions, the largest Fourier order
+])
+def test_curved_adaptive_matches_reference(grlbm, W, oracle, kw):
     if not oracle.available("ref_strict"):
         pytest.skip("the reference build is absent")
-    case = W.curved_shell(nx_=40, ny_=36, n_dir=16, n_fourier=5, steps=20)
+    case = W.curved_shell(**kw)
     case["streaming_type"] = W.CURVED_ADAPTIVE
     ref = oracle.run(case, "ref_strict")
     ours = run_ours(grlbm, case, ref)
@@ -68,19 +72,23 @@ def test_curved_adaptive_matches_reference(grlbm, W, oracle):
 
 def precision_cases(W):
     """Adaptive cases for the precision form: the flat beam, a moving
-    anisotropically scattering fluid (flat and curved), and a curved shell."""
+    anisotropically scattering fluid (flat and curved), and curved shells
+    (the second with ragged rows, 12 directions and the largest Fourier
+    order)."""
     beam = W.flat_beam(nx_=40, ny_=30, n_dir=16, steps=25)
     beam["streaming_type"] = W.FLAT_ADAPTIVE
     shell = W.curved_shell(nx_=48, ny_=40, n_dir=24, n_fourier=7, steps=20)
     shell["streaming_type"] = W.CURVED_ADAPTIVE
+    wide = W.curved_shell(nx_=37, ny_=23, n_dir=12, n_fourier=64, steps=10)
+    wide["streaming_type"] = W.CURVED_ADAPTIVE
     return [beam,
             W.moving_scatter(nx_=30, ny_=26, n_dir=20, steps=12, metric_kind=W.MINKOWSKI,
                              streaming_type=W.FLAT_ADAPTIVE),
             W.moving_scatter(nx_=30, ny_=26, n_dir=20, steps=12, streaming_type=W.CURVED_ADAPTIVE),
-            shell]
+            shell, wide]
 
 
-@pytest.mark.parametrize("k", [0, 1, 2, 3])
+@pytest.mark.parametrize("k", [0, 1, 2, 3, 4])
 def test_precision_form_adaptive_against_plain(grlbm, W, k):
     """Adaptive streaming in the precision form (FP32 stream and moment-space
     collide, FP32 Fourier basis) against the plain form on the same tables:
