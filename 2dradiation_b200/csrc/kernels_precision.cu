@@ -21,7 +21,8 @@
 // nFF_d . F_ff) -- so each iteration is evaluated on the six moments with
 // per-cell sums of the direction terms (O(1) per iteration instead of a pass
 // over the directions); the converged intensities are written in one final
-// pass whose Kahan sums give the stored moments.
+// pass, and the last iterate's moments -- the affine map's moments of exactly
+// those intensities -- are the stored moments.
 #include <cudaTypedefs.h>
 
 #include "approx_math.hpp"
@@ -520,8 +521,8 @@ __device__ __forceinline__ bool step_tile(const PrecStepArgs &a, const CUtensorM
             }
             diff = sqrtf(s2);
         }
-        // write the last iterate; its compensated sums are the stored moments
-        km.zero();
+        // write the intensities of the last iterate; its moments m, the
+        // affine map's moments of exactly these intensities, are the stored ones
         const float e = eta + k0 * fE;
         const float scale = CURVED ? a.ia3[ij] : 1.f;
         const float ra = h0 * e, rb1 = h0 * k3 * fFx, rb2 = h0 * k3 * fFy;
@@ -538,7 +539,7 @@ __device__ __forceinline__ bool step_tile(const PrecStepArgs &a, const CUtensorM
                 const int d = d0 + k;
                 if (d >= a.nd)
                     break;
-                const float4 c0 = dirc[2 * d], c1 = dirc[2 * d + 1];
+                const float4 c1 = dirc[2 * d + 1];
                 const float n1 = c1.z, n2 = c1.w;
                 float v;
                 if (rest)
@@ -550,11 +551,8 @@ __device__ __forceinline__ bool step_tile(const PrecStepArgs &a, const CUtensorM
                     v = g * S[k] + h * (e + k3 * (q1 * fFx + q2 * fFy));
                 }
                 Is[(unsigned)d * plane] = v * scale;
-                km.add(v, c0, c1);
             }
-            km.fold();
         }
-        m[0] = km.E.s, m[1] = km.Fx.s, m[2] = km.Fy.s, m[3] = km.Pxx.s, m[4] = km.Pxy.s, m[5] = km.Pyy.s;
     }
     if (active)
     {
@@ -824,7 +822,8 @@ __global__ void __launch_bounds__(kStepBlock) k_stream_prec_adaptive_curved(Prec
 // Moments and collide of one cell from its streamed values, with its
 // stencil rotated by its new angle: Kahan moments of the streamed values,
 // the lambda iteration in moment space (as the fixed-streaming kernel's
-// moving-fluid path), the collided state J = I / alpha^3 and its moments.
+// moving-fluid path), the collided state J = I / alpha^3, and the last
+// iterate's moments as the stored ones.
 template <bool CURVED>
 __global__ void __launch_bounds__(kStepBlock) k_collide_prec_adaptive(PrecStepArgs a, const __grid_constant__ DirTable dt)
 {
@@ -1005,8 +1004,8 @@ __global__ void __launch_bounds__(kStepBlock) k_collide_prec_adaptive(PrecStepAr
             }
             diff = sqrtf(s2);
         }
-        // the last iterate: the collided state and its compensated moments
-        km.zero();
+        // the intensities of the last iterate; its moments m, the affine
+        // map's moments of exactly these intensities, are the stored ones
         const float e = eta + k0 * fE;
         const float scale = CURVED ? a.ia3[ij] : 1.f;
         float *out = a.Iout + (unsigned)i + (unsigned)j * a.pitch;
@@ -1022,18 +1021,14 @@ __global__ void __launch_bounds__(kStepBlock) k_collide_prec_adaptive(PrecStepAr
                 const int d = d0 + k;
                 if (d >= a.nd)
                     break;
-                const float n1 = GRLBM_RN1(d), n2 = GRLBM_RN2(d), w = sw[d];
+                const float n1 = GRLBM_RN1(d), n2 = GRLBM_RN2(d);
                 float g = g0, h = h0, q1 = n1, q2 = n2;
                 if (!rest)
                     collide_coeffs(n1, n2, u1, u2, lor, adt, kak0, g, h, q1, q2);
                 const float v = g * Sv[k] + h * (e + k3 * (q1 * fFx + q2 * fFy));
                 out[(unsigned)d * a.plane] = v * scale;
-                const float wn1 = w * n1, wn2 = w * n2;
-                km.add(v, make_float4(w, wn1, wn2, wn1 * n1), make_float4(wn1 * n2, wn2 * n2, n1, n2));
             }
-            km.fold();
         }
-        m[0] = km.E.s, m[1] = km.Fx.s, m[2] = km.Fy.s, m[3] = km.Pxx.s, m[4] = km.Pxy.s, m[5] = km.Pyy.s;
     }
 #undef GRLBM_RN1
 #undef GRLBM_RN2
