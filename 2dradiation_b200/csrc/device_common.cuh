@@ -203,6 +203,9 @@ struct PlainStepArgs
     const double *coef; // [5][nf][nxy]: the Fourier coefficients, node index fastest
     int nf;
     double *S; // the streamed values of the step, [d * nxy + ij]
+    // 64-bit element offsets in the curved gather: set when the state has 2^32
+    // elements or more (and, for tests, when GRLBM_WIDE_OFFSETS=1 at creation)
+    bool wide;
 };
 
 struct PrecStepArgs

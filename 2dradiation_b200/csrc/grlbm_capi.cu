@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -66,6 +67,7 @@ struct grlbm_ctx
     // next), the source nodes' angles, and initialFluxAngle_IF
     DevBuf ang[2], src_ang_nodes, src_ang_vals;
     DevBuf rot; // adaptive: per node {sin, cos} of the inverse previous and the new rotation
+    bool wide_offsets = false; // GRLBM_WIDE_OFFSETS=1 at creation: the 64-bit gather at any size
     int64_t nsrc_ang = 0;
     std::vector<double> flux_angle;
     DevBuf ig_rows, ia3;
@@ -248,6 +250,7 @@ PlainStepArgs plain_args(grlbm_ctx *ctx, int from)
     a.g = ctx->gd;
     a.nd = ctx->st.n;
     a.ng = ctx->ng;
+    a.wide = ctx->wide_offsets || (uint64_t)ctx->st.n * (uint64_t)ctx->gd.nxy > 0xFFFFFFFFull;
     a.Iin = ctx->I[from].as<double>();
     a.Iout = ctx->I[from ^ 1].as<double>();
     a.rec = ctx->rec.as<double4>();
@@ -516,6 +519,8 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
     ctx->run = *run;
     ctx->mdesc = *metric;
     ctx->fp32 = run->precision == GRLBM_PRECISION_FP32;
+    if (const char *w = std::getenv("GRLBM_WIDE_OFFSETS"))
+        ctx->wide_offsets = w[0] == '1';
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
         return fail(nullptr, GRLBM_ERR_CUDA, "no CUDA device available");

@@ -8,6 +8,8 @@
 // change of all six moments, including ones that are pure rounding noise
 // (e.g. Fy of a nearly isotropic cell), so its iteration counts, and through
 // them E, follow the last bits of the streamed intensities.
+#include <type_traits>
+
 #include "approx_math.hpp"
 #include "device_common.cuh"
 
@@ -19,7 +21,9 @@ namespace
 // StreamCurvedFixed with IntensityAt (:478-508, 322-343)
 // `clamp_mask` receives bit q set where corner q's angular interpolation was
 // positive (kept by the clamp at zero); flat streaming keeps every corner.
-template <bool CURVED>
+// Off: the type of the state's element offsets (unsigned when the state has
+// fewer than 2^32 elements, int64_t otherwise).
+template <bool CURVED, typename Off>
 __device__ __forceinline__ double stream_value(const PlainStepArgs &a, int d, const double4 &r, int64_t i, int64_t j,
                                                int64_t ij, unsigned &clamp_mask)
 {
@@ -46,6 +50,14 @@ __device__ __forceinline__ double stream_value(const PlainStepArgs &a, int d, co
         const double w0[4] = {R0.w01.x, R0.w01.y, R0.w23.x, R0.w23.y};
         const double w1[4] = {R1.w01.x, R1.w01.y, R1.w23.x, R1.w23.y};
         const double al = __ldg(a.alpha + ij);
+        // element offsets of the 8 rows' planes
+        Off o0[4], o1[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+        {
+            o0[k] = (Off)idx0[k] * (Off)nxy;
+            o1[k] = (Off)idx1[k] * (Off)nxy;
+        }
         double Iq[4];
 #pragma unroll
         for (int q = 0; q < 4; q++) // corners 00, 01, 10, 11
@@ -56,8 +68,8 @@ __device__ __forceinline__ double stream_value(const PlainStepArgs &a, int d, co
 #pragma unroll
             for (int k = 0; k < 4; k++)
             {
-                v0 += w0[k] * __ldg(a.Iin + (int64_t)idx0[k] * nxy + n);
-                v1 += w1[k] * __ldg(a.Iin + (int64_t)idx1[k] * nxy + n);
+                v0 += w0[k] * __ldg(a.Iin + (o0[k] + (Off)n));
+                v1 += w1[k] * __ldg(a.Iin + (o1[k] + (Off)n));
             }
             double v = v0 * (1.0 - t) + v1 * t;
             if (!(0.0 < v))
@@ -432,7 +444,7 @@ constexpr int kSplitTileX = GRLBM_SPLIT_TILE_X, kSplitTileY = kStepBlock / kSpli
 #ifndef GRLBM_STREAM_MIN_BLOCKS
 #define GRLBM_STREAM_MIN_BLOCKS 1
 #endif
-template <bool CURVED, bool RECORD, bool ADAPTIVE>
+template <bool CURVED, bool RECORD, bool ADAPTIVE, bool WIDE = false>
 __global__ void __launch_bounds__(kStepBlock, GRLBM_STREAM_MIN_BLOCKS) k_stream_plain(PlainStepArgs a, StepRecord rec)
 {
     constexpr bool DFAST = ADAPTIVE ? kDirFastestAdaptive : kDirFastestFixed;
@@ -457,7 +469,7 @@ __global__ void __launch_bounds__(kStepBlock, GRLBM_STREAM_MIN_BLOCKS) k_stream_
         else
         {
             const double4 r = CURVED ? a.rec[(int64_t)d * a.g.ncell + cc] : make_double4(0, 0, 0, 0);
-            val = stream_value<CURVED>(a, d, r, i, j, ij, cm);
+            val = stream_value<CURVED, std::conditional_t<WIDE, int64_t, unsigned>>(a, d, r, i, j, ij, cm);
         }
     }
     if (RECORD)
@@ -861,6 +873,9 @@ void launch_step_plain(const PlainStepArgs &a, bool curved, cudaStream_t s, cons
                                          (size_t)5 * a.nf * kSplitTileX * sizeof(double), s>>>(a);
     else if (adaptive)
         k_stream_plain<false, false, true><<<ga, kStepBlock, 0, s>>>(a, rec);
+    else if (curved && a.wide) // 64-bit state offsets
+        record ? k_stream_plain<true, true, false, true><<<gf, kStepBlock, 0, s>>>(a, rec)
+               : k_stream_plain<true, false, false, true><<<gf, kStepBlock, 0, s>>>(a, rec);
     else if (curved)
         record ? k_stream_plain<true, true, false><<<gf, kStepBlock, 0, s>>>(a, rec)
                : k_stream_plain<true, false, false><<<gf, kStepBlock, 0, s>>>(a, rec);

@@ -77,6 +77,17 @@ def test_step_bitwise_from_reference_tables(name, grlbm, cases, golden):
 
 
 @pytest.mark.parametrize("name", GOLDEN_NAMES)
+def test_step_bitwise_with_wide_offsets(name, grlbm, cases, golden, monkeypatch):
+    """The curved gather's 64-bit element offsets, which states of 2^32
+    elements or more take, forced at this size (GRLBM_WIDE_OFFSETS=1 when the
+    context is created): the same bits as the reference."""
+    monkeypatch.setenv("GRLBM_WIDE_OFFSETS", "1")
+    ref = golden_ref(golden, name)
+    res = run_with_tables(grlbm, cases[name], ref)
+    bitwise(res, ref, MOMENTS + LF + ("I",))
+
+
+@pytest.mark.parametrize("name", GOLDEN_NAMES)
 def test_geodesic_tables_match_reference(name, grlbm, cases, golden):
     ref = golden_ref(golden, name)
     with grlbm.prepare(cases[name]) as r:
