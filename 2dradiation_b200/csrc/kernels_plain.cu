@@ -441,8 +441,10 @@ constexpr bool kDirFastestAdaptive = true, kDirFastestFixed = false;
 #define GRLBM_SPLIT_TILE_X 16
 #endif
 constexpr int kSplitTileX = GRLBM_SPLIT_TILE_X, kSplitTileY = kStepBlock / kSplitTileX;
+// resident blocks per SM the stream kernel's registers are sized for (6:
+// 80 registers, no spills in the curved gather with 32-bit offsets)
 #ifndef GRLBM_STREAM_MIN_BLOCKS
-#define GRLBM_STREAM_MIN_BLOCKS 1
+#define GRLBM_STREAM_MIN_BLOCKS 6
 #endif
 template <bool CURVED, bool RECORD, bool ADAPTIVE, bool WIDE = false>
 __global__ void __launch_bounds__(kStepBlock, GRLBM_STREAM_MIN_BLOCKS) k_stream_plain(PlainStepArgs a, StepRecord rec)
