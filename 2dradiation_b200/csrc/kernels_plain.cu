@@ -314,6 +314,12 @@ __device__ __forceinline__ double stream_value_adaptive(const PlainStepArgs &a, 
 // and the lambda-iteration statistics.
 // tw, tn1, tn2: the stencil's weights and directions (global or shared memory).
 // rot_s, rot_c: the cell's rotation (adaptive streaming).
+// Unroll of the lambda iteration's direction loops for a fluid at rest (the
+// directions' updates are independent; only the moment sums chain them).
+#ifndef GRLBM_ITER_UNROLL
+#define GRLBM_ITER_UNROLL 4
+#endif
+constexpr int kIterUnroll = GRLBM_ITER_UNROLL;
 template <bool RECORD, bool ADAPTIVE>
 __device__ __forceinline__ void finish_cell(const PlainStepArgs &a, const StepRecord &rec, bool active, bool collides,
                                             int64_t ij, int64_t cc, Moments m, const double *Sin, int64_t sst,
@@ -356,7 +362,7 @@ __device__ __forceinline__ void finish_cell(const PlainStepArgs &a, const StepRe
             if (rest)
             {
                 const double k0fE = k0 * fE;
-#pragma unroll 4
+#pragma unroll kIterUnroll
                 for (int d = 0; d < a.nd; d++)
                 {
                     const double n1 = GRLBM_N1(d), n2 = GRLBM_N2(d);
@@ -381,6 +387,7 @@ __device__ __forceinline__ void finish_cell(const PlainStepArgs &a, const StepRe
         if (rest)
         {
             const double k0fE = k0 * fE;
+#pragma unroll kIterUnroll
             for (int d = 0; d < a.nd; d++)
             {
                 const double n1 = GRLBM_N1(d), n2 = GRLBM_N2(d);
@@ -449,6 +456,7 @@ constexpr int kSplitTileX = GRLBM_SPLIT_TILE_X, kSplitTileY = kStepBlock / kSpli
 template <bool CURVED, bool RECORD, bool ADAPTIVE, bool WIDE = false>
 __global__ void __launch_bounds__(kStepBlock, GRLBM_STREAM_MIN_BLOCKS) k_stream_plain(PlainStepArgs a, StepRecord rec)
 {
+    static_assert(!(CURVED && ADAPTIVE), "curved adaptive streaming runs k_stream_plain_curved_adaptive");
     constexpr bool DFAST = ADAPTIVE ? kDirFastestAdaptive : kDirFastestFixed;
     const int d = DFAST ? blockIdx.x : blockIdx.z;
     const int bx = DFAST ? blockIdx.y : blockIdx.x, by = DFAST ? blockIdx.z : blockIdx.y;
