@@ -227,12 +227,12 @@ struct PrecStepArgs
     CUtensorMap in_map;       // TMA map of Iin: 2D, {pitch, ny * nd} floats, box of one patch plane
     // adaptive streaming only (null otherwise)
     const double *ang_old, *ang_new; // rotation angles before and after this step's update (nxy)
-    const double2 *rot_inv, *rot_new; // per node {sin, cos}: inverse previous rotation, new rotation
+    const float2 *rot_inv, *rot_new; // per node {sin, cos}: inverse previous rotation, new rotation
     // [5][nf][nxy]: the Fourier coefficients in FP32, node index fastest, with
     // the X and Y series taken about the node (its coordinates subtracted)
     const float *coef32;
     float inv_dx, inv_dy;            // 1 / dx, 1 / dy
-    const double *cx, *cy;           // nd: the stencil's unrotated directions
+    const float *cx, *cy;            // nd: the stencil's unrotated directions
     const IgRow32 *ig_rows;          // ng: the interpolation grid
     float *S;                        // [d * nxy + ij]: the streamed values of the step
     int nf;
@@ -374,6 +374,9 @@ void launch_moments_from_I32(const float *J, int64_t nxy, const StateLayout &L, 
 // evaluated once per node instead of once per gather).
 void launch_rotation_trig(int64_t nxy, const double *ang_old, const double *ang_new, double2 *rot_inv,
                           double2 *rot_new, cudaStream_t s);
+// The same, rounded to FP32 (the precision form).
+void launch_rotation_trig32(int64_t nxy, const double *ang_old, const double *ang_new, float2 *rot_inv,
+                            float2 *rot_new, cudaStream_t s);
 // The FP32 coefficient copy of adaptive streaming in the precision form:
 // coef [5][nxy][nf] (FP64) to [5][nf][nxy] (FP32), the node's x and y
 // subtracted from the constant terms of the X and Y series in FP64 first.

@@ -62,6 +62,7 @@ struct grlbm_ctx
     int ng = 0;
     // device buffers (storage type T = double for the plain form, float for the precision form)
     DevBuf I[2], rec, side, w, n1, n2, cx, cy, flags, bhmask, alpha, acube;
+    DevBuf cx32, cy32; // the precision form's adaptive streaming: the stencil directions in FP32
     DevBuf dirs64, frame_mom; // FP64 {w, n1, n2} and moments for frame output
     // adaptive streaming: rotation angles (ang[cur] current, ang[cur ^ 1] the
     // next), the source nodes' angles, and initialFluxAngle_IF
@@ -234,8 +235,8 @@ PrecStepArgs prec_args(grlbm_ctx *ctx, int from)
     a.coef32 = ctx->coef32.as<float>();
     a.inv_dx = (float)(1.0 / ctx->gd.dx);
     a.inv_dy = (float)(1.0 / ctx->gd.dy);
-    a.cx = ctx->cx.as<double>();
-    a.cy = ctx->cy.as<double>();
+    a.cx = ctx->cx32.as<float>();
+    a.cy = ctx->cy32.as<float>();
     a.ig_rows = ctx->ig_rows.as<IgRow32>();
     a.S = ctx->streamed.as<float>();
     a.nf = ctx->ss.n;
@@ -306,8 +307,8 @@ int enqueue_step(grlbm_ctx *ctx, int from)
                                  ctx->src_ang_vals.as<double>(), ctx->nsrc_ang, ctx->stream);
             a.ang_old = ctx->ang[from].as<double>();
             a.ang_new = ctx->ang[from ^ 1].as<double>();
-            a.rot_inv = ctx->rot.as<double2>();
-            a.rot_new = ctx->rot.as<double2>() + ctx->gd.nxy;
+            a.rot_inv = ctx->rot.as<float2>();
+            a.rot_new = ctx->rot.as<float2>() + ctx->gd.nxy;
             launch_step_prec_adaptive(a, ctx->dirs, curved, ctx->stream);
         }
         else
@@ -830,7 +831,13 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
             TRY(alloc(ctx, b, (size_t)nxy * sizeof(double)));
             cudaMemset(b.p, 0, b.bytes);
         }
-        TRY(alloc(ctx, ctx->rot, 2 * (size_t)nxy * sizeof(double2)));
+        TRY(alloc(ctx, ctx->rot, 2 * (size_t)nxy * (ctx->fp32 ? sizeof(float2) : sizeof(double2))));
+        if (ctx->fp32)
+        {
+            std::vector<float> cx32(ctx->st.cx.begin(), ctx->st.cx.end()), cy32(ctx->st.cy.begin(), ctx->st.cy.end());
+            TRY(upload(ctx, ctx->cx32, cx32));
+            TRY(upload(ctx, ctx->cy32, cy32));
+        }
         ctx->flux_angle.assign(nxy, 0.0);
     }
     cudaMemset(ctx->mom.p, 0, ctx->mom.bytes);

@@ -612,16 +612,18 @@ __global__ void k_rotation_update(GridDev g, const T *mom, const double *ang_old
 // previous one (RotationMatrix(angle).Inverse(), src/DataTypes.hh:625-635,
 // as IntensityAt uses it at each corner) and the new one (the cell's own
 // stencil), as {sin, cos}.
-__global__ void k_rotation_trig(int64_t nxy, const double *ang_old, const double *ang_new, double2 *rot_inv,
-                                double2 *rot_new)
+// V2: double2, or float2 for the precision form (the FP64 values rounded).
+template <typename V2>
+__global__ void k_rotation_trig(int64_t nxy, const double *ang_old, const double *ang_new, V2 *rot_inv, V2 *rot_new)
 {
+    using T = decltype(V2::x);
     const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= nxy)
         return;
     const double th = fmod(-ang_old[n] + 2.0 * kPi, 2.0 * kPi);
-    rot_inv[n] = make_double2(approx_sin(th), approx_cos(th));
+    rot_inv[n] = V2{(T)approx_sin(th), (T)approx_cos(th)};
     const double tn = ang_new[n];
-    rot_new[n] = make_double2(approx_sin(tn), approx_cos(tn));
+    rot_new[n] = V2{(T)approx_sin(tn), (T)approx_cos(tn)};
 }
 
 // The moments at the halo nodes, which the reference recomputes after every
@@ -931,6 +933,11 @@ void launch_coef_k_major(const double *coef, double *coef_k, int64_t nxy, int nf
 }
 void launch_rotation_trig(int64_t nxy, const double *ang_old, const double *ang_new, double2 *rot_inv,
                           double2 *rot_new, cudaStream_t s)
+{
+    k_rotation_trig<<<nblk(nxy, 256), 256, 0, s>>>(nxy, ang_old, ang_new, rot_inv, rot_new);
+}
+void launch_rotation_trig32(int64_t nxy, const double *ang_old, const double *ang_new, float2 *rot_inv,
+                            float2 *rot_new, cudaStream_t s)
 {
     k_rotation_trig<<<nblk(nxy, 256), 256, 0, s>>>(nxy, ang_old, ang_new, rot_inv, rot_new);
 }

@@ -635,8 +635,9 @@ constexpr int kATileX = 16, kATileY = kStepBlock / kATileX;
 // The reference's polynomial atan2 and Phi (MyAtan2<9>, Tensor2::Phi;
 // src/Utility.hh:179-254, src/DataTypes.hh:166-170) evaluated in FP32, in
 // grid-row units: nGrid * Phi(x, y) / (2 pi).  The same octants and
-// polynomial as approx_phi; the FP32 rounding adds an error of the order of
-// the FP32 rounding of the row coordinate itself.
+// polynomial as approx_phi, with the fast FP32 quotient (within 2 ulp, and
+// |z| <= 1 here); the FP32 rounding adds an error of the order of the FP32
+// rounding of the row coordinate itself.
 __device__ __forceinline__ float atan_poly9_f(float z)
 {
     const float zz = z * z;
@@ -650,13 +651,13 @@ __device__ __forceinline__ float grid_row_of(float x, float y, float rows_per_ra
     {
         if (fabsf(x) > fabsf(y))
         {
-            p = atan_poly9_f(y / x);
+            p = atan_poly9_f(__fdividef(y, x));
             if (x < 0.f)
                 p = (y >= 0.f) ? p + pi : p - pi;
         }
         else
         {
-            const float q = atan_poly9_f(x / y);
+            const float q = atan_poly9_f(__fdividef(x, y));
             p = (y > 0.f) ? half_pi - q : -q - half_pi;
         }
     }
@@ -675,8 +676,8 @@ __device__ __forceinline__ float intensity_at32(const PrecStepArgs &a, int n, un
 {
     // the inverse of the node's previous rotation, with the reference's
     // polynomial trigonometry (the plain form's values)
-    const double2 rinv = a.rot_inv[n];
-    const float sn = (float)rinv.x, cs = (float)rinv.y;
+    const float2 rinv = a.rot_inv[n];
+    const float sn = rinv.x, cs = rinv.y;
     const float w1 = v1 * cs - v2 * sn, w2 = v1 * sn + v2 * cs;
     float dd = grid_row_of(w1, w2, (float)a.ng * 0.159154943091895f);
     dd = fminf(fmaxf(dd, 1e-8f), nextafterf((float)a.ng, 0.f)); // InterpolationGrid's clamp, in FP32
@@ -705,9 +706,9 @@ __device__ __forceinline__ float stream_adaptive32(const PrecStepArgs &a, int d,
                                                    const float *cf, int ks, int qs)
 {
     const int nx = (int)a.g.nx;
-    const double2 rn = a.rot_new[ij];
-    const float sc = (float)rn.x, cc = (float)rn.y;
-    const float cxd = (float)a.cx[d], cyd = (float)a.cy[d];
+    const float2 rn = a.rot_new[ij];
+    const float sc = rn.x, cc = rn.y;
+    const float cxd = a.cx[d], cyd = a.cy[d];
     const float dir1 = cxd * cc - cyd * sc, dir2 = cxd * sc + cyd * cc;
     float it, jt, v1, v2, s3 = 1.f;
     if constexpr (CURVED)
@@ -842,7 +843,7 @@ __global__ void __launch_bounds__(kStepBlock) k_collide_prec_adaptive(PrecStepAr
     // sum w c_a c_b c_c (a <= b <= c)
     __shared__ float smom[10];
     for (int d = threadIdx.x; d < a.nd; d += kStepBlock)
-        sw[d] = dt.w[d], scx[d] = (float)a.cx[d], scy[d] = (float)a.cy[d];
+        sw[d] = dt.w[d], scx[d] = a.cx[d], scy[d] = a.cy[d];
     __syncthreads();
     if (threadIdx.x < 10)
     {
@@ -862,8 +863,8 @@ __global__ void __launch_bounds__(kStepBlock) k_collide_prec_adaptive(PrecStepAr
         smom[t] = s;
     }
     __syncthreads();
-    const double2 rn = a.rot_new[ij];
-    const float rs = (float)rn.x, rc = (float)rn.y;
+    const float2 rn = a.rot_new[ij];
+    const float rs = rn.x, rc = rn.y;
 #define GRLBM_RN1(d) (scx[d] * rc - scy[d] * rs)
 #define GRLBM_RN2(d) (scx[d] * rs + scy[d] * rc)
     KMoments km;
@@ -1188,8 +1189,8 @@ void launch_step_prec_adaptive(const PrecStepArgs &a, const DirTable &dt, bool c
     const unsigned tx = nblk(a.g.nx_, kATileX), ty = nblk(rows, kATileY);
     // UpdateRotationMatrizes from the previous moments, before the stream
     launch_rotation_update32(a.g, a.mom, a.ang_old, const_cast<double *>(a.ang_new), s);
-    launch_rotation_trig(a.g.nxy, a.ang_old, a.ang_new, const_cast<double2 *>(a.rot_inv),
-                         const_cast<double2 *>(a.rot_new), s);
+    launch_rotation_trig32(a.g.nxy, a.ang_old, a.ang_new, const_cast<float2 *>(a.rot_inv),
+                           const_cast<float2 *>(a.rot_new), s);
     const dim3 cgrid(tx, ty);
     if (curved)
     {
