@@ -215,7 +215,12 @@ __device__ __forceinline__ double intensity_at(const PlainStepArgs &a, int64_t n
     const double w1 = v1 * cs - v2 * sn, w2 = v1 * sn + v2 * cs;
     double dd = (double)a.ng * approx_phi(w1, w2) / (2.0 * kPi); // InterpolationGrid::d
     dd = dd < 1e-8 ? 1e-8 : ((double)a.ng - 1e-8 < dd ? (double)a.ng - 1e-8 : dd);
-    const int g0 = (int)floor(dd) % a.ng, g1 = (g0 + 1) % a.ng;
+    // g0 = floor(dd) % nGrid, g1 = (g0 + 1) % nGrid, without the divisions
+    // on the in-range path (the clamp keeps floor(dd) in [0, nGrid))
+    const int gz = (int)floor(dd);
+    int g0 = (unsigned)gz < (unsigned)a.ng ? gz : gz % a.ng;
+    g0 = g0 < 0 ? 0 : g0;
+    const int g1 = g0 + 1 == a.ng ? 0 : g0 + 1;
     const IgRow R0 = a.ig_rows[g0], R1 = a.ig_rows[g1];
     const int idx0[4] = {R0.idx.x, R0.idx.y, R0.idx.z, R0.idx.w};
     const int idx1[4] = {R1.idx.x, R1.idx.y, R1.idx.z, R1.idx.w};
