@@ -839,30 +839,14 @@ __global__ void __launch_bounds__(kStepBlock) k_collide_prec_adaptive(PrecStepAr
     const float *S = a.S + ij;
     // the cell's stencil, rotated (shared by the block's threads per direction)
     __shared__ float sw[kMaxDirs], scx[kMaxDirs], scy[kMaxDirs];
-    // the unrotated stencil's weighted moments: sum w, sum w c_a, sum w c_a c_b,
-    // sum w c_a c_b c_c (a <= b <= c)
-    __shared__ float smom[10];
     for (int d = threadIdx.x; d < a.nd; d += kStepBlock)
         sw[d] = dt.w[d], scx[d] = a.cx[d], scy[d] = a.cy[d];
     __syncthreads();
-    if (threadIdx.x < 10)
-    {
-        // component t: x-powers px, y-powers py of w c_x^px c_y^py
-        constexpr int px[10] = {0, 1, 0, 2, 1, 0, 3, 2, 1, 0}, py[10] = {0, 0, 1, 0, 1, 2, 0, 1, 2, 3};
-        const int t = threadIdx.x;
-        float s = 0.f;
-        for (int d = 0; d < a.nd; d++)
-        {
-            float v = sw[d];
-            for (int p = 0; p < px[t]; p++)
-                v *= scx[d];
-            for (int p = 0; p < py[t]; p++)
-                v *= scy[d];
-            s += v;
-        }
-        smom[t] = s;
-    }
-    __syncthreads();
+    // the unrotated stencil's weighted moments sum w, sum w c_a, sum w c_a c_b,
+    // sum w c_a c_b c_c (a <= b <= c), from the direction table's stencil sums
+    // (its directions are the stencil's under RotationMatrix(0), the identity)
+    const float smom[10] = {dt.wmom[0], dt.wmom[1], dt.wmom[2],  dt.wmom[3],  dt.wmom[4],
+                            dt.wmom[5], dt.wmom[9], dt.wmom[10], dt.wmom[11], dt.wmom[17]};
     const float2 rn = a.rot_new[ij];
     const float rs = rn.x, rc = rn.y;
 #define GRLBM_RN1(d) (scx[d] * rc - scy[d] * rs)
