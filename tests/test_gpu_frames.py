@@ -33,16 +33,22 @@ def test_run_simulation_frames_match_reference(grlbm, W, oracle, tmp_path):
         assert (ours / name).read_bytes() == (ref_dir / name).read_bytes(), name
 
 
-def test_tables_rebuilt_every_step(grlbm, W):
+@pytest.mark.parametrize("adaptive,precision", [(False, 0), (True, 0), (True, 1)])
+def test_tables_rebuilt_every_step(grlbm, W, adaptive, precision):
     """Config::updateFourierHarmonics: with a static metric, rebuilding the
     tables before every step reproduces the tables-once run bit for bit (as
-    it does in the reference); the table statistics show the rebuilds."""
+    it does in the reference); the table statistics show the rebuilds.  With
+    CurvedAdaptive streaming the rebuild also refreshes the coefficient
+    copies the adaptive stream reads (FP64 node-major, or FP32 about the node
+    in the precision form)."""
     import numpy as np
     case = W.curved_shell(nx_=40, ny_=32, n_dir=16, n_fourier=5, steps=6)
-    with grlbm.prepare(case) as a:
+    if adaptive:
+        case["streaming_type"] = W.CURVED_ADAPTIVE
+    with grlbm.prepare(case, precision) as a:
         a.step(6)
         Ea = a.moments_if()["E"]
-    with grlbm.prepare(case) as b:
+    with grlbm.prepare(case, precision) as b:
         b.update_tables_each_step(True, case["rk_tol"])
         b.step(6)
         Eb = b.moments_if()["E"]
