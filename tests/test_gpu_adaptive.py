@@ -98,3 +98,25 @@ def test_precision_form_adaptive_against_plain(grlbm, W, k):
     res = grlbm.run(case, grlbm.PRECISION_FP32)
     for key in ("E", "Fx", "Fy"):
         assert rel_l2(res[key], ref[key]) <= 2e-5, (key, rel_l2(res[key], ref[key]))
+
+
+def test_precision_form_adaptive_from_set_coefficients(grlbm, W):
+    """Coefficients handed in through grlbm_set_fourier_coefficients (as a
+    caller of the reference may set coefficientsS/X/Y/Cx/Cy) feed the
+    precision form's FP32 copy as well: the same run as with the tables built
+    in place, within the precision form's tolerance of the plain form."""
+    case = W.curved_shell(nx_=37, ny_=23, n_dir=12, n_fourier=7, steps=10)
+    case["streaming_type"] = W.CURVED_ADAPTIVE
+    with grlbm.prepare(case, grlbm.PLAIN_FP64) as p:
+        coef = p.coefficients()
+        p.step(int(case["n_steps"]))
+        ref = dict(p.moments_if())
+    with grlbm.Radiation(case, grlbm.PRECISION_FP32) as r:
+        r.set_fields(case["fields"])
+        r.set_initial_data(case["fields"])
+        r.load_initial_data()
+        r.set_coefficients(coef)
+        r.step(int(case["n_steps"]))
+        res = dict(r.moments_if())
+    for key in ("E", "Fx", "Fy"):
+        assert rel_l2(res[key], ref[key]) <= 2e-5, (key, rel_l2(res[key], ref[key]))
