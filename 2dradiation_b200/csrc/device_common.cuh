@@ -59,6 +59,12 @@ static_assert(RF_DG222 % 2 == 0 && RF_T11 % 2 == 0 && RF_TI11 % 2 == 0 && kRkStr
               "fields read in pairs (16-byte loads)");
 
 constexpr int kStepBlock = 128;
+// Threads per block of the curved adaptive stream kernels: 16 cells of a row
+// times kAdaptiveBlock / 16 directions sharing the row's staged coefficients.
+#ifndef GRLBM_ADAPTIVE_BLOCK
+#define GRLBM_ADAPTIVE_BLOCK 256
+#endif
+constexpr int kAdaptiveBlock = GRLBM_ADAPTIVE_BLOCK;
 constexpr int kMaxDirs = 256;
 constexpr int kMaxFourier = 64;
 

@@ -493,11 +493,12 @@ __global__ void __launch_bounds__(kStepBlock, GRLBM_STREAM_MIN_BLOCKS) k_stream_
 }
 
 // Curved adaptive stream: a block takes 16 cells of one row for kPDirs
-// directions.  It first stages the row's Fourier coefficients (5 nF x 16
-// doubles, at most 40 KB) in shared memory, where its directions share
-// them; each warp then covers 16 cells x 2 directions.
-constexpr int kPDirs = kStepBlock / kSplitTileX;
-__global__ void __launch_bounds__(kStepBlock) k_stream_plain_curved_adaptive(PlainStepArgs a)
+// directions (16: 7% faster than 8, and 32 slower, at 400^2 x 64).  It first
+// stages the row's Fourier coefficients (5 nF x 16 doubles, at most 40 KB)
+// in shared memory, where its directions share them; each warp then covers
+// 16 cells x 2 directions.
+constexpr int kPDirs = kAdaptiveBlock / kSplitTileX;
+__global__ void __launch_bounds__(kAdaptiveBlock) k_stream_plain_curved_adaptive(PlainStepArgs a)
 {
     extern __shared__ double sco[]; // [q * nF + k][cell]
     // blockIdx.x: direction group fastest, then the row; blockIdx.y: the run of 16 cells
@@ -509,7 +510,7 @@ __global__ void __launch_bounds__(kStepBlock) k_stream_plain_curved_adaptive(Pla
     const int nrow = min(kSplitTileX, (int)a.g.nx_ + 1 - x0);
     const int64_t row0 = (int64_t)x0 + (int64_t)j * a.g.nx;
     // coefficient k of series q of node ij sits at coef[(q nF + k) nxy + ij]
-    for (int e = t; e < 5 * a.nf * kSplitTileX; e += kStepBlock)
+    for (int e = t; e < 5 * a.nf * kSplitTileX; e += kAdaptiveBlock)
     {
         const int p = e / kSplitTileX, cc = e % kSplitTileX;
         sco[e] = cc < nrow ? a.coef[(int64_t)p * a.g.nxy + row0 + cc] : 0.0;
@@ -886,7 +887,7 @@ void launch_step_plain(const PlainStepArgs &a, bool curved, cudaStream_t s, cons
     // stream
     const dim3 ga = kDirFastestAdaptive ? sgrid_df : sgrid, gf = kDirFastestFixed ? sgrid_df : sgrid;
     if (adaptive && curved)
-        k_stream_plain_curved_adaptive<<<dim3(nblk(a.nd, kPDirs) * (unsigned)(a.g.jhi - a.g.jlo), tx), kStepBlock,
+        k_stream_plain_curved_adaptive<<<dim3(nblk(a.nd, kPDirs) * (unsigned)(a.g.jhi - a.g.jlo), tx), kAdaptiveBlock,
                                          (size_t)5 * a.nf * kSplitTileX * sizeof(double), s>>>(a);
     else if (adaptive)
         k_stream_plain<false, false, true><<<ga, kStepBlock, 0, s>>>(a, rec);

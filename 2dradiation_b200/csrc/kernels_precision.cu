@@ -788,12 +788,13 @@ __global__ void __launch_bounds__(kStepBlock) k_stream_prec_adaptive_flat(PrecSt
     a.S[(size_t)d * (size_t)a.g.nxy + (size_t)ij] = stream_adaptive32<false>(a, d, i, j, ij, nullptr, 0, 0);
 }
 
-// Curved stream: a block takes 16 cells of one row for kADirs directions.
+// Curved stream: a block takes 16 cells of one row for kADirs directions
+// (16: 6% faster than 8, and 32 slower, at 400^2 x 64).
 // It first stages the row's Fourier coefficients (5 nF x 16 floats, at most
 // 20 KB) in shared memory, where its directions share them; each warp then
 // covers 16 cells x 2 directions, so a tap load reads two 16-node runs.
-constexpr int kADirs = kStepBlock / kATileX;
-__global__ void __launch_bounds__(kStepBlock) k_stream_prec_adaptive_curved(PrecStepArgs a)
+constexpr int kADirs = kAdaptiveBlock / kATileX;
+__global__ void __launch_bounds__(kAdaptiveBlock) k_stream_prec_adaptive_curved(PrecStepArgs a)
 {
     extern __shared__ float sco[]; // [q * nF + k][cell]
     // blockIdx.x: direction group fastest, then the row; blockIdx.y: the run of 16 cells
@@ -805,7 +806,7 @@ __global__ void __launch_bounds__(kStepBlock) k_stream_prec_adaptive_curved(Prec
     const int nrow = min(kATileX, (int)a.g.nx_ + 1 - x0);
     const int row0 = x0 + j * (int)a.g.nx;
     // coefficient k of series q of node ij sits at coef32[(q nF + k) nxy + ij]
-    for (int e = t; e < 5 * a.nf * kATileX; e += kStepBlock)
+    for (int e = t; e < 5 * a.nf * kATileX; e += kAdaptiveBlock)
     {
         const int p = e / kATileX, cc = e % kATileX;
         sco[e] = cc < nrow ? a.coef32[(size_t)p * (size_t)a.g.nxy + (size_t)(row0 + cc)] : 0.f;
@@ -1180,7 +1181,7 @@ void launch_step_prec_adaptive(const PrecStepArgs &a, const DirTable &dt, bool c
     {
         const dim3 sgrid(nblk(a.nd, kADirs) * (unsigned)rows, tx);
         const size_t coef_bytes = (size_t)5 * a.nf * kATileX * sizeof(float);
-        k_stream_prec_adaptive_curved<<<sgrid, kStepBlock, coef_bytes, s>>>(a);
+        k_stream_prec_adaptive_curved<<<sgrid, kAdaptiveBlock, coef_bytes, s>>>(a);
         k_collide_prec_adaptive<true><<<cgrid, kStepBlock, 0, s>>>(a, dt);
     }
     else
