@@ -65,6 +65,8 @@ constexpr int kStepBlock = 128;
 #define GRLBM_ADAPTIVE_BLOCK 256
 #endif
 constexpr int kAdaptiveBlock = GRLBM_ADAPTIVE_BLOCK;
+static_assert(kAdaptiveBlock % 32 == 0 && kAdaptiveBlock >= 32 && kAdaptiveBlock <= 1024,
+              "whole warps of 16 cells x 2 directions, within the block limit");
 constexpr int kMaxDirs = 256;
 constexpr int kMaxFourier = 64;
 
