@@ -109,6 +109,8 @@ SIGNATURES = {
     "grlbm_row_bytes": ([C.c_void_p, C.POINTER(C.c_int64)], C.c_int),
     "grlbm_copy_rows": ([C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_int32], C.c_int),
     "grlbm_departure_rows": ([C.c_void_p, C.POINTER(C.c_int32)], C.c_int),
+    "grlbm_set_tile_shape": ([C.c_void_p, C.c_int32, C.c_int32], C.c_int),
+    "grlbm_get_tile_shape": ([C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32)], C.c_int),
     "grlbm_host_stencil": ([C.c_int32, C.c_int32, _D, _D, _D, _D, C.POINTER(C.c_int64), _D], C.c_int),
     "grlbm_host_flux_table": ([C.c_int32, C.POINTER(C.c_int32), _D, _D, _D, C.c_int32], C.c_int),
     "grlbm_host_metric_arrays": ([C.POINTER(GridDesc), C.POINTER(MetricDesc), _D], C.c_int),
@@ -316,6 +318,15 @@ class Radiation:
         """Rows [j_first, j_first + n) of the state to/from a device buffer
         (stream-ordered on the context's stream)."""
         self._c(lib().grlbm_copy_rows(self.h, j_first, n, C.c_void_p(buffer_ptr), 1 if to_buffer else 0))
+
+    # ---- tiles of the precision form's fixed streaming step ----
+    def set_tile_shape(self, tile_x: int, tile_y: int):
+        self._c(lib().grlbm_set_tile_shape(self.h, tile_x, tile_y))
+
+    def tile_shape(self) -> tuple:
+        x, y = C.c_int32(), C.c_int32()
+        self._c(lib().grlbm_get_tile_shape(self.h, C.byref(x), C.byref(y)))
+        return (x.value, y.value)
 
     def departure_rows(self) -> int:
         v = C.c_int32()

@@ -70,18 +70,38 @@ static_assert(kAdaptiveBlock % 32 == 0 && kAdaptiveBlock >= 32 && kAdaptiveBlock
 constexpr int kMaxDirs = 256;
 constexpr int kMaxFourier = 64;
 
-// Where node ij = i + j nx of a direction plane sits in a state buffer.
+// Directions 0..kStateMirror-1 repeated after the last direction in the
+// cell-major FP32 state, so that every 5-direction angular window of a node
+// is one contiguous run.
+constexpr int kStateMirror = 4;
+
+// Where intensity (node ij = i + j nx, direction d) sits in a state buffer:
+// element at(ij) * sp + d * plane.  Direction-major layouts have sp = 1 and
+// plane = the plane stride; the cell-major layout has sp = dp (the direction
+// pitch) and plane = 1, and repeats directions 0..mirror-1 after the last.
 struct StateLayout
 {
-    int64_t nx, pitch, plane; // grid row length, state row pitch, plane stride (elements)
+    int64_t nx, pitch, plane; // grid row length, state row pitch (nodes), direction stride (elements)
+    int64_t sp = 1;           // node stride (elements)
+    int mirror = 0;           // directions repeated after the last one
     __host__ __device__ int64_t at(int64_t ij) const { return pitch == nx ? ij : ij + (ij / nx) * (pitch - nx); }
+    __host__ __device__ int64_t elem(int64_t ij, int64_t d) const { return at(ij) * sp + d * plane; }
     static StateLayout dense(int64_t nx, int64_t ny) { return StateLayout{nx, nx, nx * ny}; }
-    // FP32 state: rows padded to 16 bytes
+    // FP32 state of the adaptive streaming types: direction-major, rows padded to 16 bytes
     static StateLayout padded32(int64_t nx, int64_t ny)
     {
         const int64_t pitch = (nx + 3) & ~(int64_t)3;
         return StateLayout{nx, pitch, pitch * ny};
     }
+    // FP32 state of the fixed streaming types: cell-major, [ij * dp + d] with
+    // dp = nd + kStateMirror rounded up to 4 floats (16-byte node records)
+    static int direction_pitch(int nd) { return (nd + kStateMirror + 3) & ~3; }
+    static StateLayout cell_major32(int64_t nx, int nd)
+    {
+        return StateLayout{nx, nx, 1, (int64_t)direction_pitch(nd), kStateMirror};
+    }
+    // elements of a buffer of ny rows and nd directions
+    int64_t elements(int64_t ny, int nd) const { return sp == 1 ? plane * nd : pitch * ny * sp; }
 };
 
 struct GridDev
@@ -129,23 +149,23 @@ struct ProjectArgs
     double *coef;        // [5][nxy][nf]
 };
 
-// Staging of the precision-form step: per direction chunk of kChunk
-// directions the kernel holds the planes [chunk0 - kBelow, chunk0 - kBelow +
-// kSpan) of a tile's patch; an angular window has kTaps directions.
-constexpr int kChunk = 8, kBelow = 4, kSpan = kChunk + 8, kTaps = 5;
+// Directions per chunk of the adaptive precision-form kernels' moment loops.
+constexpr int kChunk = 8;
 
-// Packed window word of a precision-form record (bit fields of .x):
-//   bits  0-17  t, the blend between interpolation rows, in units of 2^-18
-//   bits 18-22  row type of the departure's interpolation row
-//   bits 23-28  first direction of the angular window minus d, plus 32
-//   bits 29-30  corner code: floor(i_dep - i) + 1 + 2 (floor(j_dep - j) + 1)
-//   bit  31     far: the departure lies outside the cell's 3x3 neighbourhood
-//               or its window outside the staged planes (read the side record)
-namespace packed
+// Packed departure record of the precision form (uint4, [c * nd + d]):
+//   .x  bits  0-17  t, the blend between interpolation rows, in units of 2^-18
+//       bits 18-22  row type of the departure's interpolation row
+//       bits 23-30  first direction of the 5-direction angular window
+//   .y  fx = i_dep - i0, the bilinear fraction, with bit 31 set when the
+//       corner column i0 is i (clear: i - 1)
+//   .z  fy likewise for the corner row
+//   .w  s^3 alpha_c^3 (0 when the departure is excised), with bit 31 set when
+//       the departure lies outside the cell's 3x3 neighbourhood (far: read
+//       the side record {i_dep - i, j_dep - j, angle coordinate, s^3 alpha_c^3})
+namespace packed32
 {
-constexpr unsigned kTBits = 18, kTypeShift = 18, kBaseShift = 23, kCodeShift = 29, kFarBit = 31;
-constexpr int kBaseBias = 32;
-} // namespace packed
+constexpr unsigned kTBits = 18, kTypeShift = 18, kStartShift = 23;
+} // namespace packed32
 
 struct DepartureArgs
 {
@@ -155,9 +175,9 @@ struct DepartureArgs
     const double *eval;  // [k][d] = Basis(k, phi_d) at the intensity directions
     const double *alpha; // nxy
     double rot_c, rot_s; // RotationMatrix(0) entries
-    double4 *rec64;      // plain records or null
-    float4 *rec32;       // precision records (packed) or null
-    float4 *side32;      // precision side records or null
+    double4 *rec64;      // plain records [d * ncell + c] or null
+    uint4 *rec32;        // precision records (packed32) [c * nd + d] or null
+    float4 *side32;      // precision side records [c * nd + d] or null
     int q, p;            // interpolation row period (row types) and its direction shift
     int row_base[32];    // first window direction of each row type
     int *clamped;
@@ -216,14 +236,13 @@ struct PlainStepArgs
     bool wide;
 };
 
+// The adaptive streaming types in the precision form (direction-major state).
 struct PrecStepArgs
 {
     GridDev g;
     int nd, ng;
     const float *Iin;
     float *Iout;
-    const float4 *rec;        // packed records
-    const float4 *side;       // side records
     const float *ia3;         // nxy: 1/alpha^3 (scale of the stored state)
     const uint8_t *flags;
     const float *u1, *u2, *lor, *adt, *eta, *k0, *k3, *ka;
@@ -231,9 +250,6 @@ struct PrecStepArgs
     unsigned long long *iter_sum;
     unsigned int *iter_max;
     unsigned pitch, plane;    // state row pitch (a multiple of 4 floats) and plane stride
-    unsigned *fault;          // set to 1 when a staging copy does not land within its time limit
-    CUtensorMap in_map;       // TMA map of Iin: 2D, {pitch, ny * nd} floats, box of one patch plane
-    // adaptive streaming only (null otherwise)
     const double *ang_old, *ang_new; // rotation angles before and after this step's update (nxy)
     const float2 *rot_inv, *rot_new; // per node {sin, cos}: inverse previous rotation, new rotation
     // [5][nf][nxy]: the Fourier coefficients in FP32, node index fastest, with
@@ -301,13 +317,41 @@ struct AdjCollideArgs
     double *g_eta, *g_ka, *g_k0;       // nxy: gradients, accumulated
 };
 
-// One problem of a batched precision-form step: its step arguments for
-// either buffer parity, its direction tables (device memory) and its tiles.
-struct BatchItem
+// The precision-form step of the fixed streaming types (cell-major state,
+// kernels_step32.cu): warps of kStep32Warps per block, each taking tiles of
+// tx x ty cells from a counter.
+constexpr int kStep32Warps = 4;
+constexpr int kStep32MaxSmem = 227 * 1024;
+struct Step32Args
 {
-    PrecStepArgs a[2]; // a[k]: the step that reads intensity buffer k
+    GridDev g;
+    int nd, ng, dp;          // directions, interpolation rows, direction pitch of the state
+    int tx, ty;              // cells per tile; a warp stages (tx + 2) x (ty + 2) nodes
+    int tiles_x, ntiles;     // tiles per row of tiles, tiles over the slab rows
+    const float *Iin;
+    float *Iout;
+    const uint4 *rec;        // packed records (curved)
+    const float4 *side;      // side records (curved)
+    const float *ia3;        // nxy: 1/alpha^3, the scale of the stored state (curved)
+    const uint8_t *flags;    // nxy: bit0 excised node (no collide), bit1 stream writes 0
+    const float *u1, *u2, *lor, *adt, *eta, *k0, *k3, *ka;
+    float *mom;              // 6*nxy
+    unsigned long long *iter_sum;
+    unsigned int *iter_max;
+    unsigned *fault;         // set to 1 when a staging copy does not land within its time limit
+    // [0] the next tile to take, [1] warps done: zero between launches (the
+    // launch's last warp clears both)
+    unsigned *tiles;
+    CUtensorMap in_map;      // Iin as a 4D tensor, one box per tile patch (encode_state_map32)
+};
+
+// One problem of a batched precision-form step: its step arguments for
+// either buffer parity and its direction tables (device memory).
+struct Batch32Item
+{
+    Step32Args a[2]; // a[k]: the step that reads intensity buffer k
     const DirTable *dt;
-    int tiles_x, tiles_y, curved, cur0;
+    int curved, cur0;
 };
 
 int64_t adj_entries_per_source(bool curved);
@@ -332,23 +376,29 @@ void launch_alpha_cube(const GridDev &g, const double *alpha, double *acube, cud
 
 cudaError_t prepare_step_plain(int smem_bytes);
 void launch_step_plain(const PlainStepArgs &a, bool curved, cudaStream_t s, const StepRecord *record = nullptr);
-cudaError_t prepare_step_prec(int smem_bytes);
-size_t step_prec_smem(int nd);
 // One block's bounded wait on an mbarrier phase nothing (arrive = 0) or one
 // arrival (arrive = 1) completes; synchronous.
 cudaError_t run_wait_selftest(int arrive, unsigned long long limit_ns, int *completed, unsigned long long *waited_ns);
-// The TMA map the precision step stages Iin through (a state buffer of
-// layout L and nd planes over ny rows each).
-cudaError_t encode_state_map(CUtensorMap *map, const float *state, const StateLayout &L, int64_t ny, int nd);
-void launch_step_prec(const PrecStepArgs &a, const DirTable &dt, bool curved, cudaStream_t s);
 // the adaptive streaming types in the precision form: stream, then moments
 // and collide (and the rotation update before, the halo moments after)
 void launch_step_prec_adaptive(const PrecStepArgs &a, const DirTable &dt, bool curved, cudaStream_t s);
-int step_prec_tiles_x(int64_t nx_);
-int step_prec_tiles_y(int64_t rows);
-cudaError_t prepare_step_batch(int smem_bytes, int *blocks_per_sm);
-void launch_step_batch(const BatchItem *items, const int *first_tile, int n_items, int total_tiles, int flip,
-                       int blocks, int smem_bytes, cudaStream_t s);
+
+// The fixed streaming types in the precision form (kernels_step32.cu).
+// Passes per lane for nd directions (an instantiated count >= nd / 32), or -1.
+int step32_passes(int nd);
+int step32_patch_stride(int tx, int ty, int dp);
+// shared memory of a block: the fixed part, and with four patch buffers
+size_t step32_smem_base();
+size_t step32_smem(int tx, int ty, int dp);
+cudaError_t prepare_step32();
+cudaError_t step32_occupancy(int P, bool curved, bool batch, size_t smem, int *blocks);
+// blocks: the persistent grid (resident blocks per SM times the SMs)
+void launch_step32(const Step32Args &a, const DirTable &dt, bool curved, int P, int blocks, cudaStream_t s);
+void launch_step_batch32(const Batch32Item *items, const int *first_tile, int n_items, int total_tiles, int flip,
+                         unsigned *counters, int P, int blocks, size_t smem, int patch_stride, cudaStream_t s);
+// The TMA map the step stages a cell-major state of nx x ny nodes through,
+// for tiles of tx x ty cells.
+cudaError_t encode_state_map32(CUtensorMap *map, const float *state, int64_t nx, int64_t ny, int dp, int tx, int ty);
 
 void launch_sources64(double *I, int64_t nxy, int nd, const int64_t *nodes, const double *vals, int64_t nsrc,
                       cudaStream_t s);

@@ -19,7 +19,10 @@
 //     the caller;
 //   * the first call on each device looks up the array's device address
 //     (cudaGetSymbolAddress, with that device current) and caches it; make
-//     that first call before capturing a stream into a CUDA graph.
+//     that first call before capturing a stream into a CUDA graph.  The cache
+//     is never invalidated: after a cudaDeviceReset in the host process the
+//     cached address is stale, so a process that resets a device must not
+//     call this entry point on that device again.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -111,6 +114,17 @@ extern "C" int grlbm_energy_noalloc(const double *E, int64_t nx_, int64_t ny_, d
         grlbm::set_global_error("grlbm_energy_noalloc: null pointer or empty grid");
         return GRLBM_ERR_ARGUMENT;
     }
+    // each size checked on its own first, so that nx_ * ny_ cannot overflow
+    constexpr int64_t kMaxCells = (int64_t)kNoAllocPartials * kNoAllocCellsPerPartial;
+    if (nx_ > kMaxCells || ny_ > kMaxCells / nx_)
+    {
+        char msg[200];
+        snprintf(msg, sizeof msg,
+                 "grlbm_energy_noalloc: %lld x %lld interior cells exceed its fixed scratch (at most %lld)",
+                 (long long)nx_, (long long)ny_, (long long)kMaxCells);
+        grlbm::set_global_error(msg);
+        return GRLBM_ERR_ARGUMENT;
+    }
     const int64_t ncell = nx_ * ny_;
     const int64_t blocks = (ncell + kNoAllocCellsPerPartial - 1) / kNoAllocCellsPerPartial;
     if (blocks > kNoAllocPartials)
@@ -129,11 +143,16 @@ extern "C" int grlbm_energy_noalloc(const double *E, int64_t nx_, int64_t ny_, d
         return GRLBM_ERR_CUDA;
     }
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // an error left by earlier, unrelated asynchronous work is not this call's
+    (void)cudaGetLastError();
     k_energy_blocks<<<(unsigned)blocks, kNoAllocCellsPerPartial, 0, s>>>(E, nx_ + 2, nx_, ncell, partials);
     k_energy_fold<<<1, 256, 0, s>>>(partials, (int)blocks, total);
-    if (cudaGetLastError() != cudaSuccess)
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess)
     {
-        grlbm::set_global_error("grlbm_energy_noalloc: kernel launch failed");
+        char msg[200];
+        snprintf(msg, sizeof msg, "grlbm_energy_noalloc: kernel launch failed: %s", cudaGetErrorString(e));
+        grlbm::set_global_error(msg);
         return GRLBM_ERR_CUDA;
     }
     return GRLBM_OK;

@@ -56,7 +56,10 @@ struct grlbm_ctx
     bool fp32 = false;
     GridDev gd{};
     StateLayout sl{};          // node positions in the state buffers
-    CUtensorMap in_map[2];     // precision form: TMA maps of the state buffers
+    // precision form, fixed streaming: the step's tile shape, passes per lane,
+    // persistent grid, and the TMA maps of the state buffers for that tile
+    int tile_x = 4, tile_y = 4, passes = 1, step_blocks = 1;
+    CUtensorMap in_map[2];
     unsigned *fault = nullptr; // mapped host word: a precision step's staging wait timed out
     int64_t ncell = 0;
     int ng = 0;
@@ -79,6 +82,7 @@ struct grlbm_ctx
     DevBuf cu1, cu2, clor, cadt, ceta, ck0, ck3, cka, mom, rkf, lfp;
     DevBuf coef, ss_cx, ss_cy, ss_w, proj_basis, eval_basis, stage;
     DevBuf src_nodes, src_vals, lf_out, energy_partial, energy_out;
+    DevBuf tile_ctr; // precision form, fixed streaming: the step's tile counter and retired warps
     // counters: [0] iteration sum, [1] iteration max (low 32 bits), [2] RK45
     // trials, [3] capped backtraces, [4] departures off the grid, [5] row
     // extent of the gathers, [6] far precision-form departures
@@ -202,7 +206,7 @@ const float *state_scale(const grlbm_ctx *ctx)
     return (ctx->fp32 && (st == GRLBM_CURVED_FIXED || st == GRLBM_CURVED_ADAPTIVE)) ? ctx->ia3.as<float>() : nullptr;
 }
 
-// Arguments of the precision-form step that reads intensity buffer `from`.
+// Arguments of the adaptive precision-form step that reads intensity buffer `from`.
 PrecStepArgs prec_args(grlbm_ctx *ctx, int from)
 {
     unsigned long long *cnt = ctx->counters.as<unsigned long long>();
@@ -212,8 +216,6 @@ PrecStepArgs prec_args(grlbm_ctx *ctx, int from)
     a.ng = ctx->ng;
     a.Iin = ctx->I[from].as<float>();
     a.Iout = ctx->I[from ^ 1].as<float>();
-    a.rec = ctx->rec.as<float4>();
-    a.side = ctx->side.as<float4>();
     a.ia3 = ctx->ia3.as<float>();
     a.flags = ctx->flags.as<uint8_t>();
     a.u1 = ctx->cu1.as<float>();
@@ -229,9 +231,7 @@ PrecStepArgs prec_args(grlbm_ctx *ctx, int from)
     a.iter_max = reinterpret_cast<unsigned int *>(cnt + 1);
     a.pitch = (unsigned)ctx->sl.pitch;
     a.plane = (unsigned)ctx->sl.plane;
-    a.fault = ctx->fault;
-    a.in_map = ctx->in_map[from];
-    // adaptive streaming (the angles are set per step)
+    // the angles are set per step
     a.coef32 = ctx->coef32.as<float>();
     a.inv_dx = (float)(1.0 / ctx->gd.dx);
     a.inv_dy = (float)(1.0 / ctx->gd.dy);
@@ -241,6 +241,107 @@ PrecStepArgs prec_args(grlbm_ctx *ctx, int from)
     a.S = ctx->streamed.as<float>();
     a.nf = ctx->ss.n;
     return a;
+}
+
+int step32_tiles_x(const grlbm_ctx *ctx) { return (int)((ctx->gd.nx_ + ctx->tile_x - 1) / ctx->tile_x); }
+int step32_tiles(const grlbm_ctx *ctx)
+{
+    const int64_t rows = ctx->gd.jhi - ctx->gd.jlo;
+    return rows <= 0 ? 0 : step32_tiles_x(ctx) * (int)((rows + ctx->tile_y - 1) / ctx->tile_y);
+}
+
+// Arguments of the precision-form step of the fixed streaming types that
+// reads intensity buffer `from`.
+Step32Args step32_args(grlbm_ctx *ctx, int from)
+{
+    unsigned long long *cnt = ctx->counters.as<unsigned long long>();
+    Step32Args a{};
+    a.g = ctx->gd;
+    a.nd = ctx->st.n;
+    a.ng = ctx->ng;
+    a.dp = (int)ctx->sl.sp;
+    a.tx = ctx->tile_x;
+    a.ty = ctx->tile_y;
+    a.tiles_x = step32_tiles_x(ctx);
+    a.ntiles = step32_tiles(ctx);
+    a.Iin = ctx->I[from].as<float>();
+    a.Iout = ctx->I[from ^ 1].as<float>();
+    a.rec = ctx->rec.as<uint4>();
+    a.side = ctx->side.as<float4>();
+    a.ia3 = ctx->ia3.as<float>();
+    a.flags = ctx->flags.as<uint8_t>();
+    a.u1 = ctx->cu1.as<float>();
+    a.u2 = ctx->cu2.as<float>();
+    a.lor = ctx->clor.as<float>();
+    a.adt = ctx->cadt.as<float>();
+    a.eta = ctx->ceta.as<float>();
+    a.k0 = ctx->ck0.as<float>();
+    a.k3 = ctx->ck3.as<float>();
+    a.ka = ctx->cka.as<float>();
+    a.mom = ctx->mom.as<float>();
+    a.iter_sum = cnt;
+    a.iter_max = reinterpret_cast<unsigned int *>(cnt + 1);
+    a.fault = ctx->fault;
+    a.tiles = ctx->tile_ctr.as<unsigned>();
+    a.in_map = ctx->in_map[from];
+    return a;
+}
+
+// Sets the tile shape of the precision-form fixed step: the TMA maps of the
+// state buffers for its patch, and the persistent grid at its occupancy.
+int set_step32_tile(grlbm_ctx *ctx, int tx, int ty)
+{
+    const int dp = (int)ctx->sl.sp;
+    if (tx < 1 || ty < 1 || tx > 64 || ty > 64)
+        return fail(ctx, GRLBM_ERR_ARGUMENT, "tile %dx%d: each side must be in [1, 64]", tx, ty);
+    const size_t smem = step32_smem(tx, ty, dp);
+    if (smem > (size_t)kStep32MaxSmem)
+        return fail(ctx, GRLBM_ERR_ARGUMENT, "tile %dx%d: its patch of %d directions needs %zu bytes of shared memory",
+                    tx, ty, ctx->st.n, smem);
+    const bool curved = ctx->run.streaming_type == GRLBM_CURVED_FIXED;
+    int per_sm = 0, sms = 0;
+    CU(step32_occupancy(ctx->passes, curved, false, smem, &per_sm));
+    CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+    if (per_sm < 1)
+        return fail(ctx, GRLBM_ERR_ARGUMENT, "tile %dx%d does not fit on an SM", tx, ty);
+    for (int k = 0; k < 2; k++)
+    {
+        const cudaError_t e =
+            encode_state_map32(&ctx->in_map[k], ctx->I[k].as<float>(), ctx->geo.nx, ctx->geo.ny, dp, tx, ty);
+        if (e != cudaSuccess)
+            return fail(ctx, GRLBM_ERR_CUDA, "TMA map of the state: %s", cudaGetErrorString(e));
+    }
+    ctx->tile_x = tx;
+    ctx->tile_y = ty;
+    ctx->step_blocks = per_sm * sms;
+    invalidate_graphs(ctx);
+    return GRLBM_OK;
+}
+
+// The default tile: the largest candidate whose patch buffers leave the
+// register-limited occupancy of the step kernel unchanged.
+int default_step32_tile(grlbm_ctx *ctx)
+{
+    static const int cand[][2] = {{8, 8}, {8, 4}, {4, 4}, {4, 2}, {2, 2}, {1, 1}};
+    const bool curved = ctx->run.streaming_type == GRLBM_CURVED_FIXED;
+    int reg_limit = 0;
+    CU(step32_occupancy(ctx->passes, curved, false, 0, &reg_limit));
+    for (const auto &c : cand)
+    {
+        const size_t smem = step32_smem(c[0], c[1], (int)ctx->sl.sp);
+        int per_sm = 0;
+        if (smem > (size_t)kStep32MaxSmem)
+            continue;
+        CU(step32_occupancy(ctx->passes, curved, false, smem, &per_sm));
+        if (per_sm >= reg_limit || (c[0] == 1 && per_sm >= 1))
+            return set_step32_tile(ctx, c[0], c[1]);
+    }
+    return fail(ctx, GRLBM_ERR_ARGUMENT, "no tile of %d directions fits on an SM", ctx->st.n);
+}
+
+bool is_fixed32(const grlbm_ctx *ctx)
+{
+    return ctx->fp32 && (ctx->run.streaming_type == GRLBM_FLAT_FIXED || ctx->run.streaming_type == GRLBM_CURVED_FIXED);
 }
 
 // Arguments of the plain step that reads intensity buffer `from`.
@@ -298,9 +399,11 @@ int enqueue_step(grlbm_ctx *ctx, int from)
         if (ctx->run.keep_source_nodes_active && ctx->nsrc > 0)
             launch_sources32(ctx->I[from].as<float>(), ctx->sl, ctx->st.n, ctx->src_nodes.as<int64_t>(),
                              ctx->src_vals.as<float>(), ctx->nsrc, ctx->stream);
-        PrecStepArgs a = prec_args(ctx, from);
-        if (is_adaptive(ctx))
+        if (!is_adaptive(ctx))
+            launch_step32(step32_args(ctx, from), ctx->dirs, curved, ctx->passes, ctx->step_blocks, ctx->stream);
+        else
         {
+            PrecStepArgs a = prec_args(ctx, from);
             // LoadInitialData also sets the source nodes' angles (src/Radiation.cpp:170-176)
             if (ctx->run.keep_source_nodes_active && ctx->nsrc_ang > 0)
                 launch_sources64(ctx->ang[from].as<double>(), ctx->gd.nxy, 1, ctx->src_ang_nodes.as<int64_t>(),
@@ -311,8 +414,6 @@ int enqueue_step(grlbm_ctx *ctx, int from)
             a.rot_new = ctx->rot.as<float2>() + ctx->gd.nxy;
             launch_step_prec_adaptive(a, ctx->dirs, curved, ctx->stream);
         }
-        else
-            launch_step_prec(a, ctx->dirs, curved, ctx->stream);
     }
     else
     {
@@ -377,7 +478,7 @@ int build_records(grlbm_ctx *ctx)
     da.rot_c = approx_cos(0.0);
     da.rot_s = approx_sin(0.0);
     da.rec64 = ctx->fp32 ? nullptr : ctx->rec.as<double4>();
-    da.rec32 = ctx->fp32 ? ctx->rec.as<float4>() : nullptr;
+    da.rec32 = ctx->fp32 ? ctx->rec.as<uint4>() : nullptr;
     da.side32 = ctx->fp32 ? ctx->side.as<float4>() : nullptr;
     da.q = ctx->dirs.q;
     da.p = ctx->dirs.p;
@@ -505,9 +606,14 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
     const int maxdir = kMaxDirs;
     if (run->n_dir < 4 || run->n_dir > maxdir)
         return fail(nullptr, GRLBM_ERR_ARGUMENT, "n_dir must be in [4, %d]", maxdir);
+    const bool adaptive_type =
+        run->streaming_type == GRLBM_FLAT_ADAPTIVE || run->streaming_type == GRLBM_CURVED_ADAPTIVE;
     if (run->precision == GRLBM_PRECISION_FP32 &&
-        (double)StateLayout::padded32(grid->nx_ + 2, grid->ny_ + 2).plane * (double)run->n_dir >= 2147483648.0)
-        return fail(nullptr, GRLBM_ERR_ARGUMENT, "the precision form indexes with 32 bits: nx*ny*n_dir must be < 2^31");
+        (adaptive_type ? (double)StateLayout::padded32(grid->nx_ + 2, grid->ny_ + 2).plane * (double)run->n_dir
+                       : (double)(grid->nx_ + 2) * (double)(grid->ny_ + 2) *
+                             (double)StateLayout::direction_pitch(run->n_dir)) >= 2147483648.0)
+        return fail(nullptr, GRLBM_ERR_ARGUMENT,
+                    "the precision form indexes its state with 32 bits: it must hold fewer than 2^31 values");
     if (run->n_fourier < 1 || run->n_fourier > kMaxFourier)
         return fail(nullptr, GRLBM_ERR_ARGUMENT, "n_fourier must be in [1, %d]", kMaxFourier);
     if (run->initial_data_type != GRLBM_MOMENTS && run->initial_data_type != GRLBM_INTENSITIES)
@@ -794,8 +900,9 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
     TRY(upload(ctx, ctx->coef, identity_coefficients(ctx)));
 
     // state
-    ctx->sl = ctx->fp32 ? StateLayout::padded32(G.nx, G.ny) : StateLayout::dense(G.nx, G.ny);
-    const size_t ib = (size_t)ctx->sl.plane * nd * tsize(ctx);
+    ctx->sl = !ctx->fp32 ? StateLayout::dense(G.nx, G.ny)
+                         : (is_adaptive(ctx) ? StateLayout::padded32(G.nx, G.ny) : StateLayout::cell_major32(G.nx, nd));
+    const size_t ib = (size_t)ctx->sl.elements(G.ny, nd) * tsize(ctx);
     if (ctx->fp32)
     {
         if (cudaHostAlloc(reinterpret_cast<void **>(&ctx->fault), sizeof(unsigned),
@@ -812,17 +919,21 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
     if (ctx->fp32)
         TRY(alloc(ctx, ctx->side, (size_t)ctx->ncell * nd * sizeof(float4)));
     TRY(alloc(ctx, ctx->counters, 8 * sizeof(unsigned long long)));
+    TRY(alloc(ctx, ctx->tile_ctr, 2 * sizeof(unsigned)));
+    cudaMemset(ctx->tile_ctr.p, 0, ctx->tile_ctr.bytes);
     TRY(alloc(ctx, ctx->energy_partial, kPartialBlocks * sizeof(double)));
     TRY(alloc(ctx, ctx->energy_out, sizeof(double)));
     cudaMemset(ctx->I[0].p, 0, ib);
     cudaMemset(ctx->I[1].p, 0, ib);
-    if (ctx->fp32)
-        for (int k = 0; k < 2; k++)
-        {
-            const cudaError_t e = encode_state_map(&ctx->in_map[k], ctx->I[k].as<float>(), ctx->sl, G.ny, nd);
-            if (e != cudaSuccess)
-                return fail(nullptr, GRLBM_ERR_CUDA, "TMA map of the state: %s", cudaGetErrorString(e));
-        }
+    if (is_fixed32(ctx))
+    {
+        ctx->passes = step32_passes(nd);
+        if (ctx->passes < 1)
+            return fail(nullptr, GRLBM_ERR_ARGUMENT, "n_dir %d exceeds the precision step's passes", nd);
+        if (prepare_step32() != cudaSuccess)
+            return fail(nullptr, GRLBM_ERR_CUDA, "cannot reserve shared memory for the precision step");
+        TRY(default_step32_tile(ctx));
+    }
     if (is_adaptive(ctx))
     {
         // rotationAngle and rotationAngleNew start at zero (src/Radiation.cpp:3-60)
@@ -848,9 +959,8 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
     // fields default to zero (the reference's buffers are value-initialised)
     std::vector<double> zeros(nxy, 0.0);
     TRY(grlbm_set_fields(ctx, zeros.data(), zeros.data(), zeros.data(), zeros.data(), zeros.data(), zeros.data()));
-    const int smem = (int)(ctx->fp32 ? step_prec_smem(nd) : 0);
-    if ((ctx->fp32 ? prepare_step_prec(smem) : prepare_step_plain(smem)) != cudaSuccess)
-        return fail(nullptr, GRLBM_ERR_CUDA, "cannot reserve %d bytes of shared memory for the step kernel", smem);
+    if (!ctx->fp32 && prepare_step_plain(0) != cudaSuccess)
+        return fail(nullptr, GRLBM_ERR_CUDA, "cannot reserve shared memory for the step kernel");
     if (cudaDeviceSynchronize() != cudaSuccess)
         return fail(nullptr, GRLBM_ERR_CUDA, "device error during set-up");
 #undef TRY
@@ -1435,7 +1545,8 @@ int grlbm_row_bytes(const grlbm_ctx *ctx, int64_t *bytes)
 {
     if (!ctx || !bytes)
         return GRLBM_ERR_ARGUMENT;
-    *bytes = ctx->sl.pitch * (int64_t)ctx->st.n * (int64_t)tsize(ctx);
+    *bytes = ctx->sl.sp == 1 ? ctx->sl.pitch * (int64_t)ctx->st.n * (int64_t)tsize(ctx)
+                             : ctx->sl.pitch * ctx->sl.sp * (int64_t)tsize(ctx);
     return GRLBM_OK;
 }
 
@@ -1449,7 +1560,19 @@ int grlbm_copy_rows(grlbm_ctx *ctx, int64_t j_first, int64_t n, void *buffer, in
     if (n == 0)
         return GRLBM_OK;
     cudaSetDevice(ctx->device);
-    const size_t es = tsize(ctx), width = (size_t)n * ctx->sl.pitch * es, pitch = (size_t)ctx->sl.plane * es;
+    const size_t es = tsize(ctx);
+    if (ctx->sl.sp != 1)
+    {
+        // cell-major: the rows are one contiguous run
+        const size_t row = (size_t)ctx->sl.pitch * (size_t)ctx->sl.sp * es;
+        char *state = static_cast<char *>(ctx->I[ctx->cur].p) + (size_t)j_first * row;
+        if (to_buffer)
+            CU(cudaMemcpyAsync(buffer, state, (size_t)n * row, cudaMemcpyDeviceToDevice, ctx->stream));
+        else
+            CU(cudaMemcpyAsync(state, buffer, (size_t)n * row, cudaMemcpyDeviceToDevice, ctx->stream));
+        return GRLBM_OK;
+    }
+    const size_t width = (size_t)n * ctx->sl.pitch * es, pitch = (size_t)ctx->sl.plane * es;
     char *state = static_cast<char *>(ctx->I[ctx->cur].p) + (size_t)j_first * ctx->sl.pitch * es;
     if (to_buffer)
         CU(cudaMemcpy2DAsync(buffer, width, state, pitch, width, (size_t)ctx->st.n, cudaMemcpyDeviceToDevice,
@@ -1457,6 +1580,28 @@ int grlbm_copy_rows(grlbm_ctx *ctx, int64_t j_first, int64_t n, void *buffer, in
     else
         CU(cudaMemcpy2DAsync(state, pitch, buffer, width, width, (size_t)ctx->st.n, cudaMemcpyDeviceToDevice,
                              ctx->stream));
+    return GRLBM_OK;
+}
+
+int grlbm_set_tile_shape(grlbm_ctx *ctx, int32_t tile_x, int32_t tile_y)
+{
+    if (!ctx)
+        return GRLBM_ERR_ARGUMENT;
+    if (!is_fixed32(ctx))
+        return fail(ctx, GRLBM_ERR_UNSUPPORTED, "tiles are a setting of the precision form's fixed streaming step");
+    cudaSetDevice(ctx->device);
+    CU(cudaStreamSynchronize(ctx->stream));
+    return set_step32_tile(ctx, tile_x, tile_y);
+}
+
+int grlbm_get_tile_shape(const grlbm_ctx *ctx, int32_t *tile_x, int32_t *tile_y)
+{
+    if (!ctx || !tile_x || !tile_y)
+        return GRLBM_ERR_ARGUMENT;
+    if (!is_fixed32(ctx))
+        return GRLBM_ERR_UNSUPPORTED;
+    *tile_x = ctx->tile_x;
+    *tile_y = ctx->tile_y;
     return GRLBM_OK;
 }
 
@@ -1581,10 +1726,11 @@ struct grlbm_batch
     int device = 0;
     cudaStream_t stream = nullptr;
     std::vector<grlbm_ctx *> ctx;
-    std::vector<BatchItem> items; // in launch order
-    std::vector<int> order;       // items[k] is context order[k]
-    DevBuf d_items, d_first, d_dirs;
-    int total_tiles = 0, smem = 0, blocks_per_sm_max = 1, blocks_per_sm = 1, sms = 1;
+    std::vector<Batch32Item> items; // in launch order
+    std::vector<int> order;         // items[k] is context order[k]
+    DevBuf d_items, d_first, d_dirs, counters;
+    int total_tiles = 0, passes = 1, patch_stride = 0, blocks_per_sm_max = 1, blocks_per_sm = 1, sms = 1;
+    size_t smem = 0;
     int largest_first = 0;
     int flip = 0; // parity of the steps taken since the items were built
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
@@ -1642,11 +1788,36 @@ void batch_drop_graphs(grlbm_batch *b)
         }
 }
 
-// (Re)build the launch list from the contexts' current buffers, in the
-// chosen order, and upload it.
+// Passes, shared memory and occupancy of the persistent kernel for the
+// problems' current tile shapes.
+int batch_geometry(grlbm_batch *b)
+{
+    b->passes = 1;
+    b->patch_stride = 0;
+    for (grlbm_ctx *c : b->ctx)
+    {
+        b->passes = std::max(b->passes, c->passes);
+        b->patch_stride = std::max(b->patch_stride, step32_patch_stride(c->tile_x, c->tile_y, (int)c->sl.sp));
+    }
+    b->smem = step32_smem_base() + (size_t)b->patch_stride * kStep32Warps;
+    if (b->smem > (size_t)kStep32MaxSmem)
+        return bfail(b, GRLBM_ERR_ARGUMENT, "the batch's largest patch needs %zu bytes of shared memory", b->smem);
+    BCU(step32_occupancy(b->passes, true, true, b->smem, &b->blocks_per_sm_max));
+    if (b->blocks_per_sm_max < 1)
+        return bfail(b, GRLBM_ERR_CUDA, "the batched kernel does not fit on an SM");
+    if (b->blocks_per_sm > b->blocks_per_sm_max)
+        b->blocks_per_sm = b->blocks_per_sm_max;
+    return GRLBM_OK;
+}
+
+// (Re)build the launch list from the contexts' current buffers and tiles, in
+// the chosen order, and upload it.
 int batch_build(grlbm_batch *b)
 {
     const int n = (int)b->ctx.size();
+    int rc = batch_geometry(b);
+    if (rc)
+        return rc;
     std::vector<int> order(n);
     for (int k = 0; k < n; k++)
         order[k] = k;
@@ -1656,26 +1827,24 @@ int batch_build(grlbm_batch *b)
             return a->ncell * a->st.n > c->ncell * c->st.n;
         });
     b->order = order;
-    b->items.assign(n, BatchItem{});
+    b->items.assign(n, Batch32Item{});
     std::vector<int> first(n + 1, 0);
     const DirTable *dirs = b->d_dirs.as<DirTable>();
     for (int k = 0; k < n; k++)
     {
         grlbm_ctx *c = b->ctx[order[k]];
-        BatchItem &it = b->items[k];
-        it.a[0] = prec_args(c, 0);
-        it.a[1] = prec_args(c, 1);
+        Batch32Item &it = b->items[k];
+        it.a[0] = step32_args(c, 0);
+        it.a[1] = step32_args(c, 1);
         it.dt = dirs + order[k];
-        it.tiles_x = step_prec_tiles_x(c->gd.nx_);
-        it.tiles_y = step_prec_tiles_y(c->gd.jhi - c->gd.jlo);
         it.curved = c->run.streaming_type == GRLBM_CURVED_FIXED;
         it.cur0 = c->cur;
-        first[k + 1] = first[k] + it.tiles_x * it.tiles_y;
+        first[k + 1] = first[k] + step32_tiles(c);
     }
     b->total_tiles = first[n];
-    if (alloc(nullptr, b->d_items, n * sizeof(BatchItem)) || alloc(nullptr, b->d_first, (n + 1) * sizeof(int)))
+    if (alloc(nullptr, b->d_items, n * sizeof(Batch32Item)) || alloc(nullptr, b->d_first, (n + 1) * sizeof(int)))
         return bfail(b, GRLBM_ERR_CUDA, "cannot allocate the batch launch list");
-    BCU(cudaMemcpy(b->d_items.p, b->items.data(), n * sizeof(BatchItem), cudaMemcpyHostToDevice));
+    BCU(cudaMemcpy(b->d_items.p, b->items.data(), n * sizeof(Batch32Item), cudaMemcpyHostToDevice));
     BCU(cudaMemcpy(b->d_first.p, first.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice));
     b->flip = 0;
     batch_drop_graphs(b);
@@ -1691,8 +1860,9 @@ int batch_enqueue(grlbm_batch *b, int n, int flip)
     if (b->blocks_per_sm > 0)
     {
         for (int s = 0; s < n; s++)
-            launch_step_batch(b->d_items.as<BatchItem>(), b->d_first.as<int>(), (int)b->items.size(),
-                              b->total_tiles, flip ^ (s & 1), b->sms * b->blocks_per_sm, b->smem, b->stream);
+            launch_step_batch32(b->d_items.as<Batch32Item>(), b->d_first.as<int>(), (int)b->items.size(),
+                                b->total_tiles, flip ^ (s & 1), b->counters.as<unsigned>(), b->passes,
+                                b->sms * b->blocks_per_sm, b->smem, b->patch_stride, b->stream);
         return GRLBM_OK;
     }
     BCU(cudaEventRecord(b->fork, b->stream));
@@ -1701,8 +1871,8 @@ int batch_enqueue(grlbm_batch *b, int n, int flip)
         grlbm_ctx *c = b->ctx[b->order[k]];
         BCU(cudaStreamWaitEvent(c->stream, b->fork, 0));
         for (int s = 0; s < n; s++)
-            launch_step_prec(prec_args(c, b->items[k].cur0 ^ flip ^ (s & 1)), c->dirs, b->items[k].curved,
-                             c->stream);
+            launch_step32(step32_args(c, b->items[k].cur0 ^ flip ^ (s & 1)), c->dirs, b->items[k].curved != 0,
+                          c->passes, c->step_blocks, c->stream);
         BCU(cudaEventRecord(b->join[k], c->stream));
         BCU(cudaStreamWaitEvent(b->stream, b->join[k], 0));
     }
@@ -1771,6 +1941,25 @@ int batch_steps(grlbm_batch *b, int n)
             return bfail(b, GRLBM_ERR_CUDA, "problem %p: %s", (void *)c, c->err.c_str());
     return GRLBM_OK;
 }
+
+// Times `trial_steps` batch steps (after one untimed step); -1 on failure.
+float batch_time(grlbm_batch *b, int trial_steps, cudaEvent_t e0, cudaEvent_t e1, int *rc)
+{
+    if ((*rc = batch_build(b)) || (*rc = batch_enqueue(b, 1, 0)))
+        return -1.f;
+    cudaEventRecord(e0, b->stream);
+    if ((*rc = batch_enqueue(b, trial_steps, 1)))
+        return -1.f;
+    cudaEventRecord(e1, b->stream);
+    if (cudaStreamSynchronize(b->stream) != cudaSuccess)
+    {
+        *rc = bfail(b, GRLBM_ERR_CUDA, "autotune: trial steps failed");
+        return -1.f;
+    }
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    return ms;
+}
 } // namespace
 
 extern "C" {
@@ -1782,7 +1971,6 @@ int grlbm_batch_create(grlbm_ctx *const *ctxs, int32_t n, grlbm_batch **out)
     *out = nullptr;
     std::unique_ptr<grlbm_batch> owner(new grlbm_batch);
     grlbm_batch *b = owner.get();
-    int max_nd = 0;
     for (int k = 0; k < n; k++)
     {
         grlbm_ctx *c = ctxs[k];
@@ -1803,7 +1991,6 @@ int grlbm_batch_create(grlbm_ctx *const *ctxs, int32_t n, grlbm_batch **out)
         for (int j = 0; j < k; j++)
             if (ctxs[j] == c)
                 return bfail(nullptr, GRLBM_ERR_ARGUMENT, "grlbm_batch_create: context %d appears twice", k);
-        max_nd = std::max(max_nd, c->st.n);
         b->ctx.push_back(c);
     }
     b->device = ctxs[0]->device;
@@ -1813,19 +2000,20 @@ int grlbm_batch_create(grlbm_ctx *const *ctxs, int32_t n, grlbm_batch **out)
     b->join.assign(n, nullptr);
     for (int k = 0; k < n; k++)
         BCU(cudaEventCreateWithFlags(&b->join[k], cudaEventDisableTiming));
-    b->smem = (int)step_prec_smem(max_nd);
-    BCU(prepare_step_batch(b->smem, &b->blocks_per_sm_max));
-    if (b->blocks_per_sm_max < 1)
-        return bfail(nullptr, GRLBM_ERR_CUDA, "grlbm_batch_create: the batched kernel does not fit on an SM");
-    b->blocks_per_sm = b->blocks_per_sm_max;
     BCU(cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, b->device));
+    if (alloc(nullptr, b->counters, 2 * sizeof(unsigned)))
+        return bfail(nullptr, GRLBM_ERR_CUDA, "grlbm_batch_create: cannot allocate the tile counters");
+    BCU(cudaMemset(b->counters.p, 0, b->counters.bytes));
     std::vector<DirTable> dirs(n);
     for (int k = 0; k < n; k++)
         dirs[k] = ctxs[k]->dirs;
     if (upload(nullptr, b->d_dirs, dirs))
         return bfail(nullptr, GRLBM_ERR_CUDA, "grlbm_batch_create: cannot upload the direction tables");
-    int rc = batch_build(b);
+    int rc = batch_geometry(b);
     if (rc)
+        return bfail(nullptr, rc, "%s", b->err.c_str());
+    b->blocks_per_sm = b->blocks_per_sm_max;
+    if ((rc = batch_build(b)))
         return bfail(nullptr, rc, "%s", b->err.c_str());
     *out = owner.release();
     return GRLBM_OK;
@@ -1857,9 +2045,12 @@ int grlbm_batch_set_shape(grlbm_batch *b, int32_t blocks_per_sm, int32_t largest
 {
     if (!b)
         return GRLBM_ERR_ARGUMENT;
+    cudaSetDevice(b->device);
+    int rc = batch_geometry(b);
+    if (rc)
+        return rc;
     if (blocks_per_sm < 0 || blocks_per_sm > b->blocks_per_sm_max)
         return bfail(b, GRLBM_ERR_ARGUMENT, "blocks_per_sm must be in [0, %d]", b->blocks_per_sm_max);
-    cudaSetDevice(b->device);
     for (grlbm_ctx *c : b->ctx)
         BCU(cudaStreamSynchronize(c->stream));
     b->blocks_per_sm = blocks_per_sm;
@@ -1895,14 +2086,14 @@ int grlbm_batch_autotune(grlbm_batch *b, int32_t trial_steps, int32_t *blocks_pe
             BCU(cudaMemcpy(saved[3 * k + q]->p, src[q]->p, src[q]->bytes, cudaMemcpyDeviceToDevice));
         }
     }
-    const int flip0 = b->flip;
-    float best = 0.f;
-    int best_bps = b->blocks_per_sm, best_lf = b->largest_first;
     cudaEvent_t e0, e1;
     BCU(cudaEventCreate(&e0));
     BCU(cudaEventCreate(&e1));
-    // persistent launches (largest problem first or not, at each resident
-    // block count), and the problems' own kernels launched concurrently
+    // 1. the launch shape: persistent launches (largest problem first or not,
+    //    at each resident block count down to two below the limit), or the
+    //    problems' own kernels launched concurrently
+    float best = -1.f;
+    int best_bps = b->blocks_per_sm, best_lf = b->largest_first;
     std::vector<std::pair<int, int>> shapes;
     for (int lf = 0; lf <= 1; lf++)
         for (int bps = b->blocks_per_sm_max; bps >= 1 && bps >= b->blocks_per_sm_max - 2; bps--)
@@ -1912,23 +2103,63 @@ int grlbm_batch_autotune(grlbm_batch *b, int32_t trial_steps, int32_t *blocks_pe
     {
         b->blocks_per_sm = shape.first;
         b->largest_first = shape.second;
-        if ((rc = batch_build(b)))
+        const float ms = batch_time(b, trial_steps, e0, e1, &rc);
+        if (rc)
             break;
-        if ((rc = batch_enqueue(b, 1, 0))) // warm-up
-            break;
-        cudaEventRecord(e0, b->stream);
-        if ((rc = batch_enqueue(b, trial_steps, 1)))
-            break;
-        cudaEventRecord(e1, b->stream);
-        if (cudaStreamSynchronize(b->stream) != cudaSuccess)
-        {
-            rc = bfail(b, GRLBM_ERR_CUDA, "autotune: trial steps failed");
-            break;
-        }
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, e0, e1);
-        if (best == 0.f || ms < best)
+        if (best < 0.f || ms < best)
             best = ms, best_bps = shape.first, best_lf = shape.second;
+    }
+    b->blocks_per_sm = best_bps;
+    b->largest_first = best_lf;
+    // 2. the tile of each size class (problems of one grid size and
+    //    direction count share a tile), largest class first: each class tries
+    //    the candidate tiles with the others fixed, and keeps the fastest
+    if (!rc)
+    {
+        std::vector<std::pair<int64_t, std::vector<grlbm_ctx *>>> classes;
+        for (grlbm_ctx *c : b->ctx)
+        {
+            const int64_t key = (c->gd.nx_ * 65536 + c->gd.ny_) * 512 + c->st.n;
+            auto it = std::find_if(classes.begin(), classes.end(), [&](const auto &x) { return x.first == key; });
+            if (it == classes.end())
+                classes.push_back({key, {c}});
+            else
+                it->second.push_back(c);
+        }
+        std::stable_sort(classes.begin(), classes.end(), [](const auto &x, const auto &y) {
+            const grlbm_ctx *a = x.second[0], *c = y.second[0];
+            return a->ncell * a->st.n * (int64_t)x.second.size() > c->ncell * c->st.n * (int64_t)y.second.size();
+        });
+        static const int cand[][2] = {{2, 2}, {4, 2}, {4, 4}, {8, 4}, {4, 8}, {8, 8}, {16, 4}, {16, 8}};
+        for (auto &cls : classes)
+        {
+            grlbm_ctx *c0 = cls.second[0];
+            int bx = c0->tile_x, by = c0->tile_y;
+            for (const auto &t : cand)
+            {
+                if (t[0] == bx && t[1] == by)
+                    continue;
+                if (step32_smem(t[0], t[1], (int)c0->sl.sp) > (size_t)kStep32MaxSmem)
+                    continue;
+                for (grlbm_ctx *c : cls.second)
+                    if ((rc = set_step32_tile(c, t[0], t[1])))
+                        break;
+                if (rc)
+                    break;
+                const float ms = batch_time(b, trial_steps, e0, e1, &rc);
+                if (rc)
+                    break;
+                if (ms < best)
+                    best = ms, bx = t[0], by = t[1];
+            }
+            if (rc)
+                break;
+            for (grlbm_ctx *c : cls.second)
+                if ((rc = set_step32_tile(c, bx, by)))
+                    break;
+            if (rc)
+                break;
+        }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -1942,15 +2173,12 @@ int grlbm_batch_autotune(grlbm_batch *b, int32_t trial_steps, int32_t *blocks_pe
     }
     if (rc)
         return rc;
-    b->blocks_per_sm = best_bps;
-    b->largest_first = best_lf;
-    (void)flip0;
     if ((rc = batch_build(b)))
         return rc;
     if (blocks_per_sm)
-        *blocks_per_sm = best_bps;
+        *blocks_per_sm = b->blocks_per_sm;
     if (largest_first)
-        *largest_first = best_lf;
+        *largest_first = b->largest_first;
     return GRLBM_OK;
 }
 

@@ -674,7 +674,7 @@ __global__ void k_moments_from_I(const T *I, int64_t nxy, StateLayout L, int nd,
         const double wd = __ldg(w + d);
         if (wd == 0.0)
             continue;
-        double v = (double)I[(int64_t)d * L.plane + sij];
+        double v = (double)I[sij * L.sp + (int64_t)d * L.plane];
         if (scale)
             v = v / (double)scale[ij];
         const double c1 = __ldg(n1 + d), c2 = __ldg(n2 + d);
@@ -700,7 +700,9 @@ __global__ void k_sources(T *I, StateLayout L, int nd, const int64_t *nodes, con
         return;
     const int64_t s = tid / nd;
     const int d = (int)(tid - s * nd);
-    I[(int64_t)d * L.plane + L.at(nodes[s])] = vals[tid];
+    I[L.elem(nodes[s], d)] = vals[tid];
+    if (d < L.mirror) // the cell-major state repeats the first directions after the last
+        I[L.elem(nodes[s], nd + d)] = vals[tid];
 }
 
 // Radiation::ComputeMomentsLF (src/Radiation.cpp:270-301)
@@ -807,7 +809,7 @@ __global__ void k_coef_k_major(const double *coef, double *coef_k, int64_t nxy, 
     coef_k[t] = coef[q * per + ij * nf + k];
 }
 
-// cell-major double [ij][d] <-> direction-major T [d][ij]
+// the boundary's cell-major double [ij][d] <-> a state buffer of layout L
 template <class T>
 __global__ void k_to_dirmajor(const double *in, T *out, int64_t nxy, StateLayout L, int nd, const float *scale)
 {
@@ -827,7 +829,12 @@ __global__ void k_to_dirmajor(const double *in, T *out, int64_t nxy, StateLayout
         const int d = d0 + r;
         const int64_t ij = ij0 + threadIdx.x;
         if (ij < nxy && d < nd)
-            out[(int64_t)d * L.plane + L.at(ij)] = scale ? (T)tile[threadIdx.x][r] * (T)scale[ij] : (T)tile[threadIdx.x][r];
+        {
+            const T v = scale ? (T)tile[threadIdx.x][r] * (T)scale[ij] : (T)tile[threadIdx.x][r];
+            out[L.elem(ij, d)] = v;
+            if (d < L.mirror) // the cell-major state repeats the first directions after the last
+                out[L.elem(ij, nd + d)] = v;
+        }
     }
 }
 template <class T>
@@ -841,8 +848,7 @@ __global__ void k_to_cellmajor(const T *in, double *out, int64_t nxy, StateLayou
         const int d = d0 + r;
         const int64_t ij = ij0 + threadIdx.x;
         if (ij < nxy && d < nd)
-            tile[threadIdx.x][r] = scale ? (double)in[(int64_t)d * L.plane + L.at(ij)] / (double)scale[ij]
-                                         : (double)in[(int64_t)d * L.plane + L.at(ij)];
+            tile[threadIdx.x][r] = scale ? (double)in[L.elem(ij, d)] / (double)scale[ij] : (double)in[L.elem(ij, d)];
     }
     __syncthreads();
     for (int r = threadIdx.y; r < 32; r += 8)

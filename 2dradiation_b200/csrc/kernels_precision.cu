@@ -1,45 +1,15 @@
-// Precision form of the radiation step: FP32 intensities and stream/collide
-// arithmetic (contracted FMAs allowed), Kahan-compensated FP32 moment sums,
-// on departure records derived from the FP64 geodesic tables.
-//
-// State: for curved streaming the stored intensity is J = I / alpha^3 (I
-// itself for flat streaming).  The reference multiplies each corner's
-// angular interpolation by (alpha_c / alpha_n)^3 after clamping it at zero
-// (src/Radiation.cpp:502-505, 342); as alpha_n^-3 > 0 commutes with the clamp,
-// gathering J gives the same value without loading alpha at every corner.
-//
-// Stream: one thread per interior cell loops over the directions, staged in
-// shared memory a chunk of planes at a time; each (cell, direction) reads its
-// 16-byte packed record (window row type, window start, blend t, corner code,
-// fx, fy, s^3 alpha_c^3), takes the window's weights W0 + t D from the
-// row-type table (the two cubic rows of IntensityAt pre-blended into a
-// 5-direction window), gathers the window at the 4 bilinear corners and
-// multiplies by s^3 alpha_c^3.  Offsets are 32-bit.
-//
-// Collide: the lambda iteration of src/Radiation.cpp:661-722 is affine in
-// the previous moments -- I_d = g_d S_d + h_d (eta + kappa0 E_ff + 3 kappa1
-// nFF_d . F_ff) -- so each iteration is evaluated on the six moments with
-// per-cell sums of the direction terms (O(1) per iteration instead of a pass
-// over the directions); the converged intensities are written in one final
-// pass, and the last iterate's moments -- the affine map's moments of exactly
-// those intensities -- are the stored moments.
+// Precision form of the adaptive streaming types (FlatAdaptive,
+// CurvedAdaptive): FP32 intensities and stream/collide arithmetic (contracted
+// FMAs allowed), Kahan-compensated FP32 moment sums, on a direction-major
+// FP32 state (J = I / alpha^3 for curved streaming).  The fixed streaming
+// types have their own kernel (kernels_step32.cu).  Also here: the bounded
+// mbarrier wait's self-test and the FP32 coefficient copy of adaptive
+// streaming.
 #include <cudaTypedefs.h>
 
 #include "approx_math.hpp"
 #include "device_common.cuh"
-
-// Tuning of the step kernels: resident blocks per SM the register budget is
-// sized for, and the unroll of the per-direction loop (the batch kernel,
-// which holds both streaming types, keeps the smaller one).
-#ifndef GRLBM_PREC_MIN_BLOCKS
-#define GRLBM_PREC_MIN_BLOCKS 5
-#endif
-#ifndef GRLBM_PREC_UNROLL
-#define GRLBM_PREC_UNROLL 4
-#endif
-#ifndef GRLBM_BATCH_UNROLL
-#define GRLBM_BATCH_UNROLL 1
-#endif
+#include "tma_util.cuh"
 
 namespace grlbm
 {
@@ -91,261 +61,6 @@ struct KMoments
     }
 };
 
-// Tile of cells per block and the shared-memory stage of the state around it:
-// a (kTileX + 2) x (kTileY + 2) patch of each direction plane, for a rolling
-// window of planes.  Chunk k covers directions [kChunk k, kChunk (k+1)) and
-// reads virtual planes [kChunk k - kBelow, kChunk k + kSpan - kBelow) (a
-// departure's angular window starts at most 3 directions below its own and
-// spans 5; plane v holds direction v mod nDir).  Plane v lives in ring slot
-// (v + kBelow) mod kRing; slots 0..kMirror-1 are also kept in slots
-// kRing..kRing+kMirror-1, so the 5 planes of any window sit at consecutive
-// slots and a window's taps are fixed offsets from one address.  The next
-// chunk's planes are brought in while the current chunk runs, into slots it
-// does not read.
-//
-// Staging is done by the TMA engine: the state is one 2D tensor of
-// {pitch, ny * nDir} floats (rows padded to 16 bytes), and each patch plane
-// is one tensor copy (cp.async.bulk.tensor) of a kBoxX x kPatchY box into its
-// slot, completing on the block's mbarrier.  One thread issues a chunk's
-// copies; every thread waits on the barrier with a time limit.  Box columns
-// past the grid's row (x >= pitch) arrive as zeros and rows past the last
-// plane too; none of them is read.
-#ifndef GRLBM_PREC_TILE_X
-#define GRLBM_PREC_TILE_X 32
-#endif
-constexpr int kTileX = GRLBM_PREC_TILE_X, kTileY = kStepBlock / GRLBM_PREC_TILE_X;
-static_assert(kTileX * kTileY == kStepBlock, "tile = block");
-static_assert(kTileX % 4 == 0, "tile origins on 16-byte boundaries");
-constexpr int kPatchX = kTileX + 2, kPatchY = kTileY + 2;
-constexpr int kRing = 32, kMirror = kTaps - 1;
-static_assert(kSpan + kChunk <= kRing && (kRing & (kRing - 1)) == 0, "ring");
-constexpr int kRingSlots = kRing + kMirror;
-// the box: a patch row rounded up to 16 bytes, the slot: a box rounded up to
-// 128 bytes (the alignment of a tensor copy's shared destination)
-constexpr int kBoxX = (kPatchX + 3) / 4 * 4;
-constexpr unsigned kBoxBytes = kBoxX * kPatchY * sizeof(float);
-constexpr int kSlot = (kBoxX * kPatchY + 31) / 32 * 32;
-constexpr int kRingAlign = 128;
-// time limits of a staging wait (copies land within microseconds), and of
-// the drain of copies in flight after one has run out
-constexpr unsigned long long kWaitNs = 200000000ull, kDrainNs = 1000000ull;
-
-__device__ __forceinline__ unsigned smem_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
-    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-}
-// the issuing thread's arrival on the current phase, announcing `bytes` of copies
-__device__ __forceinline__ void mbar_arrive_expect(unsigned bar, unsigned bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
-}
-// one box of a 2D tensor at element coordinates (x, y) into shared memory
-__device__ __forceinline__ void tma_load_2d(unsigned dst, const CUtensorMap *map, int x, int y, unsigned bar)
-{
-    asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
-        "[%4];\n" ::"r"(dst),
-        "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(bar)
-        : "memory");
-}
-__device__ __forceinline__ bool mbar_test(unsigned bar, unsigned parity)
-{
-    unsigned done;
-    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, "
-                 "p;\n}\n"
-                 : "=r"(done)
-                 : "r"(bar), "r"(parity)
-                 : "memory");
-    return done != 0;
-}
-__device__ __forceinline__ unsigned long long global_ns()
-{
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-// Wait for the phase of the given parity to complete, for limit_ns at most;
-// false at once when another block has already raised the fault word.
-__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity, unsigned long long limit_ns,
-                                          const unsigned *fault)
-{
-    if (mbar_test(bar, parity))
-        return true;
-    if (fault && *reinterpret_cast<const volatile unsigned *>(fault))
-        return false;
-    const unsigned long long t0 = global_ns();
-    do
-    {
-        if (mbar_test(bar, parity))
-            return true;
-    } while (global_ns() - t0 < limit_ns);
-    return false;
-}
-
-// the tile's stage: shared addresses of slot 0 and of the mbarrier, and the
-// patch origin (node coordinates)
-struct Stage
-{
-    unsigned ring, bar;
-    int x0, y0;
-};
-
-// Shared layout: the mbarrier (16 bytes), then the ring from the next
-// kRingAlign boundary, the row-type table and the direction coefficients.
-constexpr int kBarBytes = 16;
-__device__ __forceinline__ float *ring_base(unsigned char *smem_raw)
-{
-    const unsigned at = smem_addr(smem_raw) + kBarBytes;
-    return reinterpret_cast<float *>(smem_raw + kBarBytes + ((kRingAlign - (at & (kRingAlign - 1))) & (kRingAlign - 1)));
-}
-
-// Stage virtual planes [v0, v0 + n) into their ring slots (and mirrors):
-// one phase of the mbarrier, issued by thread 0.
-__device__ __forceinline__ void stage_planes(const PrecStepArgs &a, const CUtensorMap *map, const Stage &st, int v0,
-                                             int n)
-{
-    if (threadIdx.x != 0)
-        return;
-    unsigned boxes = 0;
-    for (int p = 0; p < n; p++)
-        boxes += (((v0 + p + kBelow) & (kRing - 1)) < kMirror) ? 2u : 1u;
-    mbar_arrive_expect(st.bar, boxes * kBoxBytes);
-    int d = v0 % a.nd;
-    d = d < 0 ? d + a.nd : d;
-    for (int p = 0; p < n; p++)
-    {
-        const int sl = (v0 + p + kBelow) & (kRing - 1);
-        const int y = d * (int)a.g.ny + st.y0;
-        tma_load_2d(st.ring + (unsigned)(sl * kSlot) * 4u, map, st.x0, y, st.bar);
-        if (sl < kMirror)
-            tma_load_2d(st.ring + (unsigned)((sl + kRing) * kSlot) * 4u, map, st.x0, y, st.bar);
-        d = (d + 1 == a.nd) ? 0 : d + 1;
-    }
-}
-
-// The four bilinear corners of a 5-tap angular window read from global
-// memory, each clamped at zero: the rare departures whose corners or window
-// fall outside the staged patch (kept out of line: it is cold code).
-__device__ __noinline__ float4 window_corners_global(const float *__restrict__ I, unsigned plane, int nd, int base,
-                                                     unsigned c00, unsigned pitch, float w0, float w1, float w2,
-                                                     float w3, float w4)
-{
-    const float w[kTaps] = {w0, w1, w2, w3, w4};
-    const unsigned off[4] = {c00, c00 + pitch, c00 + 1u, c00 + pitch + 1u}; // corners 00 01 10 11
-    float cv[4];
-#pragma unroll
-    for (int q = 0; q < 4; q++)
-    {
-        float v = 0.f;
-        int dk = base;
-#pragma unroll
-        for (int k = 0; k < kTaps; k++)
-        {
-            v = fmaf(w[k], __ldg(I + (unsigned)dk * plane + off[q]), v);
-            dk = (dk + 1 == nd) ? 0 : dk + 1;
-        }
-        cv[q] = fmaxf(v, 0.f);
-    }
-    return make_float4(cv[0], cv[1], cv[2], cv[3]);
-}
-
-// One curved stream value from a side record {i_dep - i, j_dep - j, angle
-// coordinate, s^3 alpha_c^3}, all taps from global memory: the departures
-// whose packed record is marked far (cold code, kept out of line).
-__device__ __noinline__ float stream_curved_far(const float *__restrict__ Iin, const float4 *__restrict__ side,
-                                                unsigned plane, unsigned pitch, int nx, int ny, int nd, int ng,
-                                                const float *rowtab,
-                                                int q, int p, float inv_q, unsigned rec_index, int i, int j)
-{
-    const float4 r = side[rec_index];
-    const float fli = floorf(r.x), flj = floorf(r.y);
-    const float fx = r.x - fli, fy = r.y - flj;
-    const int i0 = min(max(i + (int)fli, 0), nx - 2);
-    const int j0 = min(max(j + (int)flj, 0), ny - 2);
-    const float z = r.z == r.z ? r.z : 0.f;
-    const float g = fminf(fmaxf(floorf(z), 0.f), (float)(ng - 1));
-    const float t = fminf(fmaxf(z - g, 0.f), 1.f);
-    const float m = floorf((g + 0.5f) * inv_q);
-    const int rt = min(max((int)fmaf(-m, (float)q, g), 0), q - 1);
-    const float *row = rowtab + rt * 12;
-    int base = (int)fmaf(m, (float)p, row[10]) % nd;
-    const float4 c = window_corners_global(Iin, plane, nd, base, (unsigned)i0 + (unsigned)j0 * pitch, pitch, fmaf(t, row[4], row[0]), fmaf(t, row[5], row[1]),
-                                           fmaf(t, row[6], row[2]), fmaf(t, row[7], row[3]),
-                                           fmaf(t, row[9], row[8]));
-    const float f0 = fmaf(fx, c.z - c.x, c.x);
-    const float f1 = fmaf(fx, c.w - c.y, c.y);
-    return r.w * fmaf(fy, f1 - f0, f0);
-}
-
-// One curved stream value (StreamCurvedFixed with IntensityAt,
-// src/Radiation.cpp:478-508, 322-343) from its packed record: the 4 bilinear
-// corners of the departure, each the 5-tap angular window (the two cubic
-// rows of the interpolation grid, src/Stencil.cpp:109-162, blended in t)
-// clamped at zero, then bilinear in (fx, fy) and scaled by s^3 alpha_c^3.
-// `cell` is the slot offset of the cell's lower-left neighbour.
-__device__ __forceinline__ float stream_curved(const PrecStepArgs &a, const DirTable &dt, const float *ring,
-                                               const float *rowtab, int d, const float4 &r, int cell,
-                                               unsigned rec_index, int i, int j)
-{
-    const unsigned word = __float_as_uint(r.x);
-    if (word >> packed::kFarBit)
-        return stream_curved_far(a.Iin, a.side, a.plane, a.pitch, (int)a.g.nx, (int)a.g.ny, a.nd, a.ng, rowtab, dt.q,
-                                 dt.p, dt.inv_q, rec_index, i, j);
-    const float t = (float)(word & ((1u << packed::kTBits) - 1u)) * (1.f / (float)(1u << packed::kTBits));
-    const float4 *row = reinterpret_cast<const float4 *>(rowtab + ((word >> packed::kTypeShift) & 31u) * 12);
-    const float4 R0 = row[0], R1 = row[1], R2 = row[2];
-    const float w0 = fmaf(t, R1.x, R0.x), w1 = fmaf(t, R1.y, R0.y), w2 = fmaf(t, R1.z, R0.z);
-    const float w3 = fmaf(t, R1.w, R0.w), w4 = fmaf(t, R2.y, R2.x);
-    // ring slot of the window's first plane: virtual plane d + dbase
-    const int slot = (d + (int)((word >> packed::kBaseShift) & 63u) - packed::kBaseBias + kBelow) & (kRing - 1);
-    const unsigned code = word >> packed::kCodeShift; // bit 31 is clear here
-    const float *p = ring + slot * kSlot + cell + (int)(code & 1u) + (int)(code >> 1) * kBoxX;
-#define GRLBM_WINDOW(o)                                                                                    \
-    fmaxf(fmaf(w4, p[4 * kSlot + (o)],                                                                     \
-               fmaf(w3, p[3 * kSlot + (o)], fmaf(w2, p[2 * kSlot + (o)], fmaf(w1, p[kSlot + (o)], w0 * p[(o)])))), \
-          0.f)
-    const float c00 = GRLBM_WINDOW(0);
-    const float c01 = GRLBM_WINDOW(kBoxX);
-    const float c10 = GRLBM_WINDOW(1);
-    const float c11 = GRLBM_WINDOW(kBoxX + 1);
-#undef GRLBM_WINDOW
-    const float f0 = fmaf(r.y, c10 - c00, c00);
-    const float f1 = fmaf(r.y, c11 - c01, c01);
-    return r.w * fmaf(r.z, f1 - f0, f0);
-}
-
-// One flat stream value of direction d (StreamFlatFixed, src/Radiation.cpp:394-410).
-__device__ __forceinline__ float stream_flat(const PrecStepArgs &a, const DirTable &dt, const float *ring, int d,
-                                             const Stage &st, int i, int j)
-{
-    const int x0 = st.x0, y0 = st.y0;
-    const int nx = (int)a.g.nx;
-    const float ox = dt.ox[d], oy = dt.oy[d];
-    const float fli = floorf(ox), flj = floorf(oy);
-    const float fx = ox - fli, fy = oy - flj;
-    const int i0 = min(max(i + (int)fli, 0), nx - 2);
-    const int j0 = min(max(j + (int)flj, 0), (int)a.g.ny - 2);
-    const int lx = i0 - x0, ly = j0 - y0;
-    float c00, c01, c10, c11;
-    if ((unsigned)lx <= (unsigned)kTileX && (unsigned)ly <= (unsigned)kTileY)
-    {
-        const float *p = ring + ((d + kBelow) & (kRing - 1)) * kSlot + ly * kBoxX + lx;
-        c00 = p[0], c01 = p[kBoxX], c10 = p[1], c11 = p[kBoxX + 1];
-    }
-    else
-    {
-        const unsigned pitch = a.pitch;
-        const float *p = a.Iin + (unsigned)d * a.plane + (unsigned)i0 + (unsigned)j0 * pitch;
-        c00 = __ldg(p), c01 = __ldg(p + pitch), c10 = __ldg(p + 1), c11 = __ldg(p + pitch + 1);
-    }
-    const float f0 = fmaf(fx, c10 - c00, c00);
-    const float f1 = fmaf(fx, c11 - c01, c01);
-    return fmaf(fy, f1 - f0, f0);
-}
-
 // direction coefficients of the affine collide map for a moving fluid
 __device__ __forceinline__ void collide_coeffs(float n1, float n2, float u1, float u2, float lor, float adt,
                                                float kak0, float &g, float &h, float &q1, float &q2)
@@ -357,271 +72,6 @@ __device__ __forceinline__ void collide_coeffs(float n1, float n2, float u1, flo
     q2 = (n2 - sc * u2) / A;
     g = 1.f / (1.f + adt * kak0 * A);
     h = adt / (A * A) * g;
-}
-
-// One tile (kTileX x kTileY cells of the slab rows) of one step: stream,
-// moments and collide for its cells.  bx, by: tile coordinates; parity: the
-// phase parity of the block's staging mbarrier, carried from tile to tile.
-// Returns false (for the whole block) when a staging wait ran out of time:
-// the fault word is then set and the tile is abandoned.
-template <bool CURVED, int UNROLL>
-__device__ __forceinline__ bool step_tile(const PrecStepArgs &a, const CUtensorMap *map, const DirTable &dt, int bx,
-                                          int by, unsigned char *smem_raw, unsigned &parity)
-{
-    float *ring = ring_base(smem_raw);
-    const int t = threadIdx.x;
-    const int tx = t % kTileX, ty = t / kTileX;
-    // patch origin (node coordinates); tiles cover the slab rows [jlo, jhi)
-    const int x0 = bx * kTileX, y0 = (int)a.g.jlo - 1 + by * kTileY;
-    const int i = 1 + x0 + tx, j = 1 + y0 + ty;
-    const bool active = i <= (int)a.g.nx_ && j < (int)a.g.jhi;
-    const int ii = active ? i : 1, jj = active ? j : 1;
-    const int ij = ii + jj * (int)a.g.nx;
-    const int cc = (ii - 1) + (jj - 1) * (int)a.g.nx_;
-    const unsigned nxy = (unsigned)a.g.nxy, plane = a.plane;
-    const uint8_t fl = active ? a.flags[ij] : (uint8_t)3;
-    const bool live = active && !(CURVED && (fl & 2));
-    const bool collides = active && !(fl & 1);
-    // The streamed intensities of a colliding cell wait in its own output
-    // slots until the lambda iteration has converged (nothing else reads or
-    // writes them in this step).
-    float *Is = a.Iout + (unsigned)ii + (unsigned)jj * a.pitch;
-
-    // row-type table of the angular interpolation and direction coefficients
-    // of the moment sums, from the kernel parameter
-    float *rowtab = ring + kRingSlots * kSlot;
-    float4 *dirc = reinterpret_cast<float4 *>(rowtab + kMaxRowTypes * 12);
-    if (CURVED)
-        for (int k = t; k < dt.q * 12; k += kStepBlock)
-            rowtab[k] = dt.rowtab[k];
-    for (int k = t; k < 2 * a.nd; k += kStepBlock)
-        dirc[k] = reinterpret_cast<const float4 *>(dt.dirc)[k];
-
-    const Stage st{smem_addr(ring), smem_addr(smem_raw), x0, y0};
-    const int cell = ty * kBoxX + tx; // slot offset of node (i - 1, j - 1)
-    stage_planes(a, map, st, -kBelow, kSpan);
-
-    KMoments km;
-    km.zero();
-    // records are read once per step: streaming loads, prefetched two
-    // directions ahead (the last record stands in past the end)
-    const float4 *rp = a.rec + cc;
-    const unsigned rs = (unsigned)a.g.ncell;
-    const unsigned dlast = (unsigned)(a.nd - 1);
-    float4 r0 = make_float4(0.f, 0.f, 0.f, 0.f), r1 = r0;
-    if (CURVED)
-    {
-        r0 = __ldcs(rp);
-        r1 = __ldcs(rp + min(1u, dlast) * rs);
-    }
-    for (int chunk0 = 0; chunk0 < a.nd; chunk0 += kChunk)
-    {
-        // this chunk's planes landed and are visible; the previous chunk is
-        // done with its slots
-        const bool landed = mbar_wait(st.bar, parity, kWaitNs, a.fault);
-        if (__syncthreads_or(!landed))
-        {
-            // report it, let the copies in flight land and give up the tile
-            if (t == 0 && a.fault)
-                *reinterpret_cast<volatile unsigned *>(a.fault) = 1u;
-            mbar_wait(st.bar, parity, kDrainNs, nullptr);
-            return false;
-        }
-        parity ^= 1u;
-        if (chunk0 + kChunk < a.nd)
-            stage_planes(a, map, st, chunk0 + kSpan - kBelow, kChunk);
-        const int dend = min(chunk0 + kChunk, a.nd);
-#pragma unroll(UNROLL)
-        for (int d = chunk0; d < dend; d++)
-        {
-            float4 r2 = r0;
-            if (CURVED)
-                r2 = __ldcs(rp + min((unsigned)(d + 2), dlast) * rs);
-            float v = 0.f;
-            if (live)
-                v = CURVED ? stream_curved(a, dt, ring, rowtab, d, r0, cell, (unsigned)cc + (unsigned)d * rs, ii, jj)
-                           : stream_flat(a, dt, ring, d, st, ii, jj);
-            if (collides)
-                Is[(unsigned)d * plane] = v;
-            km.add(v, dirc[2 * d], dirc[2 * d + 1]);
-            r0 = r1;
-            r1 = r2;
-        }
-        km.fold();
-    }
-    float m[6] = {km.E.s, km.Fx.s, km.Fy.s, km.Pxx.s, km.Pxy.s, km.Pyy.s};
-
-    int cycles = 0;
-    if (collides)
-    {
-        const float u1 = a.u1[ij], u2 = a.u2[ij], lor = a.lor[ij], adt = a.adt[ij];
-        const float eta = a.eta[ij], k0 = a.k0[ij], k3 = a.k3[ij], kak0 = a.ka[ij] + a.k0[ij];
-        const bool rest = (u1 == 0.f) && (u2 == 0.f);
-        // m_new[q] = A[q] + (eta + k0 fE) B[q] + k3 (fFx C[q] + fFy D[q])
-        float A6[6], B6[6], C6[6], D6[6];
-        float g0 = 0.f, h0 = 0.f;
-        if (rest)
-        {
-            g0 = 1.f / (1.f + adt * kak0);
-            h0 = adt * g0;
-#pragma unroll
-            for (int q = 0; q < 6; q++)
-            {
-                A6[q] = g0 * m[q];
-                B6[q] = h0 * dt.wmom[q];
-                C6[q] = h0 * dt.wmom[6 + q];
-                D6[q] = h0 * dt.wmom[12 + q];
-            }
-        }
-        else
-        {
-#pragma unroll
-            for (int q = 0; q < 6; q++)
-                A6[q] = B6[q] = C6[q] = D6[q] = 0.f;
-            for (int d = 0; d < a.nd; d++)
-            {
-                const float n1 = dt.n1[d], n2 = dt.n2[d], w = dt.w[d];
-                float g, h, q1, q2;
-                collide_coeffs(n1, n2, u1, u2, lor, adt, kak0, g, h, q1, q2);
-                const float mu[6] = {1.f, n1, n2, n1 * n1, n1 * n2, n2 * n2};
-                const float gs = w * g * Is[(unsigned)d * plane], wh = w * h;
-#pragma unroll
-                for (int q = 0; q < 6; q++)
-                {
-                    A6[q] += gs * mu[q];
-                    B6[q] += wh * mu[q];
-                    C6[q] += wh * q1 * mu[q];
-                    D6[q] += wh * q2 * mu[q];
-                }
-            }
-        }
-        float diff = 1.f;
-        float fE = 0.f, fFx = 0.f, fFy = 0.f;
-        while (fabsf(diff) > 1e-4f && cycles < 100)
-        {
-            cycles++;
-            const float pE = m[0], pFx = m[1], pFy = m[2], pPxx = m[3], pPxy = m[4], pPyy = m[5];
-            const float uF = u1 * pFx + u2 * pFy;
-            const float uxP = u1 * pPxx + u2 * pPxy;
-            const float uyP = u1 * pPxy + u2 * pPyy;
-            const float uuP = u1 * uxP + u2 * uyP;
-            fE = lor * lor * (pE - 2.f * uF + uuP);
-            const float rr = lor / (1.f + lor) * ((2.f * lor + 1.f) * uF - lor * uuP);
-            fFx = lor * lor * (pFx - lor * pE * u1 - uxP + u1 * rr);
-            fFy = lor * lor * (pFy - lor * pE * u2 - uyP + u2 * rr);
-            const float e = eta + k0 * fE;
-            const float prev[6] = {pE, pFx, pFy, pPxx, pPxy, pPyy};
-            float s2 = 0.f;
-#pragma unroll
-            for (int q = 0; q < 6; q++)
-            {
-                m[q] = A6[q] + e * B6[q] + k3 * (fFx * C6[q] + fFy * D6[q]);
-                const float x = (prev[q] - m[q]) / m[q];
-                s2 += x * x;
-            }
-            diff = sqrtf(s2);
-        }
-        // write the intensities of the last iterate; its moments m, the
-        // affine map's moments of exactly these intensities, are the stored ones
-        const float e = eta + k0 * fE;
-        const float scale = CURVED ? a.ia3[ij] : 1.f;
-        const float ra = h0 * e, rb1 = h0 * k3 * fFx, rb2 = h0 * k3 * fFy;
-        for (int d0 = 0; d0 < a.nd; d0 += 8)
-        {
-            // the parked stream values of 8 directions, loaded together
-            float S[8];
-#pragma unroll
-            for (int k = 0; k < 8; k++)
-                S[k] = (d0 + k < a.nd) ? Is[(unsigned)(d0 + k) * plane] : 0.f;
-#pragma unroll
-            for (int k = 0; k < 8; k++)
-            {
-                const int d = d0 + k;
-                if (d >= a.nd)
-                    break;
-                const float4 c1 = dirc[2 * d + 1];
-                const float n1 = c1.z, n2 = c1.w;
-                float v;
-                if (rest)
-                    v = fmaf(g0, S[k], fmaf(rb1, n1, fmaf(rb2, n2, ra)));
-                else
-                {
-                    float g, h, q1, q2;
-                    collide_coeffs(n1, n2, u1, u2, lor, adt, kak0, g, h, q1, q2);
-                    v = g * S[k] + h * (e + k3 * (q1 * fFx + q2 * fFy));
-                }
-                Is[(unsigned)d * plane] = v * scale;
-            }
-        }
-    }
-    if (active)
-    {
-#pragma unroll
-        for (int q = 0; q < 6; q++)
-            a.mom[(unsigned)ij + q * nxy] = m[q];
-    }
-    // lambda-iteration statistics: warp sums and maxima, one atomic per warp
-    unsigned sum = (unsigned)cycles, mx = (unsigned)cycles;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1)
-    {
-        sum += __shfl_xor_sync(0xffffffffu, sum, o);
-        mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    }
-    if ((t & 31) == 0 && sum)
-    {
-        atomicAdd(a.iter_sum, (unsigned long long)sum);
-        atomicMax(a.iter_max, mx);
-    }
-    return true;
-}
-
-template <bool CURVED>
-__global__ void __launch_bounds__(kStepBlock, GRLBM_PREC_MIN_BLOCKS)
-    k_step_prec(const __grid_constant__ PrecStepArgs a, const __grid_constant__ DirTable dt)
-{
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    if (threadIdx.x == 0)
-        mbar_init(smem_addr(smem_raw), 1);
-    __syncthreads();
-    unsigned parity = 0;
-    step_tile<CURVED, GRLBM_PREC_UNROLL>(a, &a.in_map, dt, blockIdx.x, blockIdx.y, smem_raw, parity);
-}
-
-// Many problems in one persistent launch: the blocks walk the concatenated
-// tile list (problem k owns tiles [first_tile[k], first_tile[k+1])) with a
-// grid-stride loop; each tile runs the same code as the single-problem
-// kernel, so every problem's result is the one it gets alone.
-__global__ void __launch_bounds__(kStepBlock, GRLBM_PREC_MIN_BLOCKS)
-    k_step_batch(const BatchItem *__restrict__ items, const int *__restrict__ first_tile, int n_items,
-                 int total_tiles, int flip)
-{
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    if (threadIdx.x == 0)
-        mbar_init(smem_addr(smem_raw), 1);
-    __syncthreads();
-    unsigned parity = 0;
-    for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x)
-    {
-        int lo = 0, hi = n_items - 1;
-        while (lo < hi)
-        {
-            const int mid = (lo + hi + 1) >> 1;
-            if (first_tile[mid] <= tile)
-                lo = mid;
-            else
-                hi = mid - 1;
-        }
-        const BatchItem &it = items[lo];
-        const int local = tile - first_tile[lo];
-        const int bx = local % it.tiles_x, by = local / it.tiles_x;
-        const PrecStepArgs &a = it.a[it.cur0 ^ flip];
-        const bool ok = it.curved ? step_tile<true, GRLBM_BATCH_UNROLL>(a, &a.in_map, *it.dt, bx, by, smem_raw, parity)
-                                  : step_tile<false, GRLBM_BATCH_UNROLL>(a, &a.in_map, *it.dt, bx, by, smem_raw, parity);
-        if (!ok)
-            return; // the barrier's phase is unknown: the block stops (the fault word is set)
-        __syncthreads(); // the next tile reuses the shared stage
-    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1084,68 +534,6 @@ cudaError_t run_wait_selftest(int arrive, unsigned long long limit_ns, int *comp
     return e;
 }
 
-int step_prec_tiles_x(int64_t nx_) { return (int)nblk(nx_, kTileX); }
-int step_prec_tiles_y(int64_t rows) { return (int)nblk(rows, kTileY); }
-
-cudaError_t prepare_step_batch(int smem_bytes, int *blocks_per_sm)
-{
-    cudaError_t e = cudaFuncSetAttribute(k_step_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)step_prec_smem(kMaxDirs));
-    if (e != cudaSuccess)
-        return e;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_step_batch, kStepBlock, smem_bytes);
-}
-void launch_step_batch(const BatchItem *items, const int *first_tile, int n_items, int total_tiles, int flip,
-                       int blocks, int smem_bytes, cudaStream_t s)
-{
-    k_step_batch<<<blocks, kStepBlock, smem_bytes, s>>>(items, first_tile, n_items, total_tiles, flip);
-}
-
-// The state as a 2D tensor of {pitch, ny * nd} floats (row y = d ny + j),
-// read in boxes of one patch plane.
-cudaError_t encode_state_map(CUtensorMap *map, const float *state, const StateLayout &L, int64_t ny, int nd)
-{
-    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
-    if (!encode)
-    {
-        void *fn = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        const cudaError_t e =
-            cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &fn, 12000, cudaEnableDefault, &q);
-        if (e != cudaSuccess)
-            return e;
-        if (q != cudaDriverEntryPointSuccess || !fn)
-            return cudaErrorNotSupported;
-        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
-    }
-    if (L.pitch % 4 != 0 || reinterpret_cast<uintptr_t>(state) % 16 != 0)
-        return cudaErrorInvalidValue;
-    const cuuint64_t dims[2] = {(cuuint64_t)L.pitch, (cuuint64_t)(ny * nd)};
-    const cuuint64_t strides[1] = {(cuuint64_t)L.pitch * sizeof(float)};
-    const cuuint32_t box[2] = {(cuuint32_t)kBoxX, (cuuint32_t)kPatchY};
-    const cuuint32_t elem[2] = {1, 1};
-    const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float *>(state), dims, strides, box,
-                              elem, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
-}
-
-size_t step_prec_smem(int nd)
-{
-    return kBarBytes + kRingAlign + ((size_t)kRingSlots * kSlot + kMaxRowTypes * 12 + 8 * (size_t)nd) * sizeof(float);
-}
-
-// The shared-memory limit is a property of the kernel, shared by every
-// context in the process: it is set for the largest direction count, so
-// that no context's set-up lowers it below another's launches.
-cudaError_t prepare_step_prec(int)
-{
-    const int smem_bytes = (int)step_prec_smem(kMaxDirs);
-    cudaError_t e = cudaFuncSetAttribute(k_step_prec<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
-    if (e != cudaSuccess)
-        return e;
-    return cudaFuncSetAttribute(k_step_prec<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
-}
 __global__ void k_coef_about_node32(GridDev g, const double *coef, float *coef32, int nf)
 {
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1193,15 +581,4 @@ void launch_step_prec_adaptive(const PrecStepArgs &a, const DirTable &dt, bool c
     launch_zero_halo_moments32(a.g, a.mom, s);
 }
 
-void launch_step_prec(const PrecStepArgs &a, const DirTable &dt, bool curved, cudaStream_t s)
-{
-    const size_t smem = step_prec_smem(a.nd);
-    if (a.g.jhi <= a.g.jlo)
-        return;
-    const dim3 grid(nblk(a.g.nx_, kTileX), nblk(a.g.jhi - a.g.jlo, kTileY));
-    if (curved)
-        k_step_prec<true><<<grid, kStepBlock, smem, s>>>(a, dt);
-    else
-        k_step_prec<false><<<grid, kStepBlock, smem, s>>>(a, dt);
-}
 } // namespace grlbm

@@ -346,14 +346,27 @@ __global__ void __launch_bounds__(128) k_fourier_project(ProjectArgs a)
 
 // Departure records from the Fourier series: what StreamCurvedFixed
 // evaluates every step (src/Radiation.cpp:478-499) and the angle part of
-// IntensityAt (:324-328).  One thread per (direction, interior cell).
+// IntensityAt (:324-328).  One thread per (interior cell, direction): plain
+// records are written direction-major ([d * ncell + c], threads over cells
+// fastest), precision records cell-major ([c * nd + d], threads over
+// directions fastest).
 __global__ void __launch_bounds__(128) k_departure(DepartureArgs a)
 {
     const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (tid >= a.g.ncell * a.nd)
         return;
-    const int d = (int)(tid / a.g.ncell);
-    const int64_t c = tid - (int64_t)d * a.g.ncell;
+    int d;
+    int64_t c;
+    if (a.rec32)
+    {
+        c = tid / a.nd;
+        d = (int)(tid - c * a.nd);
+    }
+    else
+    {
+        d = (int)(tid / a.g.ncell);
+        c = tid - (int64_t)d * a.g.ncell;
+    }
     const int64_t i = 1 + c % a.g.nx_, j = 1 + c / a.g.nx_;
     const int64_t ij = i + j * a.g.nx;
     const int64_t fs = a.g.nxy * a.nf;
@@ -414,7 +427,8 @@ __global__ void __launch_bounds__(128) k_departure(DepartureArgs a)
     }
     if (a.rec32)
     {
-        // packed record: corner code, row type, window start and blend
+        // packed record (packed32): row type, window start and blend; the
+        // corner in the fractions' sign bits, far in the scale's
         const double fxd = floor((double)r32.x), fyd = floor((double)r32.y);
         const bool near = (fxd == -1.0 || fxd == 0.0) && (fyd == -1.0 || fyd == 0.0);
         double ddc = dd == dd ? dd : 0.0;
@@ -423,23 +437,16 @@ __global__ void __launch_bounds__(128) k_departure(DepartureArgs a)
         double t = ddc - (double)g;
         t = t < 0.0 ? 0.0 : (t > 1.0 ? 1.0 : t);
         const int rt = g % a.q, m = g / a.q;
-        int dbase = (a.row_base[rt] + a.p * m) % a.nd - d;
-        if (2 * dbase > a.nd)
-            dbase -= a.nd;
-        else if (2 * dbase <= -a.nd)
-            dbase += a.nd;
-        const int rel = d % kChunk + dbase + kBelow;
-        const bool inspan = rel >= 0 && rel <= kSpan - kTaps;
-        unsigned tq = (unsigned)(t * (double)(1u << packed::kTBits) + 0.5);
-        tq = tq > (1u << packed::kTBits) - 1u ? (1u << packed::kTBits) - 1u : tq;
-        const unsigned code = near ? (unsigned)(fxd + 1.0) + 2u * (unsigned)(fyd + 1.0) : 0u;
-        const bool far = !near || !inspan;
-        const unsigned word = tq | ((unsigned)rt << packed::kTypeShift) |
-                              ((unsigned)((far ? 0 : dbase) + packed::kBaseBias) << packed::kBaseShift) |
-                              (code << packed::kCodeShift) | ((far ? 1u : 0u) << packed::kFarBit);
+        const unsigned start = (unsigned)((a.row_base[rt] + a.p * m) % a.nd);
+        unsigned tq = (unsigned)(t * (double)(1u << packed32::kTBits) + 0.5);
+        tq = tq > (1u << packed32::kTBits) - 1u ? (1u << packed32::kTBits) - 1u : tq;
+        const unsigned word = tq | ((unsigned)rt << packed32::kTypeShift) | (start << packed32::kStartShift);
         const float fx = near ? (float)((double)r32.x - fxd) : 0.f, fy = near ? (float)((double)r32.y - fyd) : 0.f;
-        a.rec32[tid] = make_float4(__uint_as_float(word), fx, fy, r32.w);
-        if (far && a.far)
+        const unsigned ux = __float_as_uint(fx) | (near && fxd == 0.0 ? 0x80000000u : 0u);
+        const unsigned uy = __float_as_uint(fy) | (near && fyd == 0.0 ? 0x80000000u : 0u);
+        const unsigned uw = __float_as_uint(r32.w) | (near ? 0u : 0x80000000u);
+        a.rec32[tid] = make_uint4(word, ux, uy, uw);
+        if (!near && a.far)
             atomicAdd(a.far, 1ull);
         a.side32[tid] = r32;
     }

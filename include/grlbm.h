@@ -15,7 +15,7 @@
  *    arrays have nx*ny entries indexed ij = i + j*nx with nx = nx_+2
  *    (src/Grid.cpp:14, 44-47); intensities are cell-major I[ij*nDir + d]
  *    (src/Radiation.cpp:89-92).  They are copied at call time; the caller
- *    keeps ownership.  Device layouts are private (direction-major).
+ *    keeps ownership.  Device layouts are private.
  *  - A context is used by one host thread at a time; all GPU work is ordered
  *    on the context's CUDA stream and every entry point returns after its
  *    work has completed (synchronous), except where stated.
@@ -237,16 +237,27 @@ int grlbm_energy_noalloc(const double *E, int64_t nx_, int64_t ny_, double *tota
  * [j_first, j_end) only (1 <= j_first < j_end <= ny - 1; the default is all
  * interior rows). */
 int grlbm_set_rows(grlbm_ctx *ctx, int64_t j_first, int64_t j_end);
-/* Bytes of one node row of the intensity state over all directions
- * (nx * nDir * 8 for GRLBM_PLAIN_FP64; GRLBM_PRECISION_FP32 keeps its rows
- * padded to a multiple of 4 floats: ((nx + 3) / 4 * 4) * nDir * 4). */
+/* Bytes of one node row of the intensity state over all directions:
+ * nx * nDir * 8 for GRLBM_PLAIN_FP64; for GRLBM_PRECISION_FP32 with fixed
+ * streaming nx * dp * 4, each node holding dp = (nDir + 4 rounded up to a
+ * multiple of 4) floats (its directions, then directions 0..3 again). */
 int grlbm_row_bytes(const grlbm_ctx *ctx, int64_t *bytes);
 /* Copies node rows [j_first, j_first + n) of the current intensity state
  * (every direction) to (to_buffer = 1) or from (to_buffer = 0) a contiguous
- * device buffer laid out [direction][row][i] (i over the padded row for
- * GRLBM_PRECISION_FP32), n * row_bytes bytes.  Enqueued on the context's
- * stream; returns before it completes. */
+ * device buffer, n * row_bytes bytes, laid out [direction][row][i] for
+ * GRLBM_PLAIN_FP64 and [row][i][direction] for GRLBM_PRECISION_FP32.
+ * Enqueued on the context's stream; returns before it completes. */
 int grlbm_copy_rows(grlbm_ctx *ctx, int64_t j_first, int64_t n, void *buffer, int32_t to_buffer);
+/* ---- tiles of the precision step --------------------------------------------
+ * No counterpart in the reference.  The GRLBM_PRECISION_FP32 step of the
+ * fixed streaming types runs as warps that each take tiles of tile_x x
+ * tile_y cells, staging each tile's (tile_x + 2) x (tile_y + 2) node patch of
+ * the state in shared memory.  The default tile is the largest of 8x8, 8x4,
+ * 4x4, 4x2, 2x2 whose patch leaves the kernel's resident warps unchanged.
+ * The result does not depend on the tile.  GRLBM_ERR_ARGUMENT when the patch
+ * does not fit in shared memory; GRLBM_ERR_UNSUPPORTED for other contexts. */
+int grlbm_set_tile_shape(grlbm_ctx *ctx, int32_t tile_x, int32_t tile_y);
+int grlbm_get_tile_shape(const grlbm_ctx *ctx, int32_t *tile_x, int32_t *tile_y);
 /* The most node rows away from its cell that any stream gather reads (from
  * the departure records of the last table build; from the stencil for flat
  * streaming): the ghost depth a band needs on each side. */
@@ -277,10 +288,13 @@ int grlbm_batch_step(grlbm_batch *batch, int32_t n_steps);
 int grlbm_batch_set_shape(grlbm_batch *batch, int32_t blocks_per_sm, int32_t largest_first);
 /* Times trial_steps steps for each launch shape -- the persistent launch at
  * resident blocks per SM (the occupancy limit and up to two fewer) with the
- * problems' tiles as given or largest problem first, and the concurrent
- * launches (0) -- keeps the fastest, and puts every problem back in the
- * state it had before the call.  The choice is returned in *blocks_per_sm and
- * *largest_first (either may be NULL). */
+ * problems in the order given or largest problem first, and the concurrent
+ * launches (0) -- and keeps the fastest; then, per size class (problems of
+ * one grid size and direction count), largest class first, times candidate
+ * tile shapes (grlbm_set_tile_shape) with the other classes fixed and keeps
+ * the fastest.  Every problem is put back in the state it had before the
+ * call.  The launch shape is returned in *blocks_per_sm and *largest_first
+ * (either may be NULL), the tiles by grlbm_get_tile_shape. */
 int grlbm_batch_autotune(grlbm_batch *batch, int32_t trial_steps, int32_t *blocks_per_sm, int32_t *largest_first);
 /* ---- adjoint ------------------------------------------------------------------
  * No counterpart in the reference.  Gradients of a loss of the final
