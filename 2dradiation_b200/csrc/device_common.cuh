@@ -319,14 +319,16 @@ struct AdjCollideArgs
 
 // The precision-form step of the fixed streaming types (cell-major state,
 // kernels_step32.cu): warps of kStep32Warps per block, each taking tiles of
-// tx x ty cells from a counter.
+// tx x ty <= kStep32UnitCells cells from a counter.
 constexpr int kStep32Warps = 4;
+constexpr int kStep32UnitCells = 16;
 constexpr int kStep32MaxSmem = 227 * 1024;
 struct Step32Args
 {
     GridDev g;
     int nd, ng, dp;          // directions, interpolation rows, direction pitch of the state
     int tx, ty;              // cells per tile; a warp stages (tx + 2) x (ty + 2) nodes
+    int ss, patch_floats;    // row stride of the streamed-value buffer, floats of the patch buffer
     int tiles_x, ntiles;     // tiles per row of tiles, tiles over the slab rows
     const float *Iin;
     float *Iout;
@@ -386,16 +388,21 @@ void launch_step_prec_adaptive(const PrecStepArgs &a, const DirTable &dt, bool c
 // The fixed streaming types in the precision form (kernels_step32.cu).
 // Passes per lane for nd directions (an instantiated count >= nd / 32), or -1.
 int step32_passes(int nd);
-int step32_patch_stride(int tx, int ty, int dp);
-// shared memory of a block: the fixed part, and with four patch buffers
-size_t step32_smem_base();
-size_t step32_smem(int tx, int ty, int dp);
+// Warp buffers: the patch (floats) and the streamed values of the tile's
+// cells (row stride s, s = 2 mod 32 >= nd: conflict-free for lanes over the
+// directions and for two lanes per cell over interleaved directions).
+int step32_s_stride(int nd);
+int step32_patch_floats(int tx, int ty, int dp);
+int step32_warp_stride(int tx, int ty, int dp, int nd);
+// shared memory of a block of the single-problem kernel, and of the batch kernel
+size_t step32_smem(int tx, int ty, int dp, int nd);
+size_t step32_batch_smem(int warp_stride);
 cudaError_t prepare_step32();
 cudaError_t step32_occupancy(int P, bool curved, bool batch, size_t smem, int *blocks);
 // blocks: the persistent grid (resident blocks per SM times the SMs)
 void launch_step32(const Step32Args &a, const DirTable &dt, bool curved, int P, int blocks, cudaStream_t s);
 void launch_step_batch32(const Batch32Item *items, const int *first_tile, int n_items, int total_tiles, int flip,
-                         unsigned *counters, int P, int blocks, size_t smem, int patch_stride, cudaStream_t s);
+                         unsigned *counters, int P, int blocks, size_t smem, int warp_stride, cudaStream_t s);
 // The TMA map the step stages a cell-major state of nx x ny nodes through,
 // for tiles of tx x ty cells.
 cudaError_t encode_state_map32(CUtensorMap *map, const float *state, int64_t nx, int64_t ny, int dp, int tx, int ty);

@@ -262,6 +262,8 @@ Step32Args step32_args(grlbm_ctx *ctx, int from)
     a.dp = (int)ctx->sl.sp;
     a.tx = ctx->tile_x;
     a.ty = ctx->tile_y;
+    a.ss = step32_s_stride(a.nd);
+    a.patch_floats = step32_patch_floats(a.tx, a.ty, a.dp);
     a.tiles_x = step32_tiles_x(ctx);
     a.ntiles = step32_tiles(ctx);
     a.Iin = ctx->I[from].as<float>();
@@ -292,9 +294,9 @@ Step32Args step32_args(grlbm_ctx *ctx, int from)
 int set_step32_tile(grlbm_ctx *ctx, int tx, int ty)
 {
     const int dp = (int)ctx->sl.sp;
-    if (tx < 1 || ty < 1 || tx > 64 || ty > 64)
-        return fail(ctx, GRLBM_ERR_ARGUMENT, "tile %dx%d: each side must be in [1, 64]", tx, ty);
-    const size_t smem = step32_smem(tx, ty, dp);
+    if (tx < 1 || ty < 1 || tx * ty > kStep32UnitCells)
+        return fail(ctx, GRLBM_ERR_ARGUMENT, "tile %dx%d: at least 1 and at most %d cells", tx, ty, kStep32UnitCells);
+    const size_t smem = step32_smem(tx, ty, dp, ctx->st.n);
     if (smem > (size_t)kStep32MaxSmem)
         return fail(ctx, GRLBM_ERR_ARGUMENT, "tile %dx%d: its patch of %d directions needs %zu bytes of shared memory",
                     tx, ty, ctx->st.n, smem);
@@ -322,13 +324,13 @@ int set_step32_tile(grlbm_ctx *ctx, int tx, int ty)
 // register-limited occupancy of the step kernel unchanged.
 int default_step32_tile(grlbm_ctx *ctx)
 {
-    static const int cand[][2] = {{8, 8}, {8, 4}, {4, 4}, {4, 2}, {2, 2}, {1, 1}};
+    static const int cand[][2] = {{4, 4}, {8, 2}, {4, 2}, {2, 2}, {2, 1}, {1, 1}};
     const bool curved = ctx->run.streaming_type == GRLBM_CURVED_FIXED;
     int reg_limit = 0;
     CU(step32_occupancy(ctx->passes, curved, false, 0, &reg_limit));
     for (const auto &c : cand)
     {
-        const size_t smem = step32_smem(c[0], c[1], (int)ctx->sl.sp);
+        const size_t smem = step32_smem(c[0], c[1], (int)ctx->sl.sp, ctx->st.n);
         int per_sm = 0;
         if (smem > (size_t)kStep32MaxSmem)
             continue;
@@ -1729,7 +1731,7 @@ struct grlbm_batch
     std::vector<Batch32Item> items; // in launch order
     std::vector<int> order;         // items[k] is context order[k]
     DevBuf d_items, d_first, d_dirs, counters;
-    int total_tiles = 0, passes = 1, patch_stride = 0, blocks_per_sm_max = 1, blocks_per_sm = 1, sms = 1;
+    int total_tiles = 0, passes = 1, warp_stride = 0, blocks_per_sm_max = 1, blocks_per_sm = 1, sms = 1;
     size_t smem = 0;
     int largest_first = 0;
     int flip = 0; // parity of the steps taken since the items were built
@@ -1793,13 +1795,13 @@ void batch_drop_graphs(grlbm_batch *b)
 int batch_geometry(grlbm_batch *b)
 {
     b->passes = 1;
-    b->patch_stride = 0;
+    b->warp_stride = 0;
     for (grlbm_ctx *c : b->ctx)
     {
         b->passes = std::max(b->passes, c->passes);
-        b->patch_stride = std::max(b->patch_stride, step32_patch_stride(c->tile_x, c->tile_y, (int)c->sl.sp));
+        b->warp_stride = std::max(b->warp_stride, step32_warp_stride(c->tile_x, c->tile_y, (int)c->sl.sp, c->st.n));
     }
-    b->smem = step32_smem_base() + (size_t)b->patch_stride * kStep32Warps;
+    b->smem = step32_batch_smem(b->warp_stride);
     if (b->smem > (size_t)kStep32MaxSmem)
         return bfail(b, GRLBM_ERR_ARGUMENT, "the batch's largest patch needs %zu bytes of shared memory", b->smem);
     BCU(step32_occupancy(b->passes, true, true, b->smem, &b->blocks_per_sm_max));
@@ -1862,7 +1864,7 @@ int batch_enqueue(grlbm_batch *b, int n, int flip)
         for (int s = 0; s < n; s++)
             launch_step_batch32(b->d_items.as<Batch32Item>(), b->d_first.as<int>(), (int)b->items.size(),
                                 b->total_tiles, flip ^ (s & 1), b->counters.as<unsigned>(), b->passes,
-                                b->sms * b->blocks_per_sm, b->smem, b->patch_stride, b->stream);
+                                b->sms * b->blocks_per_sm, b->smem, b->warp_stride, b->stream);
         return GRLBM_OK;
     }
     BCU(cudaEventRecord(b->fork, b->stream));
@@ -2130,7 +2132,7 @@ int grlbm_batch_autotune(grlbm_batch *b, int32_t trial_steps, int32_t *blocks_pe
             const grlbm_ctx *a = x.second[0], *c = y.second[0];
             return a->ncell * a->st.n * (int64_t)x.second.size() > c->ncell * c->st.n * (int64_t)y.second.size();
         });
-        static const int cand[][2] = {{2, 2}, {4, 2}, {4, 4}, {8, 4}, {4, 8}, {8, 8}, {16, 4}, {16, 8}};
+        static const int cand[][2] = {{2, 2}, {4, 2}, {2, 4}, {4, 4}, {8, 2}, {2, 8}, {16, 1}};
         for (auto &cls : classes)
         {
             grlbm_ctx *c0 = cls.second[0];
@@ -2139,7 +2141,7 @@ int grlbm_batch_autotune(grlbm_batch *b, int32_t trial_steps, int32_t *blocks_pe
             {
                 if (t[0] == bx && t[1] == by)
                     continue;
-                if (step32_smem(t[0], t[1], (int)c0->sl.sp) > (size_t)kStep32MaxSmem)
+                if (step32_smem(t[0], t[1], (int)c0->sl.sp, c0->st.n) > (size_t)kStep32MaxSmem)
                     continue;
                 for (grlbm_ctx *c : cls.second)
                     if ((rc = set_step32_tile(c, t[0], t[1])))

@@ -11,13 +11,15 @@
 // (src/Radiation.cpp:502-505, 342); alpha_n^-3 > 0 commutes with the clamp,
 // so gathering J needs no alpha at the corners.
 //
-// Work split: every warp works alone.  It takes tiles of tx x ty cells from a
-// counter, stages the tile's (tx + 2) x (ty + 2) node patch of the whole state
-// (all directions) into its own shared-memory buffer with one TMA tensor copy,
-// and steps the tile's cells one after another with its lanes over the
-// directions (direction d = lane + 32 p on pass p).  A lane's streamed values
-// stay in registers through the moments, the lambda iteration and the write
-// of the collided state, which is coalesced along the directions.
+// Work split: every warp works alone.  It takes tiles of tx x ty <= 16 cells
+// from a counter and stages the tile's (tx + 2) x (ty + 2) node patch of the
+// whole state (all directions) into its own shared-memory buffer with one TMA
+// tensor copy.  Phase 1 streams the tile's cells one after another with the
+// lanes over the directions (direction d = lane + 32 p on pass p), into the
+// warp's buffer of streamed values; the next tile's copy is then issued into
+// the free patch buffer, to land while phase 2 takes the moments and collides
+// with two lanes per cell (each summing every other direction), and phase 3
+// writes the cells' new state, coalesced along the directions.
 //
 // Per (cell, direction) the lane reads its 16-byte packed departure record
 // (window row type, window start, blend t, corner fractions with the corner in
@@ -27,10 +29,9 @@
 // zero and interpolates.  Departures outside the cell's 3x3 neighbourhood read
 // a side record and gather from global memory (cold code).
 //
-// Moments: per-lane products with the direction's quadrature coefficients,
-// summed over the warp by a compensated butterfly (each level an error-free
-// two-sum, the rounding errors carried alongside), so every lane holds the
-// same compensated sums.
+// Moments: each of a cell's two lanes sums its directions in FP32 chunks of 8
+// folded into Kahan accumulators; the two lanes' compensated sums are
+// combined by an exact two-sum, so both hold the same moments.
 //
 // Collide: the lambda iteration of src/Radiation.cpp:661-722 is affine in
 // the previous moments -- I_d = g_d S_d + h_d (eta + kappa0 E_ff + 3 kappa1
@@ -45,7 +46,7 @@
 #include "tma_util.cuh"
 
 #ifndef GRLBM_STEP32_MIN_BLOCKS
-#define GRLBM_STEP32_MIN_BLOCKS 5
+#define GRLBM_STEP32_MIN_BLOCKS 3
 #endif
 
 namespace grlbm
@@ -53,31 +54,23 @@ namespace grlbm
 namespace
 {
 constexpr int kWarps = kStep32Warps;
+constexpr int kUnitCells = kStep32UnitCells;
 constexpr int kThreads = 32 * kWarps;
 // time limits of a staging wait (a copy lands within microseconds) and of the
 // drain of a copy in flight after a wait has run out
 constexpr unsigned long long kWaitNs = 200000000ull, kDrainNs = 2000000000ull;
-// shared layout: the warps' mbarriers, the row-type table, then the warps'
-// patch buffers from the next 128-byte boundary
+// shared layout: the warps' mbarriers, the row-type table and the direction
+// coefficients (single-problem kernel), then the warps' buffers from the next
+// 128-byte boundary
 constexpr int kBarBytes = 8 * kWarps;
 constexpr int kRowtabOffset = 64;
-constexpr int kPatchOffset = (kRowtabOffset + kMaxRowTypes * 12 * 4 + 127) / 128 * 128;
 static_assert(kBarBytes <= kRowtabOffset, "mbarriers before the row-type table");
+static_assert(kUnitCells == 16, "phase 2 pairs lane c and lane c + 16");
 
 __device__ __forceinline__ unsigned char *align128(unsigned char *p)
 {
     const unsigned a = smem_addr(p);
     return p + ((128u - (a & 127u)) & 127u);
-}
-
-// (s, e) += (b, eb): s + e holds a sum, e the rounding errors of its two-sums
-__device__ __forceinline__ void two_sum_acc(float &s, float &e, float b, float eb)
-{
-    const float x = s + b;
-    const float bp = x - s;
-    const float err = (s - (x - bp)) + (b - bp);
-    s = x;
-    e = (e + eb) + err;
 }
 
 // direction coefficients of the affine collide map for a moving fluid
@@ -153,51 +146,33 @@ __device__ __forceinline__ float window5(const float *p, float w0, float w1, flo
     return fmaxf(fmaf(w4, p[4], fmaf(w3, p[3], fmaf(w2, p[2], fmaf(w1, p[1], w0 * p[0])))), 0.f);
 }
 
-// A lane's per-direction constants for its P passes: the moment
-// coefficients {w, w n1, w n2, w n1^2, w n1 n2, w n2^2}, the rotated
-// direction (n1, n2), and for flat streaming the departure's corner offset
-// in the patch, its fractions and whether it lies within the 3x3
-// neighbourhood.
+// A lane's per-direction constants of flat streaming for its P passes: the
+// departure's corner offset in the patch, its fractions and whether it lies
+// within the 3x3 neighbourhood (else the far gather).
 template <int P>
-struct LaneDirs
+struct LaneFlat
 {
-    float c[P][6];
-    float n1[P], n2[P];
     float ox[P], oy[P], fx[P], fy[P];
     int off[P];
     bool near[P];
 };
 
 template <int P>
-__device__ __forceinline__ void load_lane_dirs(LaneDirs<P> &L, const DirTable &dt, int nd, int dp, int px,
-                                               bool curved)
+__device__ __forceinline__ void load_lane_flat(LaneFlat<P> &L, const DirTable &dt, int nd, int dp, int px)
 {
     const int lane = threadIdx.x & 31;
 #pragma unroll
     for (int p = 0; p < P; p++)
     {
-        const int d = lane + 32 * p;
-        const bool ok = d < nd;
-        const int dd = ok ? d : 0;
-#pragma unroll
-        for (int k = 0; k < 6; k++)
-            L.c[p][k] = ok ? dt.dirc[8 * dd + k] : 0.f;
-        L.n1[p] = dt.dirc[8 * dd + 6];
-        L.n2[p] = dt.dirc[8 * dd + 7];
-        L.ox[p] = L.oy[p] = L.fx[p] = L.fy[p] = 0.f;
-        L.off[p] = 0;
-        L.near[p] = true;
-        if (!curved)
-        {
-            const float ox = dt.ox[dd], oy = dt.oy[dd];
-            const float fli = floorf(ox), flj = floorf(oy);
-            L.ox[p] = ox;
-            L.oy[p] = oy;
-            L.fx[p] = ox - fli;
-            L.fy[p] = oy - flj;
-            L.near[p] = (fli == -1.f || fli == 0.f) && (flj == -1.f || flj == 0.f);
-            L.off[p] = L.near[p] ? ((int)fli + 1 + ((int)flj + 1) * px) * dp + dd : 0;
-        }
+        const int dd = min(lane + 32 * p, nd - 1);
+        const float ox = dt.ox[dd], oy = dt.oy[dd];
+        const float fli = floorf(ox), flj = floorf(oy);
+        L.ox[p] = ox;
+        L.oy[p] = oy;
+        L.fx[p] = ox - fli;
+        L.fy[p] = oy - flj;
+        L.near[p] = (fli == -1.f || fli == 0.f) && (flj == -1.f || flj == 0.f);
+        L.off[p] = L.near[p] ? ((int)fli + 1 + ((int)flj + 1) * px) * dp + dd : 0;
     }
 }
 
@@ -208,51 +183,83 @@ struct IterStats
     unsigned max;
 };
 
-// One tile of one step, by one warp: stage the patch, then every cell of the
-// tile.  Returns false when the staging copy did not land within its time
-// limit (the fault word is then raised and the warp must stop).
-template <bool CURVED, int P>
-__device__ __forceinline__ bool step_tile32(const Step32Args &a, const DirTable &dt, const float *rowtab,
-                                            const LaneDirs<P> &L, int tile, float *patch, unsigned bar,
-                                            unsigned &parity, IterStats &st)
+// Stage the patch of `tile` (node origin x0 = bx tx, y0 = jlo - 1 + by ty)
+// into the warp's buffer: one tensor copy, completing on the warp's mbarrier.
+__device__ __forceinline__ void stage_tile(const Step32Args &a, int tile, float *patch, unsigned bar)
 {
-    const int lane = threadIdx.x & 31;
-    const int tx = a.tx, ty = a.ty, px = tx + 2, dp = a.dp, nd = a.nd;
-    const int bx = tile % a.tiles_x, by = tile / a.tiles_x;
-    const int x0 = bx * tx, y0 = (int)a.g.jlo - 1 + by * ty; // patch origin (node coordinates)
-    if (lane == 0)
+    if ((threadIdx.x & 31) == 0)
     {
-        // the lanes' reads of the previous tile are done (__syncwarp at the end)
+        const int bx = tile % a.tiles_x, by = tile / a.tiles_x;
+        // the lanes' reads of the buffer are done (__syncwarp before the call)
         fence_proxy_async_smem();
-        mbar_arrive_expect(bar, (unsigned)(px * (ty + 2) * dp) * 4u);
-        tma_load_4d(smem_addr(patch), &a.in_map, 0, 0, x0, y0, bar);
+        mbar_arrive_expect(bar, (unsigned)((a.tx + 2) * (a.ty + 2) * a.dp) * 4u);
+        tma_load_4d(smem_addr(patch), &a.in_map, 0, 0, bx * a.tx, (int)a.g.jlo - 1 + by * a.ty, bar);
     }
+}
+
+// Waits for the warp's staged patch; on a timeout raises the fault word and
+// lets the copy in flight land (bounded) before the warp stops.
+__device__ __forceinline__ bool wait_tile(const Step32Args &a, unsigned bar, unsigned &parity)
+{
     const bool landed = mbar_wait(bar, parity, kWaitNs, a.fault);
     if (!__all_sync(0xffffffffu, landed))
     {
-        // report it and let the copy in flight land (bounded) before leaving
-        if (lane == 0 && a.fault)
+        if ((threadIdx.x & 31) == 0 && a.fault)
             *reinterpret_cast<volatile unsigned *>(a.fault) = 1u;
         mbar_wait(bar, parity, kDrainNs, nullptr);
         return false;
     }
     parity ^= 1u;
+    return true;
+}
 
-    const int nxn = (int)a.g.nx;
+// One tile of one step by one warp, its patch staged: phase 1 streams every
+// cell with the lanes over the directions into the warp's buffer S
+// ([cell][direction], row stride a.ss), then calls next() (which stages the
+// next tile into the patch buffer); phase 2 takes the moments and collides
+// with two lanes per cell (lane = cell + 16 h, h the parity of the
+// directions it sums), writing the collided values back into S; phase 3
+// stores the cells' new state, coalesced along the directions.
+template <bool CURVED, int P, class Next>
+__device__ __forceinline__ void step_unit32(const Step32Args &a, const DirTable &dt, const float *rowtab,
+                                            const float4 *dirc, const LaneFlat<P> &LF, int tile,
+                                            const float *patch, float *S, IterStats &st, Next next)
+{
+    const int lane = threadIdx.x & 31;
+    const int tx = a.tx, px = tx + 2, dp = a.dp, nd = a.nd, ss = a.ss;
+    const int bx = tile % a.tiles_x, by = tile / a.tiles_x;
+    const int x0 = bx * tx, y0 = (int)a.g.jlo - 1 + by * a.ty; // patch origin (node coordinates)
+    const int nxn = (int)a.g.nx, nx_ = (int)a.g.nx_;
     const unsigned nxy = (unsigned)a.g.nxy;
-    const int txv = min(tx, (int)a.g.nx_ - x0), tyv = min(ty, (int)a.g.jhi - 1 - y0);
+    const int txv = min(tx, nx_ - x0), tyv = min(a.ty, (int)a.g.jhi - 1 - y0);
     const int ncells = txv * tyv;
     const int pdp = px * dp;
-    // records of the cell being stepped and of the next one (prefetched)
+
+    // this lane's cell of phase 2 (c = lane mod 16), loaded now so that the
+    // loads land during the streaming
+    const int c = lane & (kUnitCells - 1), h = lane >> 4;
+    const bool cact = c < ncells;
+    const int ccx = cact ? c % txv : 0, ccy = cact ? c / txv : 0;
+    const int cij = (1 + x0 + ccx) + (1 + y0 + ccy) * nxn;
+    const uint8_t cfl = cact ? a.flags[cij] : (uint8_t)3;
+    float u1 = 0.f, u2 = 0.f, lor = 1.f, adt = 0.f, eta = 0.f, k0 = 0.f, k3 = 0.f, kak0 = 0.f, scale = 1.f;
+    if (cact && !(cfl & 1))
+    {
+        u1 = __ldg(a.u1 + cij), u2 = __ldg(a.u2 + cij), lor = __ldg(a.lor + cij), adt = __ldg(a.adt + cij);
+        eta = __ldg(a.eta + cij), k0 = __ldg(a.k0 + cij), k3 = __ldg(a.k3 + cij), kak0 = __ldg(a.ka + cij) + k0;
+    }
+    if (CURVED && cact)
+        scale = __ldg(a.ia3 + cij);
+
+    // ---- phase 1: stream every cell, lanes over the directions ----
     uint4 rc[P], rn[P];
     auto load_recs = [&](uint4(&r)[P], int k) {
-        const int cx = k % txv, cy = k / txv;
-        const int c = (x0 + cx) + (y0 + cy) * (int)a.g.nx_; // interior cell index of node (i, j)
+        const int cell = (x0 + k % txv) + (y0 + k / txv) * nx_; // interior cell index
 #pragma unroll
         for (int p = 0; p < P; p++)
         {
             const int d = lane + 32 * p;
-            r[p] = d < nd ? __ldcs(a.rec + (unsigned)c * (unsigned)nd + (unsigned)d) : make_uint4(0u, 0u, 0u, 0u);
+            r[p] = d < nd ? __ldcs(a.rec + (unsigned)cell * (unsigned)nd + (unsigned)d) : make_uint4(0u, 0u, 0u, 0u);
         }
     };
     if (CURVED)
@@ -263,21 +270,9 @@ __device__ __forceinline__ bool step_tile32(const Step32Args &a, const DirTable 
             load_recs(rn, k + 1);
         const int cx = k % txv, cy = k / txv;
         const int i = 1 + x0 + cx, j = 1 + y0 + cy;
-        const int ij = i + j * nxn;
-        const uint8_t fl = a.flags[ij];
-        const bool live = !(CURVED && (fl & 2));
-        const bool collides = !(fl & 1);
-        // per-cell fields, loaded before the gather so that they land meanwhile
-        float u1 = 0.f, u2 = 0.f, lor = 1.f, adt = 0.f, eta = 0.f, k0 = 0.f, k3 = 0.f, kak0 = 0.f;
-        if (collides)
-        {
-            u1 = __ldg(a.u1 + ij), u2 = __ldg(a.u2 + ij), lor = __ldg(a.lor + ij), adt = __ldg(a.adt + ij);
-            eta = __ldg(a.eta + ij), k0 = __ldg(a.k0 + ij), k3 = __ldg(a.k3 + ij), kak0 = __ldg(a.ka + ij) + k0;
-        }
-        const float scale = CURVED ? __ldg(a.ia3 + ij) : 1.f;
-        // patch offset of node (i - 1, j - 1), the cell's lower-left neighbour
-        const float *cellp = patch + (cy * px + cx) * dp;
-        float S[P];
+        const bool live = !(CURVED && (__shfl_sync(0xffffffffu, (int)cfl, k) & 2));
+        const float *cellp = patch + (cy * px + cx) * dp; // node (i - 1, j - 1)
+        float *Sk = S + k * ss;
 #pragma unroll
         for (int p = 0; p < P; p++)
         {
@@ -289,10 +284,8 @@ __device__ __forceinline__ bool step_tile32(const Step32Args &a, const DirTable 
                 {
                     const uint4 r = rc[p];
                     if (r.w >> 31)
-                        v = stream_far32(a.Iin,
-                                         __ldg(a.side + (unsigned)((x0 + cx) + (y0 + cy) * (int)a.g.nx_) *
-                                                            (unsigned)nd +
-                                               (unsigned)d),
+                        v = stream_far32(a.Iin, __ldg(a.side + (unsigned)((x0 + cx) + (y0 + cy) * nx_) * (unsigned)nd +
+                                                      (unsigned)d),
                                          dp, nxn, (int)a.g.ny, nd, a.ng, rowtab, dt.q, dt.p, dt.inv_q, i, j);
                     else
                     {
@@ -316,48 +309,82 @@ __device__ __forceinline__ bool step_tile32(const Step32Args &a, const DirTable 
                         v = __uint_as_float(r.w) * fmaf(fy, f1 - f0, f0);
                     }
                 }
-                else if (L.near[p])
+                else if (LF.near[p])
                 {
-                    const float *b = cellp + L.off[p];
+                    const float *b = cellp + LF.off[p];
                     const float c00 = b[0], c10 = b[dp], c01 = b[pdp], c11 = b[pdp + dp];
-                    const float f0 = fmaf(L.fx[p], c10 - c00, c00);
-                    const float f1 = fmaf(L.fx[p], c11 - c01, c01);
-                    v = fmaf(L.fy[p], f1 - f0, f0);
+                    const float f0 = fmaf(LF.fx[p], c10 - c00, c00);
+                    const float f1 = fmaf(LF.fx[p], c11 - c01, c01);
+                    v = fmaf(LF.fy[p], f1 - f0, f0);
                 }
                 else
-                    v = stream_flat_far32(a.Iin, L.ox[p], L.oy[p], dp, nxn, (int)a.g.ny, d, i, j);
+                    v = stream_flat_far32(a.Iin, LF.ox[p], LF.oy[p], dp, nxn, (int)a.g.ny, d, i, j);
             }
-            S[p] = v;
+            if (d < nd)
+                Sk[d] = v;
         }
-        // moments of the streamed values: per-lane two-sums over the passes,
-        // then the compensated butterfly over the lanes
-        float m[6], e[6];
+        if (CURVED)
+        {
+#pragma unroll
+            for (int p = 0; p < P; p++)
+                rc[p] = rn[p];
+        }
+    }
+    __syncwarp();
+    next(); // the patch buffer is free: the next tile's copy lands during phases 2 and 3
+
+    // ---- phase 2: moments and collide, two lanes per cell ----
+    if (cact)
+    {
+        float *Sc = S + c * ss;
+        // Kahan sums of FP32 partial sums over chunks of 8 of the lane's directions
+        float ks[6], kc[6], pp[6];
+#pragma unroll
+        for (int q = 0; q < 6; q++)
+            ks[q] = kc[q] = pp[q] = 0.f;
+        int n_in_chunk = 0;
+        for (int d = h; d < nd; d += 2)
+        {
+            const float v = Sc[d];
+            const float4 c0 = dirc[2 * d], c1 = dirc[2 * d + 1];
+            pp[0] = fmaf(c0.x, v, pp[0]);
+            pp[1] = fmaf(c0.y, v, pp[1]);
+            pp[2] = fmaf(c0.z, v, pp[2]);
+            pp[3] = fmaf(c0.w, v, pp[3]);
+            pp[4] = fmaf(c1.x, v, pp[4]);
+            pp[5] = fmaf(c1.y, v, pp[5]);
+            if (++n_in_chunk == 8)
+            {
+                n_in_chunk = 0;
+#pragma unroll
+                for (int q = 0; q < 6; q++)
+                {
+                    const float y = pp[q] - kc[q];
+                    const float t = ks[q] + y;
+                    kc[q] = (t - ks[q]) - y;
+                    ks[q] = t;
+                    pp[q] = 0.f;
+                }
+            }
+        }
+        float m[6];
 #pragma unroll
         for (int q = 0; q < 6; q++)
         {
-            // (products rounded on their own: an FMA would break the two-sum)
-            m[q] = __fmul_rn(L.c[0][q], S[0]);
-            e[q] = 0.f;
-#pragma unroll
-            for (int p = 1; p < P; p++)
-                two_sum_acc(m[q], e[q], __fmul_rn(L.c[p][q], S[p]), 0.f);
+            // the chunk in progress, then the two lanes' compensated sums
+            // combined symmetrically (an exact two-sum of their sums, plus
+            // both compensations), so that both lanes hold the same moments
+            const float y = pp[q] - kc[q];
+            const float t = ks[q] + y;
+            kc[q] = (t - ks[q]) - y;
+            ks[q] = t;
+            const float os = __shfl_xor_sync(0xffffffffu, ks[q], 16), oc = __shfl_xor_sync(0xffffffffu, kc[q], 16);
+            const float x = ks[q] + os;
+            const float bp = x - ks[q];
+            const float err = (ks[q] - (x - bp)) + (os - bp);
+            m[q] = x + (err - (kc[q] + oc));
         }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1)
-#pragma unroll
-            for (int q = 0; q < 6; q++)
-            {
-                const float bs = __shfl_xor_sync(0xffffffffu, m[q], o), be = __shfl_xor_sync(0xffffffffu, e[q], o);
-                two_sum_acc(m[q], e[q], bs, be);
-            }
-#pragma unroll
-        for (int q = 0; q < 6; q++)
-            m[q] += e[q];
-
-        float out[P];
-#pragma unroll
-        for (int p = 0; p < P; p++)
-            out[p] = S[p] * scale;
+        const bool collides = !(cfl & 1);
         if (collides)
         {
             int cycles = 0;
@@ -380,20 +407,17 @@ __device__ __forceinline__ bool step_tile32(const Step32Args &a, const DirTable 
             }
             else
             {
-                // per-direction sums over the warp (plain FP32 butterfly)
 #pragma unroll
                 for (int q = 0; q < 6; q++)
                     A6[q] = B6[q] = C6[q] = D6[q] = 0.f;
-#pragma unroll
-                for (int p = 0; p < P; p++)
+                for (int d = h; d < nd; d += 2)
                 {
-                    if (lane + 32 * p >= nd)
-                        continue;
-                    const float n1 = L.n1[p], n2 = L.n2[p], w = L.c[p][0];
-                    float g, h, q1, q2;
-                    collide_coeffs32(n1, n2, u1, u2, lor, adt, kak0, g, h, q1, q2);
+                    const float4 c0 = dirc[2 * d], c1 = dirc[2 * d + 1];
+                    const float n1 = c1.z, n2 = c1.w, w = c0.x;
+                    float g, hh, q1, q2;
+                    collide_coeffs32(n1, n2, u1, u2, lor, adt, kak0, g, hh, q1, q2);
                     const float mu[6] = {1.f, n1, n2, n1 * n1, n1 * n2, n2 * n2};
-                    const float gs = w * g * S[p], wh = w * h;
+                    const float gs = w * g * Sc[d], wh = w * hh;
 #pragma unroll
                     for (int q = 0; q < 6; q++)
                     {
@@ -404,15 +428,13 @@ __device__ __forceinline__ bool step_tile32(const Step32Args &a, const DirTable 
                     }
                 }
 #pragma unroll
-                for (int o = 16; o > 0; o >>= 1)
-#pragma unroll
-                    for (int q = 0; q < 6; q++)
-                    {
-                        A6[q] += __shfl_xor_sync(0xffffffffu, A6[q], o);
-                        B6[q] += __shfl_xor_sync(0xffffffffu, B6[q], o);
-                        C6[q] += __shfl_xor_sync(0xffffffffu, C6[q], o);
-                        D6[q] += __shfl_xor_sync(0xffffffffu, D6[q], o);
-                    }
+                for (int q = 0; q < 6; q++)
+                {
+                    A6[q] += __shfl_xor_sync(0xffffffffu, A6[q], 16);
+                    B6[q] += __shfl_xor_sync(0xffffffffu, B6[q], 16);
+                    C6[q] += __shfl_xor_sync(0xffffffffu, C6[q], 16);
+                    D6[q] += __shfl_xor_sync(0xffffffffu, D6[q], 16);
+                }
             }
             float diff = 1.f;
             float fE = 0.f, fFx = 0.f, fFy = 0.f;
@@ -440,63 +462,66 @@ __device__ __forceinline__ bool step_tile32(const Step32Args &a, const DirTable 
                 }
                 diff = sqrtf(s2);
             }
-            // the intensities of the last iterate; its moments m are the stored ones
+            // the intensities of the last iterate (its moments m are the stored ones)
             const float ee = eta + k0 * fE;
             const float ra = h0 * ee, rb1 = h0 * k3 * fFx, rb2 = h0 * k3 * fFy;
-#pragma unroll
-            for (int p = 0; p < P; p++)
+            for (int d = h; d < nd; d += 2)
             {
-                const float n1 = L.n1[p], n2 = L.n2[p];
+                const float4 c1 = dirc[2 * d + 1];
+                const float n1 = c1.z, n2 = c1.w;
                 float v;
                 if (rest)
-                    v = fmaf(g0, S[p], fmaf(rb1, n1, fmaf(rb2, n2, ra)));
+                    v = fmaf(g0, Sc[d], fmaf(rb1, n1, fmaf(rb2, n2, ra)));
                 else
                 {
-                    float g, h, q1, q2;
-                    collide_coeffs32(n1, n2, u1, u2, lor, adt, kak0, g, h, q1, q2);
-                    v = g * S[p] + h * (ee + k3 * (q1 * fFx + q2 * fFy));
+                    float g, hh, q1, q2;
+                    collide_coeffs32(n1, n2, u1, u2, lor, adt, kak0, g, hh, q1, q2);
+                    v = g * Sc[d] + hh * (ee + k3 * (q1 * fFx + q2 * fFy));
                 }
-                out[p] = v * scale;
+                Sc[d] = v * scale;
             }
-            st.sum += (unsigned)cycles;
-            st.max = max(st.max, (unsigned)cycles);
+            if (h == 0)
+            {
+                st.sum += (unsigned)cycles;
+                st.max = max(st.max, (unsigned)cycles);
+            }
         }
-        // the cell's new state, coalesced along the directions (and the
-        // mirrored directions 0..3 after the last one)
+        else if (CURVED)
+        {
+            for (int d = h; d < nd; d += 2)
+                Sc[d] *= scale;
+        }
+#pragma unroll
+        for (int q = 0; q < 3; q++)
+            a.mom[(unsigned)cij + (unsigned)(3 * h + q) * nxy] = h ? m[3 + q] : m[q];
+    }
+    __syncwarp();
+
+    // ---- phase 3: the cells' new state, coalesced along the directions
+    // (and the mirrored directions 0..3 after the last one) ----
+    for (int k = 0; k < ncells; k++)
+    {
+        const int ij = (1 + x0 + k % txv) + (1 + y0 + k / txv) * nxn;
         float *o = a.Iout + (unsigned)ij * (unsigned)dp;
+        const float *Sk = S + k * ss;
 #pragma unroll
         for (int p = 0; p < P; p++)
         {
             const int d = lane + 32 * p;
             if (d < nd)
-                o[d] = out[p];
-            if (p == 0 && lane < kStateMirror)
-                o[nd + lane] = out[0];
+                o[d] = Sk[d];
         }
-        if (lane < 6)
-        {
-            float mv = m[0];
-#pragma unroll
-            for (int q = 1; q < 6; q++)
-                mv = lane == q ? m[q] : mv;
-            a.mom[(unsigned)ij + (unsigned)lane * nxy] = mv;
-        }
-        if (CURVED)
-        {
-#pragma unroll
-            for (int p = 0; p < P; p++)
-                rc[p] = rn[p];
-        }
+        if (lane < kStateMirror)
+            o[nd + lane] = Sk[lane];
     }
-    __syncwarp();
-    return true;
+    __syncwarp(); // S is rewritten by the next tile's phase 1
 }
 
-// the warp's share of the block's shared memory
-__device__ __forceinline__ float *warp_patch(unsigned char *smem, int patch_stride)
+// the warp's patch and streamed-value buffers in the block's shared memory
+__device__ __forceinline__ float *warp_buffers(unsigned char *smem, int header, int warp_stride)
 {
     const int warp = threadIdx.x >> 5;
-    return reinterpret_cast<float *>(align128(smem + kPatchOffset) + (size_t)warp * (size_t)patch_stride);
+    return reinterpret_cast<float *>(align128(smem + header) + (size_t)warp * (size_t)warp_stride);
 }
 
 // The warp is done taking tiles from counter[0]; the launch's last warp
@@ -523,35 +548,55 @@ __device__ __forceinline__ void flush_stats(const IterStats &st, unsigned long l
     }
 }
 
+__device__ __forceinline__ int take_tile(unsigned *counter)
+{
+    int t = 0;
+    if ((threadIdx.x & 31) == 0)
+        t = (int)atomicAdd(counter, 1u);
+    return __shfl_sync(0xffffffffu, t, 0);
+}
+
+// shared layout of the single-problem kernel: the warps' mbarriers, the
+// row-type table, the direction coefficients, then the warps' buffers
+__device__ __forceinline__ int step32_header(int nd) { return kRowtabOffset + kMaxRowTypes * 12 * 4 + 32 * nd; }
+
 template <bool CURVED, int P>
 __global__ void __launch_bounds__(kThreads, GRLBM_STEP32_MIN_BLOCKS)
-    k_step_prec(const __grid_constant__ Step32Args a, const __grid_constant__ DirTable dt, int patch_stride)
+    k_step_prec(const __grid_constant__ Step32Args a, const __grid_constant__ DirTable dt, int warp_stride)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     float *rowtab = reinterpret_cast<float *>(smem + kRowtabOffset);
-    const int lane = threadIdx.x & 31;
+    float4 *dirc = reinterpret_cast<float4 *>(smem + kRowtabOffset + kMaxRowTypes * 12 * 4);
     const unsigned bar = smem_addr(smem) + 8u * (unsigned)(threadIdx.x >> 5);
-    if (lane == 0)
+    if ((threadIdx.x & 31) == 0)
         mbar_init(bar, 1);
     if (CURVED)
         for (int k = threadIdx.x; k < dt.q * 12; k += kThreads)
             rowtab[k] = dt.rowtab[k];
+    for (int k = threadIdx.x; k < 2 * a.nd; k += kThreads)
+        dirc[k] = reinterpret_cast<const float4 *>(dt.dirc)[k];
     __syncthreads();
-    float *patch = warp_patch(smem, patch_stride);
-    LaneDirs<P> L;
-    load_lane_dirs<P>(L, dt, a.nd, a.dp, a.tx + 2, CURVED);
+    float *patch = warp_buffers(smem, step32_header(a.nd), warp_stride);
+    float *S = patch + a.patch_floats;
+    LaneFlat<P> LF;
+    if (!CURVED)
+        load_lane_flat<P>(LF, dt, a.nd, a.dp, a.tx + 2);
     IterStats st{0ull, 0u};
     unsigned parity = 0;
-    for (;;)
+    int tile = take_tile(a.tiles);
+    if (tile < a.ntiles)
+        stage_tile(a, tile, patch, bar);
+    while (tile < a.ntiles)
     {
-        int tile = 0;
-        if (lane == 0)
-            tile = (int)atomicAdd(a.tiles, 1u);
-        tile = __shfl_sync(0xffffffffu, tile, 0);
-        if (tile >= a.ntiles)
+        if (!wait_tile(a, bar, parity))
             break;
-        if (!step_tile32<CURVED, P>(a, dt, rowtab, L, tile, patch, bar, parity, st))
-            break;
+        int next = a.ntiles;
+        step_unit32<CURVED, P>(a, dt, rowtab, dirc, LF, tile, patch, S, st, [&]() {
+            next = take_tile(a.tiles);
+            if (next < a.ntiles)
+                stage_tile(a, next, patch, bar);
+        });
+        tile = next;
     }
     flush_stats(st, a.iter_sum, a.iter_max);
     retire_warp(a.tiles);
@@ -560,57 +605,78 @@ __global__ void __launch_bounds__(kThreads, GRLBM_STEP32_MIN_BLOCKS)
 // Many problems in one persistent launch: the warps take tiles from one
 // counter over the concatenated tile lists (problem k owns tiles
 // [first_tile[k], first_tile[k + 1])) and step each with the single-problem
-// tile function, so every problem's result is the one it gets alone.  A
-// warp reloads its direction constants when its problem changes.
+// tile function, so every problem's result is the one it gets alone.
+__device__ __forceinline__ int batch_item_of(const int *__restrict__ first_tile, int n_items, int tile)
+{
+    int lo = 0, hi = n_items - 1;
+    while (lo < hi)
+    {
+        const int mid = (lo + hi + 1) >> 1;
+        if (first_tile[mid] <= tile)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
 template <int P>
 __global__ void __launch_bounds__(kThreads, GRLBM_STEP32_MIN_BLOCKS)
     k_step_batch32(const Batch32Item *__restrict__ items, const int *__restrict__ first_tile, int n_items,
-                   int total_tiles, int flip, unsigned *counters, int patch_stride)
+                   int total_tiles, int flip, unsigned *counters, int warp_stride)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    const int lane = threadIdx.x & 31;
     const unsigned bar = smem_addr(smem) + 8u * (unsigned)(threadIdx.x >> 5);
-    if (lane == 0)
+    if ((threadIdx.x & 31) == 0)
         mbar_init(bar, 1);
     __syncthreads();
-    float *patch = warp_patch(smem, patch_stride);
-    LaneDirs<P> L;
+    float *buf = warp_buffers(smem, kRowtabOffset, warp_stride);
+    LaneFlat<P> LF;
     IterStats st{0ull, 0u};
     unsigned parity = 0;
     int cur = -1;
     const Step32Args *ca = nullptr;
-    for (;;)
+    int tile = take_tile(counters);
+    if (tile < total_tiles)
     {
-        int tile = 0;
-        if (lane == 0)
-            tile = (int)atomicAdd(counters, 1u);
-        tile = __shfl_sync(0xffffffffu, tile, 0);
-        if (tile >= total_tiles)
+        const Batch32Item &it = items[batch_item_of(first_tile, n_items, tile)];
+        const Step32Args &na = it.a[it.cur0 ^ flip];
+        stage_tile(na, tile - first_tile[batch_item_of(first_tile, n_items, tile)], buf, bar);
+    }
+    while (tile < total_tiles)
+    {
+        const int k = batch_item_of(first_tile, n_items, tile);
+        const Batch32Item &it = items[k];
+        const Step32Args &ia = it.a[it.cur0 ^ flip];
+        if (!wait_tile(ia, bar, parity))
             break;
-        int lo = 0, hi = n_items - 1;
-        while (lo < hi)
-        {
-            const int mid = (lo + hi + 1) >> 1;
-            if (first_tile[mid] <= tile)
-                lo = mid;
-            else
-                hi = mid - 1;
-        }
-        const Batch32Item &it = items[lo];
-        if (lo != cur)
+        if (k != cur)
         {
             if (ca)
                 flush_stats(st, ca->iter_sum, ca->iter_max);
             st = IterStats{0ull, 0u};
-            cur = lo;
-            ca = &it.a[it.cur0 ^ flip];
-            load_lane_dirs<P>(L, *it.dt, ca->nd, ca->dp, ca->tx + 2, it.curved != 0);
+            cur = k;
+            ca = &ia;
+            if (!it.curved)
+                load_lane_flat<P>(LF, *it.dt, ia.nd, ia.dp, ia.tx + 2);
         }
-        const int local = tile - first_tile[lo];
-        const bool ok = it.curved ? step_tile32<true, P>(*ca, *it.dt, it.dt->rowtab, L, local, patch, bar, parity, st)
-                                  : step_tile32<false, P>(*ca, *it.dt, it.dt->rowtab, L, local, patch, bar, parity, st);
-        if (!ok)
-            break; // the barrier's phase is unknown: the warp stops (the fault word is set)
+        int next = total_tiles;
+        auto stage_next = [&]() {
+            next = take_tile(counters);
+            if (next < total_tiles)
+            {
+                const int nk = batch_item_of(first_tile, n_items, next);
+                const Batch32Item &nit = items[nk];
+                stage_tile(nit.a[nit.cur0 ^ flip], next - first_tile[nk], buf, bar);
+            }
+        };
+        const float4 *dirc = reinterpret_cast<const float4 *>(it.dt->dirc);
+        float *S = buf + ia.patch_floats;
+        if (it.curved)
+            step_unit32<true, P>(ia, *it.dt, it.dt->rowtab, dirc, LF, tile - first_tile[k], buf, S, st, stage_next);
+        else
+            step_unit32<false, P>(ia, *it.dt, it.dt->rowtab, dirc, LF, tile - first_tile[k], buf, S, st, stage_next);
+        tile = next;
     }
     if (ca)
         flush_stats(st, ca->iter_sum, ca->iter_max);
@@ -639,14 +705,22 @@ int step32_passes(int nd)
     return -1;
 }
 
-int step32_patch_stride(int tx, int ty, int dp) { return ((tx + 2) * (ty + 2) * dp * 4 + 127) / 128 * 128; }
+int step32_s_stride(int nd) { return nd + ((2 - nd) % 32 + 32) % 32; }
 
-size_t step32_smem_base() { return (size_t)kPatchOffset + 128; }
+int step32_patch_floats(int tx, int ty, int dp) { return ((tx + 2) * (ty + 2) * dp + 31) / 32 * 32; }
 
-size_t step32_smem(int tx, int ty, int dp)
+int step32_warp_stride(int tx, int ty, int dp, int nd)
 {
-    return step32_smem_base() + (size_t)kWarps * (size_t)step32_patch_stride(tx, ty, dp);
+    return ((step32_patch_floats(tx, ty, dp) + kUnitCells * step32_s_stride(nd)) * 4 + 127) / 128 * 128;
 }
+
+size_t step32_smem(int tx, int ty, int dp, int nd)
+{
+    const int header = kRowtabOffset + kMaxRowTypes * 12 * 4 + 32 * nd;
+    return (size_t)header + 128 + (size_t)kWarps * (size_t)step32_warp_stride(tx, ty, dp, nd);
+}
+
+size_t step32_batch_smem(int warp_stride) { return (size_t)kRowtabOffset + 128 + (size_t)kWarps * warp_stride; }
 
 cudaError_t prepare_step32()
 {
@@ -692,8 +766,8 @@ void launch_step32(const Step32Args &a, const DirTable &dt, bool curved, int P, 
 {
     if (a.ntiles <= 0)
         return;
-    const size_t smem = step32_smem(a.tx, a.ty, a.dp);
-    const int stride = step32_patch_stride(a.tx, a.ty, a.dp);
+    const size_t smem = step32_smem(a.tx, a.ty, a.dp, a.nd);
+    const int stride = step32_warp_stride(a.tx, a.ty, a.dp, a.nd);
     const unsigned grid = (unsigned)std::max(1, std::min(blocks, (int)nblk(a.ntiles, kWarps)));
 #define GRLBM_LAUNCH(PP)                                                                                    \
     if (P == PP)                                                                                            \
@@ -714,13 +788,13 @@ void launch_step32(const Step32Args &a, const DirTable &dt, bool curved, int P, 
 }
 
 void launch_step_batch32(const Batch32Item *items, const int *first_tile, int n_items, int total_tiles, int flip,
-                         unsigned *counters, int P, int blocks, size_t smem, int patch_stride, cudaStream_t s)
+                         unsigned *counters, int P, int blocks, size_t smem, int warp_stride, cudaStream_t s)
 {
 #define GRLBM_LAUNCH(PP)                                                                                    \
     if (P == PP)                                                                                            \
     {                                                                                                       \
         k_step_batch32<PP><<<blocks, kThreads, smem, s>>>(items, first_tile, n_items, total_tiles, flip,    \
-                                                          counters, patch_stride);                          \
+                                                          counters, warp_stride);                           \
         return;                                                                                             \
     }
     GRLBM_LAUNCH(1)

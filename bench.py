@@ -73,6 +73,13 @@ def args_parse():
                    help="steps of the adjoint workload (256^2 x 48, checkpoints every 20); 0 skips it")
     p.add_argument("--batch-steps", type=int, default=64,
                    help="timed steps of the batched form (64 uneven problems); 0 skips it")
+    p.add_argument("--profile", default=None,
+                   choices=["fp32", "fp64", "fp32-adaptive", "fp64-adaptive", "batch", "adjoint"],
+                   help="instead of measuring: build one problem and run --profile-steps steps of it, one call "
+                        "per step, for a profiler to capture (no timing, no JSON line)")
+    p.add_argument("--profile-steps", type=int, default=6)
+    p.add_argument("--profile-workload", default="curved_scatter")
+    p.add_argument("--profile-batch", type=int, default=16, help="problems of the batched form in --profile batch")
     return p.parse_args()
 
 
@@ -356,6 +363,83 @@ def run_adjoint(G, W, a, local):
             "timing": "host clock around synchronous calls; the backward includes the forward recompute"}
 
 
+def run_profile(a):
+    """A problem for a profiler to capture: the bench workload (or
+    --profile-workload) in one form, stepped one call at a time, so that
+    the profiler can skip the warm-up launches; or the batched form
+    (--profile-batch uneven problems of seed 10); or the adjoint workload
+    (forward and one backward of --profile-steps steps)."""
+    G = importlib.import_module("2dradiation_b200")
+    W = G.workloads
+    n = a.profile_steps
+    if a.profile == "batch":
+        probs = [G.prepare(c, G.PRECISION_FP32) for c in W.batch_instances(count=a.profile_batch, seed=10)]
+        with G.Batch(probs) as b:
+            for _ in range(n):
+                b.step(1)
+        print("profile: batch of", a.profile_batch, "E sum", float(sum(r.moments_if()["E"].sum() for r in probs)))
+        for r in probs:
+            r.close()
+        return
+    if a.profile == "adjoint":
+        r = G.prepare(W.adjoint_case(steps=n), G.PLAIN_FP64)
+        with G.Adjoint(r, 20) as adj:
+            r.set_intensity(np.zeros(r.nxy * r.nd))
+            adj.forward(n)
+            g = adj.backward(r.moments_if()["E"])
+        print("profile: adjoint", n, "steps, |dL/deta|", float(np.linalg.norm(g["eta"])))
+        r.close()
+        return
+    kw = dict(nx_=a.nx, ny_=a.nx, n_dir=a.dirs, steps=n)
+    if a.profile_workload != "flat_beam":
+        kw["n_fourier"] = a.fourier
+    case = W.make_case(a.profile_workload, **kw)
+    if a.profile.endswith("adaptive"):
+        case["streaming_type"] = W.FLAT_ADAPTIVE if case["streaming_type"] == W.FLAT_FIXED else W.CURVED_ADAPTIVE
+    with G.prepare(case, G.PRECISION_FP32 if a.profile.startswith("fp32") else G.PLAIN_FP64) as r:
+        for _ in range(n):
+            r.step(1)
+        print("profile:", a.profile, a.profile_workload, a.nx, a.dirs, "E sum", float(r.moments_if()["E"].sum()))
+
+
+def run_e2e(G, W, case, prec, a, world, rank, local, pg, dev):
+    """End to end through the C-ABI with pinned host buffers: every rep
+    uploads the fields and the initial intensities, runs the whole
+    `e2e_steps`-step simulation and reads the moments back (host clock, max
+    over ranks, median of the timed reps after an untimed one).  Returns the
+    seconds per rep and the moments of the last rep."""
+    import torch
+    f = case["fields"]
+    host = {k: torch.from_numpy(np.ascontiguousarray(v, dtype=np.float64)).pin_memory().numpy()
+            for k, v in f.items() if k != "is_initial"}
+    I0 = torch.zeros(W.nxy(case) * a.dirs, dtype=torch.float64).pin_memory().numpy()
+    mom = {k: torch.zeros(W.nxy(case), dtype=torch.float64).pin_memory().numpy()
+           for k in ("E", "Fx", "Fy", "Pxx", "Pxy", "Pyy")}
+    r, advance, slab = open_form(G, case, prec, world, rank, local, pg)
+    e2e_t = []
+    try:
+        for rep in range(a.e2e_reps + 1):
+            barrier(pg, dev)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            r.set_fields(host)
+            r.set_intensity(I0)
+            if slab is None:
+                r.step(a.e2e_steps)
+            else:
+                slab.step(a.e2e_steps)
+            r.moments_if(mom)
+            t1 = time.perf_counter()
+            if rep > 0:
+                e2e_t.append(t1 - t0)
+        lo, hi = slab.band if slab is not None else (1, a.nx + 1)
+        band = {k: v[lo * (a.nx + 2):hi * (a.nx + 2)].copy() for k, v in mom.items()}
+        iters = r.stats()["average_iterations"]
+    finally:
+        r.close()
+    return max_over_ranks(statistics.median(e2e_t), pg, dev), band, iters
+
+
 def run_grlbm(a, world, rank, local, pg):
     import torch
     G = importlib.import_module("2dradiation_b200")
@@ -383,33 +467,12 @@ def run_grlbm(a, world, rank, local, pg):
             states[name] = {k: v[lo * (a.nx + 2):hi * (a.nx + 2)] for k, v in r.moments_if().items()}
             forms[name]["iters"] = r.stats()
             r.close()
-        # e2e through the C-ABI with pinned host buffers
-        f = case["fields"]
-        host = {k: torch.from_numpy(np.ascontiguousarray(v, dtype=np.float64)).pin_memory().numpy()
-                for k, v in f.items() if k != "is_initial"}
-        I0 = torch.zeros(W.nxy(case) * nd, dtype=torch.float64).pin_memory().numpy()
-        mom = {k: torch.zeros(W.nxy(case), dtype=torch.float64).pin_memory().numpy()
-               for k in ("E", "Fx", "Fy", "Pxx", "Pxy", "Pyy")}
-        r, advance, slab = open_form(G, case, G.PRECISION_FP32, world, rank, local, pg) if a.e2e_reps > 0 \
-            else (None, None, None)
-        e2e_t = []
-        for rep in range(a.e2e_reps + 1 if r is not None else 0):
-            barrier(pg, dev)
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            r.set_fields(host)
-            r.set_intensity(I0)
-            if slab is None:
-                r.step(a.e2e_steps)
-            else:
-                slab.step(a.e2e_steps)
-            r.moments_if(mom)
-            t1 = time.perf_counter()
-            if rep > 0:
-                e2e_t.append(t1 - t0)
-        if r is not None:
-            r.close()
-        e2e_s = max_over_ranks(statistics.median(e2e_t) if e2e_t else float("nan"), pg, dev)
+        # e2e through the C-ABI with pinned host buffers, both forms; their
+        # moments after the whole run give the metric's accuracy condition
+        e2e = {}
+        if a.e2e_reps > 0:
+            for name, prec in (("fp32", G.PRECISION_FP32), ("fp64", G.PLAIN_FP64)):
+                e2e[name] = run_e2e(G, W, case, prec, a, world, rank, local, pg, dev)
         batched = run_batched(G, W, a, local) if a.batch_steps > 0 and world == 1 else None
         other = run_configs(G, W, local) if not a.no_configs and world == 1 else None
         adjoint = run_adjoint(G, W, a, local) if a.adjoint_steps > 0 and world == 1 else None
@@ -426,8 +489,26 @@ def run_grlbm(a, world, rank, local, pg):
     avg64 = statistics.mean(fp64["ms"]) / 1e3
     ach32 = b32 * units / avg32 / 1e9
     ach64 = b64 * units / avg64 / 1e9
-    E32, E64 = states["fp32"]["E"], states["fp64"]["E"]
     rel = lambda x, y: float(np.linalg.norm(x - y) / max(np.linalg.norm(y), 1e-300))
+    if "fp32" in e2e and "fp64" in e2e:
+        m32, m64 = e2e["fp32"][1], e2e["fp64"][1]
+        accuracy = {k + "_rel_l2_fp32_vs_fp64": max_over_ranks(rel(m32[k], m64[k]), pg, dev)
+                    for k in ("E", "Fx", "Fy")}
+        accuracy.update({"after_steps": a.e2e_steps, "from": "the e2e runs of both forms (same initial state)",
+                         "lambda_iterations_avg": {"fp32": e2e["fp32"][2], "fp64": e2e["fp64"][2]}})
+    else:
+        accuracy = {k + "_rel_l2_fp32_vs_fp64": rel(states["fp32"][k], states["fp64"][k]) for k in ("E", "Fx", "Fy")}
+        accuracy["after_steps"] = a.warmup + a.steps
+
+    def e2e_line(name):
+        if name not in e2e:
+            return None
+        sec = e2e[name][0]
+        return {"value": world * units * a.e2e_steps / sec, "unit": UNIT,
+                "h2d_bytes_per_step": int(8 * (6 * W.nxy(case) + W.nxy(case) * nd)),
+                "d2h_bytes_per_step": int(8 * 6 * W.nxy(case)),
+                "step": f"C-ABI: set fields + set intensities (host) + {a.e2e_steps} solver steps + moments to host",
+                "seconds_per_step": sec}
     line = {
         "metric": METRIC,
         "value": value,
@@ -471,21 +552,18 @@ def run_grlbm(a, world, rank, local, pg):
             "kernels": "k_stream_plain + k_collide_plain (fixed streaming; traffic per step, both kernels)",
         },
         "precision_vs_plain": value / plain,
-        "accuracy": {"E_rel_l2_fp32_vs_fp64": rel(E32, E64),
-                     "Fx_rel_l2_fp32_vs_fp64": rel(states["fp32"]["Fx"], states["fp64"]["Fx"]),
-                     "after_steps": a.warmup + a.steps},
+        # as if the step time scaled with the lambda iterations each form ran
+        # (the FP32 form's moment-space iterations cost O(1) per cell, so this
+        # bounds the iterations' share of the ratio from above)
+        "precision_vs_plain_iteration_normalised": value / plain * fp32["iters"]["average_iterations"]
+        / max(fp64["iters"]["average_iterations"], 1e-30),
+        "accuracy": accuracy,
         "table_build_ms": {"fp32": fp32["table_ms"], "fp64": fp64["table_ms"]},
         "lambda_iterations": {"fp32_avg": fp32["iters"]["average_iterations"],
                               "fp64_avg": fp64["iters"]["average_iterations"],
                               "max": fp64["iters"]["max_iterations"]},
-        "e2e": {
-            "value": world * units * a.e2e_steps / e2e_s,
-            "unit": UNIT,
-            "h2d_bytes_per_step": int(8 * (6 * W.nxy(case) + W.nxy(case) * nd)),
-            "d2h_bytes_per_step": int(8 * 6 * W.nxy(case)),
-            "step": f"C-ABI: set fields + set intensities (host) + {a.e2e_steps} solver steps + moments to host",
-            "seconds_per_step": e2e_s,
-        },
+        "e2e": e2e_line("fp32"),
+        "plain_fp64_e2e": e2e_line("fp64"),
         "gpu_launches": a.steps,
         "batched": batched,
         "other_configs": other,
@@ -518,33 +596,32 @@ def cpu_baseline(a):
 
 
 def run_reference(a, world, rank):
-    """The reference's CPU path, one solver step per bench step.  When the
-    requested steps would not finish in about three minutes at the full grid,
-    each step runs on the same problem at a coarser grid (same domain,
-    directions, Fourier order and fields): the work per cell*direction does
-    not depend on the grid size, so the rate is comparable."""
+    """The reference's CPU path on the bench's own grid, one solver step per
+    bench step.  When the requested steps would not finish in about two and a
+    half minutes, fewer steps are timed (the rate is per cell*direction
+    update, and every step does the same work): the sample says how many."""
     if rank != 0:
         return None
     cores = os.cpu_count() or 1
-    rate_guess = 3.2e6 * cores / 8.0  # measured: 3.2e6 cell*dir/s on 8 Xeon cores at 400x400x64
-    n = a.warmup + a.steps
-    nx = int((150.0 * rate_guess / (max(n, 1) * a.dirs)) ** 0.5)
-    nx = max(32, min(a.nx, nx))
-    sub = argparse.Namespace(**{**vars(a), "nx": nx})
-    res, kind, cores = cpu_run(sub, n)
-    t = res["step_times"][a.warmup:a.warmup + a.steps]
-    units = nx * nx * a.dirs
-    value = units * a.steps / float(np.sum(t))
-    sample = (f"{a.steps} timed solver steps after {a.warmup} warm-up steps on {nx}x{nx} cells "
-              f"(same domain, {a.dirs} directions, Fourier order {a.fourier}); geodesic table build "
-              f"{res['table_time_s']:.1f} s untimed; {'reference built -O3 -ffast-math -fopenmp' if kind == 'ref_fast' else 'oracle restatement'}")
+    rate_guess = 1.2e6 * cores  # measured: 1.9e7 cell*dir/s on 16 host cores at 400x400x64
+    per_step = a.nx * a.nx * a.dirs / rate_guess
+    budget = max(2, int(150.0 / per_step))
+    warm = min(a.warmup, max(1, budget // 10))
+    timed = max(1, min(a.steps, budget - warm))
+    res, kind, cores = cpu_run(a, warm + timed)
+    t = res["step_times"][warm:warm + timed]
+    units = a.nx * a.nx * a.dirs
+    value = units * timed / float(np.sum(t))
+    sample = (f"{timed} timed solver steps (of {a.steps} requested) after {warm} warm-up steps on the full "
+              f"{a.nx}x{a.nx} grid, {a.dirs} directions, Fourier order {a.fourier}; geodesic table build "
+              f"{res['table_time_s']:.1f} s untimed; "
+              f"{'reference built -O3 -ffast-math -fopenmp' if kind == 'ref_fast' else 'oracle restatement'}")
     return {
         "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world,
         "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * float(np.mean(t)),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": workload_name(a), "step": "one solver time step on the host cores (OpenMP)",
-                   "sample_grid": f"{nx}x{nx}"},
+        "config": {"workload": workload_name(a), "step": "one solver time step on the host cores (OpenMP)"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores,
                          "kind": "reference" if kind == "ref_fast" else "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -553,6 +630,9 @@ def run_reference(a, world, rank):
 
 def main():
     a = args_parse()
+    if a.profile:
+        run_profile(a)
+        return
     world, rank, local, pg = dist_setup(a)
     try:
         if a.impl == "reference":

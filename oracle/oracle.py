@@ -221,12 +221,25 @@ def run(case: dict, kind: str = "oracle", metric_override: np.ndarray | None = N
     return res
 
 
-def build(with_reference: bool | None = None, ref_root: str = "/root/reference") -> None:
+def reference_root() -> str:
+    """Where the reference tree is read from: $GRLBM_REFERENCE, else the
+    default of the build recipe (oracle/Makefile, REF ?= ...)."""
+    env = os.environ.get("GRLBM_REFERENCE")
+    if env:
+        return env
+    for line in (HERE / "Makefile").read_text().splitlines():
+        if line.startswith("REF ?="):
+            return line.split("=", 1)[1].strip()
+    return ""
+
+
+def build(with_reference: bool | None = None, ref_root: str | None = None) -> None:
     """Build liboracle.so, and the reference libraries when the reference tree
     is present (or when with_reference is True)."""
     import subprocess
     subprocess.run(["make", "-s", "-C", str(HERE), "oracle"], check=True)
+    ref_root = ref_root or reference_root()
     if with_reference is None:
-        with_reference = os.path.isdir(os.path.join(ref_root, "src"))
+        with_reference = bool(ref_root) and os.path.isdir(os.path.join(ref_root, "src"))
     if with_reference:
         subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF={ref_root}"], check=True)
