@@ -55,6 +55,11 @@ namespace
 {
 constexpr int kWarps = kStep32Warps;
 constexpr int kUnitCells = kStep32UnitCells;
+// cells whose records are loaded ahead of the one being streamed
+#ifndef GRLBM_STEP32_REC_AHEAD
+#define GRLBM_STEP32_REC_AHEAD 3
+#endif
+constexpr int kRecAhead = GRLBM_STEP32_REC_AHEAD;
 constexpr int kThreads = 32 * kWarps;
 // time limits of a staging wait (a copy lands within microseconds) and of the
 // drain of a copy in flight after a wait has run out
@@ -252,22 +257,36 @@ __device__ __forceinline__ void step_unit32(const Step32Args &a, const DirTable 
         scale = __ldg(a.ia3 + cij);
 
     // ---- phase 1: stream every cell, lanes over the directions ----
-    uint4 rc[P], rn[P];
+    // The records of the next kRecAhead cells are in flight while a cell is
+    // streamed: a ring of kRecAhead + 1 register sets, indexed statically
+    // (the cell loop is unrolled by the ring's length).
+    constexpr int R = kRecAhead + 1;
+    uint4 rq[R][P];
     auto load_recs = [&](uint4(&r)[P], int k) {
         const int cell = (x0 + k % txv) + (y0 + k / txv) * nx_; // interior cell index
 #pragma unroll
         for (int p = 0; p < P; p++)
         {
             const int d = lane + 32 * p;
-            r[p] = d < nd ? __ldcs(a.rec + (unsigned)cell * (unsigned)nd + (unsigned)d) : make_uint4(0u, 0u, 0u, 0u);
+            r[p] = (k < ncells && d < nd) ? __ldcs(a.rec + (unsigned)cell * (unsigned)nd + (unsigned)d)
+                                          : make_uint4(0u, 0u, 0u, 0u);
         }
     };
     if (CURVED)
-        load_recs(rc, 0);
-    for (int k = 0; k < ncells; k++)
     {
-        if (CURVED && k + 1 < ncells)
-            load_recs(rn, k + 1);
+#pragma unroll
+        for (int u = 0; u < R - 1; u++)
+            load_recs(rq[u], u);
+    }
+    for (int k0 = 0; k0 < ncells; k0 += R)
+#pragma unroll
+    for (int u = 0; u < R; u++)
+    {
+        const int k = k0 + u;
+        if (k >= ncells)
+            break;
+        if (CURVED)
+            load_recs(rq[(u + R - 1) % R], k + R - 1);
         const int cx = k % txv, cy = k / txv;
         const int i = 1 + x0 + cx, j = 1 + y0 + cy;
         const bool live = !(CURVED && (__shfl_sync(0xffffffffu, (int)cfl, k) & 2));
@@ -282,7 +301,7 @@ __device__ __forceinline__ void step_unit32(const Step32Args &a, const DirTable 
             {
                 if (CURVED)
                 {
-                    const uint4 r = rc[p];
+                    const uint4 r = rq[u][p];
                     if (r.w >> 31)
                         v = stream_far32(a.Iin, __ldg(a.side + (unsigned)((x0 + cx) + (y0 + cy) * nx_) * (unsigned)nd +
                                                       (unsigned)d),
@@ -323,12 +342,6 @@ __device__ __forceinline__ void step_unit32(const Step32Args &a, const DirTable 
             if (d < nd)
                 Sk[d] = v;
         }
-        if (CURVED)
-        {
-#pragma unroll
-            for (int p = 0; p < P; p++)
-                rc[p] = rn[p];
-        }
     }
     __syncwarp();
     next(); // the patch buffer is free: the next tile's copy lands during phases 2 and 3
@@ -336,6 +349,8 @@ __device__ __forceinline__ void step_unit32(const Step32Args &a, const DirTable 
     // ---- phase 2: moments and collide, two lanes per cell ----
     if (cact)
     {
+        // the two lanes of this cell (every shuffle of phase 2 is between them)
+        const unsigned pair = 0x10001u << c;
         float *Sc = S + c * ss;
         // Kahan sums of FP32 partial sums over chunks of 8 of the lane's directions
         float ks[6], kc[6], pp[6];
@@ -378,7 +393,7 @@ __device__ __forceinline__ void step_unit32(const Step32Args &a, const DirTable 
             const float t = ks[q] + y;
             kc[q] = (t - ks[q]) - y;
             ks[q] = t;
-            const float os = __shfl_xor_sync(0xffffffffu, ks[q], 16), oc = __shfl_xor_sync(0xffffffffu, kc[q], 16);
+            const float os = __shfl_xor_sync(pair, ks[q], 16), oc = __shfl_xor_sync(pair, kc[q], 16);
             const float x = ks[q] + os;
             const float bp = x - ks[q];
             const float err = (ks[q] - (x - bp)) + (os - bp);
@@ -430,10 +445,10 @@ __device__ __forceinline__ void step_unit32(const Step32Args &a, const DirTable 
 #pragma unroll
                 for (int q = 0; q < 6; q++)
                 {
-                    A6[q] += __shfl_xor_sync(0xffffffffu, A6[q], 16);
-                    B6[q] += __shfl_xor_sync(0xffffffffu, B6[q], 16);
-                    C6[q] += __shfl_xor_sync(0xffffffffu, C6[q], 16);
-                    D6[q] += __shfl_xor_sync(0xffffffffu, D6[q], 16);
+                    A6[q] += __shfl_xor_sync(pair, A6[q], 16);
+                    B6[q] += __shfl_xor_sync(pair, B6[q], 16);
+                    C6[q] += __shfl_xor_sync(pair, C6[q], 16);
+                    D6[q] += __shfl_xor_sync(pair, D6[q], 16);
                 }
             }
             float diff = 1.f;
