@@ -554,12 +554,23 @@ __device__ __forceinline__ void retire_warp(unsigned *counter)
     }
 }
 
+// The warp's lambda-iteration statistics (each lane counted its own cells):
+// summed and maximised over the lanes, one atomic each.  Called by the whole
+// warp.
 __device__ __forceinline__ void flush_stats(const IterStats &st, unsigned long long *iter_sum, unsigned *iter_max)
 {
-    if ((threadIdx.x & 31) == 0 && st.sum)
+    unsigned long long sum = st.sum;
+    unsigned mx = st.max;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
     {
-        atomicAdd(iter_sum, st.sum);
-        atomicMax(iter_max, st.max);
+        sum += __shfl_xor_sync(0xffffffffu, sum, o);
+        mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    }
+    if ((threadIdx.x & 31) == 0 && sum)
+    {
+        atomicAdd(iter_sum, sum);
+        atomicMax(iter_max, mx);
     }
 }
 
