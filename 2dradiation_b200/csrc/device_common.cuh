@@ -402,7 +402,8 @@ cudaError_t step32_occupancy(int P, bool curved, bool batch, size_t smem, int *b
 // blocks: the persistent grid (resident blocks per SM times the SMs)
 void launch_step32(const Step32Args &a, const DirTable &dt, bool curved, int P, int blocks, cudaStream_t s);
 void launch_step_batch32(const Batch32Item *items, const int *first_tile, int n_items, int total_tiles, int flip,
-                         unsigned *counters, int P, int blocks, size_t smem, int warp_stride, cudaStream_t s);
+                         unsigned *counters, int P, int blocks, size_t smem, int warp_stride, int s_offset,
+                         cudaStream_t s);
 // The TMA map the step stages a cell-major state of nx x ny nodes through,
 // for tiles of tx x ty cells.
 cudaError_t encode_state_map32(CUtensorMap *map, const float *state, int64_t nx, int64_t ny, int dp, int tx, int ty);

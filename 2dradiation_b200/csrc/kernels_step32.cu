@@ -55,11 +55,6 @@ namespace
 {
 constexpr int kWarps = kStep32Warps;
 constexpr int kUnitCells = kStep32UnitCells;
-// cells whose records are loaded ahead of the one being streamed
-#ifndef GRLBM_STEP32_REC_AHEAD
-#define GRLBM_STEP32_REC_AHEAD 3
-#endif
-constexpr int kRecAhead = GRLBM_STEP32_REC_AHEAD;
 constexpr int kThreads = 32 * kWarps;
 // time limits of a staging wait (a copy lands within microseconds) and of the
 // drain of a copy in flight after a wait has run out
@@ -257,90 +252,133 @@ __device__ __forceinline__ void step_unit32(const Step32Args &a, const DirTable 
         scale = __ldg(a.ia3 + cij);
 
     // ---- phase 1: stream every cell, lanes over the directions ----
-    // The records of the next kRecAhead cells are in flight while a cell is
-    // streamed: a ring of kRecAhead + 1 register sets, indexed statically
-    // (the cell loop is unrolled by the ring's length).
-    constexpr int R = kRecAhead + 1;
-    uint4 rq[R][P];
-    auto load_recs = [&](uint4(&r)[P], int k) {
-        const int cell = (x0 + k % txv) + (y0 + k / txv) * nx_; // interior cell index
+    // Lane c (< 16) holds its cell's interior index, node index, patch offset
+    // and flags; the cell loop reads them by shuffle.  Cell k's records are
+    // loaded while cell k - 1 streams, and cell k + 3's are prefetched into L2.
+    const int ccell = (x0 + ccx) + (y0 + ccy) * nx_;
+    const int cpo = (ccy * px + ccx) * dp;
+    uint4 rc[P], rn[P];
+    auto load_recs = [&](uint4(&r)[P], int cell) {
 #pragma unroll
         for (int p = 0; p < P; p++)
         {
             const int d = lane + 32 * p;
-            r[p] = (k < ncells && d < nd) ? __ldcs(a.rec + (unsigned)cell * (unsigned)nd + (unsigned)d)
-                                          : make_uint4(0u, 0u, 0u, 0u);
+            r[p] = d < nd ? __ldcs(a.rec + (unsigned)cell * (unsigned)nd + (unsigned)d) : make_uint4(0u, 0u, 0u, 0u);
+        }
+    };
+    auto prefetch_recs = [&](int cell) {
+#pragma unroll
+        for (int p = 0; p < P; p++)
+        {
+            const int d = lane + 32 * p;
+            if (d < nd)
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(a.rec + (unsigned)cell * (unsigned)nd + (unsigned)d));
         }
     };
     if (CURVED)
     {
+        load_recs(rc, __shfl_sync(0xffffffffu, ccell, 0));
 #pragma unroll
-        for (int u = 0; u < R - 1; u++)
-            load_recs(rq[u], u);
+        for (int k = 1; k < 4; k++)
+        {
+            const int cell = __shfl_sync(0xffffffffu, ccell, k);
+            if (k < ncells)
+                prefetch_recs(cell);
+        }
     }
-    for (int k0 = 0; k0 < ncells; k0 += R)
-#pragma unroll
-    for (int u = 0; u < R; u++)
+    for (int k = 0; k < ncells; k++)
     {
-        const int k = k0 + u;
-        if (k >= ncells)
-            break;
+        const int cell1 = __shfl_sync(0xffffffffu, ccell, (k + 1) & 15);
+        const int cell4 = __shfl_sync(0xffffffffu, ccell, (k + 4) & 15);
+        const int ijk = __shfl_sync(0xffffffffu, cij, k);
+        const int pok = __shfl_sync(0xffffffffu, cpo, k);
+        const int flk = __shfl_sync(0xffffffffu, (int)cfl, k);
         if (CURVED)
-            load_recs(rq[(u + R - 1) % R], k + R - 1);
-        const int cx = k % txv, cy = k / txv;
-        const int i = 1 + x0 + cx, j = 1 + y0 + cy;
-        const bool live = !(CURVED && (__shfl_sync(0xffffffffu, (int)cfl, k) & 2));
-        const float *cellp = patch + (cy * px + cx) * dp; // node (i - 1, j - 1)
+        {
+            if (k + 1 < ncells)
+                load_recs(rn, cell1);
+            if (k + 4 < ncells)
+                prefetch_recs(cell4);
+        }
+        const float *cellp = patch + pok; // node (i - 1, j - 1) of cell k
         float *Sk = S + k * ss;
+        float v[P];
+        bool far[P];
 #pragma unroll
         for (int p = 0; p < P; p++)
+            v[p] = 0.f, far[p] = false;
+        if (!(CURVED && (flk & 2))) // a cell inside the excision streams zeros
         {
-            const int d = lane + 32 * p;
-            float v = 0.f;
-            if (d < nd && live)
+            // every lane gathers (a direction past the last has a zero record: its
+            // window reads valid patch nodes and is scaled by 0)
+#pragma unroll
+            for (int p = 0; p < P; p++)
             {
                 if (CURVED)
                 {
-                    const uint4 r = rq[u][p];
-                    if (r.w >> 31)
-                        v = stream_far32(a.Iin, __ldg(a.side + (unsigned)((x0 + cx) + (y0 + cy) * nx_) * (unsigned)nd +
-                                                      (unsigned)d),
-                                         dp, nxn, (int)a.g.ny, nd, a.ng, rowtab, dt.q, dt.p, dt.inv_q, i, j);
-                    else
-                    {
-                        const unsigned word = r.x;
-                        const float t = (float)(word & ((1u << packed32::kTBits) - 1u)) *
-                                        (1.f / (float)(1u << packed32::kTBits));
-                        const float4 *row =
-                            reinterpret_cast<const float4 *>(rowtab + ((word >> packed32::kTypeShift) & 31u) * 12);
-                        const float4 R0 = row[0], R1 = row[1], R2 = row[2];
-                        const float w0 = fmaf(t, R1.x, R0.x), w1 = fmaf(t, R1.y, R0.y), w2 = fmaf(t, R1.z, R0.z);
-                        const float w3 = fmaf(t, R1.w, R0.w), w4 = fmaf(t, R2.y, R2.x);
-                        const int s = (int)((word >> packed32::kStartShift) & 255u);
-                        const float *p00 = cellp + (int)(r.y >> 31) * dp + (int)(r.z >> 31) * pdp + s;
-                        const float c00 = window5(p00, w0, w1, w2, w3, w4);
-                        const float c10 = window5(p00 + dp, w0, w1, w2, w3, w4);
-                        const float c01 = window5(p00 + pdp, w0, w1, w2, w3, w4);
-                        const float c11 = window5(p00 + pdp + dp, w0, w1, w2, w3, w4);
-                        const float fx = __uint_as_float(r.y & 0x7fffffffu), fy = __uint_as_float(r.z & 0x7fffffffu);
-                        const float f0 = fmaf(fx, c10 - c00, c00);
-                        const float f1 = fmaf(fx, c11 - c01, c01);
-                        v = __uint_as_float(r.w) * fmaf(fy, f1 - f0, f0);
-                    }
+                    const uint4 r = rc[p];
+                    far[p] = (r.w >> 31) != 0;
+                    const unsigned word = r.x;
+                    const float t = (float)(word & ((1u << packed32::kTBits) - 1u)) *
+                                    (1.f / (float)(1u << packed32::kTBits));
+                    const float4 *row =
+                        reinterpret_cast<const float4 *>(rowtab + ((word >> packed32::kTypeShift) & 31u) * 12);
+                    const float4 R0 = row[0], R1 = row[1], R2 = row[2];
+                    const float w0 = fmaf(t, R1.x, R0.x), w1 = fmaf(t, R1.y, R0.y), w2 = fmaf(t, R1.z, R0.z);
+                    const float w3 = fmaf(t, R1.w, R0.w), w4 = fmaf(t, R2.y, R2.x);
+                    const int s = (int)((word >> packed32::kStartShift) & 255u);
+                    const float *p00 = cellp + (int)(r.y >> 31) * dp + (int)(r.z >> 31) * pdp + s;
+                    const float c00 = window5(p00, w0, w1, w2, w3, w4);
+                    const float c10 = window5(p00 + dp, w0, w1, w2, w3, w4);
+                    const float c01 = window5(p00 + pdp, w0, w1, w2, w3, w4);
+                    const float c11 = window5(p00 + pdp + dp, w0, w1, w2, w3, w4);
+                    const float fx = __uint_as_float(r.y & 0x7fffffffu), fy = __uint_as_float(r.z & 0x7fffffffu);
+                    const float f0 = fmaf(fx, c10 - c00, c00);
+                    const float f1 = fmaf(fx, c11 - c01, c01);
+                    v[p] = __uint_as_float(r.w & 0x7fffffffu) * fmaf(fy, f1 - f0, f0);
                 }
-                else if (LF.near[p])
+                else
                 {
+                    far[p] = !LF.near[p];
                     const float *b = cellp + LF.off[p];
                     const float c00 = b[0], c10 = b[dp], c01 = b[pdp], c11 = b[pdp + dp];
                     const float f0 = fmaf(LF.fx[p], c10 - c00, c00);
                     const float f1 = fmaf(LF.fx[p], c11 - c01, c01);
-                    v = fmaf(LF.fy[p], f1 - f0, f0);
+                    v[p] = fmaf(LF.fy[p], f1 - f0, f0);
                 }
-                else
-                    v = stream_flat_far32(a.Iin, LF.ox[p], LF.oy[p], dp, nxn, (int)a.g.ny, d, i, j);
             }
+            // departures outside the 3x3 neighbourhood (rare): from global memory
+            bool any = false;
+#pragma unroll
+            for (int p = 0; p < P; p++)
+                any |= far[p];
+            if (__any_sync(0xffffffffu, any))
+            {
+                const int i = ijk % nxn, j = ijk / nxn;
+                const int cell = (i - 1) + (j - 1) * nx_;
+#pragma unroll
+                for (int p = 0; p < P; p++)
+                {
+                    const int d = lane + 32 * p;
+                    if (far[p] && d < nd)
+                        v[p] = CURVED ? stream_far32(a.Iin, __ldg(a.side + (unsigned)cell * (unsigned)nd + (unsigned)d),
+                                                     dp, nxn, (int)a.g.ny, nd, a.ng, rowtab, dt.q, dt.p, dt.inv_q, i, j)
+                                      : stream_flat_far32(a.Iin, LF.ox[p], LF.oy[p], dp, nxn, (int)a.g.ny, d, i, j);
+                }
+            }
+        }
+#pragma unroll
+        for (int p = 0; p < P; p++)
+        {
+            const int d = lane + 32 * p;
             if (d < nd)
-                Sk[d] = v;
+                Sk[d] = v[p];
+        }
+        if (CURVED)
+        {
+#pragma unroll
+            for (int p = 0; p < P; p++)
+                rc[p] = rn[p];
         }
     }
     __syncwarp();
@@ -353,46 +391,45 @@ __device__ __forceinline__ void step_unit32(const Step32Args &a, const DirTable 
         const unsigned pair = 0x10001u << c;
         float *Sc = S + c * ss;
         // Kahan sums of FP32 partial sums over chunks of 8 of the lane's directions
-        float ks[6], kc[6], pp[6];
+        float ks[6], kc[6];
 #pragma unroll
         for (int q = 0; q < 6; q++)
-            ks[q] = kc[q] = pp[q] = 0.f;
-        int n_in_chunk = 0;
-        for (int d = h; d < nd; d += 2)
+            ks[q] = kc[q] = 0.f;
+        for (int d0 = h; d0 < nd; d0 += 16)
         {
-            const float v = Sc[d];
-            const float4 c0 = dirc[2 * d], c1 = dirc[2 * d + 1];
-            pp[0] = fmaf(c0.x, v, pp[0]);
-            pp[1] = fmaf(c0.y, v, pp[1]);
-            pp[2] = fmaf(c0.z, v, pp[2]);
-            pp[3] = fmaf(c0.w, v, pp[3]);
-            pp[4] = fmaf(c1.x, v, pp[4]);
-            pp[5] = fmaf(c1.y, v, pp[5]);
-            if (++n_in_chunk == 8)
-            {
-                n_in_chunk = 0;
+            // FP32 partial sums over 8 of the lane's directions (a direction
+            // past the last contributes zero), then folded into the Kahan sums
+            float pp[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
 #pragma unroll
-                for (int q = 0; q < 6; q++)
-                {
-                    const float y = pp[q] - kc[q];
-                    const float t = ks[q] + y;
-                    kc[q] = (t - ks[q]) - y;
-                    ks[q] = t;
-                    pp[q] = 0.f;
-                }
+            for (int kk = 0; kk < 8; kk++)
+            {
+                const int d = d0 + 2 * kk;
+                const int dd = min(d, nd - 1);
+                const float v = d < nd ? Sc[dd] : 0.f;
+                const float4 c0 = dirc[2 * dd], c1 = dirc[2 * dd + 1];
+                pp[0] = fmaf(c0.x, v, pp[0]);
+                pp[1] = fmaf(c0.y, v, pp[1]);
+                pp[2] = fmaf(c0.z, v, pp[2]);
+                pp[3] = fmaf(c0.w, v, pp[3]);
+                pp[4] = fmaf(c1.x, v, pp[4]);
+                pp[5] = fmaf(c1.y, v, pp[5]);
+            }
+#pragma unroll
+            for (int q = 0; q < 6; q++)
+            {
+                const float y = pp[q] - kc[q];
+                const float t = ks[q] + y;
+                kc[q] = (t - ks[q]) - y;
+                ks[q] = t;
             }
         }
         float m[6];
 #pragma unroll
         for (int q = 0; q < 6; q++)
         {
-            // the chunk in progress, then the two lanes' compensated sums
-            // combined symmetrically (an exact two-sum of their sums, plus
-            // both compensations), so that both lanes hold the same moments
-            const float y = pp[q] - kc[q];
-            const float t = ks[q] + y;
-            kc[q] = (t - ks[q]) - y;
-            ks[q] = t;
+            // the two lanes' compensated sums combined symmetrically (an exact
+            // two-sum of their sums, plus both compensations), so that both
+            // lanes hold the same moments
             const float os = __shfl_xor_sync(pair, ks[q], 16), oc = __shfl_xor_sync(pair, kc[q], 16);
             const float x = ks[q] + os;
             const float bp = x - ks[q];
@@ -649,7 +686,7 @@ __device__ __forceinline__ int batch_item_of(const int *__restrict__ first_tile,
 template <int P>
 __global__ void __launch_bounds__(kThreads, GRLBM_STEP32_MIN_BLOCKS)
     k_step_batch32(const Batch32Item *__restrict__ items, const int *__restrict__ first_tile, int n_items,
-                   int total_tiles, int flip, unsigned *counters, int warp_stride)
+                   int total_tiles, int flip, unsigned *counters, int warp_stride, int s_offset)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     const unsigned bar = smem_addr(smem) + 8u * (unsigned)(threadIdx.x >> 5);
@@ -697,7 +734,9 @@ __global__ void __launch_bounds__(kThreads, GRLBM_STEP32_MIN_BLOCKS)
             }
         };
         const float4 *dirc = reinterpret_cast<const float4 *>(it.dt->dirc);
-        float *S = buf + ia.patch_floats;
+        // (the streamed values sit past the largest patch of the batch: the
+        // next tile's copy, of any problem, never reaches them)
+        float *S = buf + s_offset;
         if (it.curved)
             step_unit32<true, P>(ia, *it.dt, it.dt->rowtab, dirc, LF, tile - first_tile[k], buf, S, st, stage_next);
         else
@@ -814,13 +853,14 @@ void launch_step32(const Step32Args &a, const DirTable &dt, bool curved, int P, 
 }
 
 void launch_step_batch32(const Batch32Item *items, const int *first_tile, int n_items, int total_tiles, int flip,
-                         unsigned *counters, int P, int blocks, size_t smem, int warp_stride, cudaStream_t s)
+                         unsigned *counters, int P, int blocks, size_t smem, int warp_stride, int s_offset,
+                         cudaStream_t s)
 {
 #define GRLBM_LAUNCH(PP)                                                                                    \
     if (P == PP)                                                                                            \
     {                                                                                                       \
         k_step_batch32<PP><<<blocks, kThreads, smem, s>>>(items, first_tile, n_items, total_tiles, flip,    \
-                                                          counters, warp_stride);                           \
+                                                          counters, warp_stride, s_offset);                 \
         return;                                                                                             \
     }
     GRLBM_LAUNCH(1)

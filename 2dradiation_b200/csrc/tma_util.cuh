@@ -30,6 +30,18 @@ __device__ __forceinline__ bool mbar_test(unsigned bar, unsigned parity)
                  : "memory");
     return done != 0;
 }
+// The same, but the thread may sleep in the instruction until the phase
+// completes or about `hint_ns` nanoseconds pass (no busy spinning).
+__device__ __forceinline__ bool mbar_test_sleep(unsigned bar, unsigned parity, unsigned hint_ns)
+{
+    unsigned done;
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\tselp.u32 %0, "
+                 "1, 0, p;\n}\n"
+                 : "=r"(done)
+                 : "r"(bar), "r"(parity), "r"(hint_ns)
+                 : "memory");
+    return done != 0;
+}
 __device__ __forceinline__ unsigned long long global_ns()
 {
     unsigned long long t;
@@ -37,7 +49,9 @@ __device__ __forceinline__ unsigned long long global_ns()
     return t;
 }
 // Wait for the phase of the given parity to complete, for limit_ns at most;
-// false at once when another block has already raised the fault word.
+// false at once when another block has already raised the fault word.  The
+// thread sleeps in the wait instruction (up to 20 us at a time) instead of
+// spinning.
 __device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity, unsigned long long limit_ns,
                                           const unsigned *fault)
 {
@@ -48,7 +62,7 @@ __device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity, unsigne
     const unsigned long long t0 = global_ns();
     do
     {
-        if (mbar_test(bar, parity))
+        if (mbar_test_sleep(bar, parity, 20000u))
             return true;
     } while (global_ns() - t0 < limit_ns);
     return false;
