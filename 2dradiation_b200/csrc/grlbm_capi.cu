@@ -320,24 +320,23 @@ int set_step32_tile(grlbm_ctx *ctx, int tx, int ty)
     return GRLBM_OK;
 }
 
-// The default tile: the largest candidate whose patch buffers leave the
-// register-limited occupancy of the step kernel unchanged.
+// The default tile: the first candidate (16 cells fill phase 2's lane pairs)
+// that keeps at least two blocks per SM, else the first that fits at all.
 int default_step32_tile(grlbm_ctx *ctx)
 {
     static const int cand[][2] = {{4, 4}, {8, 2}, {4, 2}, {2, 2}, {2, 1}, {1, 1}};
     const bool curved = ctx->run.streaming_type == GRLBM_CURVED_FIXED;
-    int reg_limit = 0;
-    CU(step32_occupancy(ctx->passes, curved, false, 0, &reg_limit));
-    for (const auto &c : cand)
-    {
-        const size_t smem = step32_smem(c[0], c[1], (int)ctx->sl.sp, ctx->st.n);
-        int per_sm = 0;
-        if (smem > (size_t)kStep32MaxSmem)
-            continue;
-        CU(step32_occupancy(ctx->passes, curved, false, smem, &per_sm));
-        if (per_sm >= reg_limit || (c[0] == 1 && per_sm >= 1))
-            return set_step32_tile(ctx, c[0], c[1]);
-    }
+    for (int need = 2; need >= 1; need--)
+        for (const auto &c : cand)
+        {
+            const size_t smem = step32_smem(c[0], c[1], (int)ctx->sl.sp, ctx->st.n);
+            int per_sm = 0;
+            if (smem > (size_t)kStep32MaxSmem)
+                continue;
+            CU(step32_occupancy(ctx->passes, curved, false, smem, &per_sm));
+            if (per_sm >= need)
+                return set_step32_tile(ctx, c[0], c[1]);
+        }
     return fail(ctx, GRLBM_ERR_ARGUMENT, "no tile of %d directions fits on an SM", ctx->st.n);
 }
 

@@ -509,7 +509,10 @@ __device__ __forceinline__ void step_unit32(const Step32Args &a, const DirTable 
                 for (int q = 0; q < 6; q++)
                 {
                     m[q] = A6[q] + ee * B6[q] + k3 * (fFx * C6[q] + fFy * D6[q]);
-                    const float x = (prev[q] - m[q]) / m[q];
+                    // the exit test's relative change, with the fast quotient (the
+                    // FP32 form's choice: a noise moment near zero would otherwise
+                    // take the IEEE division's slow path; 0 / 0 is still NaN)
+                    const float x = __fdividef(prev[q] - m[q], m[q]);
                     s2 += x * x;
                 }
                 diff = sqrtf(s2);
@@ -553,7 +556,7 @@ __device__ __forceinline__ void step_unit32(const Step32Args &a, const DirTable 
     // (and the mirrored directions 0..3 after the last one) ----
     for (int k = 0; k < ncells; k++)
     {
-        const int ij = (1 + x0 + k % txv) + (1 + y0 + k / txv) * nxn;
+        const int ij = __shfl_sync(0xffffffffu, cij, k);
         float *o = a.Iout + (unsigned)ij * (unsigned)dp;
         const float *Sk = S + k * ss;
 #pragma unroll

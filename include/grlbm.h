@@ -253,8 +253,8 @@ int grlbm_copy_rows(grlbm_ctx *ctx, int64_t j_first, int64_t n, void *buffer, in
  * fixed streaming types runs as warps that each take tiles of tile_x x
  * tile_y cells (at most 16), staging each tile's (tile_x + 2) x (tile_y + 2)
  * node patch of the state in shared memory.  The default tile is the first
- * of 4x4, 8x2, 4x2, 2x2, 2x1, 1x1 whose buffers leave the kernel's resident
- * warps unchanged.  The result does not depend on the tile.
+ * of 4x4, 8x2, 4x2, 2x2, 2x1, 1x1 whose buffers leave room for two blocks
+ * of the kernel per SM.  The result does not depend on the tile.
  * GRLBM_ERR_ARGUMENT for more than 16 cells or buffers that do not fit in
  * shared memory; GRLBM_ERR_UNSUPPORTED for other contexts. */
 int grlbm_set_tile_shape(grlbm_ctx *ctx, int32_t tile_x, int32_t tile_y);
