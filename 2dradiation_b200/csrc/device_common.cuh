@@ -320,13 +320,14 @@ struct AdjCollideArgs
 // The precision-form step of the fixed streaming types (cell-major state,
 // kernels_step32.cu): warps of kStep32Warps per block, each taking tiles of
 // tx x ty <= kStep32UnitCells cells from a counter.
-constexpr int kStep32Warps = 4;
+constexpr int kStep32Warps = 6;
 constexpr int kStep32UnitCells = 16;
 constexpr int kStep32MaxSmem = 227 * 1024;
 struct Step32Args
 {
     GridDev g;
     int nd, ng, dp;          // directions, interpolation rows, direction pitch of the state
+    int dps;                 // a node's floats in the staged patch (dp padded to a multiple of 32)
     int tx, ty;              // cells per tile; a warp stages (tx + 2) x (ty + 2) nodes
     int ss, patch_floats;    // row stride of the streamed-value buffer, floats of the patch buffer
     int tiles_x, ntiles;     // tiles per row of tiles, tiles over the slab rows
@@ -392,6 +393,10 @@ int step32_passes(int nd);
 // cells (row stride s, s = 2 mod 32 >= nd: conflict-free for lanes over the
 // directions and for two lanes per cell over interleaved directions).
 int step32_s_stride(int nd);
+// A node's floats in the staged patch: dp padded to a multiple of 32 (while
+// that stays within the TMA box's 256), so that lanes reading neighbouring
+// nodes at the same direction offset hit disjoint banks.
+int step32_patch_node_floats(int dp);
 int step32_patch_floats(int tx, int ty, int dp);
 int step32_warp_stride(int tx, int ty, int dp, int nd);
 // shared memory of a block of the single-problem kernel, and of the batch kernel

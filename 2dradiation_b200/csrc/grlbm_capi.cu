@@ -260,6 +260,7 @@ Step32Args step32_args(grlbm_ctx *ctx, int from)
     a.nd = ctx->st.n;
     a.ng = ctx->ng;
     a.dp = (int)ctx->sl.sp;
+    a.dps = step32_patch_node_floats(a.dp);
     a.tx = ctx->tile_x;
     a.ty = ctx->tile_y;
     a.ss = step32_s_stride(a.nd);

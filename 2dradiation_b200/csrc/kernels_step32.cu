@@ -11,6 +11,11 @@
 // (src/Radiation.cpp:502-505, 342); alpha_n^-3 > 0 commutes with the clamp,
 // so gathering J needs no alpha at the corners.
 //
+// In shared memory a node's run is padded to dps floats, a multiple of 32
+// (the TMA box is wider than the node's dp floats; the rest is zero fill):
+// lanes whose departures fall in different corner columns or rows then read
+// disjoint banks.
+//
 // Work split: every warp works alone.  It takes tiles of tx x ty <= 16 cells
 // from a counter and stages the tile's (tx + 2) x (ty + 2) node patch of the
 // whole state (all directions) into its own shared-memory buffer with one TMA
@@ -46,7 +51,7 @@
 #include "tma_util.cuh"
 
 #ifndef GRLBM_STEP32_MIN_BLOCKS
-#define GRLBM_STEP32_MIN_BLOCKS 3
+#define GRLBM_STEP32_MIN_BLOCKS 2
 #endif
 
 namespace grlbm
@@ -158,7 +163,7 @@ struct LaneFlat
 };
 
 template <int P>
-__device__ __forceinline__ void load_lane_flat(LaneFlat<P> &L, const DirTable &dt, int nd, int dp, int px)
+__device__ __forceinline__ void load_lane_flat(LaneFlat<P> &L, const DirTable &dt, int nd, int dps, int px)
 {
     const int lane = threadIdx.x & 31;
 #pragma unroll
@@ -172,7 +177,20 @@ __device__ __forceinline__ void load_lane_flat(LaneFlat<P> &L, const DirTable &d
         L.fx[p] = ox - fli;
         L.fy[p] = oy - flj;
         L.near[p] = (fli == -1.f || fli == 0.f) && (flj == -1.f || flj == 0.f);
-        L.off[p] = L.near[p] ? ((int)fli + 1 + ((int)flj + 1) * px) * dp + dd : 0;
+        L.off[p] = L.near[p] ? ((int)fli + 1 + ((int)flj + 1) * px) * dps + dd : 0;
+    }
+}
+
+// A lane's rotated directions (n1, n2) for its P passes (phase 3's map).
+template <int P>
+__device__ __forceinline__ void load_lane_dirs(float2 (&LN)[P], const float4 *dirc, int nd)
+{
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int p = 0; p < P; p++)
+    {
+        const float4 c1 = dirc[2 * min(lane + 32 * p, nd - 1) + 1];
+        LN[p] = make_float2(c1.z, c1.w);
     }
 }
 
@@ -192,7 +210,7 @@ __device__ __forceinline__ void stage_tile(const Step32Args &a, int tile, float 
         const int bx = tile % a.tiles_x, by = tile / a.tiles_x;
         // the lanes' reads of the buffer are done (__syncwarp before the call)
         fence_proxy_async_smem();
-        mbar_arrive_expect(bar, (unsigned)((a.tx + 2) * (a.ty + 2) * a.dp) * 4u);
+        mbar_arrive_expect(bar, (unsigned)((a.tx + 2) * (a.ty + 2) * a.dps) * 4u);
         tma_load_4d(smem_addr(patch), &a.in_map, 0, 0, bx * a.tx, (int)a.g.jlo - 1 + by * a.ty, bar);
     }
 }
@@ -222,18 +240,18 @@ __device__ __forceinline__ bool wait_tile(const Step32Args &a, unsigned bar, uns
 // stores the cells' new state, coalesced along the directions.
 template <bool CURVED, int P, class Next>
 __device__ __forceinline__ void step_unit32(const Step32Args &a, const DirTable &dt, const float *rowtab,
-                                            const float4 *dirc, const LaneFlat<P> &LF, int tile,
-                                            const float *patch, float *S, IterStats &st, Next next)
+                                            const float4 *dirc, const LaneFlat<P> &LF, const float2 (&LN)[P],
+                                            int tile, const float *patch, float *S, IterStats &st, Next next)
 {
     const int lane = threadIdx.x & 31;
-    const int tx = a.tx, px = tx + 2, dp = a.dp, nd = a.nd, ss = a.ss;
+    const int tx = a.tx, px = tx + 2, dp = a.dp, dps = a.dps, nd = a.nd, ss = a.ss;
     const int bx = tile % a.tiles_x, by = tile / a.tiles_x;
     const int x0 = bx * tx, y0 = (int)a.g.jlo - 1 + by * a.ty; // patch origin (node coordinates)
     const int nxn = (int)a.g.nx, nx_ = (int)a.g.nx_;
     const unsigned nxy = (unsigned)a.g.nxy;
     const int txv = min(tx, nx_ - x0), tyv = min(a.ty, (int)a.g.jhi - 1 - y0);
     const int ncells = txv * tyv;
-    const int pdp = px * dp;
+    const int pdp = px * dps; // patch offset of the next node row
 
     // this lane's cell of phase 2 (c = lane mod 16), loaded now so that the
     // loads land during the streaming
@@ -256,7 +274,7 @@ __device__ __forceinline__ void step_unit32(const Step32Args &a, const DirTable 
     // and flags; the cell loop reads them by shuffle.  Cell k's records are
     // loaded while cell k - 1 streams, and cell k + 3's are prefetched into L2.
     const int ccell = (x0 + ccx) + (y0 + ccy) * nx_;
-    const int cpo = (ccy * px + ccx) * dp;
+    const int cpo = (ccy * px + ccx) * dps;
     uint4 rc[P], rn[P];
     auto load_recs = [&](uint4(&r)[P], int cell) {
 #pragma unroll
@@ -327,11 +345,11 @@ __device__ __forceinline__ void step_unit32(const Step32Args &a, const DirTable 
                     const float w0 = fmaf(t, R1.x, R0.x), w1 = fmaf(t, R1.y, R0.y), w2 = fmaf(t, R1.z, R0.z);
                     const float w3 = fmaf(t, R1.w, R0.w), w4 = fmaf(t, R2.y, R2.x);
                     const int s = (int)((word >> packed32::kStartShift) & 255u);
-                    const float *p00 = cellp + (int)(r.y >> 31) * dp + (int)(r.z >> 31) * pdp + s;
+                    const float *p00 = cellp + (int)(r.y >> 31) * dps + (int)(r.z >> 31) * pdp + s;
                     const float c00 = window5(p00, w0, w1, w2, w3, w4);
-                    const float c10 = window5(p00 + dp, w0, w1, w2, w3, w4);
+                    const float c10 = window5(p00 + dps, w0, w1, w2, w3, w4);
                     const float c01 = window5(p00 + pdp, w0, w1, w2, w3, w4);
-                    const float c11 = window5(p00 + pdp + dp, w0, w1, w2, w3, w4);
+                    const float c11 = window5(p00 + pdp + dps, w0, w1, w2, w3, w4);
                     const float fx = __uint_as_float(r.y & 0x7fffffffu), fy = __uint_as_float(r.z & 0x7fffffffu);
                     const float f0 = fmaf(fx, c10 - c00, c00);
                     const float f1 = fmaf(fx, c11 - c01, c01);
@@ -341,7 +359,7 @@ __device__ __forceinline__ void step_unit32(const Step32Args &a, const DirTable 
                 {
                     far[p] = !LF.near[p];
                     const float *b = cellp + LF.off[p];
-                    const float c00 = b[0], c10 = b[dp], c01 = b[pdp], c11 = b[pdp + dp];
+                    const float c00 = b[0], c10 = b[dps], c01 = b[pdp], c11 = b[pdp + dps];
                     const float f0 = fmaf(LF.fx[p], c10 - c00, c00);
                     const float f1 = fmaf(LF.fx[p], c11 - c01, c01);
                     v[p] = fmaf(LF.fy[p], f1 - f0, f0);
@@ -385,6 +403,9 @@ __device__ __forceinline__ void step_unit32(const Step32Args &a, const DirTable 
     next(); // the patch buffer is free: the next tile's copy lands during phases 2 and 3
 
     // ---- phase 2: moments and collide, two lanes per cell ----
+    // phase 3's map of the streamed values of this lane's cell: og S + oa +
+    // ob1 n1 + ob2 n2 (identity where phase 2 has written the values already)
+    float og = 1.f, oa = 0.f, ob1 = 0.f, ob2 = 0.f;
     if (cact)
     {
         // the two lanes of this cell (every shuffle of phase 2 is between them)
@@ -517,23 +538,28 @@ __device__ __forceinline__ void step_unit32(const Step32Args &a, const DirTable 
                 }
                 diff = sqrtf(s2);
             }
-            // the intensities of the last iterate (its moments m are the stored ones)
+            // the intensities of the last iterate (its moments m are the stored
+            // ones): for a fluid at rest the affine map with the coefficients
+            // phase 3 applies, I_d = g0 S_d + ra + rb1 n1_d + rb2 n2_d (times the
+            // state's scale); a moving fluid's here, per direction
             const float ee = eta + k0 * fE;
-            const float ra = h0 * ee, rb1 = h0 * k3 * fFx, rb2 = h0 * k3 * fFy;
-            for (int d = h; d < nd; d += 2)
+            if (rest)
             {
-                const float4 c1 = dirc[2 * d + 1];
-                const float n1 = c1.z, n2 = c1.w;
-                float v;
-                if (rest)
-                    v = fmaf(g0, Sc[d], fmaf(rb1, n1, fmaf(rb2, n2, ra)));
-                else
+                og = g0 * scale;
+                oa = h0 * ee * scale;
+                ob1 = h0 * k3 * fFx * scale;
+                ob2 = h0 * k3 * fFy * scale;
+            }
+            else
+            {
+                for (int d = h; d < nd; d += 2)
                 {
+                    const float4 c1 = dirc[2 * d + 1];
+                    const float n1 = c1.z, n2 = c1.w;
                     float g, hh, q1, q2;
                     collide_coeffs32(n1, n2, u1, u2, lor, adt, kak0, g, hh, q1, q2);
-                    v = g * Sc[d] + hh * (ee + k3 * (q1 * fFx + q2 * fFy));
+                    Sc[d] = (g * Sc[d] + hh * (ee + k3 * (q1 * fFx + q2 * fFy))) * scale;
                 }
-                Sc[d] = v * scale;
             }
             if (h == 0)
             {
@@ -541,11 +567,8 @@ __device__ __forceinline__ void step_unit32(const Step32Args &a, const DirTable 
                 st.max = max(st.max, (unsigned)cycles);
             }
         }
-        else if (CURVED)
-        {
-            for (int d = h; d < nd; d += 2)
-                Sc[d] *= scale;
-        }
+        else
+            og = scale;
 #pragma unroll
         for (int q = 0; q < 3; q++)
             a.mom[(unsigned)cij + (unsigned)(3 * h + q) * nxy] = h ? m[3 + q] : m[q];
@@ -557,17 +580,23 @@ __device__ __forceinline__ void step_unit32(const Step32Args &a, const DirTable 
     for (int k = 0; k < ncells; k++)
     {
         const int ij = __shfl_sync(0xffffffffu, cij, k);
+        const float g = __shfl_sync(0xffffffffu, og, k), ca = __shfl_sync(0xffffffffu, oa, k);
+        const float cb1 = __shfl_sync(0xffffffffu, ob1, k), cb2 = __shfl_sync(0xffffffffu, ob2, k);
         float *o = a.Iout + (unsigned)ij * (unsigned)dp;
         const float *Sk = S + k * ss;
+        float first = 0.f;
 #pragma unroll
         for (int p = 0; p < P; p++)
         {
             const int d = lane + 32 * p;
+            const float v = fmaf(g, Sk[min(d, nd - 1)], fmaf(cb1, LN[p].x, fmaf(cb2, LN[p].y, ca)));
             if (d < nd)
-                o[d] = Sk[d];
+                o[d] = v;
+            if (p == 0)
+                first = v;
         }
         if (lane < kStateMirror)
-            o[nd + lane] = Sk[lane];
+            o[nd + lane] = first;
     }
     __syncwarp(); // S is rewritten by the next tile's phase 1
 }
@@ -646,7 +675,9 @@ __global__ void __launch_bounds__(kThreads, GRLBM_STEP32_MIN_BLOCKS)
     float *S = patch + a.patch_floats;
     LaneFlat<P> LF;
     if (!CURVED)
-        load_lane_flat<P>(LF, dt, a.nd, a.dp, a.tx + 2);
+        load_lane_flat<P>(LF, dt, a.nd, a.dps, a.tx + 2);
+    float2 LN[P];
+    load_lane_dirs<P>(LN, dirc, a.nd);
     IterStats st{0ull, 0u};
     unsigned parity = 0;
     int tile = take_tile(a.tiles);
@@ -657,7 +688,7 @@ __global__ void __launch_bounds__(kThreads, GRLBM_STEP32_MIN_BLOCKS)
         if (!wait_tile(a, bar, parity))
             break;
         int next = a.ntiles;
-        step_unit32<CURVED, P>(a, dt, rowtab, dirc, LF, tile, patch, S, st, [&]() {
+        step_unit32<CURVED, P>(a, dt, rowtab, dirc, LF, LN, tile, patch, S, st, [&]() {
             next = take_tile(a.tiles);
             if (next < a.ntiles)
                 stage_tile(a, next, patch, bar);
@@ -698,6 +729,7 @@ __global__ void __launch_bounds__(kThreads, GRLBM_STEP32_MIN_BLOCKS)
     __syncthreads();
     float *buf = warp_buffers(smem, kRowtabOffset, warp_stride);
     LaneFlat<P> LF;
+    float2 LN[P];
     IterStats st{0ull, 0u};
     unsigned parity = 0;
     int cur = -1;
@@ -724,7 +756,8 @@ __global__ void __launch_bounds__(kThreads, GRLBM_STEP32_MIN_BLOCKS)
             cur = k;
             ca = &ia;
             if (!it.curved)
-                load_lane_flat<P>(LF, *it.dt, ia.nd, ia.dp, ia.tx + 2);
+                load_lane_flat<P>(LF, *it.dt, ia.nd, ia.dps, ia.tx + 2);
+            load_lane_dirs<P>(LN, reinterpret_cast<const float4 *>(it.dt->dirc), ia.nd);
         }
         int next = total_tiles;
         auto stage_next = [&]() {
@@ -741,9 +774,11 @@ __global__ void __launch_bounds__(kThreads, GRLBM_STEP32_MIN_BLOCKS)
         // next tile's copy, of any problem, never reaches them)
         float *S = buf + s_offset;
         if (it.curved)
-            step_unit32<true, P>(ia, *it.dt, it.dt->rowtab, dirc, LF, tile - first_tile[k], buf, S, st, stage_next);
+            step_unit32<true, P>(ia, *it.dt, it.dt->rowtab, dirc, LF, LN, tile - first_tile[k], buf, S, st,
+                                 stage_next);
         else
-            step_unit32<false, P>(ia, *it.dt, it.dt->rowtab, dirc, LF, tile - first_tile[k], buf, S, st, stage_next);
+            step_unit32<false, P>(ia, *it.dt, it.dt->rowtab, dirc, LF, LN, tile - first_tile[k], buf, S, st,
+                                  stage_next);
         tile = next;
     }
     if (ca)
@@ -775,7 +810,16 @@ int step32_passes(int nd)
 
 int step32_s_stride(int nd) { return nd + ((2 - nd) % 32 + 32) % 32; }
 
-int step32_patch_floats(int tx, int ty, int dp) { return ((tx + 2) * (ty + 2) * dp + 31) / 32 * 32; }
+int step32_patch_node_floats(int dp)
+{
+    const int padded = (dp + 31) / 32 * 32;
+    return padded <= 256 ? padded : dp;
+}
+
+int step32_patch_floats(int tx, int ty, int dp)
+{
+    return ((tx + 2) * (ty + 2) * step32_patch_node_floats(dp) + 31) / 32 * 32;
+}
 
 int step32_warp_stride(int tx, int ty, int dp, int nd)
 {
@@ -875,10 +919,13 @@ void launch_step_batch32(const Batch32Item *items, const int *first_tile, int n_
 #undef GRLBM_LAUNCH
 }
 
-// The cell-major state as a 4D tensor {c0, dp / c0, nx, ny} (c0: the largest
-// multiple of 4 that divides dp and is at most 256, the TMA's box limit), read
-// in boxes {c0, dp / c0, tx + 2, ty + 2}: one box is a tile's whole patch,
-// landing in shared memory as [node row][node][direction].
+// The cell-major state as a 4D tensor {c0, dp / c0, nx, ny} read in boxes
+// {box0, dp / c0, tx + 2, ty + 2}: one box is a tile's whole patch, landing
+// in shared memory as [node row][node][direction].  When dp is at most 256,
+// c0 = dp and the box's first extent is the padded node run
+// (step32_patch_node_floats: its floats past dp are the copy's zero fill);
+// else c0 is the largest multiple of 4 that divides dp and is at most 256,
+// the box's extent limit, and the run is not padded.
 cudaError_t encode_state_map32(CUtensorMap *map, const float *state, int64_t nx, int64_t ny, int dp, int tx, int ty)
 {
     static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
@@ -897,16 +944,22 @@ cudaError_t encode_state_map32(CUtensorMap *map, const float *state, int64_t nx,
     if (dp % 4 != 0 || reinterpret_cast<uintptr_t>(state) % 16 != 0 || tx < 1 || ty < 1 || tx + 2 > 256 ||
         ty + 2 > 256)
         return cudaErrorInvalidValue;
-    int c0 = 0;
-    for (int c = 4; c <= 256 && c <= dp; c += 4)
-        if (dp % c == 0)
-            c0 = c;
-    if (c0 == 0 || dp / c0 > 256)
+    int c0 = 0, box0 = 0;
+    if (dp <= 256)
+        c0 = dp, box0 = step32_patch_node_floats(dp);
+    else
+    {
+        for (int c = 4; c <= 256 && c <= dp; c += 4)
+            if (dp % c == 0)
+                c0 = c;
+        box0 = c0;
+    }
+    if (c0 == 0 || dp / c0 > 256 || (box0 != c0 && dp / c0 != 1))
         return cudaErrorInvalidValue;
     const cuuint64_t dims[4] = {(cuuint64_t)c0, (cuuint64_t)(dp / c0), (cuuint64_t)nx, (cuuint64_t)ny};
     const cuuint64_t strides[3] = {(cuuint64_t)c0 * sizeof(float), (cuuint64_t)dp * sizeof(float),
                                    (cuuint64_t)nx * (cuuint64_t)dp * sizeof(float)};
-    const cuuint32_t box[4] = {(cuuint32_t)c0, (cuuint32_t)(dp / c0), (cuuint32_t)(tx + 2), (cuuint32_t)(ty + 2)};
+    const cuuint32_t box[4] = {(cuuint32_t)box0, (cuuint32_t)(dp / c0), (cuuint32_t)(tx + 2), (cuuint32_t)(ty + 2)};
     const cuuint32_t elem[4] = {1, 1, 1, 1};
     const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<float *>(state), dims, strides, box,
                               elem, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
