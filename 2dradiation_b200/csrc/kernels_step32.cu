@@ -231,6 +231,66 @@ __device__ __forceinline__ bool wait_tile(const Step32Args &a, unsigned bar, uns
     return true;
 }
 
+// A tile's cells as phase 1 and phase 2 need them: lane c (< 16, and its
+// partner c + 16) holds cell c's node index, interior cell index, patch
+// offset, flags and fields; and every lane its directions' records of cell
+// 0.  Loaded for the next tile while the current one is finished, so that
+// none of these loads stalls the streaming.
+template <int P>
+struct UnitCells
+{
+    int x0, y0, txv, ncells;
+    int cij, ccell, cpo, cfl;
+    float u1, u2, lor, adt, eta, k0, k3, kak0, scale;
+    uint4 rec0[P];
+};
+
+template <bool CURVED, int P>
+__device__ __forceinline__ void load_unit(const Step32Args &a, int tile, UnitCells<P> &U)
+{
+    const int lane = threadIdx.x & 31;
+    const int tx = a.tx, px = tx + 2, nd = a.nd;
+    const int bx = tile % a.tiles_x, by = tile / a.tiles_x;
+    U.x0 = bx * tx;
+    U.y0 = (int)a.g.jlo - 1 + by * a.ty;
+    U.txv = min(tx, (int)a.g.nx_ - U.x0);
+    U.ncells = U.txv * min(a.ty, (int)a.g.jhi - 1 - U.y0);
+    const int c = lane & (kUnitCells - 1);
+    const bool cact = c < U.ncells;
+    const int ccx = cact ? c % U.txv : 0, ccy = cact ? c / U.txv : 0;
+    U.cij = (1 + U.x0 + ccx) + (1 + U.y0 + ccy) * (int)a.g.nx;
+    U.ccell = (U.x0 + ccx) + (U.y0 + ccy) * (int)a.g.nx_;
+    U.cpo = (ccy * px + ccx) * a.dps;
+    U.cfl = cact ? (int)a.flags[U.cij] : 3;
+    // (fields exist at every node: loaded without waiting for the flags)
+    U.u1 = __ldg(a.u1 + U.cij), U.u2 = __ldg(a.u2 + U.cij), U.lor = __ldg(a.lor + U.cij);
+    U.adt = __ldg(a.adt + U.cij), U.eta = __ldg(a.eta + U.cij), U.k0 = __ldg(a.k0 + U.cij);
+    U.k3 = __ldg(a.k3 + U.cij), U.kak0 = __ldg(a.ka + U.cij);
+    U.scale = CURVED ? __ldg(a.ia3 + U.cij) : 1.f;
+    if (CURVED)
+    {
+        const int cell0 = __shfl_sync(0xffffffffu, U.ccell, 0);
+#pragma unroll
+        for (int p = 0; p < P; p++)
+        {
+            const int d = lane + 32 * p;
+            U.rec0[p] = d < nd ? __ldcs(a.rec + (unsigned)cell0 * (unsigned)nd + (unsigned)d) : make_uint4(0u, 0u, 0u, 0u);
+        }
+#pragma unroll
+        for (int k = 1; k < 4; k++)
+        {
+            const int cell = __shfl_sync(0xffffffffu, U.ccell, k);
+#pragma unroll
+            for (int p = 0; p < P; p++)
+            {
+                const int d = lane + 32 * p;
+                if (k < U.ncells && d < nd)
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(a.rec + (unsigned)cell * (unsigned)nd + (unsigned)d));
+            }
+        }
+    }
+}
+
 // One tile of one step by one warp, its patch staged: phase 1 streams every
 // cell with the lanes over the directions into the warp's buffer S
 // ([cell][direction], row stride a.ss), then calls next() (which stages the
@@ -241,40 +301,26 @@ __device__ __forceinline__ bool wait_tile(const Step32Args &a, unsigned bar, uns
 template <bool CURVED, int P, class Next>
 __device__ __forceinline__ void step_unit32(const Step32Args &a, const DirTable &dt, const float *rowtab,
                                             const float4 *dirc, const LaneFlat<P> &LF, const float2 (&LN)[P],
-                                            int tile, const float *patch, float *S, IterStats &st, Next next)
+                                            const UnitCells<P> &U, const float *patch, float *S, IterStats &st,
+                                            Next next)
 {
     const int lane = threadIdx.x & 31;
     const int tx = a.tx, px = tx + 2, dp = a.dp, dps = a.dps, nd = a.nd, ss = a.ss;
-    const int bx = tile % a.tiles_x, by = tile / a.tiles_x;
-    const int x0 = bx * tx, y0 = (int)a.g.jlo - 1 + by * a.ty; // patch origin (node coordinates)
+    (void)tx;
     const int nxn = (int)a.g.nx, nx_ = (int)a.g.nx_;
     const unsigned nxy = (unsigned)a.g.nxy;
-    const int txv = min(tx, nx_ - x0), tyv = min(a.ty, (int)a.g.jhi - 1 - y0);
-    const int ncells = txv * tyv;
+    const int ncells = U.ncells;
     const int pdp = px * dps; // patch offset of the next node row
-
-    // this lane's cell of phase 2 (c = lane mod 16), loaded now so that the
-    // loads land during the streaming
     const int c = lane & (kUnitCells - 1), h = lane >> 4;
     const bool cact = c < ncells;
-    const int ccx = cact ? c % txv : 0, ccy = cact ? c / txv : 0;
-    const int cij = (1 + x0 + ccx) + (1 + y0 + ccy) * nxn;
-    const uint8_t cfl = cact ? a.flags[cij] : (uint8_t)3;
-    float u1 = 0.f, u2 = 0.f, lor = 1.f, adt = 0.f, eta = 0.f, k0 = 0.f, k3 = 0.f, kak0 = 0.f, scale = 1.f;
-    if (cact && !(cfl & 1))
-    {
-        u1 = __ldg(a.u1 + cij), u2 = __ldg(a.u2 + cij), lor = __ldg(a.lor + cij), adt = __ldg(a.adt + cij);
-        eta = __ldg(a.eta + cij), k0 = __ldg(a.k0 + cij), k3 = __ldg(a.k3 + cij), kak0 = __ldg(a.ka + cij) + k0;
-    }
-    if (CURVED && cact)
-        scale = __ldg(a.ia3 + cij);
+    const int cij = U.cij, ccell = U.ccell, cpo = U.cpo, cfl = U.cfl;
+    const float u1 = U.u1, u2 = U.u2, lor = U.lor, adt = U.adt, eta = U.eta, k0 = U.k0, k3 = U.k3, kak0 = U.kak0;
+    const float scale = U.scale;
 
     // ---- phase 1: stream every cell, lanes over the directions ----
-    // Lane c (< 16) holds its cell's interior index, node index, patch offset
-    // and flags; the cell loop reads them by shuffle.  Cell k's records are
-    // loaded while cell k - 1 streams, and cell k + 3's are prefetched into L2.
-    const int ccell = (x0 + ccx) + (y0 + ccy) * nx_;
-    const int cpo = (ccy * px + ccx) * dps;
+    // The cell loop reads the cells' tables from lanes 0..15 by shuffle.
+    // Cell k's records are loaded while cell k - 1 streams, and cell k + 3's
+    // are prefetched into L2 (cell 0's came with the tile's tables).
     uint4 rc[P], rn[P];
     auto load_recs = [&](uint4(&r)[P], int cell) {
 #pragma unroll
@@ -295,14 +341,9 @@ __device__ __forceinline__ void step_unit32(const Step32Args &a, const DirTable 
     };
     if (CURVED)
     {
-        load_recs(rc, __shfl_sync(0xffffffffu, ccell, 0));
 #pragma unroll
-        for (int k = 1; k < 4; k++)
-        {
-            const int cell = __shfl_sync(0xffffffffu, ccell, k);
-            if (k < ncells)
-                prefetch_recs(cell);
-        }
+        for (int p = 0; p < P; p++)
+            rc[p] = U.rec0[p];
     }
     for (int k = 0; k < ncells; k++)
     {
@@ -310,7 +351,7 @@ __device__ __forceinline__ void step_unit32(const Step32Args &a, const DirTable 
         const int cell4 = __shfl_sync(0xffffffffu, ccell, (k + 4) & 15);
         const int ijk = __shfl_sync(0xffffffffu, cij, k);
         const int pok = __shfl_sync(0xffffffffu, cpo, k);
-        const int flk = __shfl_sync(0xffffffffu, (int)cfl, k);
+        const int flk = __shfl_sync(0xffffffffu, cfl, k);
         if (CURVED)
         {
             if (k + 1 < ncells)
@@ -681,18 +722,27 @@ __global__ void __launch_bounds__(kThreads, GRLBM_STEP32_MIN_BLOCKS)
     IterStats st{0ull, 0u};
     unsigned parity = 0;
     int tile = take_tile(a.tiles);
+    UnitCells<P> U;
     if (tile < a.ntiles)
+    {
         stage_tile(a, tile, patch, bar);
+        load_unit<CURVED, P>(a, tile, U);
+    }
     while (tile < a.ntiles)
     {
         if (!wait_tile(a, bar, parity))
             break;
         int next = a.ntiles;
-        step_unit32<CURVED, P>(a, dt, rowtab, dirc, LF, LN, tile, patch, S, st, [&]() {
+        UnitCells<P> N;
+        step_unit32<CURVED, P>(a, dt, rowtab, dirc, LF, LN, U, patch, S, st, [&]() {
             next = take_tile(a.tiles);
             if (next < a.ntiles)
+            {
                 stage_tile(a, next, patch, bar);
+                load_unit<CURVED, P>(a, next, N);
+            }
         });
+        U = N;
         tile = next;
     }
     flush_stats(st, a.iter_sum, a.iter_max);
@@ -734,13 +784,21 @@ __global__ void __launch_bounds__(kThreads, GRLBM_STEP32_MIN_BLOCKS)
     unsigned parity = 0;
     int cur = -1;
     const Step32Args *ca = nullptr;
+    // stage a tile of the batch and load its cells' tables
+    auto start_tile = [&](int t, UnitCells<P> &u) {
+        const int nk = batch_item_of(first_tile, n_items, t);
+        const Batch32Item &nit = items[nk];
+        const Step32Args &na = nit.a[nit.cur0 ^ flip];
+        stage_tile(na, t - first_tile[nk], buf, bar);
+        if (nit.curved)
+            load_unit<true, P>(na, t - first_tile[nk], u);
+        else
+            load_unit<false, P>(na, t - first_tile[nk], u);
+    };
     int tile = take_tile(counters);
+    UnitCells<P> U;
     if (tile < total_tiles)
-    {
-        const Batch32Item &it = items[batch_item_of(first_tile, n_items, tile)];
-        const Step32Args &na = it.a[it.cur0 ^ flip];
-        stage_tile(na, tile - first_tile[batch_item_of(first_tile, n_items, tile)], buf, bar);
-    }
+        start_tile(tile, U);
     while (tile < total_tiles)
     {
         const int k = batch_item_of(first_tile, n_items, tile);
@@ -760,25 +818,21 @@ __global__ void __launch_bounds__(kThreads, GRLBM_STEP32_MIN_BLOCKS)
             load_lane_dirs<P>(LN, reinterpret_cast<const float4 *>(it.dt->dirc), ia.nd);
         }
         int next = total_tiles;
+        UnitCells<P> N;
         auto stage_next = [&]() {
             next = take_tile(counters);
             if (next < total_tiles)
-            {
-                const int nk = batch_item_of(first_tile, n_items, next);
-                const Batch32Item &nit = items[nk];
-                stage_tile(nit.a[nit.cur0 ^ flip], next - first_tile[nk], buf, bar);
-            }
+                start_tile(next, N);
         };
         const float4 *dirc = reinterpret_cast<const float4 *>(it.dt->dirc);
         // (the streamed values sit past the largest patch of the batch: the
         // next tile's copy, of any problem, never reaches them)
         float *S = buf + s_offset;
         if (it.curved)
-            step_unit32<true, P>(ia, *it.dt, it.dt->rowtab, dirc, LF, LN, tile - first_tile[k], buf, S, st,
-                                 stage_next);
+            step_unit32<true, P>(ia, *it.dt, it.dt->rowtab, dirc, LF, LN, U, buf, S, st, stage_next);
         else
-            step_unit32<false, P>(ia, *it.dt, it.dt->rowtab, dirc, LF, LN, tile - first_tile[k], buf, S, st,
-                                  stage_next);
+            step_unit32<false, P>(ia, *it.dt, it.dt->rowtab, dirc, LF, LN, U, buf, S, st, stage_next);
+        U = N;
         tile = next;
     }
     if (ca)
