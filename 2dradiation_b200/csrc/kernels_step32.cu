@@ -265,7 +265,7 @@ __device__ __forceinline__ void load_unit(const Step32Args &a, int tile, UnitCel
     // (fields exist at every node: loaded without waiting for the flags)
     U.u1 = __ldg(a.u1 + U.cij), U.u2 = __ldg(a.u2 + U.cij), U.lor = __ldg(a.lor + U.cij);
     U.adt = __ldg(a.adt + U.cij), U.eta = __ldg(a.eta + U.cij), U.k0 = __ldg(a.k0 + U.cij);
-    U.k3 = __ldg(a.k3 + U.cij), U.kak0 = __ldg(a.ka + U.cij);
+    U.k3 = __ldg(a.k3 + U.cij), U.kak0 = __ldg(a.ka + U.cij) + U.k0;
     U.scale = CURVED ? __ldg(a.ia3 + U.cij) : 1.f;
     if (CURVED)
     {
