@@ -110,6 +110,12 @@ SIGNATURES = {
     "grlbm_copy_rows": ([C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_int32], C.c_int),
     "grlbm_departure_rows": ([C.c_void_p, C.POINTER(C.c_int32)], C.c_int),
     "grlbm_set_tile_shape": ([C.c_void_p, C.c_int32, C.c_int32], C.c_int),
+    "grlbm_write_log": ([C.c_void_p, C.c_char_p], C.c_int),
+    "grlbm_host_write_log": ([C.POINTER(GridDesc), C.POINTER(MetricDesc), C.c_int32, C.c_int32, C.c_char_p,
+                              C.c_int64, C.c_int32, C.c_double, C.POINTER(C.c_char_p), _D, C.c_int32,
+                              C.c_char_p], C.c_int),
+    "grlbm_trace_begin": ([C.c_void_p, C.c_char_p], C.c_int),
+    "grlbm_trace_end": ([C.c_void_p], C.c_int),
     "grlbm_get_tile_shape": ([C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32)], C.c_int),
     "grlbm_host_stencil": ([C.c_int32, C.c_int32, _D, _D, _D, _D, C.POINTER(C.c_int64), _D], C.c_int),
     "grlbm_host_flux_table": ([C.c_int32, C.POINTER(C.c_int32), _D, _D, _D, C.c_int32], C.c_int),
@@ -171,6 +177,16 @@ def host_flux_table(n: int) -> dict:
     a, s, z = np.zeros(k), np.zeros(k), np.zeros(k)
     _check(lib().grlbm_host_flux_table(n, C.byref(size), _p(a), _p(s), _p(z), k))
     return {"inputs": a, "sigma": s, "normalization": z}
+
+
+def host_write_log(case: dict, date: str, time_steps: int, max_iterations: int, average_iterations: float,
+                   times: list, directory: str):
+    """Log.txt (Logger::Write's format) from given values, without a GPU."""
+    names = (C.c_char_p * max(len(times), 1))(*[n.encode() for n, _ in times])
+    secs = np.ascontiguousarray([t for _, t in times] or [0.0], dtype=np.float64)
+    _check(lib().grlbm_host_write_log(C.byref(grid_desc(case)), C.byref(metric_desc(case)), int(case["n_dir"]),
+                                      int(case["n_fourier"]), date.encode(), int(time_steps), int(max_iterations),
+                                      float(average_iterations), names, _p(secs), len(times), directory.encode()))
 
 
 def host_metric_arrays(case: dict) -> np.ndarray:
@@ -304,6 +320,16 @@ class Radiation:
         self._c(lib().grlbm_run_simulation(self.h, t0, sim_time, write_period, 1 if save_initial else 0,
                                            directory.encode() if directory else None, C.byref(n)))
         return n.value
+
+    # ---- Log.txt and the profile session (Logger::Write, Profiler::Session) ----
+    def write_log(self, directory: str):
+        self._c(lib().grlbm_write_log(self.h, directory.encode()))
+
+    def trace_begin(self, path: str):
+        self._c(lib().grlbm_trace_begin(self.h, path.encode()))
+
+    def trace_end(self):
+        self._c(lib().grlbm_trace_end(self.h))
 
     # ---- slab decomposition (one band of interior node rows per rank) ----
     def set_rows(self, j_first: int, j_end: int):

@@ -18,6 +18,7 @@
 #include "device_common.cuh"
 #include "frames.hpp"
 #include "host_setup.hpp"
+#include "runlog.hpp"
 
 using namespace grlbm;
 
@@ -96,6 +97,12 @@ struct grlbm_ctx
     int32_t update_max_substeps = 0;
     int64_t steps = 0;
     double table_ms = 0;
+    // the last grlbm_run_simulation's Log.txt contents, and a profile session
+    RunLog runlog;
+    double frame_s = 0; // host time spent writing CSV frames
+    bool tracing = false;
+    std::string trace_path;
+    std::vector<TraceEvent> trace;
     cudaGraphExec_t graph[2] = {nullptr, nullptr}; // kGraphSteps steps from buffer 0 / 1
     ~grlbm_ctx()
     {
@@ -116,6 +123,24 @@ void set_global_error(const char *msg) { g_create_error = msg; }
 
 namespace
 {
+// One traced entry point of a profile session (grlbm_trace_begin): the
+// event is recorded when the scope ends.
+struct TraceScope
+{
+    grlbm_ctx *ctx;
+    const char *name;
+    long long t0;
+    TraceScope(grlbm_ctx *c, const char *n) : ctx(c), name(n), t0(c && c->tracing ? trace_now_us() : 0) {}
+    ~TraceScope()
+    {
+        if (ctx && ctx->tracing)
+            ctx->trace.push_back(TraceEvent{name, t0, trace_now_us(), trace_thread_id()});
+    }
+};
+
+constexpr const char *kStepName = "grlbm_step (stream, moments, collide)";
+constexpr const char *kTablesName = "void Radiation::UpdateFourierCoefficients()";
+
 constexpr int kGraphSteps = 32;
 constexpr int kPartialBlocks = 592; // 4 x 148 SMs
 
@@ -1175,6 +1200,7 @@ int grlbm_update_fourier_coefficients(grlbm_ctx *ctx, double rk_tol, int32_t max
 {
     if (!ctx)
         return GRLBM_ERR_ARGUMENT;
+    TraceScope trace(ctx, kTablesName);
     if (!(rk_tol > 0))
         return fail(ctx, GRLBM_ERR_ARGUMENT, "rk_tol must be positive");
     cudaSetDevice(ctx->device);
@@ -1319,6 +1345,7 @@ int grlbm_sync(grlbm_ctx *ctx)
 
 int grlbm_step(grlbm_ctx *ctx, int32_t n_steps)
 {
+    TraceScope trace(ctx, kStepName);
     int rc = grlbm_step_async(ctx, n_steps);
     if (rc)
         return rc;
@@ -1454,8 +1481,15 @@ int grlbm_write_frame_csv(grlbm_ctx *ctx, float time, const char *directory, con
     CU(cudaStreamSynchronize(ctx->stream));
     std::string err;
     // E_LF, Fx_LF, Fy_LF, F_LF (src/Radiation.cpp:780)
-    if (!write_frame_csv(ctx->geo, time, h.data(), h.data() + nxy, h.data() + 2 * nxy, h.data() + 6 * nxy,
-                         directory, name ? name : "", err))
+    const long long t0 = trace_now_us();
+    bool ok;
+    {
+        TraceScope trace(ctx, kFrameWriterName);
+        ok = write_frame_csv(ctx->geo, time, h.data(), h.data() + nxy, h.data() + 2 * nxy, h.data() + 6 * nxy,
+                             directory, name ? name : "", err);
+    }
+    ctx->frame_s += (double)(trace_now_us() - t0) / 1e6;
+    if (!ok)
         return fail(ctx, GRLBM_ERR_HOST, "%s", err.c_str());
     return GRLBM_OK;
 }
@@ -1468,42 +1502,157 @@ int grlbm_run_simulation(grlbm_ctx *ctx, double t0, double sim_time, double writ
     if (!(sim_time >= 0.0) || !(write_period > 0.0))
         return fail(ctx, GRLBM_ERR_ARGUMENT, "sim_time must be >= 0 and write_period > 0");
     // src/Radiation.cpp:748-750, 772-832 (the tables are built beforehand,
-    // grlbm_update_fourier_coefficients; no console or profiler output)
+    // grlbm_update_fourier_coefficients; no console output).  The run's own
+    // measurements are kept for grlbm_write_log, as Logger::SetValues and
+    // the profiler's totals are (src/Radiation.cpp:750, 862-880).
+    cudaSetDevice(ctx->device);
     const int64_t time_steps = (int64_t)std::ceil(sim_time / ctx->geo.dt);
-    double current = t0, since = 0.0;
-    int rc;
-    const bool write = directory != nullptr;
-    if (write && save_initial)
+    RunLog log;
+    log.date = log_date_now();
+    unsigned long long it0 = 0;
+    CU(cudaStreamSynchronize(ctx->stream));
+    CU(cudaMemcpy(&it0, ctx->counters.p, sizeof it0, cudaMemcpyDeviceToHost));
+    ctx->frame_s = 0;
+    double step_s = 0;
+    auto steps = [&](int64_t n) {
+        const long long a = trace_now_us();
+        const int rc_ = grlbm_step(ctx, (int32_t)n);
+        step_s += (double)(trace_now_us() - a) / 1e6;
+        return rc_;
+    };
+    const long long total0 = trace_now_us();
     {
-        if ((rc = grlbm_write_frame_csv(ctx, (float)current, directory, "")))
-            return rc;
-        since = 0.0;
-    }
-    int64_t pending = 0; // steps enqueued since the last frame
-    for (int64_t n = 0; n < time_steps; n++)
-    {
-        pending++;
-        current += ctx->geo.dt;
-        since += ctx->geo.dt;
-        if (write && since >= write_period - 1e-8)
+        TraceScope total(ctx, "Total Time");
+        double current = t0, since = 0.0;
+        int rc;
+        const bool write = directory != nullptr;
+        if (write && save_initial)
         {
-            if ((rc = grlbm_step(ctx, (int32_t)pending)))
-                return rc;
-            pending = 0;
             if ((rc = grlbm_write_frame_csv(ctx, (float)current, directory, "")))
                 return rc;
             since = 0.0;
         }
-    }
-    if (pending && (rc = grlbm_step(ctx, (int32_t)pending)))
-        return rc;
-    if (write && since != 0.0)
-    {
-        if ((rc = grlbm_write_frame_csv(ctx, (float)current, directory, "")))
+        int64_t pending = 0; // steps enqueued since the last frame
+        for (int64_t n = 0; n < time_steps; n++)
+        {
+            pending++;
+            current += ctx->geo.dt;
+            since += ctx->geo.dt;
+            if (write && since >= write_period - 1e-8)
+            {
+                if ((rc = steps(pending)))
+                    return rc;
+                pending = 0;
+                if ((rc = grlbm_write_frame_csv(ctx, (float)current, directory, "")))
+                    return rc;
+                since = 0.0;
+            }
+        }
+        if (pending && (rc = steps(pending)))
             return rc;
+        if (write && since != 0.0)
+        {
+            if ((rc = grlbm_write_frame_csv(ctx, (float)current, directory, "")))
+                return rc;
+        }
     }
+    const double total_s = (double)(trace_now_us() - total0) / 1e6;
+    unsigned long long h[2];
+    CU(cudaMemcpy(h, ctx->counters.p, sizeof h, cudaMemcpyDeviceToHost));
+    log.time_steps = time_steps;
+    log.sim_time = (double)time_steps * ctx->geo.dt;
+    // the run's own lambda-iteration average (src/Radiation.cpp:856); the
+    // maximum is the context's since its creation
+    const double cells = (double)(ctx->geo.nx - 2) * (double)(ctx->gd.jhi - ctx->gd.jlo);
+    log.max_iterations = (int32_t)(unsigned)(h[1] & 0xffffffffu);
+    log.average_iterations = time_steps > 0 ? (double)(h[0] - it0) / ((double)time_steps * cells) : 0.0;
+    log.times = {{"Total Time", total_s},
+                 {kFrameWriterName, ctx->frame_s},
+                 {kStepName, step_s},
+                 {kTablesName, ctx->table_ms / 1e3}};
+    log.valid = true;
+    ctx->runlog = log;
     if (steps_out)
         *steps_out = time_steps;
+    return GRLBM_OK;
+}
+
+int grlbm_write_log(grlbm_ctx *ctx, const char *directory)
+{
+    if (!ctx)
+        return GRLBM_ERR_ARGUMENT;
+    if (!directory)
+        return fail(ctx, GRLBM_ERR_ARGUMENT, "null directory");
+    if (!ctx->runlog.valid)
+        return fail(ctx, GRLBM_ERR_STATE, "Log.txt describes a grlbm_run_simulation: run one first");
+    std::string err;
+    if (!write_log_txt(directory, ctx->geo, ctx->mdesc.kind, ctx->mdesc.m, ctx->mdesc.a, ctx->st, ctx->ss,
+                       ctx->runlog, err))
+        return fail(ctx, GRLBM_ERR_HOST, "%s", err.c_str());
+    return GRLBM_OK;
+}
+
+int grlbm_host_write_log(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, int32_t n_dir,
+                         int32_t n_fourier, const char *date, int64_t time_steps, int32_t max_iterations,
+                         double average_iterations, const char *const *time_names, const double *seconds,
+                         int32_t n_times, const char *directory)
+{
+    if (!grid || !metric || !date || !directory || (n_times > 0 && (!time_names || !seconds)) || n_times < 0 ||
+        n_dir < 1 || n_fourier < 1)
+        return fail(nullptr, GRLBM_ERR_ARGUMENT, "grlbm_host_write_log: bad arguments");
+    GridGeom G;
+    StencilTables st, ss;
+    try
+    {
+        G = GridGeom::from(*grid);
+        st = StencilTables::build(n_dir, true);
+        ss = StencilTables::build(n_fourier, false);
+    }
+    catch (const std::exception &e)
+    {
+        return fail(nullptr, GRLBM_ERR_ARGUMENT, "grlbm_host_write_log: %s", e.what());
+    }
+    RunLog log;
+    log.date = date;
+    log.time_steps = time_steps;
+    log.sim_time = (double)time_steps * G.dt;
+    log.max_iterations = max_iterations;
+    log.average_iterations = average_iterations;
+    for (int k = 0; k < n_times; k++)
+        log.times.emplace_back(time_names[k] ? time_names[k] : "", seconds[k]);
+    log.valid = true;
+    std::string err;
+    if (!write_log_txt(directory, G, metric->kind, metric->m, metric->a, st, ss, log, err))
+        return fail(nullptr, GRLBM_ERR_HOST, "%s", err.c_str());
+    return GRLBM_OK;
+}
+
+int grlbm_trace_begin(grlbm_ctx *ctx, const char *path)
+{
+    if (!ctx)
+        return GRLBM_ERR_ARGUMENT;
+    if (!path || !*path)
+        return fail(ctx, GRLBM_ERR_ARGUMENT, "null trace path");
+    if (ctx->tracing)
+        return fail(ctx, GRLBM_ERR_STATE, "a profile session is already open");
+    ctx->tracing = true;
+    ctx->trace_path = path;
+    ctx->trace.clear();
+    return GRLBM_OK;
+}
+
+int grlbm_trace_end(grlbm_ctx *ctx)
+{
+    if (!ctx)
+        return GRLBM_ERR_ARGUMENT;
+    if (!ctx->tracing)
+        return fail(ctx, GRLBM_ERR_STATE, "no profile session is open");
+    ctx->tracing = false;
+    std::string err;
+    const bool ok = write_trace_json(ctx->trace_path, ctx->trace, err);
+    ctx->trace.clear();
+    if (!ok)
+        return fail(ctx, GRLBM_ERR_HOST, "%s", err.c_str());
     return GRLBM_OK;
 }
 

@@ -345,6 +345,31 @@ int grlbm_write_frame_csv(grlbm_ctx *ctx, float time, const char *directory, con
  * NULL) receives the step count. */
 int grlbm_run_simulation(grlbm_ctx *ctx, double t0, double sim_time, double write_period, int32_t save_initial,
                          const char *directory, int64_t *steps_out);
+/* Logger::Write (src/Logger.hh:48-97) after the last grlbm_run_simulation:
+ * directory + "/Log.txt" (the directory is created) with the run's creation
+ * date, spacetime, grid, stencils, lambda-iteration counts (the average over
+ * the run's steps; the maximum since the context was created), its time
+ * measurements in seconds -- "Total Time" (the loop), the frame writer under
+ * Grid::WriteFrametoCsv's profiler name, the step calls, and the last table
+ * build under UpdateFourierCoefficients' -- the computation time (total
+ * minus frame writing) and MLUPS, in the reference's format.
+ * GRLBM_ERR_STATE before any run. */
+int grlbm_write_log(grlbm_ctx *ctx, const char *directory);
+/* The same file from given values, without a context or GPU (dates and
+ * times as the caller measured them). */
+int grlbm_host_write_log(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, int32_t n_dir,
+                         int32_t n_fourier, const char *date, int64_t time_steps, int32_t max_iterations,
+                         double average_iterations, const char *const *time_names, const double *seconds,
+                         int32_t n_times, const char *directory);
+/* A profile session (Profiler::Session::Start/End, src/Profiler.hh:77-141):
+ * between grlbm_trace_begin and grlbm_trace_end every table build, step call
+ * (grlbm_step), frame write and run loop of the context is recorded with its
+ * host start time and duration (microseconds of the profiler's clock), and
+ * grlbm_trace_end writes them to `path` in the reference's Chrome-trace JSON
+ * (directories created).  GRLBM_ERR_STATE for a second begin or an end
+ * without a begin. */
+int grlbm_trace_begin(grlbm_ctx *ctx, const char *path);
+int grlbm_trace_end(grlbm_ctx *ctx);
 /* Lambda-iteration and table-build statistics (src/Radiation.cpp:723-733,
  * 855-857). */
 int grlbm_get_stats(grlbm_ctx *ctx, grlbm_stats *stats);

@@ -59,7 +59,7 @@ class Params(C.Structure):
         ("streaming_type", C.c_int32), ("initial_data_type", C.c_int32),
         ("keep_source_nodes_active", C.c_int32), ("n_steps", C.c_int32),
         ("rk_tol", C.c_double), ("use_run_simulation", C.c_int32),
-        ("n_threads", C.c_int32),
+        ("n_threads", C.c_int32), ("update_tables_each_step", C.c_int32),
     ]
 
 
@@ -146,7 +146,8 @@ def available(kind: str) -> bool:
 
 
 def run(case: dict, kind: str = "oracle", metric_override: np.ndarray | None = None,
-        want_metric: bool = False, use_run_simulation: bool = False, n_threads: int = 0) -> dict:
+        want_metric: bool = False, use_run_simulation: bool = False, n_threads: int = 0,
+        update_tables_each_step: bool = False) -> dict:
     """Run one case (a dict as built by the package's ``workloads`` module).
 
     Returns every output of oracle/ref_api.h as numpy arrays (node arrays of
@@ -167,6 +168,7 @@ def run(case: dict, kind: str = "oracle", metric_override: np.ndarray | None = N
         keep_source_nodes_active=int(case["keep_source_nodes_active"]),
         n_steps=int(case["n_steps"]), rk_tol=case["rk_tol"],
         use_run_simulation=int(use_run_simulation), n_threads=n_threads,
+        update_tables_each_step=int(update_tables_each_step),
     )
     f = case["fields"]
     keep = []

@@ -49,6 +49,9 @@ typedef struct
     int32_t use_run_simulation;
     /* OpenMP threads (0 = leave default) */
     int32_t n_threads;
+    /* Config::updateFourierHarmonics (src/Config.hh:51): rebuild the geodesic
+     * tables at the top of every step (reference driver only) */
+    int32_t update_tables_each_step;
 } grlbm_ref_params;
 
 typedef struct

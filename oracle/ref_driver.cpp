@@ -130,7 +130,7 @@ extern "C" int ref_run(const grlbm_ref_params *p, const grlbm_ref_inputs *in, gr
         .t0 = 0,
         .simTime = (p->n_steps - 0.5) * grid.dt,
         .writePeriod = g_frame_workdir.empty() ? 1e300 : g_frame_period,
-        .updateFourierHarmonics = false,
+        .updateFourierHarmonics = p->update_tables_each_step != 0,
         .keepSourceNodesActive = p->keep_source_nodes_active != 0,
         .writeData = !g_frame_workdir.empty(),
         .printSetup = false,
@@ -191,6 +191,9 @@ extern "C" int ref_run(const grlbm_ref_params *p, const grlbm_ref_inputs *in, gr
         for (int n = 0; n < p->n_steps; n++)
         {
             auto ts = std::chrono::steady_clock::now();
+            // src/Radiation.cpp:790-793
+            if (config.updateFourierHarmonics)
+                r.UpdateFourierCoefficients();
             if (config.keepSourceNodesActive)
                 r.LoadInitialData();
             switch (config.streamingType)

@@ -124,6 +124,21 @@ def test_step_bitwise_against_oracle_at_scale(maker, kw, steps, grlbm, W, oracle
     assert res["max_iterations"] == ref["max_iterations"]
 
 
+def test_config3_full_size_against_oracle(grlbm, W, oracle):
+    """The curved-scattering workload at its full size (400^2 cells, 64
+    directions, Fourier order 16): 5 plain steps from the oracle's geodesic
+    tables are bit-identical to the oracle's, and the precision form from the
+    same tables stays within 1e-5 of them."""
+    case = W.curved_scatter(steps=5)
+    ref = oracle.run(case, "oracle", n_threads=0)
+    res = run_with_tables(grlbm, case, ref)
+    bitwise(res, ref, MOMENTS + ("I",) + LF)
+    assert res["max_iterations"] == ref["max_iterations"]
+    assert res["average_iterations"] == ref["average_iterations"]
+    res32 = run_with_tables(grlbm, case, ref, precision=1)
+    check(res32, ref, ("E", "Fx", "Fy"), tol=1e-5)
+
+
 def test_end_to_end_config2_scale(grlbm, W, oracle):
     """The curved-streaming workload (no scattering) at full grid size."""
     case = W.curved_shell(steps=30)
