@@ -1,0 +1,99 @@
+"""The C++ drop-in class RadiationB200 (include/RadiationB200.h), compiled
+against the reference's own headers and sources and linked to libgrlbm.so
+(oracle/Makefile target `facade` builds tests/facade/beam_demo.cpp).  The
+demo runs the reference's beam user code (exe/main.cpp:246-343 and 538-598)
+on the reference's Radiation and on RadiationB200 in one process.
+
+Without a GPU the facade's constructor must fail with the library's message
+(grlbm_create returns GRLBM_ERR_CUDA); on a GPU both classes must agree on
+the intensities, moments, Fourier coefficients, iteration counts and frame
+files."""
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+ROOT = Path(__file__).resolve().parents[1]
+DEMO = ROOT / "oracle" / "_ref" / "beam_demo"
+
+
+def demo():
+    if not DEMO.exists():
+        import oracle
+        ref = oracle.reference_root()
+        if not (ref and os.path.isdir(os.path.join(ref, "src"))):
+            pytest.skip("the reference tree is absent and beam_demo was not built")
+        subprocess.run(["make", "-s", "-C", str(ROOT / "oracle"), "facade", f"REF={ref}"], check=True)
+    return str(DEMO)
+
+
+def test_facade_compiles_and_refuses_without_gpu(grlbm, tmp_path):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    exe = demo()
+    out = subprocess.run([exe, "nogpu"], cwd=tmp_path, capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert out.stdout.startswith("refused: libgrlbm: "), out.stdout
+    assert "CUDA" in out.stdout or "device" in out.stdout
+
+
+def test_facade_keeps_reference_members_and_hides_base():
+    """Radiation's methods are not virtual: RadiationB200 inherits it
+    privately, so binding it to a Radiation& must not compile, while user
+    code that writes the reference's public buffers must."""
+    import oracle
+    ref = oracle.reference_root()
+    if not (ref and os.path.isdir(os.path.join(ref, "src"))):
+        pytest.skip("the reference tree is absent")
+    inc = ["-I", str(ROOT / "oracle" / "eigen_standin"), "-I", os.path.join(ref, "src"), "-I", str(ROOT / "include")]
+    good = ('#include "RadiationB200.h"\n'
+            'void f(RadiationB200 &r) { r.kappa0[0] = 1; r.initialI[r.Index(0, 0)] = 2; '
+            'r.isInitialGridPoint[0] = true; r.RunSimulation(); double e = r.E[0] + r.Fx_LF[0]; (void)e; }\n')
+    bad = '#include "RadiationB200.h"\nRadiation &f(RadiationB200 &r) { return r; }\n'
+    for src, ok in ((good, True), (bad, False)):
+        res = subprocess.run(["g++", "-std=c++20", "-fsyntax-only", "-w", *inc, "-x", "c++", "-"], input=src,
+                             capture_output=True, text=True, timeout=300)
+        assert (res.returncode == 0) == ok, res.stderr[-2000:]
+        if not ok:
+            assert "inaccessible base" in res.stderr or "private" in res.stderr
+
+
+def read_frames(directory):
+    frames = {}
+    for p in sorted(Path(directory).glob("*.csv")):
+        rows = [ln for ln in p.read_text().splitlines() if not ln.startswith("#")]
+        frames[p.name] = np.array([[float(v) for v in ln.split(",")] for ln in rows])
+    return frames
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["flat", "curved"])
+def test_facade_matches_reference_radiation(tmp_path, kind):
+    exe = demo()
+    work = tmp_path / "run"
+    work.mkdir()
+    out = subprocess.run([exe, kind, str(work)], capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stdout + out.stderr
+    rows = {}
+    for ln in out.stdout.splitlines():
+        parts = ln.split()
+        if len(parts) == 3 and parts[0] != "total":
+            rows[parts[0]] = (float(parts[1]), float(parts[2]))
+    for name in ("I", "E", "Fx", "Fy", "Pxx", "E_LF", "F_LF", "coefficientsS", "coefficientsX"):
+        diff, mag = rows[name]
+        assert mag > 0, name
+        assert diff <= 1e-12 * mag, (name, diff, mag)
+    assert rows["maxItterationCount"][0] == rows["maxItterationCount"][1]
+    a, b = rows["averageItterationCount"]
+    assert abs(a - b) <= 1e-12 * abs(a)
+    assert rows["timeSteps"][0] == rows["timeSteps"][1] > 0
+    ref = read_frames(tmp_path / "output" / "ref" / "Moments")
+    ours = read_frames(tmp_path / "output" / "b200" / "Moments")
+    assert len(ref) >= 3 and sorted(ref) == sorted(ours)
+    for name in ref:
+        assert np.allclose(ours[name], ref[name], rtol=1e-9, atol=1e-12), name
+    assert (tmp_path / "output" / "b200" / "Log.txt").exists()
+    assert (work / "output" / "b200" / "profileResults.json").exists()
