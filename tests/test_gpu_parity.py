@@ -127,8 +127,13 @@ def test_step_bitwise_against_oracle_at_scale(maker, kw, steps, grlbm, W, oracle
 def test_config3_full_size_against_oracle(grlbm, W, oracle):
     """The curved-scattering workload at its full size (400^2 cells, 64
     directions, Fourier order 16): 5 plain steps from the oracle's geodesic
-    tables are bit-identical to the oracle's, and the precision form from the
-    same tables stays within 1e-5 of them."""
+    tables are bit-identical to the oracle's.  The precision form from the
+    same tables stays within the lambda iteration's own tolerance (1e-4,
+    src/Radiation.h:16) of them: in the first steps, before the field settles,
+    the exit test (src/Radiation.cpp:710-716) divides moments that are
+    rounding noise, so the two arithmetics can stop a cell's iteration at
+    different cycles.  The 1e-5 bound of the precision form applies after the
+    2000 steps of the workload (test_gpu_properties)."""
     case = W.curved_scatter(steps=5)
     ref = oracle.run(case, "oracle", n_threads=0)
     res = run_with_tables(grlbm, case, ref)
@@ -136,7 +141,7 @@ def test_config3_full_size_against_oracle(grlbm, W, oracle):
     assert res["max_iterations"] == ref["max_iterations"]
     assert res["average_iterations"] == ref["average_iterations"]
     res32 = run_with_tables(grlbm, case, ref, precision=1)
-    check(res32, ref, ("E", "Fx", "Fy"), tol=1e-5)
+    check(res32, ref, ("E", "Fx", "Fy"), tol=1e-4)
 
 
 def test_end_to_end_config2_scale(grlbm, W, oracle):
