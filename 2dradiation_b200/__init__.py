@@ -27,7 +27,7 @@ ERRORS = {1: "ARGUMENT", 2: "CUDA", 3: "STATE", 4: "UNSUPPORTED", 5: "NONCONVERG
 MINKOWSKI, SCHWARZSCHILD, KERRSCHILD = 0, 1, 2
 FLAT_FIXED, FLAT_ADAPTIVE, CURVED_FIXED, CURVED_ADAPTIVE, GEODESIC_FIXED = 0, 1, 2, 3, 4
 MOMENTS, INTENSITIES = 0, 1
-PLAIN_FP64, PRECISION_FP32 = 0, 1
+PLAIN_FP64, PRECISION_FP32, FAST_FP64 = 0, 1, 2
 
 
 class GrlbmError(RuntimeError):

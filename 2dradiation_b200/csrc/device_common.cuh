@@ -100,6 +100,13 @@ struct StateLayout
     {
         return StateLayout{nx, nx, 1, (int64_t)direction_pitch(nd), kStateMirror};
     }
+    // FP64 state of the fast form: cell-major, dp = nd + kStateMirror rounded
+    // up to 2 doubles (16-byte node records)
+    static int direction_pitch64(int nd) { return (nd + kStateMirror + 1) & ~1; }
+    static StateLayout cell_major64(int64_t nx, int nd)
+    {
+        return StateLayout{nx, nx, 1, (int64_t)direction_pitch64(nd), kStateMirror};
+    }
     // elements of a buffer of ny rows and nd directions
     int64_t elements(int64_t ny, int nd) const { return sp == 1 ? plane * nd : pitch * ny * sp; }
 };
@@ -167,6 +174,25 @@ namespace packed32
 constexpr unsigned kTBits = 18, kTypeShift = 18, kStartShift = 23;
 } // namespace packed32
 
+// Packed departure record of the fast FP64 form (double4, [c * nd + d]): the
+// fractions are stored as 1 + f in [1, 2), whose exponent field is always
+// 1023, so the field and the sign bit carry the record's small integers (the
+// reader restores the exponent and subtracts 1, exactly):
+//   .x  1 + fx, fx = i_dep - i0; sign set when the corner column i0 is i
+//       (clear: i - 1); exponent bits 0-4: row type of the interpolation row
+//   .y  1 + fy likewise for the corner row (exponent unused)
+//   .z  1 + t, the blend between interpolation rows; exponent bits 0-7: the
+//       first direction of the 5-direction angular window
+//   .w  s^3 alpha_c^3 (0 when excised); sign set when the departure lies
+//       outside the cell's 3x3 neighbourhood (far: read the side record
+//       {i_dep - i, j_dep - j, angle coordinate, s^3 alpha_c^3})
+namespace packed64
+{
+constexpr unsigned kExpShift = 20;            // the exponent field in the high word
+constexpr unsigned kMantHi = 0x000FFFFFu;     // the high word's mantissa bits
+constexpr unsigned kOne = 0x3FF00000u;        // the high word of 1.0
+} // namespace packed64
+
 struct DepartureArgs
 {
     GridDev g;
@@ -178,6 +204,8 @@ struct DepartureArgs
     double4 *rec64;      // plain records [d * ncell + c] or null
     uint4 *rec32;        // precision records (packed32) [c * nd + d] or null
     float4 *side32;      // precision side records [c * nd + d] or null
+    double4 *recf;       // fast FP64 records (packed64) [c * nd + d] or null
+    double4 *sidef;      // fast FP64 side records [c * nd + d] or null
     int q, p;            // interpolation row period (row types) and its direction shift
     int row_base[32];    // first window direction of each row type
     int *clamped;
@@ -348,6 +376,47 @@ struct Step32Args
     CUtensorMap in_map;      // Iin as a 4D tensor, one box per tile patch (encode_state_map32)
 };
 
+// The fast FP64 step of the fixed streaming types (cell-major FP64 state,
+// kernels_step64.cu): the same warp-per-tile scheme with kStep64Warps warps
+// per block.
+constexpr int kStep64Warps = 4;
+struct Step64Args
+{
+    GridDev g;
+    int nd, ng, dp;          // directions, interpolation rows, direction pitch of the state
+    int q;                   // row types of the angular windows (the DirTable64's q)
+    int dps;                 // a node's doubles in the staged patch (dp padded to a multiple of 16)
+    int tx, ty;              // cells per tile
+    int ss, patch_elems;     // row stride of the streamed-value buffer, doubles of the patch buffer
+    int tiles_x, ntiles;
+    const double *Iin;
+    double *Iout;
+    const double4 *rec;      // packed records (packed64, curved)
+    const double4 *side;     // side records (curved)
+    const double *ia3;       // nxy: 1/alpha^3, the scale of the stored state (curved)
+    const uint8_t *flags;
+    const double *u1, *u2, *lor, *adt, *eta, *k0, *k3, *ka;
+    double *mom;             // 6*nxy
+    unsigned long long *iter_sum;
+    unsigned int *iter_max;
+    unsigned *fault;
+    unsigned *tiles;         // [0] next tile, [1] warps done (zero between launches)
+    CUtensorMap in_map;      // Iin as a 4D tensor, one box per tile patch (encode_state_map64)
+};
+
+// Direction tables of the fast FP64 step (device memory, copied into each
+// block's shared memory): the angular rows and moment coefficients of
+// DirTable in FP64, and the flat departures' products c dt.
+struct __align__(16) DirTable64
+{
+    double rowtab[kMaxRowTypes * 12];
+    double dirc[kMaxDirs * 8];
+    double wmom[18];
+    double cxdt[kMaxDirs], cydt[kMaxDirs];
+    int q, p;
+    double inv_q;
+};
+
 // One problem of a batched precision-form step: its step arguments for
 // either buffer parity and its direction tables (device memory).
 struct Batch32Item
@@ -413,8 +482,23 @@ void launch_step_batch32(const Batch32Item *items, const int *first_tile, int n_
 // for tiles of tx x ty cells.
 cudaError_t encode_state_map32(CUtensorMap *map, const float *state, int64_t nx, int64_t ny, int dp, int tx, int ty);
 
+// The fast FP64 step of the fixed streaming types (kernels_step64.cu), with
+// the same roles as the step32 functions above.
+int step64_passes(int nd);
+int step64_s_stride(int nd);
+int step64_patch_node_elems(int dp);
+int step64_warp_stride(int tx, int ty, int dp, int nd);
+size_t step64_smem(int tx, int ty, int dp, int nd, int q);
+cudaError_t prepare_step64();
+cudaError_t step64_occupancy(int P, bool curved, size_t smem, int *blocks);
+void launch_step64(const Step64Args &a, const DirTable64 *dt, bool curved, int P, int blocks, cudaStream_t s);
+cudaError_t encode_state_map64(CUtensorMap *map, const double *state, int64_t nx, int64_t ny, int dp, int tx, int ty);
+
 void launch_sources64(double *I, int64_t nxy, int nd, const int64_t *nodes, const double *vals, int64_t nsrc,
                       cudaStream_t s);
+// the same into a state of layout L (the fast FP64 form's cell-major state)
+void launch_sources64L(double *I, const StateLayout &L, int nd, const int64_t *nodes, const double *vals,
+                       int64_t nsrc, cudaStream_t s);
 void launch_sources32(float *I, const StateLayout &L, int nd, const int64_t *nodes, const float *vals, int64_t nsrc,
                       cudaStream_t s);
 // [5][nxy][nf] -> [5][nf][nxy]
@@ -432,6 +516,15 @@ void launch_to_cellmajor64(const double *in, double *out, int64_t nxy, int nd, c
 void launch_to_cellmajor32(const float *in, double *out, int64_t nxy, const StateLayout &L, int nd,
                            const float *scale, cudaStream_t s);
 void launch_widen32(const float *in, double *out, int64_t n, cudaStream_t s);
+// The fast FP64 form's cell-major state (layout L, stored as I * scale where
+// scale is given): from and to the boundary's cell-major [ij][d], and
+// ComputeMomentsIF of it.
+void launch_to_state64(const double *in, double *out, int64_t nxy, const StateLayout &L, int nd, const double *scale,
+                       cudaStream_t s);
+void launch_from_state64(const double *in, double *out, int64_t nxy, const StateLayout &L, int nd, const double *scale,
+                         cudaStream_t s);
+void launch_moments_from_state64(const double *J, int64_t nxy, const StateLayout &L, int nd, const double *w,
+                                 const double *n1, const double *n2, const double *scale, double *mom, cudaStream_t s);
 // ComputeMomentsIF from the current intensities (FP64 out, 6 * nxy)
 // (ang: per-node rotation angles of adaptive streaming, with n1/n2 the
 // unrotated stencil directions; null otherwise)

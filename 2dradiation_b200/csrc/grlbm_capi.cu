@@ -55,6 +55,7 @@ struct grlbm_ctx
     StencilTables st, ss;
     MetricArrays M;
     bool fp32 = false;
+    bool fast64 = false; // GRLBM_FAST_FP64: cell-major FP64 state, the fast FP64 step
     GridDev gd{};
     StateLayout sl{};          // node positions in the state buffers
     // precision form, fixed streaming: the step's tile shape, passes per lane,
@@ -80,6 +81,7 @@ struct grlbm_ctx
     DevBuf streamed; // plain form: the streamed values of a step
     DevBuf coef_k;   // adaptive streaming: the coefficients as [5][nf][nxy]
     DirTable dirs{}; // precision-form direction tables (kernel parameter)
+    DevBuf dirs64t;  // the fast FP64 form's direction tables (a DirTable64 in device memory)
     DevBuf cu1, cu2, clor, cadt, ceta, ck0, ck3, cka, mom, rkf, lfp;
     DevBuf coef, ss_cx, ss_cy, ss_w, proj_basis, eval_basis, stage;
     DevBuf src_nodes, src_vals, lf_out, energy_partial, energy_out;
@@ -268,6 +270,19 @@ PrecStepArgs prec_args(grlbm_ctx *ctx, int from)
     return a;
 }
 
+bool is_fixed32(const grlbm_ctx *ctx)
+{
+    return ctx->fp32 && (ctx->run.streaming_type == GRLBM_FLAT_FIXED || ctx->run.streaming_type == GRLBM_CURVED_FIXED);
+}
+// the warp-per-tile steps on a cell-major state: FP32 fixed streaming and the fast FP64 form
+bool is_tiled(const grlbm_ctx *ctx) { return is_fixed32(ctx) || ctx->fast64; }
+
+// per-node factor between the fast FP64 form's stored state and I (null: none)
+const double *state_scale64(const grlbm_ctx *ctx)
+{
+    return (ctx->fast64 && ctx->run.streaming_type == GRLBM_CURVED_FIXED) ? ctx->ia3.as<double>() : nullptr;
+}
+
 int step32_tiles_x(const grlbm_ctx *ctx) { return (int)((ctx->gd.nx_ + ctx->tile_x - 1) / ctx->tile_x); }
 int step32_tiles(const grlbm_ctx *ctx)
 {
@@ -315,27 +330,87 @@ Step32Args step32_args(grlbm_ctx *ctx, int from)
     return a;
 }
 
-// Sets the tile shape of the precision-form fixed step: the TMA maps of the
-// state buffers for its patch, and the persistent grid at its occupancy.
+// Arguments of the fast FP64 step that reads intensity buffer `from`.
+Step64Args step64_args(grlbm_ctx *ctx, int from)
+{
+    unsigned long long *cnt = ctx->counters.as<unsigned long long>();
+    Step64Args a{};
+    a.g = ctx->gd;
+    a.nd = ctx->st.n;
+    a.ng = ctx->ng;
+    a.dp = (int)ctx->sl.sp;
+    a.q = ctx->dirs.q;
+    a.dps = step64_patch_node_elems(a.dp);
+    a.tx = ctx->tile_x;
+    a.ty = ctx->tile_y;
+    a.ss = step64_s_stride(a.nd);
+    a.patch_elems = (((a.tx + 2) * (a.ty + 2) * a.dps + 15) / 16) * 16;
+    a.tiles_x = step32_tiles_x(ctx);
+    a.ntiles = step32_tiles(ctx);
+    a.Iin = ctx->I[from].as<double>();
+    a.Iout = ctx->I[from ^ 1].as<double>();
+    a.rec = ctx->rec.as<double4>();
+    a.side = ctx->side.as<double4>();
+    a.ia3 = ctx->ia3.as<double>();
+    a.flags = ctx->flags.as<uint8_t>();
+    a.u1 = ctx->cu1.as<double>();
+    a.u2 = ctx->cu2.as<double>();
+    a.lor = ctx->clor.as<double>();
+    a.adt = ctx->cadt.as<double>();
+    a.eta = ctx->ceta.as<double>();
+    a.k0 = ctx->ck0.as<double>();
+    a.k3 = ctx->ck3.as<double>();
+    a.ka = ctx->cka.as<double>();
+    a.mom = ctx->mom.as<double>();
+    a.iter_sum = cnt;
+    a.iter_max = reinterpret_cast<unsigned int *>(cnt + 1);
+    a.fault = ctx->fault;
+    a.tiles = ctx->tile_ctr.as<unsigned>();
+    a.in_map = ctx->in_map[from];
+    return a;
+}
+
+// shared memory and resident blocks per SM of the context's tiled step at a tile shape
+int tiled_fit(grlbm_ctx *ctx, int tx, int ty, size_t *smem, int *per_sm)
+{
+    const int dp = (int)ctx->sl.sp;
+    const bool curved = ctx->run.streaming_type == GRLBM_CURVED_FIXED;
+    *smem = ctx->fast64 ? step64_smem(tx, ty, dp, ctx->st.n, curved ? ctx->dirs.q : 0) : step32_smem(tx, ty, dp, ctx->st.n);
+    *per_sm = 0;
+    if (*smem > (size_t)kStep32MaxSmem)
+        return GRLBM_OK;
+    if (ctx->fast64)
+        CU(step64_occupancy(ctx->passes, curved, *smem, per_sm));
+    else
+        CU(step32_occupancy(ctx->passes, curved, false, *smem, per_sm));
+    return GRLBM_OK;
+}
+
+// Sets the tile shape of the tiled step (FP32 fixed streaming, fast FP64):
+// the TMA maps of the state buffers for its patch, and the persistent grid at
+// its occupancy.
 int set_step32_tile(grlbm_ctx *ctx, int tx, int ty)
 {
     const int dp = (int)ctx->sl.sp;
     if (tx < 1 || ty < 1 || tx * ty > kStep32UnitCells)
         return fail(ctx, GRLBM_ERR_ARGUMENT, "tile %dx%d: at least 1 and at most %d cells", tx, ty, kStep32UnitCells);
-    const size_t smem = step32_smem(tx, ty, dp, ctx->st.n);
+    size_t smem = 0;
+    int per_sm = 0, sms = 0;
+    int rc = tiled_fit(ctx, tx, ty, &smem, &per_sm);
+    if (rc)
+        return rc;
     if (smem > (size_t)kStep32MaxSmem)
         return fail(ctx, GRLBM_ERR_ARGUMENT, "tile %dx%d: its patch of %d directions needs %zu bytes of shared memory",
                     tx, ty, ctx->st.n, smem);
-    const bool curved = ctx->run.streaming_type == GRLBM_CURVED_FIXED;
-    int per_sm = 0, sms = 0;
-    CU(step32_occupancy(ctx->passes, curved, false, smem, &per_sm));
     CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
     if (per_sm < 1)
         return fail(ctx, GRLBM_ERR_ARGUMENT, "tile %dx%d does not fit on an SM", tx, ty);
     for (int k = 0; k < 2; k++)
     {
         const cudaError_t e =
-            encode_state_map32(&ctx->in_map[k], ctx->I[k].as<float>(), ctx->geo.nx, ctx->geo.ny, dp, tx, ty);
+            ctx->fast64
+                ? encode_state_map64(&ctx->in_map[k], ctx->I[k].as<double>(), ctx->geo.nx, ctx->geo.ny, dp, tx, ty)
+                : encode_state_map32(&ctx->in_map[k], ctx->I[k].as<float>(), ctx->geo.nx, ctx->geo.ny, dp, tx, ty);
         if (e != cudaSuccess)
             return fail(ctx, GRLBM_ERR_CUDA, "TMA map of the state: %s", cudaGetErrorString(e));
     }
@@ -351,25 +426,20 @@ int set_step32_tile(grlbm_ctx *ctx, int tx, int ty)
 int default_step32_tile(grlbm_ctx *ctx)
 {
     static const int cand[][2] = {{4, 4}, {8, 2}, {4, 2}, {2, 2}, {2, 1}, {1, 1}};
-    const bool curved = ctx->run.streaming_type == GRLBM_CURVED_FIXED;
     for (int need = 2; need >= 1; need--)
         for (const auto &c : cand)
         {
-            const size_t smem = step32_smem(c[0], c[1], (int)ctx->sl.sp, ctx->st.n);
+            size_t smem = 0;
             int per_sm = 0;
-            if (smem > (size_t)kStep32MaxSmem)
-                continue;
-            CU(step32_occupancy(ctx->passes, curved, false, smem, &per_sm));
+            const int rc = tiled_fit(ctx, c[0], c[1], &smem, &per_sm);
+            if (rc)
+                return rc;
             if (per_sm >= need)
                 return set_step32_tile(ctx, c[0], c[1]);
         }
     return fail(ctx, GRLBM_ERR_ARGUMENT, "no tile of %d directions fits on an SM", ctx->st.n);
 }
 
-bool is_fixed32(const grlbm_ctx *ctx)
-{
-    return ctx->fp32 && (ctx->run.streaming_type == GRLBM_FLAT_FIXED || ctx->run.streaming_type == GRLBM_CURVED_FIXED);
-}
 
 // Arguments of the plain step that reads intensity buffer `from`.
 PlainStepArgs plain_args(grlbm_ctx *ctx, int from)
@@ -421,7 +491,15 @@ int enqueue_step(grlbm_ctx *ctx, int from)
 {
     const bool curved = is_curved(ctx);
     unsigned long long *cnt = ctx->counters.as<unsigned long long>();
-    if (ctx->fp32)
+    if (ctx->fast64)
+    {
+        if (ctx->run.keep_source_nodes_active && ctx->nsrc > 0)
+            launch_sources64L(ctx->I[from].as<double>(), ctx->sl, ctx->st.n, ctx->src_nodes.as<int64_t>(),
+                              ctx->src_vals.as<double>(), ctx->nsrc, ctx->stream);
+        launch_step64(step64_args(ctx, from), ctx->dirs64t.as<DirTable64>(), curved, ctx->passes, ctx->step_blocks,
+                      ctx->stream);
+    }
+    else if (ctx->fp32)
     {
         if (ctx->run.keep_source_nodes_active && ctx->nsrc > 0)
             launch_sources32(ctx->I[from].as<float>(), ctx->sl, ctx->st.n, ctx->src_nodes.as<int64_t>(),
@@ -504,9 +582,11 @@ int build_records(grlbm_ctx *ctx)
     da.alpha = ctx->alpha.as<double>();
     da.rot_c = approx_cos(0.0);
     da.rot_s = approx_sin(0.0);
-    da.rec64 = ctx->fp32 ? nullptr : ctx->rec.as<double4>();
+    da.rec64 = ctx->fp32 || ctx->fast64 ? nullptr : ctx->rec.as<double4>();
     da.rec32 = ctx->fp32 ? ctx->rec.as<uint4>() : nullptr;
     da.side32 = ctx->fp32 ? ctx->side.as<float4>() : nullptr;
+    da.recf = ctx->fast64 ? ctx->rec.as<double4>() : nullptr;
+    da.sidef = ctx->fast64 ? ctx->side.as<double4>() : nullptr;
     da.q = ctx->dirs.q;
     da.p = ctx->dirs.p;
     for (int r = 0; r < ctx->dirs.q && r < kMaxRowTypes; r++)
@@ -628,7 +708,8 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
     if (run->streaming_type == GRLBM_GEODESIC_FIXED)
         return fail(nullptr, GRLBM_ERR_UNSUPPORTED,
                     "GeodesicFixed (a performance test of the reference) is not built");
-    if (run->precision != GRLBM_PLAIN_FP64 && run->precision != GRLBM_PRECISION_FP32)
+    if (run->precision != GRLBM_PLAIN_FP64 && run->precision != GRLBM_PRECISION_FP32 &&
+        run->precision != GRLBM_FAST_FP64)
         return fail(nullptr, GRLBM_ERR_ARGUMENT, "unknown precision %d", run->precision);
     const int maxdir = kMaxDirs;
     if (run->n_dir < 4 || run->n_dir > maxdir)
@@ -641,6 +722,15 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
                              (double)StateLayout::direction_pitch(run->n_dir)) >= 2147483648.0)
         return fail(nullptr, GRLBM_ERR_ARGUMENT,
                     "the precision form indexes its state with 32 bits: it must hold fewer than 2^31 values");
+    if (run->precision == GRLBM_FAST_FP64)
+    {
+        if (adaptive_type)
+            return fail(nullptr, GRLBM_ERR_UNSUPPORTED, "the fast FP64 form steps the fixed streaming types only");
+        if ((double)(grid->nx_ + 2) * (double)(grid->ny_ + 2) * (double)StateLayout::direction_pitch64(run->n_dir) >=
+            2147483648.0)
+            return fail(nullptr, GRLBM_ERR_ARGUMENT,
+                        "the fast FP64 form indexes its nodes with 32 bits: its state must hold fewer than 2^31 values");
+    }
     if (run->n_fourier < 1 || run->n_fourier > kMaxFourier)
         return fail(nullptr, GRLBM_ERR_ARGUMENT, "n_fourier must be in [1, %d]", kMaxFourier);
     if (run->initial_data_type != GRLBM_MOMENTS && run->initial_data_type != GRLBM_INTENSITIES)
@@ -653,6 +743,7 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
     ctx->run = *run;
     ctx->mdesc = *metric;
     ctx->fp32 = run->precision == GRLBM_PRECISION_FP32;
+    ctx->fast64 = run->precision == GRLBM_FAST_FP64;
     if (const char *w = std::getenv("GRLBM_WIDE_OFFSETS"))
         ctx->wide_offsets = w[0] == '1';
     int ndev = 0;
@@ -734,7 +825,9 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
     TRY(upload_t(ctx, ctx->n2, n2));
     TRY(upload(ctx, ctx->cx, ctx->st.cx));
     TRY(upload(ctx, ctx->cy, ctx->st.cy));
-    if (ctx->fp32)
+    // the fast FP64 form's tables, built beside the FP32 ones
+    std::unique_ptr<DirTable64> t64(ctx->fast64 ? new DirTable64{} : nullptr);
+    if (ctx->fp32 || ctx->fast64)
     {
         // each cubic row g of the reference's interpolation grid blended with
         // row g+1 into one 5-direction window starting at row g's first
@@ -775,20 +868,27 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
                 W0[k] = ctx->st.ig_weight[4 * g + k];
                 W1[k + shift] = ctx->st.ig_weight[4 * g1 + k];
             }
-            float row[12];
+            double rowd[12];
             for (int k = 0; k < 4; k++)
             {
-                row[k] = (float)W0[k];
-                row[4 + k] = (float)(W1[k] - W0[k]);
+                rowd[k] = W0[k];
+                rowd[4 + k] = W1[k] - W0[k];
             }
-            row[8] = (float)W0[4];
-            row[9] = (float)(W1[4] - W0[4]);
-            row[10] = (float)base[g];
-            row[11] = 0.f;
+            rowd[8] = W0[4];
+            rowd[9] = W1[4] - W0[4];
+            rowd[10] = (double)base[g];
+            rowd[11] = 0.0;
+            float row[12];
+            for (int k = 0; k < 12; k++)
+                row[k] = (float)rowd[k];
             const int r = g % q, m = g / q;
             float *t = &dt.rowtab[r * 12];
             if (m == 0)
+            {
                 std::memcpy(t, row, sizeof row);
+                if (t64)
+                    std::memcpy(&t64->rowtab[r * 12], rowd, sizeof rowd);
+            }
             else
             {
                 // The row must act on the same directions with the same
@@ -811,6 +911,26 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
                 for (int k = 0; k < 2 * nd; k++)
                     if (std::fabs(eff_row[k] - eff_type[k]) > 1e-6)
                         return fail(nullptr, GRLBM_ERR_HOST, "interpolation row %d does not repeat row %d", g, r);
+                if (t64)
+                {
+                    // the same in FP64: the rows of a type may differ in the
+                    // reference's rounding only
+                    std::fill(eff_row.begin(), eff_row.end(), 0.0);
+                    std::fill(eff_type.begin(), eff_type.end(), 0.0);
+                    const double *td = &t64->rowtab[r * 12];
+                    for (int k = 0; k < 5; k++)
+                    {
+                        eff_row[(base[g] + k) % nd] += k < 4 ? rowd[k] : rowd[8];
+                        eff_row[nd + (base[g] + k) % nd] += k < 4 ? rowd[4 + k] : rowd[9];
+                        eff_type[(tb + k) % nd] += k < 4 ? td[k] : td[8];
+                        eff_type[nd + (tb + k) % nd] += k < 4 ? td[4 + k] : td[9];
+                    }
+                    for (int k = 0; k < 2 * nd; k++)
+                        if (std::fabs(eff_row[k] - eff_type[k]) > 1e-12)
+                            return fail(nullptr, GRLBM_ERR_HOST,
+                                        "interpolation row %d repeats row %d only to %.3g in FP64", g, r,
+                                        std::fabs(eff_row[k] - eff_type[k]));
+                }
             }
         }
         dt.q = q;
@@ -841,6 +961,27 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
         }
         for (int q = 0; q < 18; q++)
             dt.wmom[q] = (float)wm[q];
+        if (t64)
+        {
+            t64->q = q;
+            t64->p = pstep;
+            t64->inv_q = 1.0 / (double)q;
+            for (int d = 0; d < nd; d++)
+            {
+                const double wd = ctx->st.w[d];
+                const double cf[8] = {wd, wd * n1[d], wd * n2[d], wd * n1[d] * n1[d], wd * n1[d] * n2[d],
+                                      wd * n2[d] * n2[d], n1[d], n2[d]};
+                for (int k = 0; k < 8; k++)
+                    t64->dirc[8 * d + k] = cf[k];
+                // the products c dt of the reference's flat departure (src/Radiation.cpp:398-399)
+                t64->cxdt[d] = ctx->st.cx[d] * G.dt;
+                t64->cydt[d] = ctx->st.cy[d] * G.dt;
+            }
+            for (int q = 0; q < 18; q++)
+                t64->wmom[q] = wm[q];
+            std::vector<DirTable64> one(1, *t64);
+            TRY(upload(ctx, ctx->dirs64t, one));
+        }
     }
     // the interpolation grid's rows: the plain form's stream, and adaptive
     // streaming in either form
@@ -902,7 +1043,7 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
     TRY(upload(ctx, ctx->alpha, alpha));
     TRY(upload(ctx, ctx->flags, flags));
     TRY(upload(ctx, ctx->bhmask, bh));
-    if (ctx->fp32)
+    if (ctx->fp32 || ctx->fast64)
         TRY(upload_t(ctx, ctx->ia3, ia3));
     else
     {
@@ -927,10 +1068,11 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
     TRY(upload(ctx, ctx->coef, identity_coefficients(ctx)));
 
     // state
-    ctx->sl = !ctx->fp32 ? StateLayout::dense(G.nx, G.ny)
-                         : (is_adaptive(ctx) ? StateLayout::padded32(G.nx, G.ny) : StateLayout::cell_major32(G.nx, nd));
+    ctx->sl = ctx->fast64 ? StateLayout::cell_major64(G.nx, nd)
+              : !ctx->fp32 ? StateLayout::dense(G.nx, G.ny)
+                           : (is_adaptive(ctx) ? StateLayout::padded32(G.nx, G.ny) : StateLayout::cell_major32(G.nx, nd));
     const size_t ib = (size_t)ctx->sl.elements(G.ny, nd) * tsize(ctx);
-    if (ctx->fp32)
+    if (ctx->fp32 || ctx->fast64)
     {
         if (cudaHostAlloc(reinterpret_cast<void **>(&ctx->fault), sizeof(unsigned),
                           cudaHostAllocMapped | cudaHostAllocPortable) != cudaSuccess)
@@ -939,12 +1081,12 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
     }
     TRY(alloc(ctx, ctx->I[0], ib));
     TRY(alloc(ctx, ctx->I[1], ib));
-    if (!ctx->fp32 || is_adaptive(ctx))
+    if ((!ctx->fp32 && !ctx->fast64) || is_adaptive(ctx))
         TRY(alloc(ctx, ctx->streamed, (size_t)nxy * nd * tsize(ctx)));
     TRY(alloc(ctx, ctx->mom, (size_t)6 * nxy * tsize(ctx)));
     TRY(alloc(ctx, ctx->rec, (size_t)ctx->ncell * nd * (ctx->fp32 ? sizeof(float4) : sizeof(double4))));
-    if (ctx->fp32)
-        TRY(alloc(ctx, ctx->side, (size_t)ctx->ncell * nd * sizeof(float4)));
+    if (ctx->fp32 || ctx->fast64)
+        TRY(alloc(ctx, ctx->side, (size_t)ctx->ncell * nd * (ctx->fp32 ? sizeof(float4) : sizeof(double4))));
     TRY(alloc(ctx, ctx->counters, 8 * sizeof(unsigned long long)));
     TRY(alloc(ctx, ctx->tile_ctr, 2 * sizeof(unsigned)));
     cudaMemset(ctx->tile_ctr.p, 0, ctx->tile_ctr.bytes);
@@ -952,13 +1094,13 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
     TRY(alloc(ctx, ctx->energy_out, sizeof(double)));
     cudaMemset(ctx->I[0].p, 0, ib);
     cudaMemset(ctx->I[1].p, 0, ib);
-    if (is_fixed32(ctx))
+    if (is_tiled(ctx))
     {
-        ctx->passes = step32_passes(nd);
+        ctx->passes = ctx->fast64 ? step64_passes(nd) : step32_passes(nd);
         if (ctx->passes < 1)
-            return fail(nullptr, GRLBM_ERR_ARGUMENT, "n_dir %d exceeds the precision step's passes", nd);
-        if (prepare_step32() != cudaSuccess)
-            return fail(nullptr, GRLBM_ERR_CUDA, "cannot reserve shared memory for the precision step");
+            return fail(nullptr, GRLBM_ERR_ARGUMENT, "n_dir %d exceeds the tiled step's passes", nd);
+        if ((ctx->fast64 ? prepare_step64() : prepare_step32()) != cudaSuccess)
+            return fail(nullptr, GRLBM_ERR_CUDA, "cannot reserve shared memory for the tiled step");
         TRY(default_step32_tile(ctx));
     }
     if (is_adaptive(ctx))
@@ -1084,6 +1226,19 @@ int grlbm_set_initial_data(grlbm_ctx *ctx, const uint8_t *is_initial, const doub
         return fail(ctx, GRLBM_ERR_HOST, "source set-up failed: %s", e.what());
     }
     ctx->nsrc = (int64_t)S.nodes.size();
+    if (ctx->fast64 && is_curved(ctx))
+    {
+        // the fast FP64 form stores I / alpha^3
+        const int nd = ctx->st.n;
+        for (size_t s_ = 0; s_ < S.nodes.size(); s_++)
+        {
+            const double a = ctx->M.at(ALPHA, S.nodes[s_]);
+            const double s3 = 1.0 / (a * a * a);
+            const double scale = (std::isfinite(s3) && s3 > 0.0) ? s3 : 1.0;
+            for (int d = 0; d < nd; d++)
+                S.intensities[s_ * nd + d] *= scale;
+        }
+    }
     if (ctx->fp32 && is_curved(ctx))
     {
         // the precision form stores I / alpha^3
@@ -1119,7 +1274,10 @@ int grlbm_load_initial_data(grlbm_ctx *ctx)
     // both buffers: halo and excised nodes are read from whichever is current
     for (int b = 0; b < 2; b++)
     {
-        if (ctx->fp32)
+        if (ctx->fast64)
+            launch_sources64L(ctx->I[b].as<double>(), ctx->sl, ctx->st.n, ctx->src_nodes.as<int64_t>(),
+                              ctx->src_vals.as<double>(), ctx->nsrc, ctx->stream);
+        else if (ctx->fp32)
             launch_sources32(ctx->I[b].as<float>(), ctx->sl, ctx->st.n, ctx->src_nodes.as<int64_t>(),
                              ctx->src_vals.as<float>(), ctx->nsrc, ctx->stream);
         else
@@ -1162,7 +1320,10 @@ int grlbm_set_intensity(grlbm_ctx *ctx, const double *I)
     CU(cudaMemcpyAsync(ctx->stage.p, I, ctx->stage.bytes, cudaMemcpyHostToDevice, ctx->stream));
     for (int b = 0; b < 2; b++)
     {
-        if (ctx->fp32)
+        if (ctx->fast64)
+            launch_to_state64(ctx->stage.as<double>(), ctx->I[b].as<double>(), nxy, ctx->sl, nd, state_scale64(ctx),
+                              ctx->stream);
+        else if (ctx->fp32)
             launch_to_dirmajor32(ctx->stage.as<double>(), ctx->I[b].as<float>(), nxy, ctx->sl, nd,
                                  state_scale(ctx), ctx->stream);
         else
@@ -1185,7 +1346,10 @@ int grlbm_get_intensity(grlbm_ctx *ctx, double *I)
     int rc = alloc(ctx, ctx->stage, (size_t)nxy * nd * sizeof(double));
     if (rc)
         return rc;
-    if (ctx->fp32)
+    if (ctx->fast64)
+        launch_from_state64(ctx->I[ctx->cur].as<double>(), ctx->stage.as<double>(), nxy, ctx->sl, nd, state_scale64(ctx),
+                            ctx->stream);
+    else if (ctx->fp32)
         launch_to_cellmajor32(ctx->I[ctx->cur].as<float>(), ctx->stage.as<double>(), nxy, ctx->sl, nd, state_scale(ctx),
                               ctx->stream);
     else
@@ -1462,7 +1626,10 @@ int grlbm_write_frame_csv(grlbm_ctx *ctx, float time, const char *directory, con
     }
     else
     {
-        if (is_adaptive(ctx))
+        if (ctx->fast64)
+            launch_moments_from_state64(ctx->I[ctx->cur].as<double>(), nxy, ctx->sl, nd, d64, d64 + nd, d64 + 2 * nd,
+                                        state_scale64(ctx), ctx->frame_mom.as<double>(), ctx->stream);
+        else if (is_adaptive(ctx))
             launch_moments_from_I64(ctx->I[ctx->cur].as<double>(), nxy, nd, d64, ctx->cx.as<double>(),
                                     ctx->cy.as<double>(), ctx->ang[ctx->cur].as<double>(),
                                     ctx->frame_mom.as<double>(), ctx->stream);
@@ -1738,8 +1905,9 @@ int grlbm_set_tile_shape(grlbm_ctx *ctx, int32_t tile_x, int32_t tile_y)
 {
     if (!ctx)
         return GRLBM_ERR_ARGUMENT;
-    if (!is_fixed32(ctx))
-        return fail(ctx, GRLBM_ERR_UNSUPPORTED, "tiles are a setting of the precision form's fixed streaming step");
+    if (!is_tiled(ctx))
+        return fail(ctx, GRLBM_ERR_UNSUPPORTED,
+                    "tiles are a setting of the fixed streaming step of the precision and fast FP64 forms");
     cudaSetDevice(ctx->device);
     CU(cudaStreamSynchronize(ctx->stream));
     return set_step32_tile(ctx, tile_x, tile_y);
@@ -1749,7 +1917,7 @@ int grlbm_get_tile_shape(const grlbm_ctx *ctx, int32_t *tile_x, int32_t *tile_y)
 {
     if (!ctx || !tile_x || !tile_y)
         return GRLBM_ERR_ARGUMENT;
-    if (!is_fixed32(ctx))
+    if (!is_tiled(ctx))
         return GRLBM_ERR_UNSUPPORTED;
     *tile_x = ctx->tile_x;
     *tile_y = ctx->tile_y;
@@ -1804,7 +1972,7 @@ int grlbm_get_stats(grlbm_ctx *ctx, grlbm_stats *s)
     s->rk_nonconverged = (int32_t)(unsigned)h[3];
     s->departures_off_grid = (int32_t)(unsigned)h[4];
     s->table_ms = ctx->table_ms;
-    s->far_departures = ctx->fp32 ? (int64_t)h[6] : 0;
+    s->far_departures = ctx->fp32 || ctx->fast64 ? (int64_t)h[6] : 0;
     return GRLBM_OK;
 }
 
@@ -2405,7 +2573,7 @@ int grlbm_adjoint_create(grlbm_ctx *ctx, int32_t checkpoint_every, grlbm_adjoint
     if (!ctx || !out || checkpoint_every < 1)
         return afail(nullptr, GRLBM_ERR_ARGUMENT, "grlbm_adjoint_create: null context/output or interval < 1");
     *out = nullptr;
-    if (ctx->fp32)
+    if (ctx->fp32 || ctx->fast64)
         return afail(nullptr, GRLBM_ERR_UNSUPPORTED, "grlbm_adjoint_create: the adjoint follows GRLBM_PLAIN_FP64");
     if (is_adaptive(ctx))
         return afail(nullptr, GRLBM_ERR_UNSUPPORTED, "grlbm_adjoint_create: the adjoint follows the fixed streaming types");

@@ -652,9 +652,9 @@ __global__ void k_zero_halo_moments(GridDev g, T *mom)
 // (J / (1 / alpha^3)) first.
 // With `ang` (adaptive streaming) the directions are the stencil's rotated
 // by each node's angle, n1/n2 then holding the unrotated directions.
-template <typename T>
+template <typename T, typename SC>
 __global__ void k_moments_from_I(const T *I, int64_t nxy, StateLayout L, int nd, const double *w,
-                                 const double *n1, const double *n2, const float *scale, const double *ang,
+                                 const double *n1, const double *n2, const SC *scale, const double *ang,
                                  double *mom)
 {
     const int64_t ij = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -810,8 +810,8 @@ __global__ void k_coef_k_major(const double *coef, double *coef_k, int64_t nxy, 
 }
 
 // the boundary's cell-major double [ij][d] <-> a state buffer of layout L
-template <class T>
-__global__ void k_to_dirmajor(const double *in, T *out, int64_t nxy, StateLayout L, int nd, const float *scale)
+template <class T, class SC>
+__global__ void k_to_dirmajor(const double *in, T *out, int64_t nxy, StateLayout L, int nd, const SC *scale)
 {
     __shared__ double tile[32][33];
     const int64_t ij0 = (int64_t)blockIdx.x * 32;
@@ -837,8 +837,8 @@ __global__ void k_to_dirmajor(const double *in, T *out, int64_t nxy, StateLayout
         }
     }
 }
-template <class T>
-__global__ void k_to_cellmajor(const T *in, double *out, int64_t nxy, StateLayout L, int nd, const float *scale)
+template <class T, class SC>
+__global__ void k_to_cellmajor(const T *in, double *out, int64_t nxy, StateLayout L, int nd, const SC *scale)
 {
     __shared__ double tile[32][33];
     const int64_t ij0 = (int64_t)blockIdx.x * 32;
@@ -988,38 +988,58 @@ void launch_energy32(const GridDev &g, const float *E, double *partial, int nblo
 }
 void launch_to_dirmajor64(const double *in, double *out, int64_t nxy, int nd, cudaStream_t s)
 {
-    k_to_dirmajor<double><<<dim3(nblk(nxy, 32), nblk(nd, 32)), dim3(32, 8), 0, s>>>(in, out, nxy, StateLayout{nxy, nxy, nxy}, nd,
-                                                                                      nullptr);
+    k_to_dirmajor<double, double><<<dim3(nblk(nxy, 32), nblk(nd, 32)), dim3(32, 8), 0, s>>>(
+        in, out, nxy, StateLayout{nxy, nxy, nxy}, nd, nullptr);
 }
 void launch_to_dirmajor32(const double *in, float *out, int64_t nxy, const StateLayout &L, int nd,
                           const float *scale, cudaStream_t s)
 {
-    k_to_dirmajor<float><<<dim3(nblk(nxy, 32), nblk(nd, 32)), dim3(32, 8), 0, s>>>(in, out, nxy, L, nd, scale);
+    k_to_dirmajor<float, float><<<dim3(nblk(nxy, 32), nblk(nd, 32)), dim3(32, 8), 0, s>>>(in, out, nxy, L, nd, scale);
 }
 void launch_to_cellmajor64(const double *in, double *out, int64_t nxy, int nd, cudaStream_t s)
 {
-    k_to_cellmajor<double><<<dim3(nblk(nxy, 32), nblk(nd, 32)), dim3(32, 8), 0, s>>>(in, out, nxy, StateLayout{nxy, nxy, nxy}, nd,
-                                                                                       nullptr);
+    k_to_cellmajor<double, double><<<dim3(nblk(nxy, 32), nblk(nd, 32)), dim3(32, 8), 0, s>>>(
+        in, out, nxy, StateLayout{nxy, nxy, nxy}, nd, nullptr);
 }
 void launch_to_cellmajor32(const float *in, double *out, int64_t nxy, const StateLayout &L, int nd,
                            const float *scale, cudaStream_t s)
 {
-    k_to_cellmajor<float><<<dim3(nblk(nxy, 32), nblk(nd, 32)), dim3(32, 8), 0, s>>>(in, out, nxy, L, nd, scale);
+    k_to_cellmajor<float, float><<<dim3(nblk(nxy, 32), nblk(nd, 32)), dim3(32, 8), 0, s>>>(in, out, nxy, L, nd, scale);
 }
 void launch_moments_from_I64(const double *I, int64_t nxy, int nd, const double *w, const double *n1,
                              const double *n2, const double *ang, double *mom, cudaStream_t s)
 {
-    k_moments_from_I<double><<<nblk(nxy, 128), 128, 0, s>>>(I, nxy, StateLayout{nxy, nxy, nxy}, nd, w, n1, n2, nullptr, ang,
-                                                             mom);
+    k_moments_from_I<double, double><<<nblk(nxy, 128), 128, 0, s>>>(I, nxy, StateLayout{nxy, nxy, nxy}, nd, w, n1, n2,
+                                                                     nullptr, ang, mom);
 }
 void launch_moments_from_I32(const float *J, int64_t nxy, const StateLayout &L, int nd, const double *w,
                              const double *n1, const double *n2, const float *scale, const double *ang, double *mom,
                              cudaStream_t s)
 {
-    k_moments_from_I<float><<<nblk(nxy, 128), 128, 0, s>>>(J, nxy, L, nd, w, n1, n2, scale, ang, mom);
+    k_moments_from_I<float, float><<<nblk(nxy, 128), 128, 0, s>>>(J, nxy, L, nd, w, n1, n2, scale, ang, mom);
 }
 void launch_widen32(const float *in, double *out, int64_t n, cudaStream_t s)
 {
     k_widen<<<nblk(n, 256), 256, 0, s>>>(in, out, n);
+}
+void launch_sources64L(double *I, const StateLayout &L, int nd, const int64_t *nodes, const double *vals,
+                       int64_t nsrc, cudaStream_t s)
+{
+    k_sources<double><<<nblk(nsrc * nd, 256), 256, 0, s>>>(I, L, nd, nodes, vals, nsrc);
+}
+void launch_to_state64(const double *in, double *out, int64_t nxy, const StateLayout &L, int nd, const double *scale,
+                       cudaStream_t s)
+{
+    k_to_dirmajor<double, double><<<dim3(nblk(nxy, 32), nblk(nd, 32)), dim3(32, 8), 0, s>>>(in, out, nxy, L, nd, scale);
+}
+void launch_from_state64(const double *in, double *out, int64_t nxy, const StateLayout &L, int nd, const double *scale,
+                         cudaStream_t s)
+{
+    k_to_cellmajor<double, double><<<dim3(nblk(nxy, 32), nblk(nd, 32)), dim3(32, 8), 0, s>>>(in, out, nxy, L, nd, scale);
+}
+void launch_moments_from_state64(const double *J, int64_t nxy, const StateLayout &L, int nd, const double *w,
+                                 const double *n1, const double *n2, const double *scale, double *mom, cudaStream_t s)
+{
+    k_moments_from_I<double, double><<<nblk(nxy, 128), 128, 0, s>>>(J, nxy, L, nd, w, n1, n2, scale, nullptr, mom);
 }
 } // namespace grlbm

@@ -48,7 +48,7 @@
 #include <algorithm>
 
 #include "device_common.cuh"
-#include "tma_util.cuh"
+#include "step_common.cuh"
 
 #ifndef GRLBM_STEP32_MIN_BLOCKS
 #define GRLBM_STEP32_MIN_BLOCKS 2
@@ -61,9 +61,6 @@ namespace
 constexpr int kWarps = kStep32Warps;
 constexpr int kUnitCells = kStep32UnitCells;
 constexpr int kThreads = 32 * kWarps;
-// time limits of a staging wait (a copy lands within microseconds) and of the
-// drain of a copy in flight after a wait has run out
-constexpr unsigned long long kWaitNs = 200000000ull, kDrainNs = 2000000000ull;
 // shared layout: the warps' mbarriers, the row-type table and the direction
 // coefficients (single-problem kernel), then the warps' buffers from the next
 // 128-byte boundary
@@ -71,12 +68,6 @@ constexpr int kBarBytes = 8 * kWarps;
 constexpr int kRowtabOffset = 64;
 static_assert(kBarBytes <= kRowtabOffset, "mbarriers before the row-type table");
 static_assert(kUnitCells == 16, "phase 2 pairs lane c and lane c + 16");
-
-__device__ __forceinline__ unsigned char *align128(unsigned char *p)
-{
-    const unsigned a = smem_addr(p);
-    return p + ((128u - (a & 127u)) & 127u);
-}
 
 // direction coefficients of the affine collide map for a moving fluid
 __device__ __forceinline__ void collide_coeffs32(float n1, float n2, float u1, float u2, float lor, float adt,
@@ -194,13 +185,6 @@ __device__ __forceinline__ void load_lane_dirs(float2 (&LN)[P], const float4 *di
     }
 }
 
-// Per-warp running statistics of the lambda iteration.
-struct IterStats
-{
-    unsigned long long sum;
-    unsigned max;
-};
-
 // Stage the patch of `tile` (node origin x0 = bx tx, y0 = jlo - 1 + by ty)
 // into the warp's buffer: one tensor copy, completing on the warp's mbarrier.
 __device__ __forceinline__ void stage_tile(const Step32Args &a, int tile, float *patch, unsigned bar)
@@ -213,22 +197,6 @@ __device__ __forceinline__ void stage_tile(const Step32Args &a, int tile, float 
         mbar_arrive_expect(bar, (unsigned)((a.tx + 2) * (a.ty + 2) * a.dps) * 4u);
         tma_load_4d(smem_addr(patch), &a.in_map, 0, 0, bx * a.tx, (int)a.g.jlo - 1 + by * a.ty, bar);
     }
-}
-
-// Waits for the warp's staged patch; on a timeout raises the fault word and
-// lets the copy in flight land (bounded) before the warp stops.
-__device__ __forceinline__ bool wait_tile(const Step32Args &a, unsigned bar, unsigned &parity)
-{
-    const bool landed = mbar_wait(bar, parity, kWaitNs, a.fault);
-    if (!__all_sync(0xffffffffu, landed))
-    {
-        if ((threadIdx.x & 31) == 0 && a.fault)
-            *reinterpret_cast<volatile unsigned *>(a.fault) = 1u;
-        mbar_wait(bar, parity, kDrainNs, nullptr);
-        return false;
-    }
-    parity ^= 1u;
-    return true;
 }
 
 // A tile's cells as phase 1 and phase 2 need them: lane c (< 16, and its
@@ -301,7 +269,7 @@ __device__ __forceinline__ void load_unit(const Step32Args &a, int tile, UnitCel
 template <bool CURVED, int P, class Next>
 __device__ __forceinline__ void step_unit32(const Step32Args &a, const DirTable &dt, const float *rowtab,
                                             const float4 *dirc, const LaneFlat<P> &LF, const float2 (&LN)[P],
-                                            const UnitCells<P> &U, const float *patch, float *S, IterStats &st,
+                                            const UnitCells<P> &U, const float *patch, float *S, step::IterStats &st,
                                             Next next)
 {
     const int lane = threadIdx.x & 31;
@@ -642,56 +610,6 @@ __device__ __forceinline__ void step_unit32(const Step32Args &a, const DirTable 
     __syncwarp(); // S is rewritten by the next tile's phase 1
 }
 
-// the warp's patch and streamed-value buffers in the block's shared memory
-__device__ __forceinline__ float *warp_buffers(unsigned char *smem, int header, int warp_stride)
-{
-    const int warp = threadIdx.x >> 5;
-    return reinterpret_cast<float *>(align128(smem + header) + (size_t)warp * (size_t)warp_stride);
-}
-
-// The warp is done taking tiles from counter[0]; the launch's last warp
-// clears both words for the next launch.
-__device__ __forceinline__ void retire_warp(unsigned *counter)
-{
-    if ((threadIdx.x & 31) == 0)
-    {
-        __threadfence(); // this warp's last take is ordered before its retirement
-        if (atomicAdd(counter + 1, 1u) == gridDim.x * (unsigned)kWarps - 1u)
-        {
-            counter[0] = 0u;
-            counter[1] = 0u;
-        }
-    }
-}
-
-// The warp's lambda-iteration statistics (each lane counted its own cells):
-// summed and maximised over the lanes, one atomic each.  Called by the whole
-// warp.
-__device__ __forceinline__ void flush_stats(const IterStats &st, unsigned long long *iter_sum, unsigned *iter_max)
-{
-    unsigned long long sum = st.sum;
-    unsigned mx = st.max;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1)
-    {
-        sum += __shfl_xor_sync(0xffffffffu, sum, o);
-        mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    }
-    if ((threadIdx.x & 31) == 0 && sum)
-    {
-        atomicAdd(iter_sum, sum);
-        atomicMax(iter_max, mx);
-    }
-}
-
-__device__ __forceinline__ int take_tile(unsigned *counter)
-{
-    int t = 0;
-    if ((threadIdx.x & 31) == 0)
-        t = (int)atomicAdd(counter, 1u);
-    return __shfl_sync(0xffffffffu, t, 0);
-}
-
 // shared layout of the single-problem kernel: the warps' mbarriers, the
 // row-type table, the direction coefficients, then the warps' buffers
 __device__ __forceinline__ int step32_header(int nd) { return kRowtabOffset + kMaxRowTypes * 12 * 4 + 32 * nd; }
@@ -712,16 +630,16 @@ __global__ void __launch_bounds__(kThreads, GRLBM_STEP32_MIN_BLOCKS)
     for (int k = threadIdx.x; k < 2 * a.nd; k += kThreads)
         dirc[k] = reinterpret_cast<const float4 *>(dt.dirc)[k];
     __syncthreads();
-    float *patch = warp_buffers(smem, step32_header(a.nd), warp_stride);
+    float *patch = step::warp_buffers<float>(smem, step32_header(a.nd), warp_stride);
     float *S = patch + a.patch_floats;
     LaneFlat<P> LF;
     if (!CURVED)
         load_lane_flat<P>(LF, dt, a.nd, a.dps, a.tx + 2);
     float2 LN[P];
     load_lane_dirs<P>(LN, dirc, a.nd);
-    IterStats st{0ull, 0u};
+    step::IterStats st{0ull, 0u};
     unsigned parity = 0;
-    int tile = take_tile(a.tiles);
+    int tile = step::take_tile(a.tiles);
     UnitCells<P> U;
     if (tile < a.ntiles)
     {
@@ -730,12 +648,12 @@ __global__ void __launch_bounds__(kThreads, GRLBM_STEP32_MIN_BLOCKS)
     }
     while (tile < a.ntiles)
     {
-        if (!wait_tile(a, bar, parity))
+        if (!step::wait_tile(bar, parity, a.fault))
             break;
         int next = a.ntiles;
         UnitCells<P> N;
         step_unit32<CURVED, P>(a, dt, rowtab, dirc, LF, LN, U, patch, S, st, [&]() {
-            next = take_tile(a.tiles);
+            next = step::take_tile(a.tiles);
             if (next < a.ntiles)
             {
                 stage_tile(a, next, patch, bar);
@@ -745,8 +663,8 @@ __global__ void __launch_bounds__(kThreads, GRLBM_STEP32_MIN_BLOCKS)
         U = N;
         tile = next;
     }
-    flush_stats(st, a.iter_sum, a.iter_max);
-    retire_warp(a.tiles);
+    step::flush_stats(st, a.iter_sum, a.iter_max);
+    step::retire_warp(a.tiles, kWarps);
 }
 
 // Many problems in one persistent launch: the warps take tiles from one
@@ -777,10 +695,10 @@ __global__ void __launch_bounds__(kThreads, GRLBM_STEP32_MIN_BLOCKS)
     if ((threadIdx.x & 31) == 0)
         mbar_init(bar, 1);
     __syncthreads();
-    float *buf = warp_buffers(smem, kRowtabOffset, warp_stride);
+    float *buf = step::warp_buffers<float>(smem, kRowtabOffset, warp_stride);
     LaneFlat<P> LF;
     float2 LN[P];
-    IterStats st{0ull, 0u};
+    step::IterStats st{0ull, 0u};
     unsigned parity = 0;
     int cur = -1;
     const Step32Args *ca = nullptr;
@@ -795,7 +713,7 @@ __global__ void __launch_bounds__(kThreads, GRLBM_STEP32_MIN_BLOCKS)
         else
             load_unit<false, P>(na, t - first_tile[nk], u);
     };
-    int tile = take_tile(counters);
+    int tile = step::take_tile(counters);
     UnitCells<P> U;
     if (tile < total_tiles)
         start_tile(tile, U);
@@ -804,13 +722,13 @@ __global__ void __launch_bounds__(kThreads, GRLBM_STEP32_MIN_BLOCKS)
         const int k = batch_item_of(first_tile, n_items, tile);
         const Batch32Item &it = items[k];
         const Step32Args &ia = it.a[it.cur0 ^ flip];
-        if (!wait_tile(ia, bar, parity))
+        if (!step::wait_tile(bar, parity, ia.fault))
             break;
         if (k != cur)
         {
             if (ca)
-                flush_stats(st, ca->iter_sum, ca->iter_max);
-            st = IterStats{0ull, 0u};
+                step::flush_stats(st, ca->iter_sum, ca->iter_max);
+            st = step::IterStats{0ull, 0u};
             cur = k;
             ca = &ia;
             if (!it.curved)
@@ -820,7 +738,7 @@ __global__ void __launch_bounds__(kThreads, GRLBM_STEP32_MIN_BLOCKS)
         int next = total_tiles;
         UnitCells<P> N;
         auto stage_next = [&]() {
-            next = take_tile(counters);
+            next = step::take_tile(counters);
             if (next < total_tiles)
                 start_tile(next, N);
         };
@@ -836,8 +754,8 @@ __global__ void __launch_bounds__(kThreads, GRLBM_STEP32_MIN_BLOCKS)
         tile = next;
     }
     if (ca)
-        flush_stats(st, ca->iter_sum, ca->iter_max);
-    retire_warp(counters);
+        step::flush_stats(st, ca->iter_sum, ca->iter_max);
+    step::retire_warp(counters, kWarps);
 }
 
 inline unsigned nblk(int64_t n, int b) { return (unsigned)((n + b - 1) / b); }

@@ -357,7 +357,7 @@ __global__ void __launch_bounds__(128) k_departure(DepartureArgs a)
         return;
     int d;
     int64_t c;
-    if (a.rec32)
+    if (a.rec32 || a.recf)
     {
         c = tid / a.nd;
         d = (int)(tid - c * a.nd);
@@ -384,12 +384,14 @@ __global__ void __launch_bounds__(128) k_departure(DepartureArgs a)
     }
     double4 r64;
     float4 r32;
+    double4 sf; // the FP64 side record {i_dep - i, j_dep - j, angle coordinate, s^3 alpha_c^3}
     double dd; // angle coordinate of the departure direction
     if (dev_inside_bh(a.g, xt, yt))
     {
         r64 = make_double4((double)i, (double)j, -1.0, 0.0);
         dd = 10.0 * d + 5.0;
         r32 = make_float4(0.f, 0.f, (float)dd, 0.f);
+        sf = make_double4(0.0, 0.0, dd, 0.0);
     }
     else
     {
@@ -423,7 +425,9 @@ __global__ void __launch_bounds__(128) k_departure(DepartureArgs a)
         if (!(oy == oy))
             oy = 0.0;
         const double al = a.alpha[ij];
-        r32 = make_float4((float)ox, (float)oy, (float)dd, (float)(s3 * (al * al * al)));
+        const double s3a3 = s3 * (al * al * al);
+        r32 = make_float4((float)ox, (float)oy, (float)dd, (float)s3a3);
+        sf = make_double4(ox, oy, dd, s3a3);
     }
     if (a.rec32)
     {
@@ -449,6 +453,41 @@ __global__ void __launch_bounds__(128) k_departure(DepartureArgs a)
         if (!near && a.far)
             atomicAdd(a.far, 1ull);
         a.side32[tid] = r32;
+    }
+    if (a.recf)
+    {
+        // packed64 record: the fractions, blend and window of the FP64 side
+        // record, with the corner, row type, window start and far flag in the
+        // spare bits of 1 + f
+        const double fxd = floor(sf.x), fyd = floor(sf.y);
+        const bool near = (fxd == -1.0 || fxd == 0.0) && (fyd == -1.0 || fyd == 0.0);
+        double ddc = dd == dd ? dd : 0.0;
+        int g = (int)floor(ddc);
+        g = g < 0 ? 0 : (g > a.ng - 1 ? a.ng - 1 : g);
+        double t = ddc - (double)g;
+        t = t < 0.0 ? 0.0 : (t > 1.0 ? 1.0 : t);
+        const int rt = g % a.q, m = g / a.q;
+        const unsigned start = (unsigned)((a.row_base[rt] + a.p * m) % a.nd);
+        // 1 + f in [1, 2): a value that rounds up to 2 is kept just below it
+        auto biased = [](double f, unsigned payload) {
+            double v = 1.0 + f;
+            if (!(v < 2.0))
+                v = 1.9999999999999998;
+            const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+            const unsigned hi = ((unsigned)(b >> 32) & packed64::kMantHi) | payload;
+            return __hiloint2double((int)hi, (int)(unsigned)b);
+        };
+        const double fx = near ? sf.x - fxd : 0.0, fy = near ? sf.y - fyd : 0.0;
+        const unsigned cx = near && fxd == 0.0 ? 0x80000000u : 0u, cy = near && fyd == 0.0 ? 0x80000000u : 0u;
+        double4 rf;
+        rf.x = biased(fx, cx | ((unsigned)rt << packed64::kExpShift));
+        rf.y = biased(fy, cy);
+        rf.z = biased(t, start << packed64::kExpShift);
+        rf.w = near ? sf.w : __hiloint2double((int)((unsigned)__double2hiint(sf.w) | 0x80000000u), __double2loint(sf.w));
+        a.recf[tid] = rf;
+        if (!near && a.far)
+            atomicAdd(a.far, 1ull);
+        a.sidef[tid] = sf;
     }
     if (a.rec64)
         a.rec64[tid] = r64;

@@ -31,6 +31,13 @@
  *    itself moves by ~1e-4 under a one-ulp change of its inputs).
  *    GRLBM_PRECISION_FP32 keeps intensities and the stream/collide arithmetic
  *    in FP32 (Kahan-compensated moment sums) on top of FP64 geodesic tables.
+ *    GRLBM_FAST_FP64 (fixed streaming types only) computes in FP64 with
+ *    contracted multiply-adds, a compact stored state and the lambda
+ *    iteration run on the six moments: it matches the reference to relative
+ *    L2 <= 1e-12 where the iteration's cycle count is not decided by rounding
+ *    noise (always without scattering, kappa0 = kappa1 = 0: the first
+ *    cycle's intensities are final there), and to the iteration's tolerance
+ *    otherwise.  Batches and the adjoint take the other forms.
  */
 #ifndef GRLBM_H
 #define GRLBM_H
@@ -69,6 +76,7 @@ extern "C" {
 /* Arithmetic forms */
 #define GRLBM_PLAIN_FP64 0
 #define GRLBM_PRECISION_FP32 1
+#define GRLBM_FAST_FP64 2
 
 typedef struct grlbm_ctx grlbm_ctx;
 
@@ -240,17 +248,20 @@ int grlbm_set_rows(grlbm_ctx *ctx, int64_t j_first, int64_t j_end);
 /* Bytes of one node row of the intensity state over all directions:
  * nx * nDir * 8 for GRLBM_PLAIN_FP64; for GRLBM_PRECISION_FP32 with fixed
  * streaming nx * dp * 4, each node holding dp = (nDir + 4 rounded up to a
- * multiple of 4) floats (its directions, then directions 0..3 again). */
+ * multiple of 4) floats (its directions, then directions 0..3 again); for
+ * GRLBM_FAST_FP64 nx * dp * 8 with dp = nDir + 4 rounded up to a multiple of
+ * 2 doubles. */
 int grlbm_row_bytes(const grlbm_ctx *ctx, int64_t *bytes);
 /* Copies node rows [j_first, j_first + n) of the current intensity state
  * (every direction) to (to_buffer = 1) or from (to_buffer = 0) a contiguous
  * device buffer, n * row_bytes bytes, laid out [direction][row][i] for
- * GRLBM_PLAIN_FP64 and [row][i][direction] for GRLBM_PRECISION_FP32.
+ * GRLBM_PLAIN_FP64 and [row][i][direction] for GRLBM_PRECISION_FP32 and
+ * GRLBM_FAST_FP64.
  * Enqueued on the context's stream; returns before it completes. */
 int grlbm_copy_rows(grlbm_ctx *ctx, int64_t j_first, int64_t n, void *buffer, int32_t to_buffer);
-/* ---- tiles of the precision step --------------------------------------------
- * No counterpart in the reference.  The GRLBM_PRECISION_FP32 step of the
- * fixed streaming types runs as warps that each take tiles of tile_x x
+/* ---- tiles of the tiled steps -----------------------------------------------
+ * No counterpart in the reference.  The GRLBM_PRECISION_FP32 and
+ * GRLBM_FAST_FP64 steps of the fixed streaming types run as warps that each take tiles of tile_x x
  * tile_y cells (at most 16), staging each tile's (tile_x + 2) x (tile_y + 2)
  * node patch of the state in shared memory.  The default tile is the first
  * of 4x4, 8x2, 4x2, 2x2, 2x1, 1x1 whose buffers leave room for two blocks

@@ -113,15 +113,21 @@ void set_up(R &radiation, const Case &c, Grid &grid, Metric &metric, Stencil &st
         }
 }
 
+// name, max |a - b|, max |a|; then where the largest difference is
 void compare(const char *name, const DoubleBuffer &a, const DoubleBuffer &b)
 {
     double diff = 0, mag = 0;
+    size_t at = 0;
     for (size_t k = 0; k < a.size(); k++)
     {
-        diff = std::max(diff, std::fabs(a[k] - b[k]));
+        if (std::fabs(a[k] - b[k]) > diff)
+            diff = std::fabs(a[k] - b[k]), at = k;
         mag = std::max(mag, std::fabs(a[k]));
     }
     std::printf("%s %.17g %.17g\n", name, diff, mag);
+    if (diff > 0)
+        std::fprintf(stderr, "  %s: largest difference at element %zu of %zu: %.17g vs %.17g\n", name, at, a.size(),
+                     a[at], b[at]);
 }
 
 int run_nogpu()

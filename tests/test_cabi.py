@@ -63,7 +63,18 @@ def test_create_rejects_bad_arguments(grlbm, W, over, code):
     assert msg
 
 
-@pytest.mark.parametrize("precision", [0, 1])
+def test_fast_fp64_form_takes_fixed_streaming_only(grlbm, W):
+    """GRLBM_FAST_FP64 is refused (unsupported, before any device call) for
+    the adaptive streaming types, and for states of 2^31 values or more."""
+    case = W.curved_shell(nx_=8, ny_=8, n_dir=8, steps=1)
+    for st in (1, 3):
+        rc, msg = _create(grlbm, case, precision=2, streaming_type=st)
+        assert rc == 4 and "fixed streaming" in msg, msg
+    rc, msg = _create(grlbm, case, precision=2, nx_=6000, ny_=6000, n_dir=64)
+    assert rc == 1 and "2^31" in msg, msg
+
+
+@pytest.mark.parametrize("precision", [0, 1, 2])
 def test_direction_limit(grlbm, W, precision):
     rc, msg = _create(grlbm, W.curved_shell(nx_=8, ny_=8, n_dir=257, steps=1), precision=precision)
     assert rc == 1 and "n_dir" in msg

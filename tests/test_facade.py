@@ -77,19 +77,20 @@ def test_facade_matches_reference_radiation(tmp_path, kind):
     work.mkdir()
     out = subprocess.run([exe, kind, str(work)], capture_output=True, text=True, timeout=600)
     assert out.returncode == 0, out.stdout + out.stderr
+    detail = out.stdout + out.stderr
     rows = {}
     for ln in out.stdout.splitlines():
         parts = ln.split()
         if len(parts) == 3 and parts[0] != "total":
             rows[parts[0]] = (float(parts[1]), float(parts[2]))
+    assert rows["timeSteps"][0] == rows["timeSteps"][1] > 0, detail
     for name in ("I", "E", "Fx", "Fy", "Pxx", "E_LF", "F_LF", "coefficientsS", "coefficientsX"):
         diff, mag = rows[name]
         assert mag > 0, name
-        assert diff <= 1e-12 * mag, (name, diff, mag)
+        assert diff <= 1e-12 * mag, detail
     assert rows["maxItterationCount"][0] == rows["maxItterationCount"][1]
     a, b = rows["averageItterationCount"]
     assert abs(a - b) <= 1e-12 * abs(a)
-    assert rows["timeSteps"][0] == rows["timeSteps"][1] > 0
     ref = read_frames(tmp_path / "output" / "ref" / "Moments")
     ours = read_frames(tmp_path / "output" / "b200" / "Moments")
     assert len(ref) >= 3 and sorted(ref) == sorted(ours)

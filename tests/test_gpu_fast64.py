@@ -1,0 +1,137 @@
+"""The fast FP64 form (GRLBM_FAST_FP64): the FP64 step on a compact
+cell-major state with contracted multiply-adds and the lambda iteration run
+on the six moments.  Its contract is the plain form's third one -- relative
+L2 <= 1e-12 on E and F against the reference wherever the reference's
+iteration count is not decided by rounding noise -- and, unlike the plain
+form, not bit identity.  Without scattering (kappa0 = kappa1 = 0) the first
+cycle's intensities are final, so every such problem is stable: flat beams,
+emitting and absorbing shells, moving absorbers.  With scattering the two
+arithmetics may stop a cell's iteration at different cycles; the result then
+agrees to the iteration's own tolerance (1e-4, src/Radiation.h:16)."""
+import numpy as np
+import pytest
+from conftest import rel_l2
+from test_gpu_parity import STABLE, golden_ref, run_with_tables
+
+pytestmark = pytest.mark.gpu
+FAST = 2
+TOL = 1e-12
+
+
+def check(res, ref, keys=("E", "Fx", "Fy", "I"), tol=TOL):
+    for k in keys:
+        err = rel_l2(res[k], ref[k])
+        assert err <= tol, f"{k}: rel L2 {err:.3e} > {tol:g}"
+
+
+@pytest.mark.parametrize("name", STABLE)
+def test_stable_golden_cases_from_reference_tables(name, grlbm, cases, golden):
+    """Every stable golden case, stepped from the reference's own tables:
+    moments, lab-frame moments and intensities within 1e-12 of the
+    reference's IEEE build."""
+    ref = golden_ref(golden, name)
+    res = run_with_tables(grlbm, cases[name], ref, precision=FAST)
+    check(res, ref, ("E", "Fx", "Fy", "Pxx", "Pxy", "Pyy", "E_LF", "F_LF", "I"))
+
+
+def test_config1_flat_beam_full_size(grlbm, W, oracle):
+    """The flat beam at its stated size: 100^2 cells, 20 directions, 500
+    steps, sources kept active; the flat departures are the reference's bit
+    for bit."""
+    case = W.flat_beam()
+    ref = oracle.run(case, "oracle")
+    res = grlbm.run(case, FAST)
+    check(res, ref)
+
+
+def test_config2_curved_shell_full_size(grlbm, W, oracle):
+    """The emitting, absorbing shell at its grid size (200^2 cells, 32
+    directions, Fourier order 5), end to end with the GPU's own tables."""
+    case = W.curved_shell(steps=100)
+    ref = oracle.run(case, "oracle")
+    res = grlbm.run(case, FAST)
+    check(res, ref)
+
+
+def test_moving_absorber(grlbm, W, oracle):
+    """Moving fluid with emission and absorption, von Mises moment sources
+    kept active, Kerr-Schild: every term of the collide except scattering."""
+    case = W.moving_scatter(nx_=60, ny_=52, n_dir=24, n_fourier=5, steps=30)
+    case["fields"]["kappa0"][:] = 0.0
+    case["fields"]["kappa1"][:] = 0.0
+    ref = oracle.run(case, "oracle")
+    res = grlbm.run(case, FAST)
+    check(res, ref)
+
+
+@pytest.mark.parametrize("maker,kw", [
+    ("curved_shell", dict(nx_=37, ny_=23, n_dir=12, n_fourier=5, steps=20)),   # ragged tiles
+    ("flat_beam", dict(nx_=2, ny_=2, n_dir=8, steps=3)),                        # smallest grid
+    ("curved_shell", dict(nx_=33, ny_=24, n_dir=5, n_fourier=5, steps=10)),    # odd direction count
+    ("curved_shell", dict(nx_=40, ny_=36, n_dir=200, n_fourier=7, steps=5)),   # wide stencil
+    ("curved_shell", dict(nx_=21, ny_=21, n_dir=64, n_fourier=32, steps=8)),   # many harmonics
+])
+def test_edge_shapes(maker, kw, grlbm, W, oracle):
+    case = W.make_case(maker, **kw)
+    ref = oracle.run(case, "oracle")
+    res = grlbm.run(case, FAST)
+    check(res, ref)
+
+
+@pytest.mark.parametrize("cfl", [1.5, 2.5])
+def test_far_departures(cfl, grlbm, W, oracle):
+    """Departures more than a cell away are gathered from global memory, with
+    the corners clamped to the grid as the plain form clamps them."""
+    case = W.make_case("curved_shell", nx_=48, ny_=48, n_dir=32, n_fourier=5, steps=12)
+    case["cfl"] = cfl
+    ref = grlbm.run(case, 0)
+    res = grlbm.run(case, FAST)
+    assert res["stats"]["far_departures"] > 0
+    check(res, ref)
+    flat = W.make_case("flat_beam", nx_=40, ny_=40, n_dir=16, steps=12)
+    flat["cfl"] = cfl
+    check(grlbm.run(flat, FAST), grlbm.run(flat, 0))
+
+
+def test_scattering_within_lambda_tolerance(grlbm, W, oracle):
+    """Scattering at rest: the cycle counts may differ from the reference's,
+    so E agrees to the iteration's tolerance, and F on the energy's scale."""
+    case = W.curved_scatter(nx_=64, ny_=64, n_dir=32, n_fourier=9, steps=20)
+    ref = oracle.run(case, "oracle")
+    res = grlbm.run(case, FAST)
+    assert rel_l2(res["E"], ref["E"]) <= 1e-4
+    scale = np.linalg.norm(ref["E"])
+    for k in ("Fx", "Fy"):
+        assert np.linalg.norm(res[k] - ref[k]) <= 1e-4 * scale, k
+    assert abs(res["average_iterations"] - ref["average_iterations"]) <= 0.05 * ref["average_iterations"]
+
+
+def test_tiles_and_chunks_do_not_change_the_result(grlbm, W):
+    """Every tile shape and every way of chunking the steps gives the same
+    bits: a cell's arithmetic does not depend on its tile."""
+    case = W.curved_scatter(nx_=45, ny_=38, n_dir=24, n_fourier=5, steps=33)
+    out = []
+    for shape in [(4, 4), (8, 2), (2, 8), (4, 2), (1, 1)]:
+        with grlbm.prepare(case, FAST) as r:
+            r.set_tile_shape(*shape)
+            r.step(33)
+            out.append((r.intensity(), r.moments_if()["E"]))
+    with grlbm.prepare(case, FAST) as r:
+        for _ in range(33):
+            r.step(1)
+        out.append((r.intensity(), r.moments_if()["E"]))
+    for I, E in out[1:]:
+        assert np.array_equal(I, out[0][0]) and np.array_equal(E, out[0][1])
+
+
+def test_config3_scale_against_plain_form(grlbm, W):
+    """The curved-scattering workload at full size (400^2 x 64, Fourier order
+    16), 200 steps: within the lambda iteration's tolerance of the plain
+    form (which is bit-identical to the oracle there)."""
+    case = W.curved_scatter(steps=200)
+    ref = grlbm.run(case, 0)
+    res = grlbm.run(case, FAST)
+    assert rel_l2(res["E"], ref["E"]) <= 1e-4
+    scale = np.linalg.norm(ref["E"])
+    for k in ("Fx", "Fy"):
+        assert np.linalg.norm(res[k] - ref[k]) <= 1e-4 * scale, k
