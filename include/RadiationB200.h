@@ -81,8 +81,9 @@ public:
     using Radiation::ux;
     using Radiation::uy;
 
-    // precision: GRLBM_PLAIN_FP64 (the reference's arithmetic) or
-    // GRLBM_PRECISION_FP32; device < 0 selects the current CUDA device.
+    // precision: GRLBM_PLAIN_FP64 (the reference's arithmetic),
+    // GRLBM_PRECISION_FP32 or GRLBM_FAST_FP64; device < 0 selects the current
+    // CUDA device.
     RadiationB200(Metric &metric, Stencil &stencil, Stencil &streamingStencil, Config config,
                   int precision = GRLBM_PLAIN_FP64, int device = -1)
         : Radiation(metric, stencil, streamingStencil, config)
@@ -93,9 +94,13 @@ public:
             throw std::runtime_error("RadiationB200: GeodesicFixed streaming is not supported");
         Grid &g = metric.grid;
         // Grid(nx_, ny_, start, end) keeps one halo cell on each side
-        // (src/Grid.cpp:13-22); the descriptor takes the caller's values.
-        const grlbm_grid_desc gd{(int64_t)g.nx - 2, (int64_t)g.ny - 2, g.startx + g.dx, g.starty + g.dy,
-                                 g.endx - g.dx, g.endy - g.dy, g.GetCFL()};
+        // (src/Grid.cpp:13-22); the descriptor takes the caller's values,
+        // recovered so that the library's grid is this one bit for bit.
+        double sx, ex, sy, ey;
+        if (!RecoverInterval(g.startx, g.endx, g.dx, (int64_t)g.nx - 2, sx, ex) ||
+            !RecoverInterval(g.starty, g.endy, g.dy, (int64_t)g.ny - 2, sy, ey))
+            throw std::runtime_error("RadiationB200: the grid's start and end cannot be recovered exactly");
+        const grlbm_grid_desc gd{(int64_t)g.nx - 2, (int64_t)g.ny - 2, sx, sy, ex, ey, g.GetCFL()};
         const grlbm_metric_desc md{MetricKind(metric), metric.m, metric.a, 0.0};
         const grlbm_run_desc rd{(int32_t)stencil.nDir,
                                 (int32_t)streamingStencil.nDir,
@@ -178,6 +183,9 @@ public:
             rc = grlbm_run_simulation(ctx_, config.t0, config.simTime, config.writePeriod,
                                       config.saveInitialData ? 1 : 0, config.writeData ? frames.c_str() : nullptr,
                                       &steps);
+            if (rc == GRLBM_OK && steps != logger.timeSteps)
+                throw std::runtime_error("RadiationB200: the library ran " + std::to_string(steps) +
+                                         " steps, the reference's loop " + std::to_string(logger.timeSteps));
         }
         catch (...)
         {
@@ -207,6 +215,30 @@ private:
     grlbm_ctx *ctx_ = nullptr;
 
     void Check(int rc) { Check(rc, ctx_); }
+    // The start and end a Grid was built from, given its startx = start - d,
+    // endx = end + d and d = (end - start) / (n_ - 1) (src/Grid.cpp:16-22):
+    // start = startx + d to within rounding, searched over a few ulps for
+    // the values that give back the grid's own startx, endx and d exactly.
+    static bool RecoverInterval(double lo, double hi, double d, int64_t n_, double &start, double &end)
+    {
+        auto nudge = [](double x, int k) {
+            for (int u = 0; u < (k < 0 ? -k : k); u++)
+                x = std::nextafter(x, k < 0 ? -INFINITY : INFINITY);
+            return x;
+        };
+        for (int i = -4; i <= 4; i++)
+            for (int k = -4; k <= 4; k++)
+            {
+                const double s = nudge(lo + d, i), e = nudge(hi - d, k);
+                const double dd = (e - s) / ((double)(n_ + 2) - 1.0 - 2.0);
+                if (dd == d && s - dd == lo && e + dd == hi)
+                {
+                    start = s, end = e;
+                    return true;
+                }
+            }
+        return false;
+    }
     static void Check(int rc, grlbm_ctx *c)
     {
         if (rc != GRLBM_OK)
