@@ -74,7 +74,7 @@ def args_parse():
     p.add_argument("--batch-steps", type=int, default=64,
                    help="timed steps of the batched form (64 uneven problems); 0 skips it")
     p.add_argument("--profile", default=None,
-                   choices=["fp32", "fp64", "fp32-adaptive", "fp64-adaptive", "batch", "adjoint"],
+                   choices=["fp32", "fp64", "fast64", "fp32-adaptive", "fp64-adaptive", "batch", "adjoint"],
                    help="instead of measuring: build one problem and run --profile-steps steps of it, one call "
                         "per step, for a profiler to capture (no timing, no JSON line)")
     p.add_argument("--profile-steps", type=int, default=6)
@@ -234,16 +234,18 @@ def open_form(G, case, prec, world, rank, local, pg):
 def run_configs(G, W, local):
     """The two smaller configurations at their full sizes -- the flat beam
     (100^2 x 20, 500 steps) and the curved shell (200^2 x 32, 1000 steps) --
-    and the bench workload with adaptive streaming (50 steps), in both forms,
-    with the FP32 form's relative error of E.  Device time of the whole run
+    in the three forms, and the bench workload with adaptive streaming (50
+    steps) in the plain and precision forms, with each form's relative error
+    of E against the plain form.  Device time of the whole run
     with CUDA events (graph-replayed steps, inputs resident, no L2 flush
     between steps)."""
     import torch
     out = {}
     for name, case, forms in (
-            ("flat_beam 100x100 x 20 directions, 500 steps", W.flat_beam(), (G.PLAIN_FP64, G.PRECISION_FP32)),
+            ("flat_beam 100x100 x 20 directions, 500 steps", W.flat_beam(),
+             (G.PLAIN_FP64, G.PRECISION_FP32, G.FAST_FP64)),
             ("curved_shell 200x200 x 32 directions, Fourier order 5, 1000 steps", W.curved_shell(),
-             (G.PLAIN_FP64, G.PRECISION_FP32)),
+             (G.PLAIN_FP64, G.PRECISION_FP32, G.FAST_FP64)),
             ("curved_scatter adaptive (CurvedAdaptive) 400x400 x 64 directions, Fourier order 16, 50 steps",
              dict(W.curved_scatter(steps=50), streaming_type=W.CURVED_ADAPTIVE), (G.PLAIN_FP64, G.PRECISION_FP32))):
         n = int(case["n_steps"])
@@ -258,12 +260,14 @@ def run_configs(G, W, local):
                     r.step_async(n)
                     e1.record(ext)
                     ext.synchronize()
-                key = "fp64" if prec == G.PLAIN_FP64 else "fp32"
+                key = {G.PLAIN_FP64: "fp64", G.PRECISION_FP32: "fp32", G.FAST_FP64: "fast64"}[prec]
                 res[key] = units / (e0.elapsed_time(e1) / 1e3)
                 E[key] = r.moments_if()["E"]
         entry = {"cell_dir_per_s": res}
         if "fp32" in E:
             entry["E_rel_l2_fp32_vs_fp64"] = float(np.linalg.norm(E["fp32"] - E["fp64"]) / np.linalg.norm(E["fp64"]))
+        if "fast64" in E:
+            entry["E_rel_l2_fast64_vs_fp64"] = float(np.linalg.norm(E["fast64"] - E["fp64"]) / np.linalg.norm(E["fp64"]))
         out[name] = entry
     return out
 
@@ -396,7 +400,8 @@ def run_profile(a):
     case = W.make_case(a.profile_workload, **kw)
     if a.profile.endswith("adaptive"):
         case["streaming_type"] = W.FLAT_ADAPTIVE if case["streaming_type"] == W.FLAT_FIXED else W.CURVED_ADAPTIVE
-    with G.prepare(case, G.PRECISION_FP32 if a.profile.startswith("fp32") else G.PLAIN_FP64) as r:
+    prec = G.PRECISION_FP32 if a.profile.startswith("fp32") else (G.FAST_FP64 if a.profile == "fast64" else G.PLAIN_FP64)
+    with G.prepare(case, prec) as r:
         for _ in range(n):
             r.step(1)
         print("profile:", a.profile, a.profile_workload, a.nx, a.dirs, "E sum", float(r.moments_if()["E"].sum()))
@@ -456,7 +461,7 @@ def run_grlbm(a, world, rank, local, pg):
     with Clocks(local) as clk:
         forms = {}
         states = {}
-        for name, prec in (("fp32", G.PRECISION_FP32), ("fp64", G.PLAIN_FP64)):
+        for name, prec in (("fp32", G.PRECISION_FP32), ("fp64", G.PLAIN_FP64), ("fast64", G.FAST_FP64)):
             r, advance, slab = open_form(G, case, prec, world, rank, local, pg)
             st = r.stats()
             barrier(pg, dev)
@@ -471,24 +476,27 @@ def run_grlbm(a, world, rank, local, pg):
         # moments after the whole run give the metric's accuracy condition
         e2e = {}
         if a.e2e_reps > 0:
-            for name, prec in (("fp32", G.PRECISION_FP32), ("fp64", G.PLAIN_FP64)):
+            for name, prec in (("fp32", G.PRECISION_FP32), ("fp64", G.PLAIN_FP64), ("fast64", G.FAST_FP64)):
                 e2e[name] = run_e2e(G, W, case, prec, a, world, rank, local, pg, dev)
         batched = run_batched(G, W, a, local) if a.batch_steps > 0 and world == 1 else None
         other = run_configs(G, W, local) if not a.no_configs and world == 1 else None
         adjoint = run_adjoint(G, W, a, local) if a.adjoint_steps > 0 and world == 1 else None
     clocks = clk.summary()
 
-    fp32, fp64 = forms["fp32"], forms["fp64"]
+    fp32, fp64, fast = forms["fp32"], forms["fp64"], forms["fast64"]
     value = world * units * a.steps / (fp32["total_ms"] / 1e3)
     plain = world * units * a.steps / (fp64["total_ms"] / 1e3)
+    fast_value = world * units * a.steps / (fast["total_ms"] / 1e3)
     # algorithmic bytes per cell*direction: I read + written, 4 inputs and 6
     # moments per cell shared by the directions
     b32 = 2 * 4 + (4 + 6) * 4 / nd
     b64 = 2 * 8 + (4 + 6) * 8 / nd
     avg32 = statistics.mean(fp32["ms"]) / 1e3
     avg64 = statistics.mean(fp64["ms"]) / 1e3
+    avgf = statistics.mean(fast["ms"]) / 1e3
     ach32 = b32 * units / avg32 / 1e9
     ach64 = b64 * units / avg64 / 1e9
+    achf = b64 * units / avgf / 1e9
     rel = lambda x, y: float(np.linalg.norm(x - y) / max(np.linalg.norm(y), 1e-300))
     if "fp32" in e2e and "fp64" in e2e:
         m32, m64 = e2e["fp32"][1], e2e["fp64"][1]
@@ -499,6 +507,17 @@ def run_grlbm(a, world, rank, local, pg):
     else:
         accuracy = {k + "_rel_l2_fp32_vs_fp64": rel(states["fp32"][k], states["fp64"][k]) for k in ("E", "Fx", "Fy")}
         accuracy["after_steps"] = a.warmup + a.steps
+    # the fast FP64 form against the plain form (bit-identical to the oracle
+    # at this size) on the same runs
+    if "fast64" in e2e and "fp64" in e2e:
+        mf, m64 = e2e["fast64"][1], e2e["fp64"][1]
+        fast_accuracy = {k + "_rel_l2_fast64_vs_fp64": max_over_ranks(rel(mf[k], m64[k]), pg, dev)
+                         for k in ("E", "Fx", "Fy")}
+        fast_accuracy.update({"after_steps": a.e2e_steps, "lambda_iterations_avg": e2e["fast64"][2]})
+    else:
+        fast_accuracy = {k + "_rel_l2_fast64_vs_fp64": rel(states["fast64"][k], states["fp64"][k])
+                         for k in ("E", "Fx", "Fy")}
+        fast_accuracy["after_steps"] = a.warmup + a.steps
 
     def e2e_line(name):
         if name not in e2e:
@@ -551,6 +570,19 @@ def run_grlbm(a, world, rank, local, pg):
             "traffic": profiled_traffic("plain_step"),
             "kernels": "k_stream_plain + k_collide_plain (fixed streaming; traffic per step, both kernels)",
         },
+        "fast_fp64": {
+            "value": fast_value,
+            "ms_per_step": fast["total_ms"] / a.steps,
+            "roofline_frac": achf / peak,
+            "achieved_gbs": achf,
+            "algorithmic_bytes_per_update": b64,
+            "traffic": profiled_traffic("k_step_fast64"),
+            "kernel": "k_step_fast64<curved> (FP64, contracted FMAs, 32-byte packed records; matches the "
+                      "reference to 1e-12 where the lambda iteration's cycle count is not set by rounding noise)",
+            "accuracy": fast_accuracy,
+            "e2e": e2e_line("fast64"),
+            "fast_vs_plain": fast_value / plain,
+        },
         "precision_vs_plain": value / plain,
         # as if the step time scaled with the lambda iterations each form ran
         # (the FP32 form's moment-space iterations cost O(1) per cell, so this
@@ -558,9 +590,10 @@ def run_grlbm(a, world, rank, local, pg):
         "precision_vs_plain_iteration_normalised": value / plain * fp32["iters"]["average_iterations"]
         / max(fp64["iters"]["average_iterations"], 1e-30),
         "accuracy": accuracy,
-        "table_build_ms": {"fp32": fp32["table_ms"], "fp64": fp64["table_ms"]},
+        "table_build_ms": {"fp32": fp32["table_ms"], "fp64": fp64["table_ms"], "fast64": fast["table_ms"]},
         "lambda_iterations": {"fp32_avg": fp32["iters"]["average_iterations"],
                               "fp64_avg": fp64["iters"]["average_iterations"],
+                              "fast64_avg": fast["iters"]["average_iterations"],
                               "max": fp64["iters"]["max_iterations"]},
         "e2e": e2e_line("fp32"),
         "plain_fp64_e2e": e2e_line("fp64"),
