@@ -424,6 +424,7 @@ struct Batch32Item
     Step32Args a[2]; // a[k]: the step that reads intensity buffer k
     const DirTable *dt;
     int curved, cur0;
+    int mode; // step32_mode(nd): 0 half-warp mode, else the passes per lane
 };
 
 int64_t adj_entries_per_source(bool curved);
@@ -472,7 +473,10 @@ int step32_warp_stride(int tx, int ty, int dp, int nd);
 size_t step32_smem(int tx, int ty, int dp, int nd);
 size_t step32_batch_smem(int warp_stride);
 cudaError_t prepare_step32();
-cudaError_t step32_occupancy(int P, bool curved, bool batch, size_t smem, int *blocks);
+cudaError_t step32_occupancy(int P, bool curved, bool batch, size_t smem, int *blocks, int nd);
+// The step's mode for nd directions: 0 for half-warp mode (at most 16
+// directions: phases 1 and 3 take two cells at a time), else its passes.
+int step32_mode(int nd);
 // blocks: the persistent grid (resident blocks per SM times the SMs)
 void launch_step32(const Step32Args &a, const DirTable &dt, bool curved, int P, int blocks, cudaStream_t s);
 void launch_step_batch32(const Batch32Item *items, const int *first_tile, int n_items, int total_tiles, int flip,

@@ -382,7 +382,7 @@ int tiled_fit(grlbm_ctx *ctx, int tx, int ty, size_t *smem, int *per_sm)
     if (ctx->fast64)
         CU(step64_occupancy(ctx->passes, curved, *smem, per_sm));
     else
-        CU(step32_occupancy(ctx->passes, curved, false, *smem, per_sm));
+        CU(step32_occupancy(ctx->passes, curved, false, *smem, per_sm, ctx->st.n));
     return GRLBM_OK;
 }
 
@@ -2133,7 +2133,7 @@ int batch_geometry(grlbm_batch *b)
     b->smem = step32_batch_smem(b->warp_stride);
     if (b->smem > (size_t)kStep32MaxSmem)
         return bfail(b, GRLBM_ERR_ARGUMENT, "the batch's largest patch needs %zu bytes of shared memory", b->smem);
-    BCU(step32_occupancy(b->passes, true, true, b->smem, &b->blocks_per_sm_max));
+    BCU(step32_occupancy(b->passes, true, true, b->smem, &b->blocks_per_sm_max, 0));
     if (b->blocks_per_sm_max < 1)
         return bfail(b, GRLBM_ERR_CUDA, "the batched kernel does not fit on an SM");
     if (b->blocks_per_sm > b->blocks_per_sm_max)
@@ -2170,6 +2170,7 @@ int batch_build(grlbm_batch *b)
         it.dt = dirs + order[k];
         it.curved = c->run.streaming_type == GRLBM_CURVED_FIXED;
         it.cur0 = c->cur;
+        it.mode = step32_mode(c->st.n);
         first[k + 1] = first[k] + step32_tiles(c);
     }
     b->total_tiles = first[n];

@@ -46,6 +46,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <type_traits>
 
 #include "device_common.cuh"
 #include "step_common.cuh"
@@ -142,25 +143,34 @@ __device__ __forceinline__ float window5(const float *p, float w0, float w1, flo
     return fmaxf(fmaf(w4, p[4], fmaf(w3, p[3], fmaf(w2, p[2], fmaf(w1, p[1], w0 * p[0])))), 0.f);
 }
 
-// A lane's per-direction constants of flat streaming for its P passes: the
-// departure's corner offset in the patch, its fractions and whether it lies
-// within the 3x3 neighbourhood (else the far gather).
-template <int P>
+// The direction of a lane's first pass: the lane, or in half-warp mode (H:
+// at most 16 directions, the two half-warps on two cells) the lane within its
+// half-warp.
+template <bool H>
+__device__ __forceinline__ int lane_dir()
+{
+    return H ? (int)(threadIdx.x & 15) : (int)(threadIdx.x & 31);
+}
+
+// A lane's per-direction constants of flat streaming for its P passes (of PM
+// stored): the departure's corner offset in the patch, its fractions and
+// whether it lies within the 3x3 neighbourhood (else the far gather).
+template <int PM>
 struct LaneFlat
 {
-    float ox[P], oy[P], fx[P], fy[P];
-    int off[P];
-    bool near[P];
+    float ox[PM], oy[PM], fx[PM], fy[PM];
+    int off[PM];
+    bool near[PM];
 };
 
-template <int P>
-__device__ __forceinline__ void load_lane_flat(LaneFlat<P> &L, const DirTable &dt, int nd, int dps, int px)
+template <int P, bool H, int PM>
+__device__ __forceinline__ void load_lane_flat(LaneFlat<PM> &L, const DirTable &dt, int nd, int dps, int px)
 {
-    const int lane = threadIdx.x & 31;
+    const int dl = lane_dir<H>();
 #pragma unroll
     for (int p = 0; p < P; p++)
     {
-        const int dd = min(lane + 32 * p, nd - 1);
+        const int dd = min(dl + 32 * p, nd - 1);
         const float ox = dt.ox[dd], oy = dt.oy[dd];
         const float fli = floorf(ox), flj = floorf(oy);
         L.ox[p] = ox;
@@ -173,14 +183,14 @@ __device__ __forceinline__ void load_lane_flat(LaneFlat<P> &L, const DirTable &d
 }
 
 // A lane's rotated directions (n1, n2) for its P passes (phase 3's map).
-template <int P>
-__device__ __forceinline__ void load_lane_dirs(float2 (&LN)[P], const float4 *dirc, int nd)
+template <int P, bool H, int PM>
+__device__ __forceinline__ void load_lane_dirs(float2 (&LN)[PM], const float4 *dirc, int nd)
 {
-    const int lane = threadIdx.x & 31;
+    const int dl = lane_dir<H>();
 #pragma unroll
     for (int p = 0; p < P; p++)
     {
-        const float4 c1 = dirc[2 * min(lane + 32 * p, nd - 1) + 1];
+        const float4 c1 = dirc[2 * min(dl + 32 * p, nd - 1) + 1];
         LN[p] = make_float2(c1.z, c1.w);
     }
 }
@@ -201,20 +211,21 @@ __device__ __forceinline__ void stage_tile(const Step32Args &a, int tile, float 
 
 // A tile's cells as phase 1 and phase 2 need them: lane c (< 16, and its
 // partner c + 16) holds cell c's node index, interior cell index, patch
-// offset, flags and fields; and every lane its directions' records of cell
-// 0.  Loaded for the next tile while the current one is finished, so that
-// none of these loads stalls the streaming.
-template <int P>
+// offset, flags and fields; and every lane its directions' records of its
+// first cell (cell 0, or in half-warp mode cell 0 or 1 by half-warp).
+// Loaded for the next tile while the current one is finished, so that none
+// of these loads stalls the streaming.  rec0 has room for PM passes.
+template <int PM>
 struct UnitCells
 {
     int x0, y0, txv, ncells;
     int cij, ccell, cpo, cfl;
     float u1, u2, lor, adt, eta, k0, k3, kak0, scale;
-    uint4 rec0[P];
+    uint4 rec0[PM];
 };
 
-template <bool CURVED, int P>
-__device__ __forceinline__ void load_unit(const Step32Args &a, int tile, UnitCells<P> &U)
+template <bool CURVED, int P, bool H, int PM>
+__device__ __forceinline__ void load_unit(const Step32Args &a, int tile, UnitCells<PM> &U)
 {
     const int lane = threadIdx.x & 31;
     const int tx = a.tx, px = tx + 2, nd = a.nd;
@@ -237,21 +248,25 @@ __device__ __forceinline__ void load_unit(const Step32Args &a, int tile, UnitCel
     U.scale = CURVED ? __ldg(a.ia3 + U.cij) : 1.f;
     if (CURVED)
     {
-        const int cell0 = __shfl_sync(0xffffffffu, U.ccell, 0);
+        constexpr int kStep = H ? 2 : 1;
+        const int dl = lane_dir<H>(), hk = H ? (lane >> 4) : 0;
+        const int cell0 = __shfl_sync(0xffffffffu, U.ccell, hk);
 #pragma unroll
         for (int p = 0; p < P; p++)
         {
-            const int d = lane + 32 * p;
-            U.rec0[p] = d < nd ? __ldcs(a.rec + (unsigned)cell0 * (unsigned)nd + (unsigned)d) : make_uint4(0u, 0u, 0u, 0u);
+            const int d = dl + 32 * p;
+            U.rec0[p] = d < nd && hk < U.ncells ? __ldcs(a.rec + (unsigned)cell0 * (unsigned)nd + (unsigned)d)
+                                                : make_uint4(0u, 0u, 0u, 0u);
         }
 #pragma unroll
-        for (int k = 1; k < 4; k++)
+        for (int m = 1; m < 4; m++)
         {
-            const int cell = __shfl_sync(0xffffffffu, U.ccell, k);
+            const int k = m * kStep + hk;
+            const int cell = __shfl_sync(0xffffffffu, U.ccell, k & 15);
 #pragma unroll
             for (int p = 0; p < P; p++)
             {
-                const int d = lane + 32 * p;
+                const int d = dl + 32 * p;
                 if (k < U.ncells && d < nd)
                     asm volatile("prefetch.global.L2 [%0];" ::"l"(a.rec + (unsigned)cell * (unsigned)nd + (unsigned)d));
             }
@@ -265,14 +280,19 @@ __device__ __forceinline__ void load_unit(const Step32Args &a, int tile, UnitCel
 // next tile into the patch buffer); phase 2 takes the moments and collides
 // with two lanes per cell (lane = cell + 16 h, h the parity of the
 // directions it sums), writing the collided values back into S; phase 3
-// stores the cells' new state, coalesced along the directions.
-template <bool CURVED, int P, class Next>
+// stores the cells' new state, coalesced along the directions.  In
+// half-warp mode (H, at most 16 directions) phases 1 and 3 take two cells at
+// a time, one per half-warp.  P passes of the PM the lane arrays hold.
+template <bool CURVED, int P, bool H, int PM, class Next>
 __device__ __forceinline__ void step_unit32(const Step32Args &a, const DirTable &dt, const float *rowtab,
-                                            const float4 *dirc, const LaneFlat<P> &LF, const float2 (&LN)[P],
-                                            const UnitCells<P> &U, const float *patch, float *S, step::IterStats &st,
-                                            Next next)
+                                            const float4 *dirc, const LaneFlat<PM> &LF, const float2 (&LN)[PM],
+                                            const UnitCells<PM> &U, const float *patch, float *S,
+                                            step::IterStats &st, Next next)
 {
+    static_assert(!H || P == 1, "half-warp mode streams at most 16 directions");
+    constexpr int kStep = H ? 2 : 1; // cells per iteration of phases 1 and 3
     const int lane = threadIdx.x & 31;
+    const int dl = lane_dir<H>(), hk = H ? (lane >> 4) : 0;
     const int tx = a.tx, px = tx + 2, dp = a.dp, dps = a.dps, nd = a.nd, ss = a.ss;
     (void)tx;
     const int nxn = (int)a.g.nx, nx_ = (int)a.g.nx_;
@@ -286,15 +306,16 @@ __device__ __forceinline__ void step_unit32(const Step32Args &a, const DirTable 
     const float scale = U.scale;
 
     // ---- phase 1: stream every cell, lanes over the directions ----
-    // The cell loop reads the cells' tables from lanes 0..15 by shuffle.
-    // Cell k's records are loaded while cell k - 1 streams, and cell k + 3's
-    // are prefetched into L2 (cell 0's came with the tile's tables).
-    uint4 rc[P], rn[P];
-    auto load_recs = [&](uint4(&r)[P], int cell) {
+    // The cell loop reads the cells' tables from lanes 0..15 by shuffle.  A
+    // lane's next cell's records are loaded while its current cell streams,
+    // and those three cells on are prefetched into L2 (the first cell's came
+    // with the tile's tables).
+    uint4 rc[PM], rn[PM];
+    auto load_recs = [&](uint4(&r)[PM], int cell) {
 #pragma unroll
         for (int p = 0; p < P; p++)
         {
-            const int d = lane + 32 * p;
+            const int d = dl + 32 * p;
             r[p] = d < nd ? __ldcs(a.rec + (unsigned)cell * (unsigned)nd + (unsigned)d) : make_uint4(0u, 0u, 0u, 0u);
         }
     };
@@ -302,7 +323,7 @@ __device__ __forceinline__ void step_unit32(const Step32Args &a, const DirTable 
 #pragma unroll
         for (int p = 0; p < P; p++)
         {
-            const int d = lane + 32 * p;
+            const int d = dl + 32 * p;
             if (d < nd)
                 asm volatile("prefetch.global.L2 [%0];" ::"l"(a.rec + (unsigned)cell * (unsigned)nd + (unsigned)d));
         }
@@ -313,28 +334,30 @@ __device__ __forceinline__ void step_unit32(const Step32Args &a, const DirTable 
         for (int p = 0; p < P; p++)
             rc[p] = U.rec0[p];
     }
-    for (int k = 0; k < ncells; k++)
+    for (int k0_ = 0; k0_ < ncells; k0_ += kStep)
     {
-        const int cell1 = __shfl_sync(0xffffffffu, ccell, (k + 1) & 15);
-        const int cell4 = __shfl_sync(0xffffffffu, ccell, (k + 4) & 15);
-        const int ijk = __shfl_sync(0xffffffffu, cij, k);
-        const int pok = __shfl_sync(0xffffffffu, cpo, k);
-        const int flk = __shfl_sync(0xffffffffu, cfl, k);
+        const int k = k0_ + hk; // this lane's cell
+        const bool kact = k < ncells;
+        const int cell1 = __shfl_sync(0xffffffffu, ccell, (k + kStep) & 15);
+        const int cell4 = __shfl_sync(0xffffffffu, ccell, (k + 4 * kStep) & 15);
+        const int ijk = __shfl_sync(0xffffffffu, cij, k & 15);
+        const int pok = __shfl_sync(0xffffffffu, cpo, k & 15);
+        const int flk = __shfl_sync(0xffffffffu, cfl, k & 15);
         if (CURVED)
         {
-            if (k + 1 < ncells)
+            if (k + kStep < ncells)
                 load_recs(rn, cell1);
-            if (k + 4 < ncells)
+            if (k + 4 * kStep < ncells)
                 prefetch_recs(cell4);
         }
         const float *cellp = patch + pok; // node (i - 1, j - 1) of cell k
         float *Sk = S + k * ss;
-        float v[P];
-        bool far[P];
+        float v[PM];
+        bool far[PM];
 #pragma unroll
         for (int p = 0; p < P; p++)
             v[p] = 0.f, far[p] = false;
-        if (!(CURVED && (flk & 2))) // a cell inside the excision streams zeros
+        if (kact && !(CURVED && (flk & 2))) // a cell inside the excision streams zeros
         {
             // every lane gathers (a direction past the last has a zero record: its
             // window reads valid patch nodes and is scaled by 0)
@@ -374,31 +397,31 @@ __device__ __forceinline__ void step_unit32(const Step32Args &a, const DirTable 
                     v[p] = fmaf(LF.fy[p], f1 - f0, f0);
                 }
             }
-            // departures outside the 3x3 neighbourhood (rare): from global memory
-            bool any = false;
+        }
+        // departures outside the 3x3 neighbourhood (rare): from global memory
+        bool any = false;
+#pragma unroll
+        for (int p = 0; p < P; p++)
+            any |= far[p];
+        if (__any_sync(0xffffffffu, any))
+        {
+            const int i = ijk % nxn, j = ijk / nxn;
+            const int cell = (i - 1) + (j - 1) * nx_;
 #pragma unroll
             for (int p = 0; p < P; p++)
-                any |= far[p];
-            if (__any_sync(0xffffffffu, any))
             {
-                const int i = ijk % nxn, j = ijk / nxn;
-                const int cell = (i - 1) + (j - 1) * nx_;
-#pragma unroll
-                for (int p = 0; p < P; p++)
-                {
-                    const int d = lane + 32 * p;
-                    if (far[p] && d < nd)
-                        v[p] = CURVED ? stream_far32(a.Iin, __ldg(a.side + (unsigned)cell * (unsigned)nd + (unsigned)d),
-                                                     dp, nxn, (int)a.g.ny, nd, a.ng, rowtab, dt.q, dt.p, dt.inv_q, i, j)
-                                      : stream_flat_far32(a.Iin, LF.ox[p], LF.oy[p], dp, nxn, (int)a.g.ny, d, i, j);
-                }
+                const int d = dl + 32 * p;
+                if (far[p] && d < nd)
+                    v[p] = CURVED ? stream_far32(a.Iin, __ldg(a.side + (unsigned)cell * (unsigned)nd + (unsigned)d),
+                                                 dp, nxn, (int)a.g.ny, nd, a.ng, rowtab, dt.q, dt.p, dt.inv_q, i, j)
+                                  : stream_flat_far32(a.Iin, LF.ox[p], LF.oy[p], dp, nxn, (int)a.g.ny, d, i, j);
             }
         }
 #pragma unroll
         for (int p = 0; p < P; p++)
         {
-            const int d = lane + 32 * p;
-            if (d < nd)
+            const int d = dl + 32 * p;
+            if (kact && d < nd)
                 Sk[d] = v[p];
         }
         if (CURVED)
@@ -586,26 +609,28 @@ __device__ __forceinline__ void step_unit32(const Step32Args &a, const DirTable 
 
     // ---- phase 3: the cells' new state, coalesced along the directions
     // (and the mirrored directions 0..3 after the last one) ----
-    for (int k = 0; k < ncells; k++)
+    for (int k0_ = 0; k0_ < ncells; k0_ += kStep)
     {
-        const int ij = __shfl_sync(0xffffffffu, cij, k);
-        const float g = __shfl_sync(0xffffffffu, og, k), ca = __shfl_sync(0xffffffffu, oa, k);
-        const float cb1 = __shfl_sync(0xffffffffu, ob1, k), cb2 = __shfl_sync(0xffffffffu, ob2, k);
+        const int k = k0_ + hk;
+        const bool kact = k < ncells;
+        const int ij = __shfl_sync(0xffffffffu, cij, k & 15);
+        const float g = __shfl_sync(0xffffffffu, og, k & 15), ca = __shfl_sync(0xffffffffu, oa, k & 15);
+        const float cb1 = __shfl_sync(0xffffffffu, ob1, k & 15), cb2 = __shfl_sync(0xffffffffu, ob2, k & 15);
         float *o = a.Iout + (unsigned)ij * (unsigned)dp;
         const float *Sk = S + k * ss;
         float first = 0.f;
 #pragma unroll
         for (int p = 0; p < P; p++)
         {
-            const int d = lane + 32 * p;
-            const float v = fmaf(g, Sk[min(d, nd - 1)], fmaf(cb1, LN[p].x, fmaf(cb2, LN[p].y, ca)));
-            if (d < nd)
+            const int d = dl + 32 * p;
+            const float v = kact ? fmaf(g, Sk[min(d, nd - 1)], fmaf(cb1, LN[p].x, fmaf(cb2, LN[p].y, ca))) : 0.f;
+            if (kact && d < nd)
                 o[d] = v;
             if (p == 0)
                 first = v;
         }
-        if (lane < kStateMirror)
-            o[nd + lane] = first;
+        if (kact && dl < kStateMirror)
+            o[nd + dl] = first;
     }
     __syncwarp(); // S is rewritten by the next tile's phase 1
 }
@@ -614,7 +639,7 @@ __device__ __forceinline__ void step_unit32(const Step32Args &a, const DirTable 
 // row-type table, the direction coefficients, then the warps' buffers
 __device__ __forceinline__ int step32_header(int nd) { return kRowtabOffset + kMaxRowTypes * 12 * 4 + 32 * nd; }
 
-template <bool CURVED, int P>
+template <bool CURVED, int P, bool H>
 __global__ void __launch_bounds__(kThreads, GRLBM_STEP32_MIN_BLOCKS)
     k_step_prec(const __grid_constant__ Step32Args a, const __grid_constant__ DirTable dt, int warp_stride)
 {
@@ -634,9 +659,9 @@ __global__ void __launch_bounds__(kThreads, GRLBM_STEP32_MIN_BLOCKS)
     float *S = patch + a.patch_floats;
     LaneFlat<P> LF;
     if (!CURVED)
-        load_lane_flat<P>(LF, dt, a.nd, a.dps, a.tx + 2);
+        load_lane_flat<P, H>(LF, dt, a.nd, a.dps, a.tx + 2);
     float2 LN[P];
-    load_lane_dirs<P>(LN, dirc, a.nd);
+    load_lane_dirs<P, H>(LN, dirc, a.nd);
     step::IterStats st{0ull, 0u};
     unsigned parity = 0;
     int tile = step::take_tile(a.tiles);
@@ -644,7 +669,7 @@ __global__ void __launch_bounds__(kThreads, GRLBM_STEP32_MIN_BLOCKS)
     if (tile < a.ntiles)
     {
         stage_tile(a, tile, patch, bar);
-        load_unit<CURVED, P>(a, tile, U);
+        load_unit<CURVED, P, H>(a, tile, U);
     }
     while (tile < a.ntiles)
     {
@@ -652,12 +677,12 @@ __global__ void __launch_bounds__(kThreads, GRLBM_STEP32_MIN_BLOCKS)
             break;
         int next = a.ntiles;
         UnitCells<P> N;
-        step_unit32<CURVED, P>(a, dt, rowtab, dirc, LF, LN, U, patch, S, st, [&]() {
+        step_unit32<CURVED, P, H>(a, dt, rowtab, dirc, LF, LN, U, patch, S, st, [&]() {
             next = step::take_tile(a.tiles);
             if (next < a.ntiles)
             {
                 stage_tile(a, next, patch, bar);
-                load_unit<CURVED, P>(a, next, N);
+                load_unit<CURVED, P, H>(a, next, N);
             }
         });
         U = N;
@@ -670,7 +695,8 @@ __global__ void __launch_bounds__(kThreads, GRLBM_STEP32_MIN_BLOCKS)
 // Many problems in one persistent launch: the warps take tiles from one
 // counter over the concatenated tile lists (problem k owns tiles
 // [first_tile[k], first_tile[k + 1])) and step each with the single-problem
-// tile function, so every problem's result is the one it gets alone.
+// tile function at the problem's own passes (or half-warp mode), so every
+// problem's result is the one it gets alone.
 __device__ __forceinline__ int batch_item_of(const int *__restrict__ first_tile, int n_items, int tile)
 {
     int lo = 0, hi = n_items - 1;
@@ -685,7 +711,45 @@ __device__ __forceinline__ int batch_item_of(const int *__restrict__ first_tile,
     return lo;
 }
 
-template <int P>
+template <int V>
+using IntC = std::integral_constant<int, V>;
+template <bool V>
+using BoolC = std::integral_constant<bool, V>;
+
+// Calls f(IntC<P>, BoolC<H>) for an item's mode (0: half-warp mode, else its
+// passes), among the modes a kernel of PM passes holds.
+template <int PM, class F>
+__device__ __forceinline__ void with_mode(int mode, F &&f)
+{
+    if (mode == 0)
+        f(IntC<1>{}, BoolC<true>{});
+    else if (mode == 1)
+        f(IntC<1>{}, BoolC<false>{});
+    else if constexpr (PM >= 2)
+    {
+        if (mode == 2)
+            f(IntC<2>{}, BoolC<false>{});
+        else if constexpr (PM >= 3)
+        {
+            if (mode == 3)
+                f(IntC<3>{}, BoolC<false>{});
+            else if constexpr (PM >= 4)
+            {
+                if (mode == 4)
+                    f(IntC<4>{}, BoolC<false>{});
+                else if constexpr (PM >= 6)
+                {
+                    if (mode == 6)
+                        f(IntC<6>{}, BoolC<false>{});
+                    else if constexpr (PM >= 8)
+                        f(IntC<8>{}, BoolC<false>{});
+                }
+            }
+        }
+    }
+}
+
+template <int PM>
 __global__ void __launch_bounds__(kThreads, GRLBM_STEP32_MIN_BLOCKS)
     k_step_batch32(const Batch32Item *__restrict__ items, const int *__restrict__ first_tile, int n_items,
                    int total_tiles, int flip, unsigned *counters, int warp_stride, int s_offset)
@@ -696,25 +760,27 @@ __global__ void __launch_bounds__(kThreads, GRLBM_STEP32_MIN_BLOCKS)
         mbar_init(bar, 1);
     __syncthreads();
     float *buf = step::warp_buffers<float>(smem, kRowtabOffset, warp_stride);
-    LaneFlat<P> LF;
-    float2 LN[P];
+    LaneFlat<PM> LF;
+    float2 LN[PM];
     step::IterStats st{0ull, 0u};
     unsigned parity = 0;
     int cur = -1;
     const Step32Args *ca = nullptr;
     // stage a tile of the batch and load its cells' tables
-    auto start_tile = [&](int t, UnitCells<P> &u) {
+    auto start_tile = [&](int t, UnitCells<PM> &u) {
         const int nk = batch_item_of(first_tile, n_items, t);
         const Batch32Item &nit = items[nk];
         const Step32Args &na = nit.a[nit.cur0 ^ flip];
         stage_tile(na, t - first_tile[nk], buf, bar);
-        if (nit.curved)
-            load_unit<true, P>(na, t - first_tile[nk], u);
-        else
-            load_unit<false, P>(na, t - first_tile[nk], u);
+        with_mode<PM>(nit.mode, [&](auto pc, auto hc) {
+            if (nit.curved)
+                load_unit<true, decltype(pc)::value, decltype(hc)::value>(na, t - first_tile[nk], u);
+            else
+                load_unit<false, decltype(pc)::value, decltype(hc)::value>(na, t - first_tile[nk], u);
+        });
     };
     int tile = step::take_tile(counters);
-    UnitCells<P> U;
+    UnitCells<PM> U;
     if (tile < total_tiles)
         start_tile(tile, U);
     while (tile < total_tiles)
@@ -724,6 +790,7 @@ __global__ void __launch_bounds__(kThreads, GRLBM_STEP32_MIN_BLOCKS)
         const Step32Args &ia = it.a[it.cur0 ^ flip];
         if (!step::wait_tile(bar, parity, ia.fault))
             break;
+        const float4 *dirc = reinterpret_cast<const float4 *>(it.dt->dirc);
         if (k != cur)
         {
             if (ca)
@@ -731,25 +798,32 @@ __global__ void __launch_bounds__(kThreads, GRLBM_STEP32_MIN_BLOCKS)
             st = step::IterStats{0ull, 0u};
             cur = k;
             ca = &ia;
-            if (!it.curved)
-                load_lane_flat<P>(LF, *it.dt, ia.nd, ia.dps, ia.tx + 2);
-            load_lane_dirs<P>(LN, reinterpret_cast<const float4 *>(it.dt->dirc), ia.nd);
+            with_mode<PM>(it.mode, [&](auto pc, auto hc) {
+                constexpr int P = decltype(pc)::value;
+                constexpr bool H = decltype(hc)::value;
+                if (!it.curved)
+                    load_lane_flat<P, H>(LF, *it.dt, ia.nd, ia.dps, ia.tx + 2);
+                load_lane_dirs<P, H>(LN, dirc, ia.nd);
+            });
         }
         int next = total_tiles;
-        UnitCells<P> N;
+        UnitCells<PM> N;
         auto stage_next = [&]() {
             next = step::take_tile(counters);
             if (next < total_tiles)
                 start_tile(next, N);
         };
-        const float4 *dirc = reinterpret_cast<const float4 *>(it.dt->dirc);
         // (the streamed values sit past the largest patch of the batch: the
         // next tile's copy, of any problem, never reaches them)
         float *S = buf + s_offset;
-        if (it.curved)
-            step_unit32<true, P>(ia, *it.dt, it.dt->rowtab, dirc, LF, LN, U, buf, S, st, stage_next);
-        else
-            step_unit32<false, P>(ia, *it.dt, it.dt->rowtab, dirc, LF, LN, U, buf, S, st, stage_next);
+        with_mode<PM>(it.mode, [&](auto pc, auto hc) {
+            constexpr int P = decltype(pc)::value;
+            constexpr bool H = decltype(hc)::value;
+            if (it.curved)
+                step_unit32<true, P, H>(ia, *it.dt, it.dt->rowtab, dirc, LF, LN, U, buf, S, st, stage_next);
+            else
+                step_unit32<false, P, H>(ia, *it.dt, it.dt->rowtab, dirc, LF, LN, U, buf, S, st, stage_next);
+        });
         U = N;
         tile = next;
     }
@@ -760,10 +834,10 @@ __global__ void __launch_bounds__(kThreads, GRLBM_STEP32_MIN_BLOCKS)
 
 inline unsigned nblk(int64_t n, int b) { return (unsigned)((n + b - 1) / b); }
 
-template <bool CURVED, int P>
+template <bool CURVED, int P, bool H = false>
 cudaError_t set_smem_limit()
 {
-    return cudaFuncSetAttribute(k_step_prec<CURVED, P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    return cudaFuncSetAttribute(k_step_prec<CURVED, P, H>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 kStep32MaxSmem);
 }
 
@@ -778,6 +852,12 @@ int step32_passes(int nd)
         if (p >= need)
             return p;
     return -1;
+}
+
+int step32_mode(int nd)
+{
+    const int p = step32_passes(nd);
+    return p == 1 && nd <= 16 ? 0 : p;
 }
 
 int step32_s_stride(int nd) { return nd + ((2 - nd) % 32 + 32) % 32; }
@@ -823,17 +903,24 @@ cudaError_t prepare_step32()
     GRLBM_PREP(6)
     GRLBM_PREP(8)
 #undef GRLBM_PREP
+    if (e == cudaSuccess)
+        e = set_smem_limit<true, 1, true>();
+    if (e == cudaSuccess)
+        e = set_smem_limit<false, 1, true>();
     return e;
 }
 
-// resident blocks per SM of the step kernel for P passes at a shared-memory size
-cudaError_t step32_occupancy(int P, bool curved, bool batch, size_t smem, int *blocks)
+// resident blocks per SM of the step kernel for P passes at a shared-memory
+// size (single problem of nd directions, or the batch kernel)
+cudaError_t step32_occupancy(int P, bool curved, bool batch, size_t smem, int *blocks, int nd)
 {
     const void *f = nullptr;
+    if (!batch && P == 1 && nd <= 16)
+        f = curved ? (const void *)k_step_prec<true, 1, true> : (const void *)k_step_prec<false, 1, true>;
 #define GRLBM_PICK(PP)                                                                                      \
-    if (P == PP)                                                                                            \
+    if (P == PP && !f)                                                                                      \
         f = batch ? (const void *)k_step_batch32<PP>                                                        \
-                  : (curved ? (const void *)k_step_prec<true, PP> : (const void *)k_step_prec<false, PP>);
+                  : (curved ? (const void *)k_step_prec<true, PP, false> : (const void *)k_step_prec<false, PP, false>);
     GRLBM_PICK(1)
     GRLBM_PICK(2)
     GRLBM_PICK(3)
@@ -853,13 +940,21 @@ void launch_step32(const Step32Args &a, const DirTable &dt, bool curved, int P, 
     const size_t smem = step32_smem(a.tx, a.ty, a.dp, a.nd);
     const int stride = step32_warp_stride(a.tx, a.ty, a.dp, a.nd);
     const unsigned grid = (unsigned)std::max(1, std::min(blocks, (int)nblk(a.ntiles, kWarps)));
+    if (P == 1 && a.nd <= 16) // half-warp mode: two cells at a time
+    {
+        if (curved)
+            k_step_prec<true, 1, true><<<grid, kThreads, smem, s>>>(a, dt, stride);
+        else
+            k_step_prec<false, 1, true><<<grid, kThreads, smem, s>>>(a, dt, stride);
+        return;
+    }
 #define GRLBM_LAUNCH(PP)                                                                                    \
     if (P == PP)                                                                                            \
     {                                                                                                       \
         if (curved)                                                                                         \
-            k_step_prec<true, PP><<<grid, kThreads, smem, s>>>(a, dt, stride);                              \
+            k_step_prec<true, PP, false><<<grid, kThreads, smem, s>>>(a, dt, stride);                       \
         else                                                                                                \
-            k_step_prec<false, PP><<<grid, kThreads, smem, s>>>(a, dt, stride);                             \
+            k_step_prec<false, PP, false><<<grid, kThreads, smem, s>>>(a, dt, stride);                      \
         return;                                                                                             \
     }
     GRLBM_LAUNCH(1)

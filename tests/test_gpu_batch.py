@@ -93,3 +93,31 @@ def test_contexts_of_different_direction_counts_coexist(grlbm, W):
             a.step(3)
             b.step(3)
             assert np.isfinite(a.moments_if()["E"]).all() and np.isfinite(b.moments_if()["E"]).all()
+
+
+def test_batch_config5_instances_against_oracle(grlbm, W, oracle):
+    """Four instances of the batched workload (64 seeded problems of grid
+    sizes 64^2..512^2, 16/32/64 directions, flat or Schwarzschild, 500 steps)
+    -- its smallest ones, one per direction count where the draw has one --
+    stepped in one batch with the persistent launch, against the FP64
+    oracle: E within 1e-5 (relative L2)."""
+    allc = W.batch_instances(count=64, seed=10)
+    picked = []
+    for nd in (16, 32, 64):
+        small = sorted((c for c in allc if c["n_dir"] == nd), key=lambda c: c["nx_"] * c["ny_"])
+        picked += small[:1]
+    rest = sorted((c for c in allc if all(c is not p for p in picked)), key=lambda c: c["nx_"] * c["ny_"] * c["n_dir"])
+    picked += rest[:4 - len(picked)]
+    assert len(picked) == 4 and len({c["n_dir"] for c in picked}) >= 2
+    probs = [grlbm.prepare(c, grlbm.PRECISION_FP32) for c in picked]
+    try:
+        with grlbm.Batch(probs) as b:
+            b.set_shape(1, True)
+            b.step(int(picked[0]["n_steps"]))
+        for c, r in zip(picked, probs):
+            ref = oracle.run(c, "oracle", n_threads=0)
+            err = float(np.linalg.norm(r.moments_if()["E"] - ref["E"]) / np.linalg.norm(ref["E"]))
+            assert err <= 1e-5, (c["nx_"], c["n_dir"], err)
+    finally:
+        for r in probs:
+            r.close()
