@@ -472,6 +472,9 @@ int step32_warp_stride(int tx, int ty, int dp, int nd);
 // shared memory of a block of the single-problem kernel, and of the batch kernel
 size_t step32_smem(int tx, int ty, int dp, int nd);
 size_t step32_batch_smem(int warp_stride);
+// bytes at the start of each warp's batch buffer for its copy of the current
+// problem's arguments, direction scalars and q row types
+int step32_batch_item_bytes(int q);
 cudaError_t prepare_step32();
 cudaError_t step32_occupancy(int P, bool curved, bool batch, size_t smem, int *blocks, int nd);
 // The step's mode for nd directions: 0 for half-warp mode (at most 16
@@ -481,7 +484,7 @@ int step32_mode(int nd);
 void launch_step32(const Step32Args &a, const DirTable &dt, bool curved, int P, int blocks, cudaStream_t s);
 void launch_step_batch32(const Batch32Item *items, const int *first_tile, int n_items, int total_tiles, int flip,
                          unsigned *counters, int P, int blocks, size_t smem, int warp_stride, int s_offset,
-                         cudaStream_t s);
+                         int item_bytes, cudaStream_t s);
 // The TMA map the step stages a cell-major state of nx x ny nodes through,
 // for tiles of tx x ty cells.
 cudaError_t encode_state_map32(CUtensorMap *map, const float *state, int64_t nx, int64_t ny, int dp, int tx, int ty);

@@ -2056,6 +2056,7 @@ struct grlbm_batch
     std::vector<int> order;         // items[k] is context order[k]
     DevBuf d_items, d_first, d_dirs, counters;
     int total_tiles = 0, passes = 1, warp_stride = 0, s_offset = 0, blocks_per_sm_max = 1, blocks_per_sm = 1, sms = 1;
+    int item_bytes = 0; // each warp's copy of its problem's arguments and tables
     size_t smem = 0;
     int largest_first = 0;
     int flip = 0; // parity of the steps taken since the items were built
@@ -2122,14 +2123,16 @@ int batch_geometry(grlbm_batch *b)
     // streamed-value rows
     b->passes = 1;
     b->s_offset = 0;
-    int s_rows = 0;
+    int s_rows = 0, q = 1;
     for (grlbm_ctx *c : b->ctx)
     {
         b->passes = std::max(b->passes, c->passes);
         b->s_offset = std::max(b->s_offset, step32_patch_floats(c->tile_x, c->tile_y, (int)c->sl.sp));
         s_rows = std::max(s_rows, step32_s_stride(c->st.n));
+        q = std::max(q, c->dirs.q);
     }
-    b->warp_stride = ((b->s_offset + kStep32UnitCells * s_rows) * 4 + 127) / 128 * 128;
+    b->item_bytes = step32_batch_item_bytes(q);
+    b->warp_stride = b->item_bytes + ((b->s_offset + kStep32UnitCells * s_rows) * 4 + 127) / 128 * 128;
     b->smem = step32_batch_smem(b->warp_stride);
     if (b->smem > (size_t)kStep32MaxSmem)
         return bfail(b, GRLBM_ERR_ARGUMENT, "the batch's largest patch needs %zu bytes of shared memory", b->smem);
@@ -2194,7 +2197,8 @@ int batch_enqueue(grlbm_batch *b, int n, int flip)
         for (int s = 0; s < n; s++)
             launch_step_batch32(b->d_items.as<Batch32Item>(), b->d_first.as<int>(), (int)b->items.size(),
                                 b->total_tiles, flip ^ (s & 1), b->counters.as<unsigned>(), b->passes,
-                                b->sms * b->blocks_per_sm, b->smem, b->warp_stride, b->s_offset, b->stream);
+                                b->sms * b->blocks_per_sm, b->smem, b->warp_stride, b->s_offset, b->item_bytes,
+                                b->stream);
         return GRLBM_OK;
     }
     BCU(cudaEventRecord(b->fork, b->stream));

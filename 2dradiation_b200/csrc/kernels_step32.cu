@@ -283,8 +283,8 @@ __device__ __forceinline__ void load_unit(const Step32Args &a, int tile, UnitCel
 // stores the cells' new state, coalesced along the directions.  In
 // half-warp mode (H, at most 16 directions) phases 1 and 3 take two cells at
 // a time, one per half-warp.  P passes of the PM the lane arrays hold.
-template <bool CURVED, int P, bool H, int PM, class Next>
-__device__ __forceinline__ void step_unit32(const Step32Args &a, const DirTable &dt, const float *rowtab,
+template <bool CURVED, int P, bool H, int PM, class DT, class Next>
+__device__ __forceinline__ void step_unit32(const Step32Args &a, const DT &dt, const float *rowtab,
                                             const float4 *dirc, const LaneFlat<PM> &LF, const float2 (&LN)[PM],
                                             const UnitCells<PM> &U, const float *patch, float *S,
                                             step::IterStats &st, Next next)
@@ -749,23 +749,40 @@ __device__ __forceinline__ void with_mode(int mode, F &&f)
     }
 }
 
+// The scalars of a problem's direction tables that the tile function reads
+// (the batch kernel keeps a copy per warp in shared memory; 16-byte aligned,
+// as the row types that follow it are read as float4).
+struct alignas(16) DirScalars
+{
+    float wmom[18];
+    int q, p;
+    float inv_q;
+};
+
 template <int PM>
 __global__ void __launch_bounds__(kThreads, GRLBM_STEP32_MIN_BLOCKS)
     k_step_batch32(const Batch32Item *__restrict__ items, const int *__restrict__ first_tile, int n_items,
-                   int total_tiles, int flip, unsigned *counters, int warp_stride, int s_offset)
+                   int total_tiles, int flip, unsigned *counters, int warp_stride, int s_offset, int item_bytes)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     const unsigned bar = smem_addr(smem) + 8u * (unsigned)(threadIdx.x >> 5);
-    if ((threadIdx.x & 31) == 0)
+    const int lane = threadIdx.x & 31;
+    if (lane == 0)
         mbar_init(bar, 1);
     __syncthreads();
-    float *buf = step::warp_buffers<float>(smem, kRowtabOffset, warp_stride);
+    // the warp's copy of its current problem's step arguments, direction
+    // scalars and row types (read by every cell and direction), then its
+    // patch and streamed-value buffers
+    unsigned char *mine = step::align128(smem + kRowtabOffset) + (size_t)(threadIdx.x >> 5) * (size_t)warp_stride;
+    Step32Args &wa = *reinterpret_cast<Step32Args *>(mine);
+    DirScalars &wd = *reinterpret_cast<DirScalars *>(mine + sizeof(Step32Args));
+    float *wrow = reinterpret_cast<float *>(mine + sizeof(Step32Args) + sizeof(DirScalars));
+    float *buf = reinterpret_cast<float *>(mine + item_bytes);
     LaneFlat<PM> LF;
     float2 LN[PM];
     step::IterStats st{0ull, 0u};
     unsigned parity = 0;
     int cur = -1;
-    const Step32Args *ca = nullptr;
     // stage a tile of the batch and load its cells' tables
     auto start_tile = [&](int t, UnitCells<PM> &u) {
         const int nk = batch_item_of(first_tile, n_items, t);
@@ -787,23 +804,37 @@ __global__ void __launch_bounds__(kThreads, GRLBM_STEP32_MIN_BLOCKS)
     {
         const int k = batch_item_of(first_tile, n_items, tile);
         const Batch32Item &it = items[k];
-        const Step32Args &ia = it.a[it.cur0 ^ flip];
-        if (!step::wait_tile(bar, parity, ia.fault))
+        if (!step::wait_tile(bar, parity, it.a[it.cur0 ^ flip].fault))
             break;
         const float4 *dirc = reinterpret_cast<const float4 *>(it.dt->dirc);
         if (k != cur)
         {
-            if (ca)
-                step::flush_stats(st, ca->iter_sum, ca->iter_max);
+            if (cur >= 0)
+                step::flush_stats(st, wa.iter_sum, wa.iter_max);
             st = step::IterStats{0ull, 0u};
             cur = k;
-            ca = &ia;
+            __syncwarp(); // the lanes are done with the previous problem's copy
+            {
+                const unsigned *src = reinterpret_cast<const unsigned *>(&it.a[it.cur0 ^ flip]);
+                unsigned *dst = reinterpret_cast<unsigned *>(&wa);
+                for (int w = lane; w < (int)(sizeof(Step32Args) / 4); w += 32)
+                    dst[w] = src[w];
+                const DirTable &dt = *it.dt;
+                for (int w = lane; w < 18; w += 32)
+                    wd.wmom[w] = dt.wmom[w];
+                if (lane == 0)
+                    wd.q = dt.q, wd.p = dt.p, wd.inv_q = dt.inv_q;
+                if (it.curved)
+                    for (int w = lane; w < dt.q * 12; w += 32)
+                        wrow[w] = dt.rowtab[w];
+            }
+            __syncwarp();
             with_mode<PM>(it.mode, [&](auto pc, auto hc) {
                 constexpr int P = decltype(pc)::value;
                 constexpr bool H = decltype(hc)::value;
                 if (!it.curved)
-                    load_lane_flat<P, H>(LF, *it.dt, ia.nd, ia.dps, ia.tx + 2);
-                load_lane_dirs<P, H>(LN, dirc, ia.nd);
+                    load_lane_flat<P, H>(LF, *it.dt, wa.nd, wa.dps, wa.tx + 2);
+                load_lane_dirs<P, H>(LN, dirc, wa.nd);
             });
         }
         int next = total_tiles;
@@ -820,15 +851,15 @@ __global__ void __launch_bounds__(kThreads, GRLBM_STEP32_MIN_BLOCKS)
             constexpr int P = decltype(pc)::value;
             constexpr bool H = decltype(hc)::value;
             if (it.curved)
-                step_unit32<true, P, H>(ia, *it.dt, it.dt->rowtab, dirc, LF, LN, U, buf, S, st, stage_next);
+                step_unit32<true, P, H>(wa, wd, wrow, dirc, LF, LN, U, buf, S, st, stage_next);
             else
-                step_unit32<false, P, H>(ia, *it.dt, it.dt->rowtab, dirc, LF, LN, U, buf, S, st, stage_next);
+                step_unit32<false, P, H>(wa, wd, wrow, dirc, LF, LN, U, buf, S, st, stage_next);
         });
         U = N;
         tile = next;
     }
-    if (ca)
-        step::flush_stats(st, ca->iter_sum, ca->iter_max);
+    if (cur >= 0)
+        step::flush_stats(st, wa.iter_sum, wa.iter_max);
     step::retire_warp(counters, kWarps);
 }
 
@@ -883,6 +914,8 @@ size_t step32_smem(int tx, int ty, int dp, int nd)
     const int header = kRowtabOffset + kMaxRowTypes * 12 * 4 + 32 * nd;
     return (size_t)header + 128 + (size_t)kWarps * (size_t)step32_warp_stride(tx, ty, dp, nd);
 }
+
+int step32_batch_item_bytes(int q) { return (int)((sizeof(Step32Args) + sizeof(DirScalars) + 4 * 12 * q + 127) / 128 * 128); }
 
 size_t step32_batch_smem(int warp_stride) { return (size_t)kRowtabOffset + 128 + (size_t)kWarps * warp_stride; }
 
@@ -968,13 +1001,13 @@ void launch_step32(const Step32Args &a, const DirTable &dt, bool curved, int P, 
 
 void launch_step_batch32(const Batch32Item *items, const int *first_tile, int n_items, int total_tiles, int flip,
                          unsigned *counters, int P, int blocks, size_t smem, int warp_stride, int s_offset,
-                         cudaStream_t s)
+                         int item_bytes, cudaStream_t s)
 {
 #define GRLBM_LAUNCH(PP)                                                                                    \
     if (P == PP)                                                                                            \
     {                                                                                                       \
         k_step_batch32<PP><<<blocks, kThreads, smem, s>>>(items, first_tile, n_items, total_tiles, flip,    \
-                                                          counters, warp_stride, s_offset);                 \
+                                                          counters, warp_stride, s_offset, item_bytes);     \
         return;                                                                                             \
     }
     GRLBM_LAUNCH(1)
