@@ -78,6 +78,7 @@ SIGNATURES = {
     "grlbm_set_fourier_coefficients": ([C.c_void_p] + [_D] * 5, C.c_int),
     "grlbm_step": ([C.c_void_p, C.c_int32], C.c_int),
     "grlbm_step_async": ([C.c_void_p, C.c_int32], C.c_int),
+    "grlbm_step_rows_async": ([C.c_void_p, C.c_int64, C.c_int64, C.c_int32], C.c_int),
     "grlbm_sync": ([C.c_void_p], C.c_int),
     "grlbm_stream": ([C.c_void_p], C.c_void_p),
     "grlbm_get_moments_if": ([C.c_void_p] + [_D] * 6, C.c_int),
@@ -286,6 +287,11 @@ class Radiation:
     def step_async(self, n: int):
         self._c(lib().grlbm_step_async(self.h, n))
 
+    def step_rows_async(self, j_first: int, j_end: int, finish: bool):
+        """One step's update of node rows [j_first, j_end), enqueued without
+        waiting; finish=True ends the step (grlbm_step_rows_async)."""
+        self._c(lib().grlbm_step_rows_async(self.h, int(j_first), int(j_end), int(bool(finish))))
+
     def sync(self):
         self._c(lib().grlbm_sync(self.h))
 
@@ -468,11 +474,14 @@ def selftest_staging_wait(arrive: bool, limit_us: int, device: int = -1) -> dict
     return {"completed": bool(done.value), "waited_us": waited.value}
 
 
-def prepare(case: dict, precision: int = PLAIN_FP64, device: int = -1) -> Radiation:
+def prepare(case: dict, precision: int = PLAIN_FP64, device: int = -1, rows: tuple | None = None) -> Radiation:
     """Construct and load a case the way RunSimulation starts
     (src/Radiation.cpp:745-746): inputs, LoadInitialData, then the geodesic
-    tables."""
+    tables.  With `rows` = (j_first, j_end) the context steps that band of
+    node rows and builds the tables of its cells only."""
     r = Radiation(case, precision, device)
+    if rows is not None:
+        r.set_rows(*rows)
     r.set_fields(case["fields"])
     r.set_initial_data(case["fields"])
     r.load_initial_data()

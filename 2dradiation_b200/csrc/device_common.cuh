@@ -141,9 +141,10 @@ struct GeodesicArgs
     int nf;
     double tol;
     int max_trials;
-    double *data; // out: [5][ncell][nf]: 1/s, x, y, vIF_x, vIF_y
+    double *data; // out: [5][cn][nf]: 1/s, x, y, vIF_x, vIF_y of the built cells
     unsigned long long *trials_total;
     int *nonconverged;
+    int64_t c0, cn; // the interior cells built: [c0, c0 + cn)
 };
 
 struct ProjectArgs
@@ -154,6 +155,7 @@ struct ProjectArgs
     const double *ss_w;  // nf
     const double *basis; // [f][k] = Basis(k, phi_f)
     double *coef;        // [5][nxy][nf]
+    int64_t c0, cn;      // the interior cells built (data holds them): [c0, c0 + cn)
 };
 
 // Directions per chunk of the adaptive precision-form kernels' moment loops.
@@ -211,6 +213,7 @@ struct DepartureArgs
     int *clamped;
     unsigned long long *far; // packed records marked far (precision form)
     int *row_extent;     // max over departures of the node rows away from the cell a gather reads
+    int64_t c0, cn;      // the interior cells built: [c0, c0 + cn)
 };
 
 // What a recording plain step writes for the adjoint (indices over the

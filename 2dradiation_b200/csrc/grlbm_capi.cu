@@ -93,6 +93,10 @@ struct grlbm_ctx
     int64_t nsrc = 0;
     int cur = 0;
     bool tables = false;
+    // node rows whose interior cells have tables (coefficients and records):
+    // the band when they were built
+    int64_t table_jlo = 0, table_jhi = 0;
+    bool partial = false; // a step enqueued in row ranges (grlbm_step_rows_async) is open
     // config.updateFourierHarmonics: rebuild the tables before every step
     bool update_each_step = false;
     double update_tol = 1e-4;
@@ -493,14 +497,31 @@ bool is_adaptive(const grlbm_ctx *ctx)
     return ctx->run.streaming_type == GRLBM_FLAT_ADAPTIVE || ctx->run.streaming_type == GRLBM_CURVED_ADAPTIVE;
 }
 
+// The step's tables exist for the band (curved streaming).
+int check_tables(grlbm_ctx *ctx)
+{
+    if (!is_curved(ctx))
+        return GRLBM_OK;
+    if (!ctx->tables)
+        return fail(ctx, GRLBM_ERR_STATE, "curved streaming needs grlbm_update_fourier_coefficients first");
+    if (ctx->gd.jlo < ctx->table_jlo || ctx->gd.jhi > ctx->table_jhi)
+        return fail(ctx, GRLBM_ERR_STATE,
+                    "the geodesic tables cover rows [%lld, %lld) only; rebuild them for the band [%lld, %lld)",
+                    (long long)ctx->table_jlo, (long long)ctx->table_jhi, (long long)ctx->gd.jlo,
+                    (long long)ctx->gd.jhi);
+    return GRLBM_OK;
+}
+
 // Enqueue one step starting from buffer `from` (no sync).
-int enqueue_step(grlbm_ctx *ctx, int from)
+// (sources: LoadInitialData at the top of the step; off for the second and
+// later row ranges of a step enqueued in parts)
+int enqueue_step(grlbm_ctx *ctx, int from, bool sources = true)
 {
     const bool curved = is_curved(ctx);
     unsigned long long *cnt = ctx->counters.as<unsigned long long>();
     if (ctx->fast64)
     {
-        if (ctx->run.keep_source_nodes_active && ctx->nsrc > 0)
+        if (sources && ctx->run.keep_source_nodes_active && ctx->nsrc > 0)
             launch_sources64L(ctx->I[from].as<double>(), ctx->sl, ctx->st.n, ctx->src_nodes.as<int64_t>(),
                               ctx->src_vals.as<double>(), ctx->nsrc, ctx->stream);
         launch_step64(step64_args(ctx, from), ctx->dirs64t.as<DirTable64>(), curved, ctx->passes, ctx->step_blocks,
@@ -508,7 +529,7 @@ int enqueue_step(grlbm_ctx *ctx, int from)
     }
     else if (ctx->fp32)
     {
-        if (ctx->run.keep_source_nodes_active && ctx->nsrc > 0)
+        if (sources && ctx->run.keep_source_nodes_active && ctx->nsrc > 0)
             launch_sources32(ctx->I[from].as<float>(), ctx->sl, ctx->st.n, ctx->src_nodes.as<int64_t>(),
                              ctx->src_vals.as<float>(), ctx->nsrc, ctx->stream);
         if (!is_adaptive(ctx))
@@ -517,7 +538,7 @@ int enqueue_step(grlbm_ctx *ctx, int from)
         {
             PrecStepArgs a = prec_args(ctx, from);
             // LoadInitialData also sets the source nodes' angles (src/Radiation.cpp:170-176)
-            if (ctx->run.keep_source_nodes_active && ctx->nsrc_ang > 0)
+            if (sources && ctx->run.keep_source_nodes_active && ctx->nsrc_ang > 0)
                 launch_sources64(ctx->ang[from].as<double>(), ctx->gd.nxy, 1, ctx->src_ang_nodes.as<int64_t>(),
                                  ctx->src_ang_vals.as<double>(), ctx->nsrc_ang, ctx->stream);
             a.ang_old = ctx->ang[from].as<double>();
@@ -529,14 +550,14 @@ int enqueue_step(grlbm_ctx *ctx, int from)
     }
     else
     {
-        if (ctx->run.keep_source_nodes_active && ctx->nsrc > 0)
+        if (sources && ctx->run.keep_source_nodes_active && ctx->nsrc > 0)
             launch_sources64(ctx->I[from].as<double>(), ctx->gd.nxy, ctx->st.n, ctx->src_nodes.as<int64_t>(),
                              ctx->src_vals.as<double>(), ctx->nsrc, ctx->stream);
         PlainStepArgs a = plain_args(ctx, from);
         if (is_adaptive(ctx))
         {
             // LoadInitialData also sets the source nodes' angles (src/Radiation.cpp:170-176)
-            if (ctx->run.keep_source_nodes_active && ctx->nsrc_ang > 0)
+            if (sources && ctx->run.keep_source_nodes_active && ctx->nsrc_ang > 0)
                 launch_sources64(ctx->ang[from].as<double>(), ctx->gd.nxy, 1, ctx->src_ang_nodes.as<int64_t>(),
                                  ctx->src_ang_vals.as<double>(), ctx->nsrc_ang, ctx->stream);
             a.ang_old = ctx->ang[from].as<double>();
@@ -598,6 +619,8 @@ int build_records(grlbm_ctx *ctx)
     da.p = ctx->dirs.p;
     for (int r = 0; r < ctx->dirs.q && r < kMaxRowTypes; r++)
         da.row_base[r] = (int)ctx->dirs.rowtab[r * 12 + 10];
+    da.c0 = (ctx->gd.jlo - 1) * ctx->gd.nx_;
+    da.cn = (ctx->gd.jhi - ctx->gd.jlo) * ctx->gd.nx_;
     da.clamped = reinterpret_cast<int *>(ctx->counters.as<unsigned long long>() + 4);
     da.row_extent = reinterpret_cast<int *>(ctx->counters.as<unsigned long long>() + 5);
     da.far = ctx->counters.as<unsigned long long>() + 6;
@@ -1376,11 +1399,12 @@ int grlbm_update_fourier_coefficients(grlbm_ctx *ctx, double rk_tol, int32_t max
         return fail(ctx, GRLBM_ERR_ARGUMENT, "rk_tol must be positive");
     cudaSetDevice(ctx->device);
     const int nf = ctx->ss.n;
-    const int64_t ncell = ctx->ncell;
+    // the cells of the band's rows (all interior cells unless grlbm_set_rows narrowed it)
+    const int64_t c0 = (ctx->gd.jlo - 1) * ctx->gd.nx_, cn = (ctx->gd.jhi - ctx->gd.jlo) * ctx->gd.nx_;
     unsigned long long *cnt = ctx->counters.as<unsigned long long>();
     CU(cudaMemsetAsync(cnt + 2, 0, 2 * sizeof(unsigned long long), ctx->stream));
     void *data = nullptr;
-    CU(cudaMallocAsync(&data, (size_t)5 * ncell * nf * sizeof(double), ctx->stream));
+    CU(cudaMallocAsync(&data, (size_t)5 * cn * nf * sizeof(double), ctx->stream));
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
@@ -1397,6 +1421,8 @@ int grlbm_update_fourier_coefficients(grlbm_ctx *ctx, double rk_tol, int32_t max
     ga.data = static_cast<double *>(data);
     ga.trials_total = cnt + 2;
     ga.nonconverged = reinterpret_cast<int *>(cnt + 3);
+    ga.c0 = c0;
+    ga.cn = cn;
     launch_geodesic(ga, ctx->stream);
 
     ProjectArgs pa{};
@@ -1406,6 +1432,8 @@ int grlbm_update_fourier_coefficients(grlbm_ctx *ctx, double rk_tol, int32_t max
     pa.ss_w = ctx->ss_w.as<double>();
     pa.basis = ctx->proj_basis.as<double>();
     pa.coef = ctx->coef.as<double>();
+    pa.c0 = c0;
+    pa.cn = cn;
     launch_project(pa, ctx->stream);
     int rc = build_records(ctx);
     cudaEventRecord(e1, ctx->stream);
@@ -1422,6 +1450,8 @@ int grlbm_update_fourier_coefficients(grlbm_ctx *ctx, double rk_tol, int32_t max
         return fail(ctx, GRLBM_ERR_CUDA, "table build failed: %s", cudaGetErrorString(le != cudaSuccess ? le : se));
     ctx->table_ms = ms;
     ctx->tables = true;
+    ctx->table_jlo = ctx->gd.jlo;
+    ctx->table_jhi = ctx->gd.jhi;
     unsigned long long h[5];
     CU(cudaMemcpy(h, cnt, sizeof h, cudaMemcpyDeviceToHost));
     const int nonconv = (int)(unsigned)h[3];
@@ -1448,6 +1478,8 @@ int grlbm_set_fourier_coefficients(grlbm_ctx *ctx, const double *S, const double
         return rc;
     CU(cudaStreamSynchronize(ctx->stream));
     ctx->tables = true;
+    ctx->table_jlo = ctx->gd.jlo;
+    ctx->table_jhi = ctx->gd.jhi;
     return GRLBM_OK;
 }
 
@@ -1470,10 +1502,12 @@ int grlbm_step_async(grlbm_ctx *ctx, int32_t n_steps)
         return GRLBM_ERR_ARGUMENT;
     if (n_steps < 0)
         return fail(ctx, GRLBM_ERR_ARGUMENT, "negative step count");
-    if (is_curved(ctx) && !ctx->tables)
-        return fail(ctx, GRLBM_ERR_STATE, "curved streaming needs grlbm_update_fourier_coefficients first");
+    int rc = check_tables(ctx);
+    if (rc)
+        return rc;
+    if (ctx->partial)
+        return fail(ctx, GRLBM_ERR_STATE, "a step enqueued in row ranges is not finished");
     cudaSetDevice(ctx->device);
-    int rc;
     if (ctx->update_each_step)
     {
         // UpdateFourierCoefficients at the top of every step (src/Radiation.cpp:790-791)
@@ -1503,6 +1537,42 @@ int grlbm_step_async(grlbm_ctx *ctx, int32_t n_steps)
         ctx->cur ^= 1;
     }
     ctx->steps += n_steps;
+    return GRLBM_OK;
+}
+
+int grlbm_step_rows_async(grlbm_ctx *ctx, int64_t j_first, int64_t j_end, int32_t finish)
+{
+    if (!ctx)
+        return GRLBM_ERR_ARGUMENT;
+    if (j_first < ctx->gd.jlo || j_end > ctx->gd.jhi || j_first > j_end)
+        return fail(ctx, GRLBM_ERR_ARGUMENT, "rows [%lld, %lld) outside the band [%lld, %lld)", (long long)j_first,
+                    (long long)j_end, (long long)ctx->gd.jlo, (long long)ctx->gd.jhi);
+    if (ctx->update_each_step)
+        return fail(ctx, GRLBM_ERR_UNSUPPORTED, "tables rebuilt every step are not stepped in row ranges");
+    if (is_adaptive(ctx))
+        return fail(ctx, GRLBM_ERR_UNSUPPORTED, "adaptive streaming is not split into row ranges");
+    int rc = check_tables(ctx);
+    if (rc)
+        return rc;
+    cudaSetDevice(ctx->device);
+    if (j_end > j_first)
+    {
+        const int64_t lo = ctx->gd.jlo, hi = ctx->gd.jhi;
+        ctx->gd.jlo = j_first;
+        ctx->gd.jhi = j_end;
+        rc = enqueue_step(ctx, ctx->cur, !ctx->partial);
+        ctx->gd.jlo = lo;
+        ctx->gd.jhi = hi;
+        if (rc)
+            return rc;
+        ctx->partial = true;
+    }
+    if (finish)
+    {
+        ctx->cur ^= 1;
+        ctx->steps++;
+        ctx->partial = false;
+    }
     return GRLBM_OK;
 }
 

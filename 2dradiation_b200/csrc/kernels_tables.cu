@@ -266,13 +266,14 @@ __device__ double rk45_backtrace(const GridDev &g, const double *__restrict__ rk
 __global__ void __launch_bounds__(128, 4) k_geodesic(GeodesicArgs a)
 {
     const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int64_t total = a.g.ncell * a.nf;
+    const int64_t total = a.cn * a.nf;
     int trials = 0;
     bool capped = false;
     if (tid < total)
     {
-        const int64_t c = tid / a.nf;
-        const int f = (int)(tid - c * a.nf);
+        const int64_t lc = tid / a.nf; // the cell within the built range
+        const int f = (int)(tid - lc * a.nf);
+        const int64_t c = a.c0 + lc;
         const int64_t i = 1 + c % a.g.nx_, j = 1 + c / a.g.nx_;
         const int64_t ij = i + j * a.g.nx;
         double x1 = a.g.startx + (double)i * a.g.dx, x2 = a.g.starty + (double)j * a.g.dy;
@@ -292,8 +293,8 @@ __global__ void __launch_bounds__(128, 4) k_geodesic(GeodesicArgs a)
             v1 = v2 = 0.0;
         double i11, i12, i21, i22;
         tetrad_block(a.g, a.rkf, x1, x2, RF_TI11, i11, i12, i21, i22);
-        const int64_t stride = a.g.ncell * a.nf;
-        const int64_t o = c * a.nf + f;
+        const int64_t stride = a.cn * a.nf;
+        const int64_t o = lc * a.nf + f;
         a.data[o] = 1.0 / s;
         a.data[o + stride] = x1;
         a.data[o + 2 * stride] = x2;
@@ -329,14 +330,15 @@ __global__ void __launch_bounds__(128, 4) k_geodesic(GeodesicArgs a)
 __global__ void __launch_bounds__(128) k_fourier_project(ProjectArgs a)
 {
     const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int64_t per_field = a.g.ncell * a.nf;
+    const int64_t per_field = a.cn * a.nf;
     if (tid >= 5 * per_field)
         return;
     const int field = (int)(tid / per_field);
     const int64_t r = tid - field * per_field;
-    const int64_t c = r / a.nf;
-    const int k = (int)(r - c * a.nf);
-    const double *d = a.data + field * per_field + c * a.nf;
+    const int64_t lc = r / a.nf; // the cell within the built range
+    const int k = (int)(r - lc * a.nf);
+    const int64_t c = a.c0 + lc;
+    const double *d = a.data + field * per_field + lc * a.nf;
     double acc = 0.0;
     for (int f = 0; f < a.nf; f++)
         acc += (d[f] * __ldg(a.ss_w + f)) * __ldg(a.basis + f * a.nf + k);
@@ -353,19 +355,21 @@ __global__ void __launch_bounds__(128) k_fourier_project(ProjectArgs a)
 __global__ void __launch_bounds__(128) k_departure(DepartureArgs a)
 {
     const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (tid >= a.g.ncell * a.nd)
+    if (tid >= a.cn * a.nd)
         return;
     int d;
-    int64_t c;
+    int64_t c, ri; // the cell, and its record's index
     if (a.rec32 || a.recf)
     {
-        c = tid / a.nd;
-        d = (int)(tid - c * a.nd);
+        c = a.c0 + tid / a.nd;
+        d = (int)(tid % a.nd);
+        ri = c * a.nd + d;
     }
     else
     {
-        d = (int)(tid / a.g.ncell);
-        c = tid - (int64_t)d * a.g.ncell;
+        d = (int)(tid / a.cn);
+        c = a.c0 + (tid - (int64_t)d * a.cn);
+        ri = (int64_t)d * a.g.ncell + c;
     }
     const int64_t i = 1 + c % a.g.nx_, j = 1 + c / a.g.nx_;
     const int64_t ij = i + j * a.g.nx;
@@ -449,10 +453,10 @@ __global__ void __launch_bounds__(128) k_departure(DepartureArgs a)
         const unsigned ux = __float_as_uint(fx) | (near && fxd == 0.0 ? 0x80000000u : 0u);
         const unsigned uy = __float_as_uint(fy) | (near && fyd == 0.0 ? 0x80000000u : 0u);
         const unsigned uw = __float_as_uint(r32.w) | (near ? 0u : 0x80000000u);
-        a.rec32[tid] = make_uint4(word, ux, uy, uw);
+        a.rec32[ri] = make_uint4(word, ux, uy, uw);
         if (!near && a.far)
             atomicAdd(a.far, 1ull);
-        a.side32[tid] = r32;
+        a.side32[ri] = r32;
     }
     if (a.recf)
     {
@@ -484,13 +488,13 @@ __global__ void __launch_bounds__(128) k_departure(DepartureArgs a)
         rf.y = biased(fy, cy);
         rf.z = biased(t, start << packed64::kExpShift);
         rf.w = near ? sf.w : __hiloint2double((int)((unsigned)__double2hiint(sf.w) | 0x80000000u), __double2loint(sf.w));
-        a.recf[tid] = rf;
+        a.recf[ri] = rf;
         if (!near && a.far)
             atomicAdd(a.far, 1ull);
-        a.sidef[tid] = sf;
+        a.sidef[ri] = sf;
     }
     if (a.rec64)
-        a.rec64[tid] = r64;
+        a.rec64[ri] = r64;
 }
 
 // (alpha_ij / alpha_n)^3 for the 3x3 neighbours n of each interior node, as
@@ -515,15 +519,15 @@ static inline unsigned nblk(int64_t n, int b) { return (unsigned)((n + b - 1) / 
 
 void launch_geodesic(const GeodesicArgs &a, cudaStream_t s)
 {
-    k_geodesic<<<nblk(a.g.ncell * a.nf, 128), 128, 0, s>>>(a);
+    k_geodesic<<<nblk(a.cn * a.nf, 128), 128, 0, s>>>(a);
 }
 void launch_project(const ProjectArgs &a, cudaStream_t s)
 {
-    k_fourier_project<<<nblk(5 * a.g.ncell * a.nf, 128), 128, 0, s>>>(a);
+    k_fourier_project<<<nblk(5 * a.cn * a.nf, 128), 128, 0, s>>>(a);
 }
 void launch_departure(const DepartureArgs &a, cudaStream_t s)
 {
-    k_departure<<<nblk(a.g.ncell * a.nd, 128), 128, 0, s>>>(a);
+    k_departure<<<nblk(a.cn * a.nd, 128), 128, 0, s>>>(a);
 }
 void launch_alpha_cube(const GridDev &g, const double *alpha, double *acube, cudaStream_t s)
 {

@@ -9,10 +9,14 @@ departure records bound it: grlbm_departure_rows), so a rank that holds its
 band plus `ghost` up-to-date rows on each side steps its band exactly as a
 single GPU would: the results are bit-identical to the single-GPU run.
 
-Each rank keeps the whole grid in its context (tables are built for every
-cell; rows outside band + ghosts go stale and are never read), so the state
-is replicated and the work is divided.  The exchange is point-to-point over
-torch.distributed: NCCL between GPUs (NVLink), gloo for the CPU tests.
+Each rank's context holds the grid's state, but builds the geodesic tables
+of its band's cells only, and steps only its band (rows outside band +
+ghosts go stale and are never read).  The exchange is point-to-point over
+torch.distributed: NCCL between GPUs (NVLink), gloo for the CPU tests.  A
+step overlaps it with the band's inner rows -- those whose gathers stay
+within the band -- and updates the edge rows once the ghost rows are in:
+with NCCL every wait is a dependency between CUDA streams, and the host never
+waits on the GPU within a step.
 """
 from __future__ import annotations
 
@@ -55,6 +59,9 @@ class RadiationRows:
     def step(self, n: int = 1):
         self.rad.step_async(n)
 
+    def step_rows(self, j_first: int, j_end: int, finish: bool):
+        self.rad.step_rows_async(j_first, j_end, finish)
+
     def energy(self) -> float:
         return self.rad.energy()  # grlbm_energy: the band's interior cells
 
@@ -91,30 +98,56 @@ class Slab:
             ops.append(dist.P2POp(dist.irecv, self.recv_hi, self.rank + 1, self.group))
         return ops
 
+    def _send(self):
+        """Packs the `ghost` rows at each edge of the band and starts their
+        exchange with the neighbours; returns the pending requests."""
+        lo, hi, g, st = self.band[0], self.band[1], self.ghost, self.state
+        if self.send_lo is not None:
+            st.copy_rows(lo, g, self.send_lo, True)
+        if self.send_hi is not None:
+            st.copy_rows(hi - g, g, self.send_hi, True)
+        return dist.batch_isend_irecv(self._ops())
+
+    def _receive(self, reqs):
+        """Waits for the exchange (NCCL: the state's stream waits) and
+        unpacks the neighbours' rows next to the band."""
+        lo, hi, g, st = self.band[0], self.band[1], self.ghost, self.state
+        for req in reqs:
+            req.wait()
+        if self.recv_lo is not None:
+            st.copy_rows(lo - g, g, self.recv_lo, False)
+        if self.recv_hi is not None:
+            st.copy_rows(hi, g, self.recv_hi, False)
+
     def exchange(self):
         """Sends the `ghost` rows at each edge of the band to the neighbour
         and receives the neighbour's rows next to the band."""
         if self.world == 1 or self.ghost == 0:
             return
-        lo, hi, g, st = self.band[0], self.band[1], self.ghost, self.state
-        ctx = torch.cuda.stream(st.stream) if st.stream is not None else _Null()
-        with ctx:
-            if self.send_lo is not None:
-                st.copy_rows(lo, g, self.send_lo, True)
-            if self.send_hi is not None:
-                st.copy_rows(hi - g, g, self.send_hi, True)
-            for req in dist.batch_isend_irecv(self._ops()):
-                req.wait()
-            if self.recv_lo is not None:
-                st.copy_rows(lo - g, g, self.recv_lo, False)
-            if self.recv_hi is not None:
-                st.copy_rows(hi, g, self.recv_hi, False)
+        st = self.state
+        with (torch.cuda.stream(st.stream) if st.stream is not None else _Null()):
+            self._receive(self._send())
 
     def step(self, n: int = 1):
-        """n time steps of the band, each after a ghost-row exchange."""
-        for _ in range(n):
-            self.exchange()
-            self.state.step(1)
+        """n time steps of the band.  Each starts the ghost-row exchange,
+        updates the inner rows [lo + g, hi - g) meanwhile (their gathers
+        read the band only), then, with the ghost rows in, the edge rows."""
+        st = self.state
+        if self.world == 1 or self.ghost == 0:
+            st.step(n)
+            return
+        lo, hi, g = self.band[0], self.band[1], self.ghost
+        edges = [(lo, min(lo + g, hi)), (max(hi - g, lo + g), hi)]
+        with (torch.cuda.stream(st.stream) if st.stream is not None else _Null()):
+            for _ in range(n):
+                reqs = self._send()
+                if lo + g < hi - g:
+                    st.step_rows(lo + g, hi - g, False)
+                self._receive(reqs)
+                for a, b in edges:
+                    if a < b:
+                        st.step_rows(a, b, False)
+                st.step_rows(hi, hi, True)
 
     def energy(self) -> float:
         """The global energy: the bands' FP64 sums added by one all-reduce."""
@@ -133,12 +166,24 @@ class _Null:
         return False
 
 
+def ghost_rows(local: int, device, world: int, group=None) -> int:
+    """The ghost depth all ranks use: the largest of the ranks' own
+    (grlbm_departure_rows over each band's cells)."""
+    if world == 1:
+        return local
+    t = torch.tensor([local], dtype=torch.int64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX, group=group)
+    return int(t.item())
+
+
 def open_slab(case: dict, precision: int, rank: int, world: int, device: int, group=None):
-    """A Radiation context for `case` on `device`, restricted to this rank's
-    band, with its exchange.  Returns (radiation, slab)."""
+    """A Radiation context for `case` on `device` that steps this rank's band
+    and builds the tables of its cells only, with its exchange.  Returns
+    (radiation, slab)."""
     G = __import__(__package__ or "2dradiation_b200")
-    rad = G.prepare(case, precision, device=device)
-    slab = Slab(RadiationRows(rad, torch.device("cuda", device)), rank, world, int(case["ny_"]),
-                rad.departure_rows(), group)
-    rad.set_rows(*slab.band)
+    band = partition(int(case["ny_"]), world)[rank]
+    rad = G.prepare(case, precision, device=device, rows=band)
+    dev = torch.device("cuda", device)
+    slab = Slab(RadiationRows(rad, dev), rank, world, int(case["ny_"]),
+                ghost_rows(rad.departure_rows(), dev, world, group), group)
     return rad, slab

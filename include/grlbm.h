@@ -205,6 +205,16 @@ int grlbm_step(grlbm_ctx *ctx, int32_t n_steps);
 /* Same, but only enqueues the work on the context's stream and returns
  * without waiting (for timing with events); grlbm_sync() waits. */
 int grlbm_step_async(grlbm_ctx *ctx, int32_t n_steps);
+/* No counterpart in the reference.  One step enqueued in parts: updates node
+ * rows [j_first, j_end) (within the band of grlbm_set_rows) of the next state
+ * from the current one, on the context's stream, without waiting; the first
+ * part of a step also applies the active sources.  finish = 1 ends the step
+ * (the next state becomes the current one); j_first == j_end with finish = 1
+ * only ends it.  The parts of one step must not overlap, and together cover
+ * the band.  A slab decomposition steps the band's inner rows while the
+ * rows next to it are being exchanged, and its edge rows after.  Not for
+ * adaptive streaming or tables rebuilt every step (GRLBM_ERR_UNSUPPORTED). */
+int grlbm_step_rows_async(grlbm_ctx *ctx, int64_t j_first, int64_t j_end, int32_t finish);
 int grlbm_sync(grlbm_ctx *ctx);
 /* The context's CUDA stream (a cudaStream_t), for callers that time or order
  * work around the library's launches. */
@@ -245,6 +255,11 @@ int grlbm_energy_noalloc(const double *E, int64_t nx_, int64_t ny_, double *tota
  * [j_first, j_end) only (1 <= j_first < j_end <= ny - 1; the default is all
  * interior rows). */
 int grlbm_set_rows(grlbm_ctx *ctx, int64_t j_first, int64_t j_end);
+/* (A table build -- grlbm_update_fourier_coefficients or
+ * grlbm_set_fourier_coefficients -- covers the interior cells of the band
+ * set at that time only; stepping a band outside them returns
+ * GRLBM_ERR_STATE.  Set the band first so that each rank builds its own
+ * cells' tables.) */
 /* Bytes of one node row of the intensity state over all directions:
  * nx * nDir * 8 for GRLBM_PLAIN_FP64; for GRLBM_PRECISION_FP32 with fixed
  * streaming nx * dp * 4, each node holding dp = (nDir + 4 rounded up to a

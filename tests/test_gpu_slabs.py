@@ -1,9 +1,12 @@
 """Slab decomposition on one GPU: three contexts of the same problem, each
-stepping one band of interior rows (grlbm_set_rows), exchange the rows next
-to their bands through grlbm_copy_rows before every step -- the exchange a
-multi-GPU run does over NCCL, here as device copies between contexts.  The
-bands together must reproduce the whole-grid run bit for bit, in both forms:
-every cell's arithmetic is the same, only where it runs differs."""
+stepping one band of interior rows (grlbm_set_rows) and building the tables
+of its band's cells only, exchange the rows next to their bands through
+grlbm_copy_rows before every step -- the exchange a multi-GPU run does over
+NCCL, here as device copies between contexts -- and step their bands in
+parts (grlbm_step_rows_async: inner rows, then the edge rows, as a rank
+does around its exchange).  The bands together must reproduce the
+whole-grid run bit for bit, in every form: each cell's arithmetic is the
+same, only where it runs differs."""
 import importlib
 
 import numpy as np
@@ -12,7 +15,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("precision", [0, 1, 2])
 @pytest.mark.parametrize("maker,kw", [
     ("curved_scatter", dict(nx_=64, ny_=45, n_dir=16, n_fourier=9, steps=12)),
     ("moving_scatter", dict(nx_=40, ny_=33, n_dir=24, n_fourier=5, steps=10)),
@@ -30,12 +33,10 @@ def test_bands_reproduce_whole_grid(grlbm, W, precision, maker, kw):
         ref_energy = whole.energy()
     world = 3
     bands = S.partition(int(case["ny_"]), world)
-    rads = [grlbm.prepare(case, precision) for _ in range(world)]
+    rads = [grlbm.prepare(case, precision, rows=b) for b in bands]
     try:
-        g = rads[0].departure_rows()
+        g = max(r.departure_rows() for r in rads)
         assert 1 <= g <= min(b - a for a, b in bands)
-        for r, b in zip(rads, bands):
-            r.set_rows(*b)
         dtype = torch.float32 if precision == 1 else torch.float64
         buf = torch.empty(g * rads[0].row_bytes() // dtype.itemsize, dtype=dtype, device="cuda")
         for _ in range(steps):
@@ -51,8 +52,13 @@ def test_bands_reproduce_whole_grid(grlbm, W, precision, maker, kw):
                 rads[k + 1].sync()
                 rads[k].copy_rows(lo_of_next, g, buf.data_ptr(), False)
                 rads[k].sync()
-            for r in rads:
-                r.step(1)
+            for r, (lo, hi) in zip(rads, bands):
+                parts = [(lo + g, hi - g), (lo, min(lo + g, hi)), (max(hi - g, lo + g), hi)]
+                for a, b in parts:
+                    if a < b:
+                        r.step_rows_async(a, b, False)
+                r.step_rows_async(hi, hi, True)
+                r.sync()
         nx = rads[0].nx
         for r, (lo, hi) in zip(rads, bands):
             m = r.moments_if()
@@ -67,3 +73,17 @@ def test_bands_reproduce_whole_grid(grlbm, W, precision, maker, kw):
     finally:
         for r in rads:
             r.close()
+
+
+def test_band_tables_cover_the_band_only(grlbm, W):
+    """Tables built for one band do not serve a wider one: stepping it is
+    refused until they are rebuilt."""
+    case = W.make_case("curved_shell", nx_=32, ny_=30, n_dir=12, n_fourier=5, steps=2)
+    with grlbm.prepare(case, 1, rows=(5, 12)) as r:
+        r.step(1)
+        r.set_rows(1, 31)
+        with pytest.raises(grlbm.GrlbmError) as e:
+            r.step(1)
+        assert e.value.code == 3
+        r.update_fourier_coefficients(case["rk_tol"])
+        r.step(1)

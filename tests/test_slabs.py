@@ -1,8 +1,9 @@
 """Slab decomposition host logic on CPU: the band partition, and the ghost-row
-exchange of 2dradiation_b200/slabs.py over gloo with two ranks, driving a
-CPU stand-in for a context whose step reads `ghost` rows around each cell.
-The two-rank run must equal the one-rank run bit for bit, as the GPU runs
-do (tests/test_gpu_slabs.py)."""
+exchange of 2dradiation_b200/slabs.py over gloo with two and three ranks,
+driving a CPU stand-in for a context whose step reads `ghost` rows around
+each cell.  Each step updates the band's inner rows while the exchange is
+in flight and its edge rows after it.  The multi-rank runs must equal the
+one-rank run bit for bit, as the GPU runs do (tests/test_gpu_slabs.py)."""
 import importlib
 import os
 import socket
@@ -55,15 +56,27 @@ class CpuRows:
         lo, hi = self.band
         return float(self.state[:, lo:hi, 1:-1].sum())
 
-    def step(self, n=1):
-        g, (lo, hi) = self.ghost, self.band
-        s = self.state
-        new = s.clone()
-        for j in range(lo, hi):
+    def _rows(self, new, j_first, j_end):
+        g, s = self.ghost, self.state
+        for j in range(j_first, j_end):
             rows = [min(max(j + k, 0), self.ny - 1) for k in range(-g, g + 1)]
             mix = sum((k + 2.0) * torch.roll(s[:, r, :], shifts=k, dims=1) for k, r in enumerate(rows))
             new[:, j, 1:-1] = (0.5 * s[:, j, 1:-1] + 0.5 * mix[:, 1:-1] / mix.abs().max())
-        self.state = new
+
+    def step(self, n=1):
+        for _ in range(n):
+            new = self.state.clone()
+            self._rows(new, *self.band)
+            self.state = new
+
+    def step_rows(self, j_first, j_end, finish):
+        """One step in parts (grlbm_step_rows_async): rows [j_first, j_end)
+        of the next state from the current one; finish swaps them in."""
+        if getattr(self, "_next", None) is None:
+            self._next = self.state.clone()
+        self._rows(self._next, j_first, j_end)
+        if finish:
+            self.state, self._next = self._next, None
 
 
 def _worker(rank, world, port, nx, ny_, nd, ghost, steps, out):
@@ -87,9 +100,11 @@ def _free_port():
         return s.getsockname()[1]
 
 
-@pytest.mark.parametrize("ghost", [1, 2])
-def test_two_rank_exchange_equals_one_rank(ghost):
-    nx, ny_, nd, steps = 9, 12, 3, 5
+@pytest.mark.parametrize("ghost,world,ny_", [(1, 2, 12), (2, 2, 12), (2, 3, 7), (3, 3, 11)])
+def test_multi_rank_exchange_equals_one_rank(ghost, world, ny_):
+    """(Bands of 2-4 rows with 2-3 ghost rows: the inner rows are empty or
+    single, the edge row ranges meet or overlap the band's middle.)"""
+    nx, nd, steps = 9, 3, 5
     S = slabs()
     single = CpuRows(nx + 2, ny_ + 2, nd, ghost, (1, ny_ + 1), seed=7)
     S.Slab(single, 0, 1, ny_, ghost).step(steps)
@@ -97,15 +112,16 @@ def test_two_rank_exchange_equals_one_rank(ghost):
     with ctx.Manager() as m:
         out = m.dict()
         port = _free_port()
-        procs = [ctx.Process(target=_worker, args=(r, 2, port, nx, ny_, nd, ghost, steps, out)) for r in range(2)]
+        procs = [ctx.Process(target=_worker, args=(r, world, port, nx, ny_, nd, ghost, steps, out))
+                 for r in range(world)]
         for p in procs:
             p.start()
         for p in procs:
             p.join(120)
             assert p.exitcode == 0
-        got = torch.cat([out[0], out[1]], dim=1)
-        energies = (out[("energy", 0)], out[("energy", 1)])
+        got = torch.cat([out[r] for r in range(world)], dim=1)
+        energies = [out[("energy", r)] for r in range(world)]
     assert torch.equal(got, single.state[:, 1:ny_ + 1, :])
-    # the all-reduced energy is the same on both ranks and is the whole grid's
-    assert energies[0] == energies[1]
+    # the all-reduced energy is the same on every rank and is the whole grid's
+    assert len(set(energies)) == 1
     assert abs(energies[0] - single.energy()) <= 1e-12 * abs(single.energy())
