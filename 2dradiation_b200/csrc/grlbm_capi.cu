@@ -97,6 +97,9 @@ struct grlbm_ctx
     // the band when they were built
     int64_t table_jlo = 0, table_jhi = 0;
     bool partial = false; // a step enqueued in row ranges (grlbm_step_rows_async) is open
+    // the tiled forms keep the records of the built cells only: rec and side
+    // hold cells [rec_c0, rec_c0 + rec.bytes / (record size * nd))
+    int64_t rec_c0 = 0;
     // config.updateFourierHarmonics: rebuild the tables before every step
     bool update_each_step = false;
     double update_tol = 1e-4;
@@ -313,8 +316,8 @@ Step32Args step32_args(grlbm_ctx *ctx, int from)
     a.ntiles = step32_tiles(ctx);
     a.Iin = ctx->I[from].as<float>();
     a.Iout = ctx->I[from ^ 1].as<float>();
-    a.rec = ctx->rec.as<uint4>();
-    a.side = ctx->side.as<float4>();
+    a.rec = ctx->rec.as<uint4>() - ctx->rec_c0 * a.nd;
+    a.side = ctx->side.as<float4>() - ctx->rec_c0 * a.nd;
     a.ia3 = ctx->ia3.as<float>();
     a.flags = ctx->flags.as<uint8_t>();
     a.u1 = ctx->cu1.as<float>();
@@ -353,8 +356,8 @@ Step64Args step64_args(grlbm_ctx *ctx, int from)
     a.ntiles = step32_tiles(ctx);
     a.Iin = ctx->I[from].as<double>();
     a.Iout = ctx->I[from ^ 1].as<double>();
-    a.rec = ctx->rec.as<double4>();
-    a.side = ctx->side.as<double4>();
+    a.rec = ctx->rec.as<double4>() - ctx->rec_c0 * a.nd;
+    a.side = ctx->side.as<double4>() - ctx->rec_c0 * a.nd;
     a.ia3 = ctx->ia3.as<double>();
     a.flags = ctx->flags.as<uint8_t>();
     a.u1 = ctx->cu1.as<double>();
@@ -610,11 +613,27 @@ int build_records(grlbm_ctx *ctx)
     da.alpha = ctx->alpha.as<double>();
     da.rot_c = approx_cos(0.0);
     da.rot_s = approx_sin(0.0);
+    if (ctx->fp32 || ctx->fast64)
+    {
+        // the cell-major records of the band's cells only, addressed by
+        // interior cell index through a base shifted by the first cell
+        const int64_t c0 = (ctx->gd.jlo - 1) * ctx->gd.nx_, cn = (ctx->gd.jhi - ctx->gd.jlo) * ctx->gd.nx_;
+        const size_t rs = ctx->fp32 ? sizeof(float4) : sizeof(double4);
+        void *old_rec = ctx->rec.p;
+        int rc = alloc(ctx, ctx->rec, (size_t)cn * ctx->st.n * rs);
+        if (!rc)
+            rc = alloc(ctx, ctx->side, (size_t)cn * ctx->st.n * rs);
+        if (rc)
+            return rc;
+        if (ctx->rec.p != old_rec || ctx->rec_c0 != c0)
+            invalidate_graphs(ctx); // captured steps hold the old records' base
+        ctx->rec_c0 = c0;
+    }
     da.rec64 = ctx->fp32 || ctx->fast64 ? nullptr : ctx->rec.as<double4>();
-    da.rec32 = ctx->fp32 ? ctx->rec.as<uint4>() : nullptr;
-    da.side32 = ctx->fp32 ? ctx->side.as<float4>() : nullptr;
-    da.recf = ctx->fast64 ? ctx->rec.as<double4>() : nullptr;
-    da.sidef = ctx->fast64 ? ctx->side.as<double4>() : nullptr;
+    da.rec32 = ctx->fp32 ? ctx->rec.as<uint4>() - ctx->rec_c0 * ctx->st.n : nullptr;
+    da.side32 = ctx->fp32 ? ctx->side.as<float4>() - ctx->rec_c0 * ctx->st.n : nullptr;
+    da.recf = ctx->fast64 ? ctx->rec.as<double4>() - ctx->rec_c0 * ctx->st.n : nullptr;
+    da.sidef = ctx->fast64 ? ctx->side.as<double4>() - ctx->rec_c0 * ctx->st.n : nullptr;
     da.q = ctx->dirs.q;
     da.p = ctx->dirs.p;
     for (int r = 0; r < ctx->dirs.q && r < kMaxRowTypes; r++)
@@ -1114,9 +1133,9 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
     if ((!ctx->fp32 && !ctx->fast64) || is_adaptive(ctx))
         TRY(alloc(ctx, ctx->streamed, (size_t)nxy * nd * tsize(ctx)));
     TRY(alloc(ctx, ctx->mom, (size_t)6 * nxy * tsize(ctx)));
-    TRY(alloc(ctx, ctx->rec, (size_t)ctx->ncell * nd * (ctx->fp32 ? sizeof(float4) : sizeof(double4))));
-    if (ctx->fp32 || ctx->fast64)
-        TRY(alloc(ctx, ctx->side, (size_t)ctx->ncell * nd * (ctx->fp32 ? sizeof(float4) : sizeof(double4))));
+    // (the tiled forms allocate their records with the first table build, for the band's cells)
+    if (!ctx->fp32 && !ctx->fast64)
+        TRY(alloc(ctx, ctx->rec, (size_t)ctx->ncell * nd * sizeof(double4)));
     TRY(alloc(ctx, ctx->counters, 8 * sizeof(unsigned long long)));
     TRY(alloc(ctx, ctx->tile_ctr, 2 * sizeof(unsigned)));
     cudaMemset(ctx->tile_ctr.p, 0, ctx->tile_ctr.bytes);
@@ -1152,9 +1171,8 @@ int grlbm_create(const grlbm_grid_desc *grid, const grlbm_metric_desc *metric, c
     }
     cudaMemset(ctx->mom.p, 0, ctx->mom.bytes);
     cudaMemset(ctx->counters.p, 0, ctx->counters.bytes);
-    cudaMemset(ctx->rec.p, 0, ctx->rec.bytes);
-    if (ctx->side.p)
-        cudaMemset(ctx->side.p, 0, ctx->side.bytes);
+    if (ctx->rec.p)
+        cudaMemset(ctx->rec.p, 0, ctx->rec.bytes);
     // fields default to zero (the reference's buffers are value-initialised)
     std::vector<double> zeros(nxy, 0.0);
     TRY(grlbm_set_fields(ctx, zeros.data(), zeros.data(), zeros.data(), zeros.data(), zeros.data(), zeros.data()));
