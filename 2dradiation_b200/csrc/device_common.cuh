@@ -6,30 +6,35 @@
 //                        -fmad=false (every product rounded once, as on the
 //                        reference's CPU)
 //   kernels_plain.cu     the plain FP64 step (stream + moments + collide),
-//                        LF moments, sources, energy -- FP64, -fmad=false; it
-//                        evaluates the reference's expressions in the
-//                        reference's association order, so identical inputs
-//                        give identical bits
-//   kernels_precision.cu the FP32 precision-form step -- contracted FMAs,
-//                        compact records, moment-space lambda iteration
+//                        LF moments, sources, energy, layout transposes --
+//                        FP64, -fmad=false; it evaluates the reference's
+//                        expressions in the reference's association order, so
+//                        identical inputs give identical bits
+//   kernels_step32.cu    the FP32 precision step of the fixed streaming types
+//                        and its batched form -- contracted FMAs, packed
+//                        records, moment-space lambda iteration
+//   kernels_step64.cu    the fast FP64 step of the fixed streaming types --
+//                        the same scheme in FP64, contracted FMAs
+//   kernels_precision.cu the FP32 precision step of the adaptive streaming
+//                        types
+//   adjoint.cu           the adjoint of the plain step
 //
 // Device layouts (one problem, all in HBM):
-//   intensities  I[d * plane + i + j * pitch]  direction-major, two buffers;
-//                                         FP64: pitch = nx, plane = nxy; FP32: pitch =
-//                                         nx rounded up to 4 floats, plane = pitch * ny
-//                                         (every row starts on a 16-byte boundary, as
-//                                         the step's TMA tensor copies need)
+//   plain state  I[d * nxy + ij]          direction-major FP64, two buffers
+//   FP32 adaptive state                   J[d * plane + i + j * pitch], rows
+//                                         padded to 16 bytes
+//   tiled states (FP32 fixed, fast FP64)  J[ij * dp + d], cell-major, directions
+//                                         0..3 repeated after the last (dp = nd + 4
+//                                         rounded up to 16 bytes); J = I / alpha^3
+//                                         for curved streaming
 //   plain record rec64[d * ncell + c]     {i_dep, j_dep, angle coordinate, s^3}
 //                                         (absolute grid coordinates of the
 //                                         departure point; angle < 0 marks a
 //                                         departure inside the excision)
-//   FP32 record  rec32[d * ncell + c]     {packed window word, fx, fy, s^3 alpha_c^3
-//                                         (0 when excised)}: see PackedRecord below
-//   FP32 side    side32[d * ncell + c]    {i_dep - i, j_dep - j, angle coordinate,
-//                                         s^3 alpha_c^3}, read only for departures
-//                                         the packed word marks as far
-//   FP32 state   J = I / alpha^3 for curved streaming (I for flat); the
-//                                         C-ABI converts at its boundary
+//   FP32 record  rec32[c * nd + d]        packed32 (below), with side records
+//                                         {i_dep - i, j_dep - j, angle coordinate,
+//                                         s^3 alpha_c^3} for far departures
+//   FP64 record  recf[c * nd + d]         packed64 (below), with FP64 side records
 //   rk fields    rkf[ij * kRkStride + f]  node-major pack of the 21 metric arrays
 //                                         the geodesic right-hand side reads and
 //                                         the 2x2 spatial tetrad blocks
@@ -71,8 +76,8 @@ constexpr int kMaxDirs = 256;
 constexpr int kMaxFourier = 64;
 
 // Directions 0..kStateMirror-1 repeated after the last direction in the
-// cell-major FP32 state, so that every 5-direction angular window of a node
-// is one contiguous run.
+// cell-major states, so that every 5-direction angular window of a node is
+// one contiguous run.
 constexpr int kStateMirror = 4;
 
 // Where intensity (node ij = i + j nx, direction d) sits in a state buffer:
