@@ -6,8 +6,11 @@
 //
 //   beam_demo nogpu               construct a RadiationB200; exit 0 when the
 //                                 constructor throws (prints the message)
-//   beam_demo flat|curved <dir>   run both classes in <dir>; print one line
-//                                 per compared buffer: name max|a-b| max|a|
+//   beam_demo flat|curved <dir> [precision]
+//                                 run both classes in <dir> (RadiationB200 in
+//                                 the given arithmetic form, default the
+//                                 plain one); print one line per compared
+//                                 buffer: name max|a-b| max|a|
 #include "RadiationB200.h"
 
 #include <unistd.h>
@@ -15,6 +18,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 
@@ -151,7 +155,7 @@ int run_nogpu()
     return 3;
 }
 
-int run_pair(bool curved)
+int run_pair(bool curved, int precision)
 {
     const Case c = make_case(curved);
     Grid grid(c.nx, c.ny, c.start, c.end);
@@ -165,7 +169,7 @@ int run_pair(bool curved)
     set_up(ref, c, grid, *metric, stencil);
     ref.RunSimulation();
 
-    RadiationB200 gpu(*metric, stencil, streaming, make_config(c, "b200", type));
+    RadiationB200 gpu(*metric, stencil, streaming, make_config(c, "b200", type), precision);
     set_up(gpu, c, grid, *metric, stencil);
     gpu.RunSimulation();
 
@@ -199,7 +203,7 @@ int main(int argc, char **argv)
         }
         try
         {
-            return run_pair(std::strcmp(argv[1], "curved") == 0);
+            return run_pair(std::strcmp(argv[1], "curved") == 0, argc >= 4 ? std::atoi(argv[3]) : GRLBM_PLAIN_FP64);
         }
         catch (const std::exception &e)
         {
@@ -207,6 +211,6 @@ int main(int argc, char **argv)
             return 4;
         }
     }
-    std::fprintf(stderr, "usage: beam_demo nogpu | flat <dir> | curved <dir>\n");
+    std::fprintf(stderr, "usage: beam_demo nogpu | flat <dir> [precision] | curved <dir> [precision]\n");
     return 2;
 }

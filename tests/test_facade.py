@@ -70,12 +70,15 @@ def read_frames(directory):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("precision", [0, 2])
 @pytest.mark.parametrize("kind", ["flat", "curved"])
-def test_facade_matches_reference_radiation(tmp_path, kind):
+def test_facade_matches_reference_radiation(tmp_path, kind, precision):
+    """The beams have no scattering, so the fast FP64 form (2) is held to the
+    plain form's 1e-12 as well."""
     exe = demo()
     work = tmp_path / "run"
     work.mkdir()
-    out = subprocess.run([exe, kind, str(work)], capture_output=True, text=True, timeout=600)
+    out = subprocess.run([exe, kind, str(work), str(precision)], capture_output=True, text=True, timeout=600)
     assert out.returncode == 0, out.stdout + out.stderr
     detail = out.stdout + out.stderr
     rows = {}
