@@ -237,7 +237,8 @@ def reference_root() -> str:
 
 def build(with_reference: bool | None = None, ref_root: str | None = None) -> None:
     """Build liboracle.so, and the reference libraries when the reference tree
-    is present (or when with_reference is True)."""
+    is present (or when with_reference is True).  With the reference, also the
+    beam demo of the C++ class (target `facade`) when libgrlbm.so exists."""
     import subprocess
     subprocess.run(["make", "-s", "-C", str(HERE), "oracle"], check=True)
     ref_root = ref_root or reference_root()
@@ -245,3 +246,5 @@ def build(with_reference: bool | None = None, ref_root: str | None = None) -> No
         with_reference = bool(ref_root) and os.path.isdir(os.path.join(ref_root, "src"))
     if with_reference:
         subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF={ref_root}"], check=True)
+        if (HERE.parent / "2dradiation_b200" / "libgrlbm.so").exists():
+            subprocess.run(["make", "-s", "-C", str(HERE), "facade", f"REF={ref_root}"], check=True)
