@@ -428,30 +428,31 @@ int set_step32_tile(grlbm_ctx *ctx, int tx, int ty)
     return GRLBM_OK;
 }
 
-// The default tile: the first candidate that keeps at least two blocks per
-// SM, else the first that fits at all.  In FP32, 16 cells fill phase 2's
-// lane pairs; in FP64 a 4x3 tile measured fastest at 400^2 x 64 (172 us per
-// step against 193 us for 4x2 and 243 us for 4x4, whose buffers leave room
-// for one block per SM only).
+// The default tile: the candidate with the most cells times resident blocks
+// per SM (counted up to two), the first in this order on a tie.  A tile
+// sweep at 400^2 curved scattering with 16 to 96 directions found this
+// rule's pick within 1% of the fastest in both tiled forms: 8x2 where 16-cell
+// tiles keep their occupancy, 4x4 for FP32 at 64 directions (8x2's wider
+// patch drops it to one block per SM: 128 against 91 us), 4x3 for FP64 at 64
+// directions (172 us, against 243-248 us for the 16-cell tiles at one block).
 int default_step32_tile(grlbm_ctx *ctx)
 {
-    static const int cand32[][2] = {{4, 4}, {8, 2}, {4, 2}, {2, 2}, {2, 1}, {1, 1}};
-    static const int cand64[][2] = {{4, 3}, {4, 2}, {2, 2}, {2, 1}, {1, 1}};
-    const int(*cand)[2] = ctx->fast64 ? cand64 : cand32;
-    const int ncand = ctx->fast64 ? 5 : 6;
-    for (int need = 2; need >= 1; need--)
-        for (int ci = 0; ci < ncand; ci++)
-        {
-            const int *c = cand[ci];
-            size_t smem = 0;
-            int per_sm = 0;
-            const int rc = tiled_fit(ctx, c[0], c[1], &smem, &per_sm);
-            if (rc)
-                return rc;
-            if (per_sm >= need)
-                return set_step32_tile(ctx, c[0], c[1]);
-        }
-    return fail(ctx, GRLBM_ERR_ARGUMENT, "no tile of %d directions fits on an SM", ctx->st.n);
+    static const int cand[][2] = {{8, 2}, {4, 4}, {16, 1}, {4, 3}, {3, 4}, {4, 2}, {2, 4}, {3, 3}, {2, 2}, {2, 1}, {1, 1}};
+    int best = -1, best_score = 0;
+    for (int ci = 0; ci < (int)(sizeof cand / sizeof cand[0]); ci++)
+    {
+        size_t smem = 0;
+        int per_sm = 0;
+        const int rc = tiled_fit(ctx, cand[ci][0], cand[ci][1], &smem, &per_sm);
+        if (rc)
+            return rc;
+        const int score = cand[ci][0] * cand[ci][1] * std::min(per_sm, 2);
+        if (score > best_score)
+            best = ci, best_score = score;
+    }
+    if (best < 0)
+        return fail(ctx, GRLBM_ERR_ARGUMENT, "no tile of %d directions fits on an SM", ctx->st.n);
+    return set_step32_tile(ctx, cand[best][0], cand[best][1]);
 }
 
 

@@ -276,11 +276,13 @@ int grlbm_row_bytes(const grlbm_ctx *ctx, int64_t *bytes);
 int grlbm_copy_rows(grlbm_ctx *ctx, int64_t j_first, int64_t n, void *buffer, int32_t to_buffer);
 /* ---- tiles of the tiled steps -----------------------------------------------
  * No counterpart in the reference.  The GRLBM_PRECISION_FP32 and
- * GRLBM_FAST_FP64 steps of the fixed streaming types run as warps that each take tiles of tile_x x
- * tile_y cells (at most 16), staging each tile's (tile_x + 2) x (tile_y + 2)
- * node patch of the state in shared memory.  The default tile is the first
- * of 4x4, 8x2, 4x2, 2x2, 2x1, 1x1 whose buffers leave room for two blocks
- * of the kernel per SM.  The result does not depend on the tile.
+ * GRLBM_FAST_FP64 steps of the fixed streaming types run as warps that each
+ * take tiles of tile_x x tile_y cells (at most 16), staging each tile's
+ * (tile_x + 2) x (tile_y + 2) node patch of the state in shared memory.  The
+ * default tile maximises its cells times the kernel's resident blocks per SM
+ * (counted up to two), over 8x2, 4x4, 16x1, 4x3, 3x4, 4x2, 2x4, 3x3, 2x2,
+ * 2x1, 1x1 in that order of preference.  The result does not depend on the
+ * tile.
  * GRLBM_ERR_ARGUMENT for more than 16 cells or buffers that do not fit in
  * shared memory; GRLBM_ERR_UNSUPPORTED for other contexts. */
 int grlbm_set_tile_shape(grlbm_ctx *ctx, int32_t tile_x, int32_t tile_y);
