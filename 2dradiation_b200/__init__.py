@@ -439,7 +439,8 @@ class Batch:
 
     def set_shape(self, blocks_per_sm: int, largest_first: bool = True):
         """blocks_per_sm >= 1: the persistent launch; 0: each problem's own
-        kernel, the problems' launches concurrent."""
+        kernel, the problems' launches concurrent; -m (m = 1..8): the same
+        with the grids cut to shares of m GPUs' worth of resident blocks."""
         self._c(lib().grlbm_batch_set_shape(self.h, int(blocks_per_sm), int(bool(largest_first))))
 
     def autotune(self, trial_steps: int = 4) -> dict:

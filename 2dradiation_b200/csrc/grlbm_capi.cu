@@ -429,11 +429,12 @@ int set_step32_tile(grlbm_ctx *ctx, int tx, int ty)
 }
 
 // The default tile: the candidate with the most cells times resident blocks
-// per SM (counted up to two), the first in this order on a tie.  A tile
-// sweep at 400^2 curved scattering with 16 to 96 directions found this
+// per SM (counted up to three), the first in this order on a tie.  Tile
+// sweeps at 400^2 curved scattering with 16 to 96 directions found this
 // rule's pick within 1% of the fastest in both tiled forms: 8x2 where 16-cell
-// tiles keep their occupancy, 4x4 for FP32 at 64 directions (8x2's wider
-// patch drops it to one block per SM: 128 against 91 us), 4x3 for FP64 at 64
+// tiles keep their occupancy; 4x4 for FP32 at 32 directions (three blocks
+// per SM against two for 8x2's wider patch: 64.5 against 72.6 us) and at 64
+// (8x2 drops to one block per SM: 128 against 91 us); 4x3 for FP64 at 64
 // directions (172 us, against 243-248 us for the 16-cell tiles at one block).
 int default_step32_tile(grlbm_ctx *ctx)
 {
@@ -446,7 +447,7 @@ int default_step32_tile(grlbm_ctx *ctx)
         const int rc = tiled_fit(ctx, cand[ci][0], cand[ci][1], &smem, &per_sm);
         if (rc)
             return rc;
-        const int score = cand[ci][0] * cand[ci][1] * std::min(per_sm, 2);
+        const int score = cand[ci][0] * cand[ci][1] * std::min(per_sm, 3);
         if (score > best_score)
             best = ci, best_score = score;
     }
@@ -2135,6 +2136,10 @@ int grlbm_host_metric_arrays(const grlbm_grid_desc *grid, const grlbm_metric_des
 } // extern "C"
 
 // ---------------------------------------------------------------- batches
+// the concurrent shapes share out at most this many GPUs' worth of resident
+// blocks (blocks_per_sm = -1 .. -kBatchMaxShare)
+constexpr int kBatchMaxShare = 8;
+
 struct grlbm_batch
 {
     std::string err;
@@ -2143,6 +2148,7 @@ struct grlbm_batch
     std::vector<grlbm_ctx *> ctx;
     std::vector<Batch32Item> items; // in launch order
     std::vector<int> order;         // items[k] is context order[k]
+    std::vector<int> grid;          // items[k]'s grid in the concurrent shapes
     DevBuf d_items, d_first, d_dirs, counters;
     int total_tiles = 0, passes = 1, warp_stride = 0, s_offset = 0, blocks_per_sm_max = 1, blocks_per_sm = 1, sms = 1;
     int item_bytes = 0; // each warp's copy of its problem's arguments and tables
@@ -2150,9 +2156,10 @@ struct grlbm_batch
     int largest_first = 0;
     int flip = 0; // parity of the steps taken since the items were built
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
-    // blocks_per_sm == 0: each problem's own step kernel, the problems'
+    // blocks_per_sm <= 0: each problem's own step kernel, the problems'
     // launch chains running concurrently on their streams, forked from and
-    // joined back to the batch stream by these events
+    // joined back to the batch stream by these events (below 0 with the
+    // grids cut to shares of -blocks_per_sm GPUs' worth of resident blocks)
     cudaEvent_t fork = nullptr;
     std::vector<cudaEvent_t> join;
     ~grlbm_batch()
@@ -2202,6 +2209,16 @@ void batch_drop_graphs(grlbm_batch *b)
             cudaGraphExecDestroy(g);
             g = nullptr;
         }
+}
+
+// A problem's estimated step time in arbitrary units: its cells times (its
+// directions + 48), times 1.6 for curved streaming.  The step kernel's rates
+// at 512^2 with 16, 32 and 64 directions fit a per-cell cost of a + b nd with
+// a between 40 and 57 b, curved streaming 1.5-1.75 times flat.
+double batch_cost(const grlbm_ctx *c)
+{
+    const bool curved = c->run.streaming_type == GRLBM_CURVED_FIXED;
+    return (double)c->ncell * (c->st.n + 48.0) * (curved ? 1.6 : 1.0);
 }
 
 // Passes, shared memory and occupancy of the persistent kernel for the
@@ -2266,6 +2283,22 @@ int batch_build(grlbm_batch *b)
         first[k + 1] = first[k] + step32_tiles(c);
     }
     b->total_tiles = first[n];
+    // the concurrent shapes' grids: each problem's own persistent grid, or
+    // (blocks_per_sm = -m) its share of m GPUs' worth of resident blocks by
+    // its estimated cost, so that the problems' kernels are resident side by
+    // side instead of each filling the GPU in turn
+    b->grid.assign(n, 0);
+    double wsum = 0.0;
+    for (int k = 0; k < n; k++)
+        wsum += batch_cost(b->ctx[order[k]]);
+    for (int k = 0; k < n; k++)
+    {
+        const grlbm_ctx *c = b->ctx[order[k]];
+        b->grid[k] = c->step_blocks;
+        if (b->blocks_per_sm < 0)
+            b->grid[k] = std::max(1, std::min(c->step_blocks, (int)std::ceil(-b->blocks_per_sm * c->step_blocks *
+                                                                             batch_cost(c) / wsum)));
+    }
     if (alloc(nullptr, b->d_items, n * sizeof(Batch32Item)) || alloc(nullptr, b->d_first, (n + 1) * sizeof(int)))
         return bfail(b, GRLBM_ERR_CUDA, "cannot allocate the batch launch list");
     BCU(cudaMemcpy(b->d_items.p, b->items.data(), n * sizeof(Batch32Item), cudaMemcpyHostToDevice));
@@ -2276,9 +2309,9 @@ int batch_build(grlbm_batch *b)
 }
 
 // Enqueue n steps of every problem on the batch stream, the first reading
-// the buffers of parity `flip`: one persistent launch per step, or (shape 0)
-// each problem's chain of step kernels on its own stream between a fork and
-// a join on the batch stream.
+// the buffers of parity `flip`: one persistent launch per step, or (shapes 0
+// and below) each problem's chain of step kernels on its own stream between a
+// fork and a join on the batch stream.
 int batch_enqueue(grlbm_batch *b, int n, int flip)
 {
     if (b->blocks_per_sm > 0)
@@ -2297,7 +2330,7 @@ int batch_enqueue(grlbm_batch *b, int n, int flip)
         BCU(cudaStreamWaitEvent(c->stream, b->fork, 0));
         for (int s = 0; s < n; s++)
             launch_step32(step32_args(c, b->items[k].cur0 ^ flip ^ (s & 1)), c->dirs, b->items[k].curved != 0,
-                          c->passes, c->step_blocks, c->stream);
+                          c->passes, b->grid[k], c->stream);
         BCU(cudaEventRecord(b->join[k], c->stream));
         BCU(cudaStreamWaitEvent(b->stream, b->join[k], 0));
     }
@@ -2315,6 +2348,31 @@ int batch_sync_state(grlbm_batch *b)
     return GRLBM_OK;
 }
 
+// Captures (once) the graph of kGraphSteps batch steps that starts from the
+// buffers of parity `flip`.
+int batch_graph(grlbm_batch *b, int flip)
+{
+    if (b->graph[flip])
+        return GRLBM_OK;
+    cudaGraph_t g = nullptr;
+    BCU(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    const int erc = batch_enqueue(b, kGraphSteps, flip);
+    cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+    if (erc)
+    {
+        if (g)
+            cudaGraphDestroy(g);
+        return erc;
+    }
+    if (e != cudaSuccess)
+        return bfail(b, GRLBM_ERR_CUDA, "batch graph capture failed: %s", cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&b->graph[flip], g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess)
+        return bfail(b, GRLBM_ERR_CUDA, "batch graph instantiation failed: %s", cudaGetErrorString(e));
+    return GRLBM_OK;
+}
+
 int batch_steps(grlbm_batch *b, int n)
 {
     for (grlbm_ctx *c : b->ctx)
@@ -2325,25 +2383,8 @@ int batch_steps(grlbm_batch *b, int n)
     int left = n;
     while (left >= kGraphSteps)
     {
-        if (!b->graph[b->flip])
-        {
-            cudaGraph_t g = nullptr;
-            BCU(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-            const int erc = batch_enqueue(b, kGraphSteps, b->flip);
-            cudaError_t e = cudaStreamEndCapture(b->stream, &g);
-            if (erc)
-            {
-                if (g)
-                    cudaGraphDestroy(g);
-                return erc;
-            }
-            if (e != cudaSuccess)
-                return bfail(b, GRLBM_ERR_CUDA, "batch graph capture failed: %s", cudaGetErrorString(e));
-            e = cudaGraphInstantiate(&b->graph[b->flip], g, 0);
-            cudaGraphDestroy(g);
-            if (e != cudaSuccess)
-                return bfail(b, GRLBM_ERR_CUDA, "batch graph instantiation failed: %s", cudaGetErrorString(e));
-        }
+        if ((rc = batch_graph(b, b->flip)))
+            return rc;
         BCU(cudaGraphLaunch(b->graph[b->flip], b->stream));
         left -= kGraphSteps; // even: parity unchanged
     }
@@ -2367,23 +2408,29 @@ int batch_steps(grlbm_batch *b, int n)
     return GRLBM_OK;
 }
 
-// Times `trial_steps` batch steps (after one untimed step); -1 on failure.
+// The time per step of `trial_steps` batch steps, rounded up to whole
+// graphs of kGraphSteps steps and replayed as grlbm_batch_step replays them,
+// after one untimed replay; -1 on failure.  (Each problem's launch chain in
+// the concurrent shapes spans a whole graph, so a shorter trial would time
+// mostly its tail.)
 float batch_time(grlbm_batch *b, int trial_steps, cudaEvent_t e0, cudaEvent_t e1, int *rc)
 {
-    if ((*rc = batch_build(b)) || (*rc = batch_enqueue(b, 1, 0)))
+    if ((*rc = batch_build(b)) || (*rc = batch_graph(b, 0)))
         return -1.f;
-    cudaEventRecord(e0, b->stream);
-    if ((*rc = batch_enqueue(b, trial_steps, 1)))
-        return -1.f;
-    cudaEventRecord(e1, b->stream);
-    if (cudaStreamSynchronize(b->stream) != cudaSuccess)
+    const int reps = (trial_steps + kGraphSteps - 1) / kGraphSteps;
+    bool ok = cudaGraphLaunch(b->graph[0], b->stream) == cudaSuccess &&
+              cudaEventRecord(e0, b->stream) == cudaSuccess;
+    for (int r = 0; r < reps && ok; r++)
+        ok = cudaGraphLaunch(b->graph[0], b->stream) == cudaSuccess;
+    ok = ok && cudaEventRecord(e1, b->stream) == cudaSuccess;
+    if (cudaStreamSynchronize(b->stream) != cudaSuccess || !ok)
     {
         *rc = bfail(b, GRLBM_ERR_CUDA, "autotune: trial steps failed");
         return -1.f;
     }
     float ms = 0.f;
     cudaEventElapsedTime(&ms, e0, e1);
-    return ms;
+    return ms / (float)(reps * kGraphSteps);
 }
 } // namespace
 
@@ -2474,8 +2521,9 @@ int grlbm_batch_set_shape(grlbm_batch *b, int32_t blocks_per_sm, int32_t largest
     int rc = batch_geometry(b);
     if (rc)
         return rc;
-    if (blocks_per_sm < 0 || blocks_per_sm > b->blocks_per_sm_max)
-        return bfail(b, GRLBM_ERR_ARGUMENT, "blocks_per_sm must be in [0, %d]", b->blocks_per_sm_max);
+    if (blocks_per_sm < -kBatchMaxShare || blocks_per_sm > b->blocks_per_sm_max)
+        return bfail(b, GRLBM_ERR_ARGUMENT, "blocks_per_sm must be in [%d, %d]", -kBatchMaxShare,
+                     b->blocks_per_sm_max);
     for (grlbm_ctx *c : b->ctx)
         BCU(cudaStreamSynchronize(c->stream));
     b->blocks_per_sm = blocks_per_sm;
@@ -2516,14 +2564,16 @@ int grlbm_batch_autotune(grlbm_batch *b, int32_t trial_steps, int32_t *blocks_pe
     BCU(cudaEventCreate(&e1));
     // 1. the launch shape: persistent launches (largest problem first or not,
     //    at each resident block count down to two below the limit), or the
-    //    problems' own kernels launched concurrently
+    //    problems' own kernels launched concurrently, with their own grids or
+    //    with shares of one to kBatchMaxShare GPUs' worth of resident blocks
     float best = -1.f;
     int best_bps = b->blocks_per_sm, best_lf = b->largest_first;
     std::vector<std::pair<int, int>> shapes;
     for (int lf = 0; lf <= 1; lf++)
         for (int bps = b->blocks_per_sm_max; bps >= 1 && bps >= b->blocks_per_sm_max - 2; bps--)
             shapes.emplace_back(bps, lf);
-    shapes.emplace_back(0, 1);
+    for (int m = 0; m <= kBatchMaxShare; m++)
+        shapes.emplace_back(-m, 1);
     for (const auto &shape : shapes)
     {
         b->blocks_per_sm = shape.first;
@@ -2538,9 +2588,14 @@ int grlbm_batch_autotune(grlbm_batch *b, int32_t trial_steps, int32_t *blocks_pe
     b->largest_first = best_lf;
     // 2. the tile of each size class (problems of one grid size and
     //    direction count share a tile), largest class first: each class tries
-    //    the candidate tiles with the others fixed, and keeps the fastest
+    //    the candidate tiles with the others fixed, and keeps the fastest.
+    //    Classes below 2% of the batch's estimated cost keep their tiles: their
+    //    share of a trial is within its noise.
     if (!rc)
     {
+        double wsum = 0.0;
+        for (grlbm_ctx *c : b->ctx)
+            wsum += batch_cost(c);
         std::vector<std::pair<int64_t, std::vector<grlbm_ctx *>>> classes;
         for (grlbm_ctx *c : b->ctx)
         {
@@ -2560,6 +2615,11 @@ int grlbm_batch_autotune(grlbm_batch *b, int32_t trial_steps, int32_t *blocks_pe
         {
             grlbm_ctx *c0 = cls.second[0];
             int bx = c0->tile_x, by = c0->tile_y;
+            double wc = 0.0;
+            for (grlbm_ctx *c : cls.second)
+                wc += batch_cost(c);
+            if (wc < 0.02 * wsum)
+                continue;
             for (const auto &t : cand)
             {
                 if (t[0] == bx && t[1] == by)

@@ -51,8 +51,14 @@
 #include "device_common.cuh"
 #include "step_common.cuh"
 
+// resident blocks per SM the single-problem kernel is compiled for: three
+// at one pass (at most 112 registers; 16 and 32 directions step 8-12% faster
+// than at two blocks), two at more passes (at three their registers spill)
 #ifndef GRLBM_STEP32_MIN_BLOCKS
 #define GRLBM_STEP32_MIN_BLOCKS 2
+#endif
+#ifndef GRLBM_STEP32_MIN_BLOCKS_1
+#define GRLBM_STEP32_MIN_BLOCKS_1 3
 #endif
 
 namespace grlbm
@@ -640,7 +646,7 @@ __device__ __forceinline__ void step_unit32(const Step32Args &a, const DT &dt, c
 __device__ __forceinline__ int step32_header(int nd) { return kRowtabOffset + kMaxRowTypes * 12 * 4 + 32 * nd; }
 
 template <bool CURVED, int P, bool H>
-__global__ void __launch_bounds__(kThreads, GRLBM_STEP32_MIN_BLOCKS)
+__global__ void __launch_bounds__(kThreads, P == 1 ? GRLBM_STEP32_MIN_BLOCKS_1 : GRLBM_STEP32_MIN_BLOCKS)
     k_step_prec(const __grid_constant__ Step32Args a, const __grid_constant__ DirTable dt, int warp_stride)
 {
     extern __shared__ __align__(16) unsigned char smem[];

@@ -294,8 +294,8 @@ int grlbm_departure_rows(grlbm_ctx *ctx, int32_t *rows);
 /* ---- batches ----------------------------------------------------------------
  * No counterpart in the reference.  Many GRLBM_PRECISION_FP32 problems on one
  * GPU (any grid sizes, direction counts, flat or curved streaming) stepped
- * together, replayed from CUDA graphs of 32 steps, in one of two launch
- * shapes: one persistent kernel launch per time step over all problems'
+ * together, replayed from CUDA graphs of 32 steps, in one of two kinds of
+ * launch shape: one persistent kernel launch per time step over all problems'
  * tiles, or each problem's own step kernel with the problems' launch chains
  * running concurrently inside the graph.  Each problem's result is
  * bit-identical to stepping it alone; its
@@ -313,15 +313,23 @@ const char *grlbm_batch_last_error(const grlbm_batch *batch);
 int grlbm_batch_step(grlbm_batch *batch, int32_t n_steps);
 /* Sets the launch shape: blocks_per_sm in [1, occupancy limit] for the
  * persistent launch (with the problems' tiles as given or largest problem
- * first), or 0 for the problems' own kernels launched concurrently. */
+ * first); 0 for the problems' own kernels launched concurrently, each on its
+ * own persistent grid; -m (m = 1..8) for the same concurrent launches with
+ * problem k's grid cut to ceil(m G_k w_k / sum w), at least one block, where
+ * G_k is its own grid (its kernel's resident blocks on every SM) and w_k its
+ * estimated cost (cells x (directions + 48), x 1.6 for curved streaming):
+ * m GPUs' worth of resident blocks shared out, so that the problems' kernels
+ * run side by side instead of each filling the GPU in turn. */
 int grlbm_batch_set_shape(grlbm_batch *batch, int32_t blocks_per_sm, int32_t largest_first);
-/* Times trial_steps steps for each launch shape -- the persistent launch at
- * resident blocks per SM (the occupancy limit and up to two fewer) with the
- * problems in the order given or largest problem first, and the concurrent
- * launches (0) -- and keeps the fastest; then, per size class (problems of
- * one grid size and direction count), largest class first, times candidate
- * tile shapes (grlbm_set_tile_shape) with the other classes fixed and keeps
- * the fastest.  Every problem is put back in the state it had before the
+/* Times trial_steps steps (rounded up to whole 32-step graphs, replayed as
+ * grlbm_batch_step replays them, after an untimed one) for each launch shape
+ * -- the persistent launch at resident blocks per SM (the occupancy limit and
+ * up to two fewer) with the problems in the order given or largest problem
+ * first, and the concurrent launches (0, -1, ..., -8) -- and keeps the
+ * fastest; then, per size class (problems of one grid size and direction
+ * count) holding at least 2% of the batch's estimated cost, largest class
+ * first, times candidate tile shapes (grlbm_set_tile_shape) with the other
+ * classes fixed and keeps the fastest.  Every problem is put back in the state it had before the
  * call.  The launch shape is returned in *blocks_per_sm and *largest_first
  * (either may be NULL), the tiles by grlbm_get_tile_shape. */
 int grlbm_batch_autotune(grlbm_batch *batch, int32_t trial_steps, int32_t *blocks_per_sm, int32_t *largest_first);

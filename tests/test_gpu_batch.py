@@ -23,7 +23,7 @@ def test_batch_matches_single_problems(grlbm, W):
     try:
         with grlbm.Batch(probs) as b:
             choice = b.autotune(3)
-            assert choice["blocks_per_sm"] >= 0
+            assert -8 <= choice["blocks_per_sm"]
             b.step(37)          # one 32-step graph and 5 single launches
             probs[0].step(1)    # a problem stepped on its own in between
             b.step(6)
@@ -36,10 +36,12 @@ def test_batch_matches_single_problems(grlbm, W):
             r.close()
 
 
-@pytest.mark.parametrize("shape", [(0, True), (1, False), (5, True)])
+@pytest.mark.parametrize("shape", [(0, True), (-1, True), (-3, False), (1, False), (5, True)])
 def test_batch_shapes_match_single_problems(grlbm, W, shape):
-    """Each launch shape, set explicitly: the concurrent launches (0) and the
-    persistent launch at 1 and 5 blocks per SM (capped at the occupancy limit)."""
+    """Each launch shape, set explicitly: the concurrent launches on the
+    problems' own grids (0) and on shares of one and three GPUs' worth of
+    resident blocks (-1, -3), and the persistent launch at 1 and 5 blocks per
+    SM (capped at the occupancy limit); -9 is refused."""
     cases = W.batch_instances(count=5, seed=21, sizes=(24, 37, 64), dirs=(8, 16, 32), steps=40)
     P = grlbm.PRECISION_FP32
     ref = []
@@ -57,6 +59,9 @@ def test_batch_shapes_match_single_problems(grlbm, W, shape):
                 assert bps > 1  # above this kernel's occupancy limit
                 b.set_shape(1, lf)
             b.step(35)  # one 32-step graph and 3 single steps
+            with pytest.raises(grlbm.GrlbmError) as e:
+                b.set_shape(-9, True)
+            assert e.value.code == 1
         for k, (r, I) in enumerate(zip(probs, ref)):
             assert np.array_equal(r.intensity(), I), k
     finally:
