@@ -307,8 +307,9 @@ def run_batched(G, W, a, local):
             "value": units * a.batch_steps / batch_s, "unit": UNIT,
             "separate_contexts": units * a.batch_steps / single_s, "autotune": choice,
             "timing": "host clock around the synchronous batch step (the autotuned launch shape: blocks_per_sm 0 = "
-                      "the problems' own kernels launched concurrently, else one persistent launch per step; "
-                      "32-step graphs), after an untimed round"}
+                      "the problems' own kernels launched concurrently, -m = the same on cost-weighted shares of m "
+                      "GPUs' worth of resident blocks, >= 1 = one persistent launch per step; 32-step graphs), "
+                      "after an untimed round"}
 
 
 def run_adjoint(G, W, a, local):
