@@ -187,16 +187,37 @@ def hbm_peak():
     return FALLBACK_HBM_GBS, "fallback"
 
 
-def profiled_traffic(kernel: str):
-    """DRAM bytes per launch of `kernel` from the committed ncu summary, if any."""
+def profiled_traffic(kernel: str, key: str = "dram_bytes_per_launch"):
+    """DRAM bytes per launch of `kernel` (or another per-launch figure, `key`)
+    from the committed ncu summary, if any."""
     p = ROOT / "profiles" / "traffic.json"
     if not p.exists():
         return None
     try:
         d = json.loads(p.read_text())
-        return d.get(kernel, {}).get("dram_bytes_per_launch")
+        return d.get(kernel, {}).get(key)
     except (ValueError, OSError):
         return None
+
+
+# FP64 peak of a B200: 148 SMs x 64 FP64 FMA lanes x 2 FLOP x 1.965 GHz
+FP64_PEAK_TFLOPS_NOMINAL = 148 * 64 * 2 * 1.965e9 / 1e12
+
+
+def table_build_line(fp32):
+    """The geodesic table build of the bench workload: its time, its RK45
+    trials, and its FP64 rate over the whole build from the FP64 operations
+    ncu counted in k_geodesic at this workload (DADD + DMUL + 2 DFMA)."""
+    flop = profiled_traffic("k_geodesic", "fp64_flop_per_launch")
+    ms = fp32["table_ms"]
+    out = {"ms": ms, "rk_substeps": fp32["rk_substeps"], "fp64_flop": flop,
+           "achieved_fp64_tflops": flop / (ms * 1e-3) / 1e12 if flop and ms > 0 else None,
+           "fp64_peak_tflops_nominal": FP64_PEAK_TFLOPS_NOMINAL,
+           "note": "k_geodesic + k_fourier_project + k_departure, CUDA events; FP64 operations from the committed "
+                   "ncu count of k_geodesic (built without contraction, as the reference rounds)"}
+    if out["achieved_fp64_tflops"]:
+        out["fp64_frac_nominal"] = out["achieved_fp64_tflops"] / FP64_PEAK_TFLOPS_NOMINAL
+    return out
 
 
 def time_steps(G, r, steps: int, warmup: int, flush, advance):
@@ -592,6 +613,7 @@ def run_grlbm(a, world, rank, local, pg):
         / max(fp64["iters"]["average_iterations"], 1e-30),
         "accuracy": accuracy,
         "table_build_ms": {"fp32": fp32["table_ms"], "fp64": fp64["table_ms"], "fast64": fast["table_ms"]},
+        "table_build": table_build_line(fp32),
         "lambda_iterations": {"fp32_avg": fp32["iters"]["average_iterations"],
                               "fp64_avg": fp64["iters"]["average_iterations"],
                               "fast64_avg": fast["iters"]["average_iterations"],
