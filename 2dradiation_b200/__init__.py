@@ -417,9 +417,10 @@ class Adjoint:
 
 
 class Batch:
-    """Several precision-form problems stepped together (grlbm_batch_*): one
-    persistent launch per step, or the problems' own kernels launched
-    concurrently.  The Radiation objects stay usable."""
+    """Several problems stepped together (grlbm_batch_*): the problems' own
+    steps launched concurrently (any forms), or one persistent launch per
+    step (FP32 fixed streaming without active sources).  The Radiation
+    objects stay usable."""
 
     def __init__(self, problems: list):
         self.problems = list(problems)
@@ -439,8 +440,9 @@ class Batch:
 
     def set_shape(self, blocks_per_sm: int, largest_first: bool = True):
         """blocks_per_sm >= 1: the persistent launch; 0: each problem's own
-        kernel, the problems' launches concurrent; -m (m = 1..8): the same
-        with the grids cut to shares of m GPUs' worth of resident blocks."""
+        step, the problems' launches concurrent; -m (m = 1..8): the same
+        with the tiled forms' grids cut to shares of m GPUs' worth of
+        resident blocks (the default, -4)."""
         self._c(lib().grlbm_batch_set_shape(self.h, int(blocks_per_sm), int(bool(largest_first))))
 
     def autotune(self, trial_steps: int = 4) -> dict:

@@ -519,17 +519,20 @@ int check_tables(grlbm_ctx *ctx)
 
 // Enqueue one step starting from buffer `from` (no sync).
 // (sources: LoadInitialData at the top of the step; off for the second and
-// later row ranges of a step enqueued in parts)
-int enqueue_step(grlbm_ctx *ctx, int from, bool sources = true)
+// later row ranges of a step enqueued in parts.  blocks: the tiled forms'
+// grid, 0 for the context's own)
+int enqueue_step(grlbm_ctx *ctx, int from, bool sources = true, int blocks = 0)
 {
     const bool curved = is_curved(ctx);
+    if (blocks <= 0)
+        blocks = ctx->step_blocks;
     unsigned long long *cnt = ctx->counters.as<unsigned long long>();
     if (ctx->fast64)
     {
         if (sources && ctx->run.keep_source_nodes_active && ctx->nsrc > 0)
             launch_sources64L(ctx->I[from].as<double>(), ctx->sl, ctx->st.n, ctx->src_nodes.as<int64_t>(),
                               ctx->src_vals.as<double>(), ctx->nsrc, ctx->stream);
-        launch_step64(step64_args(ctx, from), ctx->dirs64t.as<DirTable64>(), curved, ctx->passes, ctx->step_blocks,
+        launch_step64(step64_args(ctx, from), ctx->dirs64t.as<DirTable64>(), curved, ctx->passes, blocks,
                       ctx->stream);
     }
     else if (ctx->fp32)
@@ -538,7 +541,7 @@ int enqueue_step(grlbm_ctx *ctx, int from, bool sources = true)
             launch_sources32(ctx->I[from].as<float>(), ctx->sl, ctx->st.n, ctx->src_nodes.as<int64_t>(),
                              ctx->src_vals.as<float>(), ctx->nsrc, ctx->stream);
         if (!is_adaptive(ctx))
-            launch_step32(step32_args(ctx, from), ctx->dirs, curved, ctx->passes, ctx->step_blocks, ctx->stream);
+            launch_step32(step32_args(ctx, from), ctx->dirs, curved, ctx->passes, blocks, ctx->stream);
         else
         {
             PrecStepArgs a = prec_args(ctx, from);
@@ -2139,6 +2142,9 @@ int grlbm_host_metric_arrays(const grlbm_grid_desc *grid, const grlbm_metric_des
 // the concurrent shapes share out at most this many GPUs' worth of resident
 // blocks (blocks_per_sm = -1 .. -kBatchMaxShare)
 constexpr int kBatchMaxShare = 8;
+// a new batch's shape: the concurrent launches on shares of this many GPUs
+// (the fastest on the 64-problem benchmark batch, with 6)
+constexpr int kBatchDefaultShare = 4;
 
 struct grlbm_batch
 {
@@ -2152,6 +2158,10 @@ struct grlbm_batch
     DevBuf d_items, d_first, d_dirs, counters;
     int total_tiles = 0, passes = 1, warp_stride = 0, s_offset = 0, blocks_per_sm_max = 1, blocks_per_sm = 1, sms = 1;
     int item_bytes = 0; // each warp's copy of its problem's arguments and tables
+    // every problem is an FP32 fixed-streaming one without active sources:
+    // the persistent kernel can step the batch (else only the concurrent
+    // shapes, which run each problem's own step)
+    bool persistent_ok = true;
     size_t smem = 0;
     int largest_first = 0;
     int flip = 0; // parity of the steps taken since the items were built
@@ -2212,19 +2222,34 @@ void batch_drop_graphs(grlbm_batch *b)
 }
 
 // A problem's estimated step time in arbitrary units: its cells times (its
-// directions + 48), times 1.6 for curved streaming.  The step kernel's rates
-// at 512^2 with 16, 32 and 64 directions fit a per-cell cost of a + b nd with
-// a between 40 and 57 b, curved streaming 1.5-1.75 times flat.
+// directions + 48), times 1.6 for curved streaming, times its form's cost
+// against the FP32 fixed-streaming step.  The FP32 step's rates at 512^2 with
+// 16, 32 and 64 directions fit a per-cell cost of a + b nd with a between 40
+// and 57 b, curved streaming 1.5-1.75 times flat; at 400^2 x 64 the fast FP64
+// step takes 1.9 times as long, the plain FP64 step 4.7 times, and adaptive
+// streaming 4.9 (FP32) and 10.9 (plain) times.
 double batch_cost(const grlbm_ctx *c)
 {
-    const bool curved = c->run.streaming_type == GRLBM_CURVED_FIXED;
-    return (double)c->ncell * (c->st.n + 48.0) * (curved ? 1.6 : 1.0);
+    const bool curved = is_curved(c);
+    double form = 1.0;
+    if (c->fast64)
+        form = 1.9;
+    else if (is_adaptive(c))
+        form = c->fp32 ? 4.9 : 10.9;
+    else if (!c->fp32)
+        form = 4.7;
+    return (double)c->ncell * (c->st.n + 48.0) * (curved ? 1.6 : 1.0) * form;
 }
 
 // Passes, shared memory and occupancy of the persistent kernel for the
 // problems' current tile shapes.
 int batch_geometry(grlbm_batch *b)
 {
+    if (!b->persistent_ok)
+    {
+        b->blocks_per_sm_max = 0;
+        return GRLBM_OK;
+    }
     // each warp's buffer: the largest patch of the problems, then the largest
     // streamed-value rows
     b->passes = 1;
@@ -2262,10 +2287,8 @@ int batch_build(grlbm_batch *b)
     for (int k = 0; k < n; k++)
         order[k] = k;
     if (b->largest_first)
-        std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
-            const grlbm_ctx *a = b->ctx[x], *c = b->ctx[y];
-            return a->ncell * a->st.n > c->ncell * c->st.n;
-        });
+        std::stable_sort(order.begin(), order.end(),
+                         [&](int x, int y) { return batch_cost(b->ctx[x]) > batch_cost(b->ctx[y]); });
     b->order = order;
     b->items.assign(n, Batch32Item{});
     std::vector<int> first(n + 1, 0);
@@ -2274,13 +2297,16 @@ int batch_build(grlbm_batch *b)
     {
         grlbm_ctx *c = b->ctx[order[k]];
         Batch32Item &it = b->items[k];
+        it.cur0 = c->cur;
+        first[k + 1] = first[k];
+        if (!b->persistent_ok)
+            continue; // the concurrent shapes read cur0 only
         it.a[0] = step32_args(c, 0);
         it.a[1] = step32_args(c, 1);
         it.dt = dirs + order[k];
         it.curved = c->run.streaming_type == GRLBM_CURVED_FIXED;
-        it.cur0 = c->cur;
         it.mode = step32_mode(c->st.n);
-        first[k + 1] = first[k] + step32_tiles(c);
+        first[k + 1] += step32_tiles(c);
     }
     b->total_tiles = first[n];
     // the concurrent shapes' grids: each problem's own persistent grid, or
@@ -2295,7 +2321,7 @@ int batch_build(grlbm_batch *b)
     {
         const grlbm_ctx *c = b->ctx[order[k]];
         b->grid[k] = c->step_blocks;
-        if (b->blocks_per_sm < 0)
+        if (b->blocks_per_sm < 0 && is_tiled(c)) // the other forms' grids cover their work once
             b->grid[k] = std::max(1, std::min(c->step_blocks, (int)std::ceil(-b->blocks_per_sm * c->step_blocks *
                                                                              batch_cost(c) / wsum)));
     }
@@ -2329,8 +2355,8 @@ int batch_enqueue(grlbm_batch *b, int n, int flip)
         grlbm_ctx *c = b->ctx[b->order[k]];
         BCU(cudaStreamWaitEvent(c->stream, b->fork, 0));
         for (int s = 0; s < n; s++)
-            launch_step32(step32_args(c, b->items[k].cur0 ^ flip ^ (s & 1)), c->dirs, b->items[k].curved != 0,
-                          c->passes, b->grid[k], c->stream);
+            if (enqueue_step(c, b->items[k].cur0 ^ flip ^ (s & 1), true, b->grid[k]))
+                return bfail(b, GRLBM_ERR_CUDA, "problem %zu: %s", k, c->err.c_str());
         BCU(cudaEventRecord(b->join[k], c->stream));
         BCU(cudaStreamWaitEvent(b->stream, b->join[k], 0));
     }
@@ -2448,18 +2474,18 @@ int grlbm_batch_create(grlbm_ctx *const *ctxs, int32_t n, grlbm_batch **out)
         grlbm_ctx *c = ctxs[k];
         if (!c)
             return bfail(nullptr, GRLBM_ERR_ARGUMENT, "grlbm_batch_create: context %d is null", k);
-        if (!c->fp32)
-            return bfail(nullptr, GRLBM_ERR_UNSUPPORTED, "grlbm_batch_create: context %d is not GRLBM_PRECISION_FP32", k);
         if (c->device != ctxs[0]->device)
             return bfail(nullptr, GRLBM_ERR_ARGUMENT, "grlbm_batch_create: contexts on different devices");
-        if (c->run.streaming_type == GRLBM_CURVED_FIXED && !c->tables)
+        if (is_curved(c) && !c->tables)
             return bfail(nullptr, GRLBM_ERR_STATE, "grlbm_batch_create: context %d has no geodesic tables", k);
-        if (c->run.keep_source_nodes_active && c->nsrc > 0)
+        if (c->update_each_step)
             return bfail(nullptr, GRLBM_ERR_UNSUPPORTED,
-                         "grlbm_batch_create: context %d keeps source nodes active (not batched)", k);
-        if (is_adaptive(c))
-            return bfail(nullptr, GRLBM_ERR_UNSUPPORTED,
-                         "grlbm_batch_create: context %d streams adaptively (not batched)", k);
+                         "grlbm_batch_create: context %d rebuilds its tables every step (not batched)", k);
+        if (c->partial)
+            return bfail(nullptr, GRLBM_ERR_STATE, "grlbm_batch_create: context %d is inside a step taken in row ranges",
+                         k);
+        if (!is_fixed32(c) || (c->run.keep_source_nodes_active && c->nsrc > 0))
+            b->persistent_ok = false;
         for (int j = 0; j < k; j++)
             if (ctxs[j] == c)
                 return bfail(nullptr, GRLBM_ERR_ARGUMENT, "grlbm_batch_create: context %d appears twice", k);
@@ -2484,7 +2510,8 @@ int grlbm_batch_create(grlbm_ctx *const *ctxs, int32_t n, grlbm_batch **out)
     int rc = batch_geometry(b);
     if (rc)
         return bfail(nullptr, rc, "%s", b->err.c_str());
-    b->blocks_per_sm = b->blocks_per_sm_max;
+    b->blocks_per_sm = -kBatchDefaultShare;
+    b->largest_first = 1;
     if ((rc = batch_build(b)))
         return bfail(nullptr, rc, "%s", b->err.c_str());
     *out = owner.release();
@@ -2521,6 +2548,9 @@ int grlbm_batch_set_shape(grlbm_batch *b, int32_t blocks_per_sm, int32_t largest
     int rc = batch_geometry(b);
     if (rc)
         return rc;
+    if (blocks_per_sm > 0 && !b->persistent_ok)
+        return bfail(b, GRLBM_ERR_UNSUPPORTED,
+                     "the persistent launch steps FP32 fixed-streaming problems without active sources only");
     if (blocks_per_sm < -kBatchMaxShare || blocks_per_sm > b->blocks_per_sm_max)
         return bfail(b, GRLBM_ERR_ARGUMENT, "blocks_per_sm must be in [%d, %d]", -kBatchMaxShare,
                      b->blocks_per_sm_max);
@@ -2543,20 +2573,22 @@ int grlbm_batch_autotune(grlbm_batch *b, int32_t trial_steps, int32_t *blocks_pe
     int rc = batch_sync_state(b);
     if (rc)
         return rc;
-    // save every problem's state (current intensities, moments, counters);
-    // the trial steps are undone afterwards
-    const size_t n = b->ctx.size();
-    std::vector<std::unique_ptr<DevBuf>> saved(3 * n);
-    for (size_t k = 0; k < n; k++)
+    // save every problem's state (current intensities, and rotation angles
+    // for adaptive streaming; moments, counters); the trial steps are undone
+    // afterwards
+    std::vector<std::pair<DevBuf *, std::unique_ptr<DevBuf>>> saved;
+    for (grlbm_ctx *c : b->ctx)
     {
-        grlbm_ctx *c = b->ctx[k];
-        DevBuf *src[3] = {&c->I[c->cur], &c->mom, &c->counters};
-        for (int q = 0; q < 3; q++)
+        std::vector<DevBuf *> src = {&c->I[c->cur], &c->mom, &c->counters};
+        if (is_adaptive(c))
+            src.push_back(&c->ang[c->cur]);
+        for (DevBuf *d : src)
         {
-            saved[3 * k + q].reset(new DevBuf);
-            if (alloc(nullptr, *saved[3 * k + q], src[q]->bytes))
+            std::unique_ptr<DevBuf> copy(new DevBuf);
+            if (alloc(nullptr, *copy, d->bytes))
                 return bfail(b, GRLBM_ERR_CUDA, "autotune: cannot allocate a state copy");
-            BCU(cudaMemcpy(saved[3 * k + q]->p, src[q]->p, src[q]->bytes, cudaMemcpyDeviceToDevice));
+            BCU(cudaMemcpy(copy->p, d->p, d->bytes, cudaMemcpyDeviceToDevice));
+            saved.emplace_back(d, std::move(copy));
         }
     }
     cudaEvent_t e0, e1;
@@ -2599,7 +2631,9 @@ int grlbm_batch_autotune(grlbm_batch *b, int32_t trial_steps, int32_t *blocks_pe
         std::vector<std::pair<int64_t, std::vector<grlbm_ctx *>>> classes;
         for (grlbm_ctx *c : b->ctx)
         {
-            const int64_t key = (c->gd.nx_ * 65536 + c->gd.ny_) * 512 + c->st.n;
+            if (!is_tiled(c)) // the other forms have no tile
+                continue;
+            const int64_t key = ((c->gd.nx_ * 65536 + c->gd.ny_) * 512 + c->st.n) * 2 + (c->fast64 ? 1 : 0);
             auto it = std::find_if(classes.begin(), classes.end(), [&](const auto &x) { return x.first == key; });
             if (it == classes.end())
                 classes.push_back({key, {c}});
@@ -2624,7 +2658,11 @@ int grlbm_batch_autotune(grlbm_batch *b, int32_t trial_steps, int32_t *blocks_pe
             {
                 if (t[0] == bx && t[1] == by)
                     continue;
-                if (step32_smem(t[0], t[1], (int)c0->sl.sp, c0->st.n) > (size_t)kStep32MaxSmem)
+                size_t smem = 0;
+                int per_sm = 0;
+                if ((rc = tiled_fit(c0, t[0], t[1], &smem, &per_sm)))
+                    break;
+                if (smem > (size_t)kStep32MaxSmem || per_sm < 1)
                     continue;
                 for (grlbm_ctx *c : cls.second)
                     if ((rc = set_step32_tile(c, t[0], t[1])))
@@ -2648,14 +2686,10 @@ int grlbm_batch_autotune(grlbm_batch *b, int32_t trial_steps, int32_t *blocks_pe
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    // restore the saved state
-    for (size_t k = 0; k < n; k++)
-    {
-        grlbm_ctx *c = b->ctx[k];
-        DevBuf *dst[3] = {&c->I[c->cur], &c->mom, &c->counters};
-        for (int q = 0; q < 3; q++)
-            BCU(cudaMemcpy(dst[q]->p, saved[3 * k + q]->p, dst[q]->bytes, cudaMemcpyDeviceToDevice));
-    }
+    // restore the saved state (the trials leave every context's current
+    // buffer index as it was)
+    for (auto &sv : saved)
+        BCU(cudaMemcpy(sv.first->p, sv.second->p, sv.first->bytes, cudaMemcpyDeviceToDevice));
     if (rc)
         return rc;
     if ((rc = batch_build(b)))

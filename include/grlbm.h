@@ -292,16 +292,18 @@ int grlbm_get_tile_shape(const grlbm_ctx *ctx, int32_t *tile_x, int32_t *tile_y)
  * streaming): the ghost depth a band needs on each side. */
 int grlbm_departure_rows(grlbm_ctx *ctx, int32_t *rows);
 /* ---- batches ----------------------------------------------------------------
- * No counterpart in the reference.  Many GRLBM_PRECISION_FP32 problems on one
- * GPU (any grid sizes, direction counts, flat or curved streaming) stepped
- * together, replayed from CUDA graphs of 32 steps, in one of two kinds of
- * launch shape: one persistent kernel launch per time step over all problems'
- * tiles, or each problem's own step kernel with the problems' launch chains
- * running concurrently inside the graph.  Each problem's result is
- * bit-identical to stepping it alone; its
- * context stays usable (moments, intensities, statistics) between batch
- * steps.  Problems that keep source nodes active, and adaptive streaming
- * problems, are not batched (GRLBM_ERR_UNSUPPORTED).  A batch refers to its contexts: destroy it before
+ * No counterpart in the reference.  Many problems on one GPU (any form, grid
+ * size, direction count and streaming type, with or without active source
+ * nodes) stepped together, replayed from CUDA graphs of 32 steps, in one of
+ * two kinds of launch shape: each problem's own step with the problems'
+ * launch chains running concurrently inside the graph (the default: shape -4
+ * below), or one persistent kernel launch per time step over all problems'
+ * tiles (only when every problem is a GRLBM_PRECISION_FP32 fixed-streaming
+ * one without active source nodes).  Each problem's result is bit-identical
+ * to stepping it alone; its context stays usable (moments, intensities,
+ * statistics) between batch steps.  Problems that rebuild their tables every
+ * step (grlbm_set_update_tables_each_step) are not batched
+ * (GRLBM_ERR_UNSUPPORTED).  A batch refers to its contexts: destroy it before
  * them. */
 typedef struct grlbm_batch grlbm_batch;
 int grlbm_batch_create(grlbm_ctx *const *ctxs, int32_t n, grlbm_batch **out);
@@ -313,23 +315,27 @@ const char *grlbm_batch_last_error(const grlbm_batch *batch);
 int grlbm_batch_step(grlbm_batch *batch, int32_t n_steps);
 /* Sets the launch shape: blocks_per_sm in [1, occupancy limit] for the
  * persistent launch (with the problems' tiles as given or largest problem
- * first); 0 for the problems' own kernels launched concurrently, each on its
- * own persistent grid; -m (m = 1..8) for the same concurrent launches with
- * problem k's grid cut to ceil(m G_k w_k / sum w), at least one block, where
- * G_k is its own grid (its kernel's resident blocks on every SM) and w_k its
- * estimated cost (cells x (directions + 48), x 1.6 for curved streaming):
- * m GPUs' worth of resident blocks shared out, so that the problems' kernels
- * run side by side instead of each filling the GPU in turn. */
+ * first; GRLBM_ERR_UNSUPPORTED when the batch holds problems it does not
+ * step); 0 for the problems' own steps launched concurrently, each on its own
+ * grid; -m (m = 1..8) for the same concurrent launches with the grid of each
+ * tiled-form problem k (FP32 and fast FP64 fixed streaming) cut to
+ * ceil(m G_k w_k / sum w), at least one block, where G_k is its own grid (its
+ * kernel's resident blocks on every SM) and w_k its estimated cost (cells x
+ * (directions + 48), x 1.6 for curved streaming, x the form's cost against
+ * the FP32 fixed-streaming step): m GPUs' worth of resident blocks shared
+ * out, so that the problems' kernels run side by side instead of each
+ * filling the GPU in turn. */
 int grlbm_batch_set_shape(grlbm_batch *batch, int32_t blocks_per_sm, int32_t largest_first);
 /* Times trial_steps steps (rounded up to whole 32-step graphs, replayed as
  * grlbm_batch_step replays them, after an untimed one) for each launch shape
  * -- the persistent launch at resident blocks per SM (the occupancy limit and
  * up to two fewer) with the problems in the order given or largest problem
- * first, and the concurrent launches (0, -1, ..., -8) -- and keeps the
- * fastest; then, per size class (problems of one grid size and direction
- * count) holding at least 2% of the batch's estimated cost, largest class
- * first, times candidate tile shapes (grlbm_set_tile_shape) with the other
- * classes fixed and keeps the fastest.  Every problem is put back in the state it had before the
+ * first, where the batch allows it, and the concurrent launches (0, -1, ...,
+ * -8) -- and keeps the fastest; then, per size class (tiled-form problems of
+ * one form, grid size and direction count) holding at least 2% of the
+ * batch's estimated cost, largest class first, times candidate tile shapes
+ * (grlbm_set_tile_shape) with the other classes fixed and keeps the
+ * fastest.  Every problem is put back in the state it had before the
  * call.  The launch shape is returned in *blocks_per_sm and *largest_first
  * (either may be NULL), the tiles by grlbm_get_tile_shape. */
 int grlbm_batch_autotune(grlbm_batch *batch, int32_t trial_steps, int32_t *blocks_per_sm, int32_t *largest_first);

@@ -1,9 +1,10 @@
-"""Batched precision-form steps (grlbm_batch_*): problems of different grid
-sizes, direction counts and streaming types advanced together -- by one
-persistent launch per step or by their own kernels launched concurrently --
-must each match their single-problem run bit for bit, across graph-replayed
-and single steps, after autotuning (which must leave every problem as it
-was), and when a problem is also stepped on its own between batch steps."""
+"""Batched steps (grlbm_batch_*): problems of different forms, grid sizes,
+direction counts and streaming types advanced together -- by one persistent
+launch per step (FP32 fixed streaming) or by their own steps launched
+concurrently -- must each match their single-problem run bit for bit, across
+graph-replayed and single steps, after autotuning (which must leave every
+problem as it was), and when a problem is also stepped on its own between
+batch steps."""
 import numpy as np
 import pytest
 
@@ -69,20 +70,58 @@ def test_batch_shapes_match_single_problems(grlbm, W, shape):
             r.close()
 
 
-def test_batch_rejects_plain_source_and_adaptive_problems(grlbm, W):
-    c = W.batch_instances(count=1, seed=3, sizes=(24,), dirs=(8,), steps=2)[0]
-    with grlbm.prepare(c, grlbm.PLAIN_FP64) as r:
-        with pytest.raises(grlbm.GrlbmError) as e:
-            grlbm.Batch([r])
-        assert e.value.code == 4
-    beam = W.flat_beam(nx_=20, ny_=20, n_dir=8, steps=2)
-    with grlbm.prepare(beam, grlbm.PRECISION_FP32) as r:
-        with pytest.raises(grlbm.GrlbmError) as e:
-            grlbm.Batch([r])
-        assert e.value.code == 4
-    c = dict(c)
-    c["streaming_type"] = W.FLAT_ADAPTIVE
-    with grlbm.prepare(c, grlbm.PRECISION_FP32) as r:
+def _mixed_cases(grlbm, W):
+    """One small problem of every form and streaming type, and beams that keep
+    their source nodes active: (case, precision) pairs."""
+    P32, P64, F64 = grlbm.PRECISION_FP32, grlbm.PLAIN_FP64, grlbm.FAST_FP64
+    shell = W.curved_shell(nx_=30, ny_=26, n_dir=12, n_fourier=5, steps=40)
+    flat = next(c for c in W.batch_instances(count=8, seed=3, sizes=(24,), dirs=(8,), steps=40)
+                if c["streaming_type"] == W.FLAT_FIXED)
+    beam = W.flat_beam(nx_=20, ny_=18, n_dir=8, steps=40)
+    shell_ad, flat_ad = dict(shell), dict(flat)
+    shell_ad["streaming_type"] = W.CURVED_ADAPTIVE
+    flat_ad["streaming_type"] = W.FLAT_ADAPTIVE
+    return [(shell, P32), (flat, P32), (shell_ad, P32), (flat_ad, P64), (shell, P64), (shell, F64), (beam, P32),
+            (beam, F64), (flat, F64)]
+
+
+def test_mixed_batch_matches_single_problems(grlbm, W):
+    """Problems of every form in one batch -- FP32 fixed streaming (flat and
+    curved), FP32 and plain FP64 adaptive streaming, plain and fast FP64 fixed
+    streaming, and beams that keep their source nodes active -- each
+    bit-identical to its own run: in the default shape, after autotuning
+    (which must leave every problem as it was) across a 32-step graph, and on
+    the problems' own grids.  The persistent launch is refused for such a
+    batch (GRLBM_ERR_UNSUPPORTED), and so is a problem that rebuilds its
+    tables every step."""
+    cases = _mixed_cases(grlbm, W)
+    ref = []
+    for c, P in cases:
+        with grlbm.prepare(c, P) as r:
+            r.step(40)
+            ref.append((r.moments_if()["E"], r.intensity(), r.stats()["average_iterations"]))
+    probs = [grlbm.prepare(c, P) for c, P in cases]
+    try:
+        with grlbm.Batch(probs) as b:
+            b.step(5)               # the default shape: concurrent launches on shares
+            choice = b.autotune(3)
+            assert -8 <= choice["blocks_per_sm"] <= 0
+            b.step(32)              # one 32-step graph
+            with pytest.raises(grlbm.GrlbmError) as e:
+                b.set_shape(1, True)
+            assert e.value.code == 4
+            b.set_shape(0, True)
+            b.step(3)
+        for k, (r, (E, I, it)) in enumerate(zip(probs, ref)):
+            assert np.array_equal(r.moments_if()["E"], E), k
+            assert np.array_equal(r.intensity(), I), k
+            assert r.stats()["average_iterations"] == it, k
+    finally:
+        for r in probs:
+            r.close()
+    c, P = cases[4]
+    with grlbm.prepare(c, P) as r:
+        r.update_tables_each_step(True, c["rk_tol"])
         with pytest.raises(grlbm.GrlbmError) as e:
             grlbm.Batch([r])
         assert e.value.code == 4
