@@ -468,6 +468,41 @@ class Batch:
             pass
 
 
+def batch_cost(case: dict, precision: int = PRECISION_FP32) -> float:
+    """A problem's estimated step time in arbitrary units, as a batch's
+    launch shares estimate it (grlbm_batch_set_shape): cells x (directions +
+    48), x 1.6 for curved streaming, x the form's cost against the FP32
+    fixed-streaming step (fast FP64 1.9, plain FP64 4.7, adaptive streaming
+    4.9 in FP32 and 10.9 in plain FP64)."""
+    st = int(case["streaming_type"])
+    curved = st in (CURVED_FIXED, CURVED_ADAPTIVE)
+    adaptive = st in (FLAT_ADAPTIVE, CURVED_ADAPTIVE)
+    if precision == FAST_FP64:
+        form = 1.9
+    elif adaptive:
+        form = 4.9 if precision == PRECISION_FP32 else 10.9
+    else:
+        form = 1.0 if precision == PRECISION_FP32 else 4.7
+    return int(case["nx_"]) * int(case["ny_"]) * (int(case["n_dir"]) + 48.0) * (1.6 if curved else 1.0) * form
+
+
+def share_problems(cases: list, world: int, precision: int = PRECISION_FP32) -> list:
+    """Independent problems dealt to `world` GPUs as replicas, with no
+    communication between them: largest estimated cost (batch_cost) first,
+    each to the GPU with the least cost so far (the lower rank on a tie).
+    Returns each rank's problem indices in ascending order; every rank
+    computes the same deal."""
+    if world < 1:
+        raise ValueError("world must be at least 1")
+    load = [0.0] * world
+    out = [[] for _ in range(world)]
+    for k in sorted(range(len(cases)), key=lambda k: (-batch_cost(cases[k], precision), k)):
+        r = min(range(world), key=lambda r: (load[r], r))
+        load[r] += batch_cost(cases[k], precision)
+        out[r].append(k)
+    return [sorted(x) for x in out]
+
+
 def selftest_staging_wait(arrive: bool, limit_us: int, device: int = -1) -> dict:
     """One block's bounded wait on an mbarrier phase that nothing (arrive
     False) or one thread (arrive True) completes: {"completed", "waited_us"}."""

@@ -293,44 +293,61 @@ def run_configs(G, W, local):
     return out
 
 
-def run_batched(G, W, a, local):
+def run_batched(G, W, a, local, world=1, rank=0, pg=None, dev=None):
     """The batched form on 64 uneven problems (grid 64^2..512^2, 16..64
     directions, flat or Schwarzschild, seed 10): after autotuning the launch
     shape, `batch_steps` steps of all problems through the batch, against the
     same problems stepped through their own contexts (one stream each,
     enqueued back to back).  Both are timed after an untimed round of the same
-    length, which captures their 32-step graphs."""
+    length, which captures their 32-step graphs.  On N GPUs the problems are
+    dealt to the ranks as independent replicas (share_problems: balanced by
+    estimated cost, no communication); each rank batches its own, and a
+    timed region ends with the slowest rank."""
     import torch
-    cases = W.batch_instances(count=64, seed=10, steps=a.batch_steps)
+    allc = W.batch_instances(count=64, seed=10, steps=a.batch_steps)
+    units = sum(int(c["nx_"]) * int(c["ny_"]) * int(c["n_dir"]) for c in allc)
+    deal = G.share_problems(allc, world)
+    cases = [allc[k] for k in deal[rank]]
     probs = [G.prepare(c, G.PRECISION_FP32, device=local) for c in cases]
-    units = sum(int(c["nx_"]) * int(c["ny_"]) * int(c["n_dir"]) for c in cases)
+
+    def start():
+        torch.cuda.synchronize()
+        barrier(pg, dev)
+        torch.cuda.synchronize()
+        return time.perf_counter()
+
     try:
         for r in probs:  # an untimed round: graphs captured, caches warm
             r.step(a.batch_steps)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
+        t0 = start()
         for r in probs:
             r.step_async(a.batch_steps)
         for r in probs:
             r.sync()
-        single_s = time.perf_counter() - t0
-        with G.Batch(probs) as b:
-            choice = b.autotune(3)
-            b.step(a.batch_steps)
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            b.step(a.batch_steps)
-            batch_s = time.perf_counter() - t0
+        single_s = max_over_ranks(time.perf_counter() - t0, pg, dev)
+        b = G.Batch(probs) if probs else None  # a rank may be dealt no problem
+        try:
+            choice = b.autotune(3) if b else None
+            if b:
+                b.step(a.batch_steps)
+            t0 = start()
+            if b:
+                b.step(a.batch_steps)
+            batch_s = max_over_ranks(time.perf_counter() - t0, pg, dev)
+        finally:
+            if b:
+                b.close()
     finally:
         for r in probs:
             r.close()
-    return {"problems": len(cases), "cell_dir_per_step": units, "steps": a.batch_steps,
+    return {"problems": len(allc), "cell_dir_per_step": units, "steps": a.batch_steps,
             "value": units * a.batch_steps / batch_s, "unit": UNIT,
             "separate_contexts": units * a.batch_steps / single_s, "autotune": choice,
-            "timing": "host clock around the synchronous batch step (the autotuned launch shape: blocks_per_sm 0 = "
-                      "the problems' own kernels launched concurrently, -m = the same on cost-weighted shares of m "
-                      "GPUs' worth of resident blocks, >= 1 = one persistent launch per step; 32-step graphs), "
-                      "after an untimed round"}
+            "replicas": world, "problems_per_gpu": [len(x) for x in deal],
+            "timing": "host clock around the synchronous batch step, the slowest rank's (the autotuned launch "
+                      "shape, rank 0's: blocks_per_sm 0 = the problems' own kernels launched concurrently, -m = the "
+                      "same on cost-weighted shares of m GPUs' worth of resident blocks, >= 1 = one persistent "
+                      "launch per step; 32-step graphs), after an untimed round"}
 
 
 def run_adjoint(G, W, a, local):
@@ -500,7 +517,7 @@ def run_grlbm(a, world, rank, local, pg):
         if a.e2e_reps > 0:
             for name, prec in (("fp32", G.PRECISION_FP32), ("fp64", G.PLAIN_FP64), ("fast64", G.FAST_FP64)):
                 e2e[name] = run_e2e(G, W, case, prec, a, world, rank, local, pg, dev)
-        batched = run_batched(G, W, a, local) if a.batch_steps > 0 and world == 1 else None
+        batched = run_batched(G, W, a, local, world, rank, pg, dev) if a.batch_steps > 0 else None
         other = run_configs(G, W, local) if not a.no_configs and world == 1 else None
         adjoint = run_adjoint(G, W, a, local) if a.adjoint_steps > 0 and world == 1 else None
     clocks = clk.summary()
