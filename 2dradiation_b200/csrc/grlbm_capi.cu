@@ -436,24 +436,50 @@ int set_step32_tile(grlbm_ctx *ctx, int tx, int ty)
 // per SM against two for 8x2's wider patch: 64.5 against 72.6 us) and at 64
 // (8x2 drops to one block per SM: 128 against 91 us); 4x3 for FP64 at 64
 // directions (172 us, against 243-248 us for the 16-cell tiles at one block).
+//
+// Small grids leave most warps without a tile: with fewer 16-cell tiles (of
+// the rows stepped) than 0.4 (0.2) times the warps resident at that pick, the
+// rule picks among tiles of at most 12 (8) cells.  Swept at 64^2-200^2 with
+// 16-64 directions in both tiled forms, this took the FP32 step within 3% and
+// the fast FP64 step within 9% of the fastest shape, where the 16-cell pick
+// was up to 27% slower (64^2 x 64 curved, FP32: 11.3 against 15.1 us; the
+// 100^2 x 20 flat beam: 9.5 against 10.0 us).
 int default_step32_tile(grlbm_ctx *ctx)
 {
     static const int cand[][2] = {{8, 2}, {4, 4}, {16, 1}, {4, 3}, {3, 4}, {4, 2}, {2, 4}, {3, 3}, {2, 2}, {2, 1}, {1, 1}};
-    int best = -1, best_score = 0;
-    for (int ci = 0; ci < (int)(sizeof cand / sizeof cand[0]); ci++)
+    const int nc = (int)(sizeof cand / sizeof cand[0]);
+    int max_cells = kStep32UnitCells;
+    for (int pass = 0; pass < 2; pass++)
     {
-        size_t smem = 0;
-        int per_sm = 0;
-        const int rc = tiled_fit(ctx, cand[ci][0], cand[ci][1], &smem, &per_sm);
-        if (rc)
-            return rc;
-        const int score = cand[ci][0] * cand[ci][1] * std::min(per_sm, 3);
-        if (score > best_score)
-            best = ci, best_score = score;
+        int best = -1, best_score = 0, best_per_sm = 0;
+        for (int ci = 0; ci < nc; ci++)
+        {
+            if (cand[ci][0] * cand[ci][1] > max_cells)
+                continue;
+            size_t smem = 0;
+            int per_sm = 0;
+            const int rc = tiled_fit(ctx, cand[ci][0], cand[ci][1], &smem, &per_sm);
+            if (rc)
+                return rc;
+            const int score = cand[ci][0] * cand[ci][1] * std::min(per_sm, 3);
+            if (score > best_score)
+                best = ci, best_score = score, best_per_sm = per_sm;
+        }
+        if (best < 0)
+            return fail(ctx, GRLBM_ERR_ARGUMENT, "no tile of %d directions fits on an SM", ctx->st.n);
+        if (pass == 0)
+        {
+            int sms = 0;
+            CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+            const double warps = (double)best_per_sm * sms * (ctx->fast64 ? kStep64Warps : kStep32Warps);
+            const double tiles16 = (double)(ctx->gd.jhi - ctx->gd.jlo) * ctx->gd.nx_ / kStep32UnitCells;
+            max_cells = tiles16 < 0.2 * warps ? 8 : (tiles16 < 0.4 * warps ? 12 : kStep32UnitCells);
+            if (max_cells < kStep32UnitCells)
+                continue;
+        }
+        return set_step32_tile(ctx, cand[best][0], cand[best][1]);
     }
-    if (best < 0)
-        return fail(ctx, GRLBM_ERR_ARGUMENT, "no tile of %d directions fits on an SM", ctx->st.n);
-    return set_step32_tile(ctx, cand[best][0], cand[best][1]);
+    return GRLBM_OK;
 }
 
 
