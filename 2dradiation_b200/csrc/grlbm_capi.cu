@@ -439,11 +439,13 @@ int set_step32_tile(grlbm_ctx *ctx, int tx, int ty)
 //
 // Small grids leave most warps without a tile: with fewer 16-cell tiles (of
 // the rows stepped) than 0.4 (0.2) times the warps resident at that pick, the
-// rule picks among tiles of at most 12 (8) cells.  Swept at 64^2-200^2 with
+// rule picks among tiles of at most 12 (8) cells.  Swept at 64^2-128^2 with
 // 16-64 directions in both tiled forms, this took the FP32 step within 3% and
-// the fast FP64 step within 9% of the fastest shape, where the 16-cell pick
+// the fast FP64 step within 8% of the fastest shape, where the 16-cell pick
 // was up to 27% slower (64^2 x 64 curved, FP32: 11.3 against 15.1 us; the
-// 100^2 x 20 flat beam: 9.5 against 10.0 us).
+// 100^2 x 20 flat beam: 9.3 against 9.9 us).  Not covered: tile counts just
+// above one wave of warps (fast FP64 at 200^2 x 32: 4x4 34.8 us, its second
+// wave 40% full, against 31.6 us for 4x3).
 int default_step32_tile(grlbm_ctx *ctx)
 {
     static const int cand[][2] = {{8, 2}, {4, 4}, {16, 1}, {4, 3}, {3, 4}, {4, 2}, {2, 4}, {3, 3}, {2, 2}, {2, 1}, {1, 1}};
