@@ -28,6 +28,7 @@ MINKOWSKI, SCHWARZSCHILD, KERRSCHILD = 0, 1, 2
 FLAT_FIXED, FLAT_ADAPTIVE, CURVED_FIXED, CURVED_ADAPTIVE, GEODESIC_FIXED = 0, 1, 2, 3, 4
 MOMENTS, INTENSITIES = 0, 1
 PLAIN_FP64, PRECISION_FP32, FAST_FP64 = 0, 1, 2
+ROWS_ANGLES, ROWS_MOMENTS = 1, 2  # grlbm_copy_node_rows fields
 
 
 class GrlbmError(RuntimeError):
@@ -110,6 +111,8 @@ SIGNATURES = {
     "grlbm_row_bytes": ([C.c_void_p, C.POINTER(C.c_int64)], C.c_int),
     "grlbm_copy_rows": ([C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_int32], C.c_int),
     "grlbm_departure_rows": ([C.c_void_p, C.POINTER(C.c_int32)], C.c_int),
+    "grlbm_node_row_bytes": ([C.c_void_p, C.c_int32, C.POINTER(C.c_int64)], C.c_int),
+    "grlbm_copy_node_rows": ([C.c_void_p, C.c_int32, C.c_int64, C.c_int64, C.c_void_p, C.c_int32], C.c_int),
     "grlbm_set_tile_shape": ([C.c_void_p, C.c_int32, C.c_int32], C.c_int),
     "grlbm_write_log": ([C.c_void_p, C.c_char_p], C.c_int),
     "grlbm_host_write_log": ([C.POINTER(GridDesc), C.POINTER(MetricDesc), C.c_int32, C.c_int32, C.c_char_p,
@@ -364,6 +367,19 @@ class Radiation:
         v = C.c_int32()
         self._c(lib().grlbm_departure_rows(self.h, C.byref(v)))
         return v.value
+
+    def node_row_bytes(self, what: int) -> int:
+        """Bytes of one node row of ROWS_ANGLES or ROWS_MOMENTS."""
+        v = C.c_int64()
+        self._c(lib().grlbm_node_row_bytes(self.h, what, C.byref(v)))
+        return v.value
+
+    def copy_node_rows(self, what: int, j_first: int, n: int, buffer_ptr: int, to_buffer: bool):
+        """Rows [j_first, j_first + n) of the rotation angles (ROWS_ANGLES) or
+        the moments (ROWS_MOMENTS) to/from a device buffer (stream-ordered on
+        the context's stream)."""
+        self._c(lib().grlbm_copy_node_rows(self.h, what, j_first, n, C.c_void_p(buffer_ptr),
+                                           1 if to_buffer else 0))
 
     def stats(self) -> dict:
         s = Stats()

@@ -428,6 +428,42 @@ int set_step32_tile(grlbm_ctx *ctx, int tx, int ty)
     return GRLBM_OK;
 }
 
+// The node rows a curved adaptive step reads away from the band's cells: the
+// series of the departure's y about the node, c_0 - y + sum_k c_k b_k(phi)
+// with |b_k| <= sqrt 2, is bounded by |c_0 - y| + sqrt 2 sum_k |c_k| for every
+// angle; cells inside the excision stream zeros and are skipped.  The corners
+// are floor(jt) and floor(jt) + 1, and 1e-3 row absorbs the FP32 form's
+// roundings of the series and of jt.
+int adaptive_departure_rows(grlbm_ctx *ctx, int32_t *rows)
+{
+    if (!ctx->tables)
+        return fail(ctx, GRLBM_ERR_STATE, "departure rows need the Fourier coefficients");
+    cudaSetDevice(ctx->device);
+    CU(cudaStreamSynchronize(ctx->stream));
+    const int nf = ctx->ss.n;
+    const int64_t nx = ctx->gd.nx, nxy = ctx->gd.nxy, per = nxy * nf;
+    const int64_t first = ctx->gd.jlo * nx, count = (ctx->gd.jhi - ctx->gd.jlo) * nx;
+    std::vector<double> cy((size_t)count * nf);
+    std::vector<uint8_t> fl((size_t)count);
+    CU(cudaMemcpy(cy.data(), ctx->coef.as<double>() + 2 * per + first * nf, cy.size() * sizeof(double),
+                  cudaMemcpyDeviceToHost));
+    CU(cudaMemcpy(fl.data(), ctx->flags.as<uint8_t>() + first, fl.size(), cudaMemcpyDeviceToHost));
+    double far = 0.0;
+    for (int64_t n = 0; n < count; n++)
+    {
+        const int64_t i = (first + n) % nx, j = (first + n) / nx;
+        if (i < 1 || i > ctx->gd.nx_ || (fl[(size_t)n] & 2))
+            continue;
+        const double *c = cy.data() + (size_t)n * nf;
+        double b = std::fabs(c[0] - (ctx->geo.starty + (double)j * ctx->geo.dy));
+        for (int k = 1; k < nf; k++)
+            b += std::sqrt(2.0) * std::fabs(c[k]);
+        far = std::max(far, b / ctx->geo.dy);
+    }
+    *rows = (int32_t)std::floor(far + 1e-3) + 1;
+    return GRLBM_OK;
+}
+
 // The default tile: the candidate with the most cells times resident blocks
 // per SM (counted up to three), the first in this order on a tie.  Tile
 // sweeps at 400^2 curved scattering with 16 to 96 directions found this
@@ -1974,8 +2010,6 @@ int grlbm_set_rows(grlbm_ctx *ctx, int64_t j_first, int64_t j_end)
 {
     if (!ctx)
         return GRLBM_ERR_ARGUMENT;
-    if (is_adaptive(ctx))
-        return fail(ctx, GRLBM_ERR_UNSUPPORTED, "adaptive streaming is not split into bands");
     if (j_first < 1 || j_end > ctx->geo.ny - 1 || j_first >= j_end)
         return fail(ctx, GRLBM_ERR_ARGUMENT, "rows [%lld, %lld) outside the interior rows [1, %lld)",
                     (long long)j_first, (long long)j_end, (long long)(ctx->geo.ny - 1));
@@ -2029,6 +2063,52 @@ int grlbm_copy_rows(grlbm_ctx *ctx, int64_t j_first, int64_t n, void *buffer, in
     return GRLBM_OK;
 }
 
+int grlbm_node_row_bytes(const grlbm_ctx *ctx, int32_t what, int64_t *bytes)
+{
+    if (!ctx || !bytes)
+        return GRLBM_ERR_ARGUMENT;
+    if (what == GRLBM_ROWS_ANGLES)
+        *bytes = is_adaptive(ctx) ? ctx->gd.nx * (int64_t)sizeof(double) : 0;
+    else if (what == GRLBM_ROWS_MOMENTS)
+        *bytes = 6 * ctx->gd.nx * (int64_t)tsize(ctx);
+    else
+        return GRLBM_ERR_ARGUMENT;
+    return is_adaptive(ctx) || what == GRLBM_ROWS_MOMENTS ? GRLBM_OK : GRLBM_ERR_UNSUPPORTED;
+}
+
+int grlbm_copy_node_rows(grlbm_ctx *ctx, int32_t what, int64_t j_first, int64_t n, void *buffer, int32_t to_buffer)
+{
+    if (!ctx)
+        return GRLBM_ERR_ARGUMENT;
+    if (what != GRLBM_ROWS_ANGLES && what != GRLBM_ROWS_MOMENTS)
+        return fail(ctx, GRLBM_ERR_ARGUMENT, "unknown node-row field %d", what);
+    if (what == GRLBM_ROWS_ANGLES && !is_adaptive(ctx))
+        return fail(ctx, GRLBM_ERR_UNSUPPORTED, "rotation angles exist for adaptive streaming only");
+    if (!buffer || n < 0 || j_first < 0 || j_first + n > ctx->geo.ny)
+        return fail(ctx, GRLBM_ERR_ARGUMENT, "rows [%lld, %lld) outside the grid's %lld rows", (long long)j_first,
+                    (long long)(j_first + n), (long long)ctx->geo.ny);
+    if (n == 0)
+        return GRLBM_OK;
+    cudaSetDevice(ctx->device);
+    const size_t nx = (size_t)ctx->gd.nx;
+    if (what == GRLBM_ROWS_ANGLES)
+    {
+        double *ang = ctx->ang[ctx->cur].as<double>() + (size_t)j_first * nx;
+        const size_t bytes = (size_t)n * nx * sizeof(double);
+        CU(cudaMemcpyAsync(to_buffer ? buffer : ang, to_buffer ? ang : buffer, bytes, cudaMemcpyDeviceToDevice,
+                           ctx->stream));
+        return GRLBM_OK;
+    }
+    // the six moment planes: [plane][row][i] in the buffer
+    const size_t es = tsize(ctx), width = (size_t)n * nx * es, pitch = (size_t)ctx->gd.nxy * es;
+    char *mom = static_cast<char *>(ctx->mom.p) + (size_t)j_first * nx * es;
+    if (to_buffer)
+        CU(cudaMemcpy2DAsync(buffer, width, mom, pitch, width, 6, cudaMemcpyDeviceToDevice, ctx->stream));
+    else
+        CU(cudaMemcpy2DAsync(mom, pitch, buffer, width, width, 6, cudaMemcpyDeviceToDevice, ctx->stream));
+    return GRLBM_OK;
+}
+
 int grlbm_set_tile_shape(grlbm_ctx *ctx, int32_t tile_x, int32_t tile_y)
 {
     if (!ctx)
@@ -2056,8 +2136,14 @@ int grlbm_departure_rows(grlbm_ctx *ctx, int32_t *rows)
 {
     if (!ctx || !rows)
         return GRLBM_ERR_ARGUMENT;
-    if (is_adaptive(ctx))
-        return fail(ctx, GRLBM_ERR_UNSUPPORTED, "adaptive streaming is not split into bands");
+    if (ctx->run.streaming_type == GRLBM_FLAT_ADAPTIVE)
+    {
+        // any rotated direction: |dy| <= dt, the corners floor(jt) and floor(jt) + 1
+        *rows = (int32_t)std::floor(ctx->geo.dt / ctx->geo.dy) + 1;
+        return GRLBM_OK;
+    }
+    if (ctx->run.streaming_type == GRLBM_CURVED_ADAPTIVE)
+        return adaptive_departure_rows(ctx, rows);
     if (ctx->run.streaming_type == GRLBM_FLAT_FIXED)
     {
         int ext = 0;

@@ -17,6 +17,12 @@ step overlaps it with the band's inner rows -- those whose gathers stay
 within the band -- and updates the edge rows once the ghost rows are in:
 with NCCL every wait is a dependency between CUDA streams, and the host never
 waits on the GPU within a step.
+
+Adaptive streaming (src/Radiation.cpp:361-378, 415-453, 513-575) also reads
+the neighbours' rotation angles at the corners it gathers from and their
+flux moments in the angle update's 3x3 average, so its bands exchange the
+ghost rows' angles and the moment row next to the band too, and step the
+whole band after the exchange.
 """
 from __future__ import annotations
 
@@ -49,12 +55,25 @@ class RadiationRows:
         self.dtype = torch.float32 if rad.precision == 1 else torch.float64
         self.row_elems = self.row_bytes // (4 if rad.precision == 1 else 8)
         self.stream = torch.cuda.ExternalStream(rad.stream, device=device)
+        G = __import__(__package__ or "2dradiation_b200")
+        self.adaptive = int(rad.case["streaming_type"]) in (G.FLAT_ADAPTIVE, G.CURVED_ADAPTIVE)
+        # the other per-node fields of an adaptive band's exchange: (field, elements per row, dtype)
+        self.fields = [(G.ROWS_ANGLES, rad.node_row_bytes(G.ROWS_ANGLES) // 8, torch.float64),
+                       (G.ROWS_MOMENTS, rad.node_row_bytes(G.ROWS_MOMENTS) // self.dtype.itemsize,
+                        self.dtype)] if self.adaptive else []
 
     def buffer(self, rows: int) -> torch.Tensor:
         return torch.empty(rows * self.row_elems, dtype=self.dtype, device=self.device)
 
     def copy_rows(self, j_first: int, n: int, buf: torch.Tensor, to_buffer: bool):
         self.rad.copy_rows(j_first, n, buf.data_ptr(), to_buffer)
+
+    def field_buffer(self, k: int, rows: int) -> torch.Tensor:
+        _, elems, dtype = self.fields[k]
+        return torch.empty(rows * elems, dtype=dtype, device=self.device)
+
+    def copy_field_rows(self, k: int, j_first: int, n: int, buf: torch.Tensor, to_buffer: bool):
+        self.rad.copy_node_rows(self.fields[k][0], j_first, n, buf.data_ptr(), to_buffer)
 
     def step(self, n: int = 1):
         self.rad.step_async(n)
@@ -71,7 +90,10 @@ class Slab:
 
     `state` provides row_elems, dtype, buffer(rows), copy_rows(j, n, buf,
     to_buffer), step(n) and a `stream` usable as torch.cuda.stream(...) (or
-    None on CPU).  The band must be at least `ghost` rows high."""
+    None on CPU); for adaptive streaming (state.adaptive) also `fields` and
+    field_buffer(k, rows) / copy_field_rows(k, j, n, buf, to_buffer) for the
+    rotation angles (field 0, `ghost` rows) and the moments (field 1, one
+    row).  The band must be at least `ghost` rows high."""
 
     def __init__(self, state, rank: int, world: int, ny_: int, ghost: int, group=None):
         self.state, self.rank, self.world, self.group = state, rank, world, group
@@ -82,42 +104,56 @@ class Slab:
             raise ValueError(f"bands of {min(b - a for a, b in self.bands)} rows are thinner than the "
                              f"{ghost} ghost rows a step reads")
         g = ghost
-        self.send_lo = state.buffer(g) if rank > 0 else None
-        self.recv_lo = state.buffer(g) if rank > 0 else None
-        self.send_hi = state.buffer(g) if rank < world - 1 else None
-        self.recv_hi = state.buffer(g) if rank < world - 1 else None
+        self.adaptive = bool(getattr(state, "adaptive", False))
+        # per exchanged field (the intensities; for adaptive streaming also the
+        # angles and the moments): rows, and send/receive buffers below and
+        # above the band (None at the grid's edges)
+        self.parts = [(None, g)] + ([(0, g), (1, 1)] if self.adaptive else [])
+        self.bufs = []
+        for k, rows in self.parts:
+            make = (lambda n: state.buffer(n)) if k is None else (lambda n, k=k: state.field_buffer(k, n))
+            self.bufs.append({side: (make(rows), make(rows)) if (side == "lo" and rank > 0) or
+                              (side == "hi" and rank < world - 1) else None for side in ("lo", "hi")})
+
+    def _copy(self, k, j, n, buf, to_buffer):
+        if k is None:
+            self.state.copy_rows(j, n, buf, to_buffer)
+        else:
+            self.state.copy_field_rows(k, j, n, buf, to_buffer)
 
     def _ops(self):
-        lo, hi = self.band
         ops = []
-        if self.rank > 0:
-            ops.append(dist.P2POp(dist.isend, self.send_lo, self.rank - 1, self.group))
-            ops.append(dist.P2POp(dist.irecv, self.recv_lo, self.rank - 1, self.group))
-        if self.rank < self.world - 1:
-            ops.append(dist.P2POp(dist.isend, self.send_hi, self.rank + 1, self.group))
-            ops.append(dist.P2POp(dist.irecv, self.recv_hi, self.rank + 1, self.group))
+        for b in self.bufs:
+            if b["lo"] is not None:
+                ops.append(dist.P2POp(dist.isend, b["lo"][0], self.rank - 1, self.group))
+                ops.append(dist.P2POp(dist.irecv, b["lo"][1], self.rank - 1, self.group))
+            if b["hi"] is not None:
+                ops.append(dist.P2POp(dist.isend, b["hi"][0], self.rank + 1, self.group))
+                ops.append(dist.P2POp(dist.irecv, b["hi"][1], self.rank + 1, self.group))
         return ops
 
     def _send(self):
-        """Packs the `ghost` rows at each edge of the band and starts their
-        exchange with the neighbours; returns the pending requests."""
-        lo, hi, g, st = self.band[0], self.band[1], self.ghost, self.state
-        if self.send_lo is not None:
-            st.copy_rows(lo, g, self.send_lo, True)
-        if self.send_hi is not None:
-            st.copy_rows(hi - g, g, self.send_hi, True)
+        """Packs the rows at each edge of the band and starts their exchange
+        with the neighbours; returns the pending requests."""
+        lo, hi = self.band
+        for (k, rows), b in zip(self.parts, self.bufs):
+            if b["lo"] is not None:
+                self._copy(k, lo, rows, b["lo"][0], True)
+            if b["hi"] is not None:
+                self._copy(k, hi - rows, rows, b["hi"][0], True)
         return dist.batch_isend_irecv(self._ops())
 
     def _receive(self, reqs):
         """Waits for the exchange (NCCL: the state's stream waits) and
         unpacks the neighbours' rows next to the band."""
-        lo, hi, g, st = self.band[0], self.band[1], self.ghost, self.state
+        lo, hi = self.band
         for req in reqs:
             req.wait()
-        if self.recv_lo is not None:
-            st.copy_rows(lo - g, g, self.recv_lo, False)
-        if self.recv_hi is not None:
-            st.copy_rows(hi, g, self.recv_hi, False)
+        for (k, rows), b in zip(self.parts, self.bufs):
+            if b["lo"] is not None:
+                self._copy(k, lo - rows, rows, b["lo"][1], False)
+            if b["hi"] is not None:
+                self._copy(k, hi, rows, b["hi"][1], False)
 
     def exchange(self):
         """Sends the `ghost` rows at each edge of the band to the neighbour
@@ -135,6 +171,12 @@ class Slab:
         st = self.state
         if self.world == 1 or self.ghost == 0:
             st.step(n)
+            return
+        if self.adaptive:  # the angle update reads the moments next to the band: exchange, then step
+            with (torch.cuda.stream(st.stream) if st.stream is not None else _Null()):
+                for _ in range(n):
+                    self._receive(self._send())
+                    st.step(1)
             return
         lo, hi, g = self.band[0], self.band[1], self.ghost
         edges = [(lo, min(lo + g, hi)), (max(hi - g, lo + g), hi)]

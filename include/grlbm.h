@@ -274,22 +274,42 @@ int grlbm_row_bytes(const grlbm_ctx *ctx, int64_t *bytes);
  * GRLBM_FAST_FP64.
  * Enqueued on the context's stream; returns before it completes. */
 int grlbm_copy_rows(grlbm_ctx *ctx, int64_t j_first, int64_t n, void *buffer, int32_t to_buffer);
+/* The per-node fields a band of an adaptive-streaming run also takes from its
+ * neighbours before each step, besides the intensities: the current rotation
+ * angles (the stream rotates each corner's intensities by that node's angle)
+ * and the moments (the angle update averages the flux over the 3x3
+ * neighbourhood, src/Radiation.cpp:361-378). */
+#define GRLBM_ROWS_ANGLES 1  /* FP64, nx per row; adaptive streaming only */
+#define GRLBM_ROWS_MOMENTS 2 /* E, Fx, Fy, Pxx, Pxy, Pyy: 6 x nx values per row, FP32 in the precision form */
+/* Bytes of one node row of that field (GRLBM_ERR_UNSUPPORTED for angles
+ * without adaptive streaming). */
+int grlbm_node_row_bytes(const grlbm_ctx *ctx, int32_t what, int64_t *bytes);
+/* Copies node rows [j_first, j_first + n) of that field to (to_buffer = 1) or
+ * from (0) a contiguous device buffer of n * bytes-per-row, laid out [row][i]
+ * for the angles and [moment][row][i] for the moments.  Enqueued on the
+ * context's stream; returns before it completes. */
+int grlbm_copy_node_rows(grlbm_ctx *ctx, int32_t what, int64_t j_first, int64_t n, void *buffer, int32_t to_buffer);
 /* ---- tiles of the tiled steps -----------------------------------------------
  * No counterpart in the reference.  The GRLBM_PRECISION_FP32 and
  * GRLBM_FAST_FP64 steps of the fixed streaming types run as warps that each
  * take tiles of tile_x x tile_y cells (at most 16), staging each tile's
  * (tile_x + 2) x (tile_y + 2) node patch of the state in shared memory.  The
  * default tile maximises its cells times the kernel's resident blocks per SM
- * (counted up to two), over 8x2, 4x4, 16x1, 4x3, 3x4, 4x2, 2x4, 3x3, 2x2,
- * 2x1, 1x1 in that order of preference.  The result does not depend on the
- * tile.
+ * (counted up to three), over 8x2, 4x4, 16x1, 4x3, 3x4, 4x2, 2x4, 3x3, 2x2,
+ * 2x1, 1x1 in that order of preference; on small grids, with fewer 16-cell
+ * tiles than 0.4 (0.2) times the warps then resident, over the tiles of at
+ * most 12 (8) cells.  The result does not depend on the tile.
  * GRLBM_ERR_ARGUMENT for more than 16 cells or buffers that do not fit in
  * shared memory; GRLBM_ERR_UNSUPPORTED for other contexts. */
 int grlbm_set_tile_shape(grlbm_ctx *ctx, int32_t tile_x, int32_t tile_y);
 int grlbm_get_tile_shape(const grlbm_ctx *ctx, int32_t *tile_x, int32_t *tile_y);
-/* The most node rows away from its cell that any stream gather reads (from
- * the departure records of the last table build; from the stencil for flat
- * streaming): the ghost depth a band needs on each side. */
+/* The most node rows away from its cell that any stream gather reads: the
+ * ghost depth a band needs on each side.  From the departure records of the
+ * last table build (curved fixed streaming); from the stencil (flat fixed);
+ * from dt / dy for any rotated direction (flat adaptive); and for curved
+ * adaptive streaming from a bound of the departure's y series over every
+ * angle, |c_0 - y| + sqrt 2 sum_k |c_k|, over the band's cells outside the
+ * excision. */
 int grlbm_departure_rows(grlbm_ctx *ctx, int32_t *rows);
 /* ---- batches ----------------------------------------------------------------
  * No counterpart in the reference.  Many problems on one GPU (any form, grid

@@ -79,16 +79,67 @@ class CpuRows:
             self.state, self._next = self._next, None
 
 
-def _worker(rank, world, port, nx, ny_, nd, ghost, steps, out):
+class CpuAdaptiveRows(CpuRows):
+    """An adaptive-streaming stand-in: besides the intensities, per-node
+    angles and six moment planes.  A step first turns each band cell's angle
+    from the flux averaged over its 3x3 neighbourhood (the previous moments),
+    then streams from rows within `ghost` weighted by the source rows'
+    previous angles, then takes the band's moments -- the dependencies of
+    UpdateRotationMatrizes, the rotated gather and the collide."""
+
+    adaptive = True
+
+    def __init__(self, nx, ny, nd, ghost, band, seed):
+        super().__init__(nx, ny, nd, ghost, band, seed)
+        rng = np.random.default_rng(seed + 1)
+        self.ang = torch.from_numpy(rng.uniform(size=(ny, nx)))
+        self.mom = torch.from_numpy(rng.uniform(size=(6, ny, nx)))
+        self.fields = [(1, nx, torch.float64), (2, 6 * nx, torch.float64)]
+
+    def field_buffer(self, k, rows):
+        return torch.empty(rows * self.fields[k][1], dtype=torch.float64)
+
+    def copy_field_rows(self, k, j, n, buf, to_buffer):
+        view = buf.view(n, self.nx) if k == 0 else buf.view(6, n, self.nx)
+        src = self.ang[j:j + n, :] if k == 0 else self.mom[:, j:j + n, :]
+        if to_buffer:
+            view.copy_(src)
+        else:
+            src.copy_(view)
+
+    def step(self, n=1):
+        lo, hi = self.band
+        g = self.ghost
+        for _ in range(n):
+            ang = self.ang.clone()
+            flux = self.mom[1] + 2.0 * self.mom[2]
+            for j in range(lo, hi):
+                avg = sum(torch.roll(flux[j + b], shifts=a) for b in (-1, 0, 1) for a in (-1, 0, 1)) / 9.0
+                ang[j, 1:-1] = torch.atan2(avg[1:-1], 1.0 + self.mom[0, j, 1:-1])
+            new = self.state.clone()
+            s = self.state
+            for j in range(lo, hi):
+                rows = [min(max(j + k, 0), self.ny - 1) for k in range(-g, g + 1)]
+                mix = sum(torch.cos(self.ang[r, :]) * torch.roll(s[:, r, :], shifts=k, dims=1)
+                          for k, r in enumerate(rows))
+                new[:, j, 1:-1] = 0.5 * s[:, j, 1:-1] + 0.5 * torch.sin(ang[j, 1:-1]) * mix[:, 1:-1] / len(rows)
+            self.state, self.ang = new, ang
+            for q in range(6):
+                self.mom[q, lo:hi, :] = new[:, lo:hi, :].sum(dim=0) * (q + 1.0) + new[q % self.nd, lo:hi, :]
+
+
+def _worker(rank, world, port, nx, ny_, nd, ghost, steps, out, adaptive=False):
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
         S = slabs()
         band = S.partition(ny_, world)[rank]
-        rows = CpuRows(nx + 2, ny_ + 2, nd, ghost, band, seed=7)
+        rows = (CpuAdaptiveRows if adaptive else CpuRows)(nx + 2, ny_ + 2, nd, ghost, band, seed=7)
         slab = S.Slab(rows, rank, world, ny_, ghost)
         slab.step(steps)
         out[rank] = rows.state[:, band[0]:band[1], :].clone()
+        if adaptive:
+            out[("ang", rank)] = rows.ang[band[0]:band[1], :].clone()
         out[("energy", rank)] = slab.energy()
     finally:
         dist.destroy_process_group()
@@ -125,3 +176,30 @@ def test_multi_rank_exchange_equals_one_rank(ghost, world, ny_):
     # the all-reduced energy is the same on every rank and is the whole grid's
     assert len(set(energies)) == 1
     assert abs(energies[0] - single.energy()) <= 1e-12 * abs(single.energy())
+
+
+@pytest.mark.parametrize("ghost,world,ny_", [(1, 2, 8), (2, 3, 9)])
+def test_adaptive_exchange_equals_one_rank(ghost, world, ny_):
+    """Adaptive streaming's bands also exchange the ghost rows' angles and the
+    moment row next to the band, and step after the exchange: the ranks'
+    intensities and angles equal the one-rank run bit for bit."""
+    nx, nd, steps = 7, 3, 4
+    S = slabs()
+    single = CpuAdaptiveRows(nx + 2, ny_ + 2, nd, ghost, (1, ny_ + 1), seed=7)
+    S.Slab(single, 0, 1, ny_, ghost).step(steps)
+    ctx = mp.get_context("spawn")
+    with ctx.Manager() as m:
+        out = m.dict()
+        port = _free_port()
+        procs = [ctx.Process(target=_worker, args=(r, world, port, nx, ny_, nd, ghost, steps, out, True))
+                 for r in range(world)]
+        for p in procs:
+            p.start()
+        for p in procs:
+            p.join(120)
+            assert p.exitcode == 0
+        got = torch.cat([out[r] for r in range(world)], dim=1)
+        ang = torch.cat([out[("ang", r)] for r in range(world)], dim=0)
+    assert torch.equal(got, single.state[:, 1:ny_ + 1, :])
+    assert torch.equal(ang, single.ang[1:ny_ + 1, :])
+
