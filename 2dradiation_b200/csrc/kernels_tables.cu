@@ -326,24 +326,42 @@ __global__ void __launch_bounds__(128, 4) k_geodesic(GeodesicArgs a)
 
 // Fourier::GetCoefficients for the five fields of one interior cell
 // (src/FourierHarmonics.cpp:33-45): coef_k = sum_f (data_f w_f) B_k(phi_f),
-// accumulated over f in order.  One thread per (cell, field, k).
+// accumulated over f in order.  One thread per (cell, field) and kProjectK
+// consecutive k, which share each product data_f w_f (the load-bound
+// one-k-per-thread form issued three loads per multiply-add).
+constexpr int kProjectK = 4;
 __global__ void __launch_bounds__(128) k_fourier_project(ProjectArgs a)
 {
     const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int64_t per_field = a.cn * a.nf;
+    const int groups = (a.nf + kProjectK - 1) / kProjectK;
+    const int64_t per_field = a.cn * groups;
     if (tid >= 5 * per_field)
         return;
     const int field = (int)(tid / per_field);
     const int64_t r = tid - field * per_field;
-    const int64_t lc = r / a.nf; // the cell within the built range
-    const int k = (int)(r - lc * a.nf);
+    const int64_t lc = r / groups; // the cell within the built range
+    const int k0 = (int)(r - lc * groups) * kProjectK;
     const int64_t c = a.c0 + lc;
-    const double *d = a.data + field * per_field + lc * a.nf;
-    double acc = 0.0;
+    const double *d = a.data + ((int64_t)field * a.cn + lc) * a.nf;
+    double acc[kProjectK];
+#pragma unroll
+    for (int u = 0; u < kProjectK; u++)
+        acc[u] = 0.0;
     for (int f = 0; f < a.nf; f++)
-        acc += (d[f] * __ldg(a.ss_w + f)) * __ldg(a.basis + f * a.nf + k);
+    {
+        const double dw = d[f] * __ldg(a.ss_w + f);
+        const double *b = a.basis + f * a.nf + k0;
+#pragma unroll
+        for (int u = 0; u < kProjectK; u++)
+            if (k0 + u < a.nf)
+                acc[u] += dw * __ldg(b + u);
+    }
     const int64_t i = 1 + c % a.g.nx_, j = 1 + c / a.g.nx_;
-    a.coef[(int64_t)field * a.g.nxy * a.nf + (i + j * a.g.nx) * a.nf + k] = acc;
+    double *out = a.coef + (int64_t)field * a.g.nxy * a.nf + (i + j * a.g.nx) * a.nf + k0;
+#pragma unroll
+    for (int u = 0; u < kProjectK; u++)
+        if (k0 + u < a.nf)
+            out[u] = acc[u];
 }
 
 // Departure records from the Fourier series: what StreamCurvedFixed
@@ -523,7 +541,7 @@ void launch_geodesic(const GeodesicArgs &a, cudaStream_t s)
 }
 void launch_project(const ProjectArgs &a, cudaStream_t s)
 {
-    k_fourier_project<<<nblk(5 * a.cn * a.nf, 128), 128, 0, s>>>(a);
+    k_fourier_project<<<nblk(5 * a.cn * ((a.nf + kProjectK - 1) / kProjectK), 128), 128, 0, s>>>(a);
 }
 void launch_departure(const DepartureArgs &a, cudaStream_t s)
 {
