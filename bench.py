@@ -418,6 +418,13 @@ def run_profile(a):
     if a.profile == "batch":
         probs = [G.prepare(c, G.PRECISION_FP32) for c in W.batch_instances(count=a.profile_batch, seed=10)]
         with G.Batch(probs) as b:
+            # the persistent kernel at the most resident blocks per SM it allows
+            for bps in (4, 3, 2, 1):
+                try:
+                    b.set_shape(bps, True)
+                    break
+                except G.GrlbmError:
+                    continue
             for _ in range(n):
                 b.step(1)
         print("profile: batch of", a.profile_batch, "E sum", float(sum(r.moments_if()["E"].sum() for r in probs)))
