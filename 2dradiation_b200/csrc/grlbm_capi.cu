@@ -2138,8 +2138,9 @@ int grlbm_departure_rows(grlbm_ctx *ctx, int32_t *rows)
         return GRLBM_ERR_ARGUMENT;
     if (ctx->run.streaming_type == GRLBM_FLAT_ADAPTIVE)
     {
-        // any rotated direction: |dy| <= dt, the corners floor(jt) and floor(jt) + 1
-        *rows = (int32_t)std::floor(ctx->geo.dt / ctx->geo.dy) + 1;
+        // any rotated direction: |dy| <= dt, the corners floor(jt) and floor(jt)
+        // + 1 (1e-3 row absorbs the FP32 form's rounding of jt)
+        *rows = (int32_t)std::floor(ctx->geo.dt / ctx->geo.dy + 1e-3) + 1;
         return GRLBM_OK;
     }
     if (ctx->run.streaming_type == GRLBM_CURVED_ADAPTIVE)
